@@ -1,0 +1,204 @@
+"""Seeded synthetic tetrahedral meshes for the solver's workloads.
+
+The reference reads its meshes from NVTR/TecPlot files (Library/Math.h:150-291,
+`math::SimpleGrid` = {nvtr, nvkat, xyz}, Library/Math.h:26-33).  These
+generators build the same three arrays in memory:
+
+  xyz   float64 [n_nodes, 3]   node coordinates
+  tets  int32   [n_tets, 4]    node ids per tetrahedron (the reference's nvtr)
+  mat   int32   [n_tets]       material / domain id per tetrahedron (nvkat)
+
+Every hexahedron of an n x n x n grid on the unit cube is split into the six
+Kuhn (Freudenthal) tetrahedra that share the cell diagonal 0-7, with corner b of
+cell (i, j, k) at (i + (b & 1), j + ((b >> 1) & 1), k + ((b >> 2) & 1)) and node
+id i + (n+1) * (j + (n+1) * k).  Interior nodes may be jittered by a seeded
+uniform offset.  All randomness comes from numpy's PCG64 generator seeded
+explicitly, so every workload is reproducible from its seed.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+# corner sets of the six Kuhn tetrahedra of a hexahedron (corners 0..7 as above)
+KUHN_TETS = np.array(
+    [[0, 1, 3, 7], [0, 1, 5, 7], [0, 2, 3, 7], [0, 2, 6, 7], [0, 4, 5, 7], [0, 4, 6, 7]], dtype=np.int64
+)
+
+
+@dataclass
+class Mesh:
+    xyz: np.ndarray
+    tets: np.ndarray
+    mat: np.ndarray
+    n: int = 0
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def n_nodes(self) -> int:
+        return int(self.xyz.shape[0])
+
+    @property
+    def n_tets(self) -> int:
+        return int(self.tets.shape[0])
+
+
+def node_id(n: int, i, j, k):
+    return i + (n + 1) * (j + (n + 1) * k)
+
+
+def kuhn_cube(n: int, jitter: float = 0.0, seed: int = 0, origin=(0.0, 0.0, 0.0), size: float = 1.0) -> Mesh:
+    """n^3 hexahedra on [origin, origin+size]^3, six Kuhn tets each.
+
+    jitter: interior nodes move by U(-jitter*h, +jitter*h) per axis (h = size/n).
+    """
+    h = size / n
+    g = np.arange(n + 1, dtype=np.float64)
+    k, j, i = np.meshgrid(g, g, g, indexing="ij")  # node id = i + (n+1)(j + (n+1)k)
+    xyz = np.stack([i.ravel() * h + origin[0], j.ravel() * h + origin[1], k.ravel() * h + origin[2]], axis=1)
+    if jitter > 0.0:
+        ii, jj, kk = i.ravel().astype(np.int64), j.ravel().astype(np.int64), k.ravel().astype(np.int64)
+        interior = (ii > 0) & (ii < n) & (jj > 0) & (jj < n) & (kk > 0) & (kk < n)
+        rng = np.random.default_rng(seed)
+        off = rng.uniform(-jitter * h, jitter * h, size=(int(interior.sum()), 3))
+        xyz[interior] += off
+    c = np.arange(n, dtype=np.int64)
+    ck, cj, ci = np.meshgrid(c, c, c, indexing="ij")
+    ci, cj, ck = ci.ravel(), cj.ravel(), ck.ravel()
+    corners = np.stack(
+        [node_id(n, ci + (b & 1), cj + ((b >> 1) & 1), ck + ((b >> 2) & 1)) for b in range(8)], axis=1
+    )  # [n^3, 8]
+    tets = corners[:, KUHN_TETS].reshape(-1, 4).astype(np.int32)
+    mat = np.zeros(tets.shape[0], dtype=np.int32)
+    return Mesh(xyz=xyz, tets=tets, mat=mat, n=n, meta={"jitter": jitter, "seed": seed})
+
+
+def nodes_on_plane(mesh: Mesh, axis: int, value: float, tol: float = 1e-12) -> np.ndarray:
+    """Ids of nodes whose coordinate `axis` equals value, ascending."""
+    return np.nonzero(np.abs(mesh.xyz[:, axis] - value) < tol)[0].astype(np.int32)
+
+
+def boundary_faces_on_plane(mesh: Mesh, axis: int, value: float, tol: float = 1e-12):
+    """Triangles of tets with three nodes on the plane: (faces [m,3], base element [m]).
+
+    Face node order follows the tet's local node order, the way the reference's
+    Neumann reader collects them (FEM/FEM_Main.cpp:819-872, GetConfluence order).
+    """
+    on = np.abs(mesh.xyz[:, axis] - value) < tol
+    flags = on[mesh.tets]  # [E,4]
+    hit = np.nonzero(flags.sum(axis=1) == 3)[0]
+    faces = np.empty((hit.size, 3), dtype=np.int32)
+    for r, e in enumerate(hit):
+        faces[r] = mesh.tets[e][flags[e]]
+    return faces, hit.astype(np.int32)
+
+
+def tet_centroids(mesh: Mesh) -> np.ndarray:
+    return mesh.xyz[mesh.tets].mean(axis=1)
+
+
+def random_spheres(count: int, rmin: float, rmax: float, seed: int, max_tries: int = 1_000_000):
+    """`count` non-overlapping spheres in the unit cube: centres U(0,1)^3,
+    radii U(rmin, rmax), rejection-sampled in draw order."""
+    rng = np.random.default_rng(seed)
+    centres = np.empty((count, 3))
+    radii = np.empty(count)
+    m = 0
+    tries = 0
+    while m < count:
+        tries += 1
+        if tries > max_tries:
+            raise RuntimeError(f"could only place {m} of {count} spheres")
+        c = rng.uniform(0.0, 1.0, size=3)
+        r = rng.uniform(rmin, rmax)
+        if m and np.any(np.linalg.norm(centres[:m] - c, axis=1) < radii[:m] + r):
+            continue
+        centres[m] = c
+        radii[m] = r
+        m += 1
+    return centres, radii
+
+
+def mark_spheres(mesh: Mesh, centres: np.ndarray, radii: np.ndarray, material: int = 1) -> None:
+    """Sets mat = material for every tet whose centroid lies inside a sphere.
+    Only tets of the structured grid cells overlapping each sphere's bounding
+    box are tested (the mesh must come from kuhn_cube on the unit cube)."""
+    n = mesh.n
+    cen = tet_centroids(mesh)
+    for c, r in zip(centres, radii):
+        lo = np.clip(np.floor((c - r) * n).astype(int) - 1, 0, n - 1)
+        hi = np.clip(np.floor((c + r) * n).astype(int) + 1, 0, n - 1)
+        ci = np.arange(lo[0], hi[0] + 1)
+        cj = np.arange(lo[1], hi[1] + 1)
+        ck = np.arange(lo[2], hi[2] + 1)
+        kk, jj, ii = np.meshgrid(ck, cj, ci, indexing="ij")
+        cells = (ii + n * (jj + n * kk)).ravel()
+        tet_ids = (cells[:, None] * 6 + np.arange(6)[None, :]).ravel()
+        inside = np.sum((cen[tet_ids] - c) ** 2, axis=1) < r * r
+        mesh.mat[tet_ids[inside]] = material
+
+
+# ----------------------------------------------------------------------------------------------
+# Workloads (sizes and distributions of the synthetic configurations)
+# ----------------------------------------------------------------------------------------------
+
+@dataclass
+class ElasticProblem:
+    mesh: Mesh
+    E: np.ndarray
+    nu: np.ndarray
+    bc_nodes: np.ndarray      # Dirichlet nodes (ascending)
+    bc_mask: np.ndarray       # bit 0/1/2 = x/y/z component fixed
+    bc_values: np.ndarray     # [m, 3]
+    faces: np.ndarray         # traction triangles [f, 3]
+    face_elem: np.ndarray     # base tetrahedron of each triangle
+    traction: np.ndarray      # [f, 3]
+
+
+@dataclass
+class ScalarProblem:
+    mesh: Mesh
+    sigma: np.ndarray
+    bc_nodes: np.ndarray
+    bc_values: np.ndarray
+
+
+def cube_elastic(n: int = 20, jitter: float = 0.1, seed: int = 1234, E: float = 1.0, nu: float = 0.3,
+                 n_spheres: int = 0, contrast: float = 1.0, sphere_seed: int = 7,
+                 rmin: float = 0.02, rmax: float = 0.06) -> ElasticProblem:
+    """Elastic cube: u = 0 on z = 0 (all three components), traction (0, 0, -1)
+    on the z = 1 faces; optional spherical inclusions with E * contrast."""
+    mesh = kuhn_cube(n, jitter=jitter, seed=seed)
+    Es, nus = [E], [nu]
+    if n_spheres > 0:
+        centres, radii = random_spheres(n_spheres, rmin, rmax, sphere_seed)
+        mark_spheres(mesh, centres, radii, 1)
+        Es.append(E * contrast)
+        nus.append(nu)
+    bc = nodes_on_plane(mesh, 2, 0.0)
+    faces, face_elem = boundary_faces_on_plane(mesh, 2, 1.0)
+    traction = np.tile(np.array([0.0, 0.0, -1.0]), (faces.shape[0], 1))
+    return ElasticProblem(
+        mesh=mesh, E=np.array(Es), nu=np.array(nus), bc_nodes=bc,
+        bc_mask=np.full(bc.size, 7, dtype=np.int32), bc_values=np.zeros((bc.size, 3)),
+        faces=faces, face_elem=face_elem, traction=traction,
+    )
+
+
+def cube_scalar(n: int = 100, jitter: float = 0.0, seed: int = 1234, n_spheres: int = 200, contrast: float = 100.0,
+                sphere_seed: int = 2024, rmin: float = 0.02, rmax: float = 0.06) -> ScalarProblem:
+    """Electrostatics cube: permittivity 1, `contrast` inside spheres; potential 1
+    on x = 0 and 0 on x = 1.  Dirichlet nodes are listed x = 0 face first, then
+    x = 1 face, each ascending, as two boundary "types" would be read."""
+    mesh = kuhn_cube(n, jitter=jitter, seed=seed)
+    sig = [1.0]
+    if n_spheres > 0:
+        centres, radii = random_spheres(n_spheres, rmin, rmax, sphere_seed)
+        mark_spheres(mesh, centres, radii, 1)
+        sig.append(contrast)
+    left = nodes_on_plane(mesh, 0, 0.0)
+    right = nodes_on_plane(mesh, 0, 1.0)
+    nodes = np.concatenate([left, right]).astype(np.int32)
+    vals = np.concatenate([np.ones(left.size), np.zeros(right.size)])
+    return ScalarProblem(mesh=mesh, sigma=np.array(sig), bc_nodes=nodes, bc_values=vals)

@@ -1,0 +1,193 @@
+"""Test infrastructure only: Python bindings of the two oracle libraries.
+
+  ref()   -> oracle/_ref/libfemref.so      the reference's own C++ compiled from its
+                                           sources (oracle/ref_harness.cpp, oracle/Makefile)
+  port()  -> oracle/_build/libfemoracle.so the plain-C restatement (oracle/femoracle.c)
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference arm
+may import this package.  The product (multiscalefemsolver3d_b200) never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_SO = os.path.join(HERE, "_ref", "libfemref.so")
+PORT_SO = os.path.join(HERE, "_build", "libfemoracle.so")
+
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+
+
+class _RefCsr(C.Structure):
+    _fields_ = [("n", C.c_int), ("nnz", C.c_longlong), ("row_ptr", C.POINTER(C.c_int)),
+                ("col", C.POINTER(C.c_int)), ("val", C.POINTER(C.c_double)),
+                ("F", C.POINTER(C.c_double)), ("X", C.POINTER(C.c_double))]
+
+
+@dataclass
+class Csr:
+    """CSR with the diagonal included; row order [down asc, diag, up asc]."""
+    row_ptr: np.ndarray
+    col: np.ndarray
+    val: np.ndarray
+    F: np.ndarray
+    X: np.ndarray
+
+    @property
+    def n(self) -> int:
+        return self.row_ptr.size - 1
+
+    def to_scipy(self):
+        import scipy.sparse as sp
+        return sp.csr_matrix((self.val, self.col, self.row_ptr), shape=(self.n, self.n))
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+class RefLib:
+    """The reference compiled in place (oracle/_ref/libfemref.so)."""
+
+    def __init__(self, path: str = REF_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: build it with `make -C oracle ref`")
+        L = C.CDLL(path)
+        self.L = L
+        L.ref_set_quiet.argtypes = [C.c_int]
+        L.ref_free_csr.argtypes = [C.POINTER(_RefCsr)]
+        L.ref_elastic_local.argtypes = [_f64p, C.c_double, C.c_double, _f64p]
+        L.ref_scalar_local.argtypes = [_f64p, C.c_double, _f64p]
+        mesh_args = [C.c_int, _f64p, C.c_int, _i32p, _i32p]
+        L.ref_elastic_system.argtypes = mesh_args + [C.c_int, _f64p, _f64p, C.c_int, _i32p, _i32p, _f64p,
+                                                     C.c_int, _i32p, _i32p, _f64p, C.c_int, C.c_int,
+                                                     C.POINTER(_RefCsr), _f64p]
+        L.ref_elastic_driver.argtypes = mesh_args + [C.c_int, _f64p, _f64p, C.c_int, _i32p, _i32p, _f64p,
+                                                     C.c_int, _i32p, _i32p, _f64p, C.c_int, C.c_double,
+                                                     _f64p, C.POINTER(C.c_double)]
+        L.ref_scalar_system.argtypes = mesh_args + [C.c_int, _f64p, C.c_int, _i32p, _f64p, C.c_int, C.c_int,
+                                                    C.POINTER(_RefCsr), _f64p]
+        L.ref_scalar_driver.argtypes = mesh_args + [C.c_int, _f64p, C.c_int, _i32p, _f64p, C.c_int, C.c_double,
+                                                    _f64p, C.POINTER(C.c_double)]
+        L.ref_cssd_solve.argtypes = [C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_int, C.c_double,
+                                     C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.ref_ssor_apply.argtypes = [C.c_int, _i32p, _i32p, _f64p, C.c_double, _f64p, _f64p]
+        for f in ("ref_elastic_local", "ref_scalar_local", "ref_elastic_system", "ref_elastic_driver",
+                  "ref_scalar_system", "ref_scalar_driver", "ref_cssd_solve", "ref_ssor_apply"):
+            getattr(L, f).restype = C.c_int
+        L.ref_set_quiet(1)
+
+    @staticmethod
+    def _take(out: _RefCsr) -> Csr:
+        n, nnz = out.n, out.nnz
+        c = Csr(
+            row_ptr=np.ctypeslib.as_array(out.row_ptr, shape=(n + 1,)).copy(),
+            col=np.ctypeslib.as_array(out.col, shape=(nnz,)).copy(),
+            val=np.ctypeslib.as_array(out.val, shape=(nnz,)).copy(),
+            F=np.ctypeslib.as_array(out.F, shape=(n,)).copy(),
+            X=np.ctypeslib.as_array(out.X, shape=(n,)).copy(),
+        )
+        return c
+
+    def elastic_local(self, xyz4, E=1.0, nu=0.3) -> np.ndarray:
+        K = np.zeros(144)
+        rc = self.L.ref_elastic_local(_c(xyz4, np.float64).ravel(), E, nu, K)
+        assert rc == 0
+        return K.reshape(4, 4, 3, 3)
+
+    def scalar_local(self, xyz4, sigma=1.0) -> np.ndarray:
+        K = np.zeros(16)
+        rc = self.L.ref_scalar_local(_c(xyz4, np.float64).ravel(), sigma, K)
+        assert rc == 0
+        return K.reshape(4, 4)
+
+    def elastic_system(self, p, stage: int = 1, nthreads: int = 1):
+        m = p.mesh
+        out = _RefCsr()
+        t = np.zeros(2)
+        rc = self.L.ref_elastic_system(
+            m.n_nodes, _c(m.xyz, np.float64).ravel(), m.n_tets, _c(m.tets, np.int32).ravel(), _c(m.mat, np.int32),
+            len(p.E), _c(p.E, np.float64), _c(p.nu, np.float64),
+            len(p.bc_nodes), _c(p.bc_nodes, np.int32), _c(p.bc_mask, np.int32), _c(p.bc_values, np.float64).ravel(),
+            len(p.face_elem), _c(p.faces, np.int32).ravel(), _c(p.face_elem, np.int32),
+            _c(p.traction, np.float64).ravel(), nthreads, stage, C.byref(out), t)
+        assert rc == 0, rc
+        c = self._take(out)
+        self.L.ref_free_csr(C.byref(out))
+        return c, t
+
+    def elastic_driver(self, p, min_residual: float = 1e-10, nthreads: int = 1):
+        m = p.mesh
+        sol = np.zeros(3 * m.n_nodes)
+        wall = C.c_double(0)
+        rc = self.L.ref_elastic_driver(
+            m.n_nodes, _c(m.xyz, np.float64).ravel(), m.n_tets, _c(m.tets, np.int32).ravel(), _c(m.mat, np.int32),
+            len(p.E), _c(p.E, np.float64), _c(p.nu, np.float64),
+            len(p.bc_nodes), _c(p.bc_nodes, np.int32), _c(p.bc_mask, np.int32), _c(p.bc_values, np.float64).ravel(),
+            len(p.face_elem), _c(p.faces, np.int32).ravel(), _c(p.face_elem, np.int32),
+            _c(p.traction, np.float64).ravel(), nthreads, min_residual, sol, C.byref(wall))
+        assert rc == 0, rc
+        return sol, wall.value
+
+    def scalar_system(self, p, stage: int = 1, nthreads: int = 1):
+        m = p.mesh
+        out = _RefCsr()
+        t = np.zeros(2)
+        rc = self.L.ref_scalar_system(
+            m.n_nodes, _c(m.xyz, np.float64).ravel(), m.n_tets, _c(m.tets, np.int32).ravel(), _c(m.mat, np.int32),
+            len(p.sigma), _c(p.sigma, np.float64), len(p.bc_nodes), _c(p.bc_nodes, np.int32),
+            _c(p.bc_values, np.float64), nthreads, stage, C.byref(out), t)
+        assert rc == 0, rc
+        c = self._take(out)
+        self.L.ref_free_csr(C.byref(out))
+        return c, t
+
+    def scalar_driver(self, p, min_residual: float = 1e-10, nthreads: int = 1):
+        m = p.mesh
+        sol = np.zeros(m.n_nodes)
+        wall = C.c_double(0)
+        rc = self.L.ref_scalar_driver(
+            m.n_nodes, _c(m.xyz, np.float64).ravel(), m.n_tets, _c(m.tets, np.int32).ravel(), _c(m.mat, np.int32),
+            len(p.sigma), _c(p.sigma, np.float64), len(p.bc_nodes), _c(p.bc_nodes, np.int32),
+            _c(p.bc_values, np.float64), nthreads, min_residual, sol, C.byref(wall))
+        assert rc == 0, rc
+        return sol, wall.value
+
+    def cssd_solve(self, method: int, A: Csr, X0=None, maxiter: int = 100000, tol: float = 1e-10, nthreads: int = 1):
+        """method: 0 MSG (CG), 1 SSOR(0.75)-PCG, 2 BiCG_Stab, 3 BCG_Stab2, 4 GMRES(5)."""
+        X = _c(A.X if X0 is None else X0, np.float64).copy()
+        res = C.c_double(0)
+        wall = C.c_double(0)
+        rc = self.L.ref_cssd_solve(method, A.n, _c(A.row_ptr, np.int32), _c(A.col, np.int32), _c(A.val, np.float64),
+                                   _c(A.F, np.float64), X, maxiter, tol, nthreads, C.byref(res), C.byref(wall))
+        assert rc == 0, rc
+        return X, res.value, wall.value
+
+    def ssor_apply(self, A: Csr, r, w: float = 0.75):
+        z = np.zeros(A.n)
+        rc = self.L.ref_ssor_apply(A.n, _c(A.row_ptr, np.int32), _c(A.col, np.int32), _c(A.val, np.float64), w,
+                                   _c(r, np.float64), z)
+        assert rc == 0
+        return z
+
+
+_ref_singleton = None
+
+
+def ref() -> RefLib:
+    global _ref_singleton
+    if _ref_singleton is None:
+        _ref_singleton = RefLib()
+    return _ref_singleton
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+from .port import PortLib, port, port_available  # noqa: E402  (restatement bindings)
