@@ -1,0 +1,391 @@
+"""Benchmark: time to a 1e-8 relative residual on the 100^3 electrostatics workload.
+
+Workload (seeded, synthetic; no dataset): unit cube, 100^3 hexahedra split into
+6 Kuhn tetrahedra each (1,030,301 nodes = DOF, 6,000,000 tets), permittivity 1
+and 100 inside 200 non-overlapping spheres (centres U(0,1)^3, radii
+U(0.02, 0.06)), potential 1 on x = 0 and 0 on x = 1.  The reference's
+stiffness-only FEM_forBaseEliptic path (FEM/FEM.h:398-717).
+
+One step = the hot path on the resident mesh: coloured assembly into the
+portrait, Dirichlet rows + column sweep, X = F, and the solve to
+||F - AX|| / ||F|| <= 1e-8 with FP32 Jacobi-PCG inside FP64 iterative
+refinement.  The plain FP64 CG (the reference's MSG method) and FP64
+Jacobi-PCG steps are timed beside it on the same system.
+
+  value  : mean device time of one step (CUDA events on the system's stream),
+           inputs resident in HBM, L2 flushed between steps
+  e2e    : the C-ABI driver msfem_fem_scalar_driver with host buffers: mesh and
+           boundary arrays copied in, portrait built, assembled, solved, the
+           solution copied back -- wall time around the synchronous call
+  roofline: the FP32 SELL-32 SpMV (the dominant kernel), algorithmic bytes per
+           product / mean launch time (CUDA events), vs the measured HBM peak
+
+`--impl reference` runs the reference's own C++ driver (compiled from its
+sources into oracle/_ref) on the host cores: each step is the driver at a
+bounded sample size (n = 30 by default) and the time is scaled to n = 100 by
+(N_100 / N_sample)^(4/3) (CG iterations grow like 1/h, work per iteration
+like N).  Multi-GPU: each rank solves its own replica (the path does not
+shard); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time to 1e-8 rel. residual: learned+mixed vs plain FP64 CG, same B200; SpMV GB/s"
+UNIT = "ms"
+TOL = 1e-8
+SAMPLE_N = 30
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=100)
+    ap.add_argument("--sample-n", type=int, default=SAMPLE_N)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(n):
+    from multiscalefemsolver3d_b200 import meshgen
+    return meshgen.cube_scalar(n=n, n_spheres=200, contrast=100.0, rmin=0.02, rmax=0.06, sphere_seed=2024)
+
+
+def config(n, p=None, extra=None):
+    c = {"workload": f"electrostatics {n}^3 Kuhn tets, 200 spheres eps 1:100, Dirichlet x=0/x=1",
+         "n_dofs": (n + 1) ** 3, "n_tets": 6 * n ** 3, "tol": TOL,
+         "solver": "FP32 Jacobi-PCG inside FP64 iterative refinement",
+         "l2": "flushed between steps (256 MiB write) and inputs > L2", "parallelism": "replicas"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ---------------------------------------------------------------- distributed plumbing
+
+class Dist:
+    def __init__(self, want):
+        self.rank = int(os.environ.get("RANK", 0))
+        self.world = int(os.environ.get("WORLD_SIZE", 1))
+        self.local = int(os.environ.get("LOCAL_RANK", 0))
+        self.pg = None
+        if self.world > 1:
+            import torch
+            import torch.distributed as dist
+            from datetime import timedelta
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend, timeout=timedelta(seconds=600))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------- clocks
+
+class Clocks:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index=0):
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.dev = device_index
+
+    def __enter__(self):
+        try:
+            uuid = None
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
+            sel = ["-i", uuid if uuid.startswith("GPU-") else f"GPU-{uuid}"]
+        except Exception:
+            sel = []
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", *sel, f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except Exception:
+            return out
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip().lower().startswith("active"):
+                        reasons.add(nm)
+            except Exception:
+                continue
+        if sm:
+            out.update(sm_mhz=statistics.median(sm), sm_max_mhz=max(mx), reasons=sorted(reasons), samples=len(sm))
+        return out
+
+
+# ---------------------------------------------------------------- reference (CPU) timing
+
+def reference_step(n, threads):
+    import oracle
+    p = workload(n)
+    sol, wall = oracle.ref().scalar_driver(p, min_residual=TOL, nthreads=threads)
+    return wall
+
+
+def extrapolate(t_sample, n_sample, n_full):
+    return t_sample * ((n_full + 1) ** 3 / (n_sample + 1) ** 3) ** (4.0 / 3.0)
+
+
+def cpu_baseline(n_full, n_sample, runs=2):
+    import oracle
+    if not oracle.ref_available():
+        return None
+    threads = os.cpu_count() or 1
+    times = [reference_step(n_sample, threads) for _ in range(runs)]
+    t = min(times)
+    return {"value": extrapolate(t, n_sample, n_full) * 1e3, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"reference FEM_forBaseEliptic (SSOR-PCG restart loop) to 1e-8 on the same workload at "
+                      f"n={n_sample} ({(n_sample + 1) ** 3} DOF), best of {runs}: {t:.2f} s, scaled to n={n_full} "
+                      f"by (N ratio)^(4/3)"}
+
+
+def run_reference(args, D):
+    if D.rank != 0:
+        return
+    import oracle
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libfemref.so not built (reference sources absent at build time)"}))
+        return
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        reference_step(max(10, args.sample_n // 2), threads)
+    ts = [reference_step(args.sample_n, threads) for _ in range(args.steps)]
+    t = statistics.mean(ts)
+    v = extrapolate(t, args.sample_n, args.n) * 1e3
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": config(args.n, extra={"solver": "reference SSOR(0.75)-PCG restart loop (FEM/FEM.h:627-695)",
+                                            "sample_n": args.sample_n, "sample_seconds": ts}),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": f"driver at n={args.sample_n}, mean of {args.steps} runs = {t:.2f} s, "
+                                       f"scaled to n={args.n} by (N ratio)^(4/3)"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------- our arm
+
+def read_traffic():
+    path = os.path.join(ROOT, "profiles", "spmv_fp32_electrostatics_100.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return int(float(line.split(":")[1]))
+    except OSError:
+        pass
+    return None
+
+
+def peaks():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def run_ours(args, D):
+    import torch
+    from multiscalefemsolver3d_b200 import _lib, fem
+
+    torch.cuda.set_device(D.local)
+    dev = torch.device("cuda", D.local)
+    p = workload(args.n)
+    m = p.mesh
+    xyz = torch.from_numpy(m.xyz).to(dev)
+    tets = torch.from_numpy(m.tets).to(dev)
+    mat = torch.from_numpy(m.mat).to(dev)
+    bcn = torch.from_numpy(p.bc_nodes).to(dev)
+    bcv = torch.from_numpy(p.bc_values).to(dev)
+    torch.cuda.synchronize()
+
+    S = fem.System(fem.SCALAR, xyz, tets, mat)
+    stream = torch.cuda.ExternalStream(S.stream, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def step(method, precision):
+        S.clear()
+        S.assemble_scalar(p.sigma)
+        S.apply_dirichlet(bcn, bcv, fem.ROW_AND_COLUMN)
+        S.copy_f_to_x()
+        rel, it, rc = S.solve(method, precision, tol=TOL, maxiter=200000)
+        if rc != 0:
+            raise RuntimeError(f"solve rc={rc} rel={rel}")
+        return rel, it
+
+    def timed(method, precision, k):
+        ts, info = [], None
+        for _ in range(k):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rel, it = step(method, precision)
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+            st = S.stats()
+            info = {"rel_residual": rel, "iterations": it, "outer": st["outer_iterations"],
+                    "ms_solve": st["ms_solve"], "ms_assemble": st["ms_assemble"], "ms_dirichlet": st["ms_dirichlet"]}
+        return ts, info
+
+    for _ in range(args.warmup):
+        step(fem.PCG_JACOBI, fem.FP32_IR)
+    launches0 = S.stats()["total_launches"]
+    D.barrier()
+    torch.cuda.synchronize()
+    with Clocks(D.local) as clk:
+        ts, info = timed(fem.PCG_JACOBI, fem.FP32_IR, args.steps)
+    launches = (S.stats()["total_launches"] - launches0) // max(1, args.steps)
+    torch.cuda.synchronize()
+    D.barrier()
+    ms = D.max(statistics.mean(ts))
+
+    # comparators on the same system (fewer steps)
+    k2 = max(1, min(3, args.steps))
+    step(fem.CG, fem.FP64)
+    ts_cg, info_cg = timed(fem.CG, fem.FP64, k2)
+    ts_pcg, info_pcg = timed(fem.PCG_JACOBI, fem.FP64, k2)
+
+    # roofline of the dominant kernel: FP32 SpMV (and FP64 beside it)
+    spmv32_ms, spmv_bytes32 = S.bench_spmv(fem.FP32_IR, reps=200)
+    spmv64_ms, spmv_bytes64 = S.bench_spmv(fem.FP64, reps=200)
+    peak, peak_kind = peaks()
+    ach = spmv_bytes32 / (spmv32_ms * 1e-3) / 1e9
+    traffic = read_traffic()
+    n_colors, portrait_ms = S.n_colors, S.stats()["ms_portrait"]
+    S.close()
+
+    # e2e: the reference-facing driver with host (pinned) buffers
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+    hx, ht, hm = pin(m.xyz), pin(m.tets), pin(m.mat)
+    hs, hbn, hbv = pin(p.sigma), pin(p.bc_nodes), pin(p.bc_values)
+    sol = torch.empty(m.n_nodes, dtype=torch.float64).pin_memory()
+    L = _lib.load()
+    P = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+
+    def e2e_call():
+        st = _lib.Stats()
+        rc = L.msfem_fem_scalar_driver(m.n_nodes, P(hx), m.n_tets, P(ht), P(hm), hs.numel(), P(hs), hbn.numel(),
+                                       P(hbn), P(hbv), fem.PCG_JACOBI, fem.FP32_IR, TOL, 200000, P(sol),
+                                       C.byref(st))
+        if rc != 0:
+            raise RuntimeError(f"driver rc={rc}: {L.msfem_last_error()}")
+        return st
+
+    e2e_call()
+    e2e_ts = []
+    for _ in range(max(1, min(3, args.steps))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_call()
+        torch.cuda.synchronize()
+        e2e_ts.append((time.perf_counter() - t0) * 1e3)
+    e2e_ms = D.max(statistics.mean(e2e_ts))
+    h2d = sum(t.numel() * t.element_size() for t in (hx, ht, hm, hs, hbn, hbv))
+    d2h = sol.numel() * sol.element_size()
+
+    base = None
+    if D.rank == 0 and D.world == 1 and not args.no_cpu_baseline:
+        base = cpu_baseline(args.n, args.sample_n)
+
+    if D.rank == 0:
+        extra = {"iterations_inner": info["iterations"], "refinement_steps": info["outer"],
+                 "rel_residual": info["rel_residual"], "ms_assemble": info["ms_assemble"],
+                 "ms_dirichlet": info["ms_dirichlet"], "ms_solve": info["ms_solve"],
+                 "plain_fp64_cg_ms": statistics.mean(ts_cg), "plain_fp64_cg_iterations": info_cg["iterations"],
+                 "fp64_jacobi_pcg_ms": statistics.mean(ts_pcg), "fp64_jacobi_pcg_iterations": info_pcg["iterations"],
+                 "speedup_vs_plain_fp64_cg": statistics.mean(ts_cg) / ms,
+                 "spmv_fp32_ms": spmv32_ms, "spmv_fp32_gbs": ach, "spmv_fp64_ms": spmv64_ms,
+                 "spmv_fp64_gbs": spmv_bytes64 / (spmv64_ms * 1e-3) / 1e9, "portrait_ms": portrait_ms,
+                 "element_colors": n_colors, "step_ms_all": ts}
+        line = {"metric": METRIC, "value": ms, "unit": UNIT, "n_gpus": D.world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "fp32-in-f64-ir", "data": "synthetic",
+                "config": config(args.n, p, extra),
+                "e2e": {"value": e2e_ms, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "gpu_launches": int(launches),
+                "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                             "traffic": traffic, "kernel": "k_spmv<float> (SELL-32, FP32)",
+                             "peak_source": f"{peak_kind} hbm_gbs"},
+                "cpu_baseline": base,
+                "clocks": clk.summary()}
+        print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    D = Dist(args.gpus)
+    try:
+        if args.impl == "reference":
+            run_reference(args, D)
+        else:
+            run_ours(args, D)
+    finally:
+        D.close()
+
+
+if __name__ == "__main__":
+    main()

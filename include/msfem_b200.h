@@ -1,0 +1,184 @@
+/*
+ * msfem_b200.h -- C ABI of the B200 (sm_100a) implementation of the
+ * MultiscaleFEMSolver3D hot path: P1 tetrahedral assembly into the CSSD_Matrix
+ * layout and the Krylov solve on that matrix.
+ *
+ * The reference has no FFI; its "boundary" is a sequence of C++ member calls
+ * made by the FEM drivers (FEM/FEM.h).  Each entry point below replaces one
+ * step of that sequence; the comment on each names the reference code it
+ * stands for (paths relative to the reference project).
+ *
+ * Conventions
+ *  - Every function returns an int status: MSFEM_OK (0), a negative error code,
+ *    or MSFEM_NOT_CONVERGED (1) from a solver that stopped at maxiter.  Nothing
+ *    throws; msfem_last_error() returns the message of the calling thread's
+ *    last failure.  (The reference prints and continues, CSSD_Matrix.h:359-362.)
+ *  - Arrays are caller owned.  `on_device` = 0: host pointers (pinned or not),
+ *    copied in or out on the handle's stream;  = 1: CUDA device pointers on the
+ *    handle's device, used in place (no host round trip).
+ *  - DOF numbering is the reference's: scalar DOF = mesh node id
+ *    (FEM_Grid.h:509-574); elasticity DOF = 3*node + component
+ *    (Library/Math.h:1963-2054).
+ *  - Matrices export as CSR with the diagonal included and every row sorted
+ *    ascending: the reference CSSD row [A_down | Diag | A_up] laid end to end
+ *    (Library/CSSD_Matrix.h:11-15).  Structural zeros are kept.
+ *  - One handle = one system on one device with its own CUDA stream.  Calls on
+ *    different handles may run concurrently from different host threads; calls
+ *    on the same handle must not.
+ */
+#ifndef MSFEM_B200_H
+#define MSFEM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MSFEM_OK 0
+#define MSFEM_NOT_CONVERGED 1
+#define MSFEM_ERR_ARGUMENT (-1)
+#define MSFEM_ERR_CUDA (-2)
+#define MSFEM_ERR_STATE (-3)
+#define MSFEM_ERR_LIMIT (-4)
+#define MSFEM_ERR_NUMERIC (-5)
+
+enum msfem_kind { MSFEM_SCALAR = 0, MSFEM_ELASTIC = 1 };
+
+enum msfem_method {
+    MSFEM_CG = 0,          /* plain CG, CSSD_Matrix::MSG (CSSD_Matrix.h:1496-1576)                 */
+    MSFEM_PCG_JACOBI = 1,  /* the PCG loop of MSG_PreconditioningSSOR (:1302-1398), M = diag(A)    */
+    MSFEM_BICGSTAB = 2,    /* Jacobi-preconditioned BiCGStab (the role of BiCG_Stab/BCG_Stab2)      */
+    MSFEM_GMRES = 3        /* restarted GMRES(m), Jacobi-preconditioned (CSSD_Matrix::GMRES role)  */
+};
+
+enum msfem_precision {
+    MSFEM_FP64 = 0,    /* everything in FP64                                                        */
+    MSFEM_FP32_IR = 1  /* FP32 matrix + FP32 Krylov inner solves inside FP64 iterative refinement:
+                          r = F - A x and x accumulate in FP64                                      */
+};
+
+enum msfem_dirichlet_mode {
+    MSFEM_ROW_ONLY = 0,       /* row := e_d, F = X = value (FEM/FEM.h:297-324, 3-coefficient driver) */
+    MSFEM_ROW_AND_COLUMN = 1  /* rows as above, then the column sweep F -= A(:,d) F_d, A(:,d) = 0 with
+                                 the reference's forward-only walk over the boundary list
+                                 (FEM/FEM.h:506-619 scalar, :1676-1813 elasticity)                   */
+};
+
+typedef struct msfem_system* msfem_system_t;
+
+typedef struct {
+    int iterations;          /* Krylov iterations of the last solve (inner iterations for FP32_IR) */
+    int outer_iterations;    /* refinement steps (FP32_IR), restarts (GMRES), else 0               */
+    double rel_residual;     /* ||F - A X|| / ||F|| recomputed in FP64 at exit                       */
+    double ms_portrait;      /* device time of the last portrait build                             */
+    double ms_assemble;      /* device time of the last assembly (elements + scatter)              */
+    double ms_dirichlet;     /* device time of the last Dirichlet application                       */
+    double ms_solve;         /* device time of the last solve                                       */
+    double ms_spmv;          /* mean device time of one SpMV of the solve's working precision       */
+    int n_colors;            /* element colour classes used by the assembly                         */
+    int kernel_launches;     /* kernels of this library launched by the last solve                  */
+    int64_t total_launches;  /* kernels of this library launched on this handle since creation      */
+} msfem_stats;
+
+const char* msfem_last_error(void);
+int msfem_version(void);
+
+/* Grid_forScal / Grid_forMech::Initialization + CreationPortrait + CSSD_Matrix::Initialization
+ * (FEM/FEM_Grid.h:575-663, :3017-3102; :665-716, :3236-3287; Library/CSSD_Matrix.h:79-99):
+ * uploads the mesh (nvtr = tets[4*n_tets], nvkat = material[n_tets], xyz[3*n_nodes]),
+ * builds the node-level portrait (every pair of nodes of an element couples), the
+ * element -> matrix-slot map and the element colouring, and allocates the zeroed
+ * matrix, F and X.  kind = MSFEM_SCALAR (n rows = n_nodes) or MSFEM_ELASTIC
+ * (n rows = 3*n_nodes, 3x3 blocks).  material may be NULL (all zero). */
+int msfem_system_create(int kind, int n_nodes, const double* xyz, int n_tets, const int32_t* tets,
+                        const int32_t* material, int on_device, msfem_system_t* out);
+int msfem_system_destroy(msfem_system_t h);
+
+/* n_rows, scalar nnz of the CSR export (diagonal included), element colour count */
+int msfem_system_info(msfem_system_t h, int* n_rows, int64_t* nnz, int* n_colors);
+int msfem_get_stats(msfem_system_t h, msfem_stats* out);
+/* the handle's CUDA stream (cudaStream_t) */
+void* msfem_get_stream(msfem_system_t h);
+
+/* Zeroes the matrix values, F and X, keeping the portrait (CSSD_Matrix::ClearVariables, :172). */
+int msfem_clear(msfem_system_t h);
+
+/* Scalar stiffness assembly: element loop + SummPartOfMatrix (FEM/FEM.h:474-482,
+ * FEM_Grid.h:103-152 with the 1-point rule, CSSD_Matrix.h:307-363).
+ * sigma[material] is the element coefficient. */
+int msfem_assemble_scalar(msfem_system_t h, const double* sigma, int n_materials);
+
+/* Linear elasticity assembly (FEM/FEM.h:1349-1384, FEM_Grid.h:2125-2192): block
+ * A[I][J] = V * B_J^T D(E, nu) B_I for J >= I and A[J][I] = A[I][J]^T (the
+ * reference's orientation), D from Domain::forMech::SetIsotropic_D
+ * (Library/Domain.h:53-78).  Materials with E <= 0 contribute nothing. */
+int msfem_assemble_elastic(msfem_system_t h, const double* E, const double* nu, int n_materials);
+
+/* Traction load (FEM/FEM.h:1338-1343, BoundaryFace_forMech::SolveLocalBoundaryVector
+ * FEM_Grid.h:2622-2661): F[3*v+c] += traction[3*f+c] * area_f / 3 for the three
+ * nodes v of face f.  ELASTIC only. */
+int msfem_add_traction(msfem_system_t h, int n_faces, const int32_t* face_nodes, const double* traction,
+                       int on_device);
+
+/* Adds a caller vector to F (CSSD_Matrix::SummPartOfVector, :364-379, for a whole vector). */
+int msfem_add_rhs(msfem_system_t h, const double* f, int on_device);
+
+/* Dirichlet conditions on `n` DOFs in the caller's boundary-list order
+ * (the order of the reference's boundary_vertexes), see enum msfem_dirichlet_mode. */
+int msfem_apply_dirichlet(msfem_system_t h, int n, const int32_t* dofs, const double* values, int mode,
+                          int on_device);
+
+int msfem_set_x(msfem_system_t h, const double* x, int on_device);
+int msfem_get_x(msfem_system_t h, double* x, int on_device);
+int msfem_get_f(msfem_system_t h, double* f, int on_device);
+/* X := F (FEM/FEM.h:635, the scalar driver's initial guess) */
+int msfem_copy_f_to_x(msfem_system_t h);
+
+/* Solves A X = F from the current X (CSSD_Matrix::MSG / MSG_PreconditioningSSOR /
+ * BiCG_Stab / GMRES, CSSD_Matrix.h:1302-1989).  Stops when ||r||/||F|| <= tol
+ * (the reference's test) or after maxiter iterations (MSFEM_NOT_CONVERGED).
+ * restart_m: GMRES restart depth (ignored otherwise).  rel_residual / iterations
+ * may be NULL. */
+int msfem_solve(msfem_system_t h, int method, int precision, int restart_m, int maxiter, double tol,
+                double* rel_residual, int* iterations);
+
+/* y = A x in FP64 (CSSD_Matrix::MultiplicationMatrixVector, :395-423) */
+int msfem_spmv(msfem_system_t h, const double* x, double* y, int on_device);
+
+/* CSR export of the assembled matrix (sizes from msfem_system_info), host or device buffers. */
+int msfem_export_csr(msfem_system_t h, int32_t* row_ptr, int32_t* col, double* val, int on_device);
+
+/* Measurement helper (no counterpart in the reference): times `reps` back-to-back
+ * FP64 (precision MSFEM_FP64) or FP32 (MSFEM_FP32_IR) SpMV launches with CUDA
+ * events on the handle's stream after 3 warm-up launches, and reports the mean
+ * device time per product and the algorithmic bytes of one product
+ * (values + column indices + row structure + x + y, each counted once). */
+int msfem_bench_spmv(msfem_system_t h, int precision, int reps, double* ms_per_product, int64_t* bytes_per_product);
+
+/* One-call drivers: the reference driver sequence on the GPU, host buffers in and out.
+ *
+ * FEM::FEM_forBaseEliptic, stiffness-only overload (FEM/FEM.h:398-717):
+ * create -> assemble (sigma per material) -> Dirichlet rows + column sweep ->
+ * X = F -> solve to min_residual.  solution: n_nodes doubles. */
+int msfem_fem_scalar_driver(int n_nodes, const double* xyz, int n_tets, const int32_t* tets,
+                            const int32_t* material, int n_materials, const double* sigma,
+                            int n_bc, const int32_t* bc_nodes, const double* bc_values,
+                            int method, int precision, double min_residual, int maxiter,
+                            double* solution, msfem_stats* stats);
+
+/* FEM::FEM_forElasticDeformation (FEM/FEM.h:1286-1961): create -> traction ->
+ * assemble -> Dirichlet (mask bit c = component c fixed, values[3*i+c]) with the
+ * column sweep -> solve to min_residual from X = Dirichlet values, 0 elsewhere.
+ * solution: 3*n_nodes doubles, node-major. */
+int msfem_fem_elastic_driver(int n_nodes, const double* xyz, int n_tets, const int32_t* tets,
+                             const int32_t* material, int n_materials, const double* E, const double* nu,
+                             int n_bc, const int32_t* bc_nodes, const int32_t* bc_mask, const double* bc_values,
+                             int n_faces, const int32_t* face_nodes, const double* face_traction,
+                             int method, int precision, double min_residual, int maxiter,
+                             double* solution, msfem_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MSFEM_B200_H */

@@ -1,0 +1,107 @@
+"""ctypes binding of libmsfem_b200.so (the C ABI in include/msfem_b200.h).
+
+The library is loaded from the package directory; if it is missing the import
+fails loudly (there is no fallback path).  Build it with
+`python -m multiscalefemsolver3d_b200.build`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libmsfem_b200.so")
+
+MSFEM_OK = 0
+MSFEM_NOT_CONVERGED = 1
+
+SCALAR, ELASTIC = 0, 1
+CG, PCG_JACOBI, BICGSTAB, GMRES = 0, 1, 2, 3
+FP64, FP32_IR = 0, 1
+ROW_ONLY, ROW_AND_COLUMN = 0, 1
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int),
+        ("outer_iterations", C.c_int),
+        ("rel_residual", C.c_double),
+        ("ms_portrait", C.c_double),
+        ("ms_assemble", C.c_double),
+        ("ms_dirichlet", C.c_double),
+        ("ms_solve", C.c_double),
+        ("ms_spmv", C.c_double),
+        ("n_colors", C.c_int),
+        ("kernel_launches", C.c_int),
+        ("total_launches", C.c_int64),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# (name, restype, argtypes); arrays are passed as void pointers so that numpy
+# host arrays and CUDA device pointers (torch .data_ptr()) both fit
+_P = C.c_void_p
+_SIGS = [
+    ("msfem_last_error", C.c_char_p, []),
+    ("msfem_version", C.c_int, []),
+    ("msfem_system_create", C.c_int, [C.c_int, C.c_int, _P, C.c_int, _P, _P, C.c_int, C.POINTER(C.c_void_p)]),
+    ("msfem_system_destroy", C.c_int, [C.c_void_p]),
+    ("msfem_system_info", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int64), C.POINTER(C.c_int)]),
+    ("msfem_get_stats", C.c_int, [C.c_void_p, C.POINTER(Stats)]),
+    ("msfem_get_stream", C.c_void_p, [C.c_void_p]),
+    ("msfem_clear", C.c_int, [C.c_void_p]),
+    ("msfem_assemble_scalar", C.c_int, [C.c_void_p, _P, C.c_int]),
+    ("msfem_assemble_elastic", C.c_int, [C.c_void_p, _P, _P, C.c_int]),
+    ("msfem_add_traction", C.c_int, [C.c_void_p, C.c_int, _P, _P, C.c_int]),
+    ("msfem_add_rhs", C.c_int, [C.c_void_p, _P, C.c_int]),
+    ("msfem_apply_dirichlet", C.c_int, [C.c_void_p, C.c_int, _P, _P, C.c_int, C.c_int]),
+    ("msfem_set_x", C.c_int, [C.c_void_p, _P, C.c_int]),
+    ("msfem_get_x", C.c_int, [C.c_void_p, _P, C.c_int]),
+    ("msfem_get_f", C.c_int, [C.c_void_p, _P, C.c_int]),
+    ("msfem_copy_f_to_x", C.c_int, [C.c_void_p]),
+    ("msfem_solve", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                              C.POINTER(C.c_double), C.POINTER(C.c_int)]),
+    ("msfem_spmv", C.c_int, [C.c_void_p, _P, _P, C.c_int]),
+    ("msfem_export_csr", C.c_int, [C.c_void_p, _P, _P, _P, C.c_int]),
+    ("msfem_bench_spmv", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+    ("msfem_fem_scalar_driver", C.c_int, [C.c_int, _P, C.c_int, _P, _P, C.c_int, _P, C.c_int, _P, _P, C.c_int,
+                                          C.c_int, C.c_double, C.c_int, _P, C.POINTER(Stats)]),
+    ("msfem_fem_elastic_driver", C.c_int, [C.c_int, _P, C.c_int, _P, _P, C.c_int, _P, _P, C.c_int, _P, _P, _P,
+                                           C.c_int, _P, _P, C.c_int, C.c_int, C.c_double, C.c_int, _P,
+                                           C.POINTER(Stats)]),
+]
+
+EXPORTED = [name for name, _, _ in _SIGS]
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Loads the library (once).  Raises if it is missing: no CPU fallback exists."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing; build it with `python -m multiscalefemsolver3d_b200.build`")
+    L = C.CDLL(path)
+    for name, res, args in _SIGS:
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+class MsfemError(RuntimeError):
+    def __init__(self, rc: int, where: str):
+        msg = load().msfem_last_error().decode(errors="replace")
+        super().__init__(f"{where} failed ({rc}): {msg}")
+        self.rc = rc
+
+
+def check(rc: int, where: str) -> int:
+    if rc < 0:
+        raise MsfemError(rc, where)
+    return rc

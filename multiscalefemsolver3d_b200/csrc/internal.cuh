@@ -1,0 +1,157 @@
+// Internal declarations shared by the CUDA translation units of libmsfem_b200.so.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "msfem_b200.h"
+
+namespace msfem {
+
+void set_error(const char* fmt, ...);
+
+#define MSFEM_CK(call)                                                                                   \
+    do {                                                                                                 \
+        cudaError_t e_ = (call);                                                                         \
+        if (e_ != cudaSuccess) {                                                                         \
+            ::msfem::set_error("%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_));       \
+            return MSFEM_ERR_CUDA;                                                                       \
+        }                                                                                                \
+    } while (0)
+
+#define MSFEM_TRY(expr)               \
+    do {                              \
+        int rc_ = (expr);             \
+        if (rc_ < 0) return rc_;      \
+    } while (0)
+
+constexpr int kSlice = 32;        // rows (or block rows) per SELL slice = one warp
+constexpr int kChunk = 4;         // scalar SELL: entries per lane per 128-bit load group
+constexpr int kMaxCandidates = 256;  // portrait: candidates per row handled by one warp
+constexpr int kReduceBlocks = 148 * 4;  // fixed grid of the vector kernels (deterministic reductions)
+constexpr int kVecThreads = 256;
+
+// device scratch that lives with a system and is allocated on first use
+template <class T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    ~DBuf() { release(); }
+    int alloc(size_t count) {
+        if (count <= n && p) return 0;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        if (count == 0) return 0;
+        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        if (e != cudaSuccess) {
+            set_error("cudaMalloc(%zu bytes): %s", count * sizeof(T), cudaGetErrorString(e));
+            p = nullptr;
+            return MSFEM_ERR_CUDA;
+        }
+        n = count;
+        return 0;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+// SELL-32 copy of the matrix used by the solvers (rebuilt when values change).
+// scalar:  entry (slice s, position k, lane l) at slice_ptr[s] + (k/4)*128 + 4*l + k%4
+// block3:  block (s, k, l) column at slice_ptr[s] + 32*k + l, its 9 values at
+//          9*slice_ptr[s] + (9*k + e)*32 + l   (e = 3*a + b, row a / column b of the 3x3 block)
+struct Sell {
+    int n_slices = 0;
+    int64_t stored = 0;  // stored entries (scalar) or blocks (block3), padding included
+    DBuf<int64_t> slice_ptr;
+    DBuf<int32_t> col;
+    DBuf<double> val64;
+    DBuf<float> val32;
+    bool pattern_ok = false;
+    bool values_ok = false;
+};
+
+// Device-resident scalars of a Krylov solve.  Written by the last block of the
+// reduction kernels, read by the following kernels: no host round trip per iteration.
+struct KState {
+    double rz, rz_new, rr, ff, pq, alpha, beta, omega, tol2;
+    double r0v, tt, ts, rho_old;  // BiCGStab
+    int iter, maxiter, done, breakdown;
+    unsigned int ticket[4];
+};
+
+struct System {
+    int kind = MSFEM_SCALAR;
+    int bs = 1;  // 1 scalar, 3 elasticity
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int n_nodes = 0, n_tets = 0, n_rows = 0;
+
+    DBuf<double> xyz;
+    DBuf<int32_t> tets;
+    DBuf<int32_t> mat;
+
+    // node -> element incidence (CSR)
+    DBuf<int32_t> inc_ptr, inc_elem;
+    // node-level portrait, diagonal included, rows sorted
+    DBuf<int32_t> nrp, ncol;
+    int64_t nnzb = 0;
+    // element (e, I, J) -> node-portrait slot, e*16 + 4*I + J
+    DBuf<int32_t> eslot;
+    // element colouring: elements listed colour by colour
+    DBuf<int32_t> color_elems;
+    std::vector<int> color_off;  // host copy, size n_colors + 1
+
+    // values: scalar val[slot]; elasticity val[9*slot + 3*a + b]
+    DBuf<double> val;
+    DBuf<double> F, X;
+
+    // solver data
+    Sell sell;
+    DBuf<double> diag64;  // diagonal of A (FP64)
+    DBuf<float> dinv32;   // 1/diag (FP32)
+    DBuf<double> dinv64;  // 1/diag (FP64)
+    DBuf<double> work64;  // Krylov vectors (FP64)
+    DBuf<float> work32;   // Krylov vectors (FP32)
+    DBuf<double> partial; // reduction partials
+    DBuf<KState> kstate;
+    KState* h_kstate = nullptr;  // pinned mirror for polling
+    DBuf<double> gm;      // GMRES: Hessenberg / rotations / y on the device
+
+    bool zero_diag = false;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    msfem_stats stats{};
+    int launches = 0;          // kernels of the current solve
+    int64_t total_launches = 0;  // kernels of this library launched on the handle
+
+    void invalidate_values() { sell.values_ok = false; }
+};
+
+// ---- mesh / portrait (portrait.cu)
+int build_topology(System& s);
+// ---- assembly (assemble.cu)
+int assemble_scalar(System& s, const double* sigma, int n_mat);
+int assemble_elastic(System& s, const double* E, const double* nu, int n_mat);
+int add_traction(System& s, int n_faces, const int32_t* d_faces, const double* d_traction);
+// ---- boundary conditions (bc.cu)
+int apply_dirichlet(System& s, int n, const int32_t* d_dofs, const double* d_values, int mode);
+// ---- SpMV and SELL (spmv.cu)
+int prepare_sell(System& s);
+int spmv64(System& s, const double* x, double* y);
+int spmv32(System& s, const float* x, float* y);
+int residual64(System& s, const double* x, const double* f, double* r, double* rr_out);
+// ---- Krylov (krylov.cu)
+int solve(System& s, int method, int precision, int restart_m, int maxiter, double tol, double* relres, int* iters);
+
+}  // namespace msfem

@@ -1,0 +1,722 @@
+// Krylov solvers on the SELL-32 matrix with device-resident scalars.
+//
+// Every iteration is a short fixed sequence of kernels; the reductions inside
+// them are two-stage and deterministic (each block writes its partial sum, the
+// last block to arrive adds the partials in index order and derives the next
+// scalar, e.g. alpha = (r,z)/(p,Ap)), so the host never waits inside an
+// iteration.  A chunk of iterations is captured once into a CUDA graph and
+// replayed; the host reads the solver state only between chunks.  When the
+// stopping test fires, the remaining kernels of the chunk return at once.
+//
+// Stopping test: sqrt((r,r)/(F,F)) <= tol on the recurrence residual, as in
+// CSSD_Matrix::MSG / MSG_PreconditioningSSOR (CSSD_Matrix.h:1336, :1524); the
+// reported residual is recomputed as ||F - A X|| / ||F|| in FP64 at exit.
+#include <cmath>
+
+#include "devutil.cuh"
+#include "internal.cuh"
+#include "spmv.cuh"
+
+namespace msfem {
+namespace {
+
+constexpr int kMaxOuter = 60;
+
+inline unsigned grid_for(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+// ------------------------------------------------------------------ vector kernels
+
+template <class VT>
+__global__ void __launch_bounds__(kVecThreads) k_dot_self(int n, const VT* __restrict__ a, double* __restrict__ partial,
+                                                          unsigned int* ticket, double* out)
+{
+    __shared__ double sh[32];
+    double acc[1] = {0.0};
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double v = (double)a[i];
+        acc[0] += v * v;
+    }
+    block_sum<1>(acc, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = acc[0];
+    if (arrive_last(ticket)) {
+        double t[1];
+        reduce_partials<1>(partial, gridDim.x, 0, t, sh);
+        if (threadIdx.x == 0) {
+            *out = t[0];
+            *ticket = 0;
+        }
+    }
+}
+
+// z = M^{-1} r, p = z, (r,z), (r,r); sets rz, rr and the initial stopping test
+template <class VT, bool JAC>
+__global__ void __launch_bounds__(kVecThreads) k_pcg_init(int n, const VT* __restrict__ r, const VT* __restrict__ dinv,
+                                                          VT* __restrict__ z, VT* __restrict__ p, KState* S,
+                                                          double* __restrict__ partial)
+{
+    __shared__ double sh[64];
+    double acc[2] = {0.0, 0.0};
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const VT rv = r[i];
+        const VT zv = JAC ? rv * dinv[i] : rv;
+        z[i] = zv;
+        p[i] = zv;
+        acc[0] += (double)rv * (double)zv;
+        acc[1] += (double)rv * (double)rv;
+    }
+    block_sum<2>(acc, sh);
+    if (threadIdx.x == 0) {
+        partial[blockIdx.x] = acc[0];
+        partial[gridDim.x + blockIdx.x] = acc[1];
+    }
+    if (arrive_last(&S->ticket[0])) {
+        double t[2];
+        reduce_partials<2>(partial, gridDim.x, gridDim.x, t, sh);
+        if (threadIdx.x == 0) {
+            S->rz = t[0];
+            S->rr = t[1];
+            S->iter = 0;
+            S->breakdown = 0;
+            S->done = (t[1] <= S->tol2) ? 1 : 0;
+            S->ticket[0] = 0;
+        }
+    }
+}
+
+// q = A p, (p, q) -> alpha = rz / (p, q)
+template <class VT>
+__global__ void __launch_bounds__(256) k_pcg_spmv(SellView<VT> A, const VT* __restrict__ p, VT* __restrict__ q,
+                                                  KState* S, double* __restrict__ partial)
+{
+    if (S->done) return;
+    __shared__ double sh[32];
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    double acc[1] = {0.0};
+    if (warp < A.n_slices) {
+        if (A.bs == 1) {
+            const VT v = sell_row_scalar<VT>(A, warp, lane, p);
+            const int row = warp * kSlice + lane;
+            if (row < A.n_rows) {
+                q[row] = v;
+                acc[0] = (double)p[row] * (double)v;
+            }
+        } else {
+            VT v[3];
+            sell_row_block<VT>(A, warp, lane, p, v);
+            const int brow = warp * kSlice + lane;
+            if (brow < A.n_brows)
+                for (int c = 0; c < 3; c++) {
+                    q[3 * (int64_t)brow + c] = v[c];
+                    acc[0] += (double)p[3 * (int64_t)brow + c] * (double)v[c];
+                }
+        }
+    }
+    block_sum<1>(acc, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = acc[0];
+    if (arrive_last(&S->ticket[0])) {
+        double t[1];
+        reduce_partials<1>(partial, gridDim.x, 0, t, sh);
+        if (threadIdx.x == 0) {
+            S->pq = t[0];
+            if (t[0] == 0.0 || t[0] != t[0]) {
+                S->breakdown = 1;
+                S->done = 1;
+            }
+            S->alpha = S->rz / t[0];
+            S->ticket[0] = 0;
+        }
+    }
+}
+
+// x += alpha p, r -= alpha q, z = M^{-1} r, (r,z), (r,r) -> beta, stopping test
+template <class VT, bool JAC>
+__global__ void __launch_bounds__(kVecThreads) k_pcg_update(int n, VT* __restrict__ x, VT* __restrict__ r,
+                                                            VT* __restrict__ z, const VT* __restrict__ p,
+                                                            const VT* __restrict__ q, const VT* __restrict__ dinv,
+                                                            KState* S, double* __restrict__ partial)
+{
+    if (S->done) return;
+    __shared__ double sh[64];
+    const VT alpha = (VT)S->alpha;
+    double acc[2] = {0.0, 0.0};
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        x[i] += alpha * p[i];
+        const VT rv = r[i] - alpha * q[i];
+        r[i] = rv;
+        const VT zv = JAC ? rv * dinv[i] : rv;
+        z[i] = zv;
+        acc[0] += (double)rv * (double)zv;
+        acc[1] += (double)rv * (double)rv;
+    }
+    block_sum<2>(acc, sh);
+    if (threadIdx.x == 0) {
+        partial[blockIdx.x] = acc[0];
+        partial[gridDim.x + blockIdx.x] = acc[1];
+    }
+    if (arrive_last(&S->ticket[0])) {
+        double t[2];
+        reduce_partials<2>(partial, gridDim.x, gridDim.x, t, sh);
+        if (threadIdx.x == 0) {
+            S->beta = t[0] / S->rz;
+            S->rz = t[0];
+            S->rr = t[1];
+            S->iter += 1;
+            if (t[1] <= S->tol2) S->done = 1;
+            else if (S->iter >= S->maxiter) S->done = 2;
+            else if (t[1] != t[1]) {
+                S->breakdown = 1;
+                S->done = 3;
+            }
+            S->ticket[0] = 0;
+        }
+    }
+}
+
+template <class VT>
+__global__ void __launch_bounds__(kVecThreads) k_pcg_p(int n, const VT* __restrict__ z, VT* __restrict__ p,
+                                                       const KState* S)
+{
+    if (S->done) return;
+    const VT beta = (VT)S->beta;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = z[i] + beta * p[i];
+}
+
+// generic residual in VT: r = b - A x  (used by the FP32 inner solve with x = 0 -> r = b)
+template <class VT>
+__global__ void __launch_bounds__(kVecThreads) k_copy(int n, const VT* __restrict__ a, VT* __restrict__ b)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = a[i];
+}
+
+// FP32-IR helpers
+__global__ void __launch_bounds__(kVecThreads) k_scale_to32(int n, const double* __restrict__ r, const double* rr,
+                                                            float* __restrict__ r32, float* __restrict__ d32)
+{
+    const double s = 1.0 / sqrt(*rr);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        r32[i] = (float)(r[i] * s);
+        d32[i] = 0.0f;
+    }
+}
+
+__global__ void __launch_bounds__(kVecThreads) k_correct(int n, double* __restrict__ x, const float* __restrict__ d32,
+                                                         const double* rr)
+{
+    const double s = sqrt(*rr);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] += s * (double)d32[i];
+}
+
+// ------------------------------------------------------------------ BiCGStab kernels
+// Preconditioned BiCGStab (van der Vorst) with M = diag(A):
+//   p = r + beta (p - omega v);  y = M^-1 p;  v = A y;  alpha = rho / (rhat, v)
+//   s = r - alpha v;  zz = M^-1 s;  t = A zz;  omega = (t, s) / (t, t)
+//   x += alpha y + omega zz;  r = s - omega t;  rho' = (rhat, r);  beta = rho'/rho * alpha/omega
+
+template <class VT>
+__global__ void __launch_bounds__(kVecThreads) k_bcg_p(int n, const VT* __restrict__ r, VT* __restrict__ p,
+                                                       const VT* __restrict__ v, VT* __restrict__ y,
+                                                       const VT* __restrict__ dinv, const KState* S)
+{
+    if (S->done) return;
+    const VT beta = (VT)S->beta, omega = (VT)S->omega;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const VT pv = r[i] + beta * (p[i] - omega * v[i]);
+        p[i] = pv;
+        y[i] = pv * dinv[i];
+    }
+}
+
+// v = A y, (rhat, v) -> alpha
+template <class VT>
+__global__ void __launch_bounds__(256) k_bcg_spmv_alpha(SellView<VT> A, const VT* __restrict__ y, VT* __restrict__ v,
+                                                        const VT* __restrict__ rhat, KState* S,
+                                                        double* __restrict__ partial)
+{
+    if (S->done) return;
+    __shared__ double sh[32];
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    double acc[1] = {0.0};
+    if (warp < A.n_slices) {
+        if (A.bs == 1) {
+            const VT t = sell_row_scalar<VT>(A, warp, lane, y);
+            const int row = warp * kSlice + lane;
+            if (row < A.n_rows) {
+                v[row] = t;
+                acc[0] = (double)rhat[row] * (double)t;
+            }
+        } else {
+            VT t[3];
+            sell_row_block<VT>(A, warp, lane, y, t);
+            const int brow = warp * kSlice + lane;
+            if (brow < A.n_brows)
+                for (int c = 0; c < 3; c++) {
+                    v[3 * (int64_t)brow + c] = t[c];
+                    acc[0] += (double)rhat[3 * (int64_t)brow + c] * (double)t[c];
+                }
+        }
+    }
+    block_sum<1>(acc, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = acc[0];
+    if (arrive_last(&S->ticket[0])) {
+        double t[1];
+        reduce_partials<1>(partial, gridDim.x, 0, t, sh);
+        if (threadIdx.x == 0) {
+            if (t[0] == 0.0 || t[0] != t[0]) {
+                S->breakdown = 1;
+                S->done = 3;
+            }
+            S->alpha = S->rho_old / t[0];
+            S->ticket[0] = 0;
+        }
+    }
+}
+
+template <class VT>
+__global__ void __launch_bounds__(kVecThreads) k_bcg_s(int n, const VT* __restrict__ r, const VT* __restrict__ v,
+                                                       VT* __restrict__ s, VT* __restrict__ zz,
+                                                       const VT* __restrict__ dinv, const KState* S)
+{
+    if (S->done) return;
+    const VT alpha = (VT)S->alpha;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const VT sv = r[i] - alpha * v[i];
+        s[i] = sv;
+        zz[i] = sv * dinv[i];
+    }
+}
+
+// t = A zz, (t, s), (t, t) -> omega
+template <class VT>
+__global__ void __launch_bounds__(256) k_bcg_spmv_omega(SellView<VT> A, const VT* __restrict__ zz, VT* __restrict__ t,
+                                                        const VT* __restrict__ s, KState* S,
+                                                        double* __restrict__ partial)
+{
+    if (S->done) return;
+    __shared__ double sh[64];
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    double acc[2] = {0.0, 0.0};
+    if (warp < A.n_slices) {
+        if (A.bs == 1) {
+            const VT tv = sell_row_scalar<VT>(A, warp, lane, zz);
+            const int row = warp * kSlice + lane;
+            if (row < A.n_rows) {
+                t[row] = tv;
+                acc[0] = (double)tv * (double)s[row];
+                acc[1] = (double)tv * (double)tv;
+            }
+        } else {
+            VT tv[3];
+            sell_row_block<VT>(A, warp, lane, zz, tv);
+            const int brow = warp * kSlice + lane;
+            if (brow < A.n_brows)
+                for (int c = 0; c < 3; c++) {
+                    t[3 * (int64_t)brow + c] = tv[c];
+                    acc[0] += (double)tv[c] * (double)s[3 * (int64_t)brow + c];
+                    acc[1] += (double)tv[c] * (double)tv[c];
+                }
+        }
+    }
+    block_sum<2>(acc, sh);
+    if (threadIdx.x == 0) {
+        partial[blockIdx.x] = acc[0];
+        partial[gridDim.x + blockIdx.x] = acc[1];
+    }
+    if (arrive_last(&S->ticket[0])) {
+        double tt[2];
+        reduce_partials<2>(partial, gridDim.x, gridDim.x, tt, sh);
+        if (threadIdx.x == 0) {
+            S->ts = tt[0];
+            S->tt = tt[1];
+            S->omega = (tt[1] > 0.0) ? tt[0] / tt[1] : 0.0;
+            S->ticket[0] = 0;
+        }
+    }
+}
+
+// x += alpha y + omega zz, r = s - omega t, (rhat, r), (r, r) -> beta, stopping test
+template <class VT>
+__global__ void __launch_bounds__(kVecThreads) k_bcg_update(int n, VT* __restrict__ x, VT* __restrict__ r,
+                                                            const VT* __restrict__ y, const VT* __restrict__ zz,
+                                                            const VT* __restrict__ s, const VT* __restrict__ t,
+                                                            const VT* __restrict__ rhat, KState* S,
+                                                            double* __restrict__ partial)
+{
+    if (S->done) return;
+    __shared__ double sh[64];
+    const VT alpha = (VT)S->alpha, omega = (VT)S->omega;
+    double acc[2] = {0.0, 0.0};
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        x[i] += alpha * y[i] + omega * zz[i];
+        const VT rv = s[i] - omega * t[i];
+        r[i] = rv;
+        acc[0] += (double)rhat[i] * (double)rv;
+        acc[1] += (double)rv * (double)rv;
+    }
+    block_sum<2>(acc, sh);
+    if (threadIdx.x == 0) {
+        partial[blockIdx.x] = acc[0];
+        partial[gridDim.x + blockIdx.x] = acc[1];
+    }
+    if (arrive_last(&S->ticket[0])) {
+        double tt[2];
+        reduce_partials<2>(partial, gridDim.x, gridDim.x, tt, sh);
+        if (threadIdx.x == 0) {
+            const double rho = tt[0];
+            S->rr = tt[1];
+            S->iter += 1;
+            if (S->omega == 0.0 || S->rho_old == 0.0) {
+                S->breakdown = 1;
+                S->done = 3;
+            } else {
+                S->beta = (rho / S->rho_old) * (S->alpha / S->omega);
+            }
+            S->rho_old = rho;
+            if (tt[1] <= S->tol2) S->done = 1;
+            else if (S->iter >= S->maxiter && !S->done) S->done = 2;
+            S->ticket[0] = 0;
+        }
+    }
+}
+
+// r = b - A x (VT) with rhat = r, p = v = 0, (r, r) -> rho_old, rr
+template <class VT>
+__global__ void __launch_bounds__(kVecThreads) k_bcg_init(int n, const VT* __restrict__ r, VT* __restrict__ rhat,
+                                                          VT* __restrict__ p, VT* __restrict__ v, KState* S,
+                                                          double* __restrict__ partial)
+{
+    __shared__ double sh[32];
+    double acc[1] = {0.0};
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const VT rv = r[i];
+        rhat[i] = rv;
+        p[i] = 0;
+        v[i] = 0;
+        acc[0] += (double)rv * (double)rv;
+    }
+    block_sum<1>(acc, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = acc[0];
+    if (arrive_last(&S->ticket[0])) {
+        double t[1];
+        reduce_partials<1>(partial, gridDim.x, 0, t, sh);
+        if (threadIdx.x == 0) {
+            S->rho_old = t[0];
+            S->rr = t[0];
+            S->beta = 0.0;
+            S->omega = 1.0;
+            S->alpha = 1.0;
+            S->iter = 0;
+            S->breakdown = 0;
+            S->done = (t[0] <= S->tol2) ? 1 : 0;
+            S->ticket[0] = 0;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ host side
+
+struct Timer {
+    System& s;
+    explicit Timer(System& sys) : s(sys) { cudaEventRecord(s.ev0, s.stream); }
+    float stop()
+    {
+        cudaEventRecord(s.ev1, s.stream);
+        cudaEventSynchronize(s.ev1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, s.ev0, s.ev1);
+        return ms;
+    }
+};
+
+int ensure_state(System& s)
+{
+    if (!s.kstate.p) {
+        MSFEM_TRY(s.kstate.alloc(1));
+        MSFEM_CK(cudaMemsetAsync(s.kstate.p, 0, sizeof(KState), s.stream));
+    }
+    if (!s.h_kstate) MSFEM_CK(cudaMallocHost(&s.h_kstate, sizeof(KState)));
+    const unsigned g = spmv_grid(s);
+    MSFEM_TRY(s.partial.alloc(std::max<size_t>(3 * (size_t)g, 3 * (size_t)kReduceBlocks) + 64));
+    return MSFEM_OK;
+}
+
+int read_state(System& s)
+{
+    MSFEM_CK(cudaMemcpyAsync(s.h_kstate, s.kstate.p, sizeof(KState), cudaMemcpyDeviceToHost, s.stream));
+    MSFEM_CK(cudaStreamSynchronize(s.stream));
+    return MSFEM_OK;
+}
+
+// sets S->ff, S->tol2 (= tol^2 * ff), S->maxiter on the device
+__global__ void k_set_limits(KState* S, double tol, int maxiter, int use_rr_as_ff)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        if (use_rr_as_ff) S->ff = S->rr;
+        S->tol2 = tol * tol * S->ff;
+        S->maxiter = maxiter;
+        S->done = 0;
+    }
+}
+
+// Runs a captured chunk of `per_iter` launches per iteration until the state says done.
+template <class F>
+int run_chunks(System& s, F&& enqueue_iteration, int per_iter, int maxiter)
+{
+    int chunk = 4;
+    cudaGraphExec_t exec[8] = {};
+    int k = 0;
+    int rc = MSFEM_OK;
+    while (true) {
+        MSFEM_TRY(read_state(s));
+        if (s.h_kstate->done) break;
+        int ci = 0;
+        while ((4 << ci) < chunk) ci++;
+        if (!exec[ci]) {
+            cudaGraph_t g;
+            MSFEM_CK(cudaStreamBeginCapture(s.stream, cudaStreamCaptureModeThreadLocal));
+            for (int i = 0; i < chunk; i++) enqueue_iteration();
+            cudaError_t e = cudaStreamEndCapture(s.stream, &g);
+            if (e != cudaSuccess) {
+                set_error("graph capture failed: %s", cudaGetErrorString(e));
+                rc = MSFEM_ERR_CUDA;
+                break;
+            }
+            e = cudaGraphInstantiate(&exec[ci], g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) {
+                set_error("graph instantiate failed: %s", cudaGetErrorString(e));
+                rc = MSFEM_ERR_CUDA;
+                break;
+            }
+        }
+        cudaError_t e = cudaGraphLaunch(exec[ci], s.stream);
+        if (e != cudaSuccess) {
+            set_error("graph launch failed: %s", cudaGetErrorString(e));
+            rc = MSFEM_ERR_CUDA;
+            break;
+        }
+        s.launches += chunk * per_iter;
+        k += chunk;
+        if (k > maxiter + 64) break;  // the device state also stops at maxiter; this is a host-side bound
+        if (chunk < 32) chunk *= 2;
+    }
+    for (auto& x : exec)
+        if (x) cudaGraphExecDestroy(x);
+    return rc;
+}
+
+template <class VT>
+struct PcgVectors {
+    VT *x, *r, *z, *p, *q;
+    const VT* dinv;
+};
+
+template <class VT, bool JAC>
+int pcg_run(System& s, PcgVectors<VT> v, int maxiter)
+{
+    const int n = s.n_rows;
+    KState* S = s.kstate.p;
+    double* part = s.partial.p;
+    k_pcg_init<VT, JAC><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, v.r, v.dinv, v.z, v.p, S, part);
+    MSFEM_CK(cudaGetLastError());
+    s.launches += 1;
+    const SellView<VT> A = sell_view<VT>(s);
+    const unsigned g = spmv_grid(s);
+    auto iteration = [&]() {
+        k_pcg_spmv<VT><<<g, 256, 0, s.stream>>>(A, v.p, v.q, S, part);
+        k_pcg_update<VT, JAC><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, v.x, v.r, v.z, v.p, v.q, v.dinv, S, part);
+        k_pcg_p<VT><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, v.z, v.p, S);
+    };
+    return run_chunks(s, iteration, 3, maxiter);
+}
+
+int true_residual(System& s, double* relres)
+{
+    double* r = s.work64.p;
+    MSFEM_TRY(residual64(s, s.X.p, s.F.p, r, &s.kstate.p->rr));
+    MSFEM_TRY(read_state(s));
+    const double rr = s.h_kstate->rr;
+    const double ff = s.h_kstate->ff;
+    *relres = ff > 0 ? std::sqrt(rr / ff) : std::sqrt(rr);
+    return MSFEM_OK;
+}
+
+int solve_pcg64(System& s, bool jacobi, int maxiter, double tol, int* iters)
+{
+    const int n = s.n_rows;
+    MSFEM_TRY(s.work64.alloc(4 * (size_t)n));
+    double* r = s.work64.p;
+    double* z = r + n;
+    double* p = z + n;
+    double* q = p + n;
+    KState* S = s.kstate.p;
+    // ff = (F, F); r = F - A X
+    k_dot_self<double><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, s.F.p, s.partial.p, &S->ticket[1], &S->ff);
+    MSFEM_TRY(residual64(s, s.X.p, s.F.p, r, &S->rr));
+    k_set_limits<<<1, 32, 0, s.stream>>>(S, tol, maxiter, 0);
+    s.launches += 3;
+    PcgVectors<double> v{s.X.p, r, z, p, q, s.dinv64.p};
+    MSFEM_TRY((jacobi ? pcg_run<double, true>(s, v, maxiter) : pcg_run<double, false>(s, v, maxiter)));
+    MSFEM_TRY(read_state(s));
+    *iters = s.h_kstate->iter;
+    return s.h_kstate->done == 1 ? MSFEM_OK : MSFEM_NOT_CONVERGED;
+}
+
+// FP32 matrix and Krylov vectors inside FP64 iterative refinement:
+//   r = F - A x (FP64);  solve A d = r / ||r|| in FP32 to a relative tolerance;  x += ||r|| d (FP64)
+int solve_ir32(System& s, bool jacobi, int maxiter, double tol, int* iters, int* outer)
+{
+    const int n = s.n_rows;
+    MSFEM_TRY(s.work64.alloc(4 * (size_t)n));
+    MSFEM_TRY(s.work32.alloc(6 * (size_t)n));
+    double* r64 = s.work64.p;
+    float* d32 = s.work32.p;
+    float* r32 = d32 + n;
+    float* z32 = r32 + n;
+    float* p32 = z32 + n;
+    float* q32 = p32 + n;
+    KState* S = s.kstate.p;
+    DBuf<double> rr_dev;
+    MSFEM_TRY(rr_dev.alloc(2));
+    k_dot_self<double><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, s.F.p, s.partial.p, &S->ticket[1], &S->ff);
+    s.launches += 1;
+    MSFEM_TRY(read_state(s));
+    const double ff = s.h_kstate->ff;
+    int total_inner = 0;
+    int k = 0;
+    double prev_rr = -1.0;
+    int stalls = 0;
+    for (k = 0; k < kMaxOuter; k++) {
+        MSFEM_TRY(residual64(s, s.X.p, s.F.p, r64, rr_dev.p));
+        s.launches += 1;
+        double rr = 0;
+        MSFEM_CK(cudaMemcpyAsync(&rr, rr_dev.p, sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+        MSFEM_CK(cudaStreamSynchronize(s.stream));
+        if (!(rr == rr)) {
+            set_error("FP32-IR: residual became NaN");
+            return MSFEM_ERR_NUMERIC;
+        }
+        if (rr <= tol * tol * ff || rr == 0.0) break;
+        if (total_inner >= maxiter) break;
+        if (prev_rr >= 0 && rr > 0.25 * prev_rr) {
+            if (++stalls >= 3) break;  // refinement no longer contracts
+        }
+        prev_rr = rr;
+        // inner tolerance: 1e-4, or just what is still missing (with margin) near the end
+        double need = tol * std::sqrt(ff / rr);
+        double tau = std::max(1e-4, std::min(0.5, 0.3 * need));
+        k_scale_to32<<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, r64, rr_dev.p, r32, d32);
+        // inner solve on (r32, r32) ~ 1: the state's ff is the inner right-hand side norm
+        k_dot_self<float><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, r32, s.partial.p, &S->ticket[1], &S->rr);
+        k_set_limits<<<1, 32, 0, s.stream>>>(S, tau, maxiter - total_inner, 1);
+        s.launches += 3;
+        PcgVectors<float> v{d32, r32, z32, p32, q32, s.dinv32.p};
+        MSFEM_TRY((jacobi ? pcg_run<float, true>(s, v, maxiter - total_inner)
+                         : pcg_run<float, false>(s, v, maxiter - total_inner)));
+        MSFEM_TRY(read_state(s));
+        total_inner += s.h_kstate->iter;
+        k_correct<<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, s.X.p, d32, rr_dev.p);
+        s.launches += 1;
+    }
+    // restore ff for the final residual report
+    k_dot_self<double><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, s.F.p, s.partial.p, &S->ticket[1], &S->ff);
+    s.launches += 1;
+    *iters = total_inner;
+    *outer = k;
+    return MSFEM_OK;
+}
+
+int solve_bicgstab64(System& s, int maxiter, double tol, int* iters)
+{
+    const int n = s.n_rows;
+    MSFEM_TRY(s.work64.alloc(9 * (size_t)n));
+    double* r = s.work64.p;
+    double* rhat = r + n;
+    double* p = rhat + n;
+    double* v = p + n;
+    double* y = v + n;
+    double* sv = y + n;
+    double* zz = sv + n;
+    double* t = zz + n;
+    KState* S = s.kstate.p;
+    double* part = s.partial.p;
+    k_dot_self<double><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, s.F.p, part, &S->ticket[1], &S->ff);
+    MSFEM_TRY(residual64(s, s.X.p, s.F.p, r, &S->rr));
+    k_set_limits<<<1, 32, 0, s.stream>>>(S, tol, maxiter, 0);
+    k_bcg_init<double><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, r, rhat, p, v, S, part);
+    MSFEM_CK(cudaGetLastError());
+    s.launches += 4;
+    const SellView<double> A = sell_view<double>(s);
+    const unsigned g = spmv_grid(s);
+    const double* dinv = s.dinv64.p;
+    double* x = s.X.p;
+    auto iteration = [&]() {
+        k_bcg_p<double><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, r, p, v, y, dinv, S);
+        k_bcg_spmv_alpha<double><<<g, 256, 0, s.stream>>>(A, y, v, rhat, S, part);
+        k_bcg_s<double><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, r, v, sv, zz, dinv, S);
+        k_bcg_spmv_omega<double><<<g, 256, 0, s.stream>>>(A, zz, t, sv, S, part);
+        k_bcg_update<double><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, x, r, y, zz, sv, t, rhat, S, part);
+    };
+    MSFEM_TRY(run_chunks(s, iteration, 5, maxiter));
+    MSFEM_TRY(read_state(s));
+    *iters = s.h_kstate->iter;
+    return s.h_kstate->done == 1 ? MSFEM_OK : MSFEM_NOT_CONVERGED;
+}
+
+}  // namespace
+
+int solve_gmres64(System& s, int m, int maxiter, double tol, int* iters, int* restarts);  // gmres.cu
+
+int solve(System& s, int method, int precision, int restart_m, int maxiter, double tol, double* relres, int* iters)
+{
+    if (maxiter <= 0 || !(tol >= 0)) {
+        set_error("solve: maxiter must be > 0 and tol >= 0");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    MSFEM_TRY(prepare_sell(s));
+    MSFEM_TRY(ensure_state(s));
+    s.launches = 0;
+    Timer timer(s);
+    int it = 0, outer = 0;
+    int rc = MSFEM_OK;
+    const bool jac = method != MSFEM_CG;
+    if (method != MSFEM_CG && s.zero_diag) {
+        set_error("solve: the matrix has a zero diagonal entry; Jacobi preconditioning is undefined (use MSFEM_CG)");
+        return MSFEM_ERR_NUMERIC;
+    }
+    switch (method) {
+    case MSFEM_CG:
+    case MSFEM_PCG_JACOBI:
+        if (precision == MSFEM_FP64) rc = solve_pcg64(s, jac, maxiter, tol, &it);
+        else if (precision == MSFEM_FP32_IR) rc = solve_ir32(s, jac, maxiter, tol, &it, &outer);
+        else rc = MSFEM_ERR_ARGUMENT;
+        break;
+    case MSFEM_BICGSTAB:
+        rc = solve_bicgstab64(s, maxiter, tol, &it);
+        break;
+    case MSFEM_GMRES:
+        rc = solve_gmres64(s, restart_m > 0 ? restart_m : 30, maxiter, tol, &it, &outer);
+        break;
+    default:
+        rc = MSFEM_ERR_ARGUMENT;
+    }
+    if (rc == MSFEM_ERR_ARGUMENT) set_error("solve: unknown method %d / precision %d", method, precision);
+    if (rc < 0) return rc;
+    double rel = 0;
+    MSFEM_TRY(true_residual(s, &rel));
+    s.launches += 1;
+    s.stats.ms_solve = timer.stop();
+    s.stats.iterations = it;
+    s.stats.outer_iterations = outer;
+    s.stats.rel_residual = rel;
+    s.stats.kernel_launches = s.launches;
+    s.total_launches += s.launches;
+    if (relres) *relres = rel;
+    if (iters) *iters = it;
+    if (precision == MSFEM_FP32_IR && rc == MSFEM_OK && !(rel <= tol * (1.0 + 1e-6))) rc = MSFEM_NOT_CONVERGED;
+    return rc;
+}
+
+}  // namespace msfem

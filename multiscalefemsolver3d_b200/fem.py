@@ -1,0 +1,228 @@
+"""Python view of the C ABI: one `System` per assembled matrix, plus the two
+driver calls.  Method names follow the reference's step names
+(CreationPortrait -> System(...), SolveLocalMatrix + SummPartOfMatrix ->
+assemble_*, first/second boundary conditions -> apply_dirichlet /
+add_traction, MSG / MSG_PreconditioningSSOR -> solve).
+
+Arrays may be numpy arrays (host) or torch CUDA tensors (device, used in
+place).  Every call goes through libmsfem_b200.so; nothing here computes.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import (BICGSTAB, CG, ELASTIC, FP32_IR, FP64, GMRES, PCG_JACOBI, ROW_AND_COLUMN, ROW_ONLY, SCALAR,
+                   Stats, check, load)
+
+__all__ = ["System", "Csr", "fem_scalar_driver", "fem_elastic_driver", "CG", "PCG_JACOBI", "BICGSTAB", "GMRES",
+           "FP64", "FP32_IR", "ROW_ONLY", "ROW_AND_COLUMN", "SCALAR", "ELASTIC"]
+
+
+def _ptr(a, dtype):
+    """(pointer, on_device, keepalive) for a numpy array or a torch tensor."""
+    if a is None:
+        return None, 0, None
+    if hasattr(a, "data_ptr") and hasattr(a, "is_cuda"):
+        if a.is_cuda:
+            import torch
+            want = {np.float64: torch.float64, np.int32: torch.int32, np.float32: torch.float32}[dtype]
+            if a.dtype != want or not a.is_contiguous():
+                raise TypeError(f"device tensor must be contiguous {want}")
+            return C.c_void_p(a.data_ptr()), 1, a
+        a = a.cpu().numpy()
+    arr = np.ascontiguousarray(a, dtype=dtype)
+    return arr.ctypes.data_as(C.c_void_p), 0, arr
+
+
+@dataclass
+class Csr:
+    """CSR with the diagonal in place; row = reference CSSD row [A_down | Diag | A_up]."""
+    row_ptr: np.ndarray
+    col: np.ndarray
+    val: np.ndarray
+    F: np.ndarray
+    X: np.ndarray
+
+    @property
+    def n(self) -> int:
+        return self.row_ptr.size - 1
+
+    def to_scipy(self):
+        import scipy.sparse as sp
+        return sp.csr_matrix((self.val, self.col, self.row_ptr), shape=(self.n, self.n))
+
+    def cssd(self):
+        """(Diag, A_up, A_down, id_column_for_A_up, id_column_for_A_down) as in Library/CSSD_Matrix.h:11-13."""
+        diag = np.zeros(self.n)
+        up, down, cu, cd = [], [], [], []
+        for i in range(self.n):
+            c = self.col[self.row_ptr[i]:self.row_ptr[i + 1]]
+            v = self.val[self.row_ptr[i]:self.row_ptr[i + 1]]
+            d = np.searchsorted(c, i)
+            diag[i] = v[d]
+            down.append(v[:d]); cd.append(c[:d])
+            up.append(v[d + 1:]); cu.append(c[d + 1:])
+        return diag, up, down, cu, cd
+
+
+class System:
+    """An assembled FEM system on the GPU (Grid + CSSD_Matrix of the reference)."""
+
+    def __init__(self, kind: int, xyz, tets, material=None):
+        L = load()
+        self.kind = kind
+        px, dx, kx = _ptr(xyz, np.float64)
+        pt, dt, kt = _ptr(tets, np.int32)
+        pm, dm, km = _ptr(material, np.int32)
+        n_nodes = int(xyz.shape[0]) if xyz.ndim == 2 else int(xyz.shape[0] // 3)
+        n_tets = int(tets.shape[0]) if tets.ndim == 2 else int(tets.shape[0] // 4)
+        h = C.c_void_p()
+        check(L.msfem_system_create(kind, n_nodes, px, n_tets, pt, pm, int(dx or dt), C.byref(h)), "system_create")
+        self.h = h
+        self.n_nodes = n_nodes
+        n_rows, nnz, nc = C.c_int(), C.c_int64(), C.c_int()
+        check(L.msfem_system_info(h, C.byref(n_rows), C.byref(nnz), C.byref(nc)), "system_info")
+        self.n_rows, self.nnz, self.n_colors = n_rows.value, nnz.value, nc.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().msfem_system_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- assembly and boundary conditions
+    def assemble_scalar(self, sigma):
+        s = np.ascontiguousarray(sigma, dtype=np.float64)
+        check(load().msfem_assemble_scalar(self.h, s.ctypes.data_as(C.c_void_p), s.size), "assemble_scalar")
+
+    def assemble_elastic(self, E, nu):
+        e = np.ascontiguousarray(E, dtype=np.float64)
+        n = np.ascontiguousarray(nu, dtype=np.float64)
+        check(load().msfem_assemble_elastic(self.h, e.ctypes.data_as(C.c_void_p), n.ctypes.data_as(C.c_void_p),
+                                            e.size), "assemble_elastic")
+
+    def add_traction(self, faces, traction):
+        pf, d1, k1 = _ptr(faces, np.int32)
+        pt, d2, k2 = _ptr(traction, np.float64)
+        nf = int(faces.shape[0]) if faces.ndim == 2 else int(faces.shape[0] // 3)
+        check(load().msfem_add_traction(self.h, nf, pf, pt, int(d1 or d2)), "add_traction")
+
+    def add_rhs(self, f):
+        p, d, k = _ptr(f, np.float64)
+        check(load().msfem_add_rhs(self.h, p, d), "add_rhs")
+
+    def apply_dirichlet(self, dofs, values, mode: int = ROW_AND_COLUMN):
+        pd, d1, k1 = _ptr(dofs, np.int32)
+        pv, d2, k2 = _ptr(values, np.float64)
+        n = int(np.asarray(dofs.shape).prod()) if hasattr(dofs, "shape") else len(dofs)
+        check(load().msfem_apply_dirichlet(self.h, n, pd, pv, mode, int(d1 or d2)), "apply_dirichlet")
+
+    def clear(self):
+        check(load().msfem_clear(self.h), "clear")
+
+    # -- vectors
+    def set_x(self, x):
+        p, d, k = _ptr(x, np.float64)
+        check(load().msfem_set_x(self.h, p, d), "set_x")
+
+    def get_x(self, out=None):
+        out = np.empty(self.n_rows) if out is None else out
+        p, d, k = _ptr(out, np.float64)
+        check(load().msfem_get_x(self.h, p, d), "get_x")
+        return out
+
+    def get_f(self):
+        out = np.empty(self.n_rows)
+        check(load().msfem_get_f(self.h, out.ctypes.data_as(C.c_void_p), 0), "get_f")
+        return out
+
+    def copy_f_to_x(self):
+        check(load().msfem_copy_f_to_x(self.h), "copy_f_to_x")
+
+    # -- solve
+    def solve(self, method: int = PCG_JACOBI, precision: int = FP64, tol: float = 1e-10, maxiter: int = 100000,
+              restart: int = 30):
+        rel, it = C.c_double(), C.c_int()
+        rc = check(load().msfem_solve(self.h, method, precision, restart, maxiter, tol, C.byref(rel), C.byref(it)),
+                   "solve")
+        return rel.value, it.value, rc
+
+    def spmv(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty(self.n_rows)
+        check(load().msfem_spmv(self.h, x.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p), 0), "spmv")
+        return y
+
+    def export_csr(self) -> Csr:
+        rp = np.empty(self.n_rows + 1, dtype=np.int32)
+        col = np.empty(self.nnz, dtype=np.int32)
+        val = np.empty(self.nnz)
+        check(load().msfem_export_csr(self.h, rp.ctypes.data_as(C.c_void_p), col.ctypes.data_as(C.c_void_p),
+                                      val.ctypes.data_as(C.c_void_p), 0), "export_csr")
+        return Csr(rp, col, val, self.get_f(), self.get_x())
+
+    def stats(self) -> dict:
+        st = Stats()
+        check(load().msfem_get_stats(self.h, C.byref(st)), "get_stats")
+        return st.as_dict()
+
+    def bench_spmv(self, precision: int = FP64, reps: int = 50):
+        ms, nb = C.c_double(), C.c_int64()
+        check(load().msfem_bench_spmv(self.h, precision, reps, C.byref(ms), C.byref(nb)), "bench_spmv")
+        return ms.value, nb.value
+
+    @property
+    def stream(self) -> int:
+        return load().msfem_get_stream(self.h) or 0
+
+
+# ------------------------------------------------------------------ one-call drivers
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+def fem_scalar_driver(p, method=PCG_JACOBI, precision=FP64, min_residual=1e-10, maxiter=200000):
+    """FEM::FEM_forBaseEliptic (stiffness-only) on the GPU; returns (solution, stats, rc)."""
+    m = p.mesh
+    xyz, tets, mat = _c(m.xyz, np.float64), _c(m.tets, np.int32), _c(m.mat, np.int32)
+    sig, bn, bv = _c(p.sigma, np.float64), _c(p.bc_nodes, np.int32), _c(p.bc_values, np.float64)
+    sol = np.empty(m.n_nodes)
+    st = Stats()
+    P = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    rc = check(load().msfem_fem_scalar_driver(m.n_nodes, P(xyz), m.n_tets, P(tets), P(mat), sig.size, P(sig),
+                                               bn.size, P(bn), P(bv), method, precision, min_residual, maxiter,
+                                               P(sol), C.byref(st)), "fem_scalar_driver")
+    return sol, st.as_dict(), rc
+
+
+def fem_elastic_driver(p, method=PCG_JACOBI, precision=FP64, min_residual=1e-10, maxiter=200000):
+    """FEM::FEM_forElasticDeformation on the GPU; returns (solution[3n], stats, rc)."""
+    m = p.mesh
+    xyz, tets, mat = _c(m.xyz, np.float64), _c(m.tets, np.int32), _c(m.mat, np.int32)
+    E, nu = _c(p.E, np.float64), _c(p.nu, np.float64)
+    bn, bm, bv = _c(p.bc_nodes, np.int32), _c(p.bc_mask, np.int32), _c(p.bc_values, np.float64)
+    fc, ft = _c(p.faces, np.int32), _c(p.traction, np.float64)
+    sol = np.empty(3 * m.n_nodes)
+    st = Stats()
+    P = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    rc = check(load().msfem_fem_elastic_driver(m.n_nodes, P(xyz), m.n_tets, P(tets), P(mat), E.size, P(E), P(nu),
+                                                bn.size, P(bn), P(bm), P(bv), fc.shape[0], P(fc), P(ft), method,
+                                                precision, min_residual, maxiter, P(sol), C.byref(st)),
+               "fem_elastic_driver")
+    return sol, st.as_dict(), rc
