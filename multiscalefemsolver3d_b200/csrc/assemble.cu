@@ -230,10 +230,10 @@ int assemble_scalar(System& s, const double* sigma, int n_mat)
         set_error("assemble_scalar: no materials");
         return MSFEM_ERR_ARGUMENT;
     }
-    DBuf<double> d_sig;
-    DBuf<int> bad;
+    DBuf<double>& d_sig = s.params;
+    DBuf<int>& bad = s.flag;
     MSFEM_TRY(d_sig.alloc(n_mat));
-    MSFEM_TRY(bad.alloc(1));
+    MSFEM_TRY(bad.alloc(8));
     MSFEM_CK(cudaEventRecord(s.ev0, s.stream));
     MSFEM_CK(cudaMemcpyAsync(d_sig.p, sigma, sizeof(double) * n_mat, cudaMemcpyHostToDevice, s.stream));
     MSFEM_CK(cudaMemsetAsync(bad.p, 0, sizeof(int), s.stream));
@@ -274,10 +274,10 @@ int assemble_elastic(System& s, const double* E, const double* nu, int n_mat)
         lame[2 * m] = a * k;
         lame[2 * m + 1] = b * k;
     }
-    DBuf<double> d_lame;
-    DBuf<int> bad;
+    DBuf<double>& d_lame = s.params;
+    DBuf<int>& bad = s.flag;
     MSFEM_TRY(d_lame.alloc(2 * (size_t)n_mat));
-    MSFEM_TRY(bad.alloc(1));
+    MSFEM_TRY(bad.alloc(8));
     MSFEM_CK(cudaEventRecord(s.ev0, s.stream));
     MSFEM_CK(cudaMemcpyAsync(d_lame.p, lame.data(), sizeof(double) * 2 * n_mat, cudaMemcpyHostToDevice, s.stream));
     MSFEM_CK(cudaMemsetAsync(bad.p, 0, sizeof(int), s.stream));
@@ -301,21 +301,21 @@ int add_traction(System& s, int n_faces, const int32_t* d_faces, const double* d
     }
     if (n_faces <= 0) return MSFEM_OK;
     const int m = 3 * n_faces;
-    DBuf<int32_t> key, idx, key2, idx2;
-    DBuf<double> contrib;
-    DBuf<int> bad;
+    DBuf<int32_t>&key = s.sc_i32[1], &idx = s.sc_i32[2], &key2 = s.sc_i32[3], &idx2 = s.sc_i32[4];
+    DBuf<double>& contrib = s.sc_f64[1];
+    DBuf<int>& bad = s.flag;
     MSFEM_TRY(key.alloc(m));
     MSFEM_TRY(idx.alloc(m));
     MSFEM_TRY(key2.alloc(m));
     MSFEM_TRY(idx2.alloc(m));
     MSFEM_TRY(contrib.alloc(3 * (size_t)m));
-    MSFEM_TRY(bad.alloc(1));
+    MSFEM_TRY(bad.alloc(8));
     MSFEM_CK(cudaMemsetAsync(bad.p, 0, sizeof(int), s.stream));
     k_traction_contrib<<<grid_for(n_faces, 128), 128, 0, s.stream>>>(n_faces, d_faces, d_traction, s.xyz.p, s.n_nodes,
                                                                      key.p, idx.p, contrib.p, bad.p);
     MSFEM_CK(cudaGetLastError());
     size_t tmp_bytes = 0;
-    DBuf<unsigned char> tmp;
+    DBuf<unsigned char>& tmp = s.sc_tmp;
     cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, key.p, key2.p, idx.p, idx2.p, m, 0, 32, s.stream);
     MSFEM_TRY(tmp.alloc(tmp_bytes + 1));
     MSFEM_CK(cub::DeviceRadixSort::SortPairs(tmp.p, tmp_bytes, key.p, key2.p, idx.p, idx2.p, m, 0, 32, s.stream));

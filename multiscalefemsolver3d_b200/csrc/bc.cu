@@ -42,10 +42,10 @@ __global__ void k_iota(int n, int32_t* a)
 __global__ void k_dirichlet_rows(int L, const int32_t* __restrict__ sdof, const int32_t* __restrict__ spos,
                                  const double* __restrict__ values, int bs, const int32_t* __restrict__ nrp,
                                  const int32_t* __restrict__ ncol, double* __restrict__ val, double* __restrict__ F,
-                                 double* __restrict__ X)
+                                 double* __restrict__ X, const int* bad)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= L) return;
+    if (i >= L || *bad) return;
     const int d = sdof[i];
     if (i + 1 < L && sdof[i + 1] == d) return;
     const double v = values[spos[i]];
@@ -105,10 +105,10 @@ __device__ __forceinline__ void eliminate(double* __restrict__ a, double& f, con
 
 __global__ void k_column_sweep(int n_rows, int bs, const int32_t* __restrict__ nrp, const int32_t* __restrict__ ncol,
                                double* __restrict__ val, double* __restrict__ F, const int32_t* __restrict__ u,
-                               const int32_t* __restrict__ st, int L, int T)
+                               const int32_t* __restrict__ st, int L, int T, const int* bad)
 {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= n_rows) return;
+    if (r >= n_rows || *bad) return;
     double f = F[r];
     const double f0 = f;
     Walk w{st, u, L, T, 0};
@@ -159,52 +159,47 @@ int apply_dirichlet(System& s, int L, const int32_t* d_dofs, const double* d_val
         return MSFEM_ERR_ARGUMENT;
     }
     cudaStream_t st = s.stream;
-    DBuf<int> bad;
-    MSFEM_TRY(bad.alloc(1));
-    MSFEM_CK(cudaEventRecord(s.ev0, st));
-    MSFEM_CK(cudaMemsetAsync(bad.p, 0, sizeof(int), st));
-    k_check_dofs<<<grid_for(L, 256), 256, 0, st>>>(L, d_dofs, s.n_rows, bad.p);
-    MSFEM_CK(cudaGetLastError());
-    int h_bad = 0;
-    MSFEM_CK(cudaMemcpyAsync(&h_bad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-    MSFEM_CK(cudaStreamSynchronize(st));
-    if (h_bad) {
-        set_error("a Dirichlet DOF is outside [0, %d)", s.n_rows);
-        return MSFEM_ERR_ARGUMENT;
-    }
-    // rows
-    DBuf<int32_t> pos, sdof, spos;
+    // scratch: sc_i32[0] may hold the caller's DOF list, so [1..4] are used here
+    DBuf<int>& bad = s.flag;
+    DBuf<int32_t>&pos = s.sc_i32[1], &sdof = s.sc_i32[2], &spos = s.sc_i32[3], &table = s.sc_i32[4];
+    MSFEM_TRY(bad.alloc(8));
     MSFEM_TRY(pos.alloc(L));
     MSFEM_TRY(sdof.alloc(L));
     MSFEM_TRY(spos.alloc(L));
-    k_iota<<<grid_for(L, 256), 256, 0, st>>>(L, pos.p);
+    int T = 0;
+    while ((2 << T) <= L) T++;  // sparse-table levels 0..T, 2^T <= L
+    if (mode == MSFEM_ROW_AND_COLUMN) MSFEM_TRY(table.alloc((size_t)(T + 1) * L));
     size_t tmp_bytes = 0;
-    DBuf<unsigned char> tmp;
     cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, d_dofs, sdof.p, pos.p, spos.p, L, 0, 32, st);
-    MSFEM_TRY(tmp.alloc(tmp_bytes + 1));
-    MSFEM_CK(cub::DeviceRadixSort::SortPairs(tmp.p, tmp_bytes, d_dofs, sdof.p, pos.p, spos.p, L, 0, 32, st));
+    MSFEM_TRY(s.sc_tmp.alloc(tmp_bytes + 1));
+
+    MSFEM_CK(cudaEventRecord(s.ev0, st));
+    MSFEM_CK(cudaMemsetAsync(bad.p, 0, sizeof(int), st));
+    // every kernel below that indexes by a DOF first reads this flag and does nothing if it is set
+    k_check_dofs<<<grid_for(L, 256), 256, 0, st>>>(L, d_dofs, s.n_rows, bad.p);
+    k_iota<<<grid_for(L, 256), 256, 0, st>>>(L, pos.p);
+    MSFEM_CK(cub::DeviceRadixSort::SortPairs(s.sc_tmp.p, tmp_bytes, d_dofs, sdof.p, pos.p, spos.p, L, 0, 32, st));
     k_dirichlet_rows<<<grid_for(L, 128), 128, 0, st>>>(L, sdof.p, spos.p, d_values, s.bs, s.nrp.p, s.ncol.p, s.val.p,
-                                                       s.F.p, s.X.p);
+                                                       s.F.p, s.X.p, bad.p);
     MSFEM_CK(cudaGetLastError());
     s.total_launches += 3;  // check, iota, rows (the radix sort's own kernels are not counted)
     if (mode == MSFEM_ROW_AND_COLUMN) {
-        int T = 0;
-        while ((2 << T) <= L) T++;  // levels 0..T with 2^T <= L
-        DBuf<int32_t> table;
-        MSFEM_TRY(table.alloc((size_t)(T + 1) * L));
         MSFEM_CK(cudaMemcpyAsync(table.p, d_dofs, sizeof(int32_t) * L, cudaMemcpyDeviceToDevice, st));
         for (int t = 1; t <= T; t++)
             k_sparse_level<<<grid_for(L, 256), 256, 0, st>>>(L, 1 << (t - 1), table.p + (size_t)(t - 1) * L,
                                                              table.p + (size_t)t * L);
         k_column_sweep<<<grid_for(s.n_rows, 128), 128, 0, st>>>(s.n_rows, s.bs, s.nrp.p, s.ncol.p, s.val.p, s.F.p,
-                                                                d_dofs, table.p, L, T);
+                                                                d_dofs, table.p, L, T, bad.p);
         MSFEM_CK(cudaGetLastError());
         s.total_launches += T + 1;
-        MSFEM_CK(cudaEventRecord(s.ev1, st));
-        MSFEM_CK(cudaStreamSynchronize(st));
-    } else {
-        MSFEM_CK(cudaEventRecord(s.ev1, st));
-        MSFEM_CK(cudaStreamSynchronize(st));
+    }
+    int h_bad = 0;
+    MSFEM_CK(cudaMemcpyAsync(&h_bad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MSFEM_CK(cudaEventRecord(s.ev1, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    if (h_bad) {
+        set_error("a Dirichlet DOF is outside [0, %d); the system is unchanged", s.n_rows);
+        return MSFEM_ERR_ARGUMENT;
     }
     float ms = 0;
     cudaEventElapsedTime(&ms, s.ev0, s.ev1);

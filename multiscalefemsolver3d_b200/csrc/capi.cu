@@ -168,6 +168,9 @@ int msfem_system_destroy(msfem_system_t h)
     if (s->h_kstate) cudaFreeHost(s->h_kstate);
     cudaStream_t st = s->stream;
     cudaEvent_t e0 = s->ev0, e1 = s->ev1;
+    for (auto& kv : s->graphs)
+        for (auto g : kv.second)
+            if (g) cudaGraphExecDestroy(g);
     delete s;  // device buffers are released by their owners
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
@@ -233,8 +236,8 @@ int msfem_add_traction(msfem_system_t h, int n_faces, const int32_t* face_nodes,
         return MSFEM_ERR_ARGUMENT;
     }
     if (n_faces == 0) return MSFEM_OK;
-    DBuf<int32_t> f;
-    DBuf<double> t;
+    DBuf<int32_t>& f = s.sc_i32[0];
+    DBuf<double>& t = s.sc_f64[0];
     MSFEM_TRY(to_device(s, f, face_nodes, 3 * (size_t)n_faces));
     MSFEM_TRY(to_device(s, t, traction, 3 * (size_t)n_faces));
     return add_traction(s, n_faces, f.p, t.p);
@@ -250,7 +253,7 @@ int msfem_add_rhs(msfem_system_t h, const double* f, int on_device)
         set_error("msfem_add_rhs: null vector");
         return MSFEM_ERR_ARGUMENT;
     }
-    DBuf<double> d;
+    DBuf<double>& d = s.sc_f64[0];
     MSFEM_TRY(to_device(s, d, f, (size_t)s.n_rows));
     k_add<<<grid_for(s.n_rows, 256), 256, 0, s.stream>>>(s.n_rows, d.p, s.F.p);
     MSFEM_CK(cudaGetLastError());
@@ -270,8 +273,8 @@ int msfem_apply_dirichlet(msfem_system_t h, int n, const int32_t* dofs, const do
         return MSFEM_ERR_ARGUMENT;
     }
     if (n == 0) return MSFEM_OK;
-    DBuf<int32_t> d;
-    DBuf<double> v;
+    DBuf<int32_t>& d = s.sc_i32[0];
+    DBuf<double>& v = s.sc_f64[0];
     MSFEM_TRY(to_device(s, d, dofs, (size_t)n));
     MSFEM_TRY(to_device(s, v, values, (size_t)n));
     return apply_dirichlet(s, n, d.p, v.p, mode);

@@ -4,8 +4,10 @@
 #include <cuda_runtime.h>
 
 #include <cstdarg>
+#include <array>
 #include <cstdint>
 #include <cstdio>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -128,6 +130,18 @@ struct System {
     DBuf<KState> kstate;
     KState* h_kstate = nullptr;  // pinned mirror for polling
     DBuf<double> gm;      // GMRES: Hessenberg / rotations / y on the device
+
+    // reusable scratch: once grown, the per-step calls (assembly, Dirichlet,
+    // solve) allocate and free nothing, so they neither block nor serialise
+    DBuf<int> flag;        // device flags (8 ints)
+    DBuf<double> params;   // material parameters
+    DBuf<int32_t> sc_i32[6];
+    DBuf<double> sc_f64[2];
+    DBuf<unsigned char> sc_tmp;
+
+    // captured iteration graphs, keyed by solver variant and vector addresses;
+    // index = log2(chunk / 4)
+    std::map<std::string, std::array<cudaGraphExec_t, 8>> graphs;
 
     bool zero_diag = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;

@@ -462,10 +462,15 @@ __global__ void k_set_limits(KState* S, double tol, int maxiter, int use_rr_as_f
 
 // Runs a captured chunk of `per_iter` launches per iteration until the state says done.
 template <class F>
-int run_chunks(System& s, F&& enqueue_iteration, int per_iter, int maxiter)
+int run_chunks(System& s, const std::string& key, F&& enqueue_iteration, int per_iter, int maxiter)
 {
     int chunk = 4;
-    cudaGraphExec_t exec[8] = {};
+    auto it = s.graphs.find(key);
+    if (it == s.graphs.end()) {
+        std::array<cudaGraphExec_t, 8> empty{};
+        it = s.graphs.emplace(key, empty).first;
+    }
+    cudaGraphExec_t* exec = it->second.data();
     int k = 0;
     int rc = MSFEM_OK;
     while (true) {
@@ -502,9 +507,19 @@ int run_chunks(System& s, F&& enqueue_iteration, int per_iter, int maxiter)
         if (k > maxiter + 64) break;  // the device state also stops at maxiter; this is a host-side bound
         if (chunk < 32) chunk *= 2;
     }
-    for (auto& x : exec)
-        if (x) cudaGraphExecDestroy(x);
     return rc;
+}
+
+std::string graph_key(const char* tag, std::initializer_list<const void*> ptrs, int n)
+{
+    std::string k(tag);
+    char buf[32];
+    for (const void* p : ptrs) {
+        std::snprintf(buf, sizeof(buf), ":%p", p);
+        k += buf;
+    }
+    std::snprintf(buf, sizeof(buf), ":%d", n);
+    return k + buf;
 }
 
 template <class VT>
@@ -529,7 +544,9 @@ int pcg_run(System& s, PcgVectors<VT> v, int maxiter)
         k_pcg_update<VT, JAC><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, v.x, v.r, v.z, v.p, v.q, v.dinv, S, part);
         k_pcg_p<VT><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, v.z, v.p, S);
     };
-    return run_chunks(s, iteration, 3, maxiter);
+    const std::string key = graph_key(sizeof(VT) == 8 ? (JAC ? "pcg64j" : "pcg64") : (JAC ? "pcg32j" : "pcg32"),
+                                      {v.x, v.r, v.z, v.p, v.q, v.dinv, A.val, A.col, (const void*)S, part}, n);
+    return run_chunks(s, key, iteration, 3, maxiter);
 }
 
 int true_residual(System& s, double* relres)
@@ -578,7 +595,7 @@ int solve_ir32(System& s, bool jacobi, int maxiter, double tol, int* iters, int*
     float* p32 = z32 + n;
     float* q32 = p32 + n;
     KState* S = s.kstate.p;
-    DBuf<double> rr_dev;
+    DBuf<double>& rr_dev = s.sc_f64[1];
     MSFEM_TRY(rr_dev.alloc(2));
     k_dot_self<double><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, s.F.p, s.partial.p, &S->ticket[1], &S->ff);
     s.launches += 1;
@@ -659,7 +676,8 @@ int solve_bicgstab64(System& s, int maxiter, double tol, int* iters)
         k_bcg_spmv_omega<double><<<g, 256, 0, s.stream>>>(A, zz, t, sv, S, part);
         k_bcg_update<double><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, x, r, y, zz, sv, t, rhat, S, part);
     };
-    MSFEM_TRY(run_chunks(s, iteration, 5, maxiter));
+    const std::string key = graph_key("bicgstab64", {x, r, rhat, p, v, y, sv, zz, t, dinv, A.val, (const void*)S, part}, n);
+    MSFEM_TRY(run_chunks(s, key, iteration, 5, maxiter));
     MSFEM_TRY(read_state(s));
     *iters = s.h_kstate->iter;
     return s.h_kstate->done == 1 ? MSFEM_OK : MSFEM_NOT_CONVERGED;

@@ -138,35 +138,82 @@ __global__ void k_element_slots(int n_tets, const int32_t* __restrict__ tets, co
         }
 }
 
-// Jones-Plassmann colouring of the element conflict graph (elements conflict when
-// they share a node).  In round `c` an uncoloured element takes colour c when its
-// priority beats every neighbour that was still uncoloured when the round began
-// (neighbours coloured c in this same round had a higher priority than it, so the
-// outcome does not depend on the order in which threads run).
-__global__ void k_color_round(int n_tets, const int32_t* __restrict__ tets, const int32_t* __restrict__ inc_ptr,
-                              const int32_t* __restrict__ inc, int32_t* color, int c, unsigned int* remaining)
+// Speculative greedy colouring of the element conflict graph (elements
+// conflict when they share a node), deterministic by construction:
+//  1. every uncoloured element proposes the smallest colour that none of its
+//     already-coloured neighbours holds (reads only colours committed in
+//     earlier rounds);
+//  2. among neighbours that proposed the same colour in this round, the one
+//     with the highest priority (hash of the id, ties by id) keeps it;
+//  3. winners are committed, losers try again in the next round.
+// Each kernel only reads arrays that no thread of the same kernel writes, so
+// the colouring -- and with it the order in which the assembly adds element
+// contributions -- is identical on every run.
+constexpr int kMaxColors = 256;
+
+__global__ void k_color_propose(int n_tets, const int32_t* __restrict__ tets, const int32_t* __restrict__ inc_ptr,
+                                const int32_t* __restrict__ inc, const int32_t* __restrict__ color,
+                                int32_t* __restrict__ tent, int* overflow)
 {
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n_tets) return;
-    if (color[e] >= 0) return;
+    if (color[e] >= 0) {
+        tent[e] = -1;
+        return;
+    }
+    unsigned used[kMaxColors / 32];
+#pragma unroll
+    for (int w = 0; w < kMaxColors / 32; w++) used[w] = 0u;
+    for (int a = 0; a < 4; a++) {
+        const int v = tets[4 * (int64_t)e + a];
+        for (int k = inc_ptr[v]; k < inc_ptr[v + 1]; k++) {
+            const int c = color[inc[k]];
+            if (c >= 0) used[c >> 5] |= 1u << (c & 31);
+        }
+    }
+    int pick = -1;
+#pragma unroll
+    for (int w = 0; w < kMaxColors / 32; w++)
+        if (pick < 0 && used[w] != 0xffffffffu) pick = 32 * w + __ffs(~used[w]) - 1;
+    if (pick < 0) atomicExch(overflow, 1);
+    tent[e] = pick;
+}
+
+__global__ void k_color_resolve(int n_tets, const int32_t* __restrict__ tets, const int32_t* __restrict__ inc_ptr,
+                                const int32_t* __restrict__ inc, const int32_t* __restrict__ tent,
+                                int32_t* __restrict__ win)
+{
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n_tets) return;
+    const int c = tent[e];
+    if (c < 0) {
+        win[e] = 0;
+        return;
+    }
     const unsigned pe = hash32((unsigned)e);
     bool best = true;
     for (int a = 0; a < 4 && best; a++) {
-        int v = tets[4 * (int64_t)e + a];
+        const int v = tets[4 * (int64_t)e + a];
         for (int k = inc_ptr[v]; k < inc_ptr[v + 1]; k++) {
-            int f = inc[k];
-            if (f == e) continue;
-            int cf = ((volatile int32_t*)color)[f];
-            if (cf >= 0 && cf != c) continue;  // coloured in an earlier round
-            unsigned pf = hash32((unsigned)f);
+            const int f = inc[k];
+            if (f == e || tent[f] != c) continue;
+            const unsigned pf = hash32((unsigned)f);
             if (pf > pe || (pf == pe && f > e)) {
                 best = false;
                 break;
             }
         }
     }
-    if (best) color[e] = c;
-    else atomicAdd(remaining, 1u);
+    win[e] = best ? 1 : 0;
+}
+
+__global__ void k_color_commit(int n_tets, const int32_t* __restrict__ tent, const int32_t* __restrict__ win,
+                               int32_t* __restrict__ color, unsigned int* remaining)
+{
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n_tets) return;
+    if (win[e]) color[e] = tent[e];
+    else if (color[e] < 0) atomicAdd(remaining, 1u);
 }
 
 // off[c] = first position of colour c in the sorted key array
@@ -175,6 +222,12 @@ __global__ void k_color_starts(int n, const int32_t* __restrict__ keys, int32_t*
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (i == 0 || keys[i] != keys[i - 1]) off[keys[i]] = i;
+}
+
+__global__ void k_max(int n, const int32_t* __restrict__ a, int32_t* mx)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) atomicMax(mx, a[i]);
 }
 
 __global__ void k_iota(int n, int32_t* a)
@@ -191,9 +244,9 @@ int build_topology(System& s)
 {
     cudaStream_t st = s.stream;
     const int N = s.n_nodes, E = s.n_tets;
-    DBuf<int> flags;
-    MSFEM_TRY(flags.alloc(4));
-    MSFEM_CK(cudaMemsetAsync(flags.p, 0, 4 * sizeof(int), st));
+    DBuf<int> flags;  // [0] bad node id, [1] overflow, [2] bad slot, [3] uncoloured count, [4] max colour
+    MSFEM_TRY(flags.alloc(8));
+    MSFEM_CK(cudaMemsetAsync(flags.p, 0, 8 * sizeof(int), st));
 
     // ---- incidence
     MSFEM_TRY(s.inc_ptr.alloc((size_t)N + 1));
@@ -252,24 +305,46 @@ int build_topology(System& s)
     MSFEM_CK(cudaGetLastError());
 
     // ---- colouring
-    DBuf<int32_t> color;
+    DBuf<int32_t> color, tent, win;
     MSFEM_TRY(color.alloc((size_t)E));
+    MSFEM_TRY(tent.alloc((size_t)E));
+    MSFEM_TRY(win.alloc((size_t)E));
     MSFEM_CK(cudaMemsetAsync(color.p, 0xff, sizeof(int32_t) * (size_t)E, st));
     unsigned int* remaining = reinterpret_cast<unsigned int*>(flags.p + 3);
-    int n_colors = 0;
-    for (int c = 0;; c++) {
-        if (c >= 4096) {
-            set_error("element colouring did not finish in 4096 rounds");
+    int rounds = 0;
+    for (;;) {
+        if (rounds >= 1024) {
+            set_error("element colouring did not finish in 1024 rounds");
             return MSFEM_ERR_LIMIT;
         }
         MSFEM_CK(cudaMemsetAsync(remaining, 0, sizeof(unsigned int), st));
-        k_color_round<<<grid_for(E, 256), 256, 0, st>>>(E, s.tets.p, s.inc_ptr.p, s.inc_elem.p, color.p, c, remaining);
+        k_color_propose<<<grid_for(E, 256), 256, 0, st>>>(E, s.tets.p, s.inc_ptr.p, s.inc_elem.p, color.p, tent.p,
+                                                          flags.p + 1);
+        k_color_resolve<<<grid_for(E, 256), 256, 0, st>>>(E, s.tets.p, s.inc_ptr.p, s.inc_elem.p, tent.p, win.p);
+        k_color_commit<<<grid_for(E, 256), 256, 0, st>>>(E, tent.p, win.p, color.p, remaining);
         MSFEM_CK(cudaGetLastError());
+        rounds++;
         unsigned int h_rem = 0;
         MSFEM_CK(cudaMemcpyAsync(&h_rem, remaining, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+        MSFEM_CK(cudaMemcpyAsync(h_flags, flags.p, sizeof(h_flags), cudaMemcpyDeviceToHost, st));
         MSFEM_CK(cudaStreamSynchronize(st));
-        n_colors = c + 1;
+        if (h_flags[1]) {
+            set_error("element colouring needs more than %d colours", kMaxColors);
+            return MSFEM_ERR_LIMIT;
+        }
         if (h_rem == 0) break;
+    }
+    int n_colors = 0;
+    {
+        // number of colours = 1 + max colour
+        int32_t* mx = flags.p + 4;
+        MSFEM_CK(cudaMemsetAsync(mx, 0, sizeof(int32_t), st));
+        k_max<<<grid_for(E, 256), 256, 0, st>>>(E, color.p, mx);
+        int32_t h_mx = 0;
+        MSFEM_CK(cudaMemcpyAsync(&h_mx, mx, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        MSFEM_CK(cudaStreamSynchronize(st));
+        n_colors = h_mx + 1;
+        MSFEM_CK(cudaMemsetAsync(mx, 0, sizeof(int32_t), st));
     }
     // elements grouped by colour, ascending element id inside a colour (stable radix sort)
     DBuf<int32_t> ids, keys_out;
@@ -284,8 +359,7 @@ int build_topology(System& s)
     MSFEM_TRY(tmp.alloc(tmp_bytes + 1));
     MSFEM_CK(cub::DeviceRadixSort::SortPairs(tmp.p, tmp_bytes, color.p, keys_out.p, ids.p, s.color_elems.p, E, 0,
                                              end_bit, st));
-    // every colour 0..n_colors-1 is non-empty (each round colours at least the
-    // highest-priority uncoloured element), so the starts are all written
+    // greedy colours are dense: every colour below the maximum is used
     DBuf<int32_t> starts;
     MSFEM_TRY(starts.alloc((size_t)n_colors));
     k_color_starts<<<grid_for(E, 256), 256, 0, st>>>(E, keys_out.p, starts.p);
@@ -301,13 +375,15 @@ int build_topology(System& s)
         return MSFEM_ERR_STATE;
     }
     s.stats.n_colors = n_colors;
-    // incidence count/fill/sort, portrait count/fill, slots, iota, colour starts, one launch per colour round
-    s.total_launches += 8 + n_colors;
+    // incidence count/fill/sort, portrait count/fill, slots, max, iota, colour starts, 3 launches per round
+    s.total_launches += 9 + 3 * rounds;
 
     cnt.release();
     tmp.release();
     flags.release();
     color.release();
+    tent.release();
+    win.release();
     ids.release();
     keys_out.release();
     return MSFEM_OK;

@@ -46,8 +46,18 @@ def assert_system_equal(G, O):
     np.testing.assert_allclose(G.val, O.val, rtol=0, atol=VAL_TOL * scale)
     np.testing.assert_allclose(G.F, O.F, rtol=0, atol=VAL_TOL * max(1.0, np.abs(O.F).max()))
     np.testing.assert_allclose(G.X, O.X, rtol=0, atol=VAL_TOL * max(1.0, np.abs(O.X).max()))
-    # structural zeros (Dirichlet rows / eliminated columns) are exact zeros in both
-    np.testing.assert_array_equal(G.val == 0.0, O.val == 0.0)
+
+
+def assert_dirichlet_structure(G, dofs, columns=True):
+    """Dirichlet rows are exact unit rows; eliminated columns are exact zeros off the diagonal."""
+    bc = np.unique(dofs)
+    for d in bc:
+        a, b = G.row_ptr[d], G.row_ptr[d + 1]
+        np.testing.assert_array_equal(G.val[a:b], (G.col[a:b] == d).astype(float))
+    if columns:
+        hit = np.isin(G.col, bc)
+        rows = np.repeat(np.arange(G.n), np.diff(G.row_ptr))
+        assert np.all(G.val[hit & (rows != G.col)] == 0.0)
 
 
 @pytest.mark.parametrize("n,spheres", [(3, 0), (6, 3), (10, 8)])
@@ -57,7 +67,9 @@ def test_elastic_assembly_and_dirichlet(cuda, port, n, spheres):
         assert_system_equal(S.export_csr(), port.elastic_system(p, stage=0))
         d, v = elastic_dofs(p)
         S.apply_dirichlet(d, v, fem.ROW_AND_COLUMN)
-        assert_system_equal(S.export_csr(), port.elastic_system(p, stage=1))
+        G = S.export_csr()
+        assert_system_equal(G, port.elastic_system(p, stage=1))
+        assert_dirichlet_structure(G, d)  # the elasticity list is sorted: every column is eliminated
 
 
 @pytest.mark.parametrize("n,spheres", [(4, 0), (9, 6), (16, 12)])
