@@ -156,6 +156,21 @@ int msfem_export_csr(msfem_system_t h, int32_t* row_ptr, int32_t* col, double* v
  * (values + column indices + row structure + x + y, each counted once). */
 int msfem_bench_spmv(msfem_system_t h, int precision, int reps, double* ms_per_product, int64_t* bytes_per_product);
 
+/* No counterpart in the reference.  r = f - A x and *rr = ||r||^2 for a caller-owned
+ * CSR matrix (device pointers: row_ptr[n_rows+1], col, val, x, f, r, and rr a single
+ * device double), launched on `stream` (a cudaStream_t, NULL = legacy default stream)
+ * and NOT synchronised.  This entry point allocates no device memory: it is meant for
+ * callers that cannot let a library call cudaMalloc (applications that give the whole
+ * device heap to their own arena, or loops that cannot absorb cudaFree's device-wide
+ * synchronisation).  Its reduction scratch is a fixed 128 KiB device array inside the
+ * library, held by every GPU that loads it until the process exits, which limits
+ * n_rows to 4,194,304 (larger sizes return MSFEM_ERR_LIMIT).  All calls share that
+ * array: calls whose kernels overlap on one GPU race and must be serialised.  The
+ * first call on each device looks the array's address up (cudaGetSymbolAddress) with
+ * that device current; make it before any stream capture on the calling thread. */
+int msfem_residual_noalloc(int n_rows, const int32_t* row_ptr, const int32_t* col, const double* val,
+                           const double* x, const double* f, double* r, double* rr, void* stream);
+
 /* One-call drivers: the reference driver sequence on the GPU, host buffers in and out.
  *
  * FEM::FEM_forBaseEliptic, stiffness-only overload (FEM/FEM.h:398-717):

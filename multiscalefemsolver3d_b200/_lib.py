@@ -14,6 +14,8 @@ LIB_PATH = os.path.join(PKG, "libmsfem_b200.so")
 
 MSFEM_OK = 0
 MSFEM_NOT_CONVERGED = 1
+MSFEM_ERR_ARGUMENT = -1
+MSFEM_ERR_LIMIT = -4
 
 SCALAR, ELASTIC = 0, 1
 CG, PCG_JACOBI, BICGSTAB, GMRES = 0, 1, 2, 3
@@ -66,6 +68,7 @@ _SIGS = [
     ("msfem_spmv", C.c_int, [C.c_void_p, _P, _P, C.c_int]),
     ("msfem_export_csr", C.c_int, [C.c_void_p, _P, _P, _P, C.c_int]),
     ("msfem_bench_spmv", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+    ("msfem_residual_noalloc", C.c_int, [C.c_int, _P, _P, _P, _P, _P, _P, _P, C.c_void_p]),
     ("msfem_fem_scalar_driver", C.c_int, [C.c_int, _P, C.c_int, _P, _P, C.c_int, _P, C.c_int, _P, _P, C.c_int,
                                           C.c_int, C.c_double, C.c_int, _P, C.POINTER(Stats)]),
     ("msfem_fem_elastic_driver", C.c_int, [C.c_int, _P, C.c_int, _P, _P, C.c_int, _P, _P, C.c_int, _P, _P, _P,
