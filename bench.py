@@ -57,22 +57,38 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=100)
-    ap.add_argument("--sample-n", type=int, default=SAMPLE_N)
+    ap.add_argument("--config", default="electrostatics", choices=["electrostatics", "elastic"],
+                    help="electrostatics: 100^3 scalar (the default workload); elastic: 128^3 heterogeneous "
+                         "elasticity, 2000 spheres E 1:100")
+    ap.add_argument("--n", type=int, default=None)
+    ap.add_argument("--sample-n", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.n is None:
+        a.n = 100 if a.config == "electrostatics" else 128
+    if a.sample_n is None:
+        a.sample_n = SAMPLE_N if a.config == "electrostatics" else 10
+    return a
 
 
-def workload(n):
+def workload(n, cfg="electrostatics"):
     from multiscalefemsolver3d_b200 import meshgen
+    if cfg == "elastic":
+        return meshgen.cube_elastic(n=n, jitter=0.0, n_spheres=2000, contrast=100.0, rmin=0.015, rmax=0.035,
+                                    sphere_seed=4096)
     return meshgen.cube_scalar(n=n, n_spheres=200, contrast=100.0, rmin=0.02, rmax=0.06, sphere_seed=2024)
 
 
-def config(n, p=None, extra=None):
-    c = {"workload": f"electrostatics {n}^3 Kuhn tets, 200 spheres eps 1:100, Dirichlet x=0/x=1",
-         "n_dofs": (n + 1) ** 3, "n_tets": 6 * n ** 3, "tol": TOL,
-         "solver": "FP32 Jacobi-PCG inside FP64 iterative refinement",
-         "l2": "flushed between steps (256 MiB write) and inputs > L2", "parallelism": "replicas"}
+def config(n, cfg="electrostatics", extra=None):
+    if cfg == "elastic":
+        c = {"workload": f"elasticity {n}^3 Kuhn tets, 2000 spheres E 1:100 (radii U(0.015,0.035)), nu 0.3, "
+                         f"u=0 at z=0, traction (0,0,-1) at z=1",
+             "n_dofs": 3 * (n + 1) ** 3, "n_tets": 6 * n ** 3}
+    else:
+        c = {"workload": f"electrostatics {n}^3 Kuhn tets, 200 spheres eps 1:100, Dirichlet x=0/x=1",
+             "n_dofs": (n + 1) ** 3, "n_tets": 6 * n ** 3}
+    c.update({"tol": TOL, "solver": "FP32 Jacobi-PCG inside FP64 iterative refinement",
+              "l2": "flushed between steps (256 MiB write) and inputs > L2", "parallelism": "replicas"})
     if extra:
         c.update(extra)
     return c
@@ -176,10 +192,13 @@ class Clocks:
 
 # ---------------------------------------------------------------- reference (CPU) timing
 
-def reference_step(n, threads):
+def reference_step(n, threads, cfg="electrostatics"):
     import oracle
-    p = workload(n)
-    sol, wall = oracle.ref().scalar_driver(p, min_residual=TOL, nthreads=threads)
+    p = workload(n, cfg)
+    if cfg == "elastic":
+        sol, wall = oracle.ref().elastic_driver(p, min_residual=TOL, nthreads=threads)
+    else:
+        sol, wall = oracle.ref().scalar_driver(p, min_residual=TOL, nthreads=threads)
     return wall
 
 
@@ -187,15 +206,16 @@ def extrapolate(t_sample, n_sample, n_full):
     return t_sample * ((n_full + 1) ** 3 / (n_sample + 1) ** 3) ** (4.0 / 3.0)
 
 
-def cpu_baseline(n_full, n_sample, runs=2):
+def cpu_baseline(n_full, n_sample, cfg="electrostatics", runs=2):
     import oracle
     if not oracle.ref_available():
         return None
     threads = os.cpu_count() or 1
-    times = [reference_step(n_sample, threads) for _ in range(runs)]
+    times = [reference_step(n_sample, threads, cfg) for _ in range(runs)]
     t = min(times)
     return {"value": extrapolate(t, n_sample, n_full) * 1e3, "unit": UNIT, "cores": threads, "kind": "reference",
-            "sample": f"reference FEM_forBaseEliptic (SSOR-PCG restart loop) to 1e-8 on the same workload at "
+            "sample": f"reference {'FEM_forElasticDeformation' if cfg == 'elastic' else 'FEM_forBaseEliptic'} "
+                      f"(SSOR-PCG restart loop) to 1e-8 on the same workload at "
                       f"n={n_sample} ({(n_sample + 1) ** 3} DOF), best of {runs}: {t:.2f} s, scaled to n={n_full} "
                       f"by (N ratio)^(4/3)"}
 
@@ -209,14 +229,14 @@ def run_reference(args, D):
         return
     threads = os.cpu_count() or 1
     for _ in range(args.warmup):
-        reference_step(max(10, args.sample_n // 2), threads)
-    ts = [reference_step(args.sample_n, threads) for _ in range(args.steps)]
+        reference_step(max(6, args.sample_n // 2), threads, args.config)
+    ts = [reference_step(args.sample_n, threads, args.config) for _ in range(args.steps)]
     t = statistics.mean(ts)
     v = extrapolate(t, args.sample_n, args.n) * 1e3
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": config(args.n, extra={"solver": "reference SSOR(0.75)-PCG restart loop (FEM/FEM.h:627-695)",
+            "config": config(args.n, args.config, extra={"solver": "reference SSOR(0.75)-PCG restart loop",
                                             "sample_n": args.sample_n, "sample_seconds": ts}),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
                              "sample": f"driver at n={args.sample_n}, mean of {args.steps} runs = {t:.2f} s, "
@@ -252,24 +272,37 @@ def run_ours(args, D):
 
     torch.cuda.set_device(D.local)
     dev = torch.device("cuda", D.local)
-    p = workload(args.n)
+    elastic = args.config == "elastic"
+    p = workload(args.n, args.config)
     m = p.mesh
     xyz = torch.from_numpy(m.xyz).to(dev)
     tets = torch.from_numpy(m.tets).to(dev)
     mat = torch.from_numpy(m.mat).to(dev)
-    bcn = torch.from_numpy(p.bc_nodes).to(dev)
-    bcv = torch.from_numpy(p.bc_values).to(dev)
+    if elastic:
+        dofs = (3 * p.bc_nodes[:, None] + np.arange(3)).ravel().astype(np.int32)
+        bcn = torch.from_numpy(dofs).to(dev)
+        bcv = torch.from_numpy(np.ascontiguousarray(p.bc_values.ravel())).to(dev)
+        faces = torch.from_numpy(p.faces).to(dev)
+        trac = torch.from_numpy(np.ascontiguousarray(p.traction)).to(dev)
+    else:
+        bcn = torch.from_numpy(p.bc_nodes).to(dev)
+        bcv = torch.from_numpy(p.bc_values).to(dev)
     torch.cuda.synchronize()
 
-    S = fem.System(fem.SCALAR, xyz, tets, mat)
+    S = fem.System(fem.ELASTIC if elastic else fem.SCALAR, xyz, tets, mat)
     stream = torch.cuda.ExternalStream(S.stream, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
     def step(method, precision):
         S.clear()
-        S.assemble_scalar(p.sigma)
-        S.apply_dirichlet(bcn, bcv, fem.ROW_AND_COLUMN)
-        S.copy_f_to_x()
+        if elastic:
+            S.add_traction(faces, trac)
+            S.assemble_elastic(p.E, p.nu)
+            S.apply_dirichlet(bcn, bcv, fem.ROW_AND_COLUMN)
+        else:
+            S.assemble_scalar(p.sigma)
+            S.apply_dirichlet(bcn, bcv, fem.ROW_AND_COLUMN)
+            S.copy_f_to_x()
         rel, it, rc = S.solve(method, precision, tol=TOL, maxiter=200000)
         if rc != 0:
             raise RuntimeError(f"solve rc={rc} rel={rel}")
@@ -321,16 +354,28 @@ def run_ours(args, D):
     # e2e: the reference-facing driver with host (pinned) buffers
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
     hx, ht, hm = pin(m.xyz), pin(m.tets), pin(m.mat)
-    hs, hbn, hbv = pin(p.sigma), pin(p.bc_nodes), pin(p.bc_values)
-    sol = torch.empty(m.n_nodes, dtype=torch.float64).pin_memory()
     L = _lib.load()
     P = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    if elastic:
+        hE, hnu, hbn, hbm, hbv = pin(p.E), pin(p.nu), pin(p.bc_nodes), pin(p.bc_mask), pin(p.bc_values)
+        hf, htr = pin(p.faces), pin(p.traction)
+        inputs = (hx, ht, hm, hE, hnu, hbn, hbm, hbv, hf, htr)
+        sol = torch.empty(3 * m.n_nodes, dtype=torch.float64).pin_memory()
+    else:
+        hs, hbn, hbv = pin(p.sigma), pin(p.bc_nodes), pin(p.bc_values)
+        inputs = (hx, ht, hm, hs, hbn, hbv)
+        sol = torch.empty(m.n_nodes, dtype=torch.float64).pin_memory()
 
     def e2e_call():
         st = _lib.Stats()
-        rc = L.msfem_fem_scalar_driver(m.n_nodes, P(hx), m.n_tets, P(ht), P(hm), hs.numel(), P(hs), hbn.numel(),
-                                       P(hbn), P(hbv), fem.PCG_JACOBI, fem.FP32_IR, TOL, 200000, P(sol),
-                                       C.byref(st))
+        if elastic:
+            rc = L.msfem_fem_elastic_driver(m.n_nodes, P(hx), m.n_tets, P(ht), P(hm), hE.numel(), P(hE), P(hnu),
+                                            hbn.numel(), P(hbn), P(hbm), P(hbv), hf.shape[0], P(hf), P(htr),
+                                            fem.PCG_JACOBI, fem.FP32_IR, TOL, 200000, P(sol), C.byref(st))
+        else:
+            rc = L.msfem_fem_scalar_driver(m.n_nodes, P(hx), m.n_tets, P(ht), P(hm), hs.numel(), P(hs),
+                                           hbn.numel(), P(hbn), P(hbv), fem.PCG_JACOBI, fem.FP32_IR, TOL, 200000,
+                                           P(sol), C.byref(st))
         if rc != 0:
             raise RuntimeError(f"driver rc={rc}: {L.msfem_last_error()}")
         return st
@@ -344,12 +389,12 @@ def run_ours(args, D):
         torch.cuda.synchronize()
         e2e_ts.append((time.perf_counter() - t0) * 1e3)
     e2e_ms = D.max(statistics.mean(e2e_ts))
-    h2d = sum(t.numel() * t.element_size() for t in (hx, ht, hm, hs, hbn, hbv))
+    h2d = sum(t.numel() * t.element_size() for t in inputs)
     d2h = sol.numel() * sol.element_size()
 
     base = None
     if D.rank == 0 and D.world == 1 and not args.no_cpu_baseline:
-        base = cpu_baseline(args.n, args.sample_n)
+        base = cpu_baseline(args.n, args.sample_n, args.config)
 
     if D.rank == 0:
         extra = {"iterations_inner": info["iterations"], "refinement_steps": info["outer"],
@@ -364,11 +409,12 @@ def run_ours(args, D):
         line = {"metric": METRIC, "value": ms, "unit": UNIT, "n_gpus": D.world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
                 "vs_baseline": None, "dtype": "fp32-in-f64-ir", "data": "synthetic",
-                "config": config(args.n, p, extra),
+                "config": config(args.n, args.config, extra),
                 "e2e": {"value": e2e_ms, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "gpu_launches": int(launches),
                 "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                             "traffic": traffic, "kernel": "k_spmv<float> (SELL-32, FP32)",
+                             "traffic": traffic if not elastic else None,
+                             "kernel": "k_spmv<float> (SELL-32, FP32" + (", 3x3 blocks)" if elastic else ")"),
                              "peak_source": f"{peak_kind} hbm_gbs"},
                 "cpu_baseline": base,
                 "clocks": clk.summary()}

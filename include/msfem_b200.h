@@ -49,13 +49,18 @@ enum msfem_method {
     MSFEM_CG = 0,          /* plain CG, CSSD_Matrix::MSG (CSSD_Matrix.h:1496-1576)                 */
     MSFEM_PCG_JACOBI = 1,  /* the PCG loop of MSG_PreconditioningSSOR (:1302-1398), M = diag(A)    */
     MSFEM_BICGSTAB = 2,    /* Jacobi-preconditioned BiCGStab (the role of BiCG_Stab/BCG_Stab2)      */
-    MSFEM_GMRES = 3        /* restarted GMRES(m), Jacobi-preconditioned (CSSD_Matrix::GMRES role)  */
+    MSFEM_GMRES = 3,       /* restarted GMRES(m), Jacobi-preconditioned (CSSD_Matrix::GMRES role)  */
+    MSFEM_MINRES = 4       /* MINRES on the Jacobi-scaled matrix: for symmetric indefinite systems,
+                              which the reference's elasticity assembly produces (its transposed
+                              element blocks leave the global matrix symmetric but indefinite) */
 };
 
 enum msfem_precision {
     MSFEM_FP64 = 0,    /* everything in FP64                                                        */
     MSFEM_FP32_IR = 1  /* FP32 matrix + FP32 Krylov inner solves inside FP64 iterative refinement:
-                          r = F - A x and x accumulate in FP64                                      */
+                          r = F - A x and x accumulate in FP64.  The inner solver is CG on the
+                          Jacobi-scaled matrix for MSFEM_PCG_JACOBI, MINRES on it for
+                          MSFEM_MINRES; other methods are FP64 only                               */
 };
 
 enum msfem_dirichlet_mode {
@@ -146,6 +151,11 @@ int msfem_solve(msfem_system_t h, int method, int precision, int restart_m, int 
 /* y = A x in FP64 (CSSD_Matrix::MultiplicationMatrixVector, :395-423) */
 int msfem_spmv(msfem_system_t h, const double* x, double* y, int on_device);
 
+/* y = (D^-1/2 A D^-1/2) x in FP32, D = diag(A): the Jacobi-scaled operator that the FP32
+ * inner solves of MSFEM_FP32_IR apply (no counterpart in the reference; exposed so that the
+ * FP32 path can be checked on its own).  x, y: n_rows floats. */
+int msfem_spmv_scaled32(msfem_system_t h, const float* x, float* y, int on_device);
+
 /* CSR export of the assembled matrix (sizes from msfem_system_info), host or device buffers. */
 int msfem_export_csr(msfem_system_t h, int32_t* row_ptr, int32_t* col, double* val, int on_device);
 
@@ -153,7 +163,8 @@ int msfem_export_csr(msfem_system_t h, int32_t* row_ptr, int32_t* col, double* v
  * FP64 (precision MSFEM_FP64) or FP32 (MSFEM_FP32_IR) SpMV launches with CUDA
  * events on the handle's stream after 3 warm-up launches, and reports the mean
  * device time per product and the algorithmic bytes of one product
- * (values + column indices + row structure + x + y, each counted once). */
+ * (values + column indices in the stored width + row structure + x + y, each
+ * counted once). */
 int msfem_bench_spmv(msfem_system_t h, int precision, int reps, double* ms_per_product, int64_t* bytes_per_product);
 
 /* No counterpart in the reference.  r = f - A x and *rr = ||r||^2 for a caller-owned

@@ -18,7 +18,7 @@ MSFEM_ERR_ARGUMENT = -1
 MSFEM_ERR_LIMIT = -4
 
 SCALAR, ELASTIC = 0, 1
-CG, PCG_JACOBI, BICGSTAB, GMRES = 0, 1, 2, 3
+CG, PCG_JACOBI, BICGSTAB, GMRES, MINRES = 0, 1, 2, 3, 4
 FP64, FP32_IR = 0, 1
 ROW_ONLY, ROW_AND_COLUMN = 0, 1
 
@@ -66,6 +66,7 @@ _SIGS = [
     ("msfem_solve", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                               C.POINTER(C.c_double), C.POINTER(C.c_int)]),
     ("msfem_spmv", C.c_int, [C.c_void_p, _P, _P, C.c_int]),
+    ("msfem_spmv_scaled32", C.c_int, [C.c_void_p, _P, _P, C.c_int]),
     ("msfem_export_csr", C.c_int, [C.c_void_p, _P, _P, _P, C.c_int]),
     ("msfem_bench_spmv", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     ("msfem_residual_noalloc", C.c_int, [C.c_int, _P, _P, _P, _P, _P, _P, _P, C.c_void_p]),

@@ -346,6 +346,22 @@ int msfem_spmv(msfem_system_t h, const double* x, double* y, int on_device)
     return MSFEM_OK;
 }
 
+int msfem_spmv_scaled32(msfem_system_t h, const float* x, float* y, int on_device)
+{
+    (void)on_device;
+    MSFEM_TRY(check_handle(h));
+    System& s = *as_sys(h);
+    MSFEM_TRY(use_device(s));
+    DBuf<float> dx, dy;
+    MSFEM_TRY(dx.alloc((size_t)s.n_rows));
+    MSFEM_TRY(dy.alloc((size_t)s.n_rows));
+    MSFEM_CK(cudaMemcpyAsync(dx.p, x, sizeof(float) * s.n_rows, cudaMemcpyDefault, s.stream));
+    MSFEM_TRY(spmv32(s, dx.p, dy.p));
+    MSFEM_CK(cudaMemcpyAsync(y, dy.p, sizeof(float) * s.n_rows, cudaMemcpyDefault, s.stream));
+    MSFEM_CK(cudaStreamSynchronize(s.stream));
+    return MSFEM_OK;
+}
+
 int msfem_export_csr(msfem_system_t h, int32_t* row_ptr, int32_t* col, double* val, int on_device)
 {
     (void)on_device;
@@ -408,11 +424,13 @@ int msfem_bench_spmv(msfem_system_t h, int precision, int reps, double* ms_per_p
     float ms = 0;
     cudaEventElapsedTime(&ms, s.ev0, s.ev1);
     if (ms_per_product) *ms_per_product = ms / reps;
-    // algorithmic bytes: each stored entry's value and column once, row structure once, x and y once
+    // algorithmic bytes: each nonzero's value and column index once (in the width the format
+    // stores: 2 bytes for 16-bit column deltas, else 4), row structure once, x and y once
     if (bytes_per_product) {
         const int64_t nnz_alg = s.nnzb * s.bs * s.bs;
+        const int64_t cw = (s.sell.col16.p && !fp32) ? 2 : 4;
         if (s.bs == 1)
-            *bytes_per_product = nnz_alg * (int64_t)(w + 4) + (int64_t)(n + 1) * 4 + 2 * (int64_t)n * w;
+            *bytes_per_product = nnz_alg * (int64_t)(w + cw) + (int64_t)(n + 1) * 4 + 2 * (int64_t)n * w;
         else
             *bytes_per_product = s.nnzb * (int64_t)(9 * w + 4) + (int64_t)(s.n_nodes + 1) * 4 + 2 * (int64_t)n * w;
     }

@@ -77,9 +77,10 @@ struct Sell {
     int n_slices = 0;
     int64_t stored = 0;  // stored entries (scalar) or blocks (block3), padding included
     DBuf<int64_t> slice_ptr;
-    DBuf<int32_t> col;
+    DBuf<int32_t> col;    // absolute column (3x3 blocks, or scalar when deltas do not fit 16 bits)
+    DBuf<int16_t> col16;  // scalar: column - min(row, n-1), when every delta fits in 16 bits
     DBuf<double> val64;
-    DBuf<float> val32;
+    DBuf<float> val32;  // Jacobi-scaled copy, D^-1/2 A D^-1/2, for the FP32 inner solves
     bool pattern_ok = false;
     bool values_ok = false;
 };
@@ -89,7 +90,12 @@ struct Sell {
 struct KState {
     double rz, rz_new, rr, ff, pq, alpha, beta, omega, tol2;
     double r0v, tt, ts, rho_old;  // BiCGStab
-    int iter, maxiter, done, breakdown;
+    double mr[16];              // MINRES: Lanczos / Givens scalars
+    double tol2_rel;            // MINRES: tol^2, scaled by the initial residual norm on the device
+    int mr_applied;             // MINRES: iteration whose solution update has been applied after stopping
+    double rr_min;              // smallest (r, r) seen in this solve
+    int stall, stall_limit;     // iterations since rr_min last fell by 2 %; stop when it reaches stall_limit
+    int iter, maxiter, done, breakdown, primed;
     unsigned int ticket[4];
 };
 
@@ -124,12 +130,15 @@ struct System {
     DBuf<double> diag64;  // diagonal of A (FP64)
     DBuf<float> dinv32;   // 1/diag (FP32)
     DBuf<double> dinv64;  // 1/diag (FP64)
+    DBuf<double> dscale;  // 1/sqrt|diag|: the FP32 SELL values hold D^-1/2 A D^-1/2
     DBuf<double> work64;  // Krylov vectors (FP64)
     DBuf<float> work32;   // Krylov vectors (FP32)
     DBuf<double> partial; // reduction partials
     DBuf<KState> kstate;
     KState* h_kstate = nullptr;  // pinned mirror for polling
     DBuf<double> gm;      // GMRES: Hessenberg / rotations / y on the device
+    DBuf<double> mr64;    // MINRES vectors (FP64)
+    DBuf<float> mr32;     // MINRES vectors (FP32)
 
     // reusable scratch: once grown, the per-step calls (assembly, Dirichlet,
     // solve) allocate and free nothing, so they neither block nor serialise
@@ -144,6 +153,7 @@ struct System {
     std::map<std::string, std::array<cudaGraphExec_t, 8>> graphs;
 
     bool zero_diag = false;
+    bool force_col32 = false;  // keep 32-bit SELL columns even when 16-bit deltas fit
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     msfem_stats stats{};
     int launches = 0;          // kernels of the current solve
@@ -167,5 +177,8 @@ int spmv32(System& s, const float* x, float* y);
 int residual64(System& s, const double* x, const double* f, double* r, double* rr_out);
 // ---- Krylov (krylov.cu)
 int solve(System& s, int method, int precision, int restart_m, int maxiter, double tol, double* relres, int* iters);
+// ---- MINRES (minres.cu): on S A S from x = 0 with right-hand side S r (FP64: x += S y) or r (FP32)
+template <class VT, bool SCALE>
+int minres_run(System& s, VT* x, const VT* r, int maxiter, double tol, int stall_unused, int* iters);
 
 }  // namespace msfem

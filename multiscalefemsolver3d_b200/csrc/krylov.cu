@@ -12,6 +12,7 @@
 // CSSD_Matrix::MSG / MSG_PreconditioningSSOR (CSSD_Matrix.h:1336, :1524); the
 // reported residual is recomputed as ||F - A X|| / ||F|| in FP64 at exit.
 #include <cmath>
+#include <cstdlib>
 
 #include "devutil.cuh"
 #include "internal.cuh"
@@ -48,10 +49,14 @@ __global__ void __launch_bounds__(kVecThreads) k_dot_self(int n, const VT* __res
     }
 }
 
+// PCG as in CSSD_Matrix::MSG_PreconditioningSSOR (CSSD_Matrix.h:1336-1362), with M = diag(A)
+// (or M = I): three kernels per iteration -- q = A p with (p, q) -> alpha; the x/r/z update with
+// (r, z), (r, r) -> beta and the stopping test; p = z + beta p.  Without a preconditioner, and for
+// the FP32 solves on the Jacobi-scaled matrix, z is r itself and is never stored.
 // z = M^{-1} r, p = z, (r,z), (r,r); sets rz, rr and the initial stopping test
 template <class VT, bool JAC>
-__global__ void __launch_bounds__(kVecThreads) k_pcg_init(int n, const VT* __restrict__ r, const VT* __restrict__ dinv,
-                                                          VT* __restrict__ z, VT* __restrict__ p, KState* S,
+__global__ void __launch_bounds__(kVecThreads) k_pcg_init(int n, const VT* r, const VT* __restrict__ dinv, VT* z,
+                                                          VT* __restrict__ p, KState* S,
                                                           double* __restrict__ partial)
 {
     __shared__ double sh[64];
@@ -59,7 +64,7 @@ __global__ void __launch_bounds__(kVecThreads) k_pcg_init(int n, const VT* __res
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const VT rv = r[i];
         const VT zv = JAC ? rv * dinv[i] : rv;
-        z[i] = zv;
+        if (JAC) z[i] = zv;  // without a preconditioner z is r itself and is never stored
         p[i] = zv;
         acc[0] += (double)rv * (double)zv;
         acc[1] += (double)rv * (double)rv;
@@ -75,6 +80,8 @@ __global__ void __launch_bounds__(kVecThreads) k_pcg_init(int n, const VT* __res
         if (threadIdx.x == 0) {
             S->rz = t[0];
             S->rr = t[1];
+            S->rr_min = t[1];
+            S->stall = 0;
             S->iter = 0;
             S->breakdown = 0;
             S->done = (t[1] <= S->tol2) ? 1 : 0;
@@ -90,15 +97,16 @@ __global__ void __launch_bounds__(256) k_pcg_spmv(SellView<VT> A, const VT* __re
 {
     if (S->done) return;
     __shared__ double sh[32];
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
     double acc[1] = {0.0};
-    if (warp < A.n_slices) {
+    for (int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; warp < A.n_slices; warp += nw) {
         if (A.bs == 1) {
             const VT v = sell_row_scalar<VT>(A, warp, lane, p);
             const int row = warp * kSlice + lane;
             if (row < A.n_rows) {
                 q[row] = v;
-                acc[0] = (double)p[row] * (double)v;
+                acc[0] += (double)p[row] * (double)v;
             }
         } else {
             VT v[3];
@@ -130,8 +138,8 @@ __global__ void __launch_bounds__(256) k_pcg_spmv(SellView<VT> A, const VT* __re
 
 // x += alpha p, r -= alpha q, z = M^{-1} r, (r,z), (r,r) -> beta, stopping test
 template <class VT, bool JAC>
-__global__ void __launch_bounds__(kVecThreads) k_pcg_update(int n, VT* __restrict__ x, VT* __restrict__ r,
-                                                            VT* __restrict__ z, const VT* __restrict__ p,
+__global__ void __launch_bounds__(kVecThreads) k_pcg_update(int n, VT* __restrict__ x, VT* r, VT* z,
+                                                            const VT* __restrict__ p,
                                                             const VT* __restrict__ q, const VT* __restrict__ dinv,
                                                             KState* S, double* __restrict__ partial)
 {
@@ -144,7 +152,7 @@ __global__ void __launch_bounds__(kVecThreads) k_pcg_update(int n, VT* __restric
         const VT rv = r[i] - alpha * q[i];
         r[i] = rv;
         const VT zv = JAC ? rv * dinv[i] : rv;
-        z[i] = zv;
+        if (JAC) z[i] = zv;
         acc[0] += (double)rv * (double)zv;
         acc[1] += (double)rv * (double)rv;
     }
@@ -161,11 +169,19 @@ __global__ void __launch_bounds__(kVecThreads) k_pcg_update(int n, VT* __restric
             S->rz = t[0];
             S->rr = t[1];
             S->iter += 1;
+            if (t[1] < 0.98 * S->rr_min) {
+                S->rr_min = t[1];
+                S->stall = 0;
+            } else {
+                S->stall += 1;
+            }
             if (t[1] <= S->tol2) S->done = 1;
             else if (S->iter >= S->maxiter) S->done = 2;
             else if (t[1] != t[1]) {
                 S->breakdown = 1;
                 S->done = 3;
+            } else if (S->stall >= S->stall_limit) {
+                S->done = 4;  // stagnated at the precision's attainable accuracy
             }
             S->ticket[0] = 0;
         }
@@ -173,7 +189,7 @@ __global__ void __launch_bounds__(kVecThreads) k_pcg_update(int n, VT* __restric
 }
 
 template <class VT>
-__global__ void __launch_bounds__(kVecThreads) k_pcg_p(int n, const VT* __restrict__ z, VT* __restrict__ p,
+__global__ void __launch_bounds__(kVecThreads) k_pcg_p(int n, const VT* z, VT* __restrict__ p,
                                                        const KState* S)
 {
     if (S->done) return;
@@ -191,22 +207,25 @@ __global__ void __launch_bounds__(kVecThreads) k_copy(int n, const VT* __restric
 }
 
 // FP32-IR helpers
+// r32 = D^-1/2 r / ||r||  (the scaled system's right-hand side), d32 = 0
 __global__ void __launch_bounds__(kVecThreads) k_scale_to32(int n, const double* __restrict__ r, const double* rr,
-                                                            float* __restrict__ r32, float* __restrict__ d32)
+                                                            const double* __restrict__ dscale, float* __restrict__ r32,
+                                                            float* __restrict__ d32)
 {
     const double s = 1.0 / sqrt(*rr);
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        r32[i] = (float)(r[i] * s);
+        r32[i] = (float)(r[i] * dscale[i] * s);
         d32[i] = 0.0f;
     }
 }
 
+// x += ||r|| D^-1/2 d32  (back from the scaled unknowns)
 __global__ void __launch_bounds__(kVecThreads) k_correct(int n, double* __restrict__ x, const float* __restrict__ d32,
-                                                         const double* rr)
+                                                         const double* __restrict__ dscale, const double* rr)
 {
     const double s = sqrt(*rr);
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        x[i] += s * (double)d32[i];
+        x[i] += s * dscale[i] * (double)d32[i];
 }
 
 // ------------------------------------------------------------------ BiCGStab kernels
@@ -449,16 +468,22 @@ int read_state(System& s)
     return MSFEM_OK;
 }
 
-// sets S->ff, S->tol2 (= tol^2 * ff), S->maxiter on the device
-__global__ void k_set_limits(KState* S, double tol, int maxiter, int use_rr_as_ff)
+// sets S->ff, S->tol2 (= tol^2 * ff), S->maxiter and the stagnation window on the device
+__global__ void k_set_limits(KState* S, double tol, int maxiter, int use_rr_as_ff, int stall_limit)
 {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         if (use_rr_as_ff) S->ff = S->rr;
         S->tol2 = tol * tol * S->ff;
         S->maxiter = maxiter;
+        S->stall_limit = stall_limit;
         S->done = 0;
     }
 }
+
+// FP32 inner solves stop when (r, r) has not set a new 2 % low for this many iterations: FP32
+// CG cannot go below about cond * eps32, and iterating on past that point only adds noise
+constexpr int kInnerStall = 200;
+constexpr int kNoStall = 0x7fffffff;
 
 // Runs a captured chunk of `per_iter` launches per iteration until the state says done.
 template <class F>
@@ -524,10 +549,11 @@ std::string graph_key(const char* tag, std::initializer_list<const void*> ptrs, 
 
 template <class VT>
 struct PcgVectors {
-    VT *x, *r, *z, *p, *q;
+    VT *x, *r, *z, *p, *q;  // z == r without a preconditioner
     const VT* dinv;
 };
 
+// r holds the initial residual on entry; x is updated in place
 template <class VT, bool JAC>
 int pcg_run(System& s, PcgVectors<VT> v, int maxiter)
 {
@@ -538,7 +564,7 @@ int pcg_run(System& s, PcgVectors<VT> v, int maxiter)
     MSFEM_CK(cudaGetLastError());
     s.launches += 1;
     const SellView<VT> A = sell_view<VT>(s);
-    const unsigned g = spmv_grid(s);
+    const unsigned g = spmv_grid_of((const void*)k_pcg_spmv<VT>, s);
     auto iteration = [&]() {
         k_pcg_spmv<VT><<<g, 256, 0, s.stream>>>(A, v.p, v.q, S, part);
         k_pcg_update<VT, JAC><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, v.x, v.r, v.z, v.p, v.q, v.dinv, S, part);
@@ -572,28 +598,37 @@ int solve_pcg64(System& s, bool jacobi, int maxiter, double tol, int* iters)
     // ff = (F, F); r = F - A X
     k_dot_self<double><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, s.F.p, s.partial.p, &S->ticket[1], &S->ff);
     MSFEM_TRY(residual64(s, s.X.p, s.F.p, r, &S->rr));
-    k_set_limits<<<1, 32, 0, s.stream>>>(S, tol, maxiter, 0);
+    k_set_limits<<<1, 32, 0, s.stream>>>(S, tol, maxiter, 0, kNoStall);
     s.launches += 3;
-    PcgVectors<double> v{s.X.p, r, z, p, q, s.dinv64.p};
+    PcgVectors<double> v{s.X.p, r, jacobi ? z : r, p, q, s.dinv64.p};  // no preconditioner: z is r
     MSFEM_TRY((jacobi ? pcg_run<double, true>(s, v, maxiter) : pcg_run<double, false>(s, v, maxiter)));
     MSFEM_TRY(read_state(s));
     *iters = s.h_kstate->iter;
     return s.h_kstate->done == 1 ? MSFEM_OK : MSFEM_NOT_CONVERGED;
 }
 
-// FP32 matrix and Krylov vectors inside FP64 iterative refinement:
-//   r = F - A x (FP64);  solve A d = r / ||r|| in FP32 to a relative tolerance;  x += ||r|| d (FP64)
-int solve_ir32(System& s, bool jacobi, int maxiter, double tol, int* iters, int* outer)
+enum Inner { INNER_CG32 = 0, INNER_MINRES32 = 1, INNER_MINRES64 = 2 };
+
+// Iterative refinement around an inner Krylov solve:
+//   r = F - A x in FP64;  inner solve of the Jacobi-scaled system (S A S) y = S r to a relative
+//   tolerance;  x += S y in FP64.
+// INNER_CG32 / INNER_MINRES32: the inner solve runs in FP32 on the FP32 copy of S A S (the right-
+// hand side S r / ||r|| is rounded to FP32 and the correction scaled back by ||r||); CG for SPD
+// matrices, MINRES for symmetric indefinite ones.  INNER_MINRES64: FP64 MINRES, whose stopping test
+// is on the scaled residual, refined until the true ||F - A x|| / ||F|| meets tol.
+int solve_refined(System& s, Inner inner, int maxiter, double tol, int* iters, int* outer)
 {
     const int n = s.n_rows;
     MSFEM_TRY(s.work64.alloc(4 * (size_t)n));
-    MSFEM_TRY(s.work32.alloc(6 * (size_t)n));
     double* r64 = s.work64.p;
-    float* d32 = s.work32.p;
-    float* r32 = d32 + n;
-    float* z32 = r32 + n;
-    float* p32 = z32 + n;
-    float* q32 = p32 + n;
+    float *d32 = nullptr, *r32 = nullptr, *p32 = nullptr, *q32 = nullptr;
+    if (inner != INNER_MINRES64) {
+        MSFEM_TRY(s.work32.alloc(4 * (size_t)n));
+        d32 = s.work32.p;
+        r32 = d32 + n;
+        p32 = r32 + n;
+        q32 = p32 + n;
+    }
     KState* S = s.kstate.p;
     DBuf<double>& rr_dev = s.sc_f64[1];
     MSFEM_TRY(rr_dev.alloc(2));
@@ -612,7 +647,7 @@ int solve_ir32(System& s, bool jacobi, int maxiter, double tol, int* iters, int*
         MSFEM_CK(cudaMemcpyAsync(&rr, rr_dev.p, sizeof(double), cudaMemcpyDeviceToHost, s.stream));
         MSFEM_CK(cudaStreamSynchronize(s.stream));
         if (!(rr == rr)) {
-            set_error("FP32-IR: residual became NaN");
+            set_error("refinement: the residual became NaN");
             return MSFEM_ERR_NUMERIC;
         }
         if (rr <= tol * tol * ff || rr == 0.0) break;
@@ -621,23 +656,49 @@ int solve_ir32(System& s, bool jacobi, int maxiter, double tol, int* iters, int*
             if (++stalls >= 3) break;  // refinement no longer contracts
         }
         prev_rr = rr;
-        // inner tolerance: 1e-4, or just what is still missing (with margin) near the end
-        double need = tol * std::sqrt(ff / rr);
-        double tau = std::max(1e-4, std::min(0.5, 0.3 * need));
-        k_scale_to32<<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, r64, rr_dev.p, r32, d32);
-        // inner solve on (r32, r32) ~ 1: the state's ff is the inner right-hand side norm
-        k_dot_self<float><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, r32, s.partial.p, &S->ticket[1], &S->rr);
-        k_set_limits<<<1, 32, 0, s.stream>>>(S, tau, maxiter - total_inner, 1);
-        s.launches += 3;
-        PcgVectors<float> v{d32, r32, z32, p32, q32, s.dinv32.p};
-        MSFEM_TRY((jacobi ? pcg_run<float, true>(s, v, maxiter - total_inner)
-                         : pcg_run<float, false>(s, v, maxiter - total_inner)));
-        MSFEM_TRY(read_state(s));
-        total_inner += s.h_kstate->iter;
-        k_correct<<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, s.X.p, d32, rr_dev.p);
-        s.launches += 1;
+        const double need = tol * std::sqrt(ff / rr);  // the reduction still missing
+        int it = 0, rc = MSFEM_OK;
+        double tau;
+        if (inner == INNER_MINRES64) {
+            tau = std::max(1e-14, std::min(0.5, 0.5 * need));
+            rc = minres_run<double, true>(s, s.X.p, r64, maxiter - total_inner, tau, 0, &it);
+            s.launches += 0;
+        } else {
+            // inner tolerance: 1e-4 (what FP32 reaches comfortably), or just what is still missing
+            tau = std::max(1e-4, std::min(0.5, 0.3 * need));
+            k_scale_to32<<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, r64, rr_dev.p, s.dscale.p, r32, d32);
+            s.launches += 1;
+            if (inner == INNER_CG32) {
+                k_dot_self<float><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, r32, s.partial.p, &S->ticket[1], &S->rr);
+                k_set_limits<<<1, 32, 0, s.stream>>>(S, tau, maxiter - total_inner, 1, kInnerStall);
+                s.launches += 2;
+                PcgVectors<float> v{d32, r32, r32, p32, q32, nullptr};  // unit diagonal: z = r
+                MSFEM_TRY((pcg_run<float, false>(s, v, maxiter - total_inner)));
+                MSFEM_TRY(read_state(s));
+                it = s.h_kstate->iter;
+                if (s.h_kstate->breakdown) rc = MSFEM_ERR_NUMERIC;
+            } else {
+                rc = minres_run<float, false>(s, d32, r32, maxiter - total_inner, tau, 0, &it);
+            }
+        }
+        total_inner += it;
+        if (std::getenv("MSFEM_TRACE")) {
+            read_state(s);
+            std::fprintf(stderr, "[msfem] refine %d (inner %d): rel %.3e tau %.1e inner iters %d rc %d (done %d rr %.3e)\n",
+                         k, (int)inner, std::sqrt(rr / ff), tau, it, rc, s.h_kstate->done, s.h_kstate->rr);
+        }
+        if (rc == MSFEM_ERR_NUMERIC) {
+            // the inner solve broke down: keep x as it is and stop
+            set_error("refinement: inner solve broke down after %d iterations", it);
+            break;
+        }
+        if (rc < 0) return rc;
+        if (inner != INNER_MINRES64) {
+            k_correct<<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, s.X.p, d32, s.dscale.p, rr_dev.p);
+            s.launches += 1;
+        }
     }
-    // restore ff for the final residual report
+    // the final residual report uses (F, F)
     k_dot_self<double><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, s.F.p, s.partial.p, &S->ticket[1], &S->ff);
     s.launches += 1;
     *iters = total_inner;
@@ -661,7 +722,7 @@ int solve_bicgstab64(System& s, int maxiter, double tol, int* iters)
     double* part = s.partial.p;
     k_dot_self<double><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, s.F.p, part, &S->ticket[1], &S->ff);
     MSFEM_TRY(residual64(s, s.X.p, s.F.p, r, &S->rr));
-    k_set_limits<<<1, 32, 0, s.stream>>>(S, tol, maxiter, 0);
+    k_set_limits<<<1, 32, 0, s.stream>>>(S, tol, maxiter, 0, kNoStall);
     k_bcg_init<double><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, r, rhat, p, v, S, part);
     MSFEM_CK(cudaGetLastError());
     s.launches += 4;
@@ -707,9 +768,22 @@ int solve(System& s, int method, int precision, int restart_m, int maxiter, doub
     switch (method) {
     case MSFEM_CG:
     case MSFEM_PCG_JACOBI:
-        if (precision == MSFEM_FP64) rc = solve_pcg64(s, jac, maxiter, tol, &it);
-        else if (precision == MSFEM_FP32_IR) rc = solve_ir32(s, jac, maxiter, tol, &it, &outer);
-        else rc = MSFEM_ERR_ARGUMENT;
+        if (precision == MSFEM_FP64) {
+            rc = solve_pcg64(s, jac, maxiter, tol, &it);
+        } else if (precision == MSFEM_FP32_IR && jac) {
+            rc = solve_refined(s, INNER_CG32, maxiter, tol, &it, &outer);
+        } else {
+            set_error("solve: FP32 iterative refinement uses a Jacobi-preconditioned inner solver; "
+                      "use MSFEM_PCG_JACOBI or MSFEM_MINRES (precision %d)", precision);
+            return MSFEM_ERR_ARGUMENT;
+        }
+        break;
+    case MSFEM_MINRES:
+        if (s.zero_diag) {
+            set_error("solve: MINRES runs on the Jacobi-scaled matrix; a zero diagonal entry makes it undefined");
+            return MSFEM_ERR_NUMERIC;
+        }
+        rc = solve_refined(s, precision == MSFEM_FP32_IR ? INNER_MINRES32 : INNER_MINRES64, maxiter, tol, &it, &outer);
         break;
     case MSFEM_BICGSTAB:
         rc = solve_bicgstab64(s, maxiter, tol, &it);
@@ -733,7 +807,8 @@ int solve(System& s, int method, int precision, int restart_m, int maxiter, doub
     s.total_launches += s.launches;
     if (relres) *relres = rel;
     if (iters) *iters = it;
-    if (precision == MSFEM_FP32_IR && rc == MSFEM_OK && !(rel <= tol * (1.0 + 1e-6))) rc = MSFEM_NOT_CONVERGED;
+    if ((precision == MSFEM_FP32_IR || method == MSFEM_MINRES) && rc == MSFEM_OK && !(rel <= tol * (1.0 + 1e-6)))
+        rc = MSFEM_NOT_CONVERGED;
     return rc;
 }
 

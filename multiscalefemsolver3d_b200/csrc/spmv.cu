@@ -56,7 +56,28 @@ __global__ void k_sell_pattern_scalar(int n_rows, const int32_t* __restrict__ rp
     }
 }
 
-__global__ void k_sell_values_scalar(int n_rows, const int32_t* __restrict__ rp, const double* __restrict__ val,
+// 16-bit deltas of the scalar SELL columns from min(row, n-1); flags overflow
+__global__ void k_sell_delta16(int n_rows, int n_slices, const int64_t* __restrict__ sp, const int32_t* __restrict__ col,
+                               int16_t* __restrict__ col16, int* overflow)
+{
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    const int slice = row / kSlice, lane = row % kSlice;
+    if (slice >= n_slices) return;
+    const int64_t base = sp[slice];
+    const int w = (int)((sp[slice + 1] - base) / kSlice);
+    const int row0 = min(row, n_rows - 1);
+    for (int k = 0; k < w; k++) {
+        const int64_t pos = base + (int64_t)(k / kChunk) * (kSlice * kChunk) + lane * kChunk + (k % kChunk);
+        const int c = row < n_rows ? col[pos] : row0;
+        const int d = c - row0;
+        if (d < -32768 || d > 32767) atomicExch(overflow, 1);
+        col16[pos] = (int16_t)d;
+    }
+}
+
+// v64 = A; v32 = D^-1/2 A D^-1/2 (the Jacobi-scaled matrix the FP32 inner solves use), scale = 1/sqrt|a_ii|
+__global__ void k_sell_values_scalar(int n_rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ncol,
+                                     const double* __restrict__ val, const double* __restrict__ scale,
                                      const int64_t* __restrict__ sp, double* __restrict__ v64, float* __restrict__ v32)
 {
     const int row = blockIdx.x * blockDim.x + threadIdx.x;
@@ -65,11 +86,12 @@ __global__ void k_sell_values_scalar(int n_rows, const int32_t* __restrict__ rp,
     const int64_t base = sp[slice];
     const int w = (int)((sp[slice + 1] - base) / kSlice);
     const int b = row < n_rows ? rp[row] : 0, len = row < n_rows ? rp[row + 1] - b : 0;
+    const double si = row < n_rows ? scale[row] : 0.0;
     for (int k = 0; k < w; k++) {
         const int64_t pos = base + (int64_t)(k / kChunk) * (kSlice * kChunk) + lane * kChunk + (k % kChunk);
         const double v = k < len ? val[b + k] : 0.0;
         v64[pos] = v;
-        v32[pos] = (float)v;
+        v32[pos] = k < len ? (float)(v * si * scale[ncol[b + k]]) : 0.0f;
     }
 }
 
@@ -86,7 +108,8 @@ __global__ void k_sell_pattern_block(int n_brows, const int32_t* __restrict__ rp
     for (int k = 0; k < w; k++) col[base + (int64_t)k * kSlice + lane] = k < len ? ncol[b + k] : pad;
 }
 
-__global__ void k_sell_values_block(int n_brows, const int32_t* __restrict__ rp, const double* __restrict__ val,
+__global__ void k_sell_values_block(int n_brows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ncol,
+                                    const double* __restrict__ val, const double* __restrict__ scale,
                                     const int64_t* __restrict__ sp, double* __restrict__ v64, float* __restrict__ v32)
 {
     const int row = blockIdx.x * blockDim.x + threadIdx.x;
@@ -97,10 +120,12 @@ __global__ void k_sell_values_block(int n_brows, const int32_t* __restrict__ rp,
     const int b = row < n_brows ? rp[row] : 0, len = row < n_brows ? rp[row + 1] - b : 0;
     for (int k = 0; k < w; k++) {
         const int64_t blk = 9 * (base + (int64_t)k * kSlice) + lane;
+        const int j = k < len ? ncol[b + k] : 0;
         for (int e = 0; e < 9; e++) {
             const double v = k < len ? val[9 * (int64_t)(b + k) + e] : 0.0;
             v64[blk + (int64_t)e * kSlice] = v;
-            v32[blk + (int64_t)e * kSlice] = (float)v;
+            v32[blk + (int64_t)e * kSlice] =
+                k < len ? (float)(v * scale[3 * (int64_t)row + e / 3] * scale[3 * (int64_t)j + e % 3]) : 0.0f;
         }
     }
 }
@@ -108,7 +133,7 @@ __global__ void k_sell_values_block(int n_brows, const int32_t* __restrict__ rp,
 // diagonal of the scalar rows and its inverses
 __global__ void k_diag(int n_rows, int bs, const int32_t* __restrict__ rp, const int32_t* __restrict__ ncol,
                        const double* __restrict__ val, double* __restrict__ d64, double* __restrict__ di64,
-                       float* __restrict__ di32, int* bad)
+                       float* __restrict__ di32, double* __restrict__ scale, int* bad)
 {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n_rows) return;
@@ -121,29 +146,33 @@ __global__ void k_diag(int n_rows, int bs, const int32_t* __restrict__ rp, const
         atomicExch(bad, 1);
         di64[r] = 0.0;
         di32[r] = 0.0f;
+        scale[r] = 1.0;
     } else {
         di64[r] = 1.0 / d;
         di32[r] = (float)(1.0 / d);
+        scale[r] = 1.0 / sqrt(fabs(d));
     }
 }
 
 template <class VT>
 __global__ void __launch_bounds__(256) k_spmv(SellView<VT> A, const VT* __restrict__ x, VT* __restrict__ y)
 {
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (warp >= A.n_slices) return;
-    if (A.bs == 1) {
-        const VT acc = sell_row_scalar<VT>(A, warp, lane, x);
-        const int row = warp * kSlice + lane;
-        if (row < A.n_rows) y[row] = acc;
-    } else {
-        VT acc[3];
-        sell_row_block<VT>(A, warp, lane, x, acc);
-        const int brow = warp * kSlice + lane;
-        if (brow < A.n_brows) {
-            y[3 * (int64_t)brow] = acc[0];
-            y[3 * (int64_t)brow + 1] = acc[1];
-            y[3 * (int64_t)brow + 2] = acc[2];
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; warp < A.n_slices; warp += nw) {
+        if (A.bs == 1) {
+            const VT acc = sell_row_scalar<VT>(A, warp, lane, x);
+            const int row = warp * kSlice + lane;
+            if (row < A.n_rows) y[row] = acc;
+        } else {
+            VT acc[3];
+            sell_row_block<VT>(A, warp, lane, x, acc);
+            const int brow = warp * kSlice + lane;
+            if (brow < A.n_brows) {
+                y[3 * (int64_t)brow] = acc[0];
+                y[3 * (int64_t)brow + 1] = acc[1];
+                y[3 * (int64_t)brow + 2] = acc[2];
+            }
         }
     }
 }
@@ -155,16 +184,17 @@ __global__ void __launch_bounds__(256) k_residual(SellView<double> A, const doub
                                                   double* __restrict__ out)
 {
     __shared__ double sh[32];
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
     double rr[1] = {0.0};
-    if (warp < A.n_slices) {
+    for (int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; warp < A.n_slices; warp += nw) {
         if (A.bs == 1) {
             const double acc = sell_row_scalar<double>(A, warp, lane, x);
             const int row = warp * kSlice + lane;
             if (row < A.n_rows) {
                 const double v = f[row] - acc;
                 r[row] = v;
-                rr[0] = v * v;
+                rr[0] += v * v;
             }
         } else {
             double acc[3];
@@ -227,33 +257,50 @@ int prepare_sell(System& s)
             k_sell_pattern_block<<<grid_for(nthreads, 128), 128, 0, st>>>(nbr, s.nrp.p, s.ncol.p, S.slice_ptr.p,
                                                                           S.col.p);
         MSFEM_CK(cudaGetLastError());
+        S.col16.release();
+        if (s.bs == 1) {
+            // scalar columns as 16-bit deltas when they fit (a Kuhn grid up to ~180^3 in natural
+            // numbering): 6 instead of 8 bytes per FP32 nonzero, 10 instead of 12 per FP64 one
+            DBuf<int> ovf;
+            MSFEM_TRY(ovf.alloc(1));
+            MSFEM_TRY(S.col16.alloc((size_t)stored));
+            MSFEM_CK(cudaMemsetAsync(ovf.p, 0, sizeof(int), st));
+            k_sell_delta16<<<grid_for(nthreads, 128), 128, 0, st>>>(nbr, S.n_slices, S.slice_ptr.p, S.col.p,
+                                                                    S.col16.p, ovf.p);
+            int h_ovf = 0;
+            MSFEM_CK(cudaMemcpyAsync(&h_ovf, ovf.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+            MSFEM_CK(cudaStreamSynchronize(st));
+            if (h_ovf || s.force_col32) S.col16.release();
+            s.total_launches += 1;
+        }
         S.pattern_ok = true;
         S.values_ok = false;
         s.total_launches += 2;
     }
     if (!S.values_ok) {
         const int64_t nthreads = (int64_t)S.n_slices * kSlice;
-        if (s.bs == 1)
-            k_sell_values_scalar<<<grid_for(nthreads, 128), 128, 0, st>>>(nbr, s.nrp.p, s.val.p, S.slice_ptr.p,
-                                                                          S.val64.p, S.val32.p);
-        else
-            k_sell_values_block<<<grid_for(nthreads, 128), 128, 0, st>>>(nbr, s.nrp.p, s.val.p, S.slice_ptr.p,
-                                                                         S.val64.p, S.val32.p);
         MSFEM_TRY(s.diag64.alloc(s.n_rows));
         MSFEM_TRY(s.dinv64.alloc(s.n_rows));
         MSFEM_TRY(s.dinv32.alloc(s.n_rows));
-        DBuf<int> bad;
-        MSFEM_TRY(bad.alloc(1));
+        MSFEM_TRY(s.dscale.alloc(s.n_rows));
+        DBuf<int>& bad = s.flag;
+        MSFEM_TRY(bad.alloc(8));
         MSFEM_CK(cudaMemsetAsync(bad.p, 0, sizeof(int), st));
         k_diag<<<grid_for(s.n_rows, 256), 256, 0, st>>>(s.n_rows, s.bs, s.nrp.p, s.ncol.p, s.val.p, s.diag64.p,
-                                                        s.dinv64.p, s.dinv32.p, bad.p);
+                                                        s.dinv64.p, s.dinv32.p, s.dscale.p, bad.p);
+        if (s.bs == 1)
+            k_sell_values_scalar<<<grid_for(nthreads, 128), 128, 0, st>>>(nbr, s.nrp.p, s.ncol.p, s.val.p, s.dscale.p,
+                                                                          S.slice_ptr.p, S.val64.p, S.val32.p);
+        else
+            k_sell_values_block<<<grid_for(nthreads, 128), 128, 0, st>>>(nbr, s.nrp.p, s.ncol.p, s.val.p, s.dscale.p,
+                                                                         S.slice_ptr.p, S.val64.p, S.val32.p);
         MSFEM_CK(cudaGetLastError());
         int h_bad = 0;
         MSFEM_CK(cudaMemcpyAsync(&h_bad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
         MSFEM_CK(cudaStreamSynchronize(st));
         s.sell.values_ok = true;
-        s.zero_diag = h_bad != 0;
-        s.total_launches += 2;  // only the Jacobi-preconditioned methods care; they check it
+        s.zero_diag = h_bad != 0;  // only the Jacobi-preconditioned methods care; they check it
+        s.total_launches += 2;
     }
     return MSFEM_OK;
 }
@@ -268,6 +315,9 @@ SellView<VT> sell_view(System& s)
     v.n_brows = s.n_nodes;
     v.sp = s.sell.slice_ptr.p;
     v.col = s.sell.col.p;
+    // 16-bit deltas pay off where the product is bandwidth-bound (FP64); the FP32 product is
+    // bound by gather latency and runs faster on the plain 32-bit columns
+    v.col16 = sizeof(VT) == 8 ? s.sell.col16.p : nullptr;
     if constexpr (sizeof(VT) == 8) v.val = reinterpret_cast<const VT*>(s.sell.val64.p);
     else v.val = reinterpret_cast<const VT*>(s.sell.val32.p);
     return v;
@@ -275,12 +325,26 @@ SellView<VT> sell_view(System& s)
 template SellView<double> sell_view<double>(System&);
 template SellView<float> sell_view<float>(System&);
 
+// Blocks for a slice-strided SpMV-type kernel: every SM filled exactly once (SMs x resident
+// blocks of 256 threads), so no partial last wave idles the GPU; never more than one warp per slice.
+unsigned spmv_grid_of(const void* kernel, const System& s)
+{
+    static int sms = 0;
+    if (!sms) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s.device);
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0) != cudaSuccess || per_sm <= 0)
+        per_sm = 4;
+    const unsigned full = grid_for((int64_t)s.sell.n_slices * 32, 256);
+    const unsigned fill = (unsigned)(sms * per_sm);
+    return full < fill ? full : fill;
+}
+
 unsigned spmv_grid(const System& s) { return grid_for((int64_t)s.sell.n_slices * 32, 256); }
 
 int spmv64(System& s, const double* x, double* y)
 {
     MSFEM_TRY(prepare_sell(s));
-    k_spmv<double><<<spmv_grid(s), 256, 0, s.stream>>>(sell_view<double>(s), x, y);
+    k_spmv<double><<<spmv_grid_of((const void*)k_spmv<double>, s), 256, 0, s.stream>>>(sell_view<double>(s), x, y);
     MSFEM_CK(cudaGetLastError());
     s.total_launches += 1;
     return MSFEM_OK;
@@ -289,7 +353,7 @@ int spmv64(System& s, const double* x, double* y)
 int spmv32(System& s, const float* x, float* y)
 {
     MSFEM_TRY(prepare_sell(s));
-    k_spmv<float><<<spmv_grid(s), 256, 0, s.stream>>>(sell_view<float>(s), x, y);
+    k_spmv<float><<<spmv_grid_of((const void*)k_spmv<float>, s), 256, 0, s.stream>>>(sell_view<float>(s), x, y);
     MSFEM_CK(cudaGetLastError());
     s.total_launches += 1;
     return MSFEM_OK;
@@ -299,8 +363,8 @@ int spmv32(System& s, const float* x, float* y)
 int residual64(System& s, const double* x, const double* f, double* r, double* rr_out)
 {
     MSFEM_TRY(prepare_sell(s));
-    const unsigned g = spmv_grid(s);
-    MSFEM_TRY(s.partial.alloc(std::max<size_t>(3 * (size_t)g, 3 * (size_t)kReduceBlocks) + 64));
+    const unsigned g = spmv_grid_of((const void*)k_residual, s);
+    MSFEM_TRY(s.partial.alloc(std::max<size_t>(3 * (size_t)spmv_grid(s), 3 * (size_t)kReduceBlocks) + 64));
     MSFEM_TRY(s.kstate.alloc(1));
     k_residual<<<g, 256, 0, s.stream>>>(sell_view<double>(s), x, f, r, s.partial.p, &s.kstate.p->ticket[3], rr_out);
     MSFEM_CK(cudaGetLastError());

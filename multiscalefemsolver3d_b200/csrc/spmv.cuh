@@ -11,12 +11,14 @@ struct SellView {
     int n_slices, bs, n_rows, n_brows;
     const int64_t* sp;
     const int32_t* col;
+    const int16_t* col16;  // non-null: scalar columns stored as 16-bit deltas from min(row, n_rows-1)
     const VT* val;
 };
 
 template <class VT>
 SellView<VT> sell_view(System& s);
-unsigned spmv_grid(const System& s);
+unsigned spmv_grid(const System& s);                          // one warp per slice
+unsigned spmv_grid_of(const void* kernel, const System& s);   // slice-strided, one full wave
 
 template <class VT>
 struct Vec4;
@@ -46,16 +48,93 @@ struct Vec4<double> {
 
 // Row `warp*32 + lane` of a scalar SELL slice times x.  All lanes of the warp
 // must call it (the loop runs to the slice width).
+// 4 consecutive 16-bit column deltas of one lane (one 8-byte load)
+__device__ __forceinline__ void load_delta4(const int16_t* p, int row0, int (&c)[4])
+{
+    const int2 q = __ldcs(reinterpret_cast<const int2*>(p));
+    c[0] = row0 + (int)(short)(q.x & 0xffff);
+    c[1] = row0 + (int)(short)((unsigned)q.x >> 16);
+    c[2] = row0 + (int)(short)(q.y & 0xffff);
+    c[3] = row0 + (int)(short)((unsigned)q.y >> 16);
+}
+
+template <class VT>
+__device__ __forceinline__ VT sell_row_scalar16(const SellView<VT>& A, int warp, int lane, const VT* __restrict__ x)
+{
+    const int64_t base = A.sp[warp];
+    const int w = (int)((A.sp[warp + 1] - base) >> 5);
+    const int row0 = min(warp * kSlice + lane, A.n_rows - 1);
+    const int16_t* cp = A.col16 + base + lane * kChunk;
+    const VT* vp = A.val + base + lane * kChunk;
+    VT acc = 0;
+    int k = 0;
+    for (; k + 4 * kChunk <= w; k += 4 * kChunk) {
+        int c[4][4];
+        VT v[4][4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            load_delta4(cp + (int64_t)(k + q * kChunk) * kSlice, row0, c[q]);
+            Vec4<VT>::load(vp + (int64_t)(k + q * kChunk) * kSlice, v[q]);
+        }
+        VT xs[4][4];
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) xs[q][e] = __ldg(x + c[q][e]);
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) acc += v[q][e] * xs[q][e];
+    }
+    for (; k < w; k += kChunk) {
+        int c[4];
+        VT v[4];
+        load_delta4(cp + (int64_t)k * kSlice, row0, c);
+        Vec4<VT>::load(vp + (int64_t)k * kSlice, v);
+#pragma unroll
+        for (int e = 0; e < 4; e++) acc += v[e] * __ldg(x + c[e]);
+    }
+    return acc;
+}
+
 template <class VT>
 __device__ __forceinline__ VT sell_row_scalar(const SellView<VT>& A, int warp, int lane, const VT* __restrict__ x)
 {
+    if (A.col16) return sell_row_scalar16<VT>(A, warp, lane, x);
     const int64_t base = A.sp[warp];
     const int w = (int)((A.sp[warp + 1] - base) >> 5);
     const int32_t* cp = A.col + base + lane * kChunk;
     const VT* vp = A.val + base + lane * kChunk;
     VT acc = 0;
+    int k = 0;
+    if constexpr (sizeof(VT) == 4) {
+        // FP32: issue the column and value loads of 4 chunks (16 entries, a whole
+        // interior Kuhn row) before the dependent x gathers, so that each warp
+        // keeps 16 independent 128-bit loads in flight instead of 2
+        for (; k + 4 * kChunk <= w; k += 4 * kChunk) {
+            int4 c[4];
+            VT v[4][4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                c[q] = __ldcs(reinterpret_cast<const int4*>(cp + (int64_t)(k + q * kChunk) * kSlice));
+                Vec4<VT>::load(vp + (int64_t)(k + q * kChunk) * kSlice, v[q]);
+            }
+            VT xs[4][4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                xs[q][0] = __ldg(x + c[q].x);
+                xs[q][1] = __ldg(x + c[q].y);
+                xs[q][2] = __ldg(x + c[q].z);
+                xs[q][3] = __ldg(x + c[q].w);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+#pragma unroll
+                for (int e = 0; e < 4; e++) acc += v[q][e] * xs[q][e];
+        }
+    }
 #pragma unroll 2
-    for (int k = 0; k < w; k += kChunk) {
+    for (; k < w; k += kChunk) {
         const int4 c = __ldcs(reinterpret_cast<const int4*>(cp + (int64_t)k * kSlice));
         VT v[4];
         Vec4<VT>::load(vp + (int64_t)k * kSlice, v);

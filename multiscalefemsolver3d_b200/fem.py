@@ -15,10 +15,10 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _lib
-from ._lib import (BICGSTAB, CG, ELASTIC, FP32_IR, FP64, GMRES, PCG_JACOBI, ROW_AND_COLUMN, ROW_ONLY, SCALAR,
+from ._lib import (BICGSTAB, CG, ELASTIC, FP32_IR, FP64, GMRES, MINRES, PCG_JACOBI, ROW_AND_COLUMN, ROW_ONLY, SCALAR,
                    Stats, check, load)
 
-__all__ = ["System", "Csr", "fem_scalar_driver", "fem_elastic_driver", "CG", "PCG_JACOBI", "BICGSTAB", "GMRES",
+__all__ = ["System", "Csr", "fem_scalar_driver", "fem_elastic_driver", "CG", "PCG_JACOBI", "BICGSTAB", "GMRES", "MINRES",
            "FP64", "FP32_IR", "ROW_ONLY", "ROW_AND_COLUMN", "SCALAR", "ELASTIC"]
 
 
@@ -166,6 +166,14 @@ class System:
         x = np.ascontiguousarray(x, dtype=np.float64)
         y = np.empty(self.n_rows)
         check(load().msfem_spmv(self.h, x.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p), 0), "spmv")
+        return y
+
+    def spmv_scaled32(self, x):
+        """y = D^-1/2 A D^-1/2 x in FP32 (the operator of the FP32 inner solves)."""
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.empty(self.n_rows, dtype=np.float32)
+        check(load().msfem_spmv_scaled32(self.h, x.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p), 0),
+              "spmv_scaled32")
         return y
 
     def export_csr(self) -> Csr:

@@ -134,3 +134,17 @@ def test_restarted_gmres_and_jacobi_pcg_converge(port, ref):
         x, res, it = fn()
         assert res < 1e-11
         assert np.linalg.norm(x - xref) / np.linalg.norm(xref) < 1e-10
+
+
+def test_reference_elasticity_matrix_is_symmetric_but_indefinite(port, ref):
+    """The reference's transposed element blocks (FEM/FEM_Grid.h:2147-2191) keep the global
+    elasticity matrix symmetric but make it indefinite (a null-Lagrangian term survives on
+    couplings between free-boundary nodes).  This is why the GPU path offers MINRES and uses it
+    inside the FP32 refinement for elasticity."""
+    p = meshgen.cube_elastic(n=6, jitter=0.0)
+    A, _ = ref.elastic_system(p, stage=1)
+    M = A.to_scipy().toarray()
+    assert np.abs(M - M.T).max() <= 1e-15 * np.abs(M).max()   # diagonal blocks: rounding only
+    s = 1.0 / np.sqrt(np.diag(M))
+    w = np.linalg.eigvalsh(s[:, None] * M * s[None, :])
+    assert w[0] < -1e-3 and w[-1] > 1.0
