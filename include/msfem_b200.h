@@ -204,6 +204,78 @@ int msfem_fem_elastic_driver(int n_nodes, const double* xyz, int n_tets, const i
                              int method, int precision, double min_residual, int maxiter,
                              double* solution, msfem_stats* stats);
 
+
+/* ---------------------------------------------------------------------------------------
+ * Batched MsFEM cell problems.
+ *
+ * The reference builds the MsFEM Order1 basis one macro cell at a time inside an OpenMP
+ * loop over cells (Grid_forMech_Poly_Order1::CreateFunctionalSpaces,
+ * MsFEM/MsFEM_Grid.h:4795-5759): per cell 24 edge problems (FEM::FEM_1D_forElasticDeformation,
+ * FEM/FEM.h:3796), 24 face problems (FEM_2D_forElasticDeformation, :4367) and 8 volume
+ * problems (FEM_3D_forElasticDeformation, :2970), each assembled and solved by its own
+ * SSOR-PCG restart loop.  Here every problem of every cell is solved in one persistent
+ * launch per problem kind.
+ * ------------------------------------------------------------------------------------- */
+
+typedef struct msfem_batch* msfem_batch_t;
+
+/* n_systems independent FEM_2D (dim 2: triangles) or FEM_3D (dim 3: tetrahedra)
+ * elasticity problems with zero source, as the cell drivers pose them.  System s owns the
+ * nodes [node_off[s], node_off[s+1]) of xyz and the elements [elem_off[s], elem_off[s+1])
+ * of elems (dim+1 node ids each, GLOBAL ids inside the system's own node range).
+ * fixed[node] = 1 marks a Dirichlet node (all three components).  n_rhs right-hand sides
+ * per system (1, 4 or 8).  The portrait is built and the matrices assembled here. */
+int msfem_batch_create(int dim, int n_systems, const int64_t* node_off, const double* xyz, const int64_t* elem_off,
+                       const int32_t* elems, const int32_t* material, int n_materials, const double* E,
+                       const double* nu, const uint8_t* fixed, int n_rhs, int on_device, msfem_batch_t* out);
+
+/* Solves every system.  x: [n_nodes][n_rhs][3] doubles; on entry the Dirichlet values at
+ * fixed nodes, on return the solution (free entries overwritten).  precision MSFEM_FP64 or
+ * MSFEM_FP32_IR (FP32 inner MINRES on the Jacobi-scaled free block, FP64 residual and
+ * accumulation).  Stops when ||F_I - A_II x_I|| <= tol ||F_I|| for every right-hand side, with
+ * F_I = -A_IB g the right-hand side of the free rows after the Dirichlet elimination (the
+ * reference's cell drivers also count the Dirichlet values g in ||F||, a measure up to ~1/h
+ * looser, and compensate with MIN_RESIDUAL = 5e-15).  maxiter bounds each inner solve,
+ * threads = CTA size (multiple of 32, <= 512).
+ * Returns MSFEM_NOT_CONVERGED when some system missed tol. */
+int msfem_batch_solve(msfem_batch_t b, double* x, int precision, double tol, int maxiter, int threads, int on_device);
+
+/* Per-system report of the last solve (host arrays of n_systems, any may be NULL) and its
+ * device time in ms. */
+int msfem_batch_report(msfem_batch_t b, int32_t* inner_iterations, int32_t* outer_iterations, double* rel_residual,
+                       double* ms);
+void msfem_batch_destroy(msfem_batch_t b);
+
+typedef struct msfem_cells* msfem_cells_t;
+
+/* n_cells MsFEM Order1 macro cells.  Cell c is the axis-aligned box
+ * box[6c..6c+5] = (x0, x1, y0, y1, z0, z1) carrying its own fine tetrahedral mesh: nodes
+ * [node_off[c], node_off[c+1]) of xyz and tets [tet_off[c], tet_off[c+1]) whose four node ids
+ * are CELL-LOCAL (0-based within the cell, as in the reference's per-cell NVTR files,
+ * MsFEM_Grid.h:4837).  Vertex v of a cell is its box corner (x_{v&1}, y_{(v>>1)&1},
+ * z_{(v>>2)&1}); a fine node must sit on each corner.  Builds the cell topology (faces,
+ * edges, face triangles) and the portraits of all face and volume problems. */
+int msfem_cells_create(int n_cells, const int64_t* node_off, const double* xyz, const int64_t* tet_off,
+                       const int32_t* tets, const int32_t* material, const double* box, int n_materials,
+                       const double* E, const double* nu, int on_device, msfem_cells_t* out);
+
+/* The Order1 basis of every cell: edge profiles (the exact FEM_1D solutions), the 4 face
+ * problems of each of the 6 faces and the 8 volume problems, in that order, on the GPU.
+ * precision / tol / maxiter / threads as for msfem_batch_solve. */
+int msfem_cells_build_bases(msfem_cells_t c, int precision, double tol, int maxiter, int threads);
+
+/* bases: [n_nodes][8][3] doubles, node-major (the reference's self_basis_functions[v][node]
+ * as Points, MsFEM_Grid.h:5510-5530, transposed to node-major). */
+int msfem_cells_get_bases(msfem_cells_t c, double* bases, int on_device);
+
+/* Per-cell report of the last build (host arrays of n_cells, any may be NULL):
+ * inner iterations, outer refinement steps and final relative residual of the volume
+ * problems, and the worst relative residual of the cell's face problems.
+ * ms[0..3] = device ms of assembly, edges, faces, volumes. */
+int msfem_cells_report(msfem_cells_t c, int32_t* inner_iterations, int32_t* outer_iterations, double* rel_residual,
+                       double* face_rel_residual, double* ms);
+void msfem_cells_destroy(msfem_cells_t c);
+
 #ifdef __cplusplus
 }
 #endif

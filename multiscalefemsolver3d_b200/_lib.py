@@ -75,6 +75,17 @@ _SIGS = [
     ("msfem_fem_elastic_driver", C.c_int, [C.c_int, _P, C.c_int, _P, _P, C.c_int, _P, _P, C.c_int, _P, _P, _P,
                                            C.c_int, _P, _P, C.c_int, C.c_int, C.c_double, C.c_int, _P,
                                            C.POINTER(Stats)]),
+    ("msfem_batch_create", C.c_int, [C.c_int, C.c_int, _P, _P, _P, _P, _P, C.c_int, _P, _P, _P, C.c_int, C.c_int,
+                                     C.POINTER(C.c_void_p)]),
+    ("msfem_batch_solve", C.c_int, [C.c_void_p, _P, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int]),
+    ("msfem_batch_report", C.c_int, [C.c_void_p, _P, _P, _P, C.POINTER(C.c_double)]),
+    ("msfem_batch_destroy", None, [C.c_void_p]),
+    ("msfem_cells_create", C.c_int, [C.c_int, _P, _P, _P, _P, _P, _P, C.c_int, _P, _P, C.c_int,
+                                     C.POINTER(C.c_void_p)]),
+    ("msfem_cells_build_bases", C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int]),
+    ("msfem_cells_get_bases", C.c_int, [C.c_void_p, _P, C.c_int]),
+    ("msfem_cells_report", C.c_int, [C.c_void_p, _P, _P, _P, _P, _P]),
+    ("msfem_cells_destroy", None, [C.c_void_p]),
 ]
 
 EXPORTED = [name for name, _, _ in _SIGS]

@@ -1,0 +1,112 @@
+"""Python view of the batched MsFEM cell problems (include/msfem_b200.h,
+msfem_batch_* and msfem_cells_*).  Every call goes through libmsfem_b200.so.
+
+`Cells` mirrors Grid_forMech_Poly_Order1::CreateFunctionalSpaces
+(MsFEM/MsFEM_Grid.h:4795-5759) for a whole batch of macro cells: build_bases()
+solves all edge, face and volume problems on the GPU and bases() returns the
+8 vector basis functions of every cell, node-major [n_nodes, 8, 3].
+
+`BatchSystems` is the batched form of the reference's cell drivers
+FEM_2D/FEM_3D_forElasticDeformation (FEM/FEM.h:4367, :2970): independent
+Dirichlet problems with zero source, several right-hand sides each.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import FP32_IR, FP64, check, load
+
+__all__ = ["Cells", "BatchSystems", "FP64", "FP32_IR"]
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class BatchSystems:
+    def __init__(self, dim, node_off, xyz, elem_off, elems, mat, E, nu, fixed, n_rhs):
+        L = load()
+        self._keep = [_c(node_off, np.int64), _c(xyz, np.float64), _c(elem_off, np.int64), _c(elems, np.int32),
+                      _c(mat, np.int32), _c(E, np.float64), _c(nu, np.float64), _c(fixed, np.uint8)]
+        no, xy, eo, el, mt, e, n, fx = self._keep
+        self.n_sys = no.size - 1
+        self.n_nodes = int(no[-1])
+        self.R = n_rhs
+        h = C.c_void_p()
+        check(L.msfem_batch_create(dim, self.n_sys, _p(no), _p(xy), _p(eo), _p(el), _p(mt), e.size, _p(e), _p(n),
+                                   _p(fx), n_rhs, 0, C.byref(h)), "batch_create")
+        self.h = h
+
+    def solve(self, x, precision=FP32_IR, tol=1e-8, maxiter=5000, threads=256):
+        """x: [n_nodes, R, 3] with the Dirichlet values at fixed nodes; returns (x, rc)."""
+        x = _c(x, np.float64).copy()
+        rc = check(load().msfem_batch_solve(self.h, _p(x), precision, tol, maxiter, threads, 0), "batch_solve")
+        return x, rc
+
+    def report(self):
+        it = np.zeros(self.n_sys, np.int32)
+        out = np.zeros(self.n_sys, np.int32)
+        rel = np.zeros(self.n_sys)
+        ms = C.c_double()
+        check(load().msfem_batch_report(self.h, _p(it), _p(out), _p(rel), C.byref(ms)), "batch_report")
+        return {"inner": it, "outer": out, "rel": rel, "ms": ms.value}
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().msfem_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Cells:
+    def __init__(self, cm):
+        """cm: meshgen.CellMeshes (or any object with the same fields)."""
+        L = load()
+        self._keep = [_c(cm.node_off, np.int64), _c(cm.xyz, np.float64), _c(cm.tet_off, np.int64),
+                      _c(cm.tets, np.int32), _c(cm.mat, np.int32), _c(cm.box, np.float64), _c(cm.E, np.float64),
+                      _c(cm.nu, np.float64)]
+        no, xy, to, te, mt, bx, e, n = self._keep
+        self.n_cells = no.size - 1
+        self.n_nodes = int(no[-1])
+        h = C.c_void_p()
+        check(L.msfem_cells_create(self.n_cells, _p(no), _p(xy), _p(to), _p(te), _p(mt), _p(bx), e.size, _p(e), _p(n),
+                                   0, C.byref(h)), "cells_create")
+        self.h = h
+
+    def build_bases(self, precision=FP32_IR, tol=1e-8, maxiter=5000, threads=256):
+        return check(load().msfem_cells_build_bases(self.h, precision, tol, maxiter, threads), "cells_build_bases")
+
+    def bases(self):
+        out = np.empty((self.n_nodes, 8, 3))
+        check(load().msfem_cells_get_bases(self.h, _p(out), 0), "cells_get_bases")
+        return out
+
+    def report(self):
+        n = self.n_cells
+        it, out = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        rel, frel, ms = np.zeros(n), np.zeros(n), np.zeros(4)
+        check(load().msfem_cells_report(self.h, _p(it), _p(out), _p(rel), _p(frel), _p(ms)), "cells_report")
+        return {"inner": it, "outer": out, "rel": rel, "face_rel": frel,
+                "ms": dict(zip(("assemble", "edges", "faces", "volumes"), ms.tolist()))}
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().msfem_cells_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

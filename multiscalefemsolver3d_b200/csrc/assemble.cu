@@ -11,45 +11,11 @@
 #include <cub/cub.cuh>
 
 #include "devutil.cuh"
+#include "element.cuh"
 #include "internal.cuh"
 
 namespace msfem {
 namespace {
-
-struct TetGeom {
-    double g[4][3];  // gradients of the four P1 basis functions
-    double vol;      // |det| / 6
-};
-
-// Gradients from edge vectors: for e_k = p_k - p_0, grad(l1) = (e2 x e3)/det,
-// grad(l2) = (e3 x e1)/det, grad(l3) = (e1 x e2)/det, grad(l0) = -sum; these are
-// the alpha[v][1..3] of Tetrahedron::SolveAlphaMatrix (GeometryShape.h:1960-2086)
-// and vol = GetVolume (:1674-1705).
-__device__ __forceinline__ void tet_geometry(const double* __restrict__ xyz, const int v[4], TetGeom& t)
-{
-    double p0[3], e1[3], e2[3], e3[3];
-#pragma unroll
-    for (int a = 0; a < 3; a++) p0[a] = xyz[3 * (int64_t)v[0] + a];
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        e1[a] = xyz[3 * (int64_t)v[1] + a] - p0[a];
-        e2[a] = xyz[3 * (int64_t)v[2] + a] - p0[a];
-        e3[a] = xyz[3 * (int64_t)v[3] + a] - p0[a];
-    }
-    const double c23[3] = {e2[1] * e3[2] - e2[2] * e3[1], e2[2] * e3[0] - e2[0] * e3[2], e2[0] * e3[1] - e2[1] * e3[0]};
-    const double c31[3] = {e3[1] * e1[2] - e3[2] * e1[1], e3[2] * e1[0] - e3[0] * e1[2], e3[0] * e1[1] - e3[1] * e1[0]};
-    const double c12[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
-    const double det = e1[0] * c23[0] + e1[1] * c23[1] + e1[2] * c23[2];
-    const double inv = 1.0 / det;
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        t.g[1][a] = c23[a] * inv;
-        t.g[2][a] = c31[a] * inv;
-        t.g[3][a] = c12[a] * inv;
-        t.g[0][a] = -(t.g[1][a] + t.g[2][a] + t.g[3][a]);
-    }
-    t.vol = fabs(det) / 6.0;
-}
 
 __device__ __forceinline__ void load_tet(const int32_t* __restrict__ tets, int e, int v[4])
 {
@@ -249,19 +215,11 @@ int assemble_scalar(System& s, const double* sigma, int n_mat)
     return finish_assembly(s, bad);
 }
 
-int assemble_elastic(System& s, const double* E, const double* nu, int n_mat)
+// Domain::forMech::SetIsotropic_D (Library/Domain.h:53-78): k = E(1-nu)/((1+nu)(1-2nu)),
+// off-diagonal normal coupling a*k, shear b*k  ->  lambda = a*k, mu = b*k; E <= 0 gives a
+// material that contributes nothing (FEM/FEM.h:1355-1363)
+void lame_params(const double* E, const double* nu, int n_mat, double* lame)
 {
-    if (s.kind != MSFEM_ELASTIC) {
-        set_error("assemble_elastic on a scalar system");
-        return MSFEM_ERR_STATE;
-    }
-    if (n_mat <= 0 || !E || !nu) {
-        set_error("assemble_elastic: no materials");
-        return MSFEM_ERR_ARGUMENT;
-    }
-    // Domain::forMech::SetIsotropic_D (Library/Domain.h:53-78): k = E(1-nu)/((1+nu)(1-2nu)),
-    // off-diagonal normal coupling a*k, shear b*k  ->  lambda = a*k, mu = b*k
-    std::vector<double> lame(2 * (size_t)n_mat);
     for (int m = 0; m < n_mat; m++) {
         if (E[m] <= 0) {
             lame[2 * m] = 0.0;
@@ -274,6 +232,20 @@ int assemble_elastic(System& s, const double* E, const double* nu, int n_mat)
         lame[2 * m] = a * k;
         lame[2 * m + 1] = b * k;
     }
+}
+
+int assemble_elastic(System& s, const double* E, const double* nu, int n_mat)
+{
+    if (s.kind != MSFEM_ELASTIC) {
+        set_error("assemble_elastic on a scalar system");
+        return MSFEM_ERR_STATE;
+    }
+    if (n_mat <= 0 || !E || !nu) {
+        set_error("assemble_elastic: no materials");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    std::vector<double> lame(2 * (size_t)n_mat);
+    lame_params(E, nu, n_mat, lame.data());
     DBuf<double>& d_lame = s.params;
     DBuf<int>& bad = s.flag;
     MSFEM_TRY(d_lame.alloc(2 * (size_t)n_mat));

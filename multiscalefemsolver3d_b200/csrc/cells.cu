@@ -1,0 +1,960 @@
+// MsFEM Order1 cell bases on the GPU (Grid_forMech_Poly_Order1::CreateFunctionalSpaces,
+// MsFEM/MsFEM_Grid.h:4795-5759), and the C ABI of the batched cell problems.
+//
+// Per macro cell (an axis-aligned box with its own fine tetrahedral mesh) the
+// reference solves, one cell per OpenMP thread:
+//   - 24 edge problems (FEM_1D_forElasticDeformation, FEM/FEM.h:3796): on each of the
+//     12 box edges, elasticity over the fine segments with the Point (1,1,1) at one
+//     end and 0 at the other (MsFEM_Grid.h:5061-5200);
+//   - 24 face problems (FEM_2D_forElasticDeformation, :4367): on each face, for each
+//     of its 4 vertices v, elasticity over the face triangles with the two edge
+//     solutions of v on the edges through v and 0 on the other two (:5205-5340);
+//   - 8 volume problems (FEM_3D_forElasticDeformation, :2970): for each vertex v,
+//     elasticity over the tetrahedra with the face solutions of v on the three faces
+//     through v and 0 on the others (:5380-5510).
+// Here the edges are solved in closed form (a segment's block is
+// ((lambda+mu) d d^T + mu I)/L, so along the edge direction d the problem is a 1-D
+// Laplacian with coefficient lambda + 2 mu and across it one with mu; the P1
+// solution at the nodes is the normalised cumulative compliance sum L/k, exact),
+// all face problems of all cells go to one persistent batched MINRES launch
+// (4 right-hand sides per face), then all volume problems to another (8 per cell).
+//
+// Cell conventions: vertex b at (x_{b&1}, y_{(b>>1)&1}, z_{(b>>2)&1}); face f
+// (0..5) = x0, x1, y0, y1, z0, z1; the vertices of a face in increasing b; an edge
+// segment takes the material of the face triangle holding it on the lower-numbered
+// of the edge's two faces (the reference takes it from the first neighbouring face
+// of the macro edge, MsFEM_Grid.h:4900-4925, an order its mesh files fix).
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <new>
+
+#include "batch.cuh"
+#include "devutil.cuh"
+#include "internal.cuh"
+
+namespace msfem {
+namespace {
+
+constexpr int kMaxEdgeNodes = 1024;  // nodes on one box edge
+
+__device__ __forceinline__ unsigned kFullMask() { return 0xffffffffu; }
+
+__host__ __device__ __forceinline__ int vertex_face_mask(int v)
+{
+    return (1 << (0 + (v & 1))) | (1 << (2 + ((v >> 1) & 1))) | (1 << (4 + ((v >> 2) & 1)));
+}
+
+// edge e (0..11): axis = e / 4, the two other axes (o0 < o1) at sides (s, t) = ((e>>1)&1, e&1)
+__host__ __device__ __forceinline__ void edge_info(int e, int& axis, int& fa, int& fb, int& vl, int& vh)
+{
+    axis = e / 4;
+    const int s = (e >> 1) & 1, t = e & 1;
+    const int o0 = axis == 0 ? 1 : 0, o1 = axis == 2 ? 1 : 2;
+    fa = 2 * o0 + s;
+    fb = 2 * o1 + t;
+    vl = (s << o0) | (t << o1);
+    vh = vl | (1 << axis);
+}
+
+// index of vertex v among the 4 vertices of face f (increasing b), or -1
+__host__ __device__ __forceinline__ int face_vertex_index(int f, int v)
+{
+    const int a = f >> 1, side = f & 1;
+    if (((v >> a) & 1) != side) return -1;
+    int k = 0;
+    for (int b = 0; b < v; b++)
+        if (((b >> a) & 1) == side) k++;
+    return k;
+}
+
+__host__ __device__ __forceinline__ int face_vertex(int f, int k)
+{
+    const int a = f >> 1, side = f & 1;
+    for (int b = 0; b < 8; b++)
+        if (((b >> a) & 1) == side && k-- == 0) return b;
+    return -1;
+}
+
+inline unsigned blocks_for(int64_t n, int threads = 256)
+{
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + threads - 1) / threads, 148 * 32));
+}
+
+// ---- topology kernels (one block per cell where the work is per cell)
+
+// tets: cell-local -> global ids (range checked)
+__global__ void k_globalize(int n_cells, const int64_t* __restrict__ node_off, const int64_t* __restrict__ tet_off,
+                            int32_t* __restrict__ tets, int* bad)
+{
+    const int c = blockIdx.x;
+    const int64_t n0 = node_off[c], nn = node_off[c + 1] - n0;
+    for (int64_t e = tet_off[c] + threadIdx.x; e < tet_off[c + 1]; e += blockDim.x)
+        for (int a = 0; a < 4; a++) {
+            const int64_t v = tets[4 * e + a];
+            if (v < 0 || v >= nn) {
+                atomicExch(bad, 1);
+                tets[4 * e + a] = (int32_t)n0;
+            } else {
+                tets[4 * e + a] = (int32_t)(n0 + v);
+            }
+        }
+}
+
+__global__ void k_face_mask(int n_cells, const int64_t* __restrict__ node_off, const double* __restrict__ xyz,
+                            const double* __restrict__ box, int32_t* __restrict__ mask, int32_t* __restrict__ vert,
+                            int* bad)
+{
+    const int c = blockIdx.x;
+    const double* bx = box + 6 * c;
+    const double size = fmax(bx[1] - bx[0], fmax(bx[3] - bx[2], bx[5] - bx[4]));
+    const double tol = 1e-9 * size;
+    for (int64_t i = node_off[c] + threadIdx.x; i < node_off[c + 1]; i += blockDim.x) {
+        int m = 0;
+        for (int f = 0; f < 6; f++)
+            if (fabs(xyz[3 * i + (f >> 1)] - bx[f]) <= tol) m |= 1 << f;
+        mask[i] = m;
+        if (__popc(m) == 3) {
+            // a corner: which vertex
+            const int v = ((m >> 1) & 1) | (((m >> 3) & 1) << 1) | (((m >> 5) & 1) << 2);
+            if (vertex_face_mask(v) == m) {
+                if (atomicCAS(&vert[8 * c + v], -1, (int32_t)i) != -1) atomicExch(bad, 2);
+            } else {
+                atomicExch(bad, 3);
+            }
+        } else if (__popc(m) > 3) {
+            atomicExch(bad, 3);
+        }
+    }
+}
+
+__global__ void k_face_flags(int64_t n, const int32_t* __restrict__ mask, int f, int32_t* __restrict__ flag)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        flag[i] = (mask[i] >> f) & 1;
+}
+
+__global__ void k_tri_flags(int64_t n_tets, const int32_t* __restrict__ tets, const int32_t* __restrict__ mask, int f,
+                            int32_t* __restrict__ flag)
+{
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n_tets; e += (int64_t)gridDim.x * blockDim.x) {
+        int k = 0;
+        for (int a = 0; a < 4; a++) k += (mask[tets[4 * e + a]] >> f) & 1;
+        flag[e] = k == 3 ? 1 : 0;
+    }
+}
+
+// face nodes of face f: global face-node index, its cell node and coordinates
+__global__ void k_face_nodes(int n_cells, int f, const int64_t* __restrict__ node_off, const int32_t* __restrict__ mask,
+                             const int32_t* __restrict__ pos, const int64_t* __restrict__ fsys_node_off,
+                             const double* __restrict__ xyz, int32_t* __restrict__ fidx, int32_t* __restrict__ fcell_node,
+                             double* __restrict__ fxyz, uint8_t* __restrict__ ffixed)
+{
+    const int c = blockIdx.x;
+    const int64_t first = pos[node_off[c]];
+    const int64_t base = fsys_node_off[6 * c + f];
+    for (int64_t i = node_off[c] + threadIdx.x; i < node_off[c + 1]; i += blockDim.x) {
+        const int m = mask[i];
+        if (!((m >> f) & 1)) {
+            fidx[i] = -1;
+            continue;
+        }
+        const int64_t k = base + (pos[i] - first);
+        fidx[i] = (int32_t)k;
+        fcell_node[k] = (int32_t)i;
+        for (int a = 0; a < 3; a++) fxyz[3 * k + a] = xyz[3 * i + a];
+        ffixed[k] = (m & ~(1 << f)) ? 1 : 0;  // the face border: nodes on another face too
+    }
+}
+
+// face triangles of face f (tet-local node order), in tet order
+__global__ void k_face_tris(int n_cells, int f, const int64_t* __restrict__ tet_off, const int32_t* __restrict__ tets,
+                            const int32_t* __restrict__ mat, const int32_t* __restrict__ mask,
+                            const int32_t* __restrict__ tpos, const int32_t* __restrict__ tflag,
+                            const int64_t* __restrict__ fsys_elem_off, const int32_t* __restrict__ fidx,
+                            int32_t* __restrict__ tri, int32_t* __restrict__ tri_mat)
+{
+    const int c = blockIdx.x;
+    const int64_t first = tpos[tet_off[c]];
+    const int64_t base = fsys_elem_off[6 * c + f];
+    for (int64_t e = tet_off[c] + threadIdx.x; e < tet_off[c + 1]; e += blockDim.x) {
+        if (!tflag[e]) continue;
+        const int64_t t = base + (tpos[e] - first);
+        int k = 0;
+        for (int a = 0; a < 4; a++) {
+            const int v = tets[4 * e + a];
+            if ((mask[v] >> f) & 1) tri[3 * t + k++] = fidx[v];
+        }
+        tri_mat[t] = mat ? mat[e] : 0;
+    }
+}
+
+// per (cell, edge): the nodes on the edge sorted along it, and for each segment the
+// face triangle (of the edge's lower face) that holds it.  One warp per edge.
+__global__ void k_edges(int n_cells, const int64_t* __restrict__ node_off, const int32_t* __restrict__ mask,
+                        const double* __restrict__ xyz, const int32_t* __restrict__ vert,
+                        const int32_t* __restrict__ fidx_all /* [6][n_nodes] */, int64_t n_nodes,
+                        const int64_t* __restrict__ fsys_elem_off, const int32_t* __restrict__ tri, int cap,
+                        int32_t* __restrict__ edge_nodes, int32_t* __restrict__ edge_len, int32_t* __restrict__ seg_tri,
+                        int* bad)
+{
+    __shared__ int32_t s_nodes[12][kMaxEdgeNodes];
+    const int c = blockIdx.x;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (w >= 12) return;
+    int axis, fa, fb, vl, vh;
+    edge_info(w, axis, fa, fb, vl, vh);
+    const int want = (1 << fa) | (1 << fb);
+    int cnt = 0;
+    for (int64_t base = node_off[c]; base < node_off[c + 1]; base += 32) {
+        const int64_t i = base + lane;
+        const bool on = i < node_off[c + 1] && (mask[i] & want) == want;
+        const unsigned bal = __ballot_sync(kFullMask(), on);
+        if (on) {
+            const int k = cnt + __popc(bal & ((1u << lane) - 1));
+            if (k < kMaxEdgeNodes) s_nodes[w][k] = (int32_t)i;
+        }
+        cnt += __popc(bal);
+    }
+    __syncwarp();
+    const int64_t eid = 12 * (int64_t)c + w;
+    if (cnt > kMaxEdgeNodes || cnt > cap || cnt < 2) {
+        if (lane == 0) {
+            atomicExch(bad, 4);
+            edge_len[eid] = 0;
+        }
+        return;
+    }
+    // rank sort by the coordinate along the edge (ties by list position)
+    for (int i = lane; i < cnt; i += 32) {
+        const double xi = xyz[3 * (int64_t)s_nodes[w][i] + axis];
+        int rank = 0;
+        for (int j = 0; j < cnt; j++) {
+            const double xj = xyz[3 * (int64_t)s_nodes[w][j] + axis];
+            rank += (xj < xi || (xj == xi && j < i)) ? 1 : 0;
+        }
+        edge_nodes[eid * cap + rank] = s_nodes[w][i];
+    }
+    __syncwarp();
+    if (lane == 0) {
+        edge_len[eid] = cnt;
+        if (edge_nodes[eid * cap] != vert[8 * c + vl] || edge_nodes[eid * cap + cnt - 1] != vert[8 * c + vh])
+            atomicExch(bad, 5);
+    }
+    __syncwarp();
+    // segment k = (node k, node k+1): the first triangle of face fa holding both
+    const int64_t t0 = fsys_elem_off[6 * c + fa], t1 = fsys_elem_off[6 * c + fa + 1];
+    const int32_t* fidx = fidx_all + (int64_t)fa * n_nodes;
+    for (int k = 0; k + 1 < cnt; k++) {
+        const int32_t a = fidx[edge_nodes[eid * cap + k]], b = fidx[edge_nodes[eid * cap + k + 1]];
+        int best = 0x7fffffff;
+        for (int64_t t = t0 + lane; t < t1; t += 32) {
+            const int32_t* q = tri + 3 * t;
+            const bool ha = q[0] == a || q[1] == a || q[2] == a;
+            const bool hb = q[0] == b || q[1] == b || q[2] == b;
+            if (ha && hb) best = min(best, (int)(t - t0));
+        }
+        best = __reduce_min_sync(kFullMask(), best);
+        if (lane == 0) {
+            if (best == 0x7fffffff) atomicExch(bad, 6);
+            seg_tri[eid * cap + k] = best == 0x7fffffff ? -1 : (int32_t)(t0 + best);
+        }
+    }
+}
+
+// ---- per-build kernels
+
+// exact edge solutions at the edge nodes: prof[node][0] (value 1 at the low end), prof[node][1] (1 at the high end)
+__global__ void k_edge_profiles(int n_edges, int cap, const int32_t* __restrict__ edge_nodes,
+                                const int32_t* __restrict__ edge_len, const int32_t* __restrict__ seg_tri,
+                                const int32_t* __restrict__ tri_mat, const double* __restrict__ lame, int n_mat,
+                                const double* __restrict__ xyz, double* __restrict__ prof, int* bad)
+{
+    for (int eid = blockIdx.x * blockDim.x + threadIdx.x; eid < n_edges; eid += gridDim.x * blockDim.x) {
+        const int n = edge_len[eid];
+        if (n < 2) continue;
+        const int32_t* nodes = edge_nodes + (int64_t)eid * cap;
+        const int64_t a0 = nodes[0], a1 = nodes[n - 1];
+        double d[3], len = 0.0;
+        for (int k = 0; k < 3; k++) {
+            d[k] = xyz[3 * a1 + k] - xyz[3 * a0 + k];
+            len += d[k] * d[k];
+        }
+        len = sqrt(len);
+        for (int k = 0; k < 3; k++) d[k] /= len;
+        const double dd = d[0] + d[1] + d[2];  // d . (1,1,1)
+        // totals of the compliance L/k along (lambda + 2 mu) and across (mu)
+        double tot_al = 0.0, tot_pe = 0.0;
+        for (int k = 0; k + 1 < n; k++) {
+            const int t = seg_tri[(int64_t)eid * cap + k];
+            const int m = t >= 0 ? tri_mat[t] : -1;
+            double L = 0.0;
+            for (int q = 0; q < 3; q++) {
+                const double u = xyz[3 * (int64_t)nodes[k + 1] + q] - xyz[3 * (int64_t)nodes[k] + q];
+                L += u * u;
+            }
+            L = sqrt(L);
+            if (m < 0 || m >= n_mat || !(lame[2 * m + 1] > 0.0)) {
+                atomicExch(bad, 7);
+                continue;
+            }
+            tot_al += L / (lame[2 * m] + 2.0 * lame[2 * m + 1]);
+            tot_pe += L / lame[2 * m + 1];
+        }
+        double c_al = 0.0, c_pe = 0.0;
+        for (int k = 0; k < n; k++) {
+            if (k > 0) {
+                const int t = seg_tri[(int64_t)eid * cap + k - 1];
+                const int m = t >= 0 ? tri_mat[t] : 0;
+                double L = 0.0;
+                for (int q = 0; q < 3; q++) {
+                    const double u = xyz[3 * (int64_t)nodes[k] + q] - xyz[3 * (int64_t)nodes[k - 1] + q];
+                    L += u * u;
+                }
+                L = sqrt(L);
+                if (m >= 0 && m < n_mat && lame[2 * m + 1] > 0.0) {
+                    c_al += L / (lame[2 * m] + 2.0 * lame[2 * m + 1]);
+                    c_pe += L / lame[2 * m + 1];
+                }
+            }
+            // value at the low end: 1 - C(k)/C_tot; at the high end: C(k)/C_tot (exact ends)
+            const double hi_al = k == n - 1 ? 1.0 : c_al / tot_al, hi_pe = k == n - 1 ? 1.0 : c_pe / tot_pe;
+            const double lo_al = k == 0 ? 1.0 : (k == n - 1 ? 0.0 : 1.0 - hi_al);
+            const double lo_pe = k == 0 ? 1.0 : (k == n - 1 ? 0.0 : 1.0 - hi_pe);
+            const double hal = k == 0 ? 0.0 : hi_al, hpe = k == 0 ? 0.0 : hi_pe;
+            if (k == 0 || k == n - 1) continue;  // corners: the face problems use the vertex identity
+            double* o = prof + 6 * (int64_t)nodes[k];
+            for (int q = 0; q < 3; q++) {
+                // Point (1,1,1) split into its part along d and across d
+                const double along = dd * d[q], across = 1.0 - along;
+                o[q] = lo_al * along + lo_pe * across;
+                o[3 + q] = hal * along + hpe * across;
+            }
+        }
+    }
+}
+
+// Dirichlet data of the face problems: fx[face node][j][3] for the 4 vertices j of the face
+__global__ void k_face_dirichlet(int64_t n_fnodes, const int32_t* __restrict__ fcell_node, const uint8_t* __restrict__ ffixed,
+                                 const int64_t* __restrict__ fsys_node_off, int n_fsys, const int32_t* __restrict__ mask,
+                                 const int32_t* __restrict__ vert, const int64_t* __restrict__ node_off, int n_cells,
+                                 const double* __restrict__ prof, double* __restrict__ fx)
+{
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n_fnodes; k += (int64_t)gridDim.x * blockDim.x) {
+        double* o = fx + 12 * k;
+        for (int q = 0; q < 12; q++) o[q] = 0.0;
+        if (!ffixed[k]) continue;
+        // the face system of this node (binary search in fsys_node_off)
+        int lo = 0, hi = n_fsys - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (fsys_node_off[mid] <= k) lo = mid;
+            else hi = mid - 1;
+        }
+        const int c = lo / 6, f = lo % 6;
+        const int64_t i = fcell_node[k];
+        const int m = mask[i];
+        for (int j = 0; j < 4; j++) {
+            const int v = face_vertex(f, j);
+            if (__popc(m) == 3) {
+                const double val = (i == vert[8 * c + v]) ? 1.0 : 0.0;
+                for (int q = 0; q < 3; q++) o[3 * j + q] = val;
+                continue;
+            }
+            // the edge through this node: faces f and g (the other bit)
+            const int g = __ffs(m & ~(1 << f)) - 1;
+            for (int e = 0; e < 12; e++) {
+                int axis, fa, fb, vl, vh;
+                edge_info(e, axis, fa, fb, vl, vh);
+                if (!((fa == f && fb == g) || (fa == g && fb == f))) continue;
+                if (v == vl || v == vh) {
+                    const double* p = prof + 6 * i + (v == vl ? 0 : 3);
+                    for (int q = 0; q < 3; q++) o[3 * j + q] = p[q];
+                }
+            }
+        }
+    }
+}
+
+// Dirichlet data of the volume problems: x[node][v][3] from the face solutions
+__global__ void k_volume_dirichlet(int64_t n_nodes, const int32_t* __restrict__ mask, const int32_t* __restrict__ fidx_all,
+                                   const double* __restrict__ fx, double* __restrict__ x)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_nodes; i += (int64_t)gridDim.x * blockDim.x) {
+        const int m = mask[i];
+        double* o = x + 24 * i;
+        for (int v = 0; v < 8; v++) {
+            const int common = m & vertex_face_mask(v);
+            double val[3] = {0.0, 0.0, 0.0};
+            if (common) {
+                const int f = __ffs(common) - 1;  // the lowest face through both
+                const int64_t k = fidx_all[(int64_t)f * n_nodes + i];
+                const int j = face_vertex_index(f, v);
+                for (int q = 0; q < 3; q++) val[q] = fx[12 * k + 3 * j + q];
+            }
+            for (int q = 0; q < 3; q++) o[3 * v + q] = val[q];
+        }
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ handles
+
+struct BatchHandle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    BatchSys b;
+    DBuf<double> xyz, lame, x;
+    int n_mat = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    float ms = 0.f;
+    ~BatchHandle()
+    {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+struct CellsHandle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int n_cells = 0, n_mat = 0;
+    int64_t n_nodes = 0, n_tets = 0;
+    std::vector<int64_t> h_node_off, h_tet_off;
+    DBuf<int64_t> node_off, tet_off;
+    DBuf<double> xyz, box, lame;
+    DBuf<int32_t> mat, mask, vert, fidx, fcell_node;
+    BatchSys faces, vols;
+    DBuf<double> fxyz, prof, fx, bx;
+    int cap = 0;
+    DBuf<int32_t> edge_nodes, edge_len, seg_tri;
+    DBuf<int> flag;
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    float ms[4] = {0, 0, 0, 0};
+    ~CellsHandle()
+    {
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+template <class T>
+int copy_in(cudaStream_t st, DBuf<T>& dst, const T* src, size_t n)
+{
+    MSFEM_TRY(dst.alloc(std::max<size_t>(1, n)));
+    if (n) MSFEM_CK(cudaMemcpyAsync(dst.p, src, n * sizeof(T), cudaMemcpyDefault, st));
+    return 0;
+}
+
+int read_flag(cudaStream_t st, DBuf<int>& flag, int* out)
+{
+    MSFEM_CK(cudaMemcpyAsync(out, flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    return 0;
+}
+
+int lame_to_device(cudaStream_t st, DBuf<double>& d, const double* E, const double* nu, int n_mat)
+{
+    std::vector<double> h(2 * (size_t)n_mat);
+    std::vector<double> hE(n_mat), hn(n_mat);
+    // E and nu may be device pointers: stage through the host
+    MSFEM_CK(cudaMemcpyAsync(hE.data(), E, sizeof(double) * n_mat, cudaMemcpyDefault, st));
+    MSFEM_CK(cudaMemcpyAsync(hn.data(), nu, sizeof(double) * n_mat, cudaMemcpyDefault, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    lame_params(hE.data(), hn.data(), n_mat, h.data());
+    MSFEM_TRY(d.alloc(2 * (size_t)n_mat));
+    MSFEM_CK(cudaMemcpyAsync(d.p, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    return 0;
+}
+
+int batch_finish(BatchSys& b, int* n_bad, double tol, double* worst)
+{
+    std::vector<double> rel(b.n_sys);
+    if (b.n_sys) MSFEM_CK(cudaMemcpyAsync(rel.data(), b.rel.p, sizeof(double) * b.n_sys, cudaMemcpyDeviceToHost, b.stream));
+    MSFEM_CK(cudaStreamSynchronize(b.stream));
+    int bad = 0;
+    double w = 0.0;
+    for (double r : rel) {
+        if (!(r <= tol)) bad++;
+        if (!(r <= w)) w = r;
+    }
+    *n_bad = bad;
+    if (worst) *worst = w;
+    return 0;
+}
+
+int cells_create(int n_cells, const int64_t* node_off, const double* xyz, const int64_t* tet_off, const int32_t* tets,
+                 const int32_t* material, const double* box, int n_mat, const double* E, const double* nu,
+                 CellsHandle& h)
+{
+    cudaStream_t st = h.stream;
+    h.n_cells = n_cells;
+    h.n_mat = n_mat;
+    h.h_node_off.resize(n_cells + 1);
+    h.h_tet_off.resize(n_cells + 1);
+    MSFEM_CK(cudaMemcpyAsync(h.h_node_off.data(), node_off, sizeof(int64_t) * (n_cells + 1), cudaMemcpyDefault, st));
+    MSFEM_CK(cudaMemcpyAsync(h.h_tet_off.data(), tet_off, sizeof(int64_t) * (n_cells + 1), cudaMemcpyDefault, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    if (h.h_node_off[0] != 0 || h.h_tet_off[0] != 0) {
+        set_error("msfem_cells_create: offsets must start at 0");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    for (int c = 0; c < n_cells; c++)
+        if (h.h_node_off[c + 1] < h.h_node_off[c] + 8 || h.h_tet_off[c + 1] <= h.h_tet_off[c]) {
+            set_error("msfem_cells_create: cell %d has fewer than 8 nodes or no tetrahedra", c);
+            return MSFEM_ERR_ARGUMENT;
+        }
+    h.n_nodes = h.h_node_off[n_cells];
+    h.n_tets = h.h_tet_off[n_cells];
+    if (h.n_nodes >= ((int64_t)1 << 31) || h.n_tets >= ((int64_t)1 << 28)) {
+        set_error("msfem_cells_create: %lld nodes / %lld tets exceed the int32 / 2^28 limits", (long long)h.n_nodes,
+                  (long long)h.n_tets);
+        return MSFEM_ERR_LIMIT;
+    }
+    MSFEM_TRY(copy_in(st, h.node_off, node_off, n_cells + 1));
+    MSFEM_TRY(copy_in(st, h.tet_off, tet_off, n_cells + 1));
+    MSFEM_TRY(copy_in(st, h.xyz, xyz, 3 * (size_t)h.n_nodes));
+    MSFEM_TRY(copy_in(st, h.box, box, 6 * (size_t)n_cells));
+    MSFEM_TRY(copy_in(st, h.vols.elems, tets, 4 * (size_t)h.n_tets));
+    if (material) {
+        MSFEM_TRY(copy_in(st, h.mat, material, (size_t)h.n_tets));
+    } else {
+        MSFEM_TRY(h.mat.alloc(h.n_tets));
+        MSFEM_CK(cudaMemsetAsync(h.mat.p, 0, sizeof(int32_t) * h.n_tets, st));
+    }
+    MSFEM_TRY(lame_to_device(st, h.lame, E, nu, n_mat));
+    MSFEM_TRY(h.flag.alloc(1));
+    MSFEM_CK(cudaMemsetAsync(h.flag.p, 0, sizeof(int), st));
+    k_globalize<<<n_cells, 256, 0, st>>>(n_cells, h.node_off.p, h.tet_off.p, h.vols.elems.p, h.flag.p);
+    MSFEM_TRY(h.mask.alloc(h.n_nodes));
+    MSFEM_TRY(h.vert.alloc(8 * (size_t)n_cells));
+    MSFEM_CK(cudaMemsetAsync(h.vert.p, 0xff, sizeof(int32_t) * 8 * n_cells, st));
+    k_face_mask<<<n_cells, 256, 0, st>>>(n_cells, h.node_off.p, h.xyz.p, h.box.p, h.mask.p, h.vert.p, h.flag.p);
+    MSFEM_CK(cudaGetLastError());
+    int bad = 0;
+    MSFEM_TRY(read_flag(st, h.flag, &bad));
+    if (bad) {
+        set_error(bad == 1 ? "msfem_cells_create: a tetrahedron node id is outside its cell"
+                           : "msfem_cells_create: a cell's corner nodes are missing, repeated or off the box");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    {
+        std::vector<int32_t> vh(8 * (size_t)n_cells);
+        MSFEM_CK(cudaMemcpyAsync(vh.data(), h.vert.p, sizeof(int32_t) * vh.size(), cudaMemcpyDeviceToHost, st));
+        MSFEM_CK(cudaStreamSynchronize(st));
+        for (size_t q = 0; q < vh.size(); q++)
+            if (vh[q] < 0) {
+                set_error("msfem_cells_create: cell %zu has no node on its corner %zu", q / 8, q % 8);
+                return MSFEM_ERR_ARGUMENT;
+            }
+    }
+
+    // face nodes and triangles: per face f a scan over all nodes / tets (cell order)
+    DBuf<int32_t> flag_n, pos_n, flag_t, pos_t[6], tflag[6];
+    DBuf<unsigned char> tmp;
+    MSFEM_TRY(flag_n.alloc(h.n_nodes + 1));
+    MSFEM_TRY(pos_n.alloc(6 * (h.n_nodes + 1)));
+    std::vector<int64_t> fcount(6 * (size_t)n_cells), tcount(6 * (size_t)n_cells);
+    std::vector<int32_t> hp(n_cells + 1);
+    auto scan = [&](const int32_t* in, int32_t* out, int64_t n) -> int {
+        size_t tb = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, tb, in, out, (int)n, st);
+        MSFEM_TRY(tmp.alloc(std::max<size_t>(tb, 1)));
+        MSFEM_CK(cub::DeviceScan::ExclusiveSum(tmp.p, tb, in, out, (int)n, st));
+        return 0;
+    };
+    // cell boundaries of a scan, to the host
+    auto gather_bounds = [&](const int32_t* pos, const std::vector<int64_t>& off, std::vector<int32_t>& out) -> int {
+        for (int c = 0; c <= n_cells; c++)
+            MSFEM_CK(cudaMemcpyAsync(&out[c], pos + off[c], sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        MSFEM_CK(cudaStreamSynchronize(st));
+        return 0;
+    };
+    for (int f = 0; f < 6; f++) {
+        k_face_flags<<<blocks_for(h.n_nodes), 256, 0, st>>>(h.n_nodes, h.mask.p, f, flag_n.p);
+        MSFEM_CK(cudaMemsetAsync(flag_n.p + h.n_nodes, 0, sizeof(int32_t), st));
+        MSFEM_TRY(scan(flag_n.p, pos_n.p + f * (h.n_nodes + 1), h.n_nodes + 1));
+        MSFEM_TRY(gather_bounds(pos_n.p + f * (h.n_nodes + 1), h.h_node_off, hp));
+        for (int c = 0; c < n_cells; c++) fcount[6 * c + f] = hp[c + 1] - hp[c];
+        MSFEM_TRY(tflag[f].alloc(h.n_tets + 1));
+        MSFEM_TRY(pos_t[f].alloc(h.n_tets + 1));
+        k_tri_flags<<<blocks_for(h.n_tets), 256, 0, st>>>(h.n_tets, h.vols.elems.p, h.mask.p, f, tflag[f].p);
+        MSFEM_CK(cudaMemsetAsync(tflag[f].p + h.n_tets, 0, sizeof(int32_t), st));
+        MSFEM_TRY(scan(tflag[f].p, pos_t[f].p, h.n_tets + 1));
+        MSFEM_TRY(gather_bounds(pos_t[f].p, h.h_tet_off, hp));
+        for (int c = 0; c < n_cells; c++) tcount[6 * c + f] = hp[c + 1] - hp[c];
+    }
+    BatchSys& F = h.faces;
+    F.dim = 2;
+    F.k1 = 3;
+    F.R = 4;
+    F.n_sys = 6 * n_cells;
+    F.stream = st;
+    F.h_node_off.assign(F.n_sys + 1, 0);
+    F.h_elem_off.assign(F.n_sys + 1, 0);
+    for (int s = 0; s < F.n_sys; s++) {
+        if (fcount[s] < 3 || tcount[s] < 1) {
+            set_error("msfem_cells_create: face %d of cell %d has %lld nodes and %lld triangles", s % 6, s / 6,
+                      (long long)fcount[s], (long long)tcount[s]);
+            return MSFEM_ERR_ARGUMENT;
+        }
+        F.h_node_off[s + 1] = F.h_node_off[s] + fcount[s];
+        F.h_elem_off[s + 1] = F.h_elem_off[s] + tcount[s];
+    }
+    F.n_nodes = F.h_node_off[F.n_sys];
+    F.n_elems = F.h_elem_off[F.n_sys];
+    MSFEM_TRY(copy_in(st, F.node_off, F.h_node_off.data(), F.n_sys + 1));
+    MSFEM_TRY(copy_in(st, F.elem_off, F.h_elem_off.data(), F.n_sys + 1));
+    MSFEM_TRY(h.fidx.alloc(6 * h.n_nodes));
+    MSFEM_TRY(h.fcell_node.alloc(F.n_nodes));
+    MSFEM_TRY(h.fxyz.alloc(3 * F.n_nodes));
+    MSFEM_TRY(F.fixed.alloc(F.n_nodes));
+    MSFEM_TRY(F.elems.alloc(3 * F.n_elems));
+    MSFEM_TRY(F.emat.alloc(F.n_elems));
+    for (int f = 0; f < 6; f++)
+        k_face_nodes<<<n_cells, 256, 0, st>>>(n_cells, f, h.node_off.p, h.mask.p, pos_n.p + f * (h.n_nodes + 1),
+                                               F.node_off.p, h.xyz.p, h.fidx.p + f * h.n_nodes, h.fcell_node.p, h.fxyz.p,
+                                               F.fixed.p);
+    for (int f = 0; f < 6; f++)
+        k_face_tris<<<n_cells, 256, 0, st>>>(n_cells, f, h.tet_off.p, h.vols.elems.p, h.mat.p, h.mask.p, pos_t[f].p,
+                                              tflag[f].p, F.elem_off.p, h.fidx.p + f * h.n_nodes, F.elems.p, F.emat.p);
+    MSFEM_CK(cudaGetLastError());
+    MSFEM_TRY(batch_build_pattern(F, h.fxyz.p));
+
+    // edges
+    {
+        // capacity: the longest edge (count with the same rule the kernel uses)
+        int cap = 2;
+        std::vector<int32_t> hm(h.n_nodes);
+        MSFEM_CK(cudaMemcpyAsync(hm.data(), h.mask.p, sizeof(int32_t) * h.n_nodes, cudaMemcpyDeviceToHost, st));
+        MSFEM_CK(cudaStreamSynchronize(st));
+        for (int c = 0; c < n_cells; c++) {
+            int cnt[12] = {0};
+            for (int64_t i = h.h_node_off[c]; i < h.h_node_off[c + 1]; i++)
+                for (int e = 0; e < 12; e++) {
+                    int axis, fa, fb, vl, vh;
+                    edge_info(e, axis, fa, fb, vl, vh);
+                    const int want = (1 << fa) | (1 << fb);
+                    if ((hm[i] & want) == want) cnt[e]++;
+                }
+            for (int e = 0; e < 12; e++) cap = std::max(cap, cnt[e]);
+        }
+        if (cap > kMaxEdgeNodes) {
+            set_error("msfem_cells_create: %d nodes on one cell edge (limit %d)", cap, kMaxEdgeNodes);
+            return MSFEM_ERR_LIMIT;
+        }
+        h.cap = cap;
+        MSFEM_TRY(h.edge_nodes.alloc(12 * (size_t)n_cells * cap));
+        MSFEM_TRY(h.edge_len.alloc(12 * (size_t)n_cells));
+        MSFEM_TRY(h.seg_tri.alloc(12 * (size_t)n_cells * cap));
+        MSFEM_CK(cudaMemsetAsync(h.flag.p, 0, sizeof(int), st));
+        k_edges<<<n_cells, 384, 0, st>>>(n_cells, h.node_off.p, h.mask.p, h.xyz.p, h.vert.p, h.fidx.p, h.n_nodes,
+                                         F.elem_off.p, F.elems.p, cap, h.edge_nodes.p, h.edge_len.p, h.seg_tri.p,
+                                         h.flag.p);
+        MSFEM_CK(cudaGetLastError());
+        MSFEM_TRY(read_flag(st, h.flag, &bad));
+        if (bad) {
+            set_error("msfem_cells_create: inconsistent cell edge (code %d: node count, ends or a segment without a "
+                      "face triangle)", bad);
+            return MSFEM_ERR_ARGUMENT;
+        }
+    }
+
+    // volumes: the cell meshes themselves
+    BatchSys& V = h.vols;
+    V.dim = 3;
+    V.k1 = 4;
+    V.R = 8;
+    V.n_sys = n_cells;
+    V.stream = st;
+    V.h_node_off = h.h_node_off;
+    V.h_elem_off = h.h_tet_off;
+    V.n_nodes = h.n_nodes;
+    V.n_elems = h.n_tets;
+    MSFEM_TRY(copy_in(st, V.node_off, h.h_node_off.data(), n_cells + 1));
+    MSFEM_TRY(copy_in(st, V.elem_off, h.h_tet_off.data(), n_cells + 1));
+    MSFEM_TRY(copy_in(st, V.emat, h.mat.p, (size_t)h.n_tets));
+    MSFEM_TRY(V.fixed.alloc(h.n_nodes));
+    {
+        // Dirichlet nodes: every node on the cell's boundary
+        std::vector<int32_t> hm(h.n_nodes);
+        std::vector<uint8_t> hf(h.n_nodes);
+        MSFEM_CK(cudaMemcpyAsync(hm.data(), h.mask.p, sizeof(int32_t) * h.n_nodes, cudaMemcpyDeviceToHost, st));
+        MSFEM_CK(cudaStreamSynchronize(st));
+        for (int64_t i = 0; i < h.n_nodes; i++) hf[i] = hm[i] ? 1 : 0;
+        MSFEM_CK(cudaMemcpyAsync(V.fixed.p, hf.data(), h.n_nodes, cudaMemcpyHostToDevice, st));
+        MSFEM_CK(cudaStreamSynchronize(st));
+    }
+    MSFEM_TRY(batch_build_pattern(V, h.xyz.p));
+    MSFEM_TRY(h.prof.alloc(6 * h.n_nodes));
+    MSFEM_TRY(h.fx.alloc(12 * F.n_nodes));
+    MSFEM_TRY(h.bx.alloc(24 * h.n_nodes));
+    for (auto& e : h.ev) MSFEM_CK(cudaEventCreate(&e));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    return 0;
+}
+
+int cells_build(CellsHandle& h, int precision, double tol, int maxiter, int threads)
+{
+    cudaStream_t st = h.stream;
+    BatchSys& F = h.faces;
+    BatchSys& V = h.vols;
+    MSFEM_CK(cudaEventRecord(h.ev[0], st));
+    MSFEM_TRY(batch_assemble(F, h.fxyz.p, h.lame.p, h.n_mat));
+    MSFEM_TRY(batch_assemble(V, h.xyz.p, h.lame.p, h.n_mat));
+    MSFEM_CK(cudaEventRecord(h.ev[1], st));
+    MSFEM_CK(cudaMemsetAsync(h.flag.p, 0, sizeof(int), st));
+    MSFEM_CK(cudaMemsetAsync(h.prof.p, 0, sizeof(double) * 6 * h.n_nodes, st));
+    const int n_edges = 12 * h.n_cells;
+    k_edge_profiles<<<blocks_for(n_edges, 128), 128, 0, st>>>(n_edges, h.cap, h.edge_nodes.p, h.edge_len.p, h.seg_tri.p,
+                                                              F.emat.p, h.lame.p, h.n_mat, h.xyz.p, h.prof.p, h.flag.p);
+    k_face_dirichlet<<<blocks_for(F.n_nodes), 256, 0, st>>>(F.n_nodes, h.fcell_node.p, F.fixed.p, F.node_off.p, F.n_sys,
+                                                            h.mask.p, h.vert.p, h.node_off.p, h.n_cells, h.prof.p, h.fx.p);
+    MSFEM_CK(cudaGetLastError());
+    MSFEM_CK(cudaEventRecord(h.ev[2], st));
+    MSFEM_TRY(batch_solve(F, h.fx.p, precision, tol, maxiter, threads));
+    MSFEM_CK(cudaEventRecord(h.ev[3], st));
+    k_volume_dirichlet<<<blocks_for(h.n_nodes), 256, 0, st>>>(h.n_nodes, h.mask.p, h.fidx.p, h.fx.p, h.bx.p);
+    MSFEM_CK(cudaGetLastError());
+    MSFEM_TRY(batch_solve(V, h.bx.p, precision, tol, maxiter, threads));
+    MSFEM_CK(cudaEventRecord(h.ev[4], st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    for (int k = 0; k < 4; k++) MSFEM_CK(cudaEventElapsedTime(&h.ms[k], h.ev[k], h.ev[k + 1]));
+    int bad = 0;
+    MSFEM_TRY(read_flag(st, h.flag, &bad));
+    if (bad) {
+        set_error("msfem_cells_build_bases: an edge segment has a material with zero shear modulus");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    int nf = 0, nv = 0;
+    MSFEM_TRY(batch_finish(F, &nf, tol, nullptr));
+    MSFEM_TRY(batch_finish(V, &nv, tol, nullptr));
+    if (nf || nv) {
+        set_error("msfem_cells_build_bases: %d face and %d volume problems missed the tolerance", nf, nv);
+        return MSFEM_NOT_CONVERGED;
+    }
+    return 0;
+}
+
+}  // namespace
+}  // namespace msfem
+
+using msfem::BatchHandle;
+using msfem::CellsHandle;
+
+struct msfem_batch : BatchHandle {};
+struct msfem_cells : CellsHandle {};
+
+extern "C" {
+
+int msfem_batch_create(int dim, int n_systems, const int64_t* node_off, const double* xyz, const int64_t* elem_off,
+                       const int32_t* elems, const int32_t* material, int n_materials, const double* E, const double* nu,
+                       const uint8_t* fixed, int n_rhs, int on_device, msfem_batch_t* out)
+{
+    using namespace msfem;
+    (void)on_device;
+    if (!out || (dim != 2 && dim != 3) || n_systems <= 0 || !node_off || !xyz || !elem_off || !elems || !fixed ||
+        n_materials <= 0 || !E || !nu || (n_rhs != 1 && n_rhs != 4 && n_rhs != 8)) {
+        set_error("msfem_batch_create: bad arguments");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    *out = nullptr;
+    std::unique_ptr<msfem_batch> h(new (std::nothrow) msfem_batch());
+    if (!h) {
+        set_error("out of host memory");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    MSFEM_CK(cudaGetDevice(&h->device));
+    MSFEM_CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    MSFEM_CK(cudaEventCreate(&h->e0));
+    MSFEM_CK(cudaEventCreate(&h->e1));
+    cudaStream_t st = h->stream;
+    BatchSys& b = h->b;
+    b.dim = dim;
+    b.k1 = dim + 1;
+    b.n_sys = n_systems;
+    b.R = n_rhs;
+    b.stream = st;
+    b.h_node_off.resize(n_systems + 1);
+    b.h_elem_off.resize(n_systems + 1);
+    MSFEM_CK(cudaMemcpyAsync(b.h_node_off.data(), node_off, sizeof(int64_t) * (n_systems + 1), cudaMemcpyDefault, st));
+    MSFEM_CK(cudaMemcpyAsync(b.h_elem_off.data(), elem_off, sizeof(int64_t) * (n_systems + 1), cudaMemcpyDefault, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    if (b.h_node_off[0] != 0 || b.h_elem_off[0] != 0) {
+        set_error("msfem_batch_create: offsets must start at 0");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    for (int s = 0; s < n_systems; s++)
+        if (b.h_node_off[s + 1] <= b.h_node_off[s] || b.h_elem_off[s + 1] < b.h_elem_off[s]) {
+            set_error("msfem_batch_create: offsets of system %d are not increasing", s);
+            return MSFEM_ERR_ARGUMENT;
+        }
+    b.n_nodes = b.h_node_off[n_systems];
+    b.n_elems = b.h_elem_off[n_systems];
+    h->n_mat = n_materials;
+    MSFEM_TRY(copy_in(st, b.node_off, b.h_node_off.data(), n_systems + 1));
+    MSFEM_TRY(copy_in(st, b.elem_off, b.h_elem_off.data(), n_systems + 1));
+    MSFEM_TRY(copy_in(st, h->xyz, xyz, 3 * (size_t)b.n_nodes));
+    MSFEM_TRY(copy_in(st, b.elems, elems, (size_t)b.k1 * b.n_elems));
+    if (material) {
+        MSFEM_TRY(copy_in(st, b.emat, material, (size_t)b.n_elems));
+    } else {
+        MSFEM_TRY(b.emat.alloc(std::max<int64_t>(1, b.n_elems)));
+        MSFEM_CK(cudaMemsetAsync(b.emat.p, 0, sizeof(int32_t) * std::max<int64_t>(1, b.n_elems), st));
+    }
+    MSFEM_TRY(copy_in(st, b.fixed, fixed, (size_t)b.n_nodes));
+    MSFEM_TRY(lame_to_device(st, h->lame, E, nu, n_materials));
+    MSFEM_TRY(batch_build_pattern(b, h->xyz.p));
+    MSFEM_TRY(batch_assemble(b, h->xyz.p, h->lame.p, n_materials));
+    *out = h.release();
+    return MSFEM_OK;
+}
+
+int msfem_batch_solve(msfem_batch_t h, double* x, int precision, double tol, int maxiter, int threads, int on_device)
+{
+    using namespace msfem;
+    if (!h || !x || maxiter <= 0 || !(tol > 0.0) || (precision != MSFEM_FP64 && precision != MSFEM_FP32_IR)) {
+        set_error("msfem_batch_solve: bad arguments");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    MSFEM_CK(cudaSetDevice(h->device));
+    BatchSys& b = h->b;
+    cudaStream_t st = h->stream;
+    const size_t n = (size_t)b.n_nodes * b.R * 3;
+    double* dx = x;
+    if (!on_device) {
+        MSFEM_TRY(h->x.alloc(n));
+        MSFEM_CK(cudaMemcpyAsync(h->x.p, x, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+        dx = h->x.p;
+    }
+    MSFEM_CK(cudaEventRecord(h->e0, st));
+    MSFEM_TRY(batch_solve(b, dx, precision, tol, maxiter, threads));
+    MSFEM_CK(cudaEventRecord(h->e1, st));
+    if (!on_device) MSFEM_CK(cudaMemcpyAsync(x, h->x.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    MSFEM_CK(cudaEventElapsedTime(&h->ms, h->e0, h->e1));
+    int nbad = 0;
+    MSFEM_TRY(batch_finish(b, &nbad, tol, nullptr));
+    if (nbad) {
+        set_error("msfem_batch_solve: %d of %d systems missed the tolerance", nbad, b.n_sys);
+        return MSFEM_NOT_CONVERGED;
+    }
+    return MSFEM_OK;
+}
+
+int msfem_batch_report(msfem_batch_t h, int32_t* inner, int32_t* outer, double* rel, double* ms)
+{
+    using namespace msfem;
+    if (!h) {
+        set_error("null handle");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    BatchSys& b = h->b;
+    cudaStream_t st = h->stream;
+    if (inner) MSFEM_CK(cudaMemcpyAsync(inner, b.iters.p, sizeof(int32_t) * b.n_sys, cudaMemcpyDeviceToHost, st));
+    if (outer) MSFEM_CK(cudaMemcpyAsync(outer, b.outers.p, sizeof(int32_t) * b.n_sys, cudaMemcpyDeviceToHost, st));
+    if (rel) MSFEM_CK(cudaMemcpyAsync(rel, b.rel.p, sizeof(double) * b.n_sys, cudaMemcpyDeviceToHost, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    if (ms) *ms = h->ms;
+    return MSFEM_OK;
+}
+
+void msfem_batch_destroy(msfem_batch_t h)
+{
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    delete h;
+}
+
+int msfem_cells_create(int n_cells, const int64_t* node_off, const double* xyz, const int64_t* tet_off,
+                       const int32_t* tets, const int32_t* material, const double* box, int n_materials,
+                       const double* E, const double* nu, int on_device, msfem_cells_t* out)
+{
+    using namespace msfem;
+    (void)on_device;
+    if (!out || n_cells <= 0 || !node_off || !xyz || !tet_off || !tets || !box || n_materials <= 0 || !E || !nu) {
+        set_error("msfem_cells_create: bad arguments");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    *out = nullptr;
+    std::unique_ptr<msfem_cells> h(new (std::nothrow) msfem_cells());
+    if (!h) {
+        set_error("out of host memory");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    MSFEM_CK(cudaGetDevice(&h->device));
+    MSFEM_CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    MSFEM_TRY(cells_create(n_cells, node_off, xyz, tet_off, tets, material, box, n_materials, E, nu, *h));
+    *out = h.release();
+    return MSFEM_OK;
+}
+
+int msfem_cells_build_bases(msfem_cells_t h, int precision, double tol, int maxiter, int threads)
+{
+    using namespace msfem;
+    if (!h || maxiter <= 0 || !(tol > 0.0) || (precision != MSFEM_FP64 && precision != MSFEM_FP32_IR)) {
+        set_error("msfem_cells_build_bases: bad arguments");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    MSFEM_CK(cudaSetDevice(h->device));
+    return cells_build(*h, precision, tol, maxiter, threads);
+}
+
+int msfem_cells_get_bases(msfem_cells_t h, double* bases, int on_device)
+{
+    using namespace msfem;
+    if (!h || !bases) {
+        set_error("msfem_cells_get_bases: bad arguments");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    MSFEM_CK(cudaSetDevice(h->device));
+    MSFEM_CK(cudaMemcpyAsync(bases, h->bx.p, sizeof(double) * 24 * h->n_nodes,
+                             on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, h->stream));
+    MSFEM_CK(cudaStreamSynchronize(h->stream));
+    return MSFEM_OK;
+}
+
+int msfem_cells_report(msfem_cells_t h, int32_t* inner, int32_t* outer, double* rel, double* face_rel, double* ms)
+{
+    using namespace msfem;
+    if (!h) {
+        set_error("null handle");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    cudaStream_t st = h->stream;
+    const int n = h->n_cells;
+    if (inner) MSFEM_CK(cudaMemcpyAsync(inner, h->vols.iters.p, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st));
+    if (outer) MSFEM_CK(cudaMemcpyAsync(outer, h->vols.outers.p, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st));
+    if (rel) MSFEM_CK(cudaMemcpyAsync(rel, h->vols.rel.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    std::vector<double> fr(6 * (size_t)n);
+    if (face_rel) MSFEM_CK(cudaMemcpyAsync(fr.data(), h->faces.rel.p, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    if (face_rel)
+        for (int c = 0; c < n; c++) {
+            double w = 0.0;
+            for (int f = 0; f < 6; f++) w = std::max(w, fr[6 * c + f]);
+            face_rel[c] = w;
+        }
+    if (ms)
+        for (int k = 0; k < 4; k++) ms[k] = h->ms[k];
+    return MSFEM_OK;
+}
+
+void msfem_cells_destroy(msfem_cells_t h)
+{
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    delete h;
+}
+
+}  // extern "C"

@@ -167,6 +167,8 @@ int build_topology(System& s);
 // ---- assembly (assemble.cu)
 int assemble_scalar(System& s, const double* sigma, int n_mat);
 int assemble_elastic(System& s, const double* E, const double* nu, int n_mat);
+// lambda, mu per material from E, nu (host): lame[2m], lame[2m+1]
+void lame_params(const double* E, const double* nu, int n_mat, double* lame);
 int add_traction(System& s, int n_faces, const int32_t* d_faces, const double* d_traction);
 // ---- boundary conditions (bc.cu)
 int apply_dirichlet(System& s, int n, const int32_t* d_dofs, const double* d_values, int mode);

@@ -202,3 +202,71 @@ def cube_scalar(n: int = 100, jitter: float = 0.0, seed: int = 1234, n_spheres: 
     nodes = np.concatenate([left, right]).astype(np.int32)
     vals = np.concatenate([np.ones(left.size), np.zeros(right.size)])
     return ScalarProblem(mesh=mesh, sigma=np.array(sig), bc_nodes=nodes, bc_values=vals)
+
+
+# ----------------------------------------------------------------------------------------------
+# MsFEM macro cells, each with its own fine mesh
+# ----------------------------------------------------------------------------------------------
+
+@dataclass
+class CellMeshes:
+    """Concatenated per-cell fine meshes (cell-local tet node ids, as the
+    reference's per-cell NVTR files hold them, MsFEM/MsFEM_Grid.h:4837)."""
+    node_off: np.ndarray   # int64 [n_cells + 1]
+    xyz: np.ndarray        # float64 [n_nodes, 3]
+    tet_off: np.ndarray    # int64 [n_cells + 1]
+    tets: np.ndarray       # int32 [n_tets, 4], cell-local
+    mat: np.ndarray        # int32 [n_tets]
+    box: np.ndarray        # float64 [n_cells, 6] (x0, x1, y0, y1, z0, z1)
+    E: np.ndarray
+    nu: np.ndarray
+    m: np.ndarray          # int32 [n_cells] fine hexahedra per cell edge
+
+    @property
+    def n_cells(self) -> int:
+        return int(self.box.shape[0])
+
+    def cell(self, c: int):
+        """(xyz, tets (local), mat, box) of cell c."""
+        a, b = self.node_off[c], self.node_off[c + 1]
+        s, t = self.tet_off[c], self.tet_off[c + 1]
+        return self.xyz[a:b], self.tets[s:t], self.mat[s:t], self.box[c]
+
+
+def msfem_cells(n_coarse: int = 16, m_choices=(8, 12, 16, 20), seed: int = 3, max_inclusions: int = 3,
+                contrast: float = 50.0, nu: float = 0.3, semi=(0.15, 0.45), cells=None) -> CellMeshes:
+    """n_coarse^3 macro cells on the unit cube; cell (i, j, k) (index i + n(j + n k)) is the box
+    [i/n, (i+1)/n] x ..., meshed by kuhn_cube(m) with m drawn per cell from m_choices.  Each
+    cell holds 1..max_inclusions axis-aligned ellipsoids (centres U(0,1)^3 and semi-axes
+    U(semi) in cell units) whose tets (by centroid) take material 1 with E = contrast.
+    `cells` restricts the batch to the listed cell indices (the draws stay those of the full grid)."""
+    rng = np.random.default_rng(seed)
+    n_all = n_coarse ** 3
+    ms = rng.choice(np.asarray(m_choices), size=n_all)
+    n_inc = rng.integers(1, max_inclusions + 1, size=n_all)
+    cen = rng.uniform(0.0, 1.0, size=(n_all, max_inclusions, 3))
+    ax = rng.uniform(semi[0], semi[1], size=(n_all, max_inclusions, 3))
+    sel = np.arange(n_all) if cells is None else np.asarray(cells)
+    h = 1.0 / n_coarse
+    templ = {}
+    for m in np.unique(ms[sel]):
+        t = kuhn_cube(int(m))
+        templ[int(m)] = (t.xyz, t.tets, tet_centroids(t))
+    xyzs, tetss, mats, boxes, noff, toff = [], [], [], [], [0], [0]
+    for c in sel:
+        i, j, k = c % n_coarse, (c // n_coarse) % n_coarse, c // (n_coarse * n_coarse)
+        lo = np.array([i, j, k], dtype=np.float64) * h
+        uxyz, utets, ucen = templ[int(ms[c])]
+        xyzs.append(lo + uxyz * h)
+        inside = np.zeros(utets.shape[0], dtype=bool)
+        for q in range(n_inc[c]):
+            inside |= (((ucen - cen[c, q]) / ax[c, q]) ** 2).sum(axis=1) < 1.0
+        tetss.append(utets)
+        mats.append(inside.astype(np.int32))
+        boxes.append([lo[0], lo[0] + h, lo[1], lo[1] + h, lo[2], lo[2] + h])
+        noff.append(noff[-1] + uxyz.shape[0])
+        toff.append(toff[-1] + utets.shape[0])
+    return CellMeshes(node_off=np.array(noff, dtype=np.int64), xyz=np.concatenate(xyzs),
+                      tet_off=np.array(toff, dtype=np.int64), tets=np.concatenate(tetss).astype(np.int32),
+                      mat=np.concatenate(mats), box=np.array(boxes), E=np.array([1.0, contrast]),
+                      nu=np.array([nu, nu]), m=ms[sel].astype(np.int32))

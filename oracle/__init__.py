@@ -77,8 +77,10 @@ class RefLib:
         L.ref_cssd_solve.argtypes = [C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_int, C.c_double,
                                      C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.ref_ssor_apply.argtypes = [C.c_int, _i32p, _i32p, _f64p, C.c_double, _f64p, _f64p]
+        L.ref_cell_problem.argtypes = [C.c_int, C.c_int, _f64p, C.c_int, _i32p, _i32p, C.c_int, _f64p, _f64p,
+                                       C.c_int, _i32p, _f64p, C.c_double, _f64p]
         for f in ("ref_elastic_local", "ref_scalar_local", "ref_elastic_system", "ref_elastic_driver",
-                  "ref_scalar_system", "ref_scalar_driver", "ref_cssd_solve", "ref_ssor_apply"):
+                  "ref_scalar_system", "ref_scalar_driver", "ref_cssd_solve", "ref_ssor_apply", "ref_cell_problem"):
             getattr(L, f).restype = C.c_int
         L.ref_set_quiet(1)
 
@@ -167,6 +169,19 @@ class RefLib:
                                    _c(A.F, np.float64), X, maxiter, tol, nthreads, C.byref(res), C.byref(wall))
         assert rc == 0, rc
         return X, res.value, wall.value
+
+    def cell_problem(self, dim: int, xyz, elems, mat, E, nu, bc_nodes, bc_values, min_residual: float = 5e-15):
+        """One MsFEM cell sub-problem (dim 1 edge, 2 face, 3 volume) through the reference's
+        FEM_1D/2D/3D_forElasticDeformation; returns the solution [n_nodes, 3]."""
+        xyz = _c(xyz, np.float64)
+        elems = _c(elems, np.int32)
+        n = xyz.shape[0]
+        sol = np.zeros(3 * n)
+        rc = self.L.ref_cell_problem(dim, n, xyz.ravel(), elems.shape[0], elems.ravel(), _c(mat, np.int32),
+                                     len(E), _c(E, np.float64), _c(nu, np.float64), len(bc_nodes),
+                                     _c(bc_nodes, np.int32), _c(bc_values, np.float64).ravel(), min_residual, sol)
+        assert rc == 0, rc
+        return sol.reshape(n, 3)
 
     def ssor_apply(self, A: Csr, r, w: float = 0.75):
         z = np.zeros(A.n)

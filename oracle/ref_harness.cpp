@@ -28,6 +28,10 @@ struct DirichletMech {
     std::vector<int> id_vertexes;
     std::function<Point<double>(Point<bool>&, int)> value;
 };
+struct DirichletMech1D { /* edge problems: one constant Point per group (FEM/FEM_Grid.h:3798) */
+    std::vector<int> id_vertexes;
+    std::function<Point<double>(Point<bool>&)> value;
+};
 struct NeumannMech {
     std::function<Point<double>(Point<double>)> value;
     std::vector<std::function<Point<double>(Point<double>)>> values;
@@ -69,16 +73,23 @@ double wall_now()
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-void make_simple_grid(math::SimpleGrid& g, int n_nodes, const double* xyz, int n_tets, const int* tets, const int* mat)
+/* math::SimpleGrid (Library/Math.h:26-33) from arrays; k nodes per element. */
+void make_simple_grid_k(math::SimpleGrid& g, int n_nodes, const double* xyz, int n_elems, int k, const int* elems,
+                        const int* mat)
 {
     g.xyz.resize(n_nodes);
     for (int i = 0; i < n_nodes; i++) g.xyz[i] = Point<double>(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
-    g.nvtr.resize(n_tets);
-    g.nvkat.resize(n_tets);
-    for (int e = 0; e < n_tets; e++) {
-        g.nvtr[e] = {tets[4 * e], tets[4 * e + 1], tets[4 * e + 2], tets[4 * e + 3]};
+    g.nvtr.resize(n_elems);
+    g.nvkat.resize(n_elems);
+    for (int e = 0; e < n_elems; e++) {
+        g.nvtr[e].assign(elems + (size_t)k * e, elems + (size_t)k * (e + 1));
         g.nvkat[e] = mat ? mat[e] : 0;
     }
+}
+
+void make_simple_grid(math::SimpleGrid& g, int n_nodes, const double* xyz, int n_tets, const int* tets, const int* mat)
+{
+    make_simple_grid_k(g, n_nodes, xyz, n_tets, 4, tets, mat);
 }
 
 struct CsrOut {
@@ -200,7 +211,8 @@ void make_scal_boundaries(int n_bc, const int* bc_node, const double* bc_val, st
     }
 }
 
-void set_materials_mech(FEM::Grid_forMech& grid, int n_mat, const double* E, const double* nu)
+template <class Grid>
+void set_materials_mech(Grid& grid, int n_mat, const double* E, const double* nu)
 {
     for (int m = 0; m < n_mat; m++) {
         grid.AddDomain();
@@ -573,6 +585,72 @@ int ref_ssor_apply(int n, const int* row_ptr, const int* col, const double* val,
     P->SolvePrecondorSSOR_SLAE(A->Diag, zz, rr);
     for (int i = 0; i < n; i++) z[i] = zz[i];
     return 0;
+}
+
+
+/* One MsFEM cell sub-problem through the reference's own drivers, the calls
+ * MsFEM/MsFEM_Grid.h:5119-5176 (edges), :5312 (faces) and :5495 (volume) make:
+ *   dim 1 -> FEM::FEM_1D_forElasticDeformation (FEM/FEM.h:3796), segments
+ *   dim 2 -> FEM::FEM_2D_forElasticDeformation (FEM/FEM.h:4367), triangles
+ *   dim 3 -> FEM::FEM_3D_forElasticDeformation (FEM/FEM.h:2970), tetrahedra
+ * elems: (dim+1) node ids per element; Dirichlet: all three components of every
+ * listed node take bc_val[3i..3i+2] (the cell drivers fix whole Points); zero
+ * source, no traction.  solution: 3*n_nodes doubles, node-major. */
+int ref_cell_problem(int dim, int n_nodes, const double* xyz, int n_elems, const int* elems, const int* mat,
+                     int n_mat, const double* E, const double* nu, int n_bc, const int* bc_node, const double* bc_val,
+                     double min_residual, double* solution)
+{
+    StdoutSilencer s;
+    math::NUM_THREADS = 1;
+    auto* g = new math::SimpleGrid();
+    make_simple_grid_k(*g, n_nodes, xyz, n_elems, dim + 1, elems, mat);
+    auto* dir = new std::vector<DirichletMech>();
+    auto* neu = new std::vector<NeumannMech>();
+    std::vector<int> mask(n_bc, 7);
+    make_mech_boundaries(n_bc, bc_node, mask.data(), bc_val, 0, nullptr, nullptr, nullptr, *dir, *neu);
+    std::function<Point<double>(bool&, int, Point<double>)> source = [](bool& is_solve, int, Point<double>) {
+        is_solve = false;
+        return Point<double>(0, 0, 0);
+    };
+    auto* sol = new std::vector<Point<double>>();
+    auto* K = new CSSD_Matrix<Tensor2Rank3D, Point<double>>();
+    char* dirname = make_tmpdir();
+    if (!dirname) return -1;
+    if (dim == 1) {
+        /* one group per node, as MsFEM_Grid.h:5061-5100 builds the two edge ends */
+        auto* dir1 = new std::vector<DirichletMech1D>(n_bc);
+        for (int i = 0; i < n_bc; i++) {
+            (*dir1)[i].id_vertexes.push_back(bc_node[i]);
+            Point<double> v(bc_val[3 * i], bc_val[3 * i + 1], bc_val[3 * i + 2]);
+            (*dir1)[i].value = [v](Point<bool>& take) {
+                take.x = take.y = take.z = true;
+                return v;
+            };
+        }
+        auto* grid = new FEM::Grid_1D_forMech();
+        set_materials_mech(*grid, n_mat, E, nu);
+        FEM::FEM_1D_forElasticDeformation(false, min_residual, *g, *dir1, *neu, source, dirname, *grid, *sol, *K);
+    } else if (dim == 2) {
+        auto* grid = new FEM::Grid_2D_forMech();
+        set_materials_mech(*grid, n_mat, E, nu);
+        FEM::FEM_2D_forElasticDeformation(false, min_residual, *g, *dir, *neu, source, dirname, *grid, *sol, *K);
+    } else if (dim == 3) {
+        auto* grid = new FEM::Grid_forMech();
+        set_materials_mech(*grid, n_mat, E, nu);
+        FEM::FEM_3D_forElasticDeformation(false, min_residual, *g, *dir, *neu, source, dirname, *grid, *sol, *K);
+    } else {
+        return -2;
+    }
+    std::string cmd = std::string("rm -rf ") + dirname;
+    if (system(cmd.c_str()) != 0) { /* best effort */ }
+    free(dirname);
+    if ((int)sol->size() != n_nodes) return -3;
+    for (int i = 0; i < n_nodes; i++) {
+        solution[3 * i] = (*sol)[i].x;
+        solution[3 * i + 1] = (*sol)[i].y;
+        solution[3 * i + 2] = (*sol)[i].z;
+    }
+    return 0; /* objects leaked on purpose, as in ref_elastic_driver */
 }
 
 }  // extern "C"
