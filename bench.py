@@ -57,9 +57,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="electrostatics", choices=["electrostatics", "elastic"],
+    ap.add_argument("--config", default="electrostatics", choices=["electrostatics", "elastic", "cells"],
                     help="electrostatics: 100^3 scalar (the default workload); elastic: 128^3 heterogeneous "
-                         "elasticity, 2000 spheres E 1:100")
+                         "elasticity, 2000 spheres E 1:100; cells: MsFEM Order1 bases of 16^3 macro cells with "
+                         "{8,12,16,20}^3 fine hexahedra each")
     ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--sample-n", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -429,11 +430,207 @@ def run_ours(args, D):
         print(json.dumps(line))
 
 
+# ---------------------------------------------------------------- MsFEM cell bases (16^3 macro cells)
+
+CELLS_SEED = 3
+
+
+def cells_workload():
+    from multiscalefemsolver3d_b200 import meshgen
+    return meshgen.msfem_cells(n_coarse=16, m_choices=(8, 12, 16, 20), seed=CELLS_SEED)
+
+
+def cells_config(cm, extra=None):
+    c = {"workload": "MsFEM Order1 bases (8 vector bases per cell: 24 edge, 24 face, 8 volume problems) of the "
+                     "16^3 macro cells of the unit cube, fine Kuhn meshes of m^3 hexahedra with m drawn from "
+                     "{8,12,16,20}, 1-3 axis-aligned ellipsoids per cell with E 1:50, nu 0.3",
+         "n_cells": int(cm.n_cells), "n_fine_nodes": int(cm.xyz.shape[0]), "n_fine_tets": int(cm.tets.shape[0]),
+         "cells_per_m": {int(m): int((cm.m == m).sum()) for m in np.unique(cm.m)},
+         "tol": TOL, "solver": "one persistent launch per problem kind: MINRES on the Jacobi-scaled free block, "
+                               "FP32 inner solves with FP64 residual refinement (FP64 fallback per cell)",
+         "l2": "flushed between steps (256 MiB write); the per-cell vectors and matrices exceed L2",
+         "parallelism": "replicas"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def kuhn_blocks(m):
+    """Node-level portrait size of an m^3 Kuhn cube: nodes + 2 * edges."""
+    edges = 3 * m * (m + 1) ** 2 + 3 * m * m * (m + 1) + m ** 3
+    return (m + 1) ** 3 + 2 * edges
+
+
+def run_cells(args, D):
+    import torch
+    from multiscalefemsolver3d_b200 import _lib
+    from multiscalefemsolver3d_b200.cells import FP32_IR, Cells
+
+    torch.cuda.set_device(D.local)
+    dev = torch.device("cuda", D.local)
+    cm = cells_workload()
+    C = Cells(cm)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        C.build_bases(FP32_IR, TOL)
+    D.barrier()
+    torch.cuda.synchronize()
+    ts, reps = [], []
+    with Clocks(D.local) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            rc = C.build_bases(FP32_IR, TOL)
+            if rc != 0:
+                raise RuntimeError(f"cells build rc={rc}")
+            rep = C.report()
+            reps.append(rep)
+            ts.append(sum(rep["ms"].values()))
+    torch.cuda.synchronize()
+    D.barrier()
+    ms = D.max(statistics.mean(ts))
+    rep = reps[-1]
+    # roofline of the volume solve (k_batch_minres<8>): per inner iteration of a cell the
+    # FP32 matrix (36 B values + 4 B column per 3x3 block) once and 10 passes over the
+    # cell's 8 x 3 FP32 Krylov vectors (SpMM in/out and the MINRES recurrences)
+    n_nodes_cell = (cm.m.astype(np.int64) + 1) ** 3
+    blocks_cell = np.array([kuhn_blocks(int(m)) for m in cm.m], dtype=np.int64)
+    per_it = blocks_cell * 40 + 10 * n_nodes_cell * 24 * 4
+    algo = float((rep["inner"].astype(np.int64) * per_it).sum())
+    vol_ms = statistics.mean(r["ms"]["volumes"] for r in reps)
+    ach = algo / (vol_ms * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+    C.close()
+
+    # e2e: create (topology + portraits) + build + bases copied back, host (pinned) buffers
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+    h = [pin(cm.node_off), pin(cm.xyz), pin(cm.tet_off), pin(cm.tets), pin(cm.mat), pin(cm.box), pin(cm.E),
+         pin(cm.nu)]
+    out = torch.empty((cm.xyz.shape[0], 8, 3), dtype=torch.float64).pin_memory()
+    L = _lib.load()
+    P = lambda t: C_.c_void_p(t.data_ptr())  # noqa: E731
+    import ctypes as C_
+
+    def e2e_call():
+        hh = C_.c_void_p()
+        _lib.check(L.msfem_cells_create(cm.n_cells, P(h[0]), P(h[1]), P(h[2]), P(h[3]), P(h[4]), P(h[5]),
+                                        h[6].numel(), P(h[6]), P(h[7]), 0, C_.byref(hh)), "cells_create")
+        try:
+            rc = L.msfem_cells_build_bases(hh, FP32_IR, TOL, 5000, 256)
+            if rc != 0:
+                raise RuntimeError(f"cells build rc={rc}")
+            _lib.check(L.msfem_cells_get_bases(hh, P(out), 0), "cells_get_bases")
+        finally:
+            L.msfem_cells_destroy(hh)
+
+    e2e_ts = []
+    for _ in range(max(1, min(2, args.steps))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_call()
+        e2e_ts.append((time.perf_counter() - t0) * 1e3)
+    e2e_ms = D.max(statistics.mean(e2e_ts))
+    h2d = sum(t.numel() * t.element_size() for t in h)
+    d2h = out.numel() * out.element_size()
+    base = None
+    if D.rank == 0 and D.world == 1 and not args.no_cpu_baseline:
+        base = cells_cpu_baseline(cm)
+    if D.rank == 0:
+        extra = {"ms_stages": {k: statistics.mean(r["ms"][k] for r in reps) for k in rep["ms"]},
+                 "inner_iterations_mean": float(rep["inner"].mean()), "inner_iterations_max": int(rep["inner"].max()),
+                 "refinement_steps_mean": float(rep["outer"].mean()), "rel_residual_max": float(rep["rel"].max()),
+                 "face_rel_residual_max": float(rep["face_rel"].max()), "step_ms_all": ts}
+        line = {"metric": METRIC, "value": ms, "unit": UNIT, "n_gpus": D.world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "fp32-in-f64-ir", "data": "synthetic",
+                "config": cells_config(cm, extra),
+                "e2e": {"value": e2e_ms, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "gpu_launches": 11,
+                "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                             "traffic": None, "kernel": "k_batch_minres<8> (volume problems, persistent)",
+                             "peak_source": f"{peak_kind} hbm_gbs"},
+                "cpu_baseline": base,
+                "clocks": clk.summary()}
+        print(json.dumps(line))
+
+
+def cells_reference_times(cm, ms_sample=(8, 12)):
+    """Seconds of the reference's own cell drivers (FEM_1D/2D/3D_forElasticDeformation, chained as
+    MsFEM_Grid.h:4795-5759 does) for one cell of each sampled m, one thread."""
+    import oracle
+    from oracle import cells as ocells
+    R = oracle.ref()
+    out = {}
+    for m in ms_sample:
+        c = int(np.nonzero(cm.m == m)[0][0])
+        xyz, tets, mat, box = cm.cell(c)
+        t0 = time.perf_counter()
+        ocells.order1_bases(xyz, tets, mat, box, cm.E, cm.nu, solver=R.cell_problem)
+        out[m] = time.perf_counter() - t0
+    return out
+
+
+def cells_extrapolate(cm, t):
+    """Whole-batch CPU time: per-cell times of the sampled m, a power law in the node count
+    fitted through them for the other m, summed over the cells and divided over the cores
+    (the reference runs one cell per OpenMP thread, MsFEM_Grid.h:4800)."""
+    ms = sorted(t)
+    N = {m: (m + 1) ** 3 for m in set(cm.m.tolist()) | set(ms)}
+    a, b = ms[0], ms[-1]
+    expo = np.log(t[b] / t[a]) / np.log(N[b] / N[a]) if b != a else 4.0 / 3.0
+    per = {m: t[a] * (N[m] / N[a]) ** expo for m in N}
+    per.update(t)
+    cores = os.cpu_count() or 1
+    total = sum(per[int(m)] for m in cm.m) / cores
+    return total, per, expo, cores
+
+
+def cells_cpu_baseline(cm):
+    import oracle
+    if not oracle.ref_available():
+        return None
+    t = cells_reference_times(cm)
+    total, per, expo, cores = cells_extrapolate(cm, t)
+    return {"value": total * 1e3, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"reference cell drivers chained for one cell each of m={sorted(t)} (one thread): "
+                      + ", ".join(f"m={m}: {t[m]:.1f} s" for m in sorted(t))
+                      + f"; other m by N^{expo:.2f}; summed over the {cm.n_cells} cells and divided over {cores} cores"}
+
+
+def run_reference_cells(args, D):
+    if D.rank != 0:
+        return
+    import oracle
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libfemref.so not built"}))
+        return
+    cm = cells_workload()
+    for _ in range(args.warmup):
+        cells_reference_times(cm, ms_sample=(8,))
+    samples = [cells_reference_times(cm) for _ in range(args.steps)]
+    t = {m: statistics.mean(s[m] for s in samples) for m in samples[0]}
+    total, per, expo, cores = cells_extrapolate(cm, t)
+    v = total * 1e3
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": cells_config(cm, extra={"solver": "reference FEM_1D/2D/3D_forElasticDeformation (SSOR-PCG "
+                                                        "restart loops, MIN_RESIDUAL 1e-15 / 5e-15)",
+                                              "sample_seconds_per_cell": t}),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
+                             "sample": f"one cell each of m={sorted(t)}, mean of {args.steps} runs; other m by "
+                                       f"N^{expo:.2f}; summed over cells / {cores} cores"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     D = Dist(args.gpus)
     try:
-        if args.impl == "reference":
+        if args.config == "cells":
+            (run_reference_cells if args.impl == "reference" else run_cells)(args, D)
+        elif args.impl == "reference":
             run_reference(args, D)
         else:
             run_ours(args, D)

@@ -276,6 +276,47 @@ int msfem_cells_report(msfem_cells_t c, int32_t* inner_iterations, int32_t* oute
                        double* face_rel_residual, double* ms);
 void msfem_cells_destroy(msfem_cells_t c);
 
+
+/* ---------------------------------------------------------------------------------------
+ * Two-level preconditioner with the MsFEM coarse space (no counterpart in the reference, which
+ * solves the MsFEM macro problem instead, MsFEM/MsFEM.h:572-1010): the Order1 cell bases of a
+ * decomposition of the fine mesh into macro cells define the prolongation P (coarse DOF
+ * (vertex V, component a) -> the a-component of the cell bases of V; nodes shared by several
+ * cells take the mean); the coarse operator is P^T K P with K the textbook (SPD) orientation of
+ * the fine element blocks, inverted densely in FP64; M^-1 = diag(A)^-1 + P A_c^-1 P^T.
+ * ------------------------------------------------------------------------------------- */
+
+typedef struct msfem_coarse* msfem_coarse_t;
+
+/* fine: an assembled elasticity system with its Dirichlet rows applied; cells: the macro cells
+ * (msfem_cells_create + msfem_cells_build_bases) whose fine meshes together are the fine mesh,
+ * cell_node_global[b] = fine node of cell node b (concatenated cell numbering);
+ * cell_vertex[8c+v] = coarse vertex id (0..n_coarse_vertices-1) of vertex v of cell c;
+ * cell_color[c]: cells of one colour share no coarse vertex (fixes the summation order);
+ * fixed_dofs: the fine Dirichlet DOFs (3*node + component).  Host arrays. */
+int msfem_coarse_create(msfem_system_t fine, msfem_cells_t cells, const int32_t* cell_node_global,
+                        int n_coarse_vertices, const int32_t* cell_vertex, const int32_t* cell_color, int n_fixed,
+                        const int32_t* fixed_dofs, msfem_coarse_t* out);
+
+/* n_coarse_dofs: free coarse DOFs; ms_setup: device ms of the setup (prolongation, coarse
+ * Galerkin matrix, FP64 inverse). */
+int msfem_coarse_info(msfem_coarse_t c, int* n_coarse_dofs, double* ms_setup);
+
+/* Inspection: the dense coarse matrix (n_coarse_dofs^2, row-major, before inversion) and the
+ * coarse DOF of each (cell, vertex, component), -1 when dropped ([n_cells][8][3]). */
+int msfem_coarse_matrix(msfem_coarse_t c, double* A, int32_t* coarse_dof);
+
+/* y = M^-1 r on the Jacobi-scaled system (FP32 host arrays of n_rows): y = r + P^ A_c^-1 P^^T r
+ * with P^ = D^1/2 P. */
+int msfem_coarse_apply(msfem_coarse_t c, const float* r, float* y);
+
+/* Solves the fine system from its current X: FP64 iterative refinement (r = F - A X, X += d)
+ * around preconditioned MINRES in FP32 on the Jacobi-scaled matrix with M^-1 above, to
+ * ||F - A X|| <= tol ||F||.  iterations: inner MINRES steps in total; outer: refinement steps. */
+int msfem_solve_twolevel(msfem_system_t fine, msfem_coarse_t c, int maxiter, double tol, double* rel_residual,
+                         int* iterations, int* outer);
+void msfem_coarse_destroy(msfem_coarse_t c);
+
 #ifdef __cplusplus
 }
 #endif

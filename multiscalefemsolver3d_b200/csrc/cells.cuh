@@ -1,0 +1,52 @@
+// Handles of the batched cell problems (cells.cu), shared with the two-level
+// preconditioner (twolevel.cu), which reads the cells' meshes and bases.
+#pragma once
+
+#include <vector>
+
+#include "batch.cuh"
+
+namespace msfem {
+
+struct BatchHandle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    BatchSys b;
+    DBuf<double> xyz, lame, x;
+    int n_mat = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    float ms = 0.f;
+    ~BatchHandle()
+    {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+struct CellsHandle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int n_cells = 0, n_mat = 0;
+    int64_t n_nodes = 0, n_tets = 0;
+    std::vector<int64_t> h_node_off, h_tet_off;
+    DBuf<int64_t> node_off, tet_off;
+    DBuf<double> xyz, box, lame;
+    DBuf<int32_t> mat, mask, vert, fidx, fcell_node;
+    BatchSys faces, vols;
+    DBuf<double> fxyz, prof, fx, bx;
+    int cap = 0;
+    DBuf<int32_t> edge_nodes, edge_len, seg_tri;
+    DBuf<int> flag;
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    float ms[4] = {0, 0, 0, 0};
+    ~CellsHandle()
+    {
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+
+}  // namespace msfem

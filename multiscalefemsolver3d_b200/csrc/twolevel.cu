@@ -1,0 +1,1152 @@
+// Two-level preconditioner with the MsFEM coarse space, and the preconditioned
+// MINRES around it (FP32 inner solves inside FP64 iterative refinement).
+//
+// Coarse space.  The Order1 bases of the macro cells (cells.cu; MsFEM/MsFEM_Grid.h:
+// 4795-5759) give the prolongation P: coarse DOF (vertex V, component a) -> fine
+// DOF (node g, a) with value psi_V^a(g), the a-component of the cell basis of V
+// (the reference uses the components this way in FiniteElement_forMech_Poly_Order1::
+// SolveLocalMatrix, MsFEM_Grid.h:3837-3975).  A fine node on a face, edge or corner
+// shared by several cells takes the mean of the cells' values; P is zero on the
+// Dirichlet DOFs of the fine problem, and coarse DOFs whose vertex carries a fine
+// Dirichlet DOF are dropped.
+//
+// Coarse operator.  The reference's element blocks make the fine matrix A
+// symmetric but indefinite; a Galerkin operator P^T A P is indefinite too and
+// cannot define an SPD preconditioner (MINRES needs one).  The coarse operator is
+// therefore the Galerkin product of the textbook (SPD) orientation of the same
+// element blocks, A_c = P^T K P with K[I][J][a][b] = V (lambda gI_a gJ_b +
+// mu gJ_a gI_b + mu delta_ab gI.gJ) -- the reference's blocks transposed --
+// assembled cell by cell from the fine tetrahedra (24 x 24 per cell, summed in
+// element order), then into a dense matrix colour by colour (cells of one colour
+// share no vertex, so every entry receives its cell terms in a fixed order).
+// A_c is inverted in FP64 by the block sweep operator with Cholesky-factored
+// 64 x 64 pivots, and applied in FP32 as a dense matrix-vector product.
+//
+// Preconditioner (on the Jacobi-scaled system S A S, S = D^-1/2):
+//   M^-1 = I + P^ A_c^-1 P^^T,  P^ = S^-1 P,
+// i.e. diag(A)^-1 + P A_c^-1 P^T in the original unknowns: SPD.
+//
+// Preconditioned MINRES (Paige & Saunders 1975, in the form of their SYMMLQ/MINRES
+// report with a preconditioner): per iteration one SpMV, one preconditioner
+// application (restriction per cell -> coarse gather -> dense GEMV -> prolongation)
+// and two inner products, in six kernels captured as a CUDA graph.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <memory>
+#include <new>
+#include <numeric>
+
+#include "cells.cuh"
+#include "devutil.cuh"
+#include "element.cuh"
+#include "internal.cuh"
+#include "spmv.cuh"
+
+namespace msfem {
+namespace {
+
+constexpr int kSB = 64;            // sweep pivot block
+constexpr int kCoarseThreads = 576;  // one thread per entry of a 24 x 24 cell matrix
+constexpr int kTetBatch = 8;
+
+struct TlState {
+    double alfa, beta, oldb, dbar, epsln, oldeps, phibar, cs, sn, phi, delta, gamma, denom, beta1, tol, bb;
+    int iter, maxiter, done, applied;
+    unsigned int ticket[4];
+};
+
+inline unsigned gridn(int64_t n, int t = 256)
+{
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + t - 1) / t, 148 * 32));
+}
+
+// ---- setup kernels
+
+__global__ void k_batch_cell(int n_cells, const int64_t* __restrict__ node_off, int32_t* __restrict__ bcell)
+{
+    const int c = blockIdx.x;
+    for (int64_t b = node_off[c] + threadIdx.x; b < node_off[c + 1]; b += blockDim.x) bcell[b] = c;
+}
+
+__global__ void k_inc_heads(int64_t n, const int32_t* __restrict__ key, int32_t* __restrict__ inc_ptr, int n_fine, int* bad)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int k = key[i];
+        if (k < 0 || k >= n_fine) {
+            atomicExch(bad, 1);
+            continue;
+        }
+        if (i == 0 || key[i - 1] != k) inc_ptr[k] = (int32_t)i;
+        if (i == n - 1) inc_ptr[n_fine] = (int32_t)n;
+    }
+}
+
+// every fine node must appear: inc_ptr[g] was preset to -1
+__global__ void k_inc_fill(int n_fine, int32_t* __restrict__ inc_ptr, int* bad)
+{
+    // a node that no cell holds is an error; fill from the right so that gaps would be visible
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n_fine; g += gridDim.x * blockDim.x)
+        if (inc_ptr[g] < 0) atomicExch(bad, 2);
+}
+
+// psi_cell[b][v][a]: mean over the cells holding the fine node of b of their basis of the
+// coarse vertex cell_vertex[c][v]; zero on fine Dirichlet DOFs and dropped coarse DOFs
+__global__ void k_psi_cell(int64_t n_batch, const int32_t* __restrict__ bcell, const int32_t* __restrict__ cng,
+                           const int32_t* __restrict__ inc_ptr, const int32_t* __restrict__ inc_b,
+                           const int32_t* __restrict__ cell_vertex, const int32_t* __restrict__ cdof,
+                           const uint8_t* __restrict__ fixed3, const double* __restrict__ bases,
+                           double* __restrict__ psi)
+{
+    for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < n_batch; b += (int64_t)gridDim.x * blockDim.x) {
+        const int c = bcell[b];
+        const int g = cng[b];
+        const int e0 = inc_ptr[g], e1 = inc_ptr[g + 1];
+        const double inv = 1.0 / (double)(e1 - e0);
+        for (int v = 0; v < 8; v++) {
+            const int V = cell_vertex[8 * c + v];
+            double acc[3] = {0, 0, 0};
+            for (int e = e0; e < e1; e++) {
+                const int b2 = inc_b[e];
+                const int c2 = bcell[b2];
+                for (int v2 = 0; v2 < 8; v2++)
+                    if (cell_vertex[8 * c2 + v2] == V) {
+                        for (int a = 0; a < 3; a++) acc[a] += bases[24 * (int64_t)b2 + 3 * v2 + a];
+                        break;
+                    }
+            }
+            for (int a = 0; a < 3; a++) {
+                const bool keep = !fixed3[3 * (int64_t)g + a] && cdof[24 * c + 3 * v + a] >= 0;
+                psi[24 * b + 3 * v + a] = keep ? acc[a] * inv : 0.0;
+            }
+        }
+    }
+}
+
+// per fine node: owner cell (the cell of its first incidence) and the scaled prolongation row
+__global__ void k_psi_hat(int n_fine, const int32_t* __restrict__ inc_ptr, const int32_t* __restrict__ inc_b,
+                          const int32_t* __restrict__ bcell, const double* __restrict__ psi,
+                          const double* __restrict__ dscale, int32_t* __restrict__ owner, float* __restrict__ psi_hat)
+{
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n_fine; g += gridDim.x * blockDim.x) {
+        const int b = inc_b[inc_ptr[g]];
+        owner[g] = bcell[b];
+        for (int j = 0; j < 24; j++) {
+            const int a = j % 3;
+            psi_hat[24 * (int64_t)g + j] = (float)(psi[24 * (int64_t)b + j] / dscale[3 * (int64_t)g + a]);
+        }
+    }
+}
+
+// cell coarse matrices K_c = sum_e P_e^T K_e P_e (textbook element blocks), 576 threads per cell
+__global__ void __launch_bounds__(kCoarseThreads) k_coarse_cells(const int64_t* __restrict__ elem_off,
+                                                                  const int32_t* __restrict__ elems,
+                                                                  const int32_t* __restrict__ emat,
+                                                                  const double* __restrict__ xyz,
+                                                                  const double* __restrict__ lame, int n_mat,
+                                                                  const double* __restrict__ psi, double* __restrict__ Kc,
+                                                                  int* bad)
+{
+    __shared__ double s_g[kTetBatch][4][3];
+    __shared__ double s_c[kTetBatch][3];  // meas, lambda, mu
+    __shared__ double s_psi[kTetBatch][4][24];
+    __shared__ double s_T[kTetBatch][12][24];
+    const int c = blockIdx.x, tid = threadIdx.x;
+    const int p = tid / 24, q = tid % 24;  // entry (v a) x (w b)
+    const int pa = p % 3;
+    double acc = 0.0;
+    const int64_t t0 = elem_off[c], t1 = elem_off[c + 1];
+    for (int64_t base = t0; base < t1; base += kTetBatch) {
+        const int nb = (int)min((int64_t)kTetBatch, t1 - base);
+        __syncthreads();
+        if (tid < nb) {
+            const int64_t e = base + tid;
+            int v[4];
+            for (int k = 0; k < 4; k++) v[k] = elems[4 * e + k];
+            TetGeom G;
+            tet_geometry(xyz, v, G);
+            for (int k = 0; k < 4; k++)
+                for (int a = 0; a < 3; a++) s_g[tid][k][a] = G.g[k][a];
+            const int m = emat ? emat[e] : 0;
+            if (m < 0 || m >= n_mat) atomicExch(bad, 1);
+            const int mm = (m < 0 || m >= n_mat) ? 0 : m;
+            s_c[tid][0] = G.vol;
+            s_c[tid][1] = lame[2 * mm];
+            s_c[tid][2] = lame[2 * mm + 1];
+        }
+        for (int i = tid; i < nb * 96; i += blockDim.x) {
+            const int t = i / 96, r = i % 96, k = r / 24, j = r % 24;
+            const int64_t node = elems[4 * (base + t) + k];
+            s_psi[t][k][j] = psi[24 * node + j];
+        }
+        __syncthreads();
+        // T[t][I a][w b] = sum_J K_e[I][J][a][b] psi[J][w b]
+        for (int i = tid; i < nb * 288; i += blockDim.x) {
+            const int t = i / 288, r = i % 288, Ia = r / 24, wb = r % 24;
+            const int I = Ia / 3, a = Ia % 3, b = wb % 3;
+            const double meas = s_c[t][0], lam = s_c[t][1], mu = s_c[t][2];
+            double sum = 0.0;
+            for (int J = 0; J < 4; J++) {
+                const double* gi = s_g[t][I];
+                const double* gj = s_g[t][J];
+                double k = lam * gi[a] * gj[b] + mu * gj[a] * gi[b];
+                if (a == b) k += mu * (gi[0] * gj[0] + gi[1] * gj[1] + gi[2] * gj[2]);
+                sum += meas * k * s_psi[t][J][wb];
+            }
+            s_T[t][Ia][wb] = sum;
+        }
+        __syncthreads();
+        for (int t = 0; t < nb; t++)
+            for (int I = 0; I < 4; I++) acc += s_psi[t][I][p] * s_T[t][3 * I + pa][q];
+    }
+    Kc[576 * (int64_t)c + tid] = acc;
+}
+
+// add the cell matrices of one colour into the dense coarse matrix
+__global__ void k_coarse_scatter(int n_sel, const int32_t* __restrict__ cells, const double* __restrict__ Kc,
+                                 const int32_t* __restrict__ cdof, double* __restrict__ A, int64_t ld)
+{
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < (int64_t)n_sel * 576;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int c = cells[t / 576];
+        const int e = (int)(t % 576), p = e / 24, q = e % 24;
+        const int dp = cdof[24 * c + p], dq = cdof[24 * c + q];
+        if (dp >= 0 && dq >= 0) A[dp * ld + dq] += Kc[576 * (int64_t)c + e];
+    }
+}
+
+__global__ void k_sym_pad(double* __restrict__ A, int64_t ld, int n, int n_pad)
+{
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < (int64_t)n_pad * n_pad;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(t / n_pad), j = (int)(t % n_pad);
+        if (i >= n || j >= n) {
+            A[i * ld + j] = (i == j) ? 1.0 : 0.0;
+        } else if (i < j) {
+            const double m = 0.5 * (A[i * ld + j] + A[j * ld + i]);
+            A[i * ld + j] = m;
+            A[j * ld + i] = m;
+        }
+    }
+}
+
+// ---- block sweep: A <- A with pivot block K swept; after all blocks A = -A0^-1
+
+// Pinv = A[K][K]^-1 via Cholesky in shared memory (one CTA)
+__global__ void __launch_bounds__(256) k_sweep_pivot(const double* __restrict__ A, int64_t ld, int k0,
+                                                     double* __restrict__ Pinv, int* bad)
+{
+    extern __shared__ double psm[];
+    double(*L)[kSB + 1] = reinterpret_cast<double(*)[kSB + 1]>(psm);
+    double(*W)[kSB + 1] = reinterpret_cast<double(*)[kSB + 1]>(psm + kSB * (kSB + 1));
+    const int tid = threadIdx.x;
+    for (int i = tid; i < kSB * kSB; i += blockDim.x) L[i / kSB][i % kSB] = A[(int64_t)(k0 + i / kSB) * ld + k0 + i % kSB];
+    __syncthreads();
+    // right-looking Cholesky, lower triangle
+    for (int j = 0; j < kSB; j++) {
+        if (tid == 0) {
+            const double d = L[j][j];
+            if (!(d > 0.0)) atomicExch(bad, 1);
+            L[j][j] = d > 0.0 ? sqrt(d) : 1.0;
+        }
+        __syncthreads();
+        const double djj = L[j][j];
+        for (int i = j + 1 + tid; i < kSB; i += blockDim.x) L[i][j] /= djj;
+        __syncthreads();
+        for (int t = tid; t < (kSB - j - 1) * (kSB - j - 1); t += blockDim.x) {
+            const int i = j + 1 + t / (kSB - j - 1), c = j + 1 + t % (kSB - j - 1);
+            if (c <= i) L[i][c] -= L[i][j] * L[c][j];
+        }
+        __syncthreads();
+    }
+    // W = L^-1 (lower), column by column: one thread per column
+    if (tid < kSB) {
+        const int c = tid;
+        for (int i = 0; i < kSB; i++) {
+            if (i < c) {
+                W[i][c] = 0.0;
+                continue;
+            }
+            double s = (i == c) ? 1.0 : 0.0;
+            for (int k = c; k < i; k++) s -= L[i][k] * W[k][c];
+            W[i][c] = s / L[i][i];
+        }
+    }
+    __syncthreads();
+    // Pinv = W^T W
+    for (int t = tid; t < kSB * kSB; t += blockDim.x) {
+        const int i = t / kSB, j = t % kSB;
+        double s = 0.0;
+        for (int k = max(i, j); k < kSB; k++) s += W[k][i] * W[k][j];
+        Pinv[t] = s;
+    }
+}
+
+// Bp = A[:, K] (old panel), Cp = Bp * Pinv
+__global__ void __launch_bounds__(256) k_sweep_panel(const double* __restrict__ A, int64_t ld, int n, int k0,
+                                                     const double* __restrict__ Pinv, double* __restrict__ Bp,
+                                                     double* __restrict__ Cp)
+{
+    __shared__ double P[kSB][kSB];
+    for (int t = threadIdx.x; t < kSB * kSB; t += blockDim.x) P[t / kSB][t % kSB] = Pinv[t];
+    __syncthreads();
+    const int row = blockIdx.x * 4 + threadIdx.x / 64;  // 4 rows per CTA, 64 threads per row
+    const int j = threadIdx.x % 64;
+    if (row >= n) return;
+    const double* a = A + (int64_t)row * ld + k0;
+    const double bj = a[j];
+    Bp[(int64_t)row * kSB + j] = bj;
+    __syncwarp();
+    double s = 0.0;
+    for (int k = 0; k < kSB; k++) s += a[k] * P[k][j];
+    Cp[(int64_t)row * kSB + j] = s;
+}
+
+// tile (I, J) of 64 x 64: A_IJ -= C_I B_J^T off the pivot block row/column; the pivot
+// row/column take C, the pivot block -Pinv
+__global__ void __launch_bounds__(256) k_sweep_update(double* __restrict__ A, int64_t ld, int kb,
+                                                      const double* __restrict__ Pinv, const double* __restrict__ Bp,
+                                                      const double* __restrict__ Cp)
+{
+    extern __shared__ double sm[];
+    double* Cs = sm;                 // [64][65]
+    double* Bs = sm + kSB * (kSB + 1);  // [64][65]
+    const int I = blockIdx.y, J = blockIdx.x;
+    const int tid = threadIdx.x;
+    const int64_t i0 = (int64_t)I * kSB, j0 = (int64_t)J * kSB;
+    if (I == kb && J == kb) {
+        for (int t = tid; t < kSB * kSB; t += blockDim.x) A[(i0 + t / kSB) * ld + j0 + t % kSB] = -Pinv[t];
+        return;
+    }
+    if (J == kb) {  // column panel: C_I
+        for (int t = tid; t < kSB * kSB; t += blockDim.x) A[(i0 + t / kSB) * ld + j0 + t % kSB] = Cp[(i0 + t / kSB) * kSB + t % kSB];
+        return;
+    }
+    if (I == kb) {  // row panel: C_J^T
+        for (int t = tid; t < kSB * kSB; t += blockDim.x) A[(i0 + t / kSB) * ld + j0 + t % kSB] = Cp[(j0 + t % kSB) * kSB + t / kSB];
+        return;
+    }
+    for (int t = tid; t < kSB * kSB; t += blockDim.x) {
+        const int r = t / kSB, k = t % kSB;
+        Cs[r * (kSB + 1) + k] = Cp[(i0 + r) * kSB + k];
+        Bs[r * (kSB + 1) + k] = Bp[(j0 + r) * kSB + k];
+    }
+    __syncthreads();
+    const int tr = tid / 16, tc = tid % 16;  // 4 x 4 outputs per thread
+    double acc[4][4] = {};
+    for (int k = 0; k < kSB; k++) {
+        double cr[4], bc[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            cr[u] = Cs[(tr + 16 * u) * (kSB + 1) + k];
+            bc[u] = Bs[(tc + 16 * u) * (kSB + 1) + k];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+#pragma unroll
+            for (int w = 0; w < 4; w++) acc[u][w] += cr[u] * bc[w];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+        for (int w = 0; w < 4; w++) A[(i0 + tr + 16 * u) * ld + j0 + tc + 16 * w] -= acc[u][w];
+}
+
+// C = -A (the swept matrix) in FP32, rows of length ld with zero columns past n
+__global__ void k_neg_to32(const double* __restrict__ A, int64_t ld, int n, float* __restrict__ C)
+{
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < (int64_t)n * ld; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = t / ld, j = t % ld;
+        C[t] = j < n ? (float)(-A[i * ld + j]) : 0.0f;
+    }
+}
+
+// ---- preconditioner application kernels (FP32)
+
+// per cell: restriction partials over its owned nodes, cpart[c][v a] = sum psi_hat[g][v a] r[g a];
+// with `lanczos`, r is first formed as r_new = z - (alfa / beta) r2 and written over `out`
+__global__ void __launch_bounds__(128) k_tl_restrict(const int32_t* __restrict__ own_ptr, const int32_t* __restrict__ own,
+                                                     const float* __restrict__ psi_hat, const float* __restrict__ z,
+                                                     const float* __restrict__ r2, float* __restrict__ out,
+                                                     float* __restrict__ cpart, const TlState* S, int lanczos)
+{
+    if (S->done) return;
+    __shared__ float red[4][24];
+    const int c = blockIdx.x;
+    const float coef = lanczos ? (float)(S->alfa / S->beta) : 0.0f;
+    float acc[24];
+#pragma unroll
+    for (int j = 0; j < 24; j++) acc[j] = 0.0f;
+    for (int k = own_ptr[c] + threadIdx.x; k < own_ptr[c + 1]; k += blockDim.x) {
+        const int64_t g = own[k];
+        float rv[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            float r = z[3 * g + a];
+            if (lanczos) {
+                r -= coef * r2[3 * g + a];
+                out[3 * g + a] = r;
+            }
+            rv[a] = r;
+        }
+        const float* ph = psi_hat + 24 * g;
+#pragma unroll
+        for (int j = 0; j < 24; j++) acc[j] += ph[j] * rv[j % 3];
+    }
+    // block reduction of 24 values (fixed order)
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < 24; j++) {
+        float v = acc[j];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[warp][j] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 24) {
+        float v = 0.0f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += red[w][threadIdx.x];
+        cpart[24 * c + threadIdx.x] = v;
+    }
+}
+
+// coarse residual: rc[d] = sum of the cell partials of coarse DOF d (fixed order)
+__global__ void k_tl_gather(int n_cf, const int32_t* __restrict__ dptr, const int32_t* __restrict__ dent,
+                            const float* __restrict__ cpart, float* __restrict__ rc, const TlState* S)
+{
+    if (S->done) return;
+    for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < n_cf; d += gridDim.x * blockDim.x) {
+        float s = 0.0f;
+        for (int e = dptr[d]; e < dptr[d + 1]; e++) s += cpart[dent[e]];
+        rc[d] = s;
+    }
+}
+
+// ec = Cinv rc, one warp per row; rows of length ld (a multiple of 64, zero padded, so every
+// float4 load is 16-byte aligned), x zero beyond n
+__global__ void __launch_bounds__(256) k_tl_gemv(int n, int ld, const float* __restrict__ C, const float* __restrict__ x,
+                                                 float* __restrict__ y, const TlState* S)
+{
+    if (S->done) return;
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += nw) {
+        const float* c = C + (int64_t)row * ld;
+        float s = 0.0f;
+        for (int k = lane * 4; k < ld; k += 128) {
+            const float4 a = __ldcs(reinterpret_cast<const float4*>(c + k));
+            const float4 b = __ldg(reinterpret_cast<const float4*>(x + k));
+            s += a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w;
+        }
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) y[row] = s;
+    }
+}
+
+// y = r + P^ ec; bb = (r, y); the last block updates the Givens recurrence.  init: first
+// application (beta1 = sqrt(bb)).
+__global__ void __launch_bounds__(kVecThreads) k_tl_prolong(int n_fine, const int32_t* __restrict__ owner,
+                                                           const int32_t* __restrict__ cdof,
+                                                           const float* __restrict__ psi_hat,
+                                                           const float* __restrict__ ec, const float* __restrict__ r,
+                                                           float* __restrict__ y, TlState* S, double* __restrict__ partial,
+                                                           int init)
+{
+    if (S->done) return;
+    __shared__ double sh[32];
+    double acc[1] = {0.0};
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n_fine; g += (int64_t)gridDim.x * blockDim.x) {
+        const int c = owner[g];
+        const int32_t* cd = cdof + 24 * c;
+        const float* ph = psi_hat + 24 * g;
+        float z[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (int j = 0; j < 24; j++) {
+            const int d = cd[j];
+            if (d >= 0) z[j % 3] += ph[j] * ec[d];
+        }
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            const float ra = r[3 * g + a];
+            const float ya = ra + z[a];
+            y[3 * g + a] = ya;
+            acc[0] += (double)ra * (double)ya;
+        }
+    }
+    block_sum<1>(acc, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = acc[0];
+    if (arrive_last(&S->ticket[0])) {
+        double t[1];
+        reduce_partials<1>(partial, gridDim.x, 0, t, sh);
+        if (threadIdx.x == 0) {
+            const double bb = t[0];
+            if (init) {
+                const double b1 = bb > 0.0 ? sqrt(bb) : 0.0;
+                S->beta1 = b1;
+                S->beta = b1;
+                S->oldb = 0.0;
+                S->phibar = b1;
+                S->dbar = 0.0;
+                S->epsln = 0.0;
+                S->cs = -1.0;
+                S->sn = 0.0;
+                S->iter = 0;
+                S->applied = -1;
+                S->done = (b1 > 0.0) ? 0 : 1;
+            } else {
+                const double beta = bb > 0.0 ? sqrt(bb) : 0.0;
+                S->oldb = S->beta;
+                S->beta = beta;
+                S->oldeps = S->epsln;
+                const double delta = S->cs * S->dbar + S->sn * S->alfa;
+                const double gbar = S->sn * S->dbar - S->cs * S->alfa;
+                S->epsln = S->sn * beta;
+                S->dbar = -S->cs * beta;
+                double gamma = sqrt(gbar * gbar + beta * beta);
+                if (!(gamma > 1e-300)) gamma = 1e-300;
+                S->cs = gbar / gamma;
+                S->sn = beta / gamma;
+                S->phi = S->cs * S->phibar;
+                S->phibar = S->sn * S->phibar;
+                S->delta = delta;
+                S->gamma = gamma;
+                S->denom = 1.0 / gamma;
+                S->iter += 1;
+                if (!(bb == bb)) S->done = 3;
+                else if (fabs(S->phibar) <= S->tol * S->beta1 || !(beta > 0.0)) S->done = 1;
+                else if (S->iter >= S->maxiter) S->done = 2;
+            }
+            S->ticket[0] = 0;
+        }
+    }
+}
+
+// v = y / beta; z = (S A S) y / beta - (beta / oldb) r1 (after the first step); alfa = (v, z)
+__global__ void __launch_bounds__(256) k_tl_spmv(SellView<float> A, const float* __restrict__ y, float* __restrict__ v,
+                                                 float* __restrict__ z, const float* __restrict__ r1, TlState* S,
+                                                 double* __restrict__ partial)
+{
+    if (S->done) return;
+    __shared__ double sh[32];
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    const float inv = (float)(1.0 / S->beta);
+    const float coef = S->iter > 0 ? (float)(S->beta / S->oldb) : 0.0f;
+    double acc[1] = {0.0};
+    for (int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; warp < A.n_slices; warp += nw) {
+        float yv[3];
+        sell_row_block<float>(A, warp, lane, y, yv);
+        const int brow = warp * kSlice + lane;
+        if (brow < A.n_brows)
+            for (int c = 0; c < 3; c++) {
+                const int64_t i = 3 * (int64_t)brow + c;
+                const float vi = y[i] * inv;
+                const float zi = yv[c] * inv - coef * r1[i];
+                v[i] = vi;
+                z[i] = zi;
+                acc[0] += (double)vi * (double)zi;
+            }
+    }
+    block_sum<1>(acc, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = acc[0];
+    if (arrive_last(&S->ticket[1])) {
+        double t[1];
+        reduce_partials<1>(partial, gridDim.x, 0, t, sh);
+        if (threadIdx.x == 0) {
+            S->alfa = t[0];
+            S->ticket[1] = 0;
+        }
+    }
+}
+
+// w_new = (v - oldeps w1 - delta w2) / gamma (over w1); x += phi w_new.  Runs on the step that
+// set the stopping flag (its update), not after.
+__global__ void __launch_bounds__(kVecThreads) k_tl_update(int n, const float* __restrict__ v, float* __restrict__ w1,
+                                                          const float* __restrict__ w2, float* __restrict__ x,
+                                                          const TlState* S)
+{
+    if (S->done && S->applied == S->iter) return;
+    if (S->done == 3) return;
+    const float oe = (float)S->oldeps, de = (float)S->delta, dn = (float)S->denom, ph = (float)S->phi;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float w = (v[i] - oe * w1[i] - de * w2[i]) * dn;
+        w1[i] = w;
+        x[i] += ph * w;
+    }
+}
+
+__global__ void k_tl_applied(TlState* S)
+{
+    if (S->done) S->applied = S->iter;
+}
+
+// rhs of the inner solve: b = S r / ||S r|| (FP32), and the copies r1 = r2 = b, x = w1 = w2 = 0
+__global__ void __launch_bounds__(kVecThreads) k_tl_norm(int n, const double* __restrict__ r, const double* __restrict__ s,
+                                                        TlState* S, double* __restrict__ partial)
+{
+    __shared__ double sh[32];
+    double acc[1] = {0.0};
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double t = s[i] * r[i];
+        acc[0] += t * t;
+    }
+    block_sum<1>(acc, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = acc[0];
+    if (arrive_last(&S->ticket[2])) {
+        double t[1];
+        reduce_partials<1>(partial, gridDim.x, 0, t, sh);
+        if (threadIdx.x == 0) {
+            S->bb = t[0];
+            S->ticket[2] = 0;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kVecThreads) k_tl_rhs(int n, const double* __restrict__ r, const double* __restrict__ s,
+                                                       const TlState* S, float* __restrict__ r1, float* __restrict__ r2,
+                                                       float* __restrict__ x, float* __restrict__ w1, float* __restrict__ w2)
+{
+    const double inv = S->bb > 0.0 ? 1.0 / sqrt(S->bb) : 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float b = (float)(s[i] * r[i] * inv);
+        r1[i] = b;
+        r2[i] = b;
+        x[i] = 0.0f;
+        w1[i] = 0.0f;
+        w2[i] = 0.0f;
+    }
+}
+
+// X += ||S r|| S x32
+__global__ void __launch_bounds__(kVecThreads) k_tl_correct(int n, double* __restrict__ X, const float* __restrict__ x,
+                                                           const double* __restrict__ s, const TlState* S)
+{
+    const double sc = sqrt(S->bb);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        X[i] += sc * s[i] * (double)x[i];
+}
+
+}  // namespace
+
+struct CoarseHandle {
+    System* fine = nullptr;
+    CellsHandle* cells = nullptr;
+    int n_cells = 0, n_cv = 0, n_cf = 0, n_pad = 0;
+    int n_fine = 0;
+    DBuf<int32_t> cdof;              // [n_cells][8][3] free coarse DOF or -1
+    DBuf<int32_t> owner;             // [n_fine] owner cell
+    DBuf<int32_t> own_ptr, own;      // owned fine nodes per cell
+    DBuf<float> psi_hat;             // [n_fine][24]
+    DBuf<int32_t> dptr, dent;        // coarse DOF -> cell partial entries
+    DBuf<float> Cinv;                // [n_cf][n_cf]
+    DBuf<double> Ac;                 // dense coarse matrix (kept for inspection), n_cf x n_cf
+    DBuf<float> cpart, rc, ec;
+    DBuf<float> vec;                 // 8 fine vectors
+    DBuf<double> r64, partial;
+    DBuf<TlState> st;
+    TlState* h_st = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    float ms_setup = 0.f;
+    ~CoarseHandle()
+    {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (h_st) cudaFreeHost(h_st);
+    }
+};
+
+namespace {
+
+int coarse_build(CoarseHandle& C, System& F, CellsHandle& Ce, const int32_t* h_cng, int n_cv, const int32_t* h_cvert,
+                 const int32_t* h_color, int n_fixed, const int32_t* h_fixed)
+{
+    cudaStream_t st = F.stream;
+    MSFEM_TRY(prepare_sell(F));
+    C.fine = &F;
+    C.cells = &Ce;
+    C.n_cells = Ce.n_cells;
+    C.n_cv = n_cv;
+    C.n_fine = F.n_nodes;
+    const int64_t nb = Ce.n_nodes;  // batch (cell-local) nodes
+    cudaEvent_t e0, e1;
+    MSFEM_CK(cudaEventCreate(&e0));
+    MSFEM_CK(cudaEventCreate(&e1));
+    MSFEM_CK(cudaEventRecord(e0, st));
+    // fine Dirichlet flags
+    std::vector<uint8_t> fixed3(3 * (size_t)F.n_nodes, 0);
+    for (int i = 0; i < n_fixed; i++) {
+        if (h_fixed[i] < 0 || h_fixed[i] >= 3 * F.n_nodes) {
+            set_error("msfem_coarse_create: Dirichlet DOF %d out of range", h_fixed[i]);
+            return MSFEM_ERR_ARGUMENT;
+        }
+        fixed3[h_fixed[i]] = 1;
+    }
+    for (int64_t b = 0; b < nb; b++)
+        if (h_cng[b] < 0 || h_cng[b] >= F.n_nodes) {
+            set_error("msfem_coarse_create: cell node %lld maps to fine node %d (out of range)", (long long)b, h_cng[b]);
+            return MSFEM_ERR_ARGUMENT;
+        }
+    // coarse DOFs: (V, a) is dropped when the fine node at the vertex has a Dirichlet a-component
+    std::vector<int32_t> vert(8 * (size_t)C.n_cells);
+    MSFEM_CK(cudaMemcpyAsync(vert.data(), Ce.vert.p, sizeof(int32_t) * vert.size(), cudaMemcpyDeviceToHost, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    std::vector<int8_t> vfix(3 * (size_t)n_cv, -1);
+    for (int c = 0; c < C.n_cells; c++)
+        for (int v = 0; v < 8; v++) {
+            const int V = h_cvert[8 * c + v];
+            if (V < 0 || V >= n_cv) {
+                set_error("msfem_coarse_create: coarse vertex id %d out of range", V);
+                return MSFEM_ERR_ARGUMENT;
+            }
+            const int g = h_cng[vert[8 * c + v]];
+            for (int a = 0; a < 3; a++) vfix[3 * V + a] = fixed3[3 * (size_t)g + a] ? 1 : 0;
+        }
+    std::vector<int32_t> dof_of(3 * (size_t)n_cv, -1);
+    int n_cf = 0;
+    for (int d = 0; d < 3 * n_cv; d++)
+        if (vfix[d] == 0) dof_of[d] = n_cf++;
+    C.n_cf = n_cf;
+    C.n_pad = (n_cf + kSB - 1) / kSB * kSB;
+    std::vector<int32_t> cdof(24 * (size_t)C.n_cells);
+    for (int c = 0; c < C.n_cells; c++)
+        for (int v = 0; v < 8; v++)
+            for (int a = 0; a < 3; a++) cdof[24 * c + 3 * v + a] = dof_of[3 * h_cvert[8 * c + v] + a];
+    // coarse DOF -> (cell, slot) entries in cell order
+    std::vector<int32_t> dcnt(n_cf + 1, 0);
+    for (size_t k = 0; k < cdof.size(); k++)
+        if (cdof[k] >= 0) dcnt[cdof[k] + 1]++;
+    for (int d = 0; d < n_cf; d++) dcnt[d + 1] += dcnt[d];
+    std::vector<int32_t> dent(dcnt[n_cf]);
+    {
+        std::vector<int32_t> fill(dcnt.begin(), dcnt.end() - 1);
+        for (size_t k = 0; k < cdof.size(); k++)
+            if (cdof[k] >= 0) dent[fill[cdof[k]]++] = (int32_t)k;
+    }
+    MSFEM_TRY(C.cdof.alloc(cdof.size()));
+    MSFEM_CK(cudaMemcpyAsync(C.cdof.p, cdof.data(), sizeof(int32_t) * cdof.size(), cudaMemcpyHostToDevice, st));
+    MSFEM_TRY(C.dptr.alloc(n_cf + 1));
+    MSFEM_TRY(C.dent.alloc(std::max<size_t>(1, dent.size())));
+    MSFEM_CK(cudaMemcpyAsync(C.dptr.p, dcnt.data(), sizeof(int32_t) * (n_cf + 1), cudaMemcpyHostToDevice, st));
+    if (!dent.empty()) MSFEM_CK(cudaMemcpyAsync(C.dent.p, dent.data(), sizeof(int32_t) * dent.size(), cudaMemcpyHostToDevice, st));
+
+    // device copies of the maps
+    DBuf<int32_t> cng, cvert, bcell, inc_ptr, keys2, vals, vals2;
+    DBuf<uint8_t> dfix;
+    MSFEM_TRY(cng.alloc(nb));
+    MSFEM_TRY(cvert.alloc(8 * (size_t)C.n_cells));
+    MSFEM_TRY(dfix.alloc(fixed3.size()));
+    MSFEM_CK(cudaMemcpyAsync(cng.p, h_cng, sizeof(int32_t) * nb, cudaMemcpyHostToDevice, st));
+    MSFEM_CK(cudaMemcpyAsync(cvert.p, h_cvert, sizeof(int32_t) * 8 * C.n_cells, cudaMemcpyHostToDevice, st));
+    MSFEM_CK(cudaMemcpyAsync(dfix.p, fixed3.data(), fixed3.size(), cudaMemcpyHostToDevice, st));
+    MSFEM_TRY(bcell.alloc(nb));
+    k_batch_cell<<<C.n_cells, 256, 0, st>>>(C.n_cells, Ce.node_off.p, bcell.p);
+    // incidence fine node -> batch nodes (stable: batch order)
+    MSFEM_TRY(vals.alloc(nb));
+    MSFEM_TRY(keys2.alloc(nb));
+    MSFEM_TRY(vals2.alloc(nb));
+    {
+        std::vector<int32_t> iota(nb);
+        std::iota(iota.begin(), iota.end(), 0);
+        MSFEM_CK(cudaMemcpyAsync(vals.p, iota.data(), sizeof(int32_t) * nb, cudaMemcpyHostToDevice, st));
+        size_t tb = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, tb, cng.p, keys2.p, vals.p, vals2.p, (int)nb, 0, 32, st);
+        DBuf<unsigned char> tmp;
+        MSFEM_TRY(tmp.alloc(std::max<size_t>(tb, 1)));
+        MSFEM_CK(cub::DeviceRadixSort::SortPairs(tmp.p, tb, cng.p, keys2.p, vals.p, vals2.p, (int)nb, 0, 32, st));
+        MSFEM_CK(cudaStreamSynchronize(st));
+    }
+    DBuf<int> flag;
+    MSFEM_TRY(flag.alloc(1));
+    MSFEM_CK(cudaMemsetAsync(flag.p, 0, sizeof(int), st));
+    MSFEM_TRY(inc_ptr.alloc((size_t)F.n_nodes + 1));
+    MSFEM_CK(cudaMemsetAsync(inc_ptr.p, 0xff, sizeof(int32_t) * ((size_t)F.n_nodes + 1), st));
+    k_inc_heads<<<gridn(nb), 256, 0, st>>>(nb, keys2.p, inc_ptr.p, F.n_nodes, flag.p);
+    k_inc_fill<<<gridn(F.n_nodes), 256, 0, st>>>(F.n_nodes, inc_ptr.p, flag.p);
+    int bad = 0;
+    MSFEM_CK(cudaMemcpyAsync(&bad, flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    if (bad) {
+        set_error("msfem_coarse_create: %s", bad == 2 ? "a fine node belongs to no cell" : "bad cell node map");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    // prolongation values
+    DBuf<double> psi;
+    MSFEM_TRY(psi.alloc(24 * (size_t)nb));
+    k_psi_cell<<<gridn(nb), 256, 0, st>>>(nb, bcell.p, cng.p, inc_ptr.p, vals2.p, cvert.p, C.cdof.p, dfix.p, Ce.bx.p, psi.p);
+    MSFEM_TRY(C.owner.alloc(F.n_nodes));
+    MSFEM_TRY(C.psi_hat.alloc(24 * (size_t)F.n_nodes));
+    k_psi_hat<<<gridn(F.n_nodes), 256, 0, st>>>(F.n_nodes, inc_ptr.p, vals2.p, bcell.p, psi.p, F.dscale.p, C.owner.p,
+                                                 C.psi_hat.p);
+    MSFEM_CK(cudaGetLastError());
+    // owned fine nodes per cell (sorted by owner, then node)
+    {
+        std::vector<int32_t> own(F.n_nodes);
+        MSFEM_CK(cudaMemcpyAsync(own.data(), C.owner.p, sizeof(int32_t) * F.n_nodes, cudaMemcpyDeviceToHost, st));
+        MSFEM_CK(cudaStreamSynchronize(st));
+        std::vector<int32_t> ptr(C.n_cells + 1, 0), lst(F.n_nodes);
+        for (int g = 0; g < F.n_nodes; g++) ptr[own[g] + 1]++;
+        for (int c = 0; c < C.n_cells; c++) ptr[c + 1] += ptr[c];
+        std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
+        for (int g = 0; g < F.n_nodes; g++) lst[fill[own[g]]++] = g;
+        MSFEM_TRY(C.own_ptr.alloc(C.n_cells + 1));
+        MSFEM_TRY(C.own.alloc(F.n_nodes));
+        MSFEM_CK(cudaMemcpyAsync(C.own_ptr.p, ptr.data(), sizeof(int32_t) * (C.n_cells + 1), cudaMemcpyHostToDevice, st));
+        MSFEM_CK(cudaMemcpyAsync(C.own.p, lst.data(), sizeof(int32_t) * F.n_nodes, cudaMemcpyHostToDevice, st));
+    }
+    // cell coarse matrices and the dense coarse matrix, colour by colour
+    DBuf<double> Kc;
+    MSFEM_TRY(Kc.alloc(576 * (size_t)C.n_cells));
+    MSFEM_CK(cudaMemsetAsync(flag.p, 0, sizeof(int), st));
+    k_coarse_cells<<<C.n_cells, kCoarseThreads, 0, st>>>(Ce.vols.elem_off.p, Ce.vols.elems.p, Ce.mat.p, Ce.xyz.p,
+                                                         Ce.lame.p, Ce.n_mat, psi.p, Kc.p, flag.p);
+    const int64_t ld = C.n_pad;
+    MSFEM_TRY(C.Ac.alloc((size_t)ld * ld));
+    MSFEM_CK(cudaMemsetAsync(C.Ac.p, 0, sizeof(double) * ld * ld, st));
+    {
+        int max_col = 0;
+        for (int c = 0; c < C.n_cells; c++) max_col = std::max(max_col, h_color[c]);
+        std::vector<int32_t> sel;
+        DBuf<int32_t> dsel;
+        MSFEM_TRY(dsel.alloc(C.n_cells));
+        for (int col = 0; col <= max_col; col++) {
+            sel.clear();
+            for (int c = 0; c < C.n_cells; c++)
+                if (h_color[c] == col) sel.push_back(c);
+            if (sel.empty()) continue;
+            MSFEM_CK(cudaMemcpyAsync(dsel.p, sel.data(), sizeof(int32_t) * sel.size(), cudaMemcpyHostToDevice, st));
+            k_coarse_scatter<<<gridn((int64_t)sel.size() * 576), 256, 0, st>>>((int)sel.size(), dsel.p, Kc.p, C.cdof.p,
+                                                                               C.Ac.p, ld);
+            MSFEM_CK(cudaStreamSynchronize(st));  // dsel is reused by the next colour
+        }
+    }
+    k_sym_pad<<<gridn((int64_t)ld * ld), 256, 0, st>>>(C.Ac.p, ld, C.n_cf, C.n_pad);
+    MSFEM_CK(cudaGetLastError());
+    MSFEM_CK(cudaMemcpyAsync(&bad, flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    if (bad) {
+        set_error("msfem_coarse_create: material id out of range");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    // invert: sweep every 64-block pivot (A becomes -A^-1), working on a copy
+    DBuf<double> W, Pinv, Bp, Cp;
+    MSFEM_TRY(W.alloc((size_t)ld * ld));
+    MSFEM_CK(cudaMemcpyAsync(W.p, C.Ac.p, sizeof(double) * ld * ld, cudaMemcpyDeviceToDevice, st));
+    MSFEM_TRY(Pinv.alloc(kSB * kSB));
+    MSFEM_TRY(Bp.alloc((size_t)ld * kSB));
+    MSFEM_TRY(Cp.alloc((size_t)ld * kSB));
+    const int nblk = C.n_pad / kSB;
+    const size_t smem = 2 * kSB * (kSB + 1) * sizeof(double);
+    MSFEM_CK(cudaFuncSetAttribute(k_sweep_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    MSFEM_CK(cudaFuncSetAttribute(k_sweep_pivot, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    MSFEM_CK(cudaMemsetAsync(flag.p, 0, sizeof(int), st));
+    for (int kb = 0; kb < nblk; kb++) {
+        k_sweep_pivot<<<1, 256, smem, st>>>(W.p, ld, kb * kSB, Pinv.p, flag.p);
+        k_sweep_panel<<<(C.n_pad + 3) / 4, 256, 0, st>>>(W.p, ld, C.n_pad, kb * kSB, Pinv.p, Bp.p, Cp.p);
+        k_sweep_update<<<dim3(nblk, nblk), 256, smem, st>>>(W.p, ld, kb, Pinv.p, Bp.p, Cp.p);
+    }
+    MSFEM_CK(cudaGetLastError());
+    MSFEM_CK(cudaMemcpyAsync(&bad, flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    if (bad) {
+        set_error("msfem_coarse_create: the coarse matrix is not positive definite");
+        return MSFEM_ERR_NUMERIC;
+    }
+    MSFEM_TRY(C.Cinv.alloc((size_t)C.n_cf * ld));
+    k_neg_to32<<<gridn((int64_t)C.n_cf * ld), 256, 0, st>>>(W.p, ld, C.n_cf, C.Cinv.p);
+    // solver storage
+    const int n = F.n_rows;
+    MSFEM_TRY(C.cpart.alloc(24 * (size_t)C.n_cells));
+    MSFEM_TRY(C.rc.alloc(C.n_pad));
+    MSFEM_TRY(C.ec.alloc(C.n_pad));
+    MSFEM_CK(cudaMemsetAsync(C.rc.p, 0, sizeof(float) * C.n_pad, st));  // the GEMV reads the zero tail
+    MSFEM_TRY(C.vec.alloc(8 * (size_t)n));
+    MSFEM_TRY(C.r64.alloc(n));
+    MSFEM_TRY(C.partial.alloc(4096));
+    MSFEM_TRY(C.st.alloc(1));
+    MSFEM_CK(cudaMemsetAsync(C.st.p, 0, sizeof(TlState), st));
+    MSFEM_CK(cudaMallocHost(&C.h_st, sizeof(TlState)));
+    MSFEM_CK(cudaEventRecord(e1, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    MSFEM_CK(cudaEventElapsedTime(&C.ms_setup, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return MSFEM_OK;
+}
+
+// y = M^-1 r (FP32, scaled space) into y; init: also sets beta1 etc.
+void precondition(CoarseHandle& C, const float* r, float* y, int init, cudaStream_t st, unsigned gprol)
+{
+    k_tl_restrict<<<C.n_cells, 128, 0, st>>>(C.own_ptr.p, C.own.p, C.psi_hat.p, r, nullptr, nullptr, C.cpart.p, C.st.p, 0);
+    k_tl_gather<<<gridn(C.n_cf), 256, 0, st>>>(C.n_cf, C.dptr.p, C.dent.p, C.cpart.p, C.rc.p, C.st.p);
+    k_tl_gemv<<<gridn((int64_t)C.n_cf * 32), 256, 0, st>>>(C.n_cf, C.n_pad, C.Cinv.p, C.rc.p, C.ec.p, C.st.p);
+    k_tl_prolong<<<gprol, kVecThreads, 0, st>>>(C.n_fine, C.owner.p, C.cdof.p, C.psi_hat.p, C.ec.p, r, y, C.st.p,
+                                                C.partial.p, init);
+}
+
+int read_st(CoarseHandle& C, cudaStream_t st)
+{
+    MSFEM_CK(cudaMemcpyAsync(C.h_st, C.st.p, sizeof(TlState), cudaMemcpyDeviceToHost, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    return 0;
+}
+
+// preconditioned MINRES (FP32) on S A S y = b, b = S r / ||S r||, from y = 0, to |phibar| <= tau beta1
+int inner_solve(CoarseHandle& C, int maxiter, double tau, int* iters)
+{
+    System& F = *C.fine;
+    cudaStream_t st = F.stream;
+    const int n = F.n_rows;
+    float* X = C.vec.p;
+    float* V = X + n;
+    float* Z = V + n;
+    float* Y = Z + n;
+    float* R[2] = {Y + n, Y + 2 * (size_t)n};
+    float* Wb[2] = {Y + 3 * (size_t)n, Y + 4 * (size_t)n};
+    TlState* S = C.st.p;
+    const unsigned gvec = kReduceBlocks;
+    k_tl_norm<<<gvec, kVecThreads, 0, st>>>(n, C.r64.p, F.dscale.p, S, C.partial.p);
+    k_tl_rhs<<<gvec, kVecThreads, 0, st>>>(n, C.r64.p, F.dscale.p, S, R[0], R[1], X, Wb[0], Wb[1]);
+    // limits, then y = M^-1 b (r2 = R[1])
+    MSFEM_TRY(read_st(C, st));
+    TlState h = *C.h_st;
+    h.tol = tau;
+    h.maxiter = maxiter;
+    h.done = 0;
+    h.applied = -1;
+    h.iter = 0;
+    for (auto& t : h.ticket) t = 0;
+    *C.h_st = h;
+    MSFEM_CK(cudaMemcpyAsync(S, C.h_st, sizeof(TlState), cudaMemcpyHostToDevice, st));
+    const unsigned gprol = kReduceBlocks;
+    precondition(C, R[1], Y, 1, st, gprol);
+    const SellView<float> A = sell_view<float>(F);
+    const unsigned gsp = spmv_grid_of((const void*)k_tl_spmv, F);
+    // two iterations: r1/r2 and w1/w2 swap each step
+    auto two = [&]() {
+        for (int p = 0; p < 2; p++) {
+            float* r1 = R[p];
+            float* r2 = R[1 - p];
+            float* w1 = Wb[p];
+            float* w2 = Wb[1 - p];
+            k_tl_spmv<<<gsp, 256, 0, st>>>(A, Y, V, Z, r1, S, C.partial.p + 2048);
+            // r2_new = z - (alfa/beta) r2 over r1's buffer, and its restriction partials
+            k_tl_restrict<<<C.n_cells, 128, 0, st>>>(C.own_ptr.p, C.own.p, C.psi_hat.p, Z, r2, r1, C.cpart.p, S, 1);
+            k_tl_gather<<<gridn(C.n_cf), 256, 0, st>>>(C.n_cf, C.dptr.p, C.dent.p, C.cpart.p, C.rc.p, S);
+            k_tl_gemv<<<gridn((int64_t)C.n_cf * 32), 256, 0, st>>>(C.n_cf, C.n_pad, C.Cinv.p, C.rc.p, C.ec.p, S);
+            k_tl_prolong<<<gprol, kVecThreads, 0, st>>>(C.n_fine, C.owner.p, C.cdof.p, C.psi_hat.p, C.ec.p, r1, Y, S,
+                                                        C.partial.p, 0);
+            k_tl_update<<<gvec, kVecThreads, 0, st>>>(n, V, w1, w2, X, S);
+            k_tl_applied<<<1, 1, 0, st>>>(S);
+        }
+    };
+    if (!C.graph) {
+        cudaGraph_t gr;
+        MSFEM_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        for (int k = 0; k < 8; k++) two();  // 16 iterations per replay
+        cudaError_t e = cudaStreamEndCapture(st, &gr);
+        if (e != cudaSuccess) {
+            set_error("two-level MINRES graph capture failed: %s", cudaGetErrorString(e));
+            return MSFEM_ERR_CUDA;
+        }
+        e = cudaGraphInstantiate(&C.graph, gr, 0);
+        cudaGraphDestroy(gr);
+        if (e != cudaSuccess) {
+            set_error("two-level MINRES graph instantiate failed: %s", cudaGetErrorString(e));
+            return MSFEM_ERR_CUDA;
+        }
+    }
+    int rounds = 0;
+    for (;;) {
+        MSFEM_TRY(read_st(C, st));
+        if (C.h_st->done) break;
+        if (16 * rounds > maxiter + 32) break;
+        for (int k = 0; k < 4; k++) MSFEM_CK(cudaGraphLaunch(C.graph, st));
+        rounds += 4;
+        F.total_launches += 4 * 16 * 7;
+    }
+    *iters = C.h_st->iter;
+    return C.h_st->done == 3 ? MSFEM_ERR_NUMERIC : MSFEM_OK;
+}
+
+int solve_twolevel(CoarseHandle& C, int maxiter, double tol, double* rel, int* iters, int* outer)
+{
+    System& F = *C.fine;
+    cudaStream_t st = F.stream;
+    MSFEM_TRY(prepare_sell(F));
+    MSFEM_TRY(F.kstate.alloc(1));
+    const int n = F.n_rows;
+    DBuf<double>& rr = F.sc_f64[1];
+    MSFEM_TRY(rr.alloc(2));
+    cudaEvent_t e0, e1;
+    MSFEM_CK(cudaEventCreate(&e0));
+    MSFEM_CK(cudaEventCreate(&e1));
+    MSFEM_CK(cudaEventRecord(e0, st));
+    // ||F||^2
+    MSFEM_TRY(residual64(F, F.X.p, F.F.p, C.r64.p, rr.p));  // also warms the path
+    double ff = 0.0;
+    {
+        // (F, F) through a zero vector: r = F - A 0
+        DBuf<double> zero;
+        MSFEM_TRY(zero.alloc(n));
+        MSFEM_CK(cudaMemsetAsync(zero.p, 0, sizeof(double) * n, st));
+        MSFEM_TRY(residual64(F, zero.p, F.F.p, C.r64.p, rr.p + 1));
+        MSFEM_CK(cudaMemcpyAsync(&ff, rr.p + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+        MSFEM_CK(cudaStreamSynchronize(st));
+    }
+    int total = 0, k = 0, rc = MSFEM_OK;
+    double r2 = 0.0, prev = -1.0;
+    for (k = 0; k < 40; k++) {
+        MSFEM_TRY(residual64(F, F.X.p, F.F.p, C.r64.p, rr.p));
+        MSFEM_CK(cudaMemcpyAsync(&r2, rr.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+        MSFEM_CK(cudaStreamSynchronize(st));
+        if (!(r2 == r2)) {
+            set_error("two-level solve: the residual became NaN");
+            return MSFEM_ERR_NUMERIC;
+        }
+        if (r2 <= tol * tol * ff || r2 == 0.0 || total >= maxiter) break;
+        if (prev >= 0.0 && r2 > 0.25 * prev) break;  // refinement no longer contracts
+        prev = r2;
+        const double need = tol * std::sqrt(ff / r2);
+        const double tau = std::max(1e-5, std::min(0.5, 0.3 * need));
+        int it = 0;
+        rc = inner_solve(C, maxiter - total, tau, &it);
+        total += it;
+        if (std::getenv("MSFEM_TRACE"))
+            std::fprintf(stderr, "[msfem] two-level refine %d: rel %.3e tau %.1e inner %d\n", k, std::sqrt(r2 / ff), tau, it);
+        if (rc == MSFEM_ERR_NUMERIC) break;
+        k_tl_correct<<<kReduceBlocks, kVecThreads, 0, st>>>(n, F.X.p, C.vec.p, F.dscale.p, C.st.p);
+    }
+    MSFEM_CK(cudaEventRecord(e1, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    MSFEM_CK(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    F.stats.ms_solve = ms;
+    F.stats.iterations = total;
+    F.stats.outer_iterations = k;
+    *rel = ff > 0 ? std::sqrt(r2 / ff) : std::sqrt(r2);
+    F.stats.rel_residual = *rel;
+    *iters = total;
+    *outer = k;
+    if (rc == MSFEM_ERR_NUMERIC) {
+        set_error("two-level solve: the inner MINRES broke down");
+        return MSFEM_ERR_NUMERIC;
+    }
+    return *rel <= tol * (1.0 + 1e-6) ? MSFEM_OK : MSFEM_NOT_CONVERGED;
+}
+
+}  // namespace
+}  // namespace msfem
+
+struct msfem_coarse : msfem::CoarseHandle {};
+struct msfem_cells;
+struct msfem_system;
+
+extern "C" {
+
+int msfem_coarse_create(msfem_system_t fine, msfem_cells_t cells, const int32_t* cell_node_global,
+                        int n_coarse_vertices, const int32_t* cell_vertex, const int32_t* cell_color, int n_fixed,
+                        const int32_t* fixed_dofs, msfem_coarse_t* out)
+{
+    using namespace msfem;
+    if (!out || !fine || !cells || !cell_node_global || n_coarse_vertices <= 0 || !cell_vertex || !cell_color ||
+        n_fixed < 0 || (n_fixed > 0 && !fixed_dofs)) {
+        set_error("msfem_coarse_create: bad arguments");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    System& F = *reinterpret_cast<System*>(fine);
+    CellsHandle& Ce = *reinterpret_cast<CellsHandle*>(cells);
+    if (F.kind != MSFEM_ELASTIC) {
+        set_error("msfem_coarse_create: the fine system must be an elasticity system");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    MSFEM_CK(cudaSetDevice(F.device));
+    *out = nullptr;
+    std::unique_ptr<msfem_coarse> h(new (std::nothrow) msfem_coarse());
+    if (!h) {
+        set_error("out of host memory");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    MSFEM_TRY(coarse_build(*h, F, Ce, cell_node_global, n_coarse_vertices, cell_vertex, cell_color, n_fixed, fixed_dofs));
+    *out = h.release();
+    return MSFEM_OK;
+}
+
+int msfem_coarse_info(msfem_coarse_t c, int* n_coarse_dofs, double* ms_setup)
+{
+    using namespace msfem;
+    if (!c) {
+        set_error("null handle");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    if (n_coarse_dofs) *n_coarse_dofs = c->n_cf;
+    if (ms_setup) *ms_setup = c->ms_setup;
+    return MSFEM_OK;
+}
+
+int msfem_coarse_matrix(msfem_coarse_t c, double* A, int32_t* coarse_dof)
+{
+    using namespace msfem;
+    if (!c) {
+        set_error("null handle");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    cudaStream_t st = c->fine->stream;
+    if (A)
+        MSFEM_CK(cudaMemcpy2DAsync(A, sizeof(double) * c->n_cf, c->Ac.p, sizeof(double) * c->n_pad,
+                                   sizeof(double) * c->n_cf, c->n_cf, cudaMemcpyDeviceToHost, st));
+    if (coarse_dof)
+        MSFEM_CK(cudaMemcpyAsync(coarse_dof, c->cdof.p, sizeof(int32_t) * 24 * c->n_cells, cudaMemcpyDeviceToHost, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    return MSFEM_OK;
+}
+
+int msfem_coarse_apply(msfem_coarse_t c, const float* r, float* y)
+{
+    using namespace msfem;
+    if (!c || !r || !y) {
+        set_error("msfem_coarse_apply: bad arguments");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    System& F = *c->fine;
+    cudaStream_t st = F.stream;
+    const int n = F.n_rows;
+    float* dr = c->vec.p + 5 * (size_t)n;  // an inner-solve work vector
+    float* dy = c->vec.p + 6 * (size_t)n;
+    MSFEM_CK(cudaMemcpyAsync(dr, r, sizeof(float) * n, cudaMemcpyHostToDevice, st));
+    MSFEM_CK(cudaMemsetAsync(c->st.p, 0, sizeof(TlState), st));
+    precondition(*c, dr, dy, 1, st, kReduceBlocks);
+    MSFEM_CK(cudaGetLastError());
+    MSFEM_CK(cudaMemcpyAsync(y, dy, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    return MSFEM_OK;
+}
+
+int msfem_solve_twolevel(msfem_system_t fine, msfem_coarse_t c, int maxiter, double tol, double* rel_residual,
+                         int* iterations, int* outer)
+{
+    using namespace msfem;
+    if (!fine || !c || maxiter <= 0 || !(tol > 0.0) || reinterpret_cast<System*>(fine) != c->fine) {
+        set_error("msfem_solve_twolevel: bad arguments (the coarse handle must belong to this system)");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    MSFEM_CK(cudaSetDevice(c->fine->device));
+    double rel = 0.0;
+    int it = 0, out = 0;
+    const int rc = solve_twolevel(*c, maxiter, tol, &rel, &it, &out);
+    if (rel_residual) *rel_residual = rel;
+    if (iterations) *iterations = it;
+    if (outer) *outer = out;
+    return rc;
+}
+
+void msfem_coarse_destroy(msfem_coarse_t c)
+{
+    if (!c) return;
+    cudaSetDevice(c->fine->device);
+    cudaStreamSynchronize(c->fine->stream);
+    delete c;
+}
+
+}  // extern "C"

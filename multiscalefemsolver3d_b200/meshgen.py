@@ -270,3 +270,57 @@ def msfem_cells(n_coarse: int = 16, m_choices=(8, 12, 16, 20), seed: int = 3, ma
                       tet_off=np.array(toff, dtype=np.int64), tets=np.concatenate(tetss).astype(np.int32),
                       mat=np.concatenate(mats), box=np.array(boxes), E=np.array([1.0, contrast]),
                       nu=np.array([nu, nu]), m=ms[sel].astype(np.int32))
+
+
+@dataclass
+class CubeCells:
+    """A structured cube mesh (kuhn_cube(n)) cut into nc^3 macro cells of H = n/nc hexahedra
+    per edge, each with its own copy of the fine mesh (cell-local numbering)."""
+    cells: CellMeshes
+    cell_node_global: np.ndarray   # int32 [cells' nodes]: fine node of each cell node
+    cell_vertex: np.ndarray        # int32 [n_cells, 8]: coarse vertex of each cell corner
+    cell_color: np.ndarray         # int32 [n_cells]: parity colour, cells of a colour share no vertex
+    n_coarse_vertices: int
+
+
+def cube_cells(mesh: Mesh, E, nu, H: int) -> CubeCells:
+    """Cells of H^3 hexahedra over kuhn_cube(n) (n % H == 0); each cell keeps the fine mesh's own
+    tetrahedra (same node order) renumbered cell-locally, so the cells' element blocks are the
+    fine problem's element blocks."""
+    n = mesh.n
+    if n % H:
+        raise ValueError("n must be a multiple of H")
+    nc = n // H
+    i = np.arange(H + 1)
+    lk, lj, li = np.meshgrid(i, i, i, indexing="ij")
+    li, lj, lk = li.ravel(), lj.ravel(), lk.ravel()          # local node (i, j, k), id li + (H+1)(lj + (H+1)lk)
+    hx = np.arange(H)
+    hk, hj, hi = np.meshgrid(hx, hx, hx, indexing="ij")
+    hi, hj, hk = hi.ravel(), hj.ravel(), hk.ravel()          # local hexahedra
+    xyzs, tets, mats, boxes, cng, cvert, color = [], [], [], [], [], [], []
+    noff, toff = [0], [0]
+    for c in range(nc ** 3):
+        ci, cj, ck = c % nc, (c // nc) % nc, c // (nc * nc)
+        g = node_id(n, ci * H + li, cj * H + lj, ck * H + lk)
+        hexes = (ci * H + hi) + n * ((cj * H + hj) + n * (ck * H + hk))
+        te = (hexes[:, None] * 6 + np.arange(6)[None, :]).ravel()
+        loc = np.full(mesh.n_nodes, -1, dtype=np.int64)
+        loc[g] = np.arange(g.size)
+        xyzs.append(mesh.xyz[g])
+        tets.append(loc[mesh.tets[te]])
+        mats.append(mesh.mat[te])
+        h = 1.0 / nc
+        boxes.append([ci * h, (ci + 1) * h, cj * h, (cj + 1) * h, ck * h, (ck + 1) * h])
+        cng.append(g)
+        cvert.append([(ci + (v & 1)) + (nc + 1) * ((cj + ((v >> 1) & 1)) + (nc + 1) * (ck + ((v >> 2) & 1)))
+                      for v in range(8)])
+        color.append((ci & 1) | ((cj & 1) << 1) | ((ck & 1) << 2))
+        noff.append(noff[-1] + g.size)
+        toff.append(toff[-1] + te.size)
+    cm = CellMeshes(node_off=np.array(noff, dtype=np.int64), xyz=np.concatenate(xyzs),
+                    tet_off=np.array(toff, dtype=np.int64), tets=np.concatenate(tets).astype(np.int32),
+                    mat=np.concatenate(mats).astype(np.int32), box=np.array(boxes), E=np.asarray(E, float),
+                    nu=np.asarray(nu, float), m=np.full(nc ** 3, H, dtype=np.int32))
+    return CubeCells(cells=cm, cell_node_global=np.concatenate(cng).astype(np.int32),
+                     cell_vertex=np.array(cvert, dtype=np.int32), cell_color=np.array(color, dtype=np.int32),
+                     n_coarse_vertices=(nc + 1) ** 3)

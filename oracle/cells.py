@@ -65,9 +65,11 @@ def element_block(g, meas, lam, mu):
     return meas * A
 
 
-def assemble(xyz, elems, mat, E, nu):
+def assemble(xyz, elems, mat, E, nu, textbook=False):
     """Global node-blocked matrix (DOF 3*node+c) as scipy CSR; the per-element formula of
-    simplex_gradients / element_block, evaluated for all elements at once."""
+    simplex_gradients / element_block, evaluated for all elements at once.  textbook=True:
+    the textbook orientation K[I][J][a][b] = V (lambda gI_a gJ_b + mu gJ_a gI_b + ...), i.e. the
+    reference's blocks transposed (symmetric positive semi-definite)."""
     import scipy.sparse as sp
     lam, mu = lame(E, nu)
     n = xyz.shape[0]
@@ -83,7 +85,10 @@ def assemble(xyz, elems, mat, E, nu):
     meas = np.sqrt(np.linalg.det(G)) / [1.0, 1.0, 2.0, 6.0][k]
     la, m_ = lam[mat][:, None, None, None, None], mu[mat][:, None, None, None, None]
     gg = np.einsum("eia,eja->eij", g, g)
-    A = la * np.einsum("eja,eib->eijab", g, g) + m_ * np.einsum("eia,ejb->eijab", g, g)
+    if textbook:
+        A = la * np.einsum("eia,ejb->eijab", g, g) + m_ * np.einsum("eja,eib->eijab", g, g)
+    else:
+        A = la * np.einsum("eja,eib->eijab", g, g) + m_ * np.einsum("eia,ejb->eijab", g, g)
     A = A + (mu[mat][:, None, None] * gg)[:, :, :, None, None] * np.eye(3)[None, None, None]
     A *= meas[:, None, None, None, None]
     r = 3 * elems[:, :, None] + np.arange(3)[None, None, :]          # [ne, k1, 3] DOFs
