@@ -311,10 +311,12 @@ int msfem_coarse_matrix(msfem_coarse_t c, double* A, int32_t* coarse_dof);
 int msfem_coarse_apply(msfem_coarse_t c, const float* r, float* y);
 
 /* Solves the fine system from its current X: FP64 iterative refinement (r = F - A X, X += d)
- * around preconditioned MINRES in FP32 on the Jacobi-scaled matrix with M^-1 above, to
- * ||F - A X|| <= tol ||F||.  iterations: inner MINRES steps in total; outer: refinement steps. */
-int msfem_solve_twolevel(msfem_system_t fine, msfem_coarse_t c, int maxiter, double tol, double* rel_residual,
-                         int* iterations, int* outer);
+ * around preconditioned MINRES with M^-1 above, to ||F - A X|| <= tol ||F||.  precision
+ * MSFEM_FP32_IR: FP32 MINRES on the Jacobi-scaled matrix; MSFEM_FP64: FP64 MINRES on the
+ * original matrix (the coarse correction stays FP32 in both).  iterations: inner MINRES steps in
+ * total; outer: refinement steps. */
+int msfem_solve_twolevel(msfem_system_t fine, msfem_coarse_t c, int precision, int maxiter, double tol,
+                         double* rel_residual, int* iterations, int* outer);
 void msfem_coarse_destroy(msfem_coarse_t c);
 
 #ifdef __cplusplus

@@ -365,49 +365,52 @@ __global__ void k_neg_to32(const double* __restrict__ A, int64_t ld, int n, floa
 
 // ---- preconditioner application kernels (FP32)
 
-// per cell: restriction partials over its owned nodes, cpart[c][v a] = sum psi_hat[g][v a] r[g a];
+// per cell: restriction partials over its owned nodes, cpart[c][v a] = sum psi_hat[g][v a] q[g a],
+// q = r (scaled FP32 system) or s r (FP64 in the original unknowns, s = D^-1/2);
 // with `lanczos`, r is first formed as r_new = z - (alfa / beta) r2 and written over `out`
+template <class VT>
 __global__ void __launch_bounds__(128) k_tl_restrict(const int32_t* __restrict__ own_ptr, const int32_t* __restrict__ own,
-                                                     const float* __restrict__ psi_hat, const float* __restrict__ z,
-                                                     const float* __restrict__ r2, float* __restrict__ out,
-                                                     float* __restrict__ cpart, const TlState* S, int lanczos)
+                                                     const float* __restrict__ psi_hat, const VT* __restrict__ z,
+                                                     const VT* __restrict__ r2, VT* __restrict__ out,
+                                                     float* __restrict__ cpart, const double* __restrict__ s,
+                                                     const TlState* S, int lanczos)
 {
     if (S->done) return;
-    __shared__ float red[4][24];
+    __shared__ VT red[4][24];
     const int c = blockIdx.x;
-    const float coef = lanczos ? (float)(S->alfa / S->beta) : 0.0f;
-    float acc[24];
+    const VT coef = lanczos ? (VT)(S->alfa / S->beta) : (VT)0;
+    VT acc[24];
 #pragma unroll
-    for (int j = 0; j < 24; j++) acc[j] = 0.0f;
+    for (int j = 0; j < 24; j++) acc[j] = 0;
     for (int k = own_ptr[c] + threadIdx.x; k < own_ptr[c + 1]; k += blockDim.x) {
         const int64_t g = own[k];
-        float rv[3];
+        VT rv[3];
 #pragma unroll
         for (int a = 0; a < 3; a++) {
-            float r = z[3 * g + a];
+            VT r = z[3 * g + a];
             if (lanczos) {
                 r -= coef * r2[3 * g + a];
                 out[3 * g + a] = r;
             }
-            rv[a] = r;
+            rv[a] = s ? (VT)(s[3 * g + a] * (double)r) : r;
         }
         const float* ph = psi_hat + 24 * g;
 #pragma unroll
-        for (int j = 0; j < 24; j++) acc[j] += ph[j] * rv[j % 3];
+        for (int j = 0; j < 24; j++) acc[j] += (VT)ph[j] * rv[j % 3];
     }
     // block reduction of 24 values (fixed order)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int j = 0; j < 24; j++) {
-        float v = acc[j];
+        VT v = acc[j];
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
         if (lane == 0) red[warp][j] = v;
     }
     __syncthreads();
     if (threadIdx.x < 24) {
-        float v = 0.0f;
+        VT v = 0;
         for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += red[w][threadIdx.x];
-        cpart[24 * c + threadIdx.x] = v;
+        cpart[24 * c + threadIdx.x] = (float)v;
     }
 }
 
@@ -444,14 +447,15 @@ __global__ void __launch_bounds__(256) k_tl_gemv(int n, int ld, const float* __r
     }
 }
 
-// y = r + P^ ec; bb = (r, y); the last block updates the Givens recurrence.  init: first
-// application (beta1 = sqrt(bb)).
+// y = r + P^ ec (scaled FP32 system) or y = s^2 r + s P^ ec (FP64, original unknowns); bb = (r, y);
+// the last block updates the Givens recurrence.  init: first application (beta1 = sqrt(bb)).
+template <class VT>
 __global__ void __launch_bounds__(kVecThreads) k_tl_prolong(int n_fine, const int32_t* __restrict__ owner,
                                                            const int32_t* __restrict__ cdof,
                                                            const float* __restrict__ psi_hat,
-                                                           const float* __restrict__ ec, const float* __restrict__ r,
-                                                           float* __restrict__ y, TlState* S, double* __restrict__ partial,
-                                                           int init)
+                                                           const float* __restrict__ ec, const VT* __restrict__ r,
+                                                           VT* __restrict__ y, const double* __restrict__ s, TlState* S,
+                                                           double* __restrict__ partial, int init)
 {
     if (S->done) return;
     __shared__ double sh[32];
@@ -468,8 +472,14 @@ __global__ void __launch_bounds__(kVecThreads) k_tl_prolong(int n_fine, const in
         }
 #pragma unroll
         for (int a = 0; a < 3; a++) {
-            const float ra = r[3 * g + a];
-            const float ya = ra + z[a];
+            const VT ra = r[3 * g + a];
+            VT ya;
+            if (s) {
+                const double sa = s[3 * g + a];
+                ya = (VT)(sa * sa * (double)ra + sa * (double)z[a]);
+            } else {
+                ya = ra + (VT)z[a];
+            }
             y[3 * g + a] = ya;
             acc[0] += (double)ra * (double)ya;
         }
@@ -523,26 +533,27 @@ __global__ void __launch_bounds__(kVecThreads) k_tl_prolong(int n_fine, const in
 }
 
 // v = y / beta; z = (S A S) y / beta - (beta / oldb) r1 (after the first step); alfa = (v, z)
-__global__ void __launch_bounds__(256) k_tl_spmv(SellView<float> A, const float* __restrict__ y, float* __restrict__ v,
-                                                 float* __restrict__ z, const float* __restrict__ r1, TlState* S,
+template <class VT>
+__global__ void __launch_bounds__(256) k_tl_spmv(SellView<VT> A, const VT* __restrict__ y, VT* __restrict__ v,
+                                                 VT* __restrict__ z, const VT* __restrict__ r1, TlState* S,
                                                  double* __restrict__ partial)
 {
     if (S->done) return;
     __shared__ double sh[32];
     const int lane = threadIdx.x & 31;
     const int nw = (gridDim.x * blockDim.x) >> 5;
-    const float inv = (float)(1.0 / S->beta);
-    const float coef = S->iter > 0 ? (float)(S->beta / S->oldb) : 0.0f;
+    const VT inv = (VT)(1.0 / S->beta);
+    const VT coef = S->iter > 0 ? (VT)(S->beta / S->oldb) : (VT)0;
     double acc[1] = {0.0};
     for (int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; warp < A.n_slices; warp += nw) {
-        float yv[3];
-        sell_row_block<float>(A, warp, lane, y, yv);
+        VT yv[3];
+        sell_row_block<VT>(A, warp, lane, y, yv);
         const int brow = warp * kSlice + lane;
         if (brow < A.n_brows)
             for (int c = 0; c < 3; c++) {
                 const int64_t i = 3 * (int64_t)brow + c;
-                const float vi = y[i] * inv;
-                const float zi = yv[c] * inv - coef * r1[i];
+                const VT vi = y[i] * inv;
+                const VT zi = yv[c] * inv - coef * r1[i];
                 v[i] = vi;
                 z[i] = zi;
                 acc[0] += (double)vi * (double)zi;
@@ -562,15 +573,16 @@ __global__ void __launch_bounds__(256) k_tl_spmv(SellView<float> A, const float*
 
 // w_new = (v - oldeps w1 - delta w2) / gamma (over w1); x += phi w_new.  Runs on the step that
 // set the stopping flag (its update), not after.
-__global__ void __launch_bounds__(kVecThreads) k_tl_update(int n, const float* __restrict__ v, float* __restrict__ w1,
-                                                          const float* __restrict__ w2, float* __restrict__ x,
+template <class VT>
+__global__ void __launch_bounds__(kVecThreads) k_tl_update(int n, const VT* __restrict__ v, VT* __restrict__ w1,
+                                                          const VT* __restrict__ w2, VT* __restrict__ x,
                                                           const TlState* S)
 {
     if (S->done && S->applied == S->iter) return;
     if (S->done == 3) return;
-    const float oe = (float)S->oldeps, de = (float)S->delta, dn = (float)S->denom, ph = (float)S->phi;
+    const VT oe = (VT)S->oldeps, de = (VT)S->delta, dn = (VT)S->denom, ph = (VT)S->phi;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const float w = (v[i] - oe * w1[i] - de * w2[i]) * dn;
+        const VT w = (v[i] - oe * w1[i] - de * w2[i]) * dn;
         w1[i] = w;
         x[i] += ph * w;
     }
@@ -581,14 +593,15 @@ __global__ void k_tl_applied(TlState* S)
     if (S->done) S->applied = S->iter;
 }
 
-// rhs of the inner solve: b = S r / ||S r|| (FP32), and the copies r1 = r2 = b, x = w1 = w2 = 0
+// rhs of the inner solve: b = S r / ||S r|| (scaled FP32 system) or r / ||r|| (FP64), and the
+// copies r1 = r2 = b, x = w1 = w2 = 0
 __global__ void __launch_bounds__(kVecThreads) k_tl_norm(int n, const double* __restrict__ r, const double* __restrict__ s,
                                                         TlState* S, double* __restrict__ partial)
 {
     __shared__ double sh[32];
     double acc[1] = {0.0};
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const double t = s[i] * r[i];
+        const double t = s ? s[i] * r[i] : r[i];
         acc[0] += t * t;
     }
     block_sum<1>(acc, sh);
@@ -603,13 +616,14 @@ __global__ void __launch_bounds__(kVecThreads) k_tl_norm(int n, const double* __
     }
 }
 
+template <class VT>
 __global__ void __launch_bounds__(kVecThreads) k_tl_rhs(int n, const double* __restrict__ r, const double* __restrict__ s,
-                                                       const TlState* S, float* __restrict__ r1, float* __restrict__ r2,
-                                                       float* __restrict__ x, float* __restrict__ w1, float* __restrict__ w2)
+                                                       const TlState* S, VT* __restrict__ r1, VT* __restrict__ r2,
+                                                       VT* __restrict__ x, VT* __restrict__ w1, VT* __restrict__ w2)
 {
     const double inv = S->bb > 0.0 ? 1.0 / sqrt(S->bb) : 0.0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const float b = (float)(s[i] * r[i] * inv);
+        const VT b = (VT)((s ? s[i] * r[i] : r[i]) * inv);
         r1[i] = b;
         r2[i] = b;
         x[i] = 0.0f;
@@ -618,13 +632,14 @@ __global__ void __launch_bounds__(kVecThreads) k_tl_rhs(int n, const double* __r
     }
 }
 
-// X += ||S r|| S x32
-__global__ void __launch_bounds__(kVecThreads) k_tl_correct(int n, double* __restrict__ X, const float* __restrict__ x,
+// X += ||S r|| S x (scaled FP32 system) or ||r|| x (FP64)
+template <class VT>
+__global__ void __launch_bounds__(kVecThreads) k_tl_correct(int n, double* __restrict__ X, const VT* __restrict__ x,
                                                            const double* __restrict__ s, const TlState* S)
 {
     const double sc = sqrt(S->bb);
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        X[i] += sc * s[i] * (double)x[i];
+        X[i] += sc * (s ? s[i] : 1.0) * (double)x[i];
 }
 
 }  // namespace
@@ -642,15 +657,16 @@ struct CoarseHandle {
     DBuf<float> Cinv;                // [n_cf][n_cf]
     DBuf<double> Ac;                 // dense coarse matrix (kept for inspection), n_cf x n_cf
     DBuf<float> cpart, rc, ec;
-    DBuf<float> vec;                 // 8 fine vectors
+    DBuf<double> vec;                // 8 fine vectors (FP64 room; the FP32 solve uses the front half)
     DBuf<double> r64, partial;
     DBuf<TlState> st;
     TlState* h_st = nullptr;
-    cudaGraphExec_t graph = nullptr;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};  // FP32, FP64 iteration graphs
     float ms_setup = 0.f;
     ~CoarseHandle()
     {
-        if (graph) cudaGraphExecDestroy(graph);
+        for (auto g : graph)
+            if (g) cudaGraphExecDestroy(g);
         if (h_st) cudaFreeHost(h_st);
     }
 };
@@ -859,7 +875,7 @@ int coarse_build(CoarseHandle& C, System& F, CellsHandle& Ce, const int32_t* h_c
     MSFEM_TRY(C.rc.alloc(C.n_pad));
     MSFEM_TRY(C.ec.alloc(C.n_pad));
     MSFEM_CK(cudaMemsetAsync(C.rc.p, 0, sizeof(float) * C.n_pad, st));  // the GEMV reads the zero tail
-    MSFEM_TRY(C.vec.alloc(8 * (size_t)n));
+    MSFEM_TRY(C.vec.alloc(8 * (size_t)n));  // doubles: room for the FP64 solve
     MSFEM_TRY(C.r64.alloc(n));
     MSFEM_TRY(C.partial.alloc(4096));
     MSFEM_TRY(C.st.alloc(1));
@@ -873,14 +889,17 @@ int coarse_build(CoarseHandle& C, System& F, CellsHandle& Ce, const int32_t* h_c
     return MSFEM_OK;
 }
 
-// y = M^-1 r (FP32, scaled space) into y; init: also sets beta1 etc.
-void precondition(CoarseHandle& C, const float* r, float* y, int init, cudaStream_t st, unsigned gprol)
+// y = M^-1 r into y (FP32: scaled system; FP64: original unknowns with s = D^-1/2);
+// init: also sets beta1 etc.
+template <class VT>
+void precondition(CoarseHandle& C, const VT* r, VT* y, int init, cudaStream_t st, unsigned gprol, const double* s)
 {
-    k_tl_restrict<<<C.n_cells, 128, 0, st>>>(C.own_ptr.p, C.own.p, C.psi_hat.p, r, nullptr, nullptr, C.cpart.p, C.st.p, 0);
+    k_tl_restrict<VT><<<C.n_cells, 128, 0, st>>>(C.own_ptr.p, C.own.p, C.psi_hat.p, r, nullptr, nullptr, C.cpart.p, s,
+                                                 C.st.p, 0);
     k_tl_gather<<<gridn(C.n_cf), 256, 0, st>>>(C.n_cf, C.dptr.p, C.dent.p, C.cpart.p, C.rc.p, C.st.p);
     k_tl_gemv<<<gridn((int64_t)C.n_cf * 32), 256, 0, st>>>(C.n_cf, C.n_pad, C.Cinv.p, C.rc.p, C.ec.p, C.st.p);
-    k_tl_prolong<<<gprol, kVecThreads, 0, st>>>(C.n_fine, C.owner.p, C.cdof.p, C.psi_hat.p, C.ec.p, r, y, C.st.p,
-                                                C.partial.p, init);
+    k_tl_prolong<VT><<<gprol, kVecThreads, 0, st>>>(C.n_fine, C.owner.p, C.cdof.p, C.psi_hat.p, C.ec.p, r, y, s, C.st.p,
+                                                    C.partial.p, init);
 }
 
 int read_st(CoarseHandle& C, cudaStream_t st)
@@ -890,23 +909,26 @@ int read_st(CoarseHandle& C, cudaStream_t st)
     return 0;
 }
 
-// preconditioned MINRES (FP32) on S A S y = b, b = S r / ||S r||, from y = 0, to |phibar| <= tau beta1
+// preconditioned MINRES from 0 on b = S r / ||S r|| (FP32, Jacobi-scaled matrix) or b = r / ||r||
+// (FP64, original matrix), to |phibar| <= tau beta1
+template <class VT>
 int inner_solve(CoarseHandle& C, int maxiter, double tau, int* iters)
 {
     System& F = *C.fine;
     cudaStream_t st = F.stream;
     const int n = F.n_rows;
-    float* X = C.vec.p;
-    float* V = X + n;
-    float* Z = V + n;
-    float* Y = Z + n;
-    float* R[2] = {Y + n, Y + 2 * (size_t)n};
-    float* Wb[2] = {Y + 3 * (size_t)n, Y + 4 * (size_t)n};
+    constexpr bool f32 = sizeof(VT) == 4;
+    const double* s = f32 ? nullptr : F.dscale.p;  // FP64 works in the original unknowns
+    VT* X = reinterpret_cast<VT*>(C.vec.p);
+    VT* V = X + n;
+    VT* Z = V + n;
+    VT* Y = Z + n;
+    VT* R[2] = {Y + n, Y + 2 * (size_t)n};
+    VT* Wb[2] = {Y + 3 * (size_t)n, Y + 4 * (size_t)n};
     TlState* S = C.st.p;
     const unsigned gvec = kReduceBlocks;
-    k_tl_norm<<<gvec, kVecThreads, 0, st>>>(n, C.r64.p, F.dscale.p, S, C.partial.p);
-    k_tl_rhs<<<gvec, kVecThreads, 0, st>>>(n, C.r64.p, F.dscale.p, S, R[0], R[1], X, Wb[0], Wb[1]);
-    // limits, then y = M^-1 b (r2 = R[1])
+    k_tl_norm<<<gvec, kVecThreads, 0, st>>>(n, C.r64.p, f32 ? F.dscale.p : nullptr, S, C.partial.p);
+    k_tl_rhs<VT><<<gvec, kVecThreads, 0, st>>>(n, C.r64.p, f32 ? F.dscale.p : nullptr, S, R[0], R[1], X, Wb[0], Wb[1]);
     MSFEM_TRY(read_st(C, st));
     TlState h = *C.h_st;
     h.tol = tau;
@@ -918,28 +940,29 @@ int inner_solve(CoarseHandle& C, int maxiter, double tau, int* iters)
     *C.h_st = h;
     MSFEM_CK(cudaMemcpyAsync(S, C.h_st, sizeof(TlState), cudaMemcpyHostToDevice, st));
     const unsigned gprol = kReduceBlocks;
-    precondition(C, R[1], Y, 1, st, gprol);
-    const SellView<float> A = sell_view<float>(F);
-    const unsigned gsp = spmv_grid_of((const void*)k_tl_spmv, F);
+    precondition<VT>(C, R[1], Y, 1, st, gprol, s);
+    const SellView<VT> A = sell_view<VT>(F);
+    const unsigned gsp = spmv_grid_of((const void*)k_tl_spmv<VT>, F);
     // two iterations: r1/r2 and w1/w2 swap each step
     auto two = [&]() {
         for (int p = 0; p < 2; p++) {
-            float* r1 = R[p];
-            float* r2 = R[1 - p];
-            float* w1 = Wb[p];
-            float* w2 = Wb[1 - p];
-            k_tl_spmv<<<gsp, 256, 0, st>>>(A, Y, V, Z, r1, S, C.partial.p + 2048);
+            VT* r1 = R[p];
+            VT* r2 = R[1 - p];
+            VT* w1 = Wb[p];
+            VT* w2 = Wb[1 - p];
+            k_tl_spmv<VT><<<gsp, 256, 0, st>>>(A, Y, V, Z, r1, S, C.partial.p + 2048);
             // r2_new = z - (alfa/beta) r2 over r1's buffer, and its restriction partials
-            k_tl_restrict<<<C.n_cells, 128, 0, st>>>(C.own_ptr.p, C.own.p, C.psi_hat.p, Z, r2, r1, C.cpart.p, S, 1);
+            k_tl_restrict<VT><<<C.n_cells, 128, 0, st>>>(C.own_ptr.p, C.own.p, C.psi_hat.p, Z, r2, r1, C.cpart.p, s, S, 1);
             k_tl_gather<<<gridn(C.n_cf), 256, 0, st>>>(C.n_cf, C.dptr.p, C.dent.p, C.cpart.p, C.rc.p, S);
             k_tl_gemv<<<gridn((int64_t)C.n_cf * 32), 256, 0, st>>>(C.n_cf, C.n_pad, C.Cinv.p, C.rc.p, C.ec.p, S);
-            k_tl_prolong<<<gprol, kVecThreads, 0, st>>>(C.n_fine, C.owner.p, C.cdof.p, C.psi_hat.p, C.ec.p, r1, Y, S,
-                                                        C.partial.p, 0);
-            k_tl_update<<<gvec, kVecThreads, 0, st>>>(n, V, w1, w2, X, S);
+            k_tl_prolong<VT><<<gprol, kVecThreads, 0, st>>>(C.n_fine, C.owner.p, C.cdof.p, C.psi_hat.p, C.ec.p, r1, Y, s,
+                                                            S, C.partial.p, 0);
+            k_tl_update<VT><<<gvec, kVecThreads, 0, st>>>(n, V, w1, w2, X, S);
             k_tl_applied<<<1, 1, 0, st>>>(S);
         }
     };
-    if (!C.graph) {
+    cudaGraphExec_t& graph = C.graph[f32 ? 0 : 1];
+    if (!graph) {
         cudaGraph_t gr;
         MSFEM_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         for (int k = 0; k < 8; k++) two();  // 16 iterations per replay
@@ -948,7 +971,7 @@ int inner_solve(CoarseHandle& C, int maxiter, double tau, int* iters)
             set_error("two-level MINRES graph capture failed: %s", cudaGetErrorString(e));
             return MSFEM_ERR_CUDA;
         }
-        e = cudaGraphInstantiate(&C.graph, gr, 0);
+        e = cudaGraphInstantiate(&graph, gr, 0);
         cudaGraphDestroy(gr);
         if (e != cudaSuccess) {
             set_error("two-level MINRES graph instantiate failed: %s", cudaGetErrorString(e));
@@ -960,7 +983,7 @@ int inner_solve(CoarseHandle& C, int maxiter, double tau, int* iters)
         MSFEM_TRY(read_st(C, st));
         if (C.h_st->done) break;
         if (16 * rounds > maxiter + 32) break;
-        for (int k = 0; k < 4; k++) MSFEM_CK(cudaGraphLaunch(C.graph, st));
+        for (int k = 0; k < 4; k++) MSFEM_CK(cudaGraphLaunch(graph, st));
         rounds += 4;
         F.total_launches += 4 * 16 * 7;
     }
@@ -968,24 +991,23 @@ int inner_solve(CoarseHandle& C, int maxiter, double tau, int* iters)
     return C.h_st->done == 3 ? MSFEM_ERR_NUMERIC : MSFEM_OK;
 }
 
-int solve_twolevel(CoarseHandle& C, int maxiter, double tol, double* rel, int* iters, int* outer)
+int solve_twolevel(CoarseHandle& C, int precision, int maxiter, double tol, double* rel, int* iters, int* outer)
 {
     System& F = *C.fine;
     cudaStream_t st = F.stream;
     MSFEM_TRY(prepare_sell(F));
     MSFEM_TRY(F.kstate.alloc(1));
     const int n = F.n_rows;
+    const bool f32 = precision == MSFEM_FP32_IR;
     DBuf<double>& rr = F.sc_f64[1];
     MSFEM_TRY(rr.alloc(2));
     cudaEvent_t e0, e1;
     MSFEM_CK(cudaEventCreate(&e0));
     MSFEM_CK(cudaEventCreate(&e1));
     MSFEM_CK(cudaEventRecord(e0, st));
-    // ||F||^2
-    MSFEM_TRY(residual64(F, F.X.p, F.F.p, C.r64.p, rr.p));  // also warms the path
     double ff = 0.0;
     {
-        // (F, F) through a zero vector: r = F - A 0
+        // (F, F) as the residual of a zero vector
         DBuf<double> zero;
         MSFEM_TRY(zero.alloc(n));
         MSFEM_CK(cudaMemsetAsync(zero.p, 0, sizeof(double) * n, st));
@@ -1007,14 +1029,20 @@ int solve_twolevel(CoarseHandle& C, int maxiter, double tol, double* rel, int* i
         if (prev >= 0.0 && r2 > 0.25 * prev) break;  // refinement no longer contracts
         prev = r2;
         const double need = tol * std::sqrt(ff / r2);
-        const double tau = std::max(1e-5, std::min(0.5, 0.3 * need));
+        // FP32 stops near its own precision; FP64 aims a little past what is missing
+        const double tau = f32 ? std::max(1e-5, std::min(0.5, 0.3 * need)) : std::max(1e-14, 0.1 * need);
         int it = 0;
-        rc = inner_solve(C, maxiter - total, tau, &it);
+        rc = f32 ? inner_solve<float>(C, maxiter - total, tau, &it) : inner_solve<double>(C, maxiter - total, tau, &it);
         total += it;
         if (std::getenv("MSFEM_TRACE"))
-            std::fprintf(stderr, "[msfem] two-level refine %d: rel %.3e tau %.1e inner %d\n", k, std::sqrt(r2 / ff), tau, it);
+            std::fprintf(stderr, "[msfem] two-level refine %d (%s): rel %.3e tau %.1e inner %d\n", k, f32 ? "fp32" : "fp64",
+                         std::sqrt(r2 / ff), tau, it);
         if (rc == MSFEM_ERR_NUMERIC) break;
-        k_tl_correct<<<kReduceBlocks, kVecThreads, 0, st>>>(n, F.X.p, C.vec.p, F.dscale.p, C.st.p);
+        if (f32)
+            k_tl_correct<float><<<kReduceBlocks, kVecThreads, 0, st>>>(n, F.X.p, reinterpret_cast<float*>(C.vec.p),
+                                                                       F.dscale.p, C.st.p);
+        else
+            k_tl_correct<double><<<kReduceBlocks, kVecThreads, 0, st>>>(n, F.X.p, C.vec.p, nullptr, C.st.p);
     }
     MSFEM_CK(cudaEventRecord(e1, st));
     MSFEM_CK(cudaStreamSynchronize(st));
@@ -1112,29 +1140,30 @@ int msfem_coarse_apply(msfem_coarse_t c, const float* r, float* y)
     System& F = *c->fine;
     cudaStream_t st = F.stream;
     const int n = F.n_rows;
-    float* dr = c->vec.p + 5 * (size_t)n;  // an inner-solve work vector
-    float* dy = c->vec.p + 6 * (size_t)n;
+    float* dr = reinterpret_cast<float*>(c->vec.p) + 5 * (size_t)n;  // inner-solve work vectors
+    float* dy = reinterpret_cast<float*>(c->vec.p) + 6 * (size_t)n;
     MSFEM_CK(cudaMemcpyAsync(dr, r, sizeof(float) * n, cudaMemcpyHostToDevice, st));
     MSFEM_CK(cudaMemsetAsync(c->st.p, 0, sizeof(TlState), st));
-    precondition(*c, dr, dy, 1, st, kReduceBlocks);
+    precondition<float>(*c, dr, dy, 1, st, kReduceBlocks, nullptr);
     MSFEM_CK(cudaGetLastError());
     MSFEM_CK(cudaMemcpyAsync(y, dy, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
     MSFEM_CK(cudaStreamSynchronize(st));
     return MSFEM_OK;
 }
 
-int msfem_solve_twolevel(msfem_system_t fine, msfem_coarse_t c, int maxiter, double tol, double* rel_residual,
-                         int* iterations, int* outer)
+int msfem_solve_twolevel(msfem_system_t fine, msfem_coarse_t c, int precision, int maxiter, double tol,
+                         double* rel_residual, int* iterations, int* outer)
 {
     using namespace msfem;
-    if (!fine || !c || maxiter <= 0 || !(tol > 0.0) || reinterpret_cast<System*>(fine) != c->fine) {
+    if (!fine || !c || maxiter <= 0 || !(tol > 0.0) || reinterpret_cast<System*>(fine) != c->fine ||
+        (precision != MSFEM_FP64 && precision != MSFEM_FP32_IR)) {
         set_error("msfem_solve_twolevel: bad arguments (the coarse handle must belong to this system)");
         return MSFEM_ERR_ARGUMENT;
     }
     MSFEM_CK(cudaSetDevice(c->fine->device));
     double rel = 0.0;
     int it = 0, out = 0;
-    const int rc = solve_twolevel(*c, maxiter, tol, &rel, &it, &out);
+    const int rc = solve_twolevel(*c, precision, maxiter, tol, &rel, &it, &out);
     if (rel_residual) *rel_residual = rel;
     if (iterations) *iterations = it;
     if (outer) *outer = out;

@@ -9,9 +9,9 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import check, load
+from ._lib import FP32_IR, FP64, check, load
 
-__all__ = ["TwoLevel"]
+__all__ = ["TwoLevel", "FP64", "FP32_IR"]
 
 
 def _c(a, dt):
@@ -41,10 +41,10 @@ class TwoLevel:
         check(L.msfem_coarse_info(h, C.byref(n), C.byref(ms)), "coarse_info")
         self.n_coarse_dofs, self.ms_setup = n.value, ms.value
 
-    def solve(self, tol=1e-8, maxiter=200000):
+    def solve(self, tol=1e-8, maxiter=200000, precision=FP32_IR):
         rel, it, out = C.c_double(), C.c_int(), C.c_int()
-        rc = check(load().msfem_solve_twolevel(self.system.h, self.h, maxiter, tol, C.byref(rel), C.byref(it),
-                                               C.byref(out)), "solve_twolevel")
+        rc = check(load().msfem_solve_twolevel(self.system.h, self.h, precision, maxiter, tol, C.byref(rel),
+                                               C.byref(it), C.byref(out)), "solve_twolevel")
         return rel.value, it.value, out.value, rc
 
     def coarse_matrix(self):

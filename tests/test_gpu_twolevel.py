@@ -8,7 +8,7 @@ import pytest
 import scipy.sparse.linalg as spl
 
 from multiscalefemsolver3d_b200 import fem, meshgen
-from multiscalefemsolver3d_b200.cells import FP64, Cells
+from multiscalefemsolver3d_b200.cells import FP32_IR, FP64, Cells
 from multiscalefemsolver3d_b200.twolevel import TwoLevel
 from oracle import twolevel as otl
 
@@ -58,13 +58,16 @@ def test_preconditioner_application_matches_oracle(case):
     assert np.linalg.norm(y - yo) <= 1e-5 * np.linalg.norm(yo)
 
 
-def test_twolevel_solve_matches_exact_solution(case):
+@pytest.mark.parametrize("precision", [FP32_IR, FP64])
+def test_twolevel_solve_matches_exact_solution(case, precision):
     p, S, cc, cells, dofs, T, P, cdof = case
     A = S.export_csr()
     x_exact = spl.spsolve(A.to_scipy().tocsc(), A.F)
     S.set_x(np.zeros(A.n))
-    rel, it, outer, rc = T.solve(tol=1e-12, maxiter=20000)
-    assert rc == 0 and rel <= 1e-12 and outer >= 2
+    rel, it, outer, rc = T.solve(tol=1e-12, maxiter=20000, precision=precision)
+    assert rc == 0 and rel <= 1e-12
+    if precision == FP32_IR:
+        assert outer >= 2
     x = S.get_x()
     assert np.linalg.norm(x - x_exact) <= 1e-8 * np.linalg.norm(x_exact)
 
@@ -73,9 +76,10 @@ def test_twolevel_cuts_iterations(case):
     """Same system, same stopping rule: MINRES with the two-level preconditioner needs fewer
     iterations than MINRES with the Jacobi scaling alone."""
     p, S, cc, cells, dofs, T, P, cdof = case
-    S.set_x(np.zeros(S.n_rows))
-    rel2, it2, _, rc2 = T.solve(tol=1e-8)
-    S.set_x(np.zeros(S.n_rows))
-    rel1, it1, rc1 = S.solve(fem.MINRES, fem.FP32_IR, tol=1e-8, maxiter=200000)
-    assert rc2 == 0 and rc1 == 0
-    assert it2 < it1, (it2, it1)
+    for prec in (FP32_IR, FP64):
+        S.set_x(np.zeros(S.n_rows))
+        rel2, it2, _, rc2 = T.solve(tol=1e-8, precision=prec)
+        S.set_x(np.zeros(S.n_rows))
+        rel1, it1, rc1 = S.solve(fem.MINRES, prec, tol=1e-8, maxiter=200000)
+        assert rc2 == 0 and rc1 == 0
+        assert it2 < it1, (prec, it2, it1)
