@@ -500,6 +500,7 @@ def run_cells(args, D):
     vol_ms = statistics.mean(r["ms"]["volumes"] for r in reps)
     ach = algo / (vol_ms * 1e-3) / 1e9
     peak, peak_kind = peaks()
+    tuned = int(rep["threads"]["volumes"])  # the e2e calls reuse the CTA size tuned above
     C.close()
 
     # e2e: create (topology + portraits) + build + bases copied back, host (pinned) buffers
@@ -516,7 +517,7 @@ def run_cells(args, D):
         _lib.check(L.msfem_cells_create(cm.n_cells, P(h[0]), P(h[1]), P(h[2]), P(h[3]), P(h[4]), P(h[5]),
                                         h[6].numel(), P(h[6]), P(h[7]), 0, C_.byref(hh)), "cells_create")
         try:
-            rc = L.msfem_cells_build_bases(hh, FP32_IR, TOL, 5000, 256)
+            rc = L.msfem_cells_build_bases(hh, FP32_IR, TOL, 5000, tuned)
             if rc != 0:
                 raise RuntimeError(f"cells build rc={rc}")
             _lib.check(L.msfem_cells_get_bases(hh, P(out), 0), "cells_get_bases")
@@ -539,7 +540,8 @@ def run_cells(args, D):
         extra = {"ms_stages": {k: statistics.mean(r["ms"][k] for r in reps) for k in rep["ms"]},
                  "inner_iterations_mean": float(rep["inner"].mean()), "inner_iterations_max": int(rep["inner"].max()),
                  "refinement_steps_mean": float(rep["outer"].mean()), "rel_residual_max": float(rep["rel"].max()),
-                 "face_rel_residual_max": float(rep["face_rel"].max()), "step_ms_all": ts}
+                 "face_rel_residual_max": float(rep["face_rel"].max()), "step_ms_all": ts,
+                 "autotuned_cta_threads": rep["threads"]}
         line = {"metric": METRIC, "value": ms, "unit": UNIT, "n_gpus": D.world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
                 "vs_baseline": None, "dtype": "fp32-in-f64-ir", "data": "synthetic",

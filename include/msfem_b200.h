@@ -236,7 +236,8 @@ int msfem_batch_create(int dim, int n_systems, const int64_t* node_off, const do
  * F_I = -A_IB g the right-hand side of the free rows after the Dirichlet elimination (the
  * reference's cell drivers also count the Dirichlet values g in ||F||, a measure up to ~1/h
  * looser, and compensate with MIN_RESIDUAL = 5e-15).  maxiter bounds each inner solve,
- * threads = CTA size (multiple of 32, <= 512).
+ * threads = CTA size (multiple of 32, <= 512; 0 = autotune: the first call times 128, 256, 384
+ * and 512 threads on the largest systems and keeps the fastest).
  * Returns MSFEM_NOT_CONVERGED when some system missed tol. */
 int msfem_batch_solve(msfem_batch_t b, double* x, int precision, double tol, int maxiter, int threads, int on_device);
 
@@ -271,9 +272,10 @@ int msfem_cells_get_bases(msfem_cells_t c, double* bases, int on_device);
 /* Per-cell report of the last build (host arrays of n_cells, any may be NULL):
  * inner iterations, outer refinement steps and final relative residual of the volume
  * problems, and the worst relative residual of the cell's face problems.
- * ms[0..3] = device ms of assembly, edges, faces, volumes. */
+ * ms[0..3] = device ms of assembly, edges, faces, volumes; threads[0..1] = CTA size the face
+ * and volume launches used (autotuned when build_bases got threads <= 0). */
 int msfem_cells_report(msfem_cells_t c, int32_t* inner_iterations, int32_t* outer_iterations, double* rel_residual,
-                       double* face_rel_residual, double* ms);
+                       double* face_rel_residual, double* ms, int32_t* threads);
 void msfem_cells_destroy(msfem_cells_t c);
 
 

@@ -43,7 +43,7 @@ class BatchSystems:
                                    _p(fx), n_rhs, 0, C.byref(h)), "batch_create")
         self.h = h
 
-    def solve(self, x, precision=FP32_IR, tol=1e-8, maxiter=5000, threads=256):
+    def solve(self, x, precision=FP32_IR, tol=1e-8, maxiter=5000, threads=0):
         """x: [n_nodes, R, 3] with the Dirichlet values at fixed nodes; returns (x, rc)."""
         x = _c(x, np.float64).copy()
         rc = check(load().msfem_batch_solve(self.h, _p(x), precision, tol, maxiter, threads, 0), "batch_solve")
@@ -84,7 +84,8 @@ class Cells:
                                    0, C.byref(h)), "cells_create")
         self.h = h
 
-    def build_bases(self, precision=FP32_IR, tol=1e-8, maxiter=5000, threads=256):
+    def build_bases(self, precision=FP32_IR, tol=1e-8, maxiter=5000, threads=0):
+        """threads = CTA size of the persistent solves; 0 autotunes it on the first build."""
         return check(load().msfem_cells_build_bases(self.h, precision, tol, maxiter, threads), "cells_build_bases")
 
     def bases(self):
@@ -96,9 +97,11 @@ class Cells:
         n = self.n_cells
         it, out = np.zeros(n, np.int32), np.zeros(n, np.int32)
         rel, frel, ms = np.zeros(n), np.zeros(n), np.zeros(4)
-        check(load().msfem_cells_report(self.h, _p(it), _p(out), _p(rel), _p(frel), _p(ms)), "cells_report")
+        thr = np.zeros(2, np.int32)
+        check(load().msfem_cells_report(self.h, _p(it), _p(out), _p(rel), _p(frel), _p(ms), _p(thr)), "cells_report")
         return {"inner": it, "outer": out, "rel": rel, "face_rel": frel,
-                "ms": dict(zip(("assemble", "edges", "faces", "volumes"), ms.tolist()))}
+                "ms": dict(zip(("assemble", "edges", "faces", "volumes"), ms.tolist())),
+                "threads": {"faces": int(thr[0]), "volumes": int(thr[1])}}
 
     def close(self):
         if getattr(self, "h", None):

@@ -559,8 +559,9 @@ __global__ void __launch_bounds__(512) k_batch_minres(BatchArgs A, int start64)
     }
 }
 
+// one persistent launch over the first n_limit systems of the queue (largest first)
 template <int R>
-int launch_minres(BatchSys& b, double* d_x, int start64, double tol, int maxiter, int threads)
+int launch_minres(BatchSys& b, double* d_x, int start64, double tol, int maxiter, int threads, int n_limit)
 {
     auto kern = k_batch_minres<R>;
     int dev = 0, sms = 0, per_sm = 0;
@@ -568,14 +569,14 @@ int launch_minres(BatchSys& b, double* d_x, int start64, double tol, int maxiter
     MSFEM_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     MSFEM_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, 0));
     if (per_sm < 1) per_sm = 1;
-    const int grid = std::min<int64_t>((int64_t)sms * per_sm, std::max(1, b.n_sys));
+    const int grid = std::min<int64_t>((int64_t)sms * per_sm, std::max(1, n_limit));
     const int64_t stride = (((int64_t)b.max_nodes * R * 3) + 31) / 32 * 32;
     const size_t need = (size_t)grid * 6 * stride * sizeof(double);  // room for FP64 vectors
     if (b.work.n < need) MSFEM_TRY(b.work.alloc(need));
     MSFEM_TRY(b.queue.alloc(1));
     MSFEM_CK(cudaMemsetAsync(b.queue.p, 0, sizeof(int), b.stream));
     BatchArgs a{};
-    a.n_sys = b.n_sys;
+    a.n_sys = n_limit;
     a.order = b.order.p;
     a.node_off = b.node_off.p;
     a.row_ptr = b.row_ptr.p;
@@ -787,23 +788,86 @@ int batch_assemble(BatchSys& b, const double* d_xyz, const double* d_lame, int n
     return 0;
 }
 
-int batch_solve(BatchSys& b, double* d_x, int precision, double tol, int maxiter, int threads)
+namespace {
+
+int launch_any(BatchSys& b, double* d_x, int start64, double tol, int maxiter, int threads, int n_limit)
 {
-    if (b.n_sys == 0) return 0;
-    if (threads <= 0) threads = 256;
-    if (threads % 32 != 0 || threads > 512) {
-        set_error("batched solve: threads per system must be a multiple of 32, at most 512");
-        return MSFEM_ERR_ARGUMENT;
-    }
-    const int start64 = precision == MSFEM_FP32_IR ? 0 : 1;
     switch (b.R) {
-    case 4: return launch_minres<4>(b, d_x, start64, tol, maxiter, threads);
-    case 8: return launch_minres<8>(b, d_x, start64, tol, maxiter, threads);
-    case 1: return launch_minres<1>(b, d_x, start64, tol, maxiter, threads);
+    case 4: return launch_minres<4>(b, d_x, start64, tol, maxiter, threads, n_limit);
+    case 8: return launch_minres<8>(b, d_x, start64, tol, maxiter, threads, n_limit);
+    case 1: return launch_minres<1>(b, d_x, start64, tol, maxiter, threads, n_limit);
     default:
         set_error("batched solve: %d right-hand sides per system (1, 4 or 8 supported)", b.R);
         return MSFEM_ERR_ARGUMENT;
     }
+}
+
+// Autotuner of the persistent launch: the CTA size (threads per system) decides how many
+// row-rhs pairs a pass covers and how many CTAs fit per SM.  Each candidate solves the same
+// sample -- the 2 x #SM largest systems, which dominate the batch's time -- from the same start
+// (x is saved and restored around each trial), timed with CUDA events; the fastest is kept for
+// this batch.  Batches smaller than the sample are not timed (the choice hardly matters there).
+int autotune(BatchSys& b, double* d_x, int start64, double tol, int maxiter)
+{
+    int dev = 0, sms = 0;
+    MSFEM_CK(cudaGetDevice(&dev));
+    MSFEM_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int sample = 2 * sms;
+    b.tune_ms.clear();
+    if (b.n_sys < 2 * sample) {
+        b.tuned_threads = 256;
+        return 0;
+    }
+    const size_t nx = (size_t)b.n_nodes * b.R * 3;
+    DBuf<double> save;
+    MSFEM_TRY(save.alloc(nx));
+    MSFEM_CK(cudaMemcpyAsync(save.p, d_x, sizeof(double) * nx, cudaMemcpyDeviceToDevice, b.stream));
+    cudaEvent_t e0, e1;
+    MSFEM_CK(cudaEventCreate(&e0));
+    MSFEM_CK(cudaEventCreate(&e1));
+    const int cand[] = {128, 256, 384, 512};
+    float best = 0.f;
+    int best_t = 256;
+    for (int t : cand) {
+        MSFEM_CK(cudaMemcpyAsync(d_x, save.p, sizeof(double) * nx, cudaMemcpyDeviceToDevice, b.stream));
+        MSFEM_CK(cudaEventRecord(e0, b.stream));
+        MSFEM_TRY(launch_any(b, d_x, start64, tol, maxiter, t, sample));
+        MSFEM_CK(cudaEventRecord(e1, b.stream));
+        MSFEM_CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        MSFEM_CK(cudaEventElapsedTime(&ms, e0, e1));
+        b.tune_ms.push_back(ms);
+        if (b.tune_ms.size() == 1 || ms < best) {
+            best = ms;
+            best_t = t;
+        }
+    }
+    MSFEM_CK(cudaMemcpyAsync(d_x, save.p, sizeof(double) * nx, cudaMemcpyDeviceToDevice, b.stream));
+    MSFEM_CK(cudaStreamSynchronize(b.stream));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b.tuned_threads = best_t;
+    return 0;
+}
+
+}  // namespace
+
+int batch_solve(BatchSys& b, double* d_x, int precision, double tol, int maxiter, int threads)
+{
+    if (b.n_sys == 0) return 0;
+    const int start64 = precision == MSFEM_FP32_IR ? 0 : 1;
+    if (threads <= 0) {
+        if (b.tuned_threads == 0 || b.tuned_precision != precision) {
+            MSFEM_TRY(autotune(b, d_x, start64, tol, maxiter));
+            b.tuned_precision = precision;
+        }
+        threads = b.tuned_threads;
+    }
+    if (threads % 32 != 0 || threads > 512) {
+        set_error("batched solve: threads per system must be a multiple of 32, at most 512");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    return launch_any(b, d_x, start64, tol, maxiter, threads, b.n_sys);
 }
 
 }  // namespace msfem

@@ -43,6 +43,8 @@ struct BatchSys {
     DBuf<int32_t> iters, outers;
     DBuf<double> rel;
     int grid = 0, threads = 0;
+    int tuned_threads = 0, tuned_precision = -1;  // autotuned CTA size (0: not tuned yet)
+    std::vector<float> tune_ms;                   // trial times of the candidates 128/256/384/512
     int64_t work_stride = 0;
     float last_ms = 0.f;
 };
@@ -52,7 +54,8 @@ int batch_build_pattern(BatchSys& b, const double* d_xyz);
 // values from the current materials (lame: [n_mat][2] lambda, mu on the device)
 int batch_assemble(BatchSys& b, const double* d_xyz, const double* d_lame, int n_mat);
 // solves every system; x: [n_nodes][R][3] FP64, fixed entries hold the Dirichlet data on
-// entry, free entries are overwritten.  precision: MSFEM_FP64 or MSFEM_FP32_IR.
+// entry, free entries are overwritten.  precision: MSFEM_FP64 or MSFEM_FP32_IR.  threads <= 0:
+// the CTA size is autotuned on the first call (cached per batch and precision).
 int batch_solve(BatchSys& b, double* d_x, int precision, double tol, int maxiter, int threads);
 
 }  // namespace msfem

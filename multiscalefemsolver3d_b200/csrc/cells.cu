@@ -884,7 +884,8 @@ int msfem_cells_get_bases(msfem_cells_t h, double* bases, int on_device)
     return MSFEM_OK;
 }
 
-int msfem_cells_report(msfem_cells_t h, int32_t* inner, int32_t* outer, double* rel, double* face_rel, double* ms)
+int msfem_cells_report(msfem_cells_t h, int32_t* inner, int32_t* outer, double* rel, double* face_rel, double* ms,
+                       int32_t* threads)
 {
     using namespace msfem;
     if (!h) {
@@ -907,6 +908,10 @@ int msfem_cells_report(msfem_cells_t h, int32_t* inner, int32_t* outer, double* 
         }
     if (ms)
         for (int k = 0; k < 4; k++) ms[k] = h->ms[k];
+    if (threads) {
+        threads[0] = h->faces.threads;
+        threads[1] = h->vols.threads;
+    }
     return MSFEM_OK;
 }
 
