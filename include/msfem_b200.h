@@ -120,6 +120,12 @@ int msfem_assemble_scalar(msfem_system_t h, const double* sigma, int n_materials
  * (Library/Domain.h:53-78).  Materials with E <= 0 contribute nothing. */
 int msfem_assemble_elastic(msfem_system_t h, const double* E, const double* nu, int n_materials);
 
+/* No counterpart in the reference: the same assembly with every block transposed, i.e. the
+ * textbook orientation A[I][J] = V * B_I^T D B_J, which is symmetric positive semi-definite
+ * (the reference's orientation is symmetric but indefinite).  Used as the operator of the
+ * smoothing and coarse levels of msfem_coarse_set_smoother. */
+int msfem_assemble_elastic_textbook(msfem_system_t h, const double* E, const double* nu, int n_materials);
+
 /* Traction load (FEM/FEM.h:1338-1343, BoundaryFace_forMech::SolveLocalBoundaryVector
  * FEM_Grid.h:2622-2661): F[3*v+c] += traction[3*f+c] * area_f / 3 for the three
  * nodes v of face f.  ELASTIC only. */
@@ -319,6 +325,13 @@ int msfem_coarse_apply(msfem_coarse_t c, const float* r, float* y);
  * total; outer: refinement steps. */
 int msfem_solve_twolevel(msfem_system_t fine, msfem_coarse_t c, int precision, int maxiter, double tol,
                          double* rel_residual, int* iterations, int* outer);
+/* Switches msfem_solve_twolevel (precision MSFEM_FP64) to the symmetric multiplicative cycle
+ * on the textbook operator: `textbook` is a second system on the same mesh assembled with
+ * msfem_assemble_elastic_textbook and given the same Dirichlet rows.  One application of M^-1:
+ * `degree` Chebyshev steps on its Jacobi-scaled FP32 matrix (spectrum bound [lmax/ratio, lmax],
+ * lmax from 30 power steps), the coarse correction, the same Chebyshev steps again; SPD, so
+ * MINRES on the reference's matrix keeps its guarantees.  The textbook system must outlive c. */
+int msfem_coarse_set_smoother(msfem_coarse_t c, msfem_system_t textbook, int degree, double ratio);
 void msfem_coarse_destroy(msfem_coarse_t c);
 
 #ifdef __cplusplus

@@ -56,6 +56,7 @@ _SIGS = [
     ("msfem_clear", C.c_int, [C.c_void_p]),
     ("msfem_assemble_scalar", C.c_int, [C.c_void_p, _P, C.c_int]),
     ("msfem_assemble_elastic", C.c_int, [C.c_void_p, _P, _P, C.c_int]),
+    ("msfem_assemble_elastic_textbook", C.c_int, [C.c_void_p, _P, _P, C.c_int]),
     ("msfem_add_traction", C.c_int, [C.c_void_p, C.c_int, _P, _P, C.c_int]),
     ("msfem_add_rhs", C.c_int, [C.c_void_p, _P, C.c_int]),
     ("msfem_apply_dirichlet", C.c_int, [C.c_void_p, C.c_int, _P, _P, C.c_int, C.c_int]),
@@ -93,6 +94,7 @@ _SIGS = [
     ("msfem_coarse_apply", C.c_int, [C.c_void_p, _P, _P]),
     ("msfem_solve_twolevel", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double, C.POINTER(C.c_double),
                                        C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ("msfem_coarse_set_smoother", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_double]),
     ("msfem_coarse_destroy", None, [C.c_void_p]),
 ]
 

@@ -74,6 +74,9 @@ __global__ void k_assemble_scalar(int count, const int32_t* __restrict__ elems, 
 //   A[I][J][a][b] = V * (lambda * gJ_a * gI_b + mu * gI_a * gJ_b + mu * delta_ab * gI.gJ)
 // (g = basis gradient), which also equals the reference's mirrored blocks
 // A[J][I] = A[I][J]^T, so all 16 blocks come from this one expression.
+// TEXTBOOK: the textbook orientation lambda gI_a gJ_b + mu gJ_a gI_b (the transpose of every
+// block), symmetric positive semi-definite; used to build preconditioners, not by the reference.
+template <bool TEXTBOOK>
 __global__ void k_assemble_elastic(int count, const int32_t* __restrict__ elems, const int32_t* __restrict__ tets,
                                    const double* __restrict__ xyz, const int32_t* __restrict__ mat,
                                    const double* __restrict__ lame /* [n_mat][2] */, int n_mat,
@@ -107,7 +110,8 @@ __global__ void k_assemble_elastic(int count, const int32_t* __restrict__ elems,
             for (int a = 0; a < 3; a++)
 #pragma unroll
                 for (int b = 0; b < 3; b++) {
-                    double k = lam * gj[a] * gi[b] + mu * gi[a] * gj[b];
+                    double k = TEXTBOOK ? lam * gi[a] * gj[b] + mu * gj[a] * gi[b]
+                                        : lam * gj[a] * gi[b] + mu * gi[a] * gj[b];
                     if (a == b) k += dd;
                     out[3 * a + b] += V * k;
                 }
@@ -234,7 +238,7 @@ void lame_params(const double* E, const double* nu, int n_mat, double* lame)
     }
 }
 
-int assemble_elastic(System& s, const double* E, const double* nu, int n_mat)
+int assemble_elastic(System& s, const double* E, const double* nu, int n_mat, bool textbook)
 {
     if (s.kind != MSFEM_ELASTIC) {
         set_error("assemble_elastic on a scalar system");
@@ -256,7 +260,8 @@ int assemble_elastic(System& s, const double* E, const double* nu, int n_mat)
     const int nc = (int)s.color_off.size() - 1;
     for (int c = 0; c < nc; c++) {
         int cnt = s.color_off[c + 1] - s.color_off[c];
-        k_assemble_elastic<<<grid_for(cnt, 128), 128, 0, s.stream>>>(cnt, s.color_elems.p + s.color_off[c], s.tets.p,
+        auto kern = textbook ? k_assemble_elastic<true> : k_assemble_elastic<false>;
+        kern<<<grid_for(cnt, 128), 128, 0, s.stream>>>(cnt, s.color_elems.p + s.color_off[c], s.tets.p,
                                                                      s.xyz.p, s.mat.p, d_lame.p, n_mat, s.eslot.p,
                                                                      s.val.p, bad.p);
     }

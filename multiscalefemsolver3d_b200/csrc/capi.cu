@@ -225,6 +225,13 @@ int msfem_assemble_elastic(msfem_system_t h, const double* E, const double* nu, 
     return assemble_elastic(*as_sys(h), E, nu, n_materials);
 }
 
+int msfem_assemble_elastic_textbook(msfem_system_t h, const double* E, const double* nu, int n_materials)
+{
+    MSFEM_TRY(check_handle(h));
+    MSFEM_TRY(use_device(*as_sys(h)));
+    return assemble_elastic(*as_sys(h), E, nu, n_materials, true);
+}
+
 int msfem_add_traction(msfem_system_t h, int n_faces, const int32_t* face_nodes, const double* traction, int on_device)
 {
     (void)on_device;

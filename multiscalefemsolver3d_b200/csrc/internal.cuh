@@ -166,7 +166,7 @@ struct System {
 int build_topology(System& s);
 // ---- assembly (assemble.cu)
 int assemble_scalar(System& s, const double* sigma, int n_mat);
-int assemble_elastic(System& s, const double* E, const double* nu, int n_mat);
+int assemble_elastic(System& s, const double* E, const double* nu, int n_mat, bool textbook = false);
 // lambda, mu per material from E, nu (host): lame[2m], lame[2m+1]
 void lame_params(const double* E, const double* nu, int n_mat, double* lame);
 int add_traction(System& s, int n_faces, const int32_t* d_faces, const double* d_traction);

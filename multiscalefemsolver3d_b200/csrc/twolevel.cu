@@ -447,6 +447,48 @@ __global__ void __launch_bounds__(256) k_tl_gemv(int n, int ld, const float* __r
     }
 }
 
+// bb = (r, M^-1 r) of the new Lanczos vector: beta' = sqrt(bb) and the MINRES Givens step;
+// init: the first application (beta1).  One thread.
+__device__ void givens_step(TlState* S, double bb, int init)
+{
+    if (init) {
+        const double b1 = bb > 0.0 ? sqrt(bb) : 0.0;
+        S->beta1 = b1;
+        S->beta = b1;
+        S->oldb = 0.0;
+        S->phibar = b1;
+        S->dbar = 0.0;
+        S->epsln = 0.0;
+        S->cs = -1.0;
+        S->sn = 0.0;
+        S->iter = 0;
+        S->applied = -1;
+        S->done = (b1 > 0.0) ? 0 : 1;
+        return;
+    }
+    const double beta = bb > 0.0 ? sqrt(bb) : 0.0;
+    S->oldb = S->beta;
+    S->beta = beta;
+    S->oldeps = S->epsln;
+    const double delta = S->cs * S->dbar + S->sn * S->alfa;
+    const double gbar = S->sn * S->dbar - S->cs * S->alfa;
+    S->epsln = S->sn * beta;
+    S->dbar = -S->cs * beta;
+    double gamma = sqrt(gbar * gbar + beta * beta);
+    if (!(gamma > 1e-300)) gamma = 1e-300;
+    S->cs = gbar / gamma;
+    S->sn = beta / gamma;
+    S->phi = S->cs * S->phibar;
+    S->phibar = S->sn * S->phibar;
+    S->delta = delta;
+    S->gamma = gamma;
+    S->denom = 1.0 / gamma;
+    S->iter += 1;
+    if (!(bb == bb)) S->done = 3;
+    else if (fabs(S->phibar) <= S->tol * S->beta1 || !(beta > 0.0)) S->done = 1;
+    else if (S->iter >= S->maxiter) S->done = 2;
+}
+
 // y = r + P^ ec (scaled FP32 system) or y = s^2 r + s P^ ec (FP64, original unknowns); bb = (r, y);
 // the last block updates the Givens recurrence.  init: first application (beta1 = sqrt(bb)).
 template <class VT>
@@ -490,43 +532,7 @@ __global__ void __launch_bounds__(kVecThreads) k_tl_prolong(int n_fine, const in
         double t[1];
         reduce_partials<1>(partial, gridDim.x, 0, t, sh);
         if (threadIdx.x == 0) {
-            const double bb = t[0];
-            if (init) {
-                const double b1 = bb > 0.0 ? sqrt(bb) : 0.0;
-                S->beta1 = b1;
-                S->beta = b1;
-                S->oldb = 0.0;
-                S->phibar = b1;
-                S->dbar = 0.0;
-                S->epsln = 0.0;
-                S->cs = -1.0;
-                S->sn = 0.0;
-                S->iter = 0;
-                S->applied = -1;
-                S->done = (b1 > 0.0) ? 0 : 1;
-            } else {
-                const double beta = bb > 0.0 ? sqrt(bb) : 0.0;
-                S->oldb = S->beta;
-                S->beta = beta;
-                S->oldeps = S->epsln;
-                const double delta = S->cs * S->dbar + S->sn * S->alfa;
-                const double gbar = S->sn * S->dbar - S->cs * S->alfa;
-                S->epsln = S->sn * beta;
-                S->dbar = -S->cs * beta;
-                double gamma = sqrt(gbar * gbar + beta * beta);
-                if (!(gamma > 1e-300)) gamma = 1e-300;
-                S->cs = gbar / gamma;
-                S->sn = beta / gamma;
-                S->phi = S->cs * S->phibar;
-                S->phibar = S->sn * S->phibar;
-                S->delta = delta;
-                S->gamma = gamma;
-                S->denom = 1.0 / gamma;
-                S->iter += 1;
-                if (!(bb == bb)) S->done = 3;
-                else if (fabs(S->phibar) <= S->tol * S->beta1 || !(beta > 0.0)) S->done = 1;
-                else if (S->iter >= S->maxiter) S->done = 2;
-            }
+            givens_step(S, t[0], init);
             S->ticket[0] = 0;
         }
     }
@@ -642,6 +648,177 @@ __global__ void __launch_bounds__(kVecThreads) k_tl_correct(int n, double* __res
         X[i] += sc * (s ? s[i] : 1.0) * (double)x[i];
 }
 
+// ---- symmetric multiplicative two-level cycle on the textbook operator (FP32, its
+// Jacobi-scaled space K^ = S_t K_t S_t): pre-smoothing by k Chebyshev steps, coarse correction
+// with P^_t = S_t^-1 P, post-smoothing by the same k steps.  M^-1 r = S_t cycle(S_t r).
+
+struct ChebCoef {
+    float inv_theta;   // first step: d = res / theta
+    float a[8], b[8];  // step i >= 1: d_i = a_i d_{i-1} + b_i res_i
+};
+
+// entry of the cycle: r_new = z - (alfa / beta) r2 (lanczos; else r_new = z), written over `out`;
+// rhat = S_t r_new; res = rhat; d = rhat / theta; x = d
+__global__ void __launch_bounds__(kVecThreads) k_mg_in(int n, const double* __restrict__ z, const double* __restrict__ r2,
+                                                      double* __restrict__ out, const double* __restrict__ st,
+                                                      float* __restrict__ rhat, float* __restrict__ res,
+                                                      float* __restrict__ d, float* __restrict__ x, ChebCoef cc,
+                                                      const TlState* S, int lanczos)
+{
+    if (S->done) return;
+    const double coef = lanczos ? S->alfa / S->beta : 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double r = z[i];
+        if (lanczos) {
+            r -= coef * r2[i];
+            out[i] = r;
+        }
+        const float rh = (float)(st[i] * r);
+        rhat[i] = rh;
+        res[i] = rh;
+        const float di = rh * cc.inv_theta;
+        d[i] = di;
+        x[i] = di;
+    }
+}
+
+// one Chebyshev step: res -= K^ d_prev; d = a d_prev + b res; x += d
+__global__ void __launch_bounds__(256) k_mg_cheb(SellView<float> A, const float* __restrict__ dprev,
+                                                 float* __restrict__ d, float* __restrict__ res, float* __restrict__ x,
+                                                 float a, float b, const TlState* S)
+{
+    if (S->done) return;
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; warp < A.n_slices; warp += nw) {
+        float kd[3];
+        sell_row_block<float>(A, warp, lane, dprev, kd);
+        const int brow = warp * kSlice + lane;
+        if (brow < A.n_brows)
+            for (int c = 0; c < 3; c++) {
+                const int64_t i = 3 * (int64_t)brow + c;
+                const float ri = res[i] - kd[c];
+                res[i] = ri;
+                const float di = a * dprev[i] + b * ri;
+                d[i] = di;
+                x[i] += di;
+            }
+    }
+}
+
+// res = rhat - K^ x; with `start`: also the first post-smoothing step d = res / theta,
+// x2 = x + d (into a second buffer: x is being gathered)
+__global__ void __launch_bounds__(256) k_mg_resid(SellView<float> A, const float* __restrict__ rhat,
+                                                  const float* __restrict__ x, float* __restrict__ res,
+                                                  float* __restrict__ d, float* __restrict__ x2, float inv_theta,
+                                                  const TlState* S, int start)
+{
+    if (S->done) return;
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; warp < A.n_slices; warp += nw) {
+        float kx[3];
+        sell_row_block<float>(A, warp, lane, x, kx);
+        const int brow = warp * kSlice + lane;
+        if (brow < A.n_brows)
+            for (int c = 0; c < 3; c++) {
+                const int64_t i = 3 * (int64_t)brow + c;
+                const float ri = rhat[i] - kx[c];
+                res[i] = ri;
+                if (start) {
+                    const float di = ri * inv_theta;
+                    d[i] = di;
+                    x2[i] = x[i] + di;
+                }
+            }
+    }
+}
+
+// x += P^_t ec
+__global__ void __launch_bounds__(kVecThreads) k_mg_prolong(int n_fine, const int32_t* __restrict__ owner,
+                                                           const int32_t* __restrict__ cdof,
+                                                           const float* __restrict__ psi, const float* __restrict__ ec,
+                                                           float* __restrict__ x, const TlState* S)
+{
+    if (S->done) return;
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n_fine; g += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t* cd = cdof + 24 * owner[g];
+        const float* ph = psi + 24 * g;
+        float z[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (int j = 0; j < 24; j++) {
+            const int dd = cd[j];
+            if (dd >= 0) z[j % 3] += ph[j] * ec[dd];
+        }
+#pragma unroll
+        for (int a = 0; a < 3; a++) x[3 * g + a] += z[a];
+    }
+}
+
+// exit of the cycle: y = S_t x (FP64), bb = (r, y) and the Givens step
+__global__ void __launch_bounds__(kVecThreads) k_mg_out(int n, const float* __restrict__ x, const double* __restrict__ st,
+                                                       const double* __restrict__ r, double* __restrict__ y, TlState* S,
+                                                       double* __restrict__ partial, int init)
+{
+    if (S->done) return;
+    __shared__ double sh[32];
+    double acc[1] = {0.0};
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double yi = st[i] * (double)x[i];
+        y[i] = yi;
+        acc[0] += r[i] * yi;
+    }
+    block_sum<1>(acc, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = acc[0];
+    if (arrive_last(&S->ticket[0])) {
+        double t[1];
+        reduce_partials<1>(partial, gridDim.x, 0, t, sh);
+        if (threadIdx.x == 0) {
+            givens_step(S, t[0], init);
+            S->ticket[0] = 0;
+        }
+    }
+}
+
+// psi_t = psi_hat * s_ref / s_t (the prolongation rescaled to the textbook system's Jacobi scaling)
+__global__ void k_mg_psi(int n_fine, const float* __restrict__ psi_hat, const double* __restrict__ s_ref,
+                         const double* __restrict__ s_t, float* __restrict__ psi_t)
+{
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < 24 * (int64_t)n_fine;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t g = t / 24;
+        const int a = (int)(t % 24) % 3;
+        psi_t[t] = (float)((double)psi_hat[t] * s_ref[3 * g + a] / s_t[3 * g + a]);
+    }
+}
+
+// ||y||^2 into *out (power iteration of the smoother set-up)
+__global__ void __launch_bounds__(kVecThreads) k_mg_norm2(int n, const float* __restrict__ y, double* __restrict__ partial,
+                                                         unsigned int* ticket, double* out)
+{
+    __shared__ double sh[32];
+    double acc[1] = {0.0};
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        acc[0] += (double)y[i] * (double)y[i];
+    block_sum<1>(acc, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = acc[0];
+    if (arrive_last(ticket)) {
+        double t[1];
+        reduce_partials<1>(partial, gridDim.x, 0, t, sh);
+        if (threadIdx.x == 0) {
+            *out = t[0];
+            *ticket = 0;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kVecThreads) k_mg_scale(int n, float* __restrict__ v, const double* norm2)
+{
+    const float inv = (float)(*norm2 > 0.0 ? 1.0 / sqrt(*norm2) : 0.0);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        v[i] *= inv;
+}
+
 }  // namespace
 
 struct CoarseHandle {
@@ -661,8 +838,15 @@ struct CoarseHandle {
     DBuf<double> r64, partial;
     DBuf<TlState> st;
     TlState* h_st = nullptr;
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};  // FP32, FP64 iteration graphs
+    cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};  // FP32, FP64, multiplicative iteration graphs
     float ms_setup = 0.f;
+    // multiplicative cycle (msfem_coarse_set_smoother): the textbook-orientation system, the
+    // Chebyshev degree and coefficients, the prolongation in its scaling, cycle vectors
+    System* text = nullptr;
+    int cheb_deg = 0;
+    double lmax = 0.0, lmin = 0.0;
+    ChebCoef cc{};
+    DBuf<float> psi_t, mgv;
     ~CoarseHandle()
     {
         for (auto g : graph)
@@ -991,6 +1175,182 @@ int inner_solve(CoarseHandle& C, int maxiter, double tau, int* iters)
     return C.h_st->done == 3 ? MSFEM_ERR_NUMERIC : MSFEM_OK;
 }
 
+// The multiplicative cycle M^-1 r into y (FP64), with bb = (r, y) and the Givens step.
+// r_in: z (lanczos) or the right-hand side (first application); r_out: where r_new goes.
+void mg_cycle(CoarseHandle& C, const double* z, const double* r2, double* r_out, double* y, int lanczos, int init,
+              cudaStream_t st)
+{
+    System& T = *C.text;
+    const int n = T.n_rows;
+    float* rhat = C.mgv.p;
+    float* res = rhat + n;
+    float* dA = res + n;
+    float* dB = dA + n;
+    float* x = dB + n;
+    float* x2 = x + n;
+    TlState* S = C.st.p;
+    const SellView<float> At = sell_view<float>(T);
+    const unsigned gsp = spmv_grid_of((const void*)k_mg_cheb, T);
+    const unsigned gvec = kReduceBlocks;
+    const double* s_t = T.dscale.p;
+    k_mg_in<<<gvec, kVecThreads, 0, st>>>(n, z, r2, r_out, s_t, rhat, res, dA, x, C.cc, S, lanczos);
+    float* d[2] = {dA, dB};
+    for (int i = 1; i < C.cheb_deg; i++)
+        k_mg_cheb<<<gsp, 256, 0, st>>>(At, d[(i - 1) & 1], d[i & 1], res, x, C.cc.a[i], C.cc.b[i], S);
+    k_mg_resid<<<gsp, 256, 0, st>>>(At, rhat, x, res, nullptr, nullptr, 0.0f, S, 0);
+    k_tl_restrict<float><<<C.n_cells, 128, 0, st>>>(C.own_ptr.p, C.own.p, C.psi_t.p, res, nullptr, nullptr, C.cpart.p,
+                                                    nullptr, S, 0);
+    k_tl_gather<<<gridn(C.n_cf), 256, 0, st>>>(C.n_cf, C.dptr.p, C.dent.p, C.cpart.p, C.rc.p, S);
+    k_tl_gemv<<<gridn((int64_t)C.n_cf * 32), 256, 0, st>>>(C.n_cf, C.n_pad, C.Cinv.p, C.rc.p, C.ec.p, S);
+    k_mg_prolong<<<gvec, kVecThreads, 0, st>>>(C.n_fine, C.owner.p, C.cdof.p, C.psi_t.p, C.ec.p, x, S);
+    k_mg_resid<<<gsp, 256, 0, st>>>(At, rhat, x, res, dA, x2, C.cc.inv_theta, S, 1);
+    for (int i = 1; i < C.cheb_deg; i++)
+        k_mg_cheb<<<gsp, 256, 0, st>>>(At, d[(i - 1) & 1], d[i & 1], res, x2, C.cc.a[i], C.cc.b[i], S);
+    k_mg_out<<<gvec, kVecThreads, 0, st>>>(n, x2, s_t, lanczos ? r_out : z, y, S, C.partial.p, init);
+}
+
+// FP64 MINRES on the original matrix with the multiplicative cycle as preconditioner
+int inner_solve_mg(CoarseHandle& C, int maxiter, double tau, int* iters)
+{
+    System& F = *C.fine;
+    cudaStream_t st = F.stream;
+    const int n = F.n_rows;
+    double* X = C.vec.p;
+    double* V = X + n;
+    double* Z = V + n;
+    double* Y = Z + n;
+    double* R[2] = {Y + n, Y + 2 * (size_t)n};
+    double* Wb[2] = {Y + 3 * (size_t)n, Y + 4 * (size_t)n};
+    TlState* S = C.st.p;
+    const unsigned gvec = kReduceBlocks;
+    k_tl_norm<<<gvec, kVecThreads, 0, st>>>(n, C.r64.p, nullptr, S, C.partial.p);
+    k_tl_rhs<double><<<gvec, kVecThreads, 0, st>>>(n, C.r64.p, nullptr, S, R[0], R[1], X, Wb[0], Wb[1]);
+    MSFEM_TRY(read_st(C, st));
+    TlState h = *C.h_st;
+    h.tol = tau;
+    h.maxiter = maxiter;
+    h.done = 0;
+    h.applied = -1;
+    h.iter = 0;
+    for (auto& t : h.ticket) t = 0;
+    *C.h_st = h;
+    MSFEM_CK(cudaMemcpyAsync(S, C.h_st, sizeof(TlState), cudaMemcpyHostToDevice, st));
+    mg_cycle(C, R[1], nullptr, nullptr, Y, 0, 1, st);
+    const SellView<double> A = sell_view<double>(F);
+    const unsigned gsp = spmv_grid_of((const void*)k_tl_spmv<double>, F);
+    auto two = [&]() {
+        for (int p = 0; p < 2; p++) {
+            double* r1 = R[p];
+            double* r2 = R[1 - p];
+            double* w1 = Wb[p];
+            double* w2 = Wb[1 - p];
+            k_tl_spmv<double><<<gsp, 256, 0, st>>>(A, Y, V, Z, r1, S, C.partial.p + 2048);
+            mg_cycle(C, Z, r2, r1, Y, 1, 0, st);  // r2_new over r1's buffer, then y = M^-1 r2_new
+            k_tl_update<double><<<gvec, kVecThreads, 0, st>>>(n, V, w1, w2, X, S);
+            k_tl_applied<<<1, 1, 0, st>>>(S);
+        }
+    };
+    cudaGraphExec_t& graph = C.graph[2];
+    if (!graph) {
+        cudaGraph_t gr;
+        MSFEM_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        for (int k = 0; k < 8; k++) two();  // 16 iterations per replay
+        cudaError_t e = cudaStreamEndCapture(st, &gr);
+        if (e != cudaSuccess) {
+            set_error("two-level MINRES graph capture failed: %s", cudaGetErrorString(e));
+            return MSFEM_ERR_CUDA;
+        }
+        e = cudaGraphInstantiate(&graph, gr, 0);
+        cudaGraphDestroy(gr);
+        if (e != cudaSuccess) {
+            set_error("two-level MINRES graph instantiate failed: %s", cudaGetErrorString(e));
+            return MSFEM_ERR_CUDA;
+        }
+    }
+    int rounds = 0;
+    for (;;) {
+        MSFEM_TRY(read_st(C, st));
+        if (C.h_st->done) break;
+        if (16 * rounds > maxiter + 32) break;
+        for (int k = 0; k < 4; k++) MSFEM_CK(cudaGraphLaunch(graph, st));
+        rounds += 4;
+        F.total_launches += 4 * 16 * (11 + 2 * (C.cheb_deg - 1));
+    }
+    *iters = C.h_st->iter;
+    return C.h_st->done == 3 ? MSFEM_ERR_NUMERIC : MSFEM_OK;
+}
+
+// Chebyshev smoothing on the textbook system: lambda_max of its Jacobi-scaled FP32 operator by
+// 30 power steps (times 1.05), lambda_min = lambda_max / ratio, and the step coefficients
+int set_smoother(CoarseHandle& C, System& T, int degree, double ratio)
+{
+    System& F = *C.fine;
+    if (T.kind != MSFEM_ELASTIC || T.n_rows != F.n_rows || T.device != F.device) {
+        set_error("msfem_coarse_set_smoother: the textbook system must be an elasticity system on the fine mesh");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    if (degree < 1 || degree > 8 || !(ratio > 1.0)) {
+        set_error("msfem_coarse_set_smoother: degree must be 1..8 and ratio > 1");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    MSFEM_TRY(prepare_sell(T));
+    cudaStream_t st = F.stream;
+    MSFEM_CK(cudaStreamSynchronize(T.stream));
+    const int n = T.n_rows;
+    MSFEM_TRY(C.psi_t.alloc(24 * (size_t)C.n_fine));
+    k_mg_psi<<<gridn(24 * (int64_t)C.n_fine), 256, 0, st>>>(C.n_fine, C.psi_hat.p, F.dscale.p, T.dscale.p, C.psi_t.p);
+    MSFEM_TRY(C.mgv.alloc(6 * (size_t)n));
+    // power iteration from a fixed pseudo-random start
+    std::vector<float> h0(n);
+    for (int i = 0; i < n; i++) h0[i] = (float)((hash32((unsigned)i) & 0xffff) / 65536.0 - 0.5);
+    float* v = C.mgv.p;
+    float* w = v + n;
+    MSFEM_CK(cudaMemcpyAsync(v, h0.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st));
+    DBuf<double> nb;
+    MSFEM_TRY(nb.alloc(2));
+    DBuf<unsigned int> tk;
+    MSFEM_TRY(tk.alloc(1));
+    MSFEM_CK(cudaMemsetAsync(tk.p, 0, sizeof(unsigned int), st));
+    k_mg_norm2<<<kReduceBlocks, kVecThreads, 0, st>>>(n, v, C.partial.p, tk.p, nb.p);
+    k_mg_scale<<<kReduceBlocks, kVecThreads, 0, st>>>(n, v, nb.p);
+    MSFEM_CK(cudaStreamSynchronize(st));
+    double lam = 0.0;
+    for (int it = 0; it < 30; it++) {
+        cudaStream_t ts = T.stream;
+        T.stream = st;  // run the textbook system's SpMV on the solve stream
+        const int rc = spmv32(T, v, w);
+        T.stream = ts;
+        MSFEM_TRY(rc);
+        k_mg_norm2<<<kReduceBlocks, kVecThreads, 0, st>>>(n, w, C.partial.p, tk.p, nb.p);
+        k_mg_scale<<<kReduceBlocks, kVecThreads, 0, st>>>(n, w, nb.p);
+        double nrm2 = 0.0;
+        MSFEM_CK(cudaMemcpyAsync(&nrm2, nb.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+        MSFEM_CK(cudaStreamSynchronize(st));
+        lam = std::sqrt(nrm2);
+        std::swap(v, w);
+    }
+    C.lmax = 1.05 * lam;
+    C.lmin = C.lmax / ratio;
+    const double theta = 0.5 * (C.lmax + C.lmin), delta = 0.5 * (C.lmax - C.lmin), sigma = theta / delta;
+    double rho = 1.0 / sigma;
+    C.cc = ChebCoef{};
+    C.cc.inv_theta = (float)(1.0 / theta);
+    for (int i = 1; i < degree; i++) {
+        const double rn = 1.0 / (2.0 * sigma - rho);
+        C.cc.a[i] = (float)(rn * rho);
+        C.cc.b[i] = (float)(2.0 * rn / delta);
+        rho = rn;
+    }
+    C.cheb_deg = degree;
+    C.text = &T;
+    if (C.graph[2]) {
+        cudaGraphExecDestroy(C.graph[2]);
+        C.graph[2] = nullptr;
+    }
+    MSFEM_CK(cudaGetLastError());
+    return MSFEM_OK;
+}
+
 int solve_twolevel(CoarseHandle& C, int precision, int maxiter, double tol, double* rel, int* iters, int* outer)
 {
     System& F = *C.fine;
@@ -1032,7 +1392,8 @@ int solve_twolevel(CoarseHandle& C, int precision, int maxiter, double tol, doub
         // FP32 stops near its own precision; FP64 aims a little past what is missing
         const double tau = f32 ? std::max(1e-5, std::min(0.5, 0.3 * need)) : std::max(1e-14, 0.1 * need);
         int it = 0;
-        rc = f32 ? inner_solve<float>(C, maxiter - total, tau, &it) : inner_solve<double>(C, maxiter - total, tau, &it);
+        if (C.text && !f32) rc = inner_solve_mg(C, maxiter - total, tau, &it);
+        else rc = f32 ? inner_solve<float>(C, maxiter - total, tau, &it) : inner_solve<double>(C, maxiter - total, tau, &it);
         total += it;
         if (std::getenv("MSFEM_TRACE"))
             std::fprintf(stderr, "[msfem] two-level refine %d (%s): rel %.3e tau %.1e inner %d\n", k, f32 ? "fp32" : "fp64",
@@ -1168,6 +1529,17 @@ int msfem_solve_twolevel(msfem_system_t fine, msfem_coarse_t c, int precision, i
     if (iterations) *iterations = it;
     if (outer) *outer = out;
     return rc;
+}
+
+int msfem_coarse_set_smoother(msfem_coarse_t c, msfem_system_t textbook, int degree, double ratio)
+{
+    using namespace msfem;
+    if (!c || !textbook) {
+        set_error("msfem_coarse_set_smoother: bad arguments");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    MSFEM_CK(cudaSetDevice(c->fine->device));
+    return set_smoother(*c, *reinterpret_cast<System*>(textbook), degree, ratio);
 }
 
 void msfem_coarse_destroy(msfem_coarse_t c)

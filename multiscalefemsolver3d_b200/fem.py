@@ -116,6 +116,13 @@ class System:
         check(load().msfem_assemble_elastic(self.h, e.ctypes.data_as(C.c_void_p), n.ctypes.data_as(C.c_void_p),
                                             e.size), "assemble_elastic")
 
+    def assemble_elastic_textbook(self, E, nu):
+        """The transposed (textbook, SPD) orientation of every element block; for preconditioners."""
+        e = np.ascontiguousarray(E, dtype=np.float64)
+        n = np.ascontiguousarray(nu, dtype=np.float64)
+        check(load().msfem_assemble_elastic_textbook(self.h, e.ctypes.data_as(C.c_void_p),
+                                                     n.ctypes.data_as(C.c_void_p), e.size), "assemble_elastic_textbook")
+
     def add_traction(self, faces, traction):
         pf, d1, k1 = _ptr(faces, np.int32)
         pt, d2, k2 = _ptr(traction, np.float64)

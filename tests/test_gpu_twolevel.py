@@ -83,3 +83,49 @@ def test_twolevel_cuts_iterations(case):
         rel1, it1, rc1 = S.solve(fem.MINRES, prec, tol=1e-8, maxiter=200000)
         assert rc2 == 0 and rc1 == 0
         assert it2 < it1, (prec, it2, it1)
+
+
+def test_textbook_assembly_is_the_blockwise_transpose(case):
+    p, S, cc, cells, dofs, T, P, cdof = case
+    R = fem.System(fem.ELASTIC, p.mesh.xyz, p.mesh.tets, p.mesh.mat)
+    R.assemble_elastic(p.E, p.nu)
+    K = fem.System(fem.ELASTIC, p.mesh.xyz, p.mesh.tets, p.mesh.mat)
+    K.assemble_elastic_textbook(p.E, p.nu)
+    a, b = R.export_csr().to_scipy(), K.export_csr().to_scipy()
+    n = a.shape[0] // 3
+    # block (I, J)[x][y] of the textbook matrix = block (I, J)[y][x] of the reference's
+    perm = np.arange(3 * n)
+    at = a.tocoo()
+    rows, cols = 3 * (at.row // 3) + at.col % 3, 3 * (at.col // 3) + at.row % 3
+    import scipy.sparse as sp
+    a_bt = sp.csr_matrix((at.data, (rows, cols)), shape=a.shape)
+    assert abs(b - a_bt).max() <= 1e-14 * abs(a).max()
+    assert abs(b - b.T).max() <= 1e-14 * abs(b).max()   # symmetric
+    del perm
+
+
+@pytest.fixture(scope="module")
+def mg_case(lib, cuda):
+    p, S, cc, cells, dofs = _setup()
+    K = fem.System(fem.ELASTIC, p.mesh.xyz, p.mesh.tets, p.mesh.mat)
+    K.assemble_elastic_textbook(p.E, p.nu)
+    K.apply_dirichlet(dofs, np.zeros(dofs.size), fem.ROW_AND_COLUMN)
+    T = TwoLevel(S, cells, cc, dofs)
+    T.set_smoother(K, degree=3, ratio=30.0)
+    return p, S, K, T, dofs
+
+
+def test_multiplicative_cycle_solve(mg_case):
+    """MINRES (FP64) on the reference's indefinite matrix with the multiplicative two-level cycle on
+    the textbook operator: the exact solution to 1e-8, in fewer iterations than Jacobi MINRES."""
+    p, S, K, T, dofs = mg_case
+    A = S.export_csr()
+    x_exact = spl.spsolve(A.to_scipy().tocsc(), A.F)
+    S.set_x(np.zeros(A.n))
+    rel, it_mg, outer, rc = T.solve(tol=1e-12, maxiter=20000, precision=FP64)
+    assert rc == 0 and rel <= 1e-12
+    assert np.linalg.norm(S.get_x() - x_exact) <= 1e-8 * np.linalg.norm(x_exact)
+    S.set_x(np.zeros(A.n))
+    rel1, it_j, rc1 = S.solve(fem.MINRES, FP64, tol=1e-12, maxiter=200000)
+    assert rc1 == 0
+    assert it_mg < it_j / 2, (it_mg, it_j)
