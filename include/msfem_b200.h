@@ -330,8 +330,11 @@ int msfem_solve_twolevel(msfem_system_t fine, msfem_coarse_t c, int precision, i
  * msfem_assemble_elastic_textbook and given the same Dirichlet rows.  One application of M^-1:
  * `degree` Chebyshev steps on its Jacobi-scaled FP32 matrix (spectrum bound [lmax/ratio, lmax],
  * lmax from 30 power steps), the coarse correction, the same Chebyshev steps again; SPD, so
- * MINRES on the reference's matrix keeps its guarantees.  The textbook system must outlive c. */
-int msfem_coarse_set_smoother(msfem_coarse_t c, msfem_system_t textbook, int degree, double ratio);
+ * MINRES on the reference's matrix keeps its guarantees.  half_matrix = 1 stores the smoother's
+ * matrix values in FP16 (arithmetic stays FP32; rounding each entry keeps the matrix symmetric, so
+ * the cycle stays SPD; it halves the bytes of the 2*degree SpMVs per cycle).  The textbook system
+ * must outlive c. */
+int msfem_coarse_set_smoother(msfem_coarse_t c, msfem_system_t textbook, int degree, double ratio, int half_matrix);
 void msfem_coarse_destroy(msfem_coarse_t c);
 
 #ifdef __cplusplus

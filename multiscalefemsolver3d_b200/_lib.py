@@ -94,7 +94,7 @@ _SIGS = [
     ("msfem_coarse_apply", C.c_int, [C.c_void_p, _P, _P]),
     ("msfem_solve_twolevel", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double, C.POINTER(C.c_double),
                                        C.POINTER(C.c_int), C.POINTER(C.c_int)]),
-    ("msfem_coarse_set_smoother", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_double]),
+    ("msfem_coarse_set_smoother", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_int]),
     ("msfem_coarse_destroy", None, [C.c_void_p]),
 ]
 

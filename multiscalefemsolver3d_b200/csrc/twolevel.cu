@@ -31,6 +31,7 @@
 // application (restriction per cell -> coarse gather -> dense GEMV -> prolongation)
 // and two inner products, in six kernels captured as a CUDA graph.
 #include <cub/cub.cuh>
+#include <cuda_fp16.h>
 
 #include <algorithm>
 #include <cmath>
@@ -652,6 +653,39 @@ __global__ void __launch_bounds__(kVecThreads) k_tl_correct(int n, double* __res
 // Jacobi-scaled space K^ = S_t K_t S_t): pre-smoothing by k Chebyshev steps, coarse correction
 // with P^_t = S_t^-1 P, post-smoothing by the same k steps.  M^-1 r = S_t cycle(S_t r).
 
+// 3x3-block SELL row times x with the values stored in FP32 or, when v16 is set, in FP16
+// (same layout); FP32 arithmetic either way
+__device__ __forceinline__ void sell_row_block_mixed(const SellView<float>& A, const __half* __restrict__ v16, int warp,
+                                                     int lane, const float* __restrict__ x, float (&acc)[3])
+{
+    if (!v16) {
+        sell_row_block<float>(A, warp, lane, x, acc);
+        return;
+    }
+    const int64_t base = A.sp[warp];
+    const int w = (int)((A.sp[warp + 1] - base) >> 5);
+    acc[0] = acc[1] = acc[2] = 0.0f;
+#pragma unroll 2
+    for (int k = 0; k < w; k++) {
+        const int64_t blk = base + (int64_t)k * kSlice;
+        const int c = __ldcs(A.col + blk + lane);
+        const __half* vb = v16 + 9 * blk + lane;
+        const float x0 = __ldg(x + 3 * (int64_t)c), x1 = __ldg(x + 3 * (int64_t)c + 1), x2 = __ldg(x + 3 * (int64_t)c + 2);
+        float v[9];
+#pragma unroll
+        for (int e = 0; e < 9; e++) v[e] = __half2float(__ldcs(vb + e * kSlice));
+        acc[0] += v[0] * x0 + v[1] * x1 + v[2] * x2;
+        acc[1] += v[3] * x0 + v[4] * x1 + v[5] * x2;
+        acc[2] += v[6] * x0 + v[7] * x1 + v[8] * x2;
+    }
+}
+
+__global__ void k_to_half(int64_t n, const float* __restrict__ a, __half* __restrict__ h)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        h[i] = __float2half_rn(a[i]);
+}
+
 struct ChebCoef {
     float inv_theta;   // first step: d = res / theta
     float a[8], b[8];  // step i >= 1: d_i = a_i d_{i-1} + b_i res_i
@@ -683,7 +717,8 @@ __global__ void __launch_bounds__(kVecThreads) k_mg_in(int n, const double* __re
 }
 
 // one Chebyshev step: res -= K^ d_prev; d = a d_prev + b res; x += d
-__global__ void __launch_bounds__(256) k_mg_cheb(SellView<float> A, const float* __restrict__ dprev,
+__global__ void __launch_bounds__(256) k_mg_cheb(SellView<float> A, const __half* __restrict__ v16,
+                                                 const float* __restrict__ dprev,
                                                  float* __restrict__ d, float* __restrict__ res, float* __restrict__ x,
                                                  float a, float b, const TlState* S)
 {
@@ -692,7 +727,7 @@ __global__ void __launch_bounds__(256) k_mg_cheb(SellView<float> A, const float*
     const int nw = (gridDim.x * blockDim.x) >> 5;
     for (int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; warp < A.n_slices; warp += nw) {
         float kd[3];
-        sell_row_block<float>(A, warp, lane, dprev, kd);
+        sell_row_block_mixed(A, v16, warp, lane, dprev, kd);
         const int brow = warp * kSlice + lane;
         if (brow < A.n_brows)
             for (int c = 0; c < 3; c++) {
@@ -708,7 +743,8 @@ __global__ void __launch_bounds__(256) k_mg_cheb(SellView<float> A, const float*
 
 // res = rhat - K^ x; with `start`: also the first post-smoothing step d = res / theta,
 // x2 = x + d (into a second buffer: x is being gathered)
-__global__ void __launch_bounds__(256) k_mg_resid(SellView<float> A, const float* __restrict__ rhat,
+__global__ void __launch_bounds__(256) k_mg_resid(SellView<float> A, const __half* __restrict__ v16,
+                                                  const float* __restrict__ rhat,
                                                   const float* __restrict__ x, float* __restrict__ res,
                                                   float* __restrict__ d, float* __restrict__ x2, float inv_theta,
                                                   const TlState* S, int start)
@@ -718,7 +754,7 @@ __global__ void __launch_bounds__(256) k_mg_resid(SellView<float> A, const float
     const int nw = (gridDim.x * blockDim.x) >> 5;
     for (int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; warp < A.n_slices; warp += nw) {
         float kx[3];
-        sell_row_block<float>(A, warp, lane, x, kx);
+        sell_row_block_mixed(A, v16, warp, lane, x, kx);
         const int brow = warp * kSlice + lane;
         if (brow < A.n_brows)
             for (int c = 0; c < 3; c++) {
@@ -847,6 +883,8 @@ struct CoarseHandle {
     double lmax = 0.0, lmin = 0.0;
     ChebCoef cc{};
     DBuf<float> psi_t, mgv;
+    DBuf<__half> val16;  // FP16 copy of the textbook system's scaled SELL values (when requested)
+    bool half_matrix = false;
     ~CoarseHandle()
     {
         for (auto g : graph)
@@ -1193,19 +1231,20 @@ void mg_cycle(CoarseHandle& C, const double* z, const double* r2, double* r_out,
     const unsigned gsp = spmv_grid_of((const void*)k_mg_cheb, T);
     const unsigned gvec = kReduceBlocks;
     const double* s_t = T.dscale.p;
+    const __half* v16 = C.half_matrix ? C.val16.p : nullptr;
     k_mg_in<<<gvec, kVecThreads, 0, st>>>(n, z, r2, r_out, s_t, rhat, res, dA, x, C.cc, S, lanczos);
     float* d[2] = {dA, dB};
     for (int i = 1; i < C.cheb_deg; i++)
-        k_mg_cheb<<<gsp, 256, 0, st>>>(At, d[(i - 1) & 1], d[i & 1], res, x, C.cc.a[i], C.cc.b[i], S);
-    k_mg_resid<<<gsp, 256, 0, st>>>(At, rhat, x, res, nullptr, nullptr, 0.0f, S, 0);
+        k_mg_cheb<<<gsp, 256, 0, st>>>(At, v16, d[(i - 1) & 1], d[i & 1], res, x, C.cc.a[i], C.cc.b[i], S);
+    k_mg_resid<<<gsp, 256, 0, st>>>(At, v16, rhat, x, res, nullptr, nullptr, 0.0f, S, 0);
     k_tl_restrict<float><<<C.n_cells, 128, 0, st>>>(C.own_ptr.p, C.own.p, C.psi_t.p, res, nullptr, nullptr, C.cpart.p,
                                                     nullptr, S, 0);
     k_tl_gather<<<gridn(C.n_cf), 256, 0, st>>>(C.n_cf, C.dptr.p, C.dent.p, C.cpart.p, C.rc.p, S);
     k_tl_gemv<<<gridn((int64_t)C.n_cf * 32), 256, 0, st>>>(C.n_cf, C.n_pad, C.Cinv.p, C.rc.p, C.ec.p, S);
     k_mg_prolong<<<gvec, kVecThreads, 0, st>>>(C.n_fine, C.owner.p, C.cdof.p, C.psi_t.p, C.ec.p, x, S);
-    k_mg_resid<<<gsp, 256, 0, st>>>(At, rhat, x, res, dA, x2, C.cc.inv_theta, S, 1);
+    k_mg_resid<<<gsp, 256, 0, st>>>(At, v16, rhat, x, res, dA, x2, C.cc.inv_theta, S, 1);
     for (int i = 1; i < C.cheb_deg; i++)
-        k_mg_cheb<<<gsp, 256, 0, st>>>(At, d[(i - 1) & 1], d[i & 1], res, x2, C.cc.a[i], C.cc.b[i], S);
+        k_mg_cheb<<<gsp, 256, 0, st>>>(At, v16, d[(i - 1) & 1], d[i & 1], res, x2, C.cc.a[i], C.cc.b[i], S);
     k_mg_out<<<gvec, kVecThreads, 0, st>>>(n, x2, s_t, lanczos ? r_out : z, y, S, C.partial.p, init);
 }
 
@@ -1282,7 +1321,7 @@ int inner_solve_mg(CoarseHandle& C, int maxiter, double tau, int* iters)
 
 // Chebyshev smoothing on the textbook system: lambda_max of its Jacobi-scaled FP32 operator by
 // 30 power steps (times 1.05), lambda_min = lambda_max / ratio, and the step coefficients
-int set_smoother(CoarseHandle& C, System& T, int degree, double ratio)
+int set_smoother(CoarseHandle& C, System& T, int degree, double ratio, int half_matrix)
 {
     System& F = *C.fine;
     if (T.kind != MSFEM_ELASTIC || T.n_rows != F.n_rows || T.device != F.device) {
@@ -1343,6 +1382,12 @@ int set_smoother(CoarseHandle& C, System& T, int degree, double ratio)
     }
     C.cheb_deg = degree;
     C.text = &T;
+    C.half_matrix = half_matrix != 0;
+    if (C.half_matrix) {
+        const int64_t nv = (int64_t)9 * T.sell.stored;
+        MSFEM_TRY(C.val16.alloc(nv));
+        k_to_half<<<gridn(nv), 256, 0, st>>>(nv, T.sell.val32.p, C.val16.p);
+    }
     if (C.graph[2]) {
         cudaGraphExecDestroy(C.graph[2]);
         C.graph[2] = nullptr;
@@ -1390,7 +1435,9 @@ int solve_twolevel(CoarseHandle& C, int precision, int maxiter, double tol, doub
         prev = r2;
         const double need = tol * std::sqrt(ff / r2);
         // FP32 stops near its own precision; FP64 aims a little past what is missing
-        const double tau = f32 ? std::max(1e-5, std::min(0.5, 0.3 * need)) : std::max(1e-14, 0.1 * need);
+        // (the multiplicative cycle's M-norm is further from the 2-norm: aim lower, one pass)
+        const double tau = f32 ? std::max(1e-5, std::min(0.5, 0.3 * need))
+                               : std::max(1e-14, (C.text ? 0.02 : 0.1) * need);
         int it = 0;
         if (C.text && !f32) rc = inner_solve_mg(C, maxiter - total, tau, &it);
         else rc = f32 ? inner_solve<float>(C, maxiter - total, tau, &it) : inner_solve<double>(C, maxiter - total, tau, &it);
@@ -1531,7 +1578,7 @@ int msfem_solve_twolevel(msfem_system_t fine, msfem_coarse_t c, int precision, i
     return rc;
 }
 
-int msfem_coarse_set_smoother(msfem_coarse_t c, msfem_system_t textbook, int degree, double ratio)
+int msfem_coarse_set_smoother(msfem_coarse_t c, msfem_system_t textbook, int degree, double ratio, int half_matrix)
 {
     using namespace msfem;
     if (!c || !textbook) {
@@ -1539,7 +1586,7 @@ int msfem_coarse_set_smoother(msfem_coarse_t c, msfem_system_t textbook, int deg
         return MSFEM_ERR_ARGUMENT;
     }
     MSFEM_CK(cudaSetDevice(c->fine->device));
-    return set_smoother(*c, *reinterpret_cast<System*>(textbook), degree, ratio);
+    return set_smoother(*c, *reinterpret_cast<System*>(textbook), degree, ratio, half_matrix);
 }
 
 void msfem_coarse_destroy(msfem_coarse_t c)

@@ -47,11 +47,13 @@ class TwoLevel:
                                                C.byref(it), C.byref(out)), "solve_twolevel")
         return rel.value, it.value, out.value, rc
 
-    def set_smoother(self, textbook_system, degree=3, ratio=30.0):
+    def set_smoother(self, textbook_system, degree=3, ratio=30.0, half_matrix=False):
         """Multiplicative cycle with Chebyshev smoothing on the textbook-orientation system
-        (fem.System assembled with assemble_elastic_textbook, same Dirichlet rows)."""
+        (fem.System assembled with assemble_elastic_textbook, same Dirichlet rows); half_matrix
+        stores the smoother's matrix values in FP16."""
         self._text = textbook_system
-        check(load().msfem_coarse_set_smoother(self.h, textbook_system.h, degree, ratio), "coarse_set_smoother")
+        check(load().msfem_coarse_set_smoother(self.h, textbook_system.h, degree, ratio, int(half_matrix)),
+              "coarse_set_smoother")
 
     def coarse_matrix(self):
         A = np.empty((self.n_coarse_dofs, self.n_coarse_dofs))

@@ -104,20 +104,21 @@ def test_textbook_assembly_is_the_blockwise_transpose(case):
     del perm
 
 
-@pytest.fixture(scope="module")
-def mg_case(lib, cuda):
+@pytest.fixture(scope="module", params=[False, True], ids=["fp32-smoother", "fp16-smoother"])
+def mg_case(lib, cuda, request):
     p, S, cc, cells, dofs = _setup()
     K = fem.System(fem.ELASTIC, p.mesh.xyz, p.mesh.tets, p.mesh.mat)
     K.assemble_elastic_textbook(p.E, p.nu)
     K.apply_dirichlet(dofs, np.zeros(dofs.size), fem.ROW_AND_COLUMN)
     T = TwoLevel(S, cells, cc, dofs)
-    T.set_smoother(K, degree=3, ratio=30.0)
+    T.set_smoother(K, degree=3, ratio=30.0, half_matrix=request.param)
     return p, S, K, T, dofs
 
 
 def test_multiplicative_cycle_solve(mg_case):
     """MINRES (FP64) on the reference's indefinite matrix with the multiplicative two-level cycle on
-    the textbook operator: the exact solution to 1e-8, in fewer iterations than Jacobi MINRES."""
+    the textbook operator (smoother matrix in FP32 or FP16): the exact solution to 1e-8, in fewer
+    iterations than Jacobi MINRES."""
     p, S, K, T, dofs = mg_case
     A = S.export_csr()
     x_exact = spl.spsolve(A.to_scipy().tocsc(), A.F)
