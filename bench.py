@@ -64,6 +64,7 @@ def parse():
     ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--sample-n", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-compare", action="store_true", help="elastic: skip the plain CG / Jacobi MINRES runs")
     a = ap.parse_args()
     if a.n is None:
         a.n = 100 if a.config == "electrostatics" else 128
@@ -626,12 +627,172 @@ def run_reference_cells(args, D):
     print(json.dumps(line))
 
 
+# ---------------------------------------------------------------- 128^3 elasticity, two-level MINRES
+
+def run_twolevel(args, D):
+    """128^3 heterogeneous elasticity (2000 spheres, E 1:100): MINRES in FP64 on the reference's
+    (indefinite) matrix, preconditioned by the symmetric multiplicative two-level cycle: FP16/FP32
+    Chebyshev smoothing on the textbook-orientation operator and the MsFEM coarse space built from
+    the batched cell bases (FP32 inner solves + FP64 check) with an FP64-inverted coarse matrix."""
+    import torch
+    from multiscalefemsolver3d_b200 import _lib, fem, meshgen
+    from multiscalefemsolver3d_b200.cells import FP32_IR, FP64, Cells
+    from multiscalefemsolver3d_b200.twolevel import TwoLevel
+
+    torch.cuda.set_device(D.local)
+    dev = torch.device("cuda", D.local)
+    p = workload(args.n, "elastic")
+    m = p.mesh
+    t_host = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    xyz, tets, mat = t_host(m.xyz), t_host(m.tets), t_host(m.mat)
+    dofs_np = (3 * p.bc_nodes[:, None] + np.arange(3)).ravel().astype(np.int32)
+    dofs, zval = t_host(dofs_np), torch.zeros(dofs_np.size, dtype=torch.float64, device=dev)
+    faces, trac = t_host(p.faces), t_host(p.traction)
+    xzero = torch.zeros(3 * m.n_nodes, dtype=torch.float64, device=dev)
+    H = 8
+    cc = meshgen.cube_cells(m, p.E, p.nu, H)
+    # portraits and cell topology: built once, as the electrostatics bench builds its portrait once
+    S = fem.System(fem.ELASTIC, xyz, tets, mat)
+    K = fem.System(fem.ELASTIC, xyz, tets, mat)
+    C = Cells(cc.cells)
+    stream = torch.cuda.ExternalStream(S.stream, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    DEG, HALF = 3, True
+
+    def step():
+        S.clear()
+        S.add_traction(faces, trac)
+        S.assemble_elastic(p.E, p.nu)
+        S.apply_dirichlet(dofs, zval, fem.ROW_AND_COLUMN)
+        K.clear()
+        K.assemble_elastic_textbook(p.E, p.nu)
+        K.apply_dirichlet(dofs, zval, fem.ROW_AND_COLUMN)
+        rcb = C.build_bases(FP32_IR, TOL)
+        if rcb != 0:
+            raise RuntimeError(f"cell bases rc={rcb}")
+        T = TwoLevel(S, C, cc, dofs_np)
+        T.set_smoother(K, degree=DEG, half_matrix=HALF)
+        S.set_x(xzero)
+        rel, it, out, rc = T.solve(tol=TOL, maxiter=400000, precision=FP64)
+        info = {"rel_residual": rel, "iterations": it, "refinement_steps": out, "coarse_dofs": T.n_coarse_dofs,
+                "coarse_setup_ms": T.ms_setup, "ms_solve": S.stats()["ms_solve"], "ms_bases": sum(C.report()["ms"].values())}
+        T.close()
+        if rc != 0:
+            raise RuntimeError(f"two-level solve rc={rc} rel={rel}")
+        return info
+
+    for _ in range(args.warmup):
+        step()
+    launches0 = S.stats()["total_launches"]
+    D.barrier()
+    torch.cuda.synchronize()
+    ts, infos = [], []
+    with Clocks(D.local) as clk:
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            infos.append(step())
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+    launches = (S.stats()["total_launches"] - launches0) // max(1, args.steps)
+    torch.cuda.synchronize()
+    D.barrier()
+    ms = D.max(statistics.mean(ts))
+    info = infos[-1]
+
+    # comparators on the same (assembled) system
+    comp = {}
+    if not args.no_compare:
+        S.set_x(xzero)
+        rel, it, rc = S.solve(fem.CG, FP64, tol=TOL, maxiter=2000)
+        cg_ms_it = S.stats()["ms_solve"] / max(1, it)
+        budget = int(5.0 * ms / cg_ms_it) + 1
+        S.set_x(xzero)
+        rel, it, rc = S.solve(fem.CG, FP64, tol=TOL, maxiter=budget)
+        comp.update({"plain_fp64_cg_ms": S.stats()["ms_solve"], "plain_fp64_cg_iterations": it,
+                     "plain_fp64_cg_rel_residual": rel, "plain_fp64_cg_reached_tol": bool(rc == 0),
+                     "plain_fp64_cg_budget": "5x the two-level step time"})
+        S.set_x(xzero)
+        rel, it, rc = S.solve(fem.MINRES, FP64, tol=TOL, maxiter=400000)
+        comp.update({"jacobi_fp64_minres_ms": S.stats()["ms_solve"], "jacobi_fp64_minres_iterations": it,
+                     "jacobi_fp64_minres_rel_residual": rel})
+    spmv32_ms, spmv_bytes32 = K.bench_spmv(FP32_IR, reps=100)
+    spmv64_ms, spmv_bytes64 = S.bench_spmv(FP64, reps=100)
+    peak, peak_kind = peaks()
+    ach = spmv_bytes32 / (spmv32_ms * 1e-3) / 1e9
+    S.close()
+    K.close()
+    C.close()
+
+    # e2e: host arrays in (mesh, materials, boundary data), portraits, cells, step, solution out
+    def e2e_call():
+        S2 = fem.System(fem.ELASTIC, m.xyz, m.tets, m.mat)
+        K2 = fem.System(fem.ELASTIC, m.xyz, m.tets, m.mat)
+        C2 = Cells(cc.cells)
+        S2.add_traction(p.faces, p.traction)
+        S2.assemble_elastic(p.E, p.nu)
+        S2.apply_dirichlet(dofs_np, np.zeros(dofs_np.size), fem.ROW_AND_COLUMN)
+        K2.assemble_elastic_textbook(p.E, p.nu)
+        K2.apply_dirichlet(dofs_np, np.zeros(dofs_np.size), fem.ROW_AND_COLUMN)
+        C2.build_bases(FP32_IR, TOL)
+        T2 = TwoLevel(S2, C2, cc, dofs_np)
+        T2.set_smoother(K2, degree=DEG, half_matrix=HALF)
+        S2.set_x(np.zeros(3 * m.n_nodes))
+        rel, it, out, rc = T2.solve(tol=TOL, maxiter=400000, precision=FP64)
+        sol = S2.get_x()
+        T2.close(), C2.close(), K2.close(), S2.close()
+        if rc != 0:
+            raise RuntimeError(f"e2e two-level rc={rc}")
+        return sol
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sol = e2e_call()
+    torch.cuda.synchronize()
+    e2e_ms = D.max((time.perf_counter() - t0) * 1e3)
+    h2d = sum(a.nbytes for a in (m.xyz, m.tets, m.mat, p.faces, p.traction, dofs_np, cc.cells.xyz, cc.cells.tets,
+                                 cc.cells.mat, cc.cells.node_off, cc.cells.tet_off, cc.cells.box,
+                                 cc.cell_node_global, cc.cell_vertex)) * 1
+    d2h = sol.nbytes
+    base = None
+    if D.rank == 0 and D.world == 1 and not args.no_cpu_baseline:
+        base = cpu_baseline(args.n, args.sample_n, "elastic")
+    if D.rank == 0:
+        extra = dict(info)
+        extra.update(comp)
+        extra.update({"speedup_vs_jacobi_fp64_minres": (comp["jacobi_fp64_minres_ms"] / ms) if comp else None,
+                      "smoother": f"Chebyshev degree {DEG} on the textbook operator, matrix values in "
+                                  f"{'FP16' if HALF else 'FP32'}, FP32 arithmetic; coarse: 8^3-hexahedron MsFEM cells",
+                      "spmv_fp32_ms": spmv32_ms, "spmv_fp32_gbs": ach, "spmv_fp64_ms": spmv64_ms,
+                      "spmv_fp64_gbs": spmv_bytes64 / (spmv64_ms * 1e-3) / 1e9, "step_ms_all": ts})
+        c = config(args.n, "elastic", extra)
+        c["solver"] = ("MINRES (FP64) preconditioned by the multiplicative two-level cycle; one step = assembly "
+                       "(reference and textbook orientation) + Dirichlet + cell bases + coarse setup + solve")
+        line = {"metric": METRIC, "value": ms, "unit": UNIT, "n_gpus": D.world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64-krylov+fp32/fp16-preconditioner", "data": "synthetic",
+                "config": c,
+                "e2e": {"value": e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+                "gpu_launches": int(launches),
+                "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                             "traffic": None, "kernel": "k_spmv<float> (SELL-32, FP32, 3x3 blocks)",
+                             "peak_source": f"{peak_kind} hbm_gbs"},
+                "cpu_baseline": base,
+                "clocks": clk.summary()}
+        print(json.dumps(line))
+
+
 def main():
     args = parse()
     D = Dist(args.gpus)
     try:
         if args.config == "cells":
             (run_reference_cells if args.impl == "reference" else run_cells)(args, D)
+        elif args.config == "elastic" and args.impl != "reference":
+            run_twolevel(args, D)
         elif args.impl == "reference":
             run_reference(args, D)
         else:
