@@ -50,10 +50,17 @@ struct NeumannScal {
 
 int g_quiet = 1;
 
-/* Redirects fd 1 to /dev/null for the lifetime of the object when quiet. */
+/* Redirects fd 1 to /dev/null for the lifetime of the object when quiet, and fd 0 from
+ * /dev/null always: the reference's drivers wait on scanf_s when a solve reports trouble
+ * (FEM/FEM.h:1933-1937, :3782-3786), which must return at once instead of blocking on a
+ * caller's open stdin. */
 struct StdoutSilencer {
     int saved = -1;
+    int saved_in = -1;
     StdoutSilencer() {
+        saved_in = dup(0);
+        int nin = open("/dev/null", O_RDONLY);
+        if (nin >= 0) { dup2(nin, 0); close(nin); }
         if (!g_quiet) return;
         fflush(stdout);
         saved = dup(1);
@@ -61,6 +68,7 @@ struct StdoutSilencer {
         if (nul >= 0) { dup2(nul, 1); close(nul); }
     }
     ~StdoutSilencer() {
+        if (saved_in >= 0) { dup2(saved_in, 0); close(saved_in); }
         if (saved < 0) return;
         fflush(stdout);
         dup2(saved, 1);
