@@ -282,6 +282,16 @@ int msfem_cells_get_bases(msfem_cells_t c, double* bases, int on_device);
  * and volume launches used (autotuned when build_bases got threads <= 0). */
 int msfem_cells_report(msfem_cells_t c, int32_t* inner_iterations, int32_t* outer_iterations, double* rel_residual,
                        double* face_rel_residual, double* ms, int32_t* threads);
+/* The MsFEM macro element matrices of every cell from its current bases
+ * (FiniteElement_forMech_Poly_Order1::SolveLocalMatrix, MsFEM/MsFEM_Grid.h:3837-3975):
+ * the polyhedron quadrature of Library/GeometryShape.h:2708-2760 (for each face cycle of the
+ * box (x0: 0 2 6 4, x1: 1 3 7 5, y0: 0 1 5 4, y1: 2 3 7 6, z0: 0 1 3 2, z1: 4 5 7 6) and each
+ * face edge, the sub-tetrahedron centroid / face centroid / edge with the 4-point rule), the
+ * basis gradients of the micro tetrahedron holding each point (the lowest index on ties), and the
+ * material of domain 0 for every cell (MsFEM/MsFEM.h:644-647).
+ * K: [n_cells][8][8][3][3] doubles, K[c][I][J] = sum_q w_q B_J^T D B_I as the reference stores
+ * A[I][J]. */
+int msfem_cells_macro_matrices(msfem_cells_t c, double* K, int on_device);
 void msfem_cells_destroy(msfem_cells_t c);
 
 

@@ -93,6 +93,12 @@ class Cells:
         check(load().msfem_cells_get_bases(self.h, _p(out), 0), "cells_get_bases")
         return out
 
+    def macro_matrices(self):
+        """[n_cells, 8, 8, 3, 3] MsFEM macro element matrices from the current bases."""
+        K = np.empty((self.n_cells, 8, 8, 3, 3))
+        check(load().msfem_cells_macro_matrices(self.h, _p(K), 0), "cells_macro_matrices")
+        return K
+
     def report(self):
         n = self.n_cells
         it, out = np.zeros(n, np.int32), np.zeros(n, np.int32)

@@ -34,6 +34,7 @@
 #include "batch.cuh"
 #include "cells.cuh"
 #include "devutil.cuh"
+#include "element.cuh"
 #include "internal.cuh"
 
 namespace msfem {
@@ -397,6 +398,142 @@ __global__ void k_volume_dirichlet(int64_t n_nodes, const int32_t* __restrict__ 
             }
             for (int q = 0; q < 3; q++) o[3 * v + q] = val[q];
         }
+    }
+}
+
+
+// ---- MsFEM macro element matrices (FiniteElement_forMech_Poly_Order1::SolveLocalMatrix,
+// MsFEM_Grid.h:3837-3975): the polyhedron quadrature (sub-tetrahedra centroid / face centroid /
+// face edge, 4-point rule each, GeometryShape.h:2708-2760, :1754-1851), the basis gradients of
+// the micro tetrahedron holding each point (the reference's nearest-element lookup,
+// GeometryGrid.h:323-340; the lowest index among ties), and D of material 0 for every cell
+// (MsFEM.h:644-647).  K[c][I][J][r][s] = sum_q w_q (B_J^T D B_I)[r][s].
+
+constexpr int kMacroQ = 96;
+__constant__ int c_face_cycles[6][4] = {{0, 2, 6, 4}, {1, 3, 7, 5}, {0, 1, 5, 4}, {2, 3, 7, 6}, {0, 1, 3, 2}, {4, 5, 7, 6}};
+
+__device__ __forceinline__ void box_vertex(const double* bx, int v, double p[3])
+{
+    p[0] = bx[0 + (v & 1)];
+    p[1] = bx[2 + ((v >> 1) & 1)];
+    p[2] = bx[4 + ((v >> 2) & 1)];
+}
+
+// column a of the strain matrix of the component-wise basis e_a psi^a (Voigt xx yy zz xy yz zx,
+// engineering shear; the rows of MsFEM_Grid.h:3868-3885), from G[comp][deriv]
+__device__ __forceinline__ void strain_column(const double* G, int a, double b[6])
+{
+    for (int k = 0; k < 6; k++) b[k] = 0.0;
+    b[a] = G[3 * a + a];
+    if (a == 0) {
+        b[3] = G[1];
+        b[5] = G[2];
+    } else if (a == 1) {
+        b[3] = G[3];
+        b[4] = G[5];
+    } else {
+        b[4] = G[7];
+        b[5] = G[6];
+    }
+}
+
+__global__ void __launch_bounds__(256) k_macro_cells(const int64_t* __restrict__ tet_off, const int32_t* __restrict__ tets,
+                                                     const double* __restrict__ xyz, const double* __restrict__ box,
+                                                     const double* __restrict__ bases, const double* __restrict__ lame,
+                                                     double* __restrict__ K, int* bad)
+{
+    extern __shared__ double sm[];
+    double* sG = sm;                                 // [96][8][9]
+    double* sP = sG + kMacroQ * 72;                  // [96][3]
+    double* sW = sP + kMacroQ * 3;                   // [96]
+    int* sT = reinterpret_cast<int*>(sW + kMacroQ);  // [96]
+    const int c = blockIdx.x, tid = threadIdx.x;
+    const double* bx = box + 6 * c;
+    if (tid < kMacroQ) {
+        const int f = tid / 16, i = (tid / 4) % 4, j = tid % 4;
+        double C[3] = {0, 0, 0}, F[3] = {0, 0, 0}, a[3], b[3];
+        for (int v = 0; v < 8; v++) {
+            double p[3];
+            box_vertex(bx, v, p);
+            for (int d = 0; d < 3; d++) C[d] += 0.125 * p[d];
+        }
+        for (int k = 0; k < 4; k++) {
+            double p[3];
+            box_vertex(bx, c_face_cycles[f][k], p);
+            for (int d = 0; d < 3; d++) F[d] += 0.25 * p[d];
+        }
+        box_vertex(bx, c_face_cycles[f][i], a);
+        box_vertex(bx, c_face_cycles[f][(i + 1) % 4], b);
+        double E1[3], E2[3], E3[3];
+        for (int d = 0; d < 3; d++) {
+            E1[d] = F[d] - C[d];
+            E2[d] = a[d] - C[d];
+            E3[d] = b[d] - C[d];
+        }
+        const double det = E1[0] * (E2[1] * E3[2] - E2[2] * E3[1]) - E1[1] * (E2[0] * E3[2] - E2[2] * E3[0]) +
+                           E1[2] * (E2[0] * E3[1] - E2[1] * E3[0]);
+        const double u = (5.0 - sqrt(5.0)) / 20.0, vv = 1.0 - 3.0 * u;
+        const double bar[3] = {j == 1 ? vv : u, j == 2 ? vv : u, j == 3 ? vv : u};
+        for (int d = 0; d < 3; d++) sP[3 * tid + d] = C[d] + bar[0] * E1[d] + bar[1] * E2[d] + bar[2] * E3[d];
+        sW[tid] = fabs(det) / 24.0;
+        sT[tid] = 0x7fffffff;
+    }
+    __syncthreads();
+    const int64_t t0 = tet_off[c], t1 = tet_off[c + 1];
+    for (int64_t e = t0 + tid; e < t1; e += blockDim.x) {
+        int v[4];
+        for (int k = 0; k < 4; k++) v[k] = tets[4 * e + k];
+        TetGeom G;
+        tet_geometry(xyz, v, G);
+        const double* p0 = xyz + 3 * (int64_t)v[0];
+        for (int q = 0; q < kMacroQ; q++) {
+            const double dx[3] = {sP[3 * q] - p0[0], sP[3 * q + 1] - p0[1], sP[3 * q + 2] - p0[2]};
+            bool in = true;
+            for (int k = 0; k < 4; k++) {
+                const double lam = (k == 0 ? 1.0 : 0.0) + G.g[k][0] * dx[0] + G.g[k][1] * dx[1] + G.g[k][2] * dx[2];
+                in = in && lam >= -1e-12;
+            }
+            if (in) atomicMin(&sT[q], (int)(e - t0));
+        }
+    }
+    __syncthreads();
+    for (int t = tid; t < kMacroQ * 8; t += blockDim.x) {
+        const int q = t / 8, I = t % 8;
+        double* out = sG + 72 * q + 9 * I;
+        if (sT[q] == 0x7fffffff) {
+            atomicExch(bad, 1);
+            for (int k = 0; k < 9; k++) out[k] = 0.0;
+            continue;
+        }
+        const int64_t e = t0 + sT[q];
+        int v[4];
+        for (int k = 0; k < 4; k++) v[k] = tets[4 * e + k];
+        TetGeom G;
+        tet_geometry(xyz, v, G);
+        for (int cc = 0; cc < 3; cc++)
+            for (int d = 0; d < 3; d++) {
+                double g = 0.0;
+                for (int k = 0; k < 4; k++) g += bases[24 * (int64_t)v[k] + 3 * I + cc] * G.g[k][d];
+                out[3 * cc + d] = g;
+            }
+    }
+    __syncthreads();
+    // D: lambda on the trace plus 2 mu on the normal strains, mu on the engineering shears
+    const double lam = lame[0], mu = lame[1];
+    for (int t = tid; t < 576; t += blockDim.x) {
+        const int I = t / 72, J = (t / 9) % 8, r = (t / 3) % 3, cs = t % 3;
+        double acc = 0.0;
+        for (int q = 0; q < kMacroQ; q++) {
+            double bi[6], bj[6];
+            strain_column(sG + 72 * q + 9 * I, cs, bi);
+            strain_column(sG + 72 * q + 9 * J, r, bj);
+            const double tr = bi[0] + bi[1] + bi[2];
+            double v = 0.0;
+            for (int k = 0; k < 3; k++) v += bj[k] * (lam * tr + 2.0 * mu * bi[k]);
+            for (int k = 3; k < 6; k++) v += bj[k] * mu * bi[k];
+            acc += sW[q] * v;
+        }
+        K[576 * (int64_t)c + t] = acc;
     }
 }
 
@@ -911,6 +1048,39 @@ int msfem_cells_report(msfem_cells_t h, int32_t* inner, int32_t* outer, double* 
     if (threads) {
         threads[0] = h->faces.threads;
         threads[1] = h->vols.threads;
+    }
+    return MSFEM_OK;
+}
+
+int msfem_cells_macro_matrices(msfem_cells_t h, double* K, int on_device)
+{
+    using namespace msfem;
+    if (!h || !K) {
+        set_error("msfem_cells_macro_matrices: bad arguments");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    MSFEM_CK(cudaSetDevice(h->device));
+    cudaStream_t st = h->stream;
+    DBuf<double> dK;
+    double* out = K;
+    if (!on_device) {
+        MSFEM_TRY(dK.alloc(576 * (size_t)h->n_cells));
+        out = dK.p;
+    }
+    const size_t smem = sizeof(double) * (96 * 72 + 96 * 3 + 96) + sizeof(int) * 96;
+    MSFEM_CK(cudaFuncSetAttribute(k_macro_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    MSFEM_CK(cudaMemsetAsync(h->flag.p, 0, sizeof(int), st));
+    k_macro_cells<<<h->n_cells, 256, smem, st>>>(h->tet_off.p, h->vols.elems.p, h->xyz.p, h->box.p, h->bx.p, h->lame.p,
+                                                 out, h->flag.p);
+    MSFEM_CK(cudaGetLastError());
+    if (!on_device)
+        MSFEM_CK(cudaMemcpyAsync(K, dK.p, sizeof(double) * 576 * h->n_cells, cudaMemcpyDeviceToHost, st));
+    int bad = 0;
+    MSFEM_CK(cudaMemcpyAsync(&bad, h->flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    if (bad) {
+        set_error("msfem_cells_macro_matrices: a quadrature point lies in no tetrahedron of its cell");
+        return MSFEM_ERR_ARGUMENT;
     }
     return MSFEM_OK;
 }

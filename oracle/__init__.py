@@ -79,8 +79,11 @@ class RefLib:
         L.ref_ssor_apply.argtypes = [C.c_int, _i32p, _i32p, _f64p, C.c_double, _f64p, _f64p]
         L.ref_cell_problem.argtypes = [C.c_int, C.c_int, _f64p, C.c_int, _i32p, _i32p, C.c_int, _f64p, _f64p,
                                        C.c_int, _i32p, _f64p, C.c_double, _f64p]
+        L.ref_poly_quadrature.argtypes = [_f64p, _i32p, _f64p, _f64p]
+        L.ref_mech_D.argtypes = [C.c_double, C.c_double, _f64p]
         for f in ("ref_elastic_local", "ref_scalar_local", "ref_elastic_system", "ref_elastic_driver",
-                  "ref_scalar_system", "ref_scalar_driver", "ref_cssd_solve", "ref_ssor_apply", "ref_cell_problem"):
+                  "ref_scalar_system", "ref_scalar_driver", "ref_cssd_solve", "ref_ssor_apply", "ref_cell_problem",
+                  "ref_poly_quadrature", "ref_mech_D"):
             getattr(L, f).restype = C.c_int
         L.ref_set_quiet(1)
 
@@ -182,6 +185,18 @@ class RefLib:
                                      _c(bc_nodes, np.int32), _c(bc_values, np.float64).ravel(), min_residual, sol)
         assert rc == 0, rc
         return sol.reshape(n, 3)
+
+    def poly_quadrature(self, xyz8, faces):
+        """The reference's macro-element quadrature: (points [96, 3], weights [96])."""
+        pts, w = np.zeros(288), np.zeros(96)
+        rc = self.L.ref_poly_quadrature(_c(xyz8, np.float64).ravel(), _c(faces, np.int32).ravel(), pts, w)
+        assert rc == 0, rc
+        return pts.reshape(96, 3), w
+
+    def mech_D(self, E, nu):
+        D = np.zeros(36)
+        assert self.L.ref_mech_D(E, nu, D) == 0
+        return D.reshape(6, 6)
 
     def ssor_apply(self, A: Csr, r, w: float = 0.75):
         z = np.zeros(A.n)

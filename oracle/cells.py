@@ -251,3 +251,99 @@ def order1_bases(xyz, tets, mat, box, E, nu, solver=None):
             val[fnodes] = s
         out[:, v, :] = solve(3, xyz, tets.astype(np.int32), mat, E, nu, bnodes, val[bnodes])
     return out
+
+
+# --------------------------------------------------------------------------------------------
+# MsFEM macro element (FiniteElement_forMech_Poly_Order1::SolveLocalMatrix, MsFEM_Grid.h:3837-3975)
+# --------------------------------------------------------------------------------------------
+
+# vertex cycles of the six box faces (face order x0, x1, y0, y1, z0, z1)
+FACE_CYCLES = np.array([[0, 2, 6, 4], [1, 3, 7, 5], [0, 1, 5, 4], [2, 3, 7, 6], [0, 1, 3, 2], [4, 5, 7, 6]])
+
+
+def box_vertices(box):
+    b = np.asarray(box, dtype=np.float64)
+    return np.array([[b[0 + (v & 1)], b[2 + ((v >> 1) & 1)], b[4 + ((v >> 2) & 1)]] for v in range(8)])
+
+
+def poly_quadrature(verts, faces=FACE_CYCLES):
+    """Polyhedron::CreateSubMeshInSelf + SetIntegrationLaw(4) (Library/GeometryShape.h:2708-2760,
+    :2820-2836): for each face, for each edge (v_i, v_i+1), the sub-tetrahedron (centroid, face
+    centroid, v_i, v_i+1) with the 4-point rule u = (5 - sqrt 5)/20, weight V_sub / 4."""
+    verts = np.asarray(verts, dtype=np.float64)
+    C = verts.mean(axis=0)
+    u = (5.0 - np.sqrt(5.0)) / 20.0
+    v = 1.0 - 3.0 * u
+    bary = np.array([[u, u, u], [v, u, u], [u, v, u], [u, u, v]])
+    pts, w = [], []
+    for f in faces:
+        F = verts[f].mean(axis=0)
+        for i in range(len(f)):
+            P = np.array([C, F, verts[f[i]], verts[f[(i + 1) % len(f)]]])
+            E = P[1:] - P[0]
+            vol = abs(np.linalg.det(E)) / 6.0
+            for b in bary:
+                pts.append(P[0] + b @ E)
+                w.append(vol / 4.0)
+    return np.array(pts), np.array(w)
+
+
+def isotropic_D(E, nu):
+    """Domain::forMech isotropic D (Library/Domain.h:53-78): Voigt order xx, yy, zz, xy, yz, zx,
+    engineering shear."""
+    k = E * (1 - nu) / ((1 + nu) * (1 - 2 * nu))
+    a = nu / (1 - nu)
+    b = (1 - 2 * nu) / (2 * (1 - nu))
+    D = np.zeros((6, 6))
+    D[:3, :3] = k * a
+    np.fill_diagonal(D[:3, :3], k)
+    D[3, 3] = D[4, 4] = D[5, 5] = k * b
+    return D
+
+
+def locate(xyz, tets, x, tol=1e-12):
+    """Index of the first tetrahedron containing x (barycentrics >= -tol), the micro element the
+    reference's nearest-element lookup (GeometryGrid.h:323-340) returns for interior points."""
+    P = xyz[tets]                                  # [E, 4, 3]
+    E = P[:, 1:, :] - P[:, :1, :]                  # [E, 3, 3]
+    lam = np.linalg.solve(np.transpose(E, (0, 2, 1)), (x - P[:, 0, :])[:, :, None])[:, :, 0]
+    l0 = 1 - lam.sum(axis=1)
+    inside = (lam.min(axis=1) >= -tol) & (l0 >= -tol)
+    hit = np.nonzero(inside)[0]
+    if hit.size == 0:
+        raise ValueError("quadrature point outside the cell mesh")
+    return int(hit[0])
+
+
+def strain_matrix(G):
+    """B (6 x 3) of the component-wise vector basis with gradient G[c][d] = d psi^c / dx_d, the rows
+    of MsFEM_Grid.h:3868-3885 (column a: the strain of e_a psi^a)."""
+    B = np.zeros((6, 3))
+    B[0, 0], B[1, 1], B[2, 2] = G[0, 0], G[1, 1], G[2, 2]
+    B[3, 0], B[3, 1] = G[0, 1], G[1, 0]
+    B[4, 2], B[4, 1] = G[2, 1], G[1, 2]
+    B[5, 2], B[5, 0] = G[2, 0], G[0, 2]
+    return B
+
+
+def macro_element_matrix(xyz, tets, bases, box, E0, nu0):
+    """[8, 8, 3, 3]: A[I][J][r][c] = sum_q w_q (B_J^T D0 B_I)[r][c] over the macro quadrature, the
+    basis gradients from the micro tetrahedron holding each point, D0 = domain 0's material
+    (MsFEM/MsFEM.h:644-647)."""
+    xyz = np.asarray(xyz, dtype=np.float64)
+    tets = np.asarray(tets, dtype=np.int64)
+    pts, w = poly_quadrature(box_vertices(box))
+    D = isotropic_D(E0, nu0)
+    A = np.zeros((8, 8, 3, 3))
+    for x, wq in zip(pts, w):
+        e = locate(xyz, tets, x)
+        g, _ = simplex_gradients(xyz[tets[e]])              # [4, 3]
+        Bs = []
+        for I in range(8):
+            G = bases[tets[e], I, :].T @ g                   # [3 comps, 3 derivs]
+            Bs.append(strain_matrix(G))
+        for I in range(8):
+            DBI = D @ Bs[I]
+            for J in range(8):
+                A[I, J] += wq * (Bs[J].T @ DBI)
+    return A

@@ -661,4 +661,54 @@ int ref_cell_problem(int dim, int n_nodes, const double* xyz, int n_elems, const
     return 0; /* objects leaked on purpose, as in ref_elastic_driver */
 }
 
+
+/* The quadrature of an MsFEM macro element (geometry::Polyhedron::CreateSubMeshInSelf and
+ * SetIntegrationLaw, Library/GeometryShape.h:2708-2760, :2820-2836): the sub-tetrahedra
+ * (centroid, face centroid, edge of the face) over every face, each with the tetrahedron's
+ * 4-point rule (:1754-1851).  xyz8: the 8 vertices; faces: 6 cycles of 4 local vertex ids.
+ * points: 3 * 96 doubles, weights: 96 doubles (faces in order, edges in order, rule points in
+ * order). */
+int ref_poly_quadrature(const double* xyz8, const int* faces, double* points, double* weights)
+{
+    StdoutSilencer s;
+    auto* P = new std::vector<Point<double>>(8);
+    std::vector<Point<double>*> ptr(8);
+    for (int i = 0; i < 8; i++) {
+        (*P)[i] = Point<double>(xyz8[3 * i], xyz8[3 * i + 1], xyz8[3 * i + 2]);
+        ptr[i] = &(*P)[i];
+    }
+    std::vector<int> ids(8);
+    for (int i = 0; i < 8; i++) ids[i] = i;
+    std::vector<std::vector<int>> fc(6, std::vector<int>(4));
+    for (int f = 0; f < 6; f++)
+        for (int k = 0; k < 4; k++) fc[f][k] = faces[4 * f + k];
+    auto* poly = new geometry::Polyhedron();
+    poly->SetGeometry(ids, fc, ptr);
+    poly->SetIntegrationLaw(4);
+    const int n = (int)poly->GetIntegrationPointsCount();
+    if (n != 96) return -2;
+    for (int q = 0; q < n; q++) {
+        Point<double> x = poly->GetIntegrationPoint(q);
+        points[3 * q] = x.x;
+        points[3 * q + 1] = x.y;
+        points[3 * q + 2] = x.z;
+        weights[q] = poly->GetIntegrationWeight(q);
+    }
+    return 0; /* objects leaked on purpose (the nodes must outlive the polyhedron) */
+}
+
+/* Domain::forMech::GetD(3) (Library/Domain.h:170-175, isotropic D of :53-78) as 36 doubles. */
+int ref_mech_D(double E, double nu, double* D)
+{
+    StdoutSilencer s;
+    auto* d = new Domain();
+    d->forMech.SetE(E);
+    d->forMech.SetV(nu);
+    auto m = d->forMech.GetD(3);
+    if (m.size() != 6) return -2;
+    for (int i = 0; i < 6; i++)
+        for (int j = 0; j < 6; j++) D[6 * i + j] = m[i][j];
+    return 0;
+}
+
 }  // extern "C"

@@ -131,3 +131,28 @@ def test_cell_meshes_generator():
         assert tets.min() == 0 and tets.max() == xyz.shape[0] - 1
         assert np.all(xyz.min(0) >= box[0::2] - 1e-15) and np.all(xyz.max(0) <= box[1::2] + 1e-15)
     assert 0.0 < cm.mat.mean() < 1.0
+
+
+def test_macro_quadrature_and_material_match_reference(ref):
+    """The macro element's quadrature (the reference's geometry::Polyhedron sub-tetrahedra with the
+    4-point rule) and its D matrix, against the reference's own objects."""
+    box = [0.1, 0.35, 0.2, 0.4, -0.1, 0.3]
+    V = cells.box_vertices(box)
+    pr, wr = ref.poly_quadrature(V, cells.FACE_CYCLES)
+    pp, wp = cells.poly_quadrature(V)
+    np.testing.assert_allclose(pp, pr, rtol=0, atol=1e-15)
+    np.testing.assert_allclose(wp, wr, rtol=0, atol=1e-18)
+    assert wp.sum() == pytest.approx(0.25 * 0.2 * 0.4, rel=1e-14)
+    np.testing.assert_allclose(cells.isotropic_D(3.0, 0.27), ref.mech_D(3.0, 0.27), rtol=0, atol=1e-14)
+
+
+def test_macro_element_matrix_properties():
+    mesh, mat = _one_cell(m=4)
+    box = [0, 1, 0, 1, 0, 1]
+    B = cells.order1_bases(mesh.xyz, mesh.tets, mat, box, E2, NU2)
+    K = cells.macro_element_matrix(mesh.xyz, mesh.tets, B, box, E2[0], NU2[0])
+    # A[J][I] = A[I][J]^T, and rigid translations (the bases add up to (1,1,1)) give no force
+    np.testing.assert_allclose(K, K.transpose(1, 0, 3, 2), rtol=0, atol=1e-14 * np.abs(K).max())
+    t = np.array([0.3, -1.2, 0.7])
+    f = np.einsum("ijrs,s->ir", K, t)
+    assert np.abs(f).max() <= 1e-12 * np.abs(K).max()

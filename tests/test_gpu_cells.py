@@ -181,3 +181,26 @@ def test_cells_reject_bad_meshes(lib, cuda):
     with pytest.raises(_lib.MsfemError) as e:
         Cells(bad)
     assert e.value.rc == _lib.MSFEM_ERR_ARGUMENT
+
+
+def test_macro_element_matrices_match_oracle(lib, cuda):
+    cm = meshgen.msfem_cells(n_coarse=2, m_choices=(3, 4, 5), seed=11)
+    C = Cells(cm)
+    assert C.build_bases(precision=FP32_IR, tol=1e-10) == 0
+    B = C.bases()
+    K = C.macro_matrices()
+    for c in range(cm.n_cells):
+        xyz, tets, mat, box = cm.cell(c)
+        want = ocells.macro_element_matrix(xyz, tets, B[cm.node_off[c]:cm.node_off[c + 1]], box, cm.E[0], cm.nu[0])
+        np.testing.assert_allclose(K[c], want, rtol=0, atol=1e-12 * np.abs(want).max())
+
+
+def test_full_size_macro_matrices_translation_free(lib, cuda, full_cells):
+    cm = full_cells
+    C = Cells(cm)
+    assert C.build_bases(precision=FP32_IR, tol=1e-8) == 0
+    K = C.macro_matrices()
+    np.testing.assert_allclose(K, K.transpose(0, 2, 1, 4, 3), rtol=0, atol=1e-13 * np.abs(K).max())
+    f = np.einsum("cijrs,s->cir", K, np.array([1.0, 1.0, 1.0]))
+    # the bases add up to (1,1,1) to the solve's accuracy (ill-conditioned cells: ~1e-4 here)
+    assert np.abs(f).max() <= 1e-3 * np.abs(K).max()
