@@ -292,7 +292,29 @@ int msfem_cells_report(msfem_cells_t c, int32_t* inner_iterations, int32_t* oute
  * K: [n_cells][8][8][3][3] doubles, K[c][I][J] = sum_q w_q B_J^T D B_I as the reference stores
  * A[I][J]. */
 int msfem_cells_macro_matrices(msfem_cells_t c, double* K, int on_device);
+/* Macro boundary loads (BoundaryFace_forMech_Poly_Order1::SolveLocalBoundaryVector,
+ * MsFEM/MsFEM_Grid.h:4104-4135): for item i = (cell, face) with a constant traction t_i,
+ * loads[i][v][a] = sum_q w_q t_a psi_v^a(x_q) over the face, with the polygon rule of
+ * Library/GeometryShape.h:2563-2600 (sub-triangles centroid / face edge, the triangle 4-point
+ * rule of :1482-1540) and the bases interpolated in the micro tetrahedron holding each point.
+ * items: [n][2] host ints, traction: [n][3], loads: [n][8][3] host doubles. */
+int msfem_cells_face_loads(msfem_cells_t c, int n_items, const int32_t* items, const double* traction, double* loads);
+
+/* The fine solution of every cell from the macro one (the MsFEM solution on the micro meshes):
+ * u[b] = sum_v U[cell_vertex[8c+v]] (.) psi_v(b), component by component.  U: [n_vertices][3],
+ * u: [cell nodes][3] (concatenated cell numbering), host arrays. */
+int msfem_cells_reconstruct(msfem_cells_t c, int n_vertices, const int32_t* cell_vertex, const double* U, double* u);
 void msfem_cells_destroy(msfem_cells_t c);
+
+/* The MsFEM macro problem (MsFEM::MsFEM_forElasticDeformation_OrderBF1_forPoly, MsFEM/MsFEM.h:
+ * 572-1010): element matrices K [n_cells][8][8][3][3] over the vertices cell_vertex[8c+v]
+ * (SummPartOfMatrix in cell order), loads F [n_vertices][3] (or NULL), every component of the
+ * listed Dirichlet vertices fixed (values [n_fixed][3]; a later duplicate wins), then MINRES
+ * (the macro matrix is symmetric, not necessarily definite) on the free vertices to
+ * ||F_I - A_II U_I|| <= tol ||F_I||.  U: [n_vertices][3] out.  Host arrays. */
+int msfem_macro_solve(int n_vertices, int n_cells, const int32_t* cell_vertex, const double* K, const double* F,
+                      int n_fixed, const int32_t* fixed_vertices, const double* fixed_values, int precision, double tol,
+                      int maxiter, double* U, int32_t* iterations, double* rel_residual);
 
 
 /* ---------------------------------------------------------------------------------------

@@ -87,7 +87,11 @@ _SIGS = [
     ("msfem_cells_get_bases", C.c_int, [C.c_void_p, _P, C.c_int]),
     ("msfem_cells_report", C.c_int, [C.c_void_p, _P, _P, _P, _P, _P, _P]),
     ("msfem_cells_macro_matrices", C.c_int, [C.c_void_p, _P, C.c_int]),
+    ("msfem_cells_face_loads", C.c_int, [C.c_void_p, C.c_int, _P, _P, _P]),
+    ("msfem_cells_reconstruct", C.c_int, [C.c_void_p, C.c_int, _P, _P, _P]),
     ("msfem_cells_destroy", None, [C.c_void_p]),
+    ("msfem_macro_solve", C.c_int, [C.c_int, C.c_int, _P, _P, _P, C.c_int, _P, _P, C.c_int, C.c_double, C.c_int,
+                                    _P, _P, _P]),
     ("msfem_coarse_create", C.c_int, [C.c_void_p, C.c_void_p, _P, C.c_int, _P, _P, C.c_int, _P,
                                       C.POINTER(C.c_void_p)]),
     ("msfem_coarse_info", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)]),

@@ -6,7 +6,8 @@
 // matrices serially in element order (CSSD_Matrix::SummPartOfMatrix,
 // Library/CSSD_Matrix.h:307-363), one cell at a time in an OpenMP loop over cells
 // (MsFEM/MsFEM_Grid.h:4800-4802).  Here every element of every system emits its
-// (k+1)^2 (row, column) node pairs, tagged element << 4 | I << 2 | J; one stable
+// (k+1)^2 (row, column) node pairs, tagged element << 2b | I << b | J (b = 2 bits for up to 4
+// nodes per element, 3 for 8); one stable
 // radix sort by (row, column) groups equal pairs (a block of the matrix) with
 // their contributions in element order.  The unique keys are the portrait (rows
 // sorted, diagonal included); the sorted tags are kept, so assembling a block is
@@ -57,6 +58,8 @@ __global__ void k_check_elements(int n_sys, const int64_t* __restrict__ node_off
         }
 }
 
+__host__ __device__ __forceinline__ int tag_bits(int k1) { return k1 > 4 ? 3 : 2; }
+
 __global__ void k_emit_pairs(int64_t e0, int64_t e1, int64_t n0, int nb, const int32_t* __restrict__ elems, int k1,
                              uint64_t* __restrict__ key, uint32_t* __restrict__ tag)
 {
@@ -69,7 +72,8 @@ __global__ void k_emit_pairs(int64_t e0, int64_t e1, int64_t n0, int nb, const i
         const uint64_t row = (uint64_t)(elems[e * k1 + a] - n0);
         const uint64_t col = (uint64_t)(elems[e * k1 + b] - n0);
         key[t] = (row << nb) | col;
-        tag[t] = ((uint32_t)e << 4) | (uint32_t)(a << 2) | (uint32_t)b;
+        const int tb = tag_bits(k1);
+        tag[t] = ((uint32_t)e << (2 * tb)) | (uint32_t)(a << tb) | (uint32_t)b;
     }
 }
 
@@ -146,6 +150,27 @@ __global__ void k_assemble_blocks(int64_t nnzb, const int64_t* __restrict__ csta
     }
 }
 
+// each block = sum of the caller's element blocks eb[e][I][J][9] in element order (8-node
+// elements: the MsFEM macro cells)
+__global__ void k_assemble_given(int64_t nnzb, const int64_t* __restrict__ cstart, const uint32_t* __restrict__ contrib,
+                                 int k1, const double* __restrict__ eb, double* __restrict__ val)
+{
+    const int tb = tag_bits(k1);
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < nnzb; s += (int64_t)gridDim.x * blockDim.x) {
+        double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int64_t c = cstart[s]; c < cstart[s + 1]; c++) {
+            const uint32_t t = contrib[c];
+            const int64_t e = t >> (2 * tb);
+            const int I = (t >> tb) & ((1 << tb) - 1), J = t & ((1 << tb) - 1);
+            const double* blk = eb + 9 * (((int64_t)e * k1 + I) * k1 + J);
+#pragma unroll
+            for (int q = 0; q < 9; q++) acc[q] += blk[q];
+        }
+#pragma unroll
+        for (int q = 0; q < 9; q++) val[9 * s + q] = acc[q];
+    }
+}
+
 // s = 1/sqrt(A_ii[a][a]) (1 when not positive), then the scaled FP32 copy, row by row
 __global__ void k_batch_scale(int64_t n_nodes, const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
                               const double* __restrict__ val, double* __restrict__ dscale)
@@ -191,6 +216,7 @@ struct BatchArgs {
     const double* dscale;
     const uint8_t* fixed;
     double* x;
+    const double* rhs;  // [n_nodes][R][3] source term, or null (zero source)
     void* work;
     int64_t work_stride;  // elements of VT per vector
     int* queue;
@@ -287,6 +313,9 @@ __device__ void residual_pass(const BatchArgs& A, int64_t n0, int np, const uint
         }
         const int64_t gi = n0 + i;
         double y[3] = {0, 0, 0};
+        if (A.rhs)
+#pragma unroll
+            for (int c = 0; c < 3; c++) y[c] = A.rhs[(n0 * R + p) * 3 + c];
         for (int64_t k = A.row_ptr[gi]; k < A.row_ptr[gi + 1]; k++) {
             const int64_t cc = A.col[k] - n0;
             const double* a = A.val64 + 9 * k;
@@ -592,6 +621,7 @@ int launch_minres(BatchSys& b, double* d_x, int start64, double tol, int maxiter
     a.iters = b.iters.p;
     a.outers = b.outers.p;
     a.rel = b.rel.p;
+    a.rhs = b.rhs;
     a.tol = tol;
     a.maxiter = maxiter;
     a.max_outer = 30;
@@ -609,8 +639,8 @@ int batch_build_pattern(BatchSys& b, const double* d_xyz)
 {
     (void)d_xyz;
     cudaStream_t st = b.stream;
-    if (b.n_elems >= ((int64_t)1 << 28)) {
-        set_error("batched systems: %lld elements exceed the 2^28 limit of the contribution tags", (long long)b.n_elems);
+    if (b.k1 > 8 || b.n_elems >= ((int64_t)1 << (32 - 2 * tag_bits(b.k1)))) {
+        set_error("batched systems: %lld elements of %d nodes exceed the contribution tags", (long long)b.n_elems, b.k1);
         return MSFEM_ERR_LIMIT;
     }
     if (b.n_nodes >= ((int64_t)1 << 31)) {
@@ -785,6 +815,25 @@ int batch_assemble(BatchSys& b, const double* d_xyz, const double* d_lame, int n
         set_error("batched systems: material id out of range");
         return MSFEM_ERR_ARGUMENT;
     }
+    return 0;
+}
+
+int batch_assemble_given(BatchSys& b, const double* d_eblocks)
+{
+    cudaStream_t st = b.stream;
+    MSFEM_TRY(b.val64.alloc(std::max<int64_t>(1, 9 * b.nnzb)));
+    MSFEM_TRY(b.val32.alloc(std::max<int64_t>(1, 9 * b.nnzb)));
+    MSFEM_TRY(b.dscale.alloc(std::max<int64_t>(1, 3 * b.n_nodes)));
+    const int blocks = (int)std::min<int64_t>((b.nnzb + 255) / 256, 148 * 16);
+    if (b.nnzb)
+        k_assemble_given<<<blocks, 256, 0, st>>>(b.nnzb, b.cstart.p, b.contrib.p, b.k1, d_eblocks, b.val64.p);
+    const int nblk = (int)std::min<int64_t>((b.n_nodes + 255) / 256, 148 * 16);
+    if (b.n_nodes) {
+        k_batch_scale<<<nblk, 256, 0, st>>>(b.n_nodes, b.row_ptr.p, b.col.p, b.val64.p, b.dscale.p);
+        k_batch_val32<<<nblk, 256, 0, st>>>(b.n_nodes, b.row_ptr.p, b.col.p, b.val64.p, b.dscale.p, b.val32.p);
+    }
+    MSFEM_CK(cudaGetLastError());
+    MSFEM_CK(cudaStreamSynchronize(st));
     return 0;
 }
 

@@ -42,6 +42,7 @@ struct BatchSys {
     DBuf<int> queue;
     DBuf<int32_t> iters, outers;
     DBuf<double> rel;
+    const double* rhs = nullptr;  // optional source term [n_nodes][R][3] (device), used by batch_solve
     int grid = 0, threads = 0;
     int tuned_threads = 0, tuned_precision = -1;  // autotuned CTA size (0: not tuned yet)
     std::vector<float> tune_ms;                   // trial times of the candidates 128/256/384/512
@@ -53,6 +54,8 @@ struct BatchSys {
 int batch_build_pattern(BatchSys& b, const double* d_xyz);
 // values from the current materials (lame: [n_mat][2] lambda, mu on the device)
 int batch_assemble(BatchSys& b, const double* d_xyz, const double* d_lame, int n_mat);
+// values from caller-given element blocks [n_elems][k1][k1][9] (device)
+int batch_assemble_given(BatchSys& b, const double* d_eblocks);
 // solves every system; x: [n_nodes][R][3] FP64, fixed entries hold the Dirichlet data on
 // entry, free entries are overwritten.  precision: MSFEM_FP64 or MSFEM_FP32_IR.  threads <= 0:
 // the CTA size is autotuned on the first call (cached per batch and precision).

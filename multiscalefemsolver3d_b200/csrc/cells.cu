@@ -537,6 +537,106 @@ __global__ void __launch_bounds__(256) k_macro_cells(const int64_t* __restrict__
     }
 }
 
+
+// ---- MsFEM macro boundary loads (BoundaryFace_forMech_Poly_Order1::SolveLocalBoundaryVector,
+// MsFEM_Grid.h:4104-4135): f[I][a] = sum_q w_q t_a psi_I^a(x_q) over the macro face, with the
+// polygon rule of GeometryShape.h:2563-2600 (sub-triangles centroid / face edge) and the triangle
+// 4-point rule of :1482-1540; psi from the micro tetrahedron holding each point.
+__global__ void __launch_bounds__(128) k_face_loads(int n_items, const int32_t* __restrict__ items,
+                                                    const double* __restrict__ traction,
+                                                    const int64_t* __restrict__ tet_off, const int32_t* __restrict__ tets,
+                                                    const double* __restrict__ xyz, const double* __restrict__ box,
+                                                    const double* __restrict__ bases, double* __restrict__ out, int* bad)
+{
+    __shared__ double sP[16][3], sW[16];
+    __shared__ int sT[16];
+    const int it = blockIdx.x, tid = threadIdx.x;
+    const int c = items[2 * it], f = items[2 * it + 1];
+    const double* bx = box + 6 * c;
+    if (tid < 16) {
+        const int i = tid / 4, j = tid % 4;
+        double F[3] = {0, 0, 0}, a[3], b[3];
+        for (int k = 0; k < 4; k++) {
+            double p[3];
+            box_vertex(bx, c_face_cycles[f][k], p);
+            for (int d = 0; d < 3; d++) F[d] += 0.25 * p[d];
+        }
+        box_vertex(bx, c_face_cycles[f][i], a);
+        box_vertex(bx, c_face_cycles[f][(i + 1) % 4], b);
+        double e1[3], e2[3];
+        for (int d = 0; d < 3; d++) {
+            e1[d] = a[d] - F[d];
+            e2[d] = b[d] - F[d];
+        }
+        const double cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+        const double detD = sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+        const double xs[4] = {1.0 / 3.0, 3.0 / 5.0, 1.0 / 5.0, 1.0 / 5.0};
+        const double ys[4] = {1.0 / 3.0, 1.0 / 5.0, 3.0 / 5.0, 1.0 / 5.0};
+        const double ws[4] = {-9.0 / 32.0, 25.0 / 96.0, 25.0 / 96.0, 25.0 / 96.0};
+        for (int d = 0; d < 3; d++) sP[tid][d] = F[d] + e1[d] * xs[j] + e2[d] * ys[j];
+        sW[tid] = ws[j] * detD;
+        sT[tid] = 0x7fffffff;
+    }
+    __syncthreads();
+    const int64_t t0 = tet_off[c], t1 = tet_off[c + 1];
+    for (int64_t e = t0 + tid; e < t1; e += blockDim.x) {
+        int v[4];
+        for (int k = 0; k < 4; k++) v[k] = tets[4 * e + k];
+        TetGeom G;
+        tet_geometry(xyz, v, G);
+        const double* p0 = xyz + 3 * (int64_t)v[0];
+        for (int q = 0; q < 16; q++) {
+            const double dx[3] = {sP[q][0] - p0[0], sP[q][1] - p0[1], sP[q][2] - p0[2]};
+            bool in = true;
+            for (int k = 0; k < 4; k++) {
+                const double lam = (k == 0 ? 1.0 : 0.0) + G.g[k][0] * dx[0] + G.g[k][1] * dx[1] + G.g[k][2] * dx[2];
+                in = in && lam >= -1e-12;
+            }
+            if (in) atomicMin(&sT[q], (int)(e - t0));
+        }
+    }
+    __syncthreads();
+    if (tid < 24) {
+        const int I = tid / 3, a = tid % 3;
+        double acc = 0.0;
+        for (int q = 0; q < 16; q++) {
+            if (sT[q] == 0x7fffffff) {
+                atomicExch(bad, 1);
+                continue;
+            }
+            const int64_t e = t0 + sT[q];
+            int v[4];
+            for (int k = 0; k < 4; k++) v[k] = tets[4 * e + k];
+            TetGeom G;
+            tet_geometry(xyz, v, G);
+            const double* p0 = xyz + 3 * (int64_t)v[0];
+            const double dx[3] = {sP[q][0] - p0[0], sP[q][1] - p0[1], sP[q][2] - p0[2]};
+            double psi = 0.0;
+            for (int k = 0; k < 4; k++) {
+                const double lam = (k == 0 ? 1.0 : 0.0) + G.g[k][0] * dx[0] + G.g[k][1] * dx[1] + G.g[k][2] * dx[2];
+                psi += lam * bases[24 * (int64_t)v[k] + 3 * I + a];
+            }
+            acc += sW[q] * traction[3 * it + a] * psi;
+        }
+        out[24 * (int64_t)it + tid] = acc;
+    }
+}
+
+// fine solution of every cell from the macro one: u[b] = sum_v U[V(c, v)] (.) psi_v(b)
+__global__ void k_reconstruct(int n_cells, const int64_t* __restrict__ node_off, const int32_t* __restrict__ cell_vertex,
+                              const double* __restrict__ U, const double* __restrict__ bases, double* __restrict__ u)
+{
+    const int c = blockIdx.x;
+    for (int64_t b = node_off[c] + threadIdx.x; b < node_off[c + 1]; b += blockDim.x) {
+        double acc[3] = {0, 0, 0};
+        for (int v = 0; v < 8; v++) {
+            const int64_t V = cell_vertex[8 * c + v];
+            for (int a = 0; a < 3; a++) acc[a] += U[3 * V + a] * bases[24 * b + 3 * v + a];
+        }
+        for (int a = 0; a < 3; a++) u[3 * b + a] = acc[a];
+    }
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ handles
@@ -1082,6 +1182,71 @@ int msfem_cells_macro_matrices(msfem_cells_t h, double* K, int on_device)
         set_error("msfem_cells_macro_matrices: a quadrature point lies in no tetrahedron of its cell");
         return MSFEM_ERR_ARGUMENT;
     }
+    return MSFEM_OK;
+}
+
+int msfem_cells_face_loads(msfem_cells_t h, int n_items, const int32_t* items, const double* traction, double* loads)
+{
+    using namespace msfem;
+    if (!h || n_items < 0 || (n_items > 0 && (!items || !traction || !loads))) {
+        set_error("msfem_cells_face_loads: bad arguments");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    if (n_items == 0) return MSFEM_OK;
+    for (int i = 0; i < n_items; i++)
+        if (items[2 * i] < 0 || items[2 * i] >= h->n_cells || items[2 * i + 1] < 0 || items[2 * i + 1] > 5) {
+            set_error("msfem_cells_face_loads: item %d names cell %d face %d", i, items[2 * i], items[2 * i + 1]);
+            return MSFEM_ERR_ARGUMENT;
+        }
+    MSFEM_CK(cudaSetDevice(h->device));
+    cudaStream_t st = h->stream;
+    DBuf<int32_t> di;
+    DBuf<double> dt, dout;
+    MSFEM_TRY(di.alloc(2 * (size_t)n_items));
+    MSFEM_TRY(dt.alloc(3 * (size_t)n_items));
+    MSFEM_TRY(dout.alloc(24 * (size_t)n_items));
+    MSFEM_CK(cudaMemcpyAsync(di.p, items, sizeof(int32_t) * 2 * n_items, cudaMemcpyHostToDevice, st));
+    MSFEM_CK(cudaMemcpyAsync(dt.p, traction, sizeof(double) * 3 * n_items, cudaMemcpyHostToDevice, st));
+    MSFEM_CK(cudaMemsetAsync(h->flag.p, 0, sizeof(int), st));
+    k_face_loads<<<n_items, 128, 0, st>>>(n_items, di.p, dt.p, h->tet_off.p, h->vols.elems.p, h->xyz.p, h->box.p, h->bx.p,
+                                          dout.p, h->flag.p);
+    MSFEM_CK(cudaGetLastError());
+    MSFEM_CK(cudaMemcpyAsync(loads, dout.p, sizeof(double) * 24 * n_items, cudaMemcpyDeviceToHost, st));
+    int bad = 0;
+    MSFEM_CK(cudaMemcpyAsync(&bad, h->flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    if (bad) {
+        set_error("msfem_cells_face_loads: a quadrature point lies in no tetrahedron of its cell");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    return MSFEM_OK;
+}
+
+int msfem_cells_reconstruct(msfem_cells_t h, int n_vertices, const int32_t* cell_vertex, const double* U, double* u)
+{
+    using namespace msfem;
+    if (!h || n_vertices <= 0 || !cell_vertex || !U || !u) {
+        set_error("msfem_cells_reconstruct: bad arguments");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    for (int k = 0; k < 8 * h->n_cells; k++)
+        if (cell_vertex[k] < 0 || cell_vertex[k] >= n_vertices) {
+            set_error("msfem_cells_reconstruct: coarse vertex id %d out of range", cell_vertex[k]);
+            return MSFEM_ERR_ARGUMENT;
+        }
+    MSFEM_CK(cudaSetDevice(h->device));
+    cudaStream_t st = h->stream;
+    DBuf<int32_t> dv;
+    DBuf<double> dU, du;
+    MSFEM_TRY(dv.alloc(8 * (size_t)h->n_cells));
+    MSFEM_TRY(dU.alloc(3 * (size_t)n_vertices));
+    MSFEM_TRY(du.alloc(3 * (size_t)h->n_nodes));
+    MSFEM_CK(cudaMemcpyAsync(dv.p, cell_vertex, sizeof(int32_t) * 8 * h->n_cells, cudaMemcpyHostToDevice, st));
+    MSFEM_CK(cudaMemcpyAsync(dU.p, U, sizeof(double) * 3 * n_vertices, cudaMemcpyHostToDevice, st));
+    k_reconstruct<<<h->n_cells, 256, 0, st>>>(h->n_cells, h->node_off.p, dv.p, dU.p, h->bx.p, du.p);
+    MSFEM_CK(cudaGetLastError());
+    MSFEM_CK(cudaMemcpyAsync(u, du.p, sizeof(double) * 3 * h->n_nodes, cudaMemcpyDeviceToHost, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
     return MSFEM_OK;
 }
 

@@ -81,9 +81,10 @@ class RefLib:
                                        C.c_int, _i32p, _f64p, C.c_double, _f64p]
         L.ref_poly_quadrature.argtypes = [_f64p, _i32p, _f64p, _f64p]
         L.ref_mech_D.argtypes = [C.c_double, C.c_double, _f64p]
+        L.ref_polygon_quadrature.argtypes = [_f64p, _f64p, _f64p]
         for f in ("ref_elastic_local", "ref_scalar_local", "ref_elastic_system", "ref_elastic_driver",
                   "ref_scalar_system", "ref_scalar_driver", "ref_cssd_solve", "ref_ssor_apply", "ref_cell_problem",
-                  "ref_poly_quadrature", "ref_mech_D"):
+                  "ref_poly_quadrature", "ref_mech_D", "ref_polygon_quadrature"):
             getattr(L, f).restype = C.c_int
         L.ref_set_quiet(1)
 
@@ -192,6 +193,12 @@ class RefLib:
         rc = self.L.ref_poly_quadrature(_c(xyz8, np.float64).ravel(), _c(faces, np.int32).ravel(), pts, w)
         assert rc == 0, rc
         return pts.reshape(96, 3), w
+
+    def polygon_quadrature(self, xyz4):
+        """The reference's macro-face quadrature: (points [16, 3], weights [16])."""
+        pts, w = np.zeros(48), np.zeros(16)
+        assert self.L.ref_polygon_quadrature(_c(xyz4, np.float64).ravel(), pts, w) == 0
+        return pts.reshape(16, 3), w
 
     def mech_D(self, E, nu):
         D = np.zeros(36)

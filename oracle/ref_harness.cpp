@@ -697,6 +697,33 @@ int ref_poly_quadrature(const double* xyz8, const int* faces, double* points, do
     return 0; /* objects leaked on purpose (the nodes must outlive the polyhedron) */
 }
 
+/* geometry::Polygon over the 4 given vertices (GeometryShape.h:2541-2640: centroid fan of
+   triangles, SetIntegrationLaw(4)): the 16 points and weights of the macro face loads. */
+int ref_polygon_quadrature(const double* xyz4, double* points, double* weights)
+{
+    StdoutSilencer s;
+    auto* P = new std::vector<Point<double>>(4);
+    std::vector<Point<double>*> ptr(4);
+    for (int i = 0; i < 4; i++) {
+        (*P)[i] = Point<double>(xyz4[3 * i], xyz4[3 * i + 1], xyz4[3 * i + 2]);
+        ptr[i] = &(*P)[i];
+    }
+    std::vector<int> ids = {0, 1, 2, 3};
+    auto* poly = new geometry::Polygon();
+    poly->SetGeometry(ids, ptr);
+    poly->SetIntegrationLaw(4);
+    const int n = (int)poly->GetIntegrationPointsCount();
+    if (n != 16) return -2;
+    for (int q = 0; q < n; q++) {
+        Point<double> x = poly->GetIntegrationPoint(q);
+        points[3 * q] = x.x;
+        points[3 * q + 1] = x.y;
+        points[3 * q + 2] = x.z;
+        weights[q] = poly->GetIntegrationWeight(q);
+    }
+    return 0; /* objects leaked on purpose, as above */
+}
+
 /* Domain::forMech::GetD(3) (Library/Domain.h:170-175, isotropic D of :53-78) as 36 doubles. */
 int ref_mech_D(double E, double nu, double* D)
 {

@@ -156,3 +156,40 @@ def test_macro_element_matrix_properties():
     t = np.array([0.3, -1.2, 0.7])
     f = np.einsum("ijrs,s->ir", K, t)
     assert np.abs(f).max() <= 1e-12 * np.abs(K).max()
+
+
+def test_macro_face_quadrature_matches_reference(ref):
+    """The macro face loads' quadrature (geometry::Polygon, centroid fan with the triangle 4-point
+    rule) against the reference's own object, on every face of a box."""
+    from oracle import msfem
+    V = cells.box_vertices([0.1, 0.35, 0.2, 0.4, -0.1, 0.3])
+    for f in range(6):
+        pr, wr = ref.polygon_quadrature(V[cells.FACE_CYCLES[f]])
+        pp, wp = msfem.polygon_quadrature(V[cells.FACE_CYCLES[f]])
+        np.testing.assert_allclose(pp, pr, rtol=0, atol=1e-15)
+        np.testing.assert_allclose(wp, wr, rtol=0, atol=1e-17)
+
+
+@pytest.mark.parametrize("spheres", [0, 3])
+def test_msfem_driver_restatement_properties(spheres):
+    """The restated macro driver on 8 cells of a cube: the loads add up to traction x area (the
+    bases are a partition of unity) and the Dirichlet vertices keep their values.  On the
+    homogeneous cube the fine solutions of neighbouring cells agree on their shared nodes; with
+    inclusions they need not, since each cell solves its own face problems with the material of its
+    own tetrahedra next to the face (cells.face_triangles), as the reference's cells do."""
+    from multiscalefemsolver3d_b200.msfem import cube_macro_boundary
+    from oracle import msfem
+    p = meshgen.cube_elastic(n=4, jitter=0.0, n_spheres=spheres, contrast=20.0, rmin=0.15, rmax=0.25, sphere_seed=2)
+    cc = meshgen.cube_cells(p.mesh, p.E, p.nu, 2)
+    cm = cc.cells
+    B = np.concatenate([cells.order1_bases(*cm.cell(c)[:3], cm.box[c], cm.E, cm.nu) for c in range(cm.n_cells)])
+    fv, fval, items, tr = cube_macro_boundary(cc)
+    U, u, K, F = msfem.driver(cc, B, fv, fval, items, tr, p.E[0], p.nu[0])
+    np.testing.assert_allclose(F.sum(axis=0), [0, 0, -1], atol=1e-13)
+    assert np.all(U[fv] == 0)
+    if spheres == 0:
+        assert np.all(U[:, 2].reshape(3, 9)[1:] < 0)
+        g = cc.cell_node_global
+        ref_u = np.zeros((p.mesh.n_nodes, 3))
+        ref_u[g] = u
+        assert np.abs(ref_u[g] - u).max() <= 1e-9 * np.abs(u).max()
