@@ -7,6 +7,17 @@ size n^3, one assembled system, optionally one FP32-IR solve to 1e-8, then
 Kernel launch order (for ncu -k/-s/-c): portrait and assembly kernels, the
 Dirichlet kernels, the solve (if --solve), then k_spmv<float> x5, then
 k_spmv<double> x5.
+
+    python -m multiscalefemsolver3d_b200.profile_case --twolevel --n 64
+
+runs the two-level elasticity solve of the 128^3 workload's kind at n^3 (n/8 macro cells per
+axis, spheres scaled with the volume): both assemblies, Dirichlet, the cell bases, coarse setup,
+the multiplicative cycle and FP64 MINRES to 1e-8.
+
+    python -m multiscalefemsolver3d_b200.profile_case --cells 8
+
+runs the batched Order1 cell bases of n^3 macro cells of the 16^3-cell workload's kind (per-cell
+resolution from {8, 12, 16, 20}, ellipsoidal inclusions E 1:50): edges, faces, volumes.
 """
 from __future__ import annotations
 
@@ -19,8 +30,14 @@ def main():
     ap.add_argument("--n", type=int, default=120)
     ap.add_argument("--solve", action="store_true")
     ap.add_argument("--elastic", action="store_true", help="elasticity cube instead of electrostatics")
+    ap.add_argument("--twolevel", action="store_true", help="two-level elasticity solve at n^3")
+    ap.add_argument("--cells", type=int, default=0, help="batched cell bases of cells^3 macro cells")
     a = ap.parse_args()
     from . import fem, meshgen
+    if a.cells:
+        return cells_case(a.cells)
+    if a.twolevel:
+        return twolevel_case(a.n)
     if a.elastic:
         p = meshgen.cube_elastic(n=a.n, n_spheres=200, contrast=100.0, rmin=0.02, rmax=0.06)
         S = fem.System(fem.ELASTIC, p.mesh.xyz, p.mesh.tets, p.mesh.mat)
@@ -43,6 +60,50 @@ def main():
     out.update(spmv32_ms=ms32, spmv32_bytes=b32, spmv64_ms=ms64, spmv64_bytes=b64)
     S.close()
     print(json.dumps(out))
+
+
+def cells_case(nc):
+    from . import meshgen
+    from .cells import FP32_IR, Cells
+    cm = meshgen.msfem_cells(n_coarse=nc, m_choices=(8, 12, 16, 20), seed=3, max_inclusions=3, contrast=50.0)
+    C = Cells(cm)
+    rc = C.build_bases(FP32_IR, 1e-8)
+    r = C.report()
+    print(json.dumps({"cells": cm.n_cells, "nodes": C.n_nodes, "rc": rc, "ms": r["ms"]}, default=str))
+    C.close()
+
+
+def twolevel_case(n):
+    import numpy as np
+
+    from . import fem, meshgen
+    from .cells import FP32_IR, FP64, Cells
+    from .twolevel import TwoLevel
+    spheres = max(1, round(2000 * (n / 128.0) ** 3))
+    p = meshgen.cube_elastic(n=n, jitter=0.0, n_spheres=spheres, contrast=100.0, rmin=0.015, rmax=0.035,
+                             sphere_seed=11)
+    m = p.mesh
+    dofs = (3 * p.bc_nodes[:, None] + np.arange(3)).ravel().astype(np.int32)
+    zval = np.zeros(dofs.size)
+    S = fem.System(fem.ELASTIC, m.xyz, m.tets, m.mat)
+    S.add_traction(p.faces, p.traction)
+    S.assemble_elastic(p.E, p.nu)
+    S.apply_dirichlet(dofs, zval, fem.ROW_AND_COLUMN)
+    K = fem.System(fem.ELASTIC, m.xyz, m.tets, m.mat)
+    K.assemble_elastic_textbook(p.E, p.nu)
+    K.apply_dirichlet(dofs, zval, fem.ROW_AND_COLUMN)
+    cc = meshgen.cube_cells(m, p.E, p.nu, 8)
+    C = Cells(cc.cells)
+    rcb = C.build_bases(FP32_IR, 1e-8)
+    T = TwoLevel(S, C, cc, dofs)
+    T.set_smoother(K, degree=3, half_matrix=True)
+    rel, it, out, rc = T.solve(tol=1e-8, maxiter=400000, precision=FP64)
+    print(json.dumps({"n": n, "dofs": S.n_rows, "rc_bases": rcb, "rc": rc, "rel": rel, "iterations": it,
+                      "ms_solve": S.stats()["ms_solve"]}))
+    T.close()
+    C.close()
+    K.close()
+    S.close()
 
 
 if __name__ == "__main__":
