@@ -65,6 +65,11 @@ def parse():
     ap.add_argument("--sample-n", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="elastic: skip the plain CG / Jacobi MINRES runs")
+    ap.add_argument("--coarse", default="learned", choices=["learned", "exact"],
+                    help="elastic: coarse-space bases predicted by the trained network (with the exact cell solve "
+                         "as per-cell fallback) or solved exactly for every cell")
+    ap.add_argument("--train-cells", type=int, default=20480, help="elastic, learned: training cells")
+    ap.add_argument("--train-epochs", type=int, default=12, help="elastic, learned: training epochs")
     a = ap.parse_args()
     if a.n is None:
         a.n = 100 if a.config == "electrostatics" else 128
@@ -662,11 +667,15 @@ def run_reference_cells(args, D):
 def run_twolevel(args, D):
     """128^3 heterogeneous elasticity (2000 spheres, E 1:100): MINRES in FP64 on the reference's
     (indefinite) matrix, preconditioned by the symmetric multiplicative two-level cycle: FP16/FP32
-    Chebyshev smoothing on the textbook-orientation operator and the MsFEM coarse space built from
-    the batched cell bases (FP32 inner solves + FP64 check) with an FP64-inverted coarse matrix."""
+    Chebyshev smoothing on the textbook-orientation operator and the MsFEM coarse space with an
+    FP64-inverted coarse matrix.  The coarse bases are predicted by the learned operator (trained
+    once, before the timed steps, on cells of the same inclusion statistics whose exact bases the
+    batched cell solver makes), with the exact cell solve as per-cell fallback; --coarse exact
+    solves every cell instead (and is also timed once as a comparator)."""
     import torch
     from multiscalefemsolver3d_b200 import _lib, fem, meshgen
     from multiscalefemsolver3d_b200.cells import FP32_IR, FP64, Cells
+    from multiscalefemsolver3d_b200.learned import CoarseNet, learned_bases, train_on_cells
     from multiscalefemsolver3d_b200.twolevel import TwoLevel
 
     torch.cuda.set_device(D.local)
@@ -688,6 +697,29 @@ def run_twolevel(args, D):
     stream = torch.cuda.ExternalStream(S.stream, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     DEG, HALF = 3, True
+    learned = args.coarse == "learned"
+    net, train_info = None, {}
+    if learned:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        net = CoarseNet(seed=0)
+        ti = train_on_cells(net, args.train_cells, seed=1, epochs=args.train_epochs, batch=128, lr=1e-3)
+        torch.cuda.synchronize()
+        L = ti.pop("losses")
+        train_info = {"train_cells": ti["cells"], "train_steps": ti["steps"], "train_s_total": time.perf_counter() - t0,
+                      "train_s_data": ti["s_data"], "train_ms_cell_solves": ti["ms_cell_solves"],
+                      "train_s_optimise": ti["s_train"], "train_loss_first": float(L[:20].mean()),
+                      "train_loss_last": float(L[-50:].mean())}
+
+    def coarse_bases(C_, cells_):
+        if learned:
+            r = learned_bases(net, C_, cells_)
+            return {"ms_bases": r["ms_predict"] + r["ms_fallback"], "ms_predict": r["ms_predict"],
+                    "fallback_cells": r["fallback_cells"], "basis_residual_median": float(np.median(r["residual"]))}
+        rcb = C_.build_bases(FP32_IR, TOL)
+        if rcb != 0:
+            raise RuntimeError(f"cell bases rc={rcb}")
+        return {"ms_bases": sum(C_.report()["ms"].values())}
 
     def step():
         S.clear()
@@ -697,15 +729,14 @@ def run_twolevel(args, D):
         K.clear()
         K.assemble_elastic_textbook(p.E, p.nu)
         K.apply_dirichlet(dofs, zval, fem.ROW_AND_COLUMN)
-        rcb = C.build_bases(FP32_IR, TOL)
-        if rcb != 0:
-            raise RuntimeError(f"cell bases rc={rcb}")
+        binfo = coarse_bases(C, cc.cells)
         T = TwoLevel(S, C, cc, dofs_np)
         T.set_smoother(K, degree=DEG, half_matrix=HALF)
         S.set_x(xzero)
         rel, it, out, rc = T.solve(tol=TOL, maxiter=400000, precision=FP64)
         info = {"rel_residual": rel, "iterations": it, "refinement_steps": out, "coarse_dofs": T.n_coarse_dofs,
-                "coarse_setup_ms": T.ms_setup, "ms_solve": S.stats()["ms_solve"], "ms_bases": sum(C.report()["ms"].values())}
+                "coarse_setup_ms": T.ms_setup, "ms_solve": S.stats()["ms_solve"]}
+        info.update(binfo)
         T.close()
         if rc != 0:
             raise RuntimeError(f"two-level solve rc={rc} rel={rel}")
@@ -735,6 +766,18 @@ def run_twolevel(args, D):
 
     # comparators on the same (assembled) system
     comp = {}
+    if learned and not args.no_compare:
+        # the same two-level solve with exact bases for every cell (the method without the network)
+        rcb = C.build_bases(FP32_IR, TOL)
+        ms_b = sum(C.report()["ms"].values())
+        T = TwoLevel(S, C, cc, dofs_np)
+        T.set_smoother(K, degree=DEG, half_matrix=HALF)
+        S.set_x(xzero)
+        rel, it, out, rc = T.solve(tol=TOL, maxiter=400000, precision=FP64)
+        comp.update({"exact_bases_ms_bases": ms_b, "exact_bases_iterations": it, "exact_bases_rel_residual": rel,
+                     "exact_bases_ms_solve": S.stats()["ms_solve"], "exact_bases_coarse_setup_ms": T.ms_setup,
+                     "exact_bases_step_ms": ms_b + T.ms_setup + S.stats()["ms_solve"]})
+        T.close()
     if not args.no_compare:
         S.set_x(xzero)
         rel, it, rc = S.solve(fem.CG, FP64, tol=TOL, maxiter=2000)
@@ -767,7 +810,7 @@ def run_twolevel(args, D):
         S2.apply_dirichlet(dofs_np, np.zeros(dofs_np.size), fem.ROW_AND_COLUMN)
         K2.assemble_elastic_textbook(p.E, p.nu)
         K2.apply_dirichlet(dofs_np, np.zeros(dofs_np.size), fem.ROW_AND_COLUMN)
-        C2.build_bases(FP32_IR, TOL)
+        coarse_bases(C2, cc.cells)
         T2 = TwoLevel(S2, C2, cc, dofs_np)
         T2.set_smoother(K2, degree=DEG, half_matrix=HALF)
         S2.set_x(np.zeros(3 * m.n_nodes))
@@ -783,6 +826,8 @@ def run_twolevel(args, D):
     sol = e2e_call()
     torch.cuda.synchronize()
     e2e_ms = D.max((time.perf_counter() - t0) * 1e3)
+    if net is not None:
+        net.close()
     h2d = sum(a.nbytes for a in (m.xyz, m.tets, m.mat, p.faces, p.traction, dofs_np, cc.cells.xyz, cc.cells.tets,
                                  cc.cells.mat, cc.cells.node_off, cc.cells.tet_off, cc.cells.box,
                                  cc.cell_node_global, cc.cell_vertex)) * 1
@@ -792,15 +837,20 @@ def run_twolevel(args, D):
         base = cpu_baseline(args.n, args.sample_n, "elastic")
     if D.rank == 0:
         extra = dict(info)
+        extra.update(train_info)
         extra.update(comp)
         extra.update({"speedup_vs_jacobi_fp64_minres": (comp["jacobi_fp64_minres_ms"] / ms) if comp else None,
                       "smoother": f"Chebyshev degree {DEG} on the textbook operator, matrix values in "
-                                  f"{'FP16' if HALF else 'FP32'}, FP32 arithmetic; coarse: 8^3-hexahedron MsFEM cells",
+                                  f"{'FP16' if HALF else 'FP32'}, FP32 arithmetic; coarse: 8^3-hexahedron MsFEM cells, "
+                                  + ("bases predicted by the learned operator (4 conv layers, 32 channels, BF16 "
+                                     "tensor cores), exact cell solve as fallback" if learned else "exact bases"),
                       "spmv_fp32_ms": spmv32_ms, "spmv_fp32_gbs": ach, "spmv_fp64_ms": spmv64_ms,
                       "spmv_fp64_gbs": spmv_bytes64 / (spmv64_ms * 1e-3) / 1e9, "step_ms_all": ts})
         c = config(args.n, "elastic", extra)
         c["solver"] = ("MINRES (FP64) preconditioned by the multiplicative two-level cycle; one step = assembly "
-                       "(reference and textbook orientation) + Dirichlet + cell bases + coarse setup + solve")
+                       "(reference and textbook orientation) + Dirichlet + coarse bases ("
+                       + ("network prediction + fallback check" if learned else "exact cell solves")
+                       + ") + coarse setup + solve; network training (once, before the steps) reported separately")
         line = {"metric": METRIC, "value": ms, "unit": UNIT, "n_gpus": D.world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64-krylov+fp32/fp16-preconditioner", "data": "synthetic",

@@ -304,6 +304,18 @@ int msfem_cells_face_loads(msfem_cells_t c, int n_items, const int32_t* items, c
  * u[b] = sum_v U[cell_vertex[8c+v]] (.) psi_v(b), component by component.  U: [n_vertices][3],
  * u: [cell nodes][3] (concatenated cell numbering), host arrays. */
 int msfem_cells_reconstruct(msfem_cells_t c, int n_vertices, const int32_t* cell_vertex, const double* U, double* u);
+/* Replace the bases of every cell ([n_nodes][8][3] doubles, as msfem_cells_get_bases returns
+ * them), e.g. with predicted ones.  No reference counterpart. */
+int msfem_cells_set_bases(msfem_cells_t c, const double* bases, int on_device);
+/* Per cell, how far its current bases are from solving the cell's volume problems: over the
+ * interior nodes, rel[c] = ||A_II psi_I + A_IB psi_B|| / ||A_IB psi_B|| (all 8 bases, the matrices
+ * of the volume problems, FEM_3D_forElasticDeformation's system for each basis); 0 up to the
+ * solver tolerance for the exact bases.  rel: host [n_cells].  No reference counterpart: the
+ * learned coarse space's fallback test. */
+int msfem_cells_basis_residual(msfem_cells_t c, double* rel);
+/* Copies the bases of cell k of src into cell dst_cells[k] of dst (k < n; same node count, same
+ * cell-local numbering): the exact bases of re-solved cells back into the full set. */
+int msfem_cells_copy_bases(msfem_cells_t dst, msfem_cells_t src, int n, const int32_t* dst_cells);
 void msfem_cells_destroy(msfem_cells_t c);
 
 /* The MsFEM macro problem (MsFEM::MsFEM_forElasticDeformation_OrderBF1_forPoly, MsFEM/MsFEM.h:
@@ -368,6 +380,42 @@ int msfem_solve_twolevel(msfem_system_t fine, msfem_coarse_t c, int precision, i
  * must outlive c. */
 int msfem_coarse_set_smoother(msfem_coarse_t c, msfem_system_t textbook, int degree, double ratio, int half_matrix);
 void msfem_coarse_destroy(msfem_coarse_t c);
+
+/* ---------------------------------------------------------------------------------------
+ * Learned coarse space (no reference counterpart: the reference's Order1 bases always come
+ * from its cell problems).  A 3D convolutional operator reads a macro cell's voxelised
+ * Young's-modulus field (16^3 voxels, s ln(E / E_ref) averaged over each voxel, plus the voxel
+ * centre) and predicts the cell's 8 vector bases on its 9^3 nodes as a correction to the
+ * trilinear functions; it is trained on bases made by msfem_cells_build_bases.  Four 3x3x3
+ * layers (4 -> 32 FP32, 32 -> 32, 32 -> 32, 32 -> 24 on BF16 tensor cores with FP32
+ * accumulation), ReLU between them; Adam on FP32 master parameters.  Cells must be 8x8x8
+ * hexahedra of six Kuhn tetrahedra in Kuhn-cube node and tetrahedron order (checked).
+ * Predicted bases only feed the two-level preconditioner's coarse space; with
+ * msfem_cells_basis_residual the caller re-solves cells whose prediction is poor. */
+typedef struct msfem_net* msfem_net_t;
+/* Number of FP32 parameters (the layout of msfem_net_get_params / set_params). */
+int msfem_net_param_count(void);
+/* New network with seeded He-uniform weights (last layer x 0.1), zero biases. */
+int msfem_net_create(uint64_t seed, double E_ref, double in_scale, msfem_net_t* out);
+int msfem_net_get_params(msfem_net_t n, float* params);
+/* Sets the parameters (host array of msfem_net_param_count() floats) and resets Adam. */
+int msfem_net_set_params(msfem_net_t n, const float* params);
+/* The network input of every cell of c: vox [n_cells][16][16][16] (host). */
+int msfem_net_voxelise(msfem_net_t n, msfem_cells_t c, float* vox);
+/* Appends every cell of c (voxels, and its current bases as the target) to the training set. */
+int msfem_net_add_cells(msfem_net_t n, msfem_cells_t c, int* n_total);
+/* `steps` Adam steps (lr, betas 0.9 / 0.999) on minibatches of `batch` cells drawn from seeded
+ * permutations of the training set; losses: [steps] host floats (or NULL). */
+int msfem_net_train(msfem_net_t n, int steps, int batch, float lr, uint64_t seed, float* losses);
+/* One forward and backward pass on host data without an update: vox [cells][4096], target
+ * [cells][729][24] (psi_exact - Q1, channel 3 v + a); loss (mean square) and grad
+ * [msfem_net_param_count()] on the host. */
+int msfem_net_loss_grad(msfem_net_t n, int cells, const float* vox, const float* target, float* loss, float* grad);
+/* The last layer's output: out [cells][4096][32] (channels 24..31 zero). */
+int msfem_net_forward(msfem_net_t n, int cells, const float* vox, float* out);
+/* Predicts the bases of every cell of c into c (as msfem_cells_set_bases would); ms: device time. */
+int msfem_net_predict(msfem_net_t n, msfem_cells_t c, float* ms);
+int msfem_net_destroy(msfem_net_t n);
 
 #ifdef __cplusplus
 }

@@ -89,6 +89,9 @@ _SIGS = [
     ("msfem_cells_macro_matrices", C.c_int, [C.c_void_p, _P, C.c_int]),
     ("msfem_cells_face_loads", C.c_int, [C.c_void_p, C.c_int, _P, _P, _P]),
     ("msfem_cells_reconstruct", C.c_int, [C.c_void_p, C.c_int, _P, _P, _P]),
+    ("msfem_cells_set_bases", C.c_int, [C.c_void_p, _P, C.c_int]),
+    ("msfem_cells_basis_residual", C.c_int, [C.c_void_p, _P]),
+    ("msfem_cells_copy_bases", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, _P]),
     ("msfem_cells_destroy", None, [C.c_void_p]),
     ("msfem_macro_solve", C.c_int, [C.c_int, C.c_int, _P, _P, _P, C.c_int, _P, _P, C.c_int, C.c_double, C.c_int,
                                     _P, _P, _P]),
@@ -101,6 +104,17 @@ _SIGS = [
                                        C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("msfem_coarse_set_smoother", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_int]),
     ("msfem_coarse_destroy", None, [C.c_void_p]),
+    ("msfem_net_param_count", C.c_int, []),
+    ("msfem_net_create", C.c_int, [C.c_uint64, C.c_double, C.c_double, C.POINTER(C.c_void_p)]),
+    ("msfem_net_get_params", C.c_int, [C.c_void_p, _P]),
+    ("msfem_net_set_params", C.c_int, [C.c_void_p, _P]),
+    ("msfem_net_voxelise", C.c_int, [C.c_void_p, C.c_void_p, _P]),
+    ("msfem_net_add_cells", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]),
+    ("msfem_net_train", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_uint64, _P]),
+    ("msfem_net_loss_grad", C.c_int, [C.c_void_p, C.c_int, _P, _P, _P, _P]),
+    ("msfem_net_forward", C.c_int, [C.c_void_p, C.c_int, _P, _P]),
+    ("msfem_net_predict", C.c_int, [C.c_void_p, C.c_void_p, _P]),
+    ("msfem_net_destroy", C.c_int, [C.c_void_p]),
 ]
 
 EXPORTED = [name for name, _, _ in _SIGS]

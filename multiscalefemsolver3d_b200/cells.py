@@ -93,6 +93,25 @@ class Cells:
         check(load().msfem_cells_get_bases(self.h, _p(out), 0), "cells_get_bases")
         return out
 
+    def set_bases(self, bases):
+        """Replaces every cell's bases ([n_nodes, 8, 3])."""
+        b = _c(bases, np.float64)
+        if b.size != 24 * self.n_nodes:
+            raise ValueError("bases must be [n_nodes, 8, 3]")
+        check(load().msfem_cells_set_bases(self.h, _p(b), 0), "cells_set_bases")
+
+    def basis_residual(self):
+        """Per cell ||A_II psi_I + A_IB psi_B|| / ||A_IB psi_B|| of the current bases in the cell's
+        volume problems (about the solver tolerance for exact bases)."""
+        rel = np.empty(self.n_cells)
+        check(load().msfem_cells_basis_residual(self.h, _p(rel)), "cells_basis_residual")
+        return rel
+
+    def copy_bases_from(self, src, dst_cells):
+        """Bases of cell k of `src` (a Cells) into cell dst_cells[k] of this set."""
+        d = _c(dst_cells, np.int32)
+        check(load().msfem_cells_copy_bases(self.h, src.h, d.size, _p(d)), "cells_copy_bases")
+
     def macro_matrices(self):
         """[n_cells, 8, 8, 3, 3] MsFEM macro element matrices from the current bases."""
         K = np.empty((self.n_cells, 8, 8, 3, 3))

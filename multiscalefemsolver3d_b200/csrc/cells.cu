@@ -622,6 +622,47 @@ __global__ void __launch_bounds__(128) k_face_loads(int n_items, const int32_t* 
     }
 }
 
+// residual of the current bases in each cell's volume problem: over the free nodes i,
+// r_i = sum_j A_ij x_j for the 8 bases (no source term); rel = ||r|| / ||sum_{j fixed} A_ij x_j||
+__global__ void __launch_bounds__(256) k_basis_residual(const int64_t* __restrict__ node_off, const int64_t* __restrict__ row_ptr,
+                                                        const int32_t* __restrict__ col, const double* __restrict__ val,
+                                                        const uint8_t* __restrict__ fixed, const double* __restrict__ x,
+                                                        double* __restrict__ rel)
+{
+    const int c = blockIdx.x;
+    double num = 0.0, den = 0.0;
+    for (int64_t i = node_off[c] + threadIdx.x; i < node_off[c + 1]; i += blockDim.x) {
+        if (fixed[i]) continue;
+        double yf[24], yb[24];
+        for (int q = 0; q < 24; q++) yf[q] = yb[q] = 0.0;
+        for (int64_t k = row_ptr[i]; k < row_ptr[i + 1]; k++) {
+            const int64_t j = col[k];
+            const double* A = val + 9 * k;
+            const double* xj = x + 24 * j;
+            double* y = fixed[j] ? yb : yf;
+            for (int r = 0; r < 8; r++)
+                for (int a = 0; a < 3; a++)
+                    y[3 * r + a] += A[3 * a] * xj[3 * r] + A[3 * a + 1] * xj[3 * r + 1] + A[3 * a + 2] * xj[3 * r + 2];
+        }
+        for (int q = 0; q < 24; q++) {
+            num += (yf[q] + yb[q]) * (yf[q] + yb[q]);
+            den += yb[q] * yb[q];
+        }
+    }
+    __shared__ double s0[256], s1[256];
+    s0[threadIdx.x] = num;
+    s1[threadIdx.x] = den;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            s0[threadIdx.x] += s0[threadIdx.x + w];
+            s1[threadIdx.x] += s1[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) rel[c] = s1[0] > 0.0 ? sqrt(s0[0] / s1[0]) : (s0[0] > 0.0 ? INFINITY : 0.0);
+}
+
 // fine solution of every cell from the macro one: u[b] = sum_v U[V(c, v)] (.) psi_v(b)
 __global__ void k_reconstruct(int n_cells, const int64_t* __restrict__ node_off, const int32_t* __restrict__ cell_vertex,
                               const double* __restrict__ U, const double* __restrict__ bases, double* __restrict__ u)
@@ -908,6 +949,7 @@ int cells_build(CellsHandle& h, int precision, double tol, int maxiter, int thre
     MSFEM_CK(cudaEventRecord(h.ev[0], st));
     MSFEM_TRY(batch_assemble(F, h.fxyz.p, h.lame.p, h.n_mat));
     MSFEM_TRY(batch_assemble(V, h.xyz.p, h.lame.p, h.n_mat));
+    h.vols_assembled = true;
     MSFEM_CK(cudaEventRecord(h.ev[1], st));
     MSFEM_CK(cudaMemsetAsync(h.flag.p, 0, sizeof(int), st));
     MSFEM_CK(cudaMemsetAsync(h.prof.p, 0, sizeof(double) * 6 * h.n_nodes, st));
@@ -1117,6 +1159,69 @@ int msfem_cells_get_bases(msfem_cells_t h, double* bases, int on_device)
     MSFEM_CK(cudaSetDevice(h->device));
     MSFEM_CK(cudaMemcpyAsync(bases, h->bx.p, sizeof(double) * 24 * h->n_nodes,
                              on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, h->stream));
+    MSFEM_CK(cudaStreamSynchronize(h->stream));
+    return MSFEM_OK;
+}
+
+int msfem_cells_set_bases(msfem_cells_t h, const double* bases, int on_device)
+{
+    using namespace msfem;
+    if (!h || !bases) {
+        set_error("msfem_cells_set_bases: bad arguments");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    MSFEM_CK(cudaSetDevice(h->device));
+    MSFEM_CK(cudaMemcpyAsync(h->bx.p, bases, sizeof(double) * 24 * h->n_nodes,
+                             on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, h->stream));
+    MSFEM_CK(cudaStreamSynchronize(h->stream));
+    return MSFEM_OK;
+}
+
+int msfem_cells_copy_bases(msfem_cells_t dst, msfem_cells_t src, int n, const int32_t* dst_cells)
+{
+    using namespace msfem;
+    if (!dst || !src || n < 0 || n > src->n_cells || (n > 0 && !dst_cells)) {
+        set_error("msfem_cells_copy_bases: bad arguments");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    for (int k = 0; k < n; k++) {
+        const int c = dst_cells[k];
+        if (c < 0 || c >= dst->n_cells ||
+            dst->h_node_off[c + 1] - dst->h_node_off[c] != src->h_node_off[k + 1] - src->h_node_off[k]) {
+            set_error("msfem_cells_copy_bases: cell %d of the source does not fit cell %d of the target", k, c);
+            return MSFEM_ERR_ARGUMENT;
+        }
+    }
+    MSFEM_CK(cudaSetDevice(dst->device));
+    MSFEM_CK(cudaStreamSynchronize(src->stream));
+    for (int k = 0; k < n; k++) {
+        const int c = dst_cells[k];
+        const int64_t nn = src->h_node_off[k + 1] - src->h_node_off[k];
+        MSFEM_CK(cudaMemcpyAsync(dst->bx.p + 24 * dst->h_node_off[c], src->bx.p + 24 * src->h_node_off[k],
+                                 sizeof(double) * 24 * nn, cudaMemcpyDeviceToDevice, dst->stream));
+    }
+    MSFEM_CK(cudaStreamSynchronize(dst->stream));
+    return MSFEM_OK;
+}
+
+int msfem_cells_basis_residual(msfem_cells_t h, double* rel)
+{
+    using namespace msfem;
+    if (!h || !rel) {
+        set_error("msfem_cells_basis_residual: bad arguments");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    MSFEM_CK(cudaSetDevice(h->device));
+    BatchSys& V = h->vols;
+    if (!h->vols_assembled) {
+        MSFEM_TRY(batch_assemble(V, h->xyz.p, h->lame.p, h->n_mat));
+        h->vols_assembled = true;
+    }
+    DBuf<double> d;
+    MSFEM_TRY(d.alloc(h->n_cells));
+    k_basis_residual<<<h->n_cells, 256, 0, h->stream>>>(V.node_off.p, V.row_ptr.p, V.col.p, V.val64.p, V.fixed.p, h->bx.p, d.p);
+    MSFEM_CK(cudaGetLastError());
+    MSFEM_CK(cudaMemcpyAsync(rel, d.p, sizeof(double) * h->n_cells, cudaMemcpyDeviceToHost, h->stream));
     MSFEM_CK(cudaStreamSynchronize(h->stream));
     return MSFEM_OK;
 }

@@ -36,6 +36,7 @@ struct CellsHandle {
     BatchSys faces, vols;
     DBuf<double> fxyz, prof, fx, bx;
     int cap = 0;
+    bool vols_assembled = false;  // volume problem matrices hold the current materials
     DBuf<int32_t> edge_nodes, edge_len, seg_tri;
     DBuf<int> flag;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};

@@ -272,6 +272,59 @@ def msfem_cells(n_coarse: int = 16, m_choices=(8, 12, 16, 20), seed: int = 3, ma
                       nu=np.array([nu, nu]), m=ms[sel].astype(np.int32))
 
 
+def subset_cells(cm: CellMeshes, idx) -> CellMeshes:
+    """The cells `idx` of cm (in that order) as their own CellMeshes."""
+    idx = np.asarray(idx, dtype=np.int64)
+    nn = cm.node_off[idx + 1] - cm.node_off[idx]
+    nt = cm.tet_off[idx + 1] - cm.tet_off[idx]
+    node_rows = np.concatenate([np.arange(cm.node_off[c], cm.node_off[c + 1]) for c in idx]) if idx.size else np.zeros(0, np.int64)
+    tet_rows = np.concatenate([np.arange(cm.tet_off[c], cm.tet_off[c + 1]) for c in idx]) if idx.size else np.zeros(0, np.int64)
+    return CellMeshes(node_off=np.concatenate([[0], np.cumsum(nn)]).astype(np.int64), xyz=cm.xyz[node_rows],
+                      tet_off=np.concatenate([[0], np.cumsum(nt)]).astype(np.int64), tets=cm.tets[tet_rows],
+                      mat=cm.mat[tet_rows], box=cm.box[idx], E=cm.E, nu=cm.nu, m=cm.m[idx])
+
+
+def sphere_cells(n_cells: int, seed: int = 0, m: int = 8, density: float = 0.58, rmin: float = 0.24,
+                 rmax: float = 0.56, contrast: float = 100.0, nu: float = 0.3, h: float = 1.0 / 16.0) -> CellMeshes:
+    """n_cells independent macro cells of kuhn_cube(m) (edge h, laid out along x) cut from a random
+    field of spherical inclusions like the elasticity workload's (2000 spheres of radius
+    U(0.015, 0.035) in the unit cube cut into 16^3 cells: radii U(0.24, 0.56) in cell units, about
+    13 % inclusion volume): sphere centres with `density` per cell volume, uniform over the cell
+    grown by rmax on every side so that spheres of neighbouring cells cut in; no two spheres of a
+    cell overlap (rejection in draw order, which favours small radii, as the workload's own
+    placement does).  Tets whose centroid lies in a sphere take material 1
+    (E = contrast, nu)."""
+    rng = np.random.default_rng(seed)
+    t = kuhn_cube(m)
+    cen = tet_centroids(t)
+    side = 1.0 + 2.0 * rmax
+    xyzs, mats, boxes = [], [], []
+    for c in range(n_cells):
+        k = rng.poisson(density * side ** 3)
+        cs, rs = [], []
+        for _ in range(k):
+            for _try in range(50):
+                p = rng.uniform(-rmax, 1.0 + rmax, size=3)
+                r = rng.uniform(rmin, rmax)
+                if all(np.linalg.norm(p - q) >= r + s for q, s in zip(cs, rs)):
+                    cs.append(p)
+                    rs.append(r)
+                    break
+        inside = np.zeros(cen.shape[0], dtype=bool)
+        for p, r in zip(cs, rs):
+            inside |= ((cen - p) ** 2).sum(axis=1) < r * r
+        lo = np.array([c * h, 0.0, 0.0])
+        xyzs.append(lo + t.xyz * h)
+        mats.append(inside.astype(np.int32))
+        boxes.append([lo[0], lo[0] + h, 0.0, h, 0.0, h])
+    nn, nt = t.xyz.shape[0], t.tets.shape[0]
+    return CellMeshes(node_off=np.arange(n_cells + 1, dtype=np.int64) * nn, xyz=np.concatenate(xyzs),
+                      tet_off=np.arange(n_cells + 1, dtype=np.int64) * nt,
+                      tets=np.tile(t.tets, (n_cells, 1)).astype(np.int32), mat=np.concatenate(mats),
+                      box=np.array(boxes), E=np.array([1.0, contrast]), nu=np.array([nu, nu]),
+                      m=np.full(n_cells, m, dtype=np.int32))
+
+
 @dataclass
 class CubeCells:
     """A structured cube mesh (kuhn_cube(n)) cut into nc^3 macro cells of H = n/nc hexahedra
