@@ -114,6 +114,7 @@ _SIGS = [
     ("msfem_net_loss_grad", C.c_int, [C.c_void_p, C.c_int, _P, _P, _P, _P]),
     ("msfem_net_forward", C.c_int, [C.c_void_p, C.c_int, _P, _P]),
     ("msfem_net_predict", C.c_int, [C.c_void_p, C.c_void_p, _P]),
+    ("msfem_net_set_tensor_path", C.c_int, [C.c_void_p, C.c_int]),
     ("msfem_net_destroy", C.c_int, [C.c_void_p]),
 ]
 

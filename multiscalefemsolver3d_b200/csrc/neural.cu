@@ -315,6 +315,188 @@ __global__ void __launch_bounds__(256, 1) k_conv32(const __nv_bfloat16* __restri
     }
 }
 
+// ---- the same convolution on the 5th-generation tensor cores (tcgen05, accumulators in TMEM).
+// One CTA (4 warps) per cell walks its 16 z-planes.  Per plane the GEMM is D[256 voxels][32] =
+// sum over 27 taps x 2 k16 steps of A_tap[256][16] B_tap[16][32], issued by one thread as 4
+// M = 64 tiles (8 y rows x 8 x of one x-half) x 54 tcgen05.mma (kind::f16, BF16 in, FP32
+// accumulate, N = 32).  Operands come from shared memory through K-major, no-swizzle descriptors
+// (8-row x 16-byte core matrices): a tile's core matrix g is y row g, 8 consecutive x records, so
+// every tap is the same descriptor with its start moved by (dy, dx) records -- the halo is stored
+// once per plane, [16-byte channel chunk][18 y][18 x] (x and y from -1 to 16, zero outside), in
+// a ring of 4 plane slots; the weights as [chunk][tap][co].  The ring lets the loads of plane
+// z + 2 overlap the MMAs and the epilogue of plane z.  TMEM: x-half h at lane offset 16 h (the
+// M = 64 accumulator layout: row m in lane m % 16 + 32 (m / 16)), y block b at column 32 b.
+// Completion is signalled on an mbarrier through tcgen05.commit; every wait on it is bounded (a
+// timeout sets *err and skips the epilogue).  The epilogue reads one voxel's 32 channels per
+// thread with tcgen05.ld and writes its 64 (BF16) or 128 (FP32) contiguous bytes.
+constexpr int kTcRow = 18 * 16;                            // one y row of records (bytes)
+constexpr int kTcChunk = 18 * kTcRow;                      // 5,184 B: one channel chunk of a plane
+constexpr int kTcSlot = 4 * kTcChunk;                      // 20,736 B: one plane
+constexpr int kTcA = 4 * kTcSlot;                          // 82,944 B: the ring
+constexpr int kTcB = 4 * kTaps * kCh * 16;                 // 55,296 B
+constexpr int kTcSmem = kTcA + kTcB + 16;                  // + mbarrier + TMEM address
+constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kCh >> 3) << 17) | ((uint32_t)(64 >> 4) << 24);
+
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | ((uint64_t)1 << 46);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(kTcIdesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity)
+{
+    for (int i = 0; i < (1 << 22); i++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// plane gz of one cell into ring slot `slot`: [chunk][18 y][18 x] records, zero outside the cell
+__device__ __forceinline__ void tc_load_plane(unsigned char* A, const __nv_bfloat16* cell_base, int gz, int slot)
+{
+    for (int q = threadIdx.x; q < 4 * 18 * 18; q += blockDim.x) {
+        const int c = q / 324, hy = (q / 18) % 18, hx = q % 18;
+        const int gy = hy - 1, gx = hx - 1;
+        const uint32_t off = slot * kTcSlot + c * kTcChunk + (hy * 18 + hx) * 16;
+        if (gz >= 0 && gz < kV && gy >= 0 && gy < kV && gx >= 0 && gx < kV)
+            cp_async16(smem_u32(A) + off, cell_base + ((size_t)((gz * kV + gy) * kV + gx) * kCh + c * 8));
+        else
+            *reinterpret_cast<uint4*>(A + off) = make_uint4(0, 0, 0, 0);
+    }
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(128, 1) k_conv32_tc(const __nv_bfloat16* __restrict__ in, const __nv_bfloat16* __restrict__ w,
+                                                      const float* __restrict__ bias, const __nv_bfloat16* __restrict__ mask,
+                                                      __nv_bfloat16* __restrict__ out, float* __restrict__ outf, int* err)
+{
+    extern __shared__ __align__(128) unsigned char sm[];
+    unsigned char* A = sm;
+    unsigned char* B = sm + kTcA;
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + kTcA + kTcB);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kTcA + kTcB + 8);
+    const int cell = blockIdx.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const __nv_bfloat16* inc = in + (size_t)cell * kVox * kCh;
+    const uint32_t bar = smem_u32(mbar);
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar));
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;\n" ::"r"(smem_u32(tslot)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    // weights [chunk][tap][co] x 16 B from w[tap][co][ci]
+    for (int q = tid; q < kTaps * kCh * 4; q += blockDim.x) {
+        const int row = q >> 2, c = q & 3;
+        cp_async16(smem_u32(B) + (c * kTaps * kCh + row) * 16, w + (size_t)row * kCh + c * 8);
+    }
+    // planes -1, 0, 1 in slots 0, 1, 2 (plane gz lives in slot (gz + 1) % 4)
+    tc_load_plane(A, inc, -1, 0);
+    tc_load_plane(A, inc, 0, 1);
+    tc_load_plane(A, inc, 1, 2);
+    cp_async_wait_all();
+    asm volatile("fence.proxy.async.shared::cta;\n" ::);
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    const uint32_t tbase = *tslot;
+    const uint32_t a0 = smem_u32(A), b0 = smem_u32(B);
+    // this thread's accumulator row: x-half h = lane / 16, row m = 16 warp + lane % 16 of the tile
+    const int h = lane >> 4, m = 16 * warp + (lane & 15);
+    bool ok = true;
+    for (int z = 0; z < kV; z++) {
+        if (tid == 0 && ok) {
+            for (int yb = 0; yb < 2; yb++)
+                for (int hh = 0; hh < 2; hh++)
+                    for (int tap = 0; tap < kTaps; tap++) {
+                        const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3, slot = (z + dz) & 3;
+                        for (int kc = 0; kc < 2; kc++) {
+                            const uint32_t aoff = slot * kTcSlot + 2 * kc * kTcChunk + ((8 * yb + dy) * 18 + 8 * hh + dx) * 16;
+                            const uint32_t boff = (2 * kc * kTaps + tap) * kCh * 16;
+                            tc_mma(tbase + ((uint32_t)(16 * hh) << 16) + 32 * yb, tc_desc(a0 + aoff, kTcChunk, kTcRow),
+                                   tc_desc(b0 + boff, kTaps * kCh * 16, 128), (tap | kc) != 0);
+                        }
+                    }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar) : "memory");
+        }
+        // plane z + 2 into the slot plane z - 2 used (its MMAs finished in the previous step)
+        tc_load_plane(A, inc, z + 2, (z + 3) & 3);
+        ok = ok && tc_wait(bar, z & 1);
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+        if (ok) {
+#pragma unroll
+            for (int yb = 0; yb < 2; yb++) {
+                uint32_t v[32];
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+                    "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                      "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+                      "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+                      "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                    : "r"(tbase + ((uint32_t)(32 * warp) << 16) + 32 * yb));
+                asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+                const int y = 8 * yb + (m >> 3), xv = 8 * h + (m & 7);
+                const size_t vox = (size_t)cell * kVox + (z * kV + y) * kV + xv;
+                if (EPI == kEpiF32) {
+                    float4* o = reinterpret_cast<float4*>(outf + vox * kCh);
+#pragma unroll
+                    for (int k = 0; k < 8; k++)
+                        o[k] = make_float4(__uint_as_float(v[4 * k]) + bias[4 * k], __uint_as_float(v[4 * k + 1]) + bias[4 * k + 1],
+                                           __uint_as_float(v[4 * k + 2]) + bias[4 * k + 2], __uint_as_float(v[4 * k + 3]) + bias[4 * k + 3]);
+                } else {
+                    __nv_bfloat162 hv[16];
+                    if (EPI == kEpiRelu) {
+#pragma unroll
+                        for (int k = 0; k < 16; k++)
+                            hv[k] = __floats2bfloat162_rn(fmaxf(__uint_as_float(v[2 * k]) + bias[2 * k], 0.f),
+                                                          fmaxf(__uint_as_float(v[2 * k + 1]) + bias[2 * k + 1], 0.f));
+                    } else {
+                        uint4 mm[4];
+                        const uint4* mp = reinterpret_cast<const uint4*>(mask + vox * kCh);
+#pragma unroll
+                        for (int k = 0; k < 4; k++) mm[k] = mp[k];
+                        const __nv_bfloat162* m2 = reinterpret_cast<const __nv_bfloat162*>(mm);
+#pragma unroll
+                        for (int k = 0; k < 16; k++)
+                            hv[k] = __floats2bfloat162_rn(__bfloat162float(m2[k].x) > 0.f ? __uint_as_float(v[2 * k]) : 0.f,
+                                                          __bfloat162float(m2[k].y) > 0.f ? __uint_as_float(v[2 * k + 1]) : 0.f);
+                    }
+                    uint4* o = reinterpret_cast<uint4*>(out + vox * kCh);
+                    const uint4* hs = reinterpret_cast<const uint4*>(hv);
+#pragma unroll
+                    for (int k = 0; k < 4; k++) o[k] = hs[k];
+                }
+            }
+        }
+        cp_async_wait_all();
+        asm volatile("fence.proxy.async.shared::cta;\n" ::);
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    }
+    if (!ok && tid == 0) atomicExch(err, 1);
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;\n" ::"r"(tbase));
+}
+
 // dW[tap][co][ci] = sum_v dZ[v][co] A[v + tap][ci] and db[co] = sum_v dZ[v][co] over the cells of
 // this CTA (one fixed-order partial per CTA).  M = co (two m16 tiles, A operand = dZ^T through
 // ldmatrix.trans), N = ci (four n8 tiles, B operand = shifted activations through ldmatrix.trans),
@@ -647,6 +829,8 @@ struct NetHandle {
     DBuf<__nv_bfloat16> a0, a1, a2, d0, d1;
     DBuf<int32_t> idx;
     DBuf<int> flag;
+    DBuf<int> err;       // set by a tcgen05 kernel whose completion wait timed out
+    int tcgen05 = 0;     // 1: layers 1-3 on tcgen05 (k_conv32_tc), 0: mma.sync (k_conv32)
     ~NetHandle()
     {
         if (stream) cudaStreamDestroy(stream);
@@ -683,8 +867,22 @@ int conv_attrs()
     MSFEM_CK(cudaFuncSetAttribute(k_conv32<kEpiF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmem));
     MSFEM_CK(cudaFuncSetAttribute(k_conv32<kEpiMask>, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmem));
     MSFEM_CK(cudaFuncSetAttribute(k_wgrad32, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgradSmem));
+    MSFEM_CK(cudaFuncSetAttribute(k_conv32_tc<kEpiRelu>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
+    MSFEM_CK(cudaFuncSetAttribute(k_conv32_tc<kEpiF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
+    MSFEM_CK(cudaFuncSetAttribute(k_conv32_tc<kEpiMask>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
     done = true;
     return 0;
+}
+
+// one 32 -> 32 convolution of n cells on the selected tensor-core path
+template <int EPI>
+void conv(NetHandle& N, int n, const __nv_bfloat16* in, const __nv_bfloat16* w, const float* bias, const __nv_bfloat16* mask,
+          __nv_bfloat16* out, float* outf)
+{
+    if (N.tcgen05)
+        k_conv32_tc<EPI><<<n, 128, kTcSmem, N.stream>>>(in, w, bias, mask, out, outf, N.err.p);
+    else
+        k_conv32<EPI><<<dim3(8, n), 256, kConvSmem, N.stream>>>(in, w, bias, mask, out, outf);
 }
 
 // forward of n cells held in N.x -> N.a0, N.a1, N.a2, N.o
@@ -694,12 +892,23 @@ int net_forward(NetHandle& N, int n)
     MSFEM_TRY(conv_attrs());
     const __nv_bfloat16* wf = N.wf.p;
     k_first_fwd<<<dim3(kV, n), 256, 0, st>>>(N.x.p, N.p.p, N.a0.p);
-    k_conv32<kEpiRelu><<<dim3(8, n), 256, kConvSmem, st>>>(N.a0.p, wf, N.p.p + layer_base(1) + kLayerW, nullptr, N.a1.p, nullptr);
-    k_conv32<kEpiRelu><<<dim3(8, n), 256, kConvSmem, st>>>(N.a1.p, wf + kLayerW, N.p.p + layer_base(2) + kLayerW, nullptr,
-                                                          N.a2.p, nullptr);
-    k_conv32<kEpiF32><<<dim3(8, n), 256, kConvSmem, st>>>(N.a2.p, wf + 2 * kLayerW, N.p.p + layer_base(3) + kLayerW, nullptr,
-                                                         nullptr, N.o.p);
+    conv<kEpiRelu>(N, n, N.a0.p, wf, N.p.p + layer_base(1) + kLayerW, nullptr, N.a1.p, nullptr);
+    conv<kEpiRelu>(N, n, N.a1.p, wf + kLayerW, N.p.p + layer_base(2) + kLayerW, nullptr, N.a2.p, nullptr);
+    conv<kEpiF32>(N, n, N.a2.p, wf + 2 * kLayerW, N.p.p + layer_base(3) + kLayerW, nullptr, nullptr, N.o.p);
     MSFEM_CK(cudaGetLastError());
+    return 0;
+}
+
+// the tcgen05 kernels' timeout flag (read after the caller's synchronisation)
+int check_err(NetHandle& N)
+{
+    int e = 0;
+    MSFEM_CK(cudaMemcpyAsync(&e, N.err.p, sizeof(int), cudaMemcpyDeviceToHost, N.stream));
+    MSFEM_CK(cudaStreamSynchronize(N.stream));
+    if (e) {
+        set_error("learned coarse space: a tensor-core completion wait timed out");
+        return MSFEM_ERR_CUDA;
+    }
     return 0;
 }
 
@@ -727,13 +936,13 @@ int net_loss_backward(NetHandle& N, int n, float* d_loss)
     const __nv_bfloat16* wb = N.wb.p;
     // layer 3
     MSFEM_TRY(wgrad_layer(N, n, N.a2.p, N.d0.p, N.g.p + layer_base(3)));
-    k_conv32<kEpiMask><<<dim3(8, n), 256, kConvSmem, st>>>(N.d0.p, wb + 2 * kLayerW, nullptr, N.a2.p, N.d1.p, nullptr);
+    conv<kEpiMask>(N, n, N.d0.p, wb + 2 * kLayerW, nullptr, N.a2.p, N.d1.p, nullptr);
     // layer 2
     MSFEM_TRY(wgrad_layer(N, n, N.a1.p, N.d1.p, N.g.p + layer_base(2)));
-    k_conv32<kEpiMask><<<dim3(8, n), 256, kConvSmem, st>>>(N.d1.p, wb + kLayerW, nullptr, N.a1.p, N.d0.p, nullptr);
+    conv<kEpiMask>(N, n, N.d1.p, wb + kLayerW, nullptr, N.a1.p, N.d0.p, nullptr);
     // layer 1
     MSFEM_TRY(wgrad_layer(N, n, N.a0.p, N.d0.p, N.g.p + layer_base(1)));
-    k_conv32<kEpiMask><<<dim3(8, n), 256, kConvSmem, st>>>(N.d0.p, wb, nullptr, N.a0.p, N.d1.p, nullptr);
+    conv<kEpiMask>(N, n, N.d0.p, wb, nullptr, N.a0.p, N.d1.p, nullptr);
     // layer 0
     const int n_parts = std::min(n, N.cap);
     const int per = (n + n_parts - 1) / n_parts;
@@ -836,6 +1045,7 @@ int msfem_net_create(uint64_t seed, double E_ref, double in_scale, msfem_net_t* 
     MSFEM_TRY(h->wf.alloc(3 * kLayerW));
     MSFEM_TRY(h->wb.alloc(3 * kLayerW));
     MSFEM_TRY(h->loss_dev.alloc(1));
+    MSFEM_TRY(h->err.alloc(1));
     // uniform(-b, b) with b = sqrt(6 / fan_in) (He), the last layer scaled by 0.1 so that the
     // untrained network starts near the trilinear coarse space; biases zero; padded rows zero
     std::vector<float> p(kParams, 0.f);
@@ -855,6 +1065,7 @@ int msfem_net_create(uint64_t seed, double E_ref, double in_scale, msfem_net_t* 
     MSFEM_CK(cudaMemsetAsync(h->g.p, 0, sizeof(float) * kParams, st));
     MSFEM_CK(cudaMemsetAsync(h->m.p, 0, sizeof(float) * kParams, st));
     MSFEM_CK(cudaMemsetAsync(h->v.p, 0, sizeof(float) * kParams, st));
+    MSFEM_CK(cudaMemsetAsync(h->err.p, 0, sizeof(int), st));
     MSFEM_TRY(upload_params(*h));
     MSFEM_CK(cudaStreamSynchronize(st));
     *out = h.release();
@@ -991,7 +1202,7 @@ int msfem_net_train(msfem_net_t h, int steps, int batch, float lr, uint64_t seed
     MSFEM_CK(cudaGetLastError());
     if (losses) MSFEM_CK(cudaMemcpyAsync(losses, dloss.p, sizeof(float) * steps, cudaMemcpyDeviceToHost, st));
     MSFEM_CK(cudaStreamSynchronize(st));
-    return MSFEM_OK;
+    return check_err(*h);
 }
 
 int msfem_net_loss_grad(msfem_net_t h, int n, const float* vox, const float* target, float* loss, float* grad)
@@ -1009,7 +1220,7 @@ int msfem_net_loss_grad(msfem_net_t h, int n, const float* vox, const float* tar
     if (loss) MSFEM_CK(cudaMemcpyAsync(loss, h->loss_dev.p, sizeof(float), cudaMemcpyDeviceToHost, st));
     if (grad) MSFEM_CK(cudaMemcpyAsync(grad, h->g.p, sizeof(float) * kParams, cudaMemcpyDeviceToHost, st));
     MSFEM_CK(cudaStreamSynchronize(st));
-    return MSFEM_OK;
+    return check_err(*h);
 }
 
 int msfem_net_forward(msfem_net_t h, int n, const float* vox, float* out)
@@ -1025,7 +1236,7 @@ int msfem_net_forward(msfem_net_t h, int n, const float* vox, float* out)
     MSFEM_TRY(net_forward(*h, n));
     MSFEM_CK(cudaMemcpyAsync(out, h->o.p, sizeof(float) * n * kVox * kCh, cudaMemcpyDeviceToHost, st));
     MSFEM_CK(cudaStreamSynchronize(st));
-    return MSFEM_OK;
+    return check_err(*h);
 }
 
 int msfem_net_predict(msfem_net_t h, msfem_cells_t cells, float* ms)
@@ -1063,6 +1274,17 @@ int msfem_net_predict(msfem_net_t h, msfem_cells_t cells, float* ms)
     MSFEM_CK(cudaGetLastError());
     if (rc) return rc;
     if (ms) *ms = t;
+    return check_err(*h);
+}
+
+int msfem_net_set_tensor_path(msfem_net_t h, int tcgen05)
+{
+    using namespace msfem;
+    if (!h || (tcgen05 != 0 && tcgen05 != 1)) {
+        set_error("msfem_net_set_tensor_path: bad arguments");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    h->tcgen05 = tcgen05;
     return MSFEM_OK;
 }
 

@@ -50,6 +50,10 @@ class CoarseNet:
         self.n_params = L.msfem_net_param_count()
         self.n_train = 0
 
+    def set_tensor_path(self, tcgen05: bool):
+        """Layers 1-3 on tcgen05 (TMEM accumulators) or on warp-level mma.sync."""
+        check(load().msfem_net_set_tensor_path(self.h, int(bool(tcgen05))), "net_set_tensor_path")
+
     def params(self) -> np.ndarray:
         p = np.empty(self.n_params, np.float32)
         check(load().msfem_net_get_params(self.h, _p(p)), "net_get_params")

@@ -18,6 +18,12 @@ the multiplicative cycle and FP64 MINRES to 1e-8.
 
 runs the batched Order1 cell bases of n^3 macro cells of the 16^3-cell workload's kind (per-cell
 resolution from {8, 12, 16, 20}, ellipsoidal inclusions E 1:50): edges, faces, volumes.
+
+    python -m multiscalefemsolver3d_b200.profile_case --net 512
+
+runs the learned coarse space's forward pass over 512 sphere cells twice: layers 1-3 on the
+mma.sync kernels (k_conv32<0>, k_conv32<0>, k_conv32<1>), then on tcgen05 (k_conv32_tc, same
+order).
 """
 from __future__ import annotations
 
@@ -32,8 +38,11 @@ def main():
     ap.add_argument("--elastic", action="store_true", help="elasticity cube instead of electrostatics")
     ap.add_argument("--twolevel", action="store_true", help="two-level elasticity solve at n^3")
     ap.add_argument("--cells", type=int, default=0, help="batched cell bases of cells^3 macro cells")
+    ap.add_argument("--net", type=int, default=0, help="network forward passes over this many cells")
     a = ap.parse_args()
     from . import fem, meshgen
+    if a.net:
+        return net_case(a.net)
     if a.cells:
         return cells_case(a.cells)
     if a.twolevel:
@@ -104,6 +113,28 @@ def twolevel_case(n):
     C.close()
     K.close()
     S.close()
+
+
+def net_case(n):
+    import time
+
+    import numpy as np
+
+    from . import meshgen
+    from .cells import Cells
+    from .learned import CoarseNet
+    net = CoarseNet(seed=0)
+    C = Cells(meshgen.sphere_cells(n, seed=3))
+    vox = net.voxelise(C)
+    out = {"cells": n}
+    for tc in (False, True):
+        net.set_tensor_path(tc)
+        t = time.perf_counter()
+        o = net.forward(vox)
+        out["tcgen05" if tc else "mma_sync"] = {"s_wall": time.perf_counter() - t, "checksum": float(np.abs(o).sum())}
+    print(json.dumps(out))
+    net.close()
+    C.close()
 
 
 if __name__ == "__main__":
