@@ -373,12 +373,20 @@ int msfem_solve_twolevel(msfem_system_t fine, msfem_coarse_t c, int precision, i
  * on the textbook operator: `textbook` is a second system on the same mesh assembled with
  * msfem_assemble_elastic_textbook and given the same Dirichlet rows.  One application of M^-1:
  * `degree` Chebyshev steps on its Jacobi-scaled FP32 matrix (spectrum bound [lmax/ratio, lmax],
- * lmax from 30 power steps), the coarse correction, the same Chebyshev steps again; SPD, so
+ * lmax from 50 power steps x 1.1, widened by the solve if a step fails), the coarse correction,
+ * the same Chebyshev steps again; SPD, so
  * MINRES on the reference's matrix keeps its guarantees.  half_matrix = 1 stores the smoother's
  * matrix values in FP16 (arithmetic stays FP32; rounding each entry keeps the matrix symmetric, so
  * the cycle stays SPD; it halves the bytes of the 2*degree SpMVs per cycle).  The textbook system
  * must outlive c. */
 int msfem_coarse_set_smoother(msfem_coarse_t c, msfem_system_t textbook, int degree, double ratio, int half_matrix);
+/* Robustness record of the two-level preconditioner: cells whose bases left [-3, 3] and were
+ * replaced by the trilinear functions of their box in the prolongation (the reference's cell
+ * operator is indefinite; a nearly singular cell problem returns bases in the thousands, which
+ * would make the coarse matrix unusable), the smoother's current lambda_max bound, and how often
+ * msfem_solve_twolevel widened it (x1.5, after a refinement step that raised the residual or
+ * broke down; the step is undone and repeated).  Any argument may be NULL. */
+int msfem_coarse_stats(msfem_coarse_t c, int* trilinear_cells, double* lambda_max, int* widened);
 void msfem_coarse_destroy(msfem_coarse_t c);
 
 /* ---------------------------------------------------------------------------------------
@@ -402,7 +410,9 @@ int msfem_net_get_params(msfem_net_t n, float* params);
 int msfem_net_set_params(msfem_net_t n, const float* params);
 /* The network input of every cell of c: vox [n_cells][16][16][16] (host). */
 int msfem_net_voxelise(msfem_net_t n, msfem_cells_t c, float* vox);
-/* Appends every cell of c (voxels, and its current bases as the target) to the training set. */
+/* Appends every cell of c (voxels, and its current bases as the target) to the training set; a
+ * cell whose bases leave [-3, 3] gets the trilinear functions as its target, as the two-level
+ * coarse build would use it. */
 int msfem_net_add_cells(msfem_net_t n, msfem_cells_t c, int* n_total);
 /* `steps` Adam steps (lr, betas 0.9 / 0.999) on minibatches of `batch` cells drawn from seeded
  * permutations of the training set; losses: [steps] host floats (or NULL). */

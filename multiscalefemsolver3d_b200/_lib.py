@@ -103,6 +103,7 @@ _SIGS = [
     ("msfem_solve_twolevel", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double, C.POINTER(C.c_double),
                                        C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("msfem_coarse_set_smoother", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_int]),
+    ("msfem_coarse_stats", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int)]),
     ("msfem_coarse_destroy", None, [C.c_void_p]),
     ("msfem_net_param_count", C.c_int, []),
     ("msfem_net_create", C.c_int, [C.c_uint64, C.c_double, C.c_double, C.POINTER(C.c_void_p)]),

@@ -22,7 +22,8 @@
 //   node   corr[n][3 v + a] = mean of L3 over the voxels touching node n (a partition: voxel x
 //          belongs to node (x + 1) / 2 along each axis), zero at the 8 cell vertices
 //   basis  psi_v^a(n) = Q1_v(n) + corr[n][3 v + a]   (Q1: trilinear in the node's grid position)
-// Loss: mean over cells, nodes and the 24 channels of (corr - (psi_exact - Q1))^2.
+// Loss: mean over cells, nodes and the 24 channels of (corr - (psi_exact - Q1))^2; a training
+// cell whose exact bases leave [-3, 3] (a nearly singular cell problem) has target corr = 0.
 // Training: Adam on the FP32 master parameters; every gradient is deterministic (fixed-order
 // partial sums, no atomics).
 #include <cuda_bf16.h>
@@ -679,9 +680,23 @@ __device__ __forceinline__ float q1(int v, int i, int j, int k)
     return ((v & 1) ? tx : 1.f - tx) * ((v & 2) ? ty : 1.f - ty) * ((v & 4) ? tz : 1.f - tz);
 }
 
-// targets y[cell][node][3 v + a] = psi_exact - Q1 from the cells' current bases
+// cells whose bases leave [-3, 3] (the bound the two-level coarse build applies: a nearly
+// singular cell problem of the reference's indefinite operator): their target is the trilinear
+// space itself (zero correction), as the coarse space would use it
+__global__ void k_wild_targets(int c_first, const int64_t* __restrict__ node_off, const double* __restrict__ bx,
+                               uint8_t* __restrict__ wild)
+{
+    const int c = blockIdx.x;
+    int bad = 0;
+    for (int64_t q = 24 * node_off[c_first + c] + threadIdx.x; q < 24 * node_off[c_first + c + 1]; q += blockDim.x)
+        bad |= !(fabs(bx[q]) <= 3.0);
+    bad = __syncthreads_or(bad);
+    if (threadIdx.x == 0) wild[c] = (uint8_t)(bad != 0);
+}
+
+// targets y[cell][node][3 v + a] = psi_exact - Q1 from the cells' current bases (0 for wild cells)
 __global__ void k_targets(int n_cells, int c_first, const int64_t* __restrict__ node_off, const double* __restrict__ bx,
-                          float* __restrict__ y)
+                          const uint8_t* __restrict__ wild, float* __restrict__ y)
 {
     const int64_t total = (int64_t)n_cells * kNodes * kOut;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
@@ -689,7 +704,7 @@ __global__ void k_targets(int n_cells, int c_first, const int64_t* __restrict__ 
         const int n = r / kOut, ch = r % kOut, v = ch / 3;
         const int i = n % kN, j = (n / kN) % kN, k = n / (kN * kN);
         const double b = bx[(node_off[c_first + cell] + n) * 24 + ch];
-        y[q] = (float)(b - (double)q1(v, i, j, k));
+        y[q] = wild[cell] ? 0.f : (float)(b - (double)q1(v, i, j, k));
     }
 }
 
@@ -1148,7 +1163,10 @@ int msfem_net_add_cells(msfem_net_t h, msfem_cells_t cells, int* n_total)
     MSFEM_TRY(log_moduli(*h, C, le));
     k_voxelise<<<grid_for((int64_t)C.n_cells * kVox), 256, 0, st>>>(C.n_cells, C.tet_off.p, C.mat.p, le.p, C.n_mat,
                                                                     nx.p + n_old * kVox);
-    k_targets<<<grid_for((int64_t)C.n_cells * kNodes * kOut), 256, 0, st>>>(C.n_cells, 0, C.node_off.p, C.bx.p,
+    DBuf<uint8_t> wild;
+    MSFEM_TRY(wild.alloc(C.n_cells));
+    k_wild_targets<<<C.n_cells, 256, 0, st>>>(0, C.node_off.p, C.bx.p, wild.p);
+    k_targets<<<grid_for((int64_t)C.n_cells * kNodes * kOut), 256, 0, st>>>(C.n_cells, 0, C.node_off.p, C.bx.p, wild.p,
                                                                             ny.p + n_old * kNodes * kOut);
     MSFEM_CK(cudaGetLastError());
     MSFEM_CK(cudaStreamSynchronize(st));

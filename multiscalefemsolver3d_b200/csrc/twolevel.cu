@@ -93,13 +93,30 @@ __global__ void k_inc_fill(int n_fine, int32_t* __restrict__ inc_ptr, int* bad)
         if (inc_ptr[g] < 0) atomicExch(bad, 2);
 }
 
+// cells whose bases leave [-kWildBasis, kWildBasis]: the reference's cell operator is indefinite,
+// and a nearly singular cell problem returns bases in the thousands, which would wreck the
+// conditioning of the coarse matrix (and the SPD-ness of its FP32 inverse)
+constexpr double kWildBasis = 3.0;
+__global__ void k_wild_cells(const int64_t* __restrict__ node_off, const double* __restrict__ bases, uint8_t* __restrict__ wild)
+{
+    const int c = blockIdx.x;
+    int bad = 0;
+    for (int64_t q = 24 * node_off[c] + threadIdx.x; q < 24 * node_off[c + 1]; q += blockDim.x) {
+        const double b = bases[q];
+        bad |= !(fabs(b) <= kWildBasis);
+    }
+    bad = __syncthreads_or(bad);
+    if (threadIdx.x == 0) wild[c] = (uint8_t)(bad != 0);
+}
+
 // psi_cell[b][v][a]: mean over the cells holding the fine node of b of their basis of the
 // coarse vertex cell_vertex[c][v]; zero on fine Dirichlet DOFs and dropped coarse DOFs
 __global__ void k_psi_cell(int64_t n_batch, const int32_t* __restrict__ bcell, const int32_t* __restrict__ cng,
                            const int32_t* __restrict__ inc_ptr, const int32_t* __restrict__ inc_b,
                            const int32_t* __restrict__ cell_vertex, const int32_t* __restrict__ cdof,
                            const uint8_t* __restrict__ fixed3, const double* __restrict__ bases,
-                           double* __restrict__ psi)
+                           const uint8_t* __restrict__ wild, const double* __restrict__ box,
+                           const double* __restrict__ cxyz, double* __restrict__ psi)
 {
     for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < n_batch; b += (int64_t)gridDim.x * blockDim.x) {
         const int c = bcell[b];
@@ -114,7 +131,18 @@ __global__ void k_psi_cell(int64_t n_batch, const int32_t* __restrict__ bcell, c
                 const int c2 = bcell[b2];
                 for (int v2 = 0; v2 < 8; v2++)
                     if (cell_vertex[8 * c2 + v2] == V) {
-                        for (int a = 0; a < 3; a++) acc[a] += bases[24 * (int64_t)b2 + 3 * v2 + a];
+                        if (wild[c2]) {
+                            // trilinear function of the cell box in place of wild bases
+                            double q = 1.0;
+                            for (int d = 0; d < 3; d++) {
+                                const double lo = box[6 * c2 + 2 * d], hi = box[6 * c2 + 2 * d + 1];
+                                const double t = (cxyz[3 * (int64_t)b2 + d] - lo) / (hi - lo);
+                                q *= ((v2 >> d) & 1) ? t : 1.0 - t;
+                            }
+                            for (int a = 0; a < 3; a++) acc[a] += q;
+                        } else {
+                            for (int a = 0; a < 3; a++) acc[a] += bases[24 * (int64_t)b2 + 3 * v2 + a];
+                        }
                         break;
                     }
             }
@@ -880,8 +908,11 @@ struct CoarseHandle {
     // Chebyshev degree and coefficients, the prolongation in its scaling, cycle vectors
     System* text = nullptr;
     int cheb_deg = 0;
-    double lmax = 0.0, lmin = 0.0;
+    double lmax = 0.0, lmin = 0.0, ratio = 30.0;
+    int widened = 0;            // times the solve widened lmax after a step that raised the residual
+    int n_trilinear = 0;        // cells whose wild bases were replaced by trilinear functions
     ChebCoef cc{};
+    DBuf<double> xkeep;         // X before the current refinement step (restored when the step fails)
     DBuf<float> psi_t, mgv;
     DBuf<__half> val16;  // FP16 copy of the textbook system's scaled SELL values (when requested)
     bool half_matrix = false;
@@ -1010,7 +1041,18 @@ int coarse_build(CoarseHandle& C, System& F, CellsHandle& Ce, const int32_t* h_c
     // prolongation values
     DBuf<double> psi;
     MSFEM_TRY(psi.alloc(24 * (size_t)nb));
-    k_psi_cell<<<gridn(nb), 256, 0, st>>>(nb, bcell.p, cng.p, inc_ptr.p, vals2.p, cvert.p, C.cdof.p, dfix.p, Ce.bx.p, psi.p);
+    DBuf<uint8_t> wild;
+    MSFEM_TRY(wild.alloc(C.n_cells));
+    k_wild_cells<<<C.n_cells, 256, 0, st>>>(Ce.node_off.p, Ce.bx.p, wild.p);
+    {
+        std::vector<uint8_t> hw(C.n_cells);
+        MSFEM_CK(cudaMemcpyAsync(hw.data(), wild.p, C.n_cells, cudaMemcpyDeviceToHost, st));
+        MSFEM_CK(cudaStreamSynchronize(st));
+        C.n_trilinear = 0;
+        for (uint8_t w : hw) C.n_trilinear += w;
+    }
+    k_psi_cell<<<gridn(nb), 256, 0, st>>>(nb, bcell.p, cng.p, inc_ptr.p, vals2.p, cvert.p, C.cdof.p, dfix.p, Ce.bx.p, wild.p,
+                                          Ce.box.p, Ce.xyz.p, psi.p);
     MSFEM_TRY(C.owner.alloc(F.n_nodes));
     MSFEM_TRY(C.psi_hat.alloc(24 * (size_t)F.n_nodes));
     k_psi_hat<<<gridn(F.n_nodes), 256, 0, st>>>(F.n_nodes, inc_ptr.p, vals2.p, bcell.p, psi.p, F.dscale.p, C.owner.p,
@@ -1319,8 +1361,34 @@ int inner_solve_mg(CoarseHandle& C, int maxiter, double tau, int* iters)
     return C.h_st->done == 3 ? MSFEM_ERR_NUMERIC : MSFEM_OK;
 }
 
+// Chebyshev step coefficients for the spectrum bound [lmax / ratio, lmax] of the Jacobi-scaled
+// textbook operator; drops the captured cycle (it holds the old coefficients)
+void cheb_coefs(CoarseHandle& C, double lmax, double ratio, int degree)
+{
+    C.lmax = lmax;
+    C.ratio = ratio;
+    C.lmin = C.lmax / ratio;
+    const double theta = 0.5 * (C.lmax + C.lmin), delta = 0.5 * (C.lmax - C.lmin), sigma = theta / delta;
+    double rho = 1.0 / sigma;
+    C.cc = ChebCoef{};
+    C.cc.inv_theta = (float)(1.0 / theta);
+    for (int i = 1; i < degree; i++) {
+        const double rn = 1.0 / (2.0 * sigma - rho);
+        C.cc.a[i] = (float)(rn * rho);
+        C.cc.b[i] = (float)(2.0 * rn / delta);
+        rho = rn;
+    }
+    C.cheb_deg = degree;
+    if (C.graph[2]) {
+        cudaGraphExecDestroy(C.graph[2]);
+        C.graph[2] = nullptr;
+    }
+}
+
 // Chebyshev smoothing on the textbook system: lambda_max of its Jacobi-scaled FP32 operator by
-// 30 power steps (times 1.05), lambda_min = lambda_max / ratio, and the step coefficients
+// 50 power steps (times 1.1), lambda_min = lambda_max / ratio.  The smoother -- and with it the
+// symmetric cycle -- is SPD only while lambda_max really bounds the spectrum; the power estimate
+// approaches it from below, so solve_twolevel widens the bound if a step ever raises the residual.
 int set_smoother(CoarseHandle& C, System& T, int degree, double ratio, int half_matrix)
 {
     System& F = *C.fine;
@@ -1354,7 +1422,7 @@ int set_smoother(CoarseHandle& C, System& T, int degree, double ratio, int half_
     k_mg_scale<<<kReduceBlocks, kVecThreads, 0, st>>>(n, v, nb.p);
     MSFEM_CK(cudaStreamSynchronize(st));
     double lam = 0.0;
-    for (int it = 0; it < 30; it++) {
+    for (int it = 0; it < 50; it++) {
         cudaStream_t ts = T.stream;
         T.stream = st;  // run the textbook system's SpMV on the solve stream
         const int rc = spmv32(T, v, w);
@@ -1368,29 +1436,14 @@ int set_smoother(CoarseHandle& C, System& T, int degree, double ratio, int half_
         lam = std::sqrt(nrm2);
         std::swap(v, w);
     }
-    C.lmax = 1.05 * lam;
-    C.lmin = C.lmax / ratio;
-    const double theta = 0.5 * (C.lmax + C.lmin), delta = 0.5 * (C.lmax - C.lmin), sigma = theta / delta;
-    double rho = 1.0 / sigma;
-    C.cc = ChebCoef{};
-    C.cc.inv_theta = (float)(1.0 / theta);
-    for (int i = 1; i < degree; i++) {
-        const double rn = 1.0 / (2.0 * sigma - rho);
-        C.cc.a[i] = (float)(rn * rho);
-        C.cc.b[i] = (float)(2.0 * rn / delta);
-        rho = rn;
-    }
-    C.cheb_deg = degree;
+    cheb_coefs(C, 1.1 * lam, ratio, degree);
+    C.widened = 0;
     C.text = &T;
     C.half_matrix = half_matrix != 0;
     if (C.half_matrix) {
         const int64_t nv = (int64_t)9 * T.sell.stored;
         MSFEM_TRY(C.val16.alloc(nv));
         k_to_half<<<gridn(nv), 256, 0, st>>>(nv, T.sell.val32.p, C.val16.p);
-    }
-    if (C.graph[2]) {
-        cudaGraphExecDestroy(C.graph[2]);
-        C.graph[2] = nullptr;
     }
     MSFEM_CK(cudaGetLastError());
     return MSFEM_OK;
@@ -1422,35 +1475,54 @@ int solve_twolevel(CoarseHandle& C, int precision, int maxiter, double tol, doub
     }
     int total = 0, k = 0, rc = MSFEM_OK;
     double r2 = 0.0, prev = -1.0;
+    const bool mg = C.text && !f32;
+    if (mg) MSFEM_TRY(C.xkeep.alloc(n));
     for (k = 0; k < 40; k++) {
         MSFEM_TRY(residual64(F, F.X.p, F.F.p, C.r64.p, rr.p));
         MSFEM_CK(cudaMemcpyAsync(&r2, rr.p, sizeof(double), cudaMemcpyDeviceToHost, st));
         MSFEM_CK(cudaStreamSynchronize(st));
-        if (!(r2 == r2)) {
-            set_error("two-level solve: the residual became NaN");
-            return MSFEM_ERR_NUMERIC;
+        const bool failed = rc == MSFEM_ERR_NUMERIC || !(r2 == r2) || (prev >= 0.0 && r2 > prev);
+        if (mg && failed && C.widened < 4) {
+            // the step broke down or raised the residual: the cycle was not SPD, so lambda_max
+            // was underestimated.  Undo the step, widen the bound and take it again.
+            MSFEM_CK(cudaMemcpyAsync(F.X.p, C.xkeep.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+            cheb_coefs(C, 1.5 * C.lmax, C.ratio, C.cheb_deg);
+            C.widened++;
+            if (std::getenv("MSFEM_TRACE"))
+                std::fprintf(stderr, "[msfem] two-level: step failed, lambda_max widened to %.4f\n", C.lmax);
+            r2 = prev;
+            rc = MSFEM_OK;
+        } else {
+            if (!(r2 == r2)) {
+                set_error("two-level solve: the residual became NaN");
+                return MSFEM_ERR_NUMERIC;
+            }
+            if (rc == MSFEM_ERR_NUMERIC) break;
+            if (r2 <= tol * tol * ff || r2 == 0.0 || total >= maxiter) break;
+            if (prev >= 0.0 && r2 > 0.25 * prev) break;  // refinement no longer contracts
         }
-        if (r2 <= tol * tol * ff || r2 == 0.0 || total >= maxiter) break;
-        if (prev >= 0.0 && r2 > 0.25 * prev) break;  // refinement no longer contracts
         prev = r2;
+        if (mg) MSFEM_CK(cudaMemcpyAsync(C.xkeep.p, F.X.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
         const double need = tol * std::sqrt(ff / r2);
         // FP32 stops near its own precision; FP64 aims a little past what is missing
         // (the multiplicative cycle's M-norm is further from the 2-norm: aim lower, one pass)
         const double tau = f32 ? std::max(1e-5, std::min(0.5, 0.3 * need))
                                : std::max(1e-14, (C.text ? 0.02 : 0.1) * need);
         int it = 0;
-        if (C.text && !f32) rc = inner_solve_mg(C, maxiter - total, tau, &it);
+        if (mg) rc = inner_solve_mg(C, maxiter - total, tau, &it);
         else rc = f32 ? inner_solve<float>(C, maxiter - total, tau, &it) : inner_solve<double>(C, maxiter - total, tau, &it);
         total += it;
         if (std::getenv("MSFEM_TRACE"))
             std::fprintf(stderr, "[msfem] two-level refine %d (%s): rel %.3e tau %.1e inner %d\n", k, f32 ? "fp32" : "fp64",
                          std::sqrt(r2 / ff), tau, it);
-        if (rc == MSFEM_ERR_NUMERIC) break;
-        if (f32)
-            k_tl_correct<float><<<kReduceBlocks, kVecThreads, 0, st>>>(n, F.X.p, reinterpret_cast<float*>(C.vec.p),
-                                                                       F.dscale.p, C.st.p);
-        else
-            k_tl_correct<double><<<kReduceBlocks, kVecThreads, 0, st>>>(n, F.X.p, C.vec.p, nullptr, C.st.p);
+        if (rc == MSFEM_ERR_NUMERIC && !mg) break;
+        if (rc != MSFEM_ERR_NUMERIC) {
+            if (f32)
+                k_tl_correct<float><<<kReduceBlocks, kVecThreads, 0, st>>>(n, F.X.p, reinterpret_cast<float*>(C.vec.p),
+                                                                           F.dscale.p, C.st.p);
+            else
+                k_tl_correct<double><<<kReduceBlocks, kVecThreads, 0, st>>>(n, F.X.p, C.vec.p, nullptr, C.st.p);
+        }
     }
     MSFEM_CK(cudaEventRecord(e1, st));
     MSFEM_CK(cudaStreamSynchronize(st));
@@ -1518,6 +1590,19 @@ int msfem_coarse_info(msfem_coarse_t c, int* n_coarse_dofs, double* ms_setup)
     }
     if (n_coarse_dofs) *n_coarse_dofs = c->n_cf;
     if (ms_setup) *ms_setup = c->ms_setup;
+    return MSFEM_OK;
+}
+
+int msfem_coarse_stats(msfem_coarse_t c, int* trilinear_cells, double* lambda_max, int* widened)
+{
+    using namespace msfem;
+    if (!c) {
+        set_error("null handle");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    if (trilinear_cells) *trilinear_cells = c->n_trilinear;
+    if (lambda_max) *lambda_max = c->lmax;
+    if (widened) *widened = c->widened;
     return MSFEM_OK;
 }
 

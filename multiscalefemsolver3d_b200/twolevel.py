@@ -55,6 +55,13 @@ class TwoLevel:
         check(load().msfem_coarse_set_smoother(self.h, textbook_system.h, degree, ratio, int(half_matrix)),
               "coarse_set_smoother")
 
+    def stats(self):
+        """{'trilinear_cells', 'lambda_max', 'widened'}: see msfem_coarse_stats."""
+        t, w = C.c_int(), C.c_int()
+        lm = C.c_double()
+        check(load().msfem_coarse_stats(self.h, C.byref(t), C.byref(lm), C.byref(w)), "coarse_stats")
+        return {"trilinear_cells": t.value, "lambda_max": lm.value, "widened": w.value}
+
     def coarse_matrix(self):
         A = np.empty((self.n_coarse_dofs, self.n_coarse_dofs))
         cdof = np.empty((self.n_cells, 8, 3), np.int32)

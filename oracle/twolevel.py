@@ -4,7 +4,10 @@ prolongation, coarse Galerkin matrix and preconditioner application.
 
   P[(g, a), (V, a)] = mean over the cells c holding fine node g of psi_{c,V}^a(g)  (the Order1
                       basis of vertex V in cell c, its a-component), 0 on fine Dirichlet DOFs;
-                      coarse DOFs (V, a) whose vertex node has a Dirichlet a-component dropped
+                      coarse DOFs (V, a) whose vertex node has a Dirichlet a-component dropped;
+                      a cell with any basis value outside [-3, 3] (the reference's indefinite
+                      cell operator near singularity) contributes the trilinear functions of its
+                      box instead
   A_c = P^T K P,     K = the textbook orientation of the fine element blocks (SPD on the free DOFs)
   M^-1 r = r + S^-1 P A_c^-1 P^T S^-1 r   on the Jacobi-scaled system (S = diag(A)^-1/2)
 """
@@ -16,11 +19,34 @@ import scipy.sparse as sp
 from . import cells as oc
 
 
+WILD_BASIS = 3.0
+
+
+def sanitized_bases(cc, bases):
+    """Bases with every wild cell (|psi| > WILD_BASIS somewhere) replaced by the trilinear
+    functions of its box, as the GPU's coarse build does."""
+    cm = cc.cells
+    out = np.array(bases, dtype=np.float64, copy=True)
+    for c in range(cm.n_cells):
+        a0, a1 = cm.node_off[c], cm.node_off[c + 1]
+        if np.all(np.abs(out[a0:a1]) <= WILD_BASIS):
+            continue
+        box = cm.box[c]
+        t = (cm.xyz[a0:a1] - box[[0, 2, 4]]) / (box[[1, 3, 5]] - box[[0, 2, 4]])
+        for v in range(8):
+            q = np.ones(a1 - a0)
+            for d in range(3):
+                q *= t[:, d] if (v >> d) & 1 else 1.0 - t[:, d]
+            out[a0:a1, v, :] = q[:, None]
+    return out
+
+
 def prolongation(cc, bases, n_fine, fixed_dofs):
     """cc: meshgen.CubeCells; bases: [cells' nodes, 8, 3] (cell-local) -> (P [3 n_fine, n_cf] CSR,
     coarse_dof [n_cells, 8, 3] (-1 dropped))."""
     fixed = np.zeros(3 * n_fine, bool)
     fixed[np.asarray(fixed_dofs)] = True
+    bases = sanitized_bases(cc, bases)
     cm = cc.cells
     n_cv = cc.n_coarse_vertices
     # coarse DOFs

@@ -130,3 +130,37 @@ def test_multiplicative_cycle_solve(mg_case):
     rel1, it_j, rc1 = S.solve(fem.MINRES, FP64, tol=1e-12, maxiter=200000)
     assert rc1 == 0
     assert it_mg < it_j / 2, (it_mg, it_j)
+
+
+def test_wild_cell_bases_do_not_break_the_cycle(lib, cuda):
+    """A 64^3 case (250 spheres E 1:100, seed 3) where one cell's exact Order1 bases reach |psi|
+    ~ 6.6e3: the reference's cell operator is indefinite and that cell problem is nearly singular.
+    Used as they are, they make the coarse matrix's condition ~4e10 and the FP32-inverted cycle
+    indefinite (MINRES diverged).  The coarse build replaces such cells by trilinear functions, so
+    the solve converges; the oracle's prolongation applies the same rule."""
+    p = meshgen.cube_elastic(n=64, jitter=0.0, n_spheres=250, contrast=100.0, rmin=0.015, rmax=0.035, sphere_seed=3)
+    m = p.mesh
+    dofs = (3 * p.bc_nodes[:, None] + np.arange(3)).ravel().astype(np.int32)
+    z = np.zeros(dofs.size)
+    S = fem.System(fem.ELASTIC, m.xyz, m.tets, m.mat)
+    S.add_traction(p.faces, p.traction)
+    S.assemble_elastic(p.E, p.nu)
+    S.apply_dirichlet(dofs, z, fem.ROW_AND_COLUMN)
+    K = fem.System(fem.ELASTIC, m.xyz, m.tets, m.mat)
+    K.assemble_elastic_textbook(p.E, p.nu)
+    K.apply_dirichlet(dofs, z, fem.ROW_AND_COLUMN)
+    cc = meshgen.cube_cells(m, p.E, p.nu, 8)
+    cells = Cells(cc.cells)
+    assert cells.build_bases(FP32_IR, 1e-8) == 0
+    assert np.abs(cells.bases()).max() > 1e3
+    T = TwoLevel(S, cells, cc, dofs)
+    st = T.stats()
+    assert st["trilinear_cells"] >= 1
+    A, _ = T.coarse_matrix()
+    w = np.linalg.eigvalsh(A)
+    assert w[0] > 0 and w[-1] / w[0] < 1e6
+    T.set_smoother(K, degree=3, half_matrix=True)
+    S.set_x(np.zeros(S.n_rows))
+    rel, it, _, rc = T.solve(tol=1e-8, maxiter=100000, precision=FP64)
+    assert rc == 0 and rel <= 1e-8
+    T.close()
