@@ -423,7 +423,16 @@ __global__ void __launch_bounds__(128) k_tl_restrict(const int32_t* __restrict__
             }
             rv[a] = s ? (VT)(s[3 * g + a] * (double)r) : r;
         }
-        const float* ph = psi_hat + 24 * g;
+        float ph[24];  // 96 bytes per node, 16-byte aligned: six float4 loads
+        const float4* p4 = reinterpret_cast<const float4*>(psi_hat + 24 * g);
+#pragma unroll
+        for (int q = 0; q < 6; q++) {
+            const float4 t = __ldg(p4 + q);
+            ph[4 * q] = t.x;
+            ph[4 * q + 1] = t.y;
+            ph[4 * q + 2] = t.z;
+            ph[4 * q + 3] = t.w;
+        }
 #pragma unroll
         for (int j = 0; j < 24; j++) acc[j] += (VT)ph[j] * rv[j % 3];
     }
@@ -681,9 +690,11 @@ __global__ void __launch_bounds__(kVecThreads) k_tl_correct(int n, double* __res
 // Jacobi-scaled space K^ = S_t K_t S_t): pre-smoothing by k Chebyshev steps, coarse correction
 // with P^_t = S_t^-1 P, post-smoothing by the same k steps.  M^-1 r = S_t cycle(S_t r).
 
-// 3x3-block SELL row times x with the values stored in FP32 or, when v16 is set, in FP16
-// (same layout); FP32 arithmetic either way
-__device__ __forceinline__ void sell_row_block_mixed(const SellView<float>& A, const __half* __restrict__ v16, int warp,
+// 3x3-block SELL row times x with the values stored in FP32 or, when v16 is set, in FP16.  The
+// FP16 values of block column k of a slice sit as 5 half2 words per lane, word p at
+// 5 * blk + 32 p + lane (blk = the slice's first block of the column; word 4 = (v8, 0)): each of
+// the 5 loads is one 128-byte line per warp.
+__device__ __forceinline__ void sell_row_block_mixed(const SellView<float>& A, const __half2* __restrict__ v16, int warp,
                                                      int lane, const float* __restrict__ x, float (&acc)[3])
 {
     if (!v16) {
@@ -697,21 +708,33 @@ __device__ __forceinline__ void sell_row_block_mixed(const SellView<float>& A, c
     for (int k = 0; k < w; k++) {
         const int64_t blk = base + (int64_t)k * kSlice;
         const int c = __ldcs(A.col + blk + lane);
-        const __half* vb = v16 + 9 * blk + lane;
+        const unsigned int* vb = reinterpret_cast<const unsigned int*>(v16) + 5 * blk + lane;
         const float x0 = __ldg(x + 3 * (int64_t)c), x1 = __ldg(x + 3 * (int64_t)c + 1), x2 = __ldg(x + 3 * (int64_t)c + 2);
-        float v[9];
+        float v[10];
 #pragma unroll
-        for (int e = 0; e < 9; e++) v[e] = __half2float(__ldcs(vb + e * kSlice));
+        for (int p = 0; p < 5; p++) {
+            const unsigned int u = __ldcs(vb + p * kSlice);
+            const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&u));
+            v[2 * p] = f.x;
+            v[2 * p + 1] = f.y;
+        }
         acc[0] += v[0] * x0 + v[1] * x1 + v[2] * x2;
         acc[1] += v[3] * x0 + v[4] * x1 + v[5] * x2;
         acc[2] += v[6] * x0 + v[7] * x1 + v[8] * x2;
     }
 }
 
-__global__ void k_to_half(int64_t n, const float* __restrict__ a, __half* __restrict__ h)
+// FP32 SELL values (9 per block: 9 blk + 32 e + lane) -> the paired FP16 layout above
+__global__ void k_to_half(int64_t stored, const float* __restrict__ a, __half2* __restrict__ h)
 {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        h[i] = __float2half_rn(a[i]);
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < stored; q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t blk = q & ~(int64_t)31;
+        const int l = (int)(q & 31);
+        float v[10];
+        for (int e = 0; e < 9; e++) v[e] = a[9 * blk + 32 * e + l];
+        v[9] = 0.0f;
+        for (int p = 0; p < 5; p++) h[5 * blk + 32 * p + l] = __floats2half2_rn(v[2 * p], v[2 * p + 1]);
+    }
 }
 
 struct ChebCoef {
@@ -745,7 +768,7 @@ __global__ void __launch_bounds__(kVecThreads) k_mg_in(int n, const double* __re
 }
 
 // one Chebyshev step: res -= K^ d_prev; d = a d_prev + b res; x += d
-__global__ void __launch_bounds__(256) k_mg_cheb(SellView<float> A, const __half* __restrict__ v16,
+__global__ void __launch_bounds__(256) k_mg_cheb(SellView<float> A, const __half2* __restrict__ v16,
                                                  const float* __restrict__ dprev,
                                                  float* __restrict__ d, float* __restrict__ res, float* __restrict__ x,
                                                  float a, float b, const TlState* S)
@@ -771,7 +794,7 @@ __global__ void __launch_bounds__(256) k_mg_cheb(SellView<float> A, const __half
 
 // res = rhat - K^ x; with `start`: also the first post-smoothing step d = res / theta,
 // x2 = x + d (into a second buffer: x is being gathered)
-__global__ void __launch_bounds__(256) k_mg_resid(SellView<float> A, const __half* __restrict__ v16,
+__global__ void __launch_bounds__(256) k_mg_resid(SellView<float> A, const __half2* __restrict__ v16,
                                                   const float* __restrict__ rhat,
                                                   const float* __restrict__ x, float* __restrict__ res,
                                                   float* __restrict__ d, float* __restrict__ x2, float inv_theta,
@@ -806,13 +829,19 @@ __global__ void __launch_bounds__(kVecThreads) k_mg_prolong(int n_fine, const in
 {
     if (S->done) return;
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n_fine; g += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t* cd = cdof + 24 * owner[g];
-        const float* ph = psi + 24 * g;
+        // 24 coarse DOFs of the owner cell and the node's 24 prolongation weights: six 16-byte loads each
+        const int4* c4 = reinterpret_cast<const int4*>(cdof + 24 * (int64_t)owner[g]);
+        const float4* p4 = reinterpret_cast<const float4*>(psi + 24 * g);
         float z[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
-        for (int j = 0; j < 24; j++) {
-            const int dd = cd[j];
-            if (dd >= 0) z[j % 3] += ph[j] * ec[dd];
+        for (int q = 0; q < 6; q++) {
+            const int4 cq = __ldg(c4 + q);
+            const float4 pq = __ldg(p4 + q);
+            const int dd[4] = {cq.x, cq.y, cq.z, cq.w};
+            const float pp[4] = {pq.x, pq.y, pq.z, pq.w};
+#pragma unroll
+            for (int t = 0; t < 4; t++)
+                if (dd[t] >= 0) z[(4 * q + t) % 3] += pp[t] * ec[dd[t]];
         }
 #pragma unroll
         for (int a = 0; a < 3; a++) x[3 * g + a] += z[a];
@@ -914,7 +943,7 @@ struct CoarseHandle {
     ChebCoef cc{};
     DBuf<double> xkeep;         // X before the current refinement step (restored when the step fails)
     DBuf<float> psi_t, mgv;
-    DBuf<__half> val16;  // FP16 copy of the textbook system's scaled SELL values (when requested)
+    DBuf<__half2> val16;  // FP16 copy of the textbook system's scaled SELL values, paired (when requested)
     bool half_matrix = false;
     ~CoarseHandle()
     {
@@ -1273,7 +1302,7 @@ void mg_cycle(CoarseHandle& C, const double* z, const double* r2, double* r_out,
     const unsigned gsp = spmv_grid_of((const void*)k_mg_cheb, T);
     const unsigned gvec = kReduceBlocks;
     const double* s_t = T.dscale.p;
-    const __half* v16 = C.half_matrix ? C.val16.p : nullptr;
+    const __half2* v16 = C.half_matrix ? C.val16.p : nullptr;
     k_mg_in<<<gvec, kVecThreads, 0, st>>>(n, z, r2, r_out, s_t, rhat, res, dA, x, C.cc, S, lanczos);
     float* d[2] = {dA, dB};
     for (int i = 1; i < C.cheb_deg; i++)
@@ -1441,9 +1470,8 @@ int set_smoother(CoarseHandle& C, System& T, int degree, double ratio, int half_
     C.text = &T;
     C.half_matrix = half_matrix != 0;
     if (C.half_matrix) {
-        const int64_t nv = (int64_t)9 * T.sell.stored;
-        MSFEM_TRY(C.val16.alloc(nv));
-        k_to_half<<<gridn(nv), 256, 0, st>>>(nv, T.sell.val32.p, C.val16.p);
+        MSFEM_TRY(C.val16.alloc(5 * (size_t)T.sell.stored));
+        k_to_half<<<gridn(T.sell.stored), 256, 0, st>>>(T.sell.stored, T.sell.val32.p, C.val16.p);
     }
     MSFEM_CK(cudaGetLastError());
     return MSFEM_OK;
