@@ -82,9 +82,13 @@ class RefLib:
         L.ref_poly_quadrature.argtypes = [_f64p, _i32p, _f64p, _f64p]
         L.ref_mech_D.argtypes = [C.c_double, C.c_double, _f64p]
         L.ref_polygon_quadrature.argtypes = [_f64p, _f64p, _f64p]
+        _i = C.c_int
+        _ip = C.POINTER(C.c_int)
+        L.ref_read_nvtr.argtypes = [C.c_char_p, _i, _i, _i, _i, _ip, _ip, _ip, _f64p, _i32p, _i32p, _i32p, _ip]
+        L.ref_read_salome.argtypes = [C.c_char_p, _i, _i, _i, _i, _ip, _ip, _f64p, _i32p, _i32p]
         for f in ("ref_elastic_local", "ref_scalar_local", "ref_elastic_system", "ref_elastic_driver",
                   "ref_scalar_system", "ref_scalar_driver", "ref_cssd_solve", "ref_ssor_apply", "ref_cell_problem",
-                  "ref_poly_quadrature", "ref_mech_D", "ref_polygon_quadrature"):
+                  "ref_poly_quadrature", "ref_mech_D", "ref_polygon_quadrature", "ref_read_nvtr", "ref_read_salome"):
             getattr(L, f).restype = C.c_int
         L.ref_set_quiet(1)
 
@@ -199,6 +203,30 @@ class RefLib:
         pts, w = np.zeros(48), np.zeros(16)
         assert self.L.ref_polygon_quadrature(_c(xyz4, np.float64).ravel(), pts, w) == 0
         return pts.reshape(16, 3), w
+
+    def read_nvtr(self, directory, k, cap_v, cap_e, cap_idx):
+        """The reference's ReadFromNVTR: (xyz [nv, 3], elements (list of index arrays), nvkat,
+        read_from_zero)."""
+        nv, ne, ni, rz = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        xyz, idx = np.zeros(3 * cap_v), np.zeros(cap_idx, np.int32)
+        ln, kat = np.zeros(cap_e, np.int32), np.zeros(cap_e, np.int32)
+        rc = self.L.ref_read_nvtr(str(directory).encode(), k, cap_v, cap_e, cap_idx, C.byref(nv), C.byref(ne), C.byref(ni),
+                                  xyz, idx, ln, kat, C.byref(rz))
+        assert rc == 0, rc
+        assert nv.value <= cap_v and ne.value <= cap_e and ni.value <= cap_idx
+        off = np.concatenate([[0], np.cumsum(ln[:ne.value])])
+        elems = [idx[off[e]:off[e + 1]].copy() for e in range(ne.value)]
+        return xyz[:3 * nv.value].reshape(-1, 3), elems, kat[:ne.value].copy(), bool(rz.value)
+
+    def read_salome(self, path, dim, map_size, cap_v, cap_e):
+        """The reference's ReadFromSalomeDat: (xyz, elements [ne, dim + 1], vertex_map or None)."""
+        nv, ne = C.c_int(), C.c_int()
+        xyz, el = np.zeros(3 * cap_v), np.zeros((dim + 1) * cap_e, np.int32)
+        vm = np.zeros(cap_v, np.int32)
+        rc = self.L.ref_read_salome(str(path).encode(), dim, map_size, cap_v, cap_e, C.byref(nv), C.byref(ne), xyz, el, vm)
+        assert rc == 0, rc
+        return (xyz[:3 * nv.value].reshape(-1, 3), el[:(dim + 1) * ne.value].reshape(-1, dim + 1),
+                vm[:nv.value].copy() if map_size >= 0 else None)
 
     def mech_D(self, E, nu):
         D = np.zeros(36)

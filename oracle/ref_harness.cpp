@@ -19,6 +19,7 @@
  */
 #include "FEM/FEM.h"
 
+#include <cstring>
 #include <fcntl.h>
 #include <sys/stat.h>
 
@@ -722,6 +723,62 @@ int ref_polygon_quadrature(const double* xyz4, double* points, double* weights)
         weights[q] = poly->GetIntegrationWeight(q);
     }
     return 0; /* objects leaked on purpose, as above */
+}
+
+/* math::SimpleGrid::ReadFromNVTR (Library/Math.h:150-291) on a directory: the reference's own
+   reader.  k = nodes per element (4) or -1 (polyhedra, flattened as the file holds them).
+   Outputs are truncated to the given capacities; counts and read_from_zero are always set. */
+int ref_read_nvtr(const char* dir, int k, int cap_v, int cap_e, int cap_idx, int* n_vert, int* n_elem, int* n_idx,
+                  double* xyz, int* idx, int* elem_len, int* nvkat, int* read_from_zero)
+{
+    StdoutSilencer s;
+    math::SimpleGrid g;
+    std::vector<char> d(dir, dir + std::strlen(dir) + 1);
+    if (!g.ReadFromNVTR(d.data(), k)) return -2;
+    *n_vert = (int)g.xyz.size();
+    *n_elem = (int)g.nvtr.size();
+    *read_from_zero = g.read_from_zero ? 1 : 0;
+    for (int i = 0; i < *n_vert && i < cap_v; i++) {
+        xyz[3 * i] = g.xyz[i].x;
+        xyz[3 * i + 1] = g.xyz[i].y;
+        xyz[3 * i + 2] = g.xyz[i].z;
+    }
+    int t = 0;
+    for (int e = 0; e < *n_elem; e++) {
+        if (e < cap_e) {
+            elem_len[e] = (int)g.nvtr[e].size();
+            nvkat[e] = g.nvkat[e];
+        }
+        for (int v : g.nvtr[e]) {
+            if (t < cap_idx) idx[t] = v;
+            t++;
+        }
+    }
+    *n_idx = t;
+    return 0;
+}
+
+/* math::SimpleGrid::ReadFromSalomeDat (Library/Math.h:35-149), the map_size variant when
+   map_size >= 0: vertex_map[i] = id - 1. */
+int ref_read_salome(const char* file, int dim, int map_size, int cap_v, int cap_e, int* n_vert, int* n_elem, double* xyz,
+                    int* elems, int* vmap)
+{
+    StdoutSilencer s;
+    math::SimpleGrid g;
+    std::vector<char> f(file, file + std::strlen(file) + 1);
+    const bool ok = map_size >= 0 ? g.ReadFromSalomeDat(f.data(), dim, map_size) : g.ReadFromSalomeDat(f.data(), dim);
+    if (!ok) return -2;
+    *n_vert = (int)g.xyz.size();
+    *n_elem = (int)g.nvtr.size();
+    for (int i = 0; i < *n_vert && i < cap_v; i++) {
+        xyz[3 * i] = g.xyz[i].x;
+        xyz[3 * i + 1] = g.xyz[i].y;
+        xyz[3 * i + 2] = g.xyz[i].z;
+        if (map_size >= 0) vmap[i] = g.vertex_map[i];
+    }
+    for (int e = 0; e < *n_elem && e < cap_e; e++)
+        for (int j = 0; j <= dim; j++) elems[(dim + 1) * e + j] = g.nvtr[e][j];
+    return 0;
 }
 
 /* Domain::forMech::GetD(3) (Library/Domain.h:170-175, isotropic D of :53-78) as 36 doubles. */
