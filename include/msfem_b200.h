@@ -223,6 +223,15 @@ int msfem_fem_elastic_driver(int n_nodes, const double* xyz, int n_tets, const i
  * launch per problem kind.
  * ------------------------------------------------------------------------------------- */
 
+/* Post-processing of an elasticity system's current solution X, per tetrahedron at its centroid
+ * (FEM/FEM_Grid.h:3289-3365 and the fields FEM/FEM_Main.cpp:1018-1040 prints).  out:
+ * [n_tets][23] doubles = U (3), grad U (9, row a = grad u_a), sigma (xx yy zz yz xz xy) of the
+ * element's own material (Domain::forMech::solve_SIGMA), von Mises as GetVonMisesStress computes
+ * it, then the driver's printed sigma_xx, sigma_yy, sigma_zz and von Mises (domain 0's E and nu
+ * for every element, as the reference driver does).  Host or device output. */
+int msfem_postprocess_elastic(msfem_system_t h, int n_materials, const double* E, const double* nu, double* out,
+                              int on_device);
+
 typedef struct msfem_batch* msfem_batch_t;
 
 /* n_systems independent FEM_2D (dim 2: triangles) or FEM_3D (dim 3: tetrahedra)

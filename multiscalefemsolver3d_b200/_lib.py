@@ -89,6 +89,7 @@ _SIGS = [
     ("msfem_cells_macro_matrices", C.c_int, [C.c_void_p, _P, C.c_int]),
     ("msfem_cells_face_loads", C.c_int, [C.c_void_p, C.c_int, _P, _P, _P]),
     ("msfem_cells_reconstruct", C.c_int, [C.c_void_p, C.c_int, _P, _P, _P]),
+    ("msfem_postprocess_elastic", C.c_int, [C.c_void_p, C.c_int, _P, _P, _P, C.c_int]),
     ("msfem_cells_set_bases", C.c_int, [C.c_void_p, _P, C.c_int]),
     ("msfem_cells_basis_residual", C.c_int, [C.c_void_p, _P]),
     ("msfem_cells_copy_bases", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, _P]),

@@ -84,6 +84,7 @@ class System:
         check(L.msfem_system_create(kind, n_nodes, px, n_tets, pt, pm, int(dx or dt), C.byref(h)), "system_create")
         self.h = h
         self.n_nodes = n_nodes
+        self.n_tets = n_tets
         n_rows, nnz, nc = C.c_int(), C.c_int64(), C.c_int()
         check(L.msfem_system_info(h, C.byref(n_rows), C.byref(nnz), C.byref(nc)), "system_info")
         self.n_rows, self.nnz, self.n_colors = n_rows.value, nnz.value, nc.value
@@ -151,6 +152,18 @@ class System:
         out = np.empty(self.n_rows) if out is None else out
         p, d, k = _ptr(out, np.float64)
         check(load().msfem_get_x(self.h, p, d), "get_x")
+        return out
+
+    def postprocess_elastic(self, E, nu):
+        """[n_tets, 23] per tetrahedron at its centroid from the current X: U, grad U (row a =
+        grad u_a), sigma (xx yy zz yz xz xy, the element's material), von Mises, and the
+        reference driver's printed sigma_xx, sigma_yy, sigma_zz, von Mises (domain 0's material)."""
+        E = np.ascontiguousarray(E, dtype=np.float64)
+        nu = np.ascontiguousarray(nu, dtype=np.float64)
+        out = np.empty((self.n_tets, 23))
+        check(load().msfem_postprocess_elastic(self.h, E.size, E.ctypes.data_as(C.c_void_p),
+                                               nu.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p), 0),
+              "postprocess_elastic")
         return out
 
     def get_f(self):

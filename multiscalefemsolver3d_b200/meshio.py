@@ -34,7 +34,7 @@ import numpy as np
 from .meshgen import CellMeshes
 
 __all__ = ["write_nvtr", "read_nvtr", "write_kraev", "read_kraev", "write_salome_dat", "read_salome_dat",
-           "write_cell_dirs", "write_macro_nvtr"]
+           "write_cell_dirs", "write_macro_nvtr", "write_tecplot", "elastic_result_fields"]
 
 
 def _ints_text(rows) -> str:
@@ -234,3 +234,42 @@ def write_macro_nvtr(directory, vertex_xyz, cell_vertex, mat=None):
             r += [4] + [int(cv[v]) for v in cyc]
         recs.append(np.array(r, dtype=np.int64))
     write_nvtr(directory, vertex_xyz, recs, mat, one_based=False)
+
+
+def write_tecplot(path, xyz, tets, mat, values, names, zone="Elastic"):
+    """The FEBLOCK tetrahedron file of FEM_Grid::printTecPlot3D (FEM/FEM_Grid.h:3367-3452): nodal
+    x, y, z (%.10e), one CELLCENTERED block per value array (%.10lf), then the 1-based
+    connectivity.  Elements of domain 10 (the reference's DEL_domain) leave the element count and
+    the connectivity (their line stays, empty); the value blocks follow the reference's loop,
+    which tests the domain of element `i` -- the value index -- for every element."""
+    xyz = np.asarray(xyz, dtype=np.float64)
+    tets = np.asarray(tets, dtype=np.int64)
+    mat = np.asarray(mat)
+    del_domain = 10
+    lines = ['TITLE     = "numerical"\n', 'VARIABLES = "x"\n "y"\n "z"\n']
+    lines += [f' "{n}"\n' for n in names]
+    n_keep = int((mat != del_domain).sum())
+    lines.append(f'ZONE T="{zone}"\n')
+    lines.append(f" N={xyz.shape[0]},  E={n_keep}, F=FEBLOCK ET=Tetrahedron \n")
+    lines.append(" VARLOCATION=(NODAL NODAL NODAL" + " CELLCENTERED" * len(values) + ")\n")
+    for d in range(3):
+        lines += [f"{v:.10e}\n" for v in xyz[:, d]]
+        lines.append("\n")
+    for i, val in enumerate(values):
+        if mat[i] != del_domain:
+            lines += [f"{v:.10f}\n" for v in np.asarray(val, dtype=np.float64)]
+        lines.append("\n")
+    for e in range(tets.shape[0]):
+        if mat[e] != del_domain:
+            lines.append("".join(f"{int(v) + 1} " for v in tets[e]))
+        lines.append("\n")
+    with open(path, "w") as f:
+        f.write("".join(lines))
+
+
+def elastic_result_fields(post):
+    """The six cell fields the elasticity driver prints (FEM/FEM_Main.cpp:1042-1052) from
+    System.postprocess_elastic's array: sigma_xx, sigma_yy, sigma_zz, VonMises_stress (the
+    driver's own formulas), Uy, Uz."""
+    names = ["sigma_xx", "sigma_yy", "sigma_zz", "VonMises_stress", "Uy", "Uz"]
+    return [post[:, 19], post[:, 20], post[:, 21], post[:, 22], post[:, 1], post[:, 2]], names

@@ -86,9 +86,10 @@ class RefLib:
         _ip = C.POINTER(C.c_int)
         L.ref_read_nvtr.argtypes = [C.c_char_p, _i, _i, _i, _i, _ip, _ip, _ip, _f64p, _i32p, _i32p, _i32p, _ip]
         L.ref_read_salome.argtypes = [C.c_char_p, _i, _i, _i, _i, _ip, _ip, _f64p, _i32p, _i32p]
+        L.ref_postprocess.argtypes = [_i, _f64p, _i, _i32p, _i32p, _i, _f64p, _f64p, _f64p, _f64p]
         for f in ("ref_elastic_local", "ref_scalar_local", "ref_elastic_system", "ref_elastic_driver",
                   "ref_scalar_system", "ref_scalar_driver", "ref_cssd_solve", "ref_ssor_apply", "ref_cell_problem",
-                  "ref_poly_quadrature", "ref_mech_D", "ref_polygon_quadrature", "ref_read_nvtr", "ref_read_salome"):
+                  "ref_poly_quadrature", "ref_mech_D", "ref_polygon_quadrature", "ref_read_nvtr", "ref_read_salome", "ref_postprocess"):
             getattr(L, f).restype = C.c_int
         L.ref_set_quiet(1)
 
@@ -227,6 +228,17 @@ class RefLib:
         assert rc == 0, rc
         return (xyz[:3 * nv.value].reshape(-1, 3), el[:(dim + 1) * ne.value].reshape(-1, dim + 1),
                 vm[:nv.value].copy() if map_size >= 0 else None)
+
+    def postprocess(self, mesh, E, nu, solution):
+        """[n_tets, 19] per element at its centroid: U, dU (row a = grad u_a), sigma (xx yy zz yz xz
+        xy) with the element's material, von Mises (FEM/FEM_Grid.h:3289-3365)."""
+        out = np.zeros(19 * mesh.n_tets)
+        E = _c(E, np.float64)
+        rc = self.L.ref_postprocess(mesh.n_nodes, _c(mesh.xyz, np.float64).ravel(), mesh.n_tets,
+                                    _c(mesh.tets, np.int32).ravel(), _c(mesh.mat, np.int32), E.size, E,
+                                    _c(nu, np.float64), _c(solution, np.float64).ravel(), out)
+        assert rc == 0, rc
+        return out.reshape(-1, 19)
 
     def mech_D(self, E, nu):
         D = np.zeros(36)

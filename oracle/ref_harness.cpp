@@ -781,6 +781,46 @@ int ref_read_salome(const char* file, int dim, int map_size, int cap_v, int cap_
     return 0;
 }
 
+/* The reference grid's post-processing at each element's centroid (FEM/FEM_Grid.h:3289-3365):
+   GetSolutionInPoint, GetDerevativeFromSolutionInPoint, GetStressTensorFromSolutionInPoint (the
+   element's own material through Domain::forMech::solve_SIGMA) and GetVonMisesStress.
+   solution: [n_nodes][3]; out: [n_tets][19] = U(3), dU(9: row a = grad u_a), sigma (xx yy zz yz
+   xz xy), von Mises. */
+int ref_postprocess(int n_nodes, const double* xyz, int n_tets, const int* tets, const int* mat, int n_mat,
+                    const double* E, const double* nu, const double* solution, double* out)
+{
+    StdoutSilencer s;
+    math::SimpleGrid g;
+    make_simple_grid(g, n_nodes, xyz, n_tets, tets, mat);
+    std::vector<DirichletMech> dir;
+    std::vector<NeumannMech> neu;
+    auto* gridp = new FEM::Grid_forMech();
+    FEM::Grid_forMech& grid = *gridp;
+    set_materials_mech(grid, n_mat, E, nu);
+    grid.Initialization(g, dir, neu);
+    std::vector<Point<double>> sol(n_nodes);
+    for (int i = 0; i < n_nodes; i++) sol[i] = Point<double>(solution[3 * i], solution[3 * i + 1], solution[3 * i + 2]);
+    for (int e = 0; e < grid.GetElementsCount(); e++) {
+        auto element = grid.GetElement(e);
+        Point<double> X = element->GetWeightCentr();
+        Point<double> U = grid.GetSolutionInPoint(e, X, sol);
+        Point<Point<double>> dU = grid.GetDerevativeFromSolutionInPoint(e, X, sol);
+        Tensor2Rank3D S = grid.GetStressTensorFromSolutionInPoint(e, X, dU);
+        double* o = out + 19 * (size_t)e;
+        o[0] = U.x; o[1] = U.y; o[2] = U.z;
+        const Point<double> rows[3] = {dU.x, dU.y, dU.z};
+        for (int a = 0; a < 3; a++) {
+            o[3 + 3 * a] = rows[a].x;
+            o[4 + 3 * a] = rows[a].y;
+            o[5 + 3 * a] = rows[a].z;
+        }
+        o[12] = S.val[0][0]; o[13] = S.val[1][1]; o[14] = S.val[2][2];
+        o[15] = S.val[1][2]; o[16] = S.val[0][2]; o[17] = S.val[0][1];
+        o[18] = grid.GetVonMisesStress(S);
+    }
+    return 0; /* grid leaked on purpose, as the other entry points do */
+}
+
 /* Domain::forMech::GetD(3) (Library/Domain.h:170-175, isotropic D of :53-78) as 36 doubles. */
 int ref_mech_D(double E, double nu, double* D)
 {

@@ -193,3 +193,17 @@ def test_msfem_driver_restatement_properties(spheres):
         ref_u = np.zeros((p.mesh.n_nodes, 3))
         ref_u[g] = u
         assert np.abs(ref_u[g] - u).max() <= 1e-9 * np.abs(u).max()
+
+
+def test_postprocessing_restatement_matches_reference(ref):
+    """Per-element U, grad U, stress (each element's material) and von Mises at the centroid
+    against the reference grid's own functions (FEM/FEM_Grid.h:3289-3365) on a jittered
+    two-material mesh with a random displacement field."""
+    from oracle import post
+    m = meshgen.kuhn_cube(3, jitter=0.15, seed=2)
+    m.mat[:] = np.random.default_rng(1).integers(0, 2, m.n_tets)
+    E, nu = np.array([1.0, 40.0]), np.array([0.3, 0.22])
+    u = np.random.default_rng(5).normal(size=(m.n_nodes, 3))
+    got = post.element_fields(m.xyz, m.tets, m.mat, E, nu, u)
+    want = ref.postprocess(m, E, nu, u)
+    np.testing.assert_allclose(got[:, :19], want, rtol=1e-12, atol=1e-12 * np.abs(want).max())
