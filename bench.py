@@ -69,7 +69,7 @@ def parse():
                     help="elastic: coarse-space bases predicted by the trained network (with the exact cell solve "
                          "as per-cell fallback) or solved exactly for every cell")
     ap.add_argument("--train-cells", type=int, default=20480, help="elastic, learned: training cells")
-    ap.add_argument("--train-epochs", type=int, default=12, help="elastic, learned: training epochs")
+    ap.add_argument("--train-epochs", type=int, default=24, help="elastic, learned: training epochs")
     a = ap.parse_args()
     if a.n is None:
         a.n = 100 if a.config == "electrostatics" else 128
