@@ -434,9 +434,10 @@ int msfem_net_loss_grad(msfem_net_t n, int cells, const float* vox, const float*
 int msfem_net_forward(msfem_net_t n, int cells, const float* vox, float* out);
 /* Predicts the bases of every cell of c into c (as msfem_cells_set_bases would); ms: device time. */
 int msfem_net_predict(msfem_net_t n, msfem_cells_t c, float* ms);
-/* Tensor-core path of layers 1-3 (forward and data gradient): 1 = tcgen05 MMA with TMEM
- * accumulators, 0 = warp-level mma.sync.  Both compute the same function (FP32 accumulation
- * order differs). */
+/* Tensor-core path of layers 1-3 (forward and data gradient): 0 = warp-level mma.sync, 1 =
+ * tcgen05 with TMEM accumulators and M = 64 voxel tiles (N = 32 channels), 2 = tcgen05 on the
+ * transposed product (M = 64 channel rows, N = 256 voxels of a plane).  All compute the same
+ * function (FP32 accumulation order may differ). */
 int msfem_net_set_tensor_path(msfem_net_t n, int tcgen05);
 int msfem_net_destroy(msfem_net_t n);
 

@@ -498,6 +498,170 @@ __global__ void __launch_bounds__(128, 1) k_conv32_tc(const __nv_bfloat16* __res
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;\n" ::"r"(tbase));
 }
 
+// ---- the transposed product on tcgen05: D^T[co][voxel] = sum_tap W_tap^T[co][ci] A_tap^T[ci][voxel].
+// One instruction now covers a whole plane: M = 64 (the 32 output channels; rows 32-63 read the
+// next tap's weights and are never used), N = 256 voxels, K = 16 -- 54 per plane instead of 216.
+// The N operand must be 256 rows of 16 bytes at one stride for every tap, so the halo is kept as
+// three x-shifted copies: a plane slot is [dx][chunk][18 y][16 x] x 16 B, three slots in a ring.
+// The weights stay [chunk][tap][co] x 16 B (plus 1 KB of zero slack read by the unused rows of
+// the last tap).  TMEM holds D^T as 64 lanes (row m in lane m % 16 + 32 (m / 16)) x 256 columns:
+// the channels of warps 0 and 1, lanes 0-15.  The epilogue reads them with tcgen05.ld, stages the
+// plane as [voxel][channel] in the ring slot that just went out of use, and copies it out with
+// 16-byte stores.
+constexpr int kTtPlane = 3 * 4 * 18 * 16 * 16;            // 55,296 B: one plane slot
+constexpr int kTtDx = 4 * 18 * 16 * 16;                   // 18,432 B between x-shifted copies
+constexpr int kTtChunk = 18 * 16 * 16;                    // 4,608 B between channel chunks
+constexpr int kTtA = 3 * kTtPlane;                        // 165,888 B: the ring
+constexpr int kTtW = kTaps * kCh * 4 * 16 + 1024;         // 56,320 B: weights + slack
+constexpr int kTtSmem = kTtA + kTtW + 16;
+constexpr uint32_t kTtIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(256 >> 3) << 17) | ((uint32_t)(64 >> 4) << 24);
+
+__device__ __forceinline__ void tt_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(kTtIdesc), "r"(accumulate));
+}
+
+// plane gz of one cell into ring slot `slot` as three x-shifted copies, zero outside the cell
+__device__ __forceinline__ void tt_load_plane(unsigned char* A, const __nv_bfloat16* cell_base, int gz, int slot)
+{
+    for (int q = threadIdx.x; q < 3 * 4 * 18 * 16; q += blockDim.x) {
+        const int x = q & 15, hy = (q >> 4) % 18, c = (q / (18 * 16)) & 3, dx = q / (4 * 18 * 16);
+        const int gy = hy - 1, gx = x + dx - 1;
+        const uint32_t off = slot * kTtPlane + dx * kTtDx + c * kTtChunk + (hy * 16 + x) * 16;
+        if (gz >= 0 && gz < kV && gy >= 0 && gy < kV && gx >= 0 && gx < kV)
+            cp_async16(smem_u32(A) + off, cell_base + ((size_t)((gz * kV + gy) * kV + gx) * kCh + c * 8));
+        else
+            *reinterpret_cast<uint4*>(A + off) = make_uint4(0, 0, 0, 0);
+    }
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(128, 1) k_conv32_tt(const __nv_bfloat16* __restrict__ in, const __nv_bfloat16* __restrict__ w,
+                                                      const float* __restrict__ bias, const __nv_bfloat16* __restrict__ mask,
+                                                      __nv_bfloat16* __restrict__ out, float* __restrict__ outf, int* err)
+{
+    extern __shared__ __align__(128) unsigned char sm[];
+    unsigned char* A = sm;
+    unsigned char* W = sm + kTtA;
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + kTtA + kTtW);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kTtA + kTtW + 8);
+    const int cell = blockIdx.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const __nv_bfloat16* inc = in + (size_t)cell * kVox * kCh;
+    const uint32_t bar = smem_u32(mbar);
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar));
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;\n" ::"r"(smem_u32(tslot)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    for (int q = tid; q < kTaps * kCh * 4; q += blockDim.x) {
+        const int row = q >> 2, c = q & 3;
+        cp_async16(smem_u32(W) + (c * kTaps * kCh + row) * 16, w + (size_t)row * kCh + c * 8);
+    }
+    for (int q = tid; q < 64; q += blockDim.x)
+        *reinterpret_cast<uint4*>(W + kTaps * kCh * 4 * 16 + 16 * q) = make_uint4(0, 0, 0, 0);
+    // planes -1, 0, 1 in slots 0, 1, 2 (plane gz in slot (gz + 1) % 3)
+    tt_load_plane(A, inc, -1, 0);
+    tt_load_plane(A, inc, 0, 1);
+    tt_load_plane(A, inc, 1, 2);
+    cp_async_wait_all();
+    asm volatile("fence.proxy.async.shared::cta;\n" ::);
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    const uint32_t tbase = *tslot;
+    const uint32_t a0 = smem_u32(A), w0 = smem_u32(W);
+    bool ok = true;
+    for (int z = 0; z < kV; z++) {
+        if (tid == 0 && ok) {
+            for (int tap = 0; tap < kTaps; tap++) {
+                const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3, slot = (z + dz) % 3;
+                for (int kc = 0; kc < 2; kc++) {
+                    const uint32_t woff = (2 * kc * kTaps + tap) * kCh * 16;
+                    const uint32_t aoff = slot * kTtPlane + dx * kTtDx + 2 * kc * kTtChunk + dy * 16 * 16;
+                    tt_mma(tbase, tc_desc(w0 + woff, kTaps * kCh * 16, 128), tc_desc(a0 + aoff, kTtChunk, 128),
+                           (tap | kc) != 0);
+                }
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar) : "memory");
+        }
+        ok = ok && tc_wait(bar, z & 1);
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+        // stage the plane in the slot of plane z - 1 (no longer read): [voxel][channel]
+        unsigned char* T = A + (z % 3) * kTtPlane;
+        if (ok && warp < 2) {
+            const int co = 16 * warp + (lane & 15);
+#pragma unroll 1
+            for (int cb = 0; cb < 8; cb++) {
+                uint32_t v[32];
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+                    "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                      "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+                      "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+                      "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                    : "r"(tbase + ((uint32_t)(32 * warp) << 16) + 32 * cb));
+                asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+                if (lane < 16) {
+#pragma unroll
+                    for (int j = 0; j < 32; j++) {
+                        const int vox = 32 * cb + j;
+                        const float a = __uint_as_float(v[j]);
+                        if (EPI == kEpiF32) {
+                            reinterpret_cast<float*>(T)[vox * kCh + co] = a + bias[co];
+                        } else {
+                            const float r = EPI == kEpiRelu ? fmaxf(a + bias[co], 0.f) : a;
+                            reinterpret_cast<__nv_bfloat16*>(T)[vox * kCh + co] = __float2bfloat16_rn(r);
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (ok) {
+            // copy out: 256 voxel records of 64 B (BF16) or 128 B (FP32), 16-byte stores
+            const size_t vbase = (size_t)cell * kVox + (size_t)z * 256;
+            if (EPI == kEpiF32) {
+                for (int q = tid; q < 256 * 8; q += blockDim.x)
+                    reinterpret_cast<uint4*>(outf + vbase * kCh)[q] = reinterpret_cast<const uint4*>(T)[q];
+            } else {
+                for (int q = tid; q < 256 * 4; q += blockDim.x) {
+                    uint4 val = reinterpret_cast<const uint4*>(T)[q];
+                    if (EPI == kEpiMask) {
+                        const uint4 mm = reinterpret_cast<const uint4*>(mask + vbase * kCh)[q];
+                        __nv_bfloat162* h = reinterpret_cast<__nv_bfloat162*>(&val);
+                        const __nv_bfloat162* m2 = reinterpret_cast<const __nv_bfloat162*>(&mm);
+#pragma unroll
+                        for (int k = 0; k < 4; k++) {
+                            const __nv_bfloat162 zero = __floats2bfloat162_rn(0.f, 0.f);
+                            h[k].x = __bfloat162float(m2[k].x) > 0.f ? h[k].x : zero.x;
+                            h[k].y = __bfloat162float(m2[k].y) > 0.f ? h[k].y : zero.y;
+                        }
+                    }
+                    reinterpret_cast<uint4*>(out + vbase * kCh)[q] = val;
+                }
+            }
+        }
+        __syncthreads();
+        // plane z + 2 into the slot just used for staging (plane z - 1's)
+        tt_load_plane(A, inc, z + 2, z % 3);
+        cp_async_wait_all();
+        asm volatile("fence.proxy.async.shared::cta;\n" ::);
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    }
+    if (!ok && tid == 0) atomicExch(err, 1);
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;\n" ::"r"(tbase));
+}
+
 // dW[tap][co][ci] = sum_v dZ[v][co] A[v + tap][ci] and db[co] = sum_v dZ[v][co] over the cells of
 // this CTA (one fixed-order partial per CTA).  M = co (two m16 tiles, A operand = dZ^T through
 // ldmatrix.trans), N = ci (four n8 tiles, B operand = shifted activations through ldmatrix.trans),
@@ -845,7 +1009,7 @@ struct NetHandle {
     DBuf<int32_t> idx;
     DBuf<int> flag;
     DBuf<int> err;       // set by a tcgen05 kernel whose completion wait timed out
-    int tcgen05 = 0;     // 1: layers 1-3 on tcgen05 (k_conv32_tc), 0: mma.sync (k_conv32)
+    int tcgen05 = 0;     // layers 1-3: 0 mma.sync (k_conv32), 1 tcgen05 M=64 tiles (k_conv32_tc), 2 tcgen05 transposed (k_conv32_tt)
     ~NetHandle()
     {
         if (stream) cudaStreamDestroy(stream);
@@ -885,6 +1049,9 @@ int conv_attrs()
     MSFEM_CK(cudaFuncSetAttribute(k_conv32_tc<kEpiRelu>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
     MSFEM_CK(cudaFuncSetAttribute(k_conv32_tc<kEpiF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
     MSFEM_CK(cudaFuncSetAttribute(k_conv32_tc<kEpiMask>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
+    MSFEM_CK(cudaFuncSetAttribute(k_conv32_tt<kEpiRelu>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTtSmem));
+    MSFEM_CK(cudaFuncSetAttribute(k_conv32_tt<kEpiF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTtSmem));
+    MSFEM_CK(cudaFuncSetAttribute(k_conv32_tt<kEpiMask>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTtSmem));
     done = true;
     return 0;
 }
@@ -894,7 +1061,9 @@ template <int EPI>
 void conv(NetHandle& N, int n, const __nv_bfloat16* in, const __nv_bfloat16* w, const float* bias, const __nv_bfloat16* mask,
           __nv_bfloat16* out, float* outf)
 {
-    if (N.tcgen05)
+    if (N.tcgen05 == 2)
+        k_conv32_tt<EPI><<<n, 128, kTtSmem, N.stream>>>(in, w, bias, mask, out, outf, N.err.p);
+    else if (N.tcgen05 == 1)
         k_conv32_tc<EPI><<<n, 128, kTcSmem, N.stream>>>(in, w, bias, mask, out, outf, N.err.p);
     else
         k_conv32<EPI><<<dim3(8, n), 256, kConvSmem, N.stream>>>(in, w, bias, mask, out, outf);
@@ -1298,7 +1467,7 @@ int msfem_net_predict(msfem_net_t h, msfem_cells_t cells, float* ms)
 int msfem_net_set_tensor_path(msfem_net_t h, int tcgen05)
 {
     using namespace msfem;
-    if (!h || (tcgen05 != 0 && tcgen05 != 1)) {
+    if (!h || tcgen05 < 0 || tcgen05 > 2) {
         set_error("msfem_net_set_tensor_path: bad arguments");
         return MSFEM_ERR_ARGUMENT;
     }

@@ -50,9 +50,10 @@ class CoarseNet:
         self.n_params = L.msfem_net_param_count()
         self.n_train = 0
 
-    def set_tensor_path(self, tcgen05: bool):
-        """Layers 1-3 on tcgen05 (TMEM accumulators) or on warp-level mma.sync."""
-        check(load().msfem_net_set_tensor_path(self.h, int(bool(tcgen05))), "net_set_tensor_path")
+    def set_tensor_path(self, path: int):
+        """Layers 1-3: 0 = warp-level mma.sync, 1 = tcgen05 with M = 64 voxel tiles, 2 = tcgen05
+        transposed product (N = 256 voxels per instruction)."""
+        check(load().msfem_net_set_tensor_path(self.h, int(path)), "net_set_tensor_path")
 
     def params(self) -> np.ndarray:
         p = np.empty(self.n_params, np.float32)
