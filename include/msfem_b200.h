@@ -100,6 +100,18 @@ int msfem_system_create(int kind, int n_nodes, const double* xyz, int n_tets, co
                         const int32_t* material, int on_device, msfem_system_t* out);
 int msfem_system_destroy(msfem_system_t h);
 
+/* A scalar system from a matrix the caller already holds in the reference's CSSD_Matrix<double,
+ * double> layout (Library/CSSD_Matrix.h:11-17): Diag[n]; row i's lower entries A_down[i] with
+ * their columns id_column_for_A_down[i] (< i) and upper entries A_up[i] with
+ * id_column_for_A_up[i] (> i), flattened with row offsets down_ptr / up_ptr [n + 1]; F and X
+ * (either may be NULL: zeros).  Host arrays; lists may be unsorted (sorted here), a repeated
+ * column is an error.  Every solver (msfem_solve, msfem_solve_gmres, FP32 refinement, Dirichlet
+ * rows, export) then runs on the GPU copy: the drop-in for CSSD_Matrix::MSG /
+ * MSG_PreconditioningSSOR / BiCG_Stab / GMRES on the reference's own matrix object.  The system
+ * has no mesh (assembly calls return an error). */
+int msfem_system_from_cssd(int n, const double* diag, const int64_t* down_ptr, const int32_t* down_col,
+                           const double* down_val, const int64_t* up_ptr, const int32_t* up_col, const double* up_val,
+                           const double* F, const double* X, msfem_system_t* out);
 /* n_rows, scalar nnz of the CSR export (diagonal included), element colour count */
 int msfem_system_info(msfem_system_t h, int* n_rows, int64_t* nnz, int* n_colors);
 int msfem_get_stats(msfem_system_t h, msfem_stats* out);

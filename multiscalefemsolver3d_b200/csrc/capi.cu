@@ -2,6 +2,7 @@
 // and argument checking around the kernels of the other translation units.
 #include <cstdarg>
 #include <cstring>
+#include <algorithm>
 #include <memory>
 #include <new>
 #include <string>
@@ -91,6 +92,16 @@ int use_device(System& s)
     return MSFEM_OK;
 }
 
+// systems imported as a matrix (msfem_system_from_cssd) have no mesh to assemble from
+int need_mesh(System& s, const char* who)
+{
+    if (!s.tets.p) {
+        set_error("%s: the system was imported as a matrix and has no mesh", who);
+        return MSFEM_ERR_ARGUMENT;
+    }
+    return MSFEM_OK;
+}
+
 }  // namespace
 }  // namespace msfem
 
@@ -159,6 +170,98 @@ int msfem_system_create(int kind, int n_nodes, const double* xyz, int n_tets, co
     return MSFEM_OK;
 }
 
+int msfem_system_from_cssd(int n, const double* diag, const int64_t* down_ptr, const int32_t* down_col,
+                           const double* down_val, const int64_t* up_ptr, const int32_t* up_col, const double* up_val,
+                           const double* F, const double* X, msfem_system_t* out)
+{
+    if (!out || n <= 0 || !diag || !down_ptr || !up_ptr) {
+        set_error("msfem_system_from_cssd: bad arguments");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    *out = nullptr;
+    if (down_ptr[0] != 0 || up_ptr[0] != 0) {
+        set_error("msfem_system_from_cssd: row offsets must start at 0");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    const int64_t n_down = down_ptr[n], n_up = up_ptr[n];
+    if ((n_down > 0 && (!down_col || !down_val)) || (n_up > 0 && (!up_col || !up_val)) ||
+        (int64_t)n + n_down + n_up > INT32_MAX) {
+        set_error("msfem_system_from_cssd: bad entry arrays or more than 2^31 entries");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    // CSR rows [A_down (columns < i, ascending) | Diag | A_up (columns > i, ascending)]: the
+    // reference's row layout; lists given unsorted are sorted here, repeated columns rejected
+    std::vector<int32_t> rp(n + 1, 0), col;
+    std::vector<double> val;
+    col.reserve(n + n_down + n_up);
+    val.reserve(n + n_down + n_up);
+    std::vector<std::pair<int32_t, double>> tmp;
+    for (int i = 0; i < n; i++) {
+        for (int part = 0; part < 3; part++) {
+            if (part == 1) {
+                col.push_back(i);
+                val.push_back(diag[i]);
+                continue;
+            }
+            const int64_t* ptr = part == 0 ? down_ptr : up_ptr;
+            const int32_t* c = part == 0 ? down_col : up_col;
+            const double* v = part == 0 ? down_val : up_val;
+            if (ptr[i + 1] < ptr[i]) {
+                set_error("msfem_system_from_cssd: row %d has decreasing offsets", i);
+                return MSFEM_ERR_ARGUMENT;
+            }
+            tmp.clear();
+            for (int64_t k = ptr[i]; k < ptr[i + 1]; k++) {
+                const int32_t j = c[k];
+                if ((part == 0 && (j < 0 || j >= i)) || (part == 2 && (j <= i || j >= n))) {
+                    set_error("msfem_system_from_cssd: row %d lists column %d in its %s part", i, j,
+                              part == 0 ? "lower" : "upper");
+                    return MSFEM_ERR_ARGUMENT;
+                }
+                tmp.emplace_back(j, v[k]);
+            }
+            std::sort(tmp.begin(), tmp.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+            for (size_t k = 0; k < tmp.size(); k++) {
+                if (k && tmp[k].first == tmp[k - 1].first) {
+                    set_error("msfem_system_from_cssd: row %d lists column %d twice", i, tmp[k].first);
+                    return MSFEM_ERR_ARGUMENT;
+                }
+                col.push_back(tmp[k].first);
+                val.push_back(tmp[k].second);
+            }
+        }
+        rp[i + 1] = (int32_t)col.size();
+    }
+    std::unique_ptr<System> s(new (std::nothrow) System());
+    if (!s) {
+        set_error("out of host memory");
+        return MSFEM_ERR_LIMIT;
+    }
+    s->kind = MSFEM_SCALAR;
+    s->bs = 1;
+    s->n_nodes = n;
+    s->n_tets = 0;
+    s->n_rows = n;
+    s->nnzb = (int64_t)col.size();
+    s->color_off = {0};
+    MSFEM_CK(cudaGetDevice(&s->device));
+    MSFEM_CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    MSFEM_CK(cudaEventCreate(&s->ev0));
+    MSFEM_CK(cudaEventCreate(&s->ev1));
+    MSFEM_TRY(to_device(*s, s->nrp, rp.data(), rp.size()));
+    MSFEM_TRY(to_device(*s, s->ncol, col.data(), col.size()));
+    MSFEM_TRY(to_device(*s, s->val, val.data(), val.size()));
+    MSFEM_TRY(s->F.alloc((size_t)n));
+    MSFEM_TRY(s->X.alloc((size_t)n));
+    if (F) MSFEM_CK(cudaMemcpyAsync(s->F.p, F, sizeof(double) * n, cudaMemcpyDefault, s->stream));
+    else MSFEM_CK(cudaMemsetAsync(s->F.p, 0, sizeof(double) * n, s->stream));
+    if (X) MSFEM_CK(cudaMemcpyAsync(s->X.p, X, sizeof(double) * n, cudaMemcpyDefault, s->stream));
+    else MSFEM_CK(cudaMemsetAsync(s->X.p, 0, sizeof(double) * n, s->stream));
+    MSFEM_CK(cudaStreamSynchronize(s->stream));
+    *out = reinterpret_cast<msfem_system_t>(s.release());
+    return MSFEM_OK;
+}
+
 int msfem_system_destroy(msfem_system_t h)
 {
     if (!h) return MSFEM_OK;
@@ -214,6 +317,7 @@ int msfem_clear(msfem_system_t h)
 int msfem_assemble_scalar(msfem_system_t h, const double* sigma, int n_materials)
 {
     MSFEM_TRY(check_handle(h));
+    MSFEM_TRY(need_mesh(*as_sys(h), "msfem_assemble_scalar"));
     MSFEM_TRY(use_device(*as_sys(h)));
     return assemble_scalar(*as_sys(h), sigma, n_materials);
 }
@@ -221,6 +325,7 @@ int msfem_assemble_scalar(msfem_system_t h, const double* sigma, int n_materials
 int msfem_assemble_elastic(msfem_system_t h, const double* E, const double* nu, int n_materials)
 {
     MSFEM_TRY(check_handle(h));
+    MSFEM_TRY(need_mesh(*as_sys(h), "msfem_assemble_elastic"));
     MSFEM_TRY(use_device(*as_sys(h)));
     return assemble_elastic(*as_sys(h), E, nu, n_materials);
 }
@@ -228,6 +333,7 @@ int msfem_assemble_elastic(msfem_system_t h, const double* E, const double* nu, 
 int msfem_assemble_elastic_textbook(msfem_system_t h, const double* E, const double* nu, int n_materials)
 {
     MSFEM_TRY(check_handle(h));
+    MSFEM_TRY(need_mesh(*as_sys(h), "msfem_assemble_elastic_textbook"));
     MSFEM_TRY(use_device(*as_sys(h)));
     return assemble_elastic(*as_sys(h), E, nu, n_materials, true);
 }
@@ -237,6 +343,7 @@ int msfem_add_traction(msfem_system_t h, int n_faces, const int32_t* face_nodes,
     (void)on_device;
     MSFEM_TRY(check_handle(h));
     System& s = *as_sys(h);
+    MSFEM_TRY(need_mesh(s, "msfem_add_traction"));
     MSFEM_TRY(use_device(s));
     if (n_faces < 0 || (n_faces > 0 && (!face_nodes || !traction))) {
         set_error("msfem_add_traction: bad arguments");

@@ -89,6 +89,49 @@ class System:
         check(L.msfem_system_info(h, C.byref(n_rows), C.byref(nnz), C.byref(nc)), "system_info")
         self.n_rows, self.nnz, self.n_colors = n_rows.value, nnz.value, nc.value
 
+    @classmethod
+    def from_cssd(cls, diag, down_cols, down_vals, up_cols, up_vals, F=None, X=None):
+        """A scalar system from the reference's CSSD_Matrix arrays (per row i: A_down[i] with
+        id_column_for_A_down[i], Diag[i], A_up[i] with id_column_for_A_up[i]); no mesh."""
+        L = load()
+        diag = np.ascontiguousarray(diag, dtype=np.float64)
+        n = diag.size
+
+        def flat(cols, vals):
+            ptr = np.zeros(n + 1, np.int64)
+            ptr[1:] = np.cumsum([len(c) for c in cols])
+            c = np.ascontiguousarray(np.concatenate([np.asarray(x, np.int32) for x in cols]) if ptr[-1] else
+                                     np.zeros(1, np.int32), dtype=np.int32)
+            v = np.ascontiguousarray(np.concatenate([np.asarray(x, np.float64) for x in vals]) if ptr[-1] else
+                                     np.zeros(1), dtype=np.float64)
+            return ptr, c, v
+
+        dp, dc, dv = flat(down_cols, down_vals)
+        up, uc, uv = flat(up_cols, up_vals)
+        keep = [diag, dp, dc, dv, up, uc, uv]
+        Fa = None if F is None else np.ascontiguousarray(F, dtype=np.float64)
+        Xa = None if X is None else np.ascontiguousarray(X, dtype=np.float64)
+        P = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)  # noqa: E731
+        h = C.c_void_p()
+        check(L.msfem_system_from_cssd(n, P(diag), P(dp), P(dc), P(dv), P(up), P(uc), P(uv), P(Fa), P(Xa), C.byref(h)),
+              "system_from_cssd")
+        del keep
+        self = cls.__new__(cls)
+        self.kind = SCALAR
+        self.h = h
+        self.n_nodes = n
+        self.n_tets = 0
+        n_rows, nnz, nc = C.c_int(), C.c_int64(), C.c_int()
+        check(L.msfem_system_info(h, C.byref(n_rows), C.byref(nnz), C.byref(nc)), "system_info")
+        self.n_rows, self.nnz, self.n_colors = n_rows.value, nnz.value, nc.value
+        return self
+
+    @classmethod
+    def from_csr(cls, A, F=None, X=None):
+        """A scalar system from a Csr (diagonal present in every row), split into the CSSD parts."""
+        diag, up, down, cu, cd = A.cssd()
+        return cls.from_cssd(diag, cd, down, cu, up, F, X)
+
     def close(self):
         if getattr(self, "h", None):
             load().msfem_system_destroy(self.h)
