@@ -60,7 +60,8 @@ enum msfem_precision {
     MSFEM_FP32_IR = 1  /* FP32 matrix + FP32 Krylov inner solves inside FP64 iterative refinement:
                           r = F - A x and x accumulate in FP64.  The inner solver is CG on the
                           Jacobi-scaled matrix for MSFEM_PCG_JACOBI, MINRES on it for
-                          MSFEM_MINRES; other methods are FP64 only                               */
+                          MSFEM_MINRES, GMRES(restart_m) on it for MSFEM_GMRES; BiCGStab is
+                          FP64 only                                                               */
 };
 
 enum msfem_dirichlet_mode {
@@ -112,6 +113,19 @@ int msfem_system_destroy(msfem_system_t h);
 int msfem_system_from_cssd(int n, const double* diag, const int64_t* down_ptr, const int32_t* down_col,
                            const double* down_val, const int64_t* up_ptr, const int32_t* up_col, const double* up_val,
                            const double* F, const double* X, msfem_system_t* out);
+/* Cracked conduction with Heaviside enrichment (no reference counterpart: the reference's XFEM,
+ * MultiXFEM/MultiXFEM_Grid.h:1090-2980, is for elasticity): a scalar system of n_dofs unknowns
+ * (the mesh nodes, then the enriched DOFs) assembled on the GPU from the mesh, the conductivity
+ * of each tetrahedron, the cracks (disc centre and unit normal, [n_cracks][3] each), the crack
+ * cutting each tetrahedron (-1: none) and its vertices' enriched DOFs (enr_dof [n_tets][4],
+ * n_nodes..n_dofs-1 where cut) -- the cut detection and numbering of
+ * multiscalefemsolver3d_b200/xfem.py.  Entries: sigma V grad(phi_i).grad(phi_j) on every
+ * tetrahedron; on a cut one, std-enr sum_s V_s (H_s - H_j) K_ij and enr-enr
+ * sum_s V_s (H_s - H_i)(H_s - H_j) K_ij with the exact side volumes V_s of the crack plane.
+ * F = X = 0; Dirichlet rows and solvers as for any system.  Host arrays. */
+int msfem_xfem_system(int n_nodes, const double* xyz, int n_tets, const int32_t* tets, const double* sigma,
+                      int n_cracks, const double* centre, const double* normal, const int32_t* crack_of_tet,
+                      const int32_t* enr_dof, int n_dofs, msfem_system_t* out);
 /* n_rows, scalar nnz of the CSR export (diagonal included), element colour count */
 int msfem_system_info(msfem_system_t h, int* n_rows, int64_t* nnz, int* n_colors);
 int msfem_get_stats(msfem_system_t h, msfem_stats* out);

@@ -50,6 +50,8 @@ _SIGS = [
     ("msfem_version", C.c_int, []),
     ("msfem_system_create", C.c_int, [C.c_int, C.c_int, _P, C.c_int, _P, _P, C.c_int, C.POINTER(C.c_void_p)]),
     ("msfem_system_from_cssd", C.c_int, [C.c_int, _P, _P, _P, _P, _P, _P, _P, _P, _P, C.POINTER(C.c_void_p)]),
+    ("msfem_xfem_system", C.c_int, [C.c_int, _P, C.c_int, _P, _P, C.c_int, _P, _P, _P, _P, C.c_int,
+                                    C.POINTER(C.c_void_p)]),
     ("msfem_system_destroy", C.c_int, [C.c_void_p]),
     ("msfem_system_info", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int64), C.POINTER(C.c_int)]),
     ("msfem_get_stats", C.c_int, [C.c_void_p, C.POINTER(Stats)]),

@@ -37,13 +37,14 @@ struct GmLayout {
 };
 
 // V0 = r / ||r|| (r and V0 may be the same vector), g = (||r||, 0, ...)
-__global__ void k_gm_start(int n, const double* r, double* V0, double* gm, GmLayout L,
+template <class VT>
+__global__ void k_gm_start(int n, const VT* r, VT* V0, double* gm, GmLayout L,
                            const KState* S)
 {
     const double beta = sqrt(S->rr);
     const double inv = beta > 0 ? 1.0 / beta : 0.0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        V0[i] = r[i] * inv;
+        V0[i] = (VT)((double)r[i] * inv);
     if (blockIdx.x == 0) {
         for (int i = threadIdx.x; i < L.m + 1; i += blockDim.x) gm[L.g() + i] = (i == 0) ? beta : 0.0;
         if (threadIdx.x == 0) {
@@ -54,46 +55,49 @@ __global__ void k_gm_start(int n, const double* r, double* V0, double* gm, GmLay
     }
 }
 
-// z = M^-1 v
-__global__ void k_gm_prec(int n, const double* __restrict__ v, const double* __restrict__ dinv, double* __restrict__ z,
+// z = M^-1 v (dinv == nullptr: the matrix is already Jacobi-scaled, z = v)
+template <class VT>
+__global__ void k_gm_prec(int n, const VT* __restrict__ v, const double* __restrict__ dinv, VT* __restrict__ z,
                           const double* gm, GmLayout L)
 {
     if (gm[L.misc() + 1] != 0.0) return;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        z[i] = v[i] * dinv[i];
+        z[i] = dinv ? (VT)((double)v[i] * dinv[i]) : v[i];
 }
 
-__global__ void __launch_bounds__(256) k_gm_spmv(SellView<double> A, const double* __restrict__ z, double* __restrict__ w,
+template <class VT>
+__global__ void __launch_bounds__(256) k_gm_spmv(SellView<VT> A, const VT* __restrict__ z, VT* __restrict__ w,
                                                  const double* gm, GmLayout L)
 {
     if (gm[L.misc() + 1] != 0.0) return;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (warp >= A.n_slices) return;
     if (A.bs == 1) {
-        const double v = sell_row_scalar<double>(A, warp, lane, z);
+        const VT v = sell_row_scalar<VT>(A, warp, lane, z);
         const int row = warp * kSlice + lane;
         if (row < A.n_rows) w[row] = v;
     } else {
-        double v[3];
-        sell_row_block<double>(A, warp, lane, z, v);
+        VT v[3];
+        sell_row_block<VT>(A, warp, lane, z, v);
         const int brow = warp * kSlice + lane;
         if (brow < A.n_brows)
             for (int c = 0; c < 3; c++) w[3 * (int64_t)brow + c] = v[c];
     }
 }
 
-// h[i] = (V_i, w), i = 0..j
-__global__ void __launch_bounds__(kVecThreads) k_gm_multidot(int n, const double* __restrict__ V, int j,
-                                                             const double* __restrict__ w, double* __restrict__ partial,
+// h[i] = (V_i, w), i = 0..j (FP64 accumulation for either vector type)
+template <class VT>
+__global__ void __launch_bounds__(kVecThreads) k_gm_multidot(int n, const VT* __restrict__ V, int j,
+                                                             const VT* __restrict__ w, double* __restrict__ partial,
                                                              unsigned int* ticket, double* gm, GmLayout L, size_t hoff)
 {
     if (gm[L.misc() + 1] != 0.0) return;
     __shared__ double sh[32];
     for (int i = 0; i <= j; i++) {
-        const double* vi = V + (size_t)i * n;
+        const VT* vi = V + (size_t)i * n;
         double acc[1] = {0.0};
         for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
-            acc[0] += vi[r] * w[r];
+            acc[0] += (double)vi[r] * (double)w[r];
         block_sum<1>(acc, sh);
         if (threadIdx.x == 0) partial[(size_t)i * gridDim.x + blockIdx.x] = acc[0];
     }
@@ -108,9 +112,9 @@ __global__ void __launch_bounds__(kVecThreads) k_gm_multidot(int n, const double
 }
 
 // w -= sum_i h[i] V_i ; with LAST, also (w, w) -> the new subdiagonal entry, and H[:, j] = h1 + h2
-template <bool LAST>
-__global__ void __launch_bounds__(kVecThreads) k_gm_orth(int n, const double* __restrict__ V, int j,
-                                                         double* __restrict__ w, double* __restrict__ partial,
+template <class VT, bool LAST>
+__global__ void __launch_bounds__(kVecThreads) k_gm_orth(int n, const VT* __restrict__ V, int j,
+                                                         VT* __restrict__ w, double* __restrict__ partial,
                                                          unsigned int* ticket, double* gm, GmLayout L, size_t hoff)
 {
     if (gm[L.misc() + 1] != 0.0) return;
@@ -120,10 +124,11 @@ __global__ void __launch_bounds__(kVecThreads) k_gm_orth(int n, const double* __
     __syncthreads();
     double acc[1] = {0.0};
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
-        double t = w[r];
-        for (int i = 0; i <= j; i++) t -= hs[i] * V[(size_t)i * n + r];
-        w[r] = t;
-        acc[0] += t * t;
+        double t = (double)w[r];
+        for (int i = 0; i <= j; i++) t -= hs[i] * (double)V[(size_t)i * n + r];
+        w[r] = (VT)t;
+        const double tv = (double)w[r];
+        acc[0] += tv * tv;
     }
     if (!LAST) return;
     block_sum<1>(acc, sh);
@@ -181,7 +186,8 @@ __global__ void k_gm_givens(int j, double* gm, GmLayout L, KState* S)
 }
 
 // V_{j+1} = w / ||w||
-__global__ void k_gm_normalize(int n, const double* __restrict__ w, double* __restrict__ vnext, int j, const double* gm,
+template <class VT>
+__global__ void k_gm_normalize(int n, const VT* __restrict__ w, VT* __restrict__ vnext, int j, const double* gm,
                                GmLayout L)
 {
     if (gm[L.misc() + 1] != 0.0) return;
@@ -189,7 +195,7 @@ __global__ void k_gm_normalize(int n, const double* __restrict__ w, double* __re
     const double norm = gm[L.misc() + 3];
     const double inv = norm > 0 ? 1.0 / norm : 0.0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        vnext[i] = w[i] * inv;
+        vnext[i] = (VT)((double)w[i] * inv);
 }
 
 // save ||w|| before the rotation overwrites H[j+1][j]
@@ -215,7 +221,8 @@ __global__ void k_gm_backsolve(double* gm, GmLayout L)
     }
 }
 
-__global__ void __launch_bounds__(kVecThreads) k_gm_update(int n, double* __restrict__ x, const double* __restrict__ V,
+template <class VT>
+__global__ void __launch_bounds__(kVecThreads) k_gm_update(int n, VT* __restrict__ x, const VT* __restrict__ V,
                                                            const double* __restrict__ dinv, const double* gm, GmLayout L)
 {
     __shared__ double ys[1024];
@@ -224,8 +231,32 @@ __global__ void __launch_bounds__(kVecThreads) k_gm_update(int n, double* __rest
     __syncthreads();
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
         double t = 0.0;
-        for (int i = 0; i < k; i++) t += ys[i] * V[(size_t)i * n + r];
-        x[r] += dinv[r] * t;
+        for (int i = 0; i < k; i++) t += ys[i] * (double)V[(size_t)i * n + r];
+        x[r] = (VT)((double)x[r] + (dinv ? dinv[r] : 1.0) * t);
+    }
+}
+
+// FP32 residual of the inner solve: V0 = b - w (w = A d), (V0, V0) into S->rr (last block)
+__global__ void __launch_bounds__(kVecThreads) k_gm_res32(int n, const float* __restrict__ b, const float* __restrict__ w,
+                                                          float* __restrict__ V0, double* __restrict__ partial,
+                                                          unsigned int* ticket, KState* S)
+{
+    __shared__ double sh[32];
+    double acc[1] = {0.0};
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        const float t = b[r] - w[r];
+        V0[r] = t;
+        acc[0] += (double)t * (double)t;
+    }
+    block_sum<1>(acc, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = acc[0];
+    if (arrive_last(ticket)) {
+        double t[1];
+        reduce_partials<1>(partial, gridDim.x, 0, t, sh);
+        if (threadIdx.x == 0) {
+            S->rr = t[0];
+            *ticket = 0;
+        }
     }
 }
 
@@ -280,30 +311,30 @@ int solve_gmres64(System& s, int m, int maxiter, double tol, int* iters, int* re
         MSFEM_CK(cudaStreamSynchronize(s.stream));
         s.launches += 1;
         if (s.h_kstate->rr <= s.h_kstate->tol2 || s.h_kstate->done || total >= maxiter) break;
-        k_gm_start<<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, V, V, s.gm.p, L, S);
+        k_gm_start<double><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, V, V, s.gm.p, L, S);
         s.launches += 1;
         if (!exec) {
             cudaGraph_t graph;
             MSFEM_CK(cudaStreamBeginCapture(s.stream, cudaStreamCaptureModeThreadLocal));
             for (int j = 0; j < m; j++) {
                 double* vj = V + (size_t)j * n;
-                k_gm_prec<<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, vj, s.dinv64.p, z, s.gm.p, L);
-                k_gm_spmv<<<g, 256, 0, s.stream>>>(A, z, w, s.gm.p, L);
-                k_gm_multidot<<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, V, j, w, part, &S->ticket[0], s.gm.p, L,
-                                                                           L.h1());
-                k_gm_orth<false><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, V, j, w, part, &S->ticket[0], s.gm.p,
-                                                                              L, L.h1());
-                k_gm_multidot<<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, V, j, w, part, &S->ticket[0], s.gm.p, L,
-                                                                           L.h2());
-                k_gm_orth<true><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, V, j, w, part, &S->ticket[0], s.gm.p,
-                                                                             L, L.h2());
+                k_gm_prec<double><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, vj, s.dinv64.p, z, s.gm.p, L);
+                k_gm_spmv<double><<<g, 256, 0, s.stream>>>(A, z, w, s.gm.p, L);
+                k_gm_multidot<double><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, V, j, w, part, &S->ticket[0], s.gm.p,
+                                                                                   L, L.h1());
+                k_gm_orth<double, false><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, V, j, w, part, &S->ticket[0],
+                                                                                      s.gm.p, L, L.h1());
+                k_gm_multidot<double><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, V, j, w, part, &S->ticket[0], s.gm.p,
+                                                                                   L, L.h2());
+                k_gm_orth<double, true><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, V, j, w, part, &S->ticket[0],
+                                                                                     s.gm.p, L, L.h2());
                 k_gm_save_norm<<<1, 1, 0, s.stream>>>(j, s.gm.p, L);
                 k_gm_givens<<<1, 1, 0, s.stream>>>(j, s.gm.p, L, S);
-                k_gm_normalize<<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, w, V + (size_t)(j + 1) * n, j, s.gm.p,
-                                                                            L);
+                k_gm_normalize<double><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, w, V + (size_t)(j + 1) * n, j,
+                                                                                    s.gm.p, L);
             }
             k_gm_backsolve<<<1, 1, 0, s.stream>>>(s.gm.p, L);
-            k_gm_update<<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, s.X.p, V, s.dinv64.p, s.gm.p, L);
+            k_gm_update<double><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, s.X.p, V, s.dinv64.p, s.gm.p, L);
             cudaError_t e = cudaStreamEndCapture(s.stream, &graph);
             if (e != cudaSuccess) {
                 set_error("GMRES graph capture failed: %s", cudaGetErrorString(e));
@@ -334,6 +365,103 @@ int solve_gmres64(System& s, int m, int maxiter, double tol, int* iters, int* re
     *iters = s.h_kstate->iter;
     *restarts = cycles;
     return (s.h_kstate->rr <= s.h_kstate->tol2) ? MSFEM_OK : MSFEM_NOT_CONVERGED;
+}
+
+// Inner solve of FP32 iterative refinement: GMRES(m) on the FP32 copy of the Jacobi-scaled matrix
+// (unit diagonal, so no preconditioner), A d = b from d = 0, to ||b - A d|| <= tau ||b||.  The
+// Krylov basis is FP32 (half the bytes of the FP64 solver per Arnoldi pass); the Hessenberg
+// matrix, the rotations and every inner product are FP64.  V is (m+1) n floats, w one more n.
+int gmres32_inner(System& s, int m, float* d, const float* b, float* V, float* w, int maxiter, double tau, int* iters)
+{
+    const int n = s.n_rows;
+    GmLayout L{m};
+    MSFEM_TRY(s.gm.alloc(L.total()));
+    MSFEM_TRY(s.partial.alloc((size_t)(m + 2) * kReduceBlocks + 64));
+    KState* S = s.kstate.p;
+    double* part = s.partial.p;
+    MSFEM_CK(cudaMemsetAsync(s.gm.p, 0, sizeof(double) * L.total(), s.stream));
+    const SellView<float> A = sell_view<float>(s);
+    const unsigned g = spmv_grid(s);
+    // (b, b) -> ff via the residual kernel with w = 0
+    MSFEM_CK(cudaMemsetAsync(w, 0, sizeof(float) * n, s.stream));
+    k_gm_res32<<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, b, w, V, part, &S->ticket[0], S);
+    s.launches += 1;
+    MSFEM_CK(cudaMemcpyAsync(s.h_kstate, S, sizeof(KState), cudaMemcpyDeviceToHost, s.stream));
+    MSFEM_CK(cudaStreamSynchronize(s.stream));
+    KState init = *s.h_kstate;
+    init.ff = init.rr;
+    init.tol2 = tau * tau * init.ff;
+    init.maxiter = maxiter;
+    init.iter = 0;
+    init.done = 0;
+    init.breakdown = 0;
+    for (auto& t : init.ticket) t = 0;
+    *s.h_kstate = init;
+    MSFEM_CK(cudaMemcpyAsync(S, s.h_kstate, sizeof(KState), cudaMemcpyHostToDevice, s.stream));
+    cudaGraphExec_t exec = nullptr;
+    int rc = MSFEM_OK;
+    bool first = true;
+    while (true) {
+        if (!first) {
+            // V_0 = b - A d
+            MSFEM_TRY(spmv32(s, d, w));
+            k_gm_res32<<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, b, w, V, part, &S->ticket[0], S);
+            s.launches += 2;
+            MSFEM_CK(cudaMemcpyAsync(s.h_kstate, S, sizeof(KState), cudaMemcpyDeviceToHost, s.stream));
+            MSFEM_CK(cudaStreamSynchronize(s.stream));
+        }
+        first = false;  // on entry d = 0 and V_0 already holds b
+        if (s.h_kstate->rr <= s.h_kstate->tol2 || s.h_kstate->done || s.h_kstate->iter >= maxiter) break;
+        k_gm_start<float><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, V, V, s.gm.p, L, S);
+        s.launches += 1;
+        if (!exec) {
+            cudaGraph_t graph;
+            MSFEM_CK(cudaStreamBeginCapture(s.stream, cudaStreamCaptureModeThreadLocal));
+            for (int j = 0; j < m; j++) {
+                const float* vj = V + (size_t)j * n;
+                k_gm_spmv<float><<<g, 256, 0, s.stream>>>(A, vj, w, s.gm.p, L);
+                k_gm_multidot<float><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, V, j, w, part, &S->ticket[0], s.gm.p,
+                                                                                  L, L.h1());
+                k_gm_orth<float, false><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, V, j, w, part, &S->ticket[0],
+                                                                                     s.gm.p, L, L.h1());
+                k_gm_multidot<float><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, V, j, w, part, &S->ticket[0], s.gm.p,
+                                                                                  L, L.h2());
+                k_gm_orth<float, true><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, V, j, w, part, &S->ticket[0],
+                                                                                    s.gm.p, L, L.h2());
+                k_gm_save_norm<<<1, 1, 0, s.stream>>>(j, s.gm.p, L);
+                k_gm_givens<<<1, 1, 0, s.stream>>>(j, s.gm.p, L, S);
+                k_gm_normalize<float><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, w, V + (size_t)(j + 1) * n, j,
+                                                                                   s.gm.p, L);
+            }
+            k_gm_backsolve<<<1, 1, 0, s.stream>>>(s.gm.p, L);
+            k_gm_update<float><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, d, V, nullptr, s.gm.p, L);
+            cudaError_t e = cudaStreamEndCapture(s.stream, &graph);
+            if (e != cudaSuccess) {
+                set_error("GMRES graph capture failed: %s", cudaGetErrorString(e));
+                return MSFEM_ERR_CUDA;
+            }
+            e = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) {
+                set_error("GMRES graph instantiate failed: %s", cudaGetErrorString(e));
+                return MSFEM_ERR_CUDA;
+            }
+        }
+        cudaError_t e = cudaGraphLaunch(exec, s.stream);
+        if (e != cudaSuccess) {
+            set_error("GMRES graph launch failed: %s", cudaGetErrorString(e));
+            rc = MSFEM_ERR_CUDA;
+            break;
+        }
+        s.launches += 8 * m + 2;
+        MSFEM_CK(cudaMemcpyAsync(s.h_kstate, S, sizeof(KState), cudaMemcpyDeviceToHost, s.stream));
+        MSFEM_CK(cudaStreamSynchronize(s.stream));
+        if (s.h_kstate->done) break;
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    if (rc < 0) return rc;
+    *iters = s.h_kstate->iter;
+    return MSFEM_OK;
 }
 
 }  // namespace msfem

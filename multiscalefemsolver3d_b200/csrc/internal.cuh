@@ -182,5 +182,7 @@ int solve(System& s, int method, int precision, int restart_m, int maxiter, doub
 // ---- MINRES (minres.cu): on S A S from x = 0 with right-hand side S r (FP64: x += S y) or r (FP32)
 template <class VT, bool SCALE>
 int minres_run(System& s, VT* x, const VT* r, int maxiter, double tol, int stall_unused, int* iters);
+// FP32 GMRES(m) inner solve on the Jacobi-scaled FP32 matrix (gmres.cu)
+int gmres32_inner(System& s, int m, float* d, const float* b, float* V, float* w, int maxiter, double tau, int* iters);
 
 }  // namespace msfem

@@ -607,23 +607,29 @@ int solve_pcg64(System& s, bool jacobi, int maxiter, double tol, int* iters)
     return s.h_kstate->done == 1 ? MSFEM_OK : MSFEM_NOT_CONVERGED;
 }
 
-enum Inner { INNER_CG32 = 0, INNER_MINRES32 = 1, INNER_MINRES64 = 2 };
+enum Inner { INNER_CG32 = 0, INNER_MINRES32 = 1, INNER_MINRES64 = 2, INNER_GMRES32 = 3 };
 
 // Iterative refinement around an inner Krylov solve:
 //   r = F - A x in FP64;  inner solve of the Jacobi-scaled system (S A S) y = S r to a relative
 //   tolerance;  x += S y in FP64.
 // INNER_CG32 / INNER_MINRES32: the inner solve runs in FP32 on the FP32 copy of S A S (the right-
 // hand side S r / ||r|| is rounded to FP32 and the correction scaled back by ||r||); CG for SPD
-// matrices, MINRES for symmetric indefinite ones.  INNER_MINRES64: FP64 MINRES, whose stopping test
+// matrices, MINRES for symmetric indefinite ones, GMRES(m) (gmres32_inner) for nonsymmetric ones.
+// INNER_MINRES64: FP64 MINRES, whose stopping test
 // is on the scaled residual, refined until the true ||F - A x|| / ||F|| meets tol.
-int solve_refined(System& s, Inner inner, int maxiter, double tol, int* iters, int* outer)
+int solve_refined(System& s, Inner inner, int maxiter, double tol, int* iters, int* outer, int restart_m = 30)
 {
     const int n = s.n_rows;
     MSFEM_TRY(s.work64.alloc(4 * (size_t)n));
     double* r64 = s.work64.p;
     float *d32 = nullptr, *r32 = nullptr, *p32 = nullptr, *q32 = nullptr;
+    if (inner == INNER_GMRES32 && (restart_m < 1 || restart_m > 1000)) {
+        set_error("GMRES restart depth must be in [1, 1000]");
+        return MSFEM_ERR_ARGUMENT;
+    }
     if (inner != INNER_MINRES64) {
-        MSFEM_TRY(s.work32.alloc(4 * (size_t)n));
+        // GMRES: d, r, then the (m+1) basis vectors and w
+        MSFEM_TRY(s.work32.alloc((inner == INNER_GMRES32 ? (size_t)restart_m + 4 : 4) * (size_t)n));
         d32 = s.work32.p;
         r32 = d32 + n;
         p32 = r32 + n;
@@ -677,6 +683,10 @@ int solve_refined(System& s, Inner inner, int maxiter, double tol, int* iters, i
                 MSFEM_TRY(read_state(s));
                 it = s.h_kstate->iter;
                 if (s.h_kstate->breakdown) rc = MSFEM_ERR_NUMERIC;
+            } else if (inner == INNER_GMRES32) {
+                float* V = r32 + n;
+                rc = gmres32_inner(s, restart_m, d32, r32, V, V + (size_t)(restart_m + 1) * n, maxiter - total_inner, tau,
+                                   &it);
             } else {
                 rc = minres_run<float, false>(s, d32, r32, maxiter - total_inner, tau, 0, &it);
             }
@@ -789,7 +799,10 @@ int solve(System& s, int method, int precision, int restart_m, int maxiter, doub
         rc = solve_bicgstab64(s, maxiter, tol, &it);
         break;
     case MSFEM_GMRES:
-        rc = solve_gmres64(s, restart_m > 0 ? restart_m : 30, maxiter, tol, &it, &outer);
+        if (precision == MSFEM_FP32_IR)
+            rc = solve_refined(s, INNER_GMRES32, maxiter, tol, &it, &outer, restart_m > 0 ? restart_m : 30);
+        else
+            rc = solve_gmres64(s, restart_m > 0 ? restart_m : 30, maxiter, tol, &it, &outer);
         break;
     default:
         rc = MSFEM_ERR_ARGUMENT;

@@ -116,14 +116,19 @@ class System:
         check(L.msfem_system_from_cssd(n, P(diag), P(dp), P(dc), P(dv), P(up), P(uc), P(uv), P(Fa), P(Xa), C.byref(h)),
               "system_from_cssd")
         del keep
+        return cls._from_handle(h)
+
+    @classmethod
+    def _from_handle(cls, h):
+        """Wraps a scalar matrix-only system handle (no mesh)."""
         self = cls.__new__(cls)
         self.kind = SCALAR
         self.h = h
-        self.n_nodes = n
         self.n_tets = 0
         n_rows, nnz, nc = C.c_int(), C.c_int64(), C.c_int()
-        check(L.msfem_system_info(h, C.byref(n_rows), C.byref(nnz), C.byref(nc)), "system_info")
+        check(load().msfem_system_info(h, C.byref(n_rows), C.byref(nnz), C.byref(nc)), "system_info")
         self.n_rows, self.nnz, self.n_colors = n_rows.value, nnz.value, nc.value
+        self.n_nodes = self.n_rows
         return self
 
     @classmethod

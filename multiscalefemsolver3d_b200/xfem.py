@@ -26,7 +26,7 @@ import numpy as np
 
 from . import meshgen
 
-__all__ = ["Cracks", "Enrichment", "random_cracks", "enrich", "side_fraction", "cube_cracked"]
+__all__ = ["Cracks", "Enrichment", "random_cracks", "enrich", "side_fraction", "cube_cracked", "build_system"]
 
 
 @dataclass
@@ -100,14 +100,28 @@ def enrich(xyz, tets, cracks: Cracks) -> Enrichment:
     tets = np.asarray(tets, dtype=np.int64)
     n_nodes, n_tets = xyz.shape[0], tets.shape[0]
     crack_of = -np.ones(n_tets, np.int64)
-    cen = xyz[tets].mean(axis=1)
+    P = xyz[tets]
+    cen = P.mean(axis=1)
+    # a tetrahedron the plane crosses has |centroid - plane| <= its diameter, so a cut one lies
+    # within radius + diameter of the centre: test only those
+    ea, eb = [0, 0, 0, 1, 1, 2], [1, 2, 3, 2, 3, 3]
+    diam = float(np.sqrt(((P[:, ea] - P[:, eb]) ** 2).sum(-1).max())) if n_tets else 0.0
+    del P
+    # centroids bucketed by z so that each crack scans only the slab it can reach
+    order = np.argsort(cen[:, 2], kind="stable")
+    zs = cen[order, 2]
     for k in range(cracks.radius.size):
-        dn = (xyz - cracks.centre[k]) @ cracks.normal[k]
-        dt = dn[tets]
-        cut = (dt.max(axis=1) > 0.0) & (dt.min(axis=1) < 0.0) & (crack_of < 0)
-        if not cut.any():
+        reach = cracks.radius[k] + diam
+        lo, hi = np.searchsorted(zs, cracks.centre[k][2] - reach), np.searchsorted(zs, cracks.centre[k][2] + reach)
+        cand = np.sort(order[lo:hi])
+        near = cand[((cen[cand] - cracks.centre[k]) ** 2).sum(axis=1) < reach ** 2]
+        if near.size == 0:
             continue
-        idx = np.nonzero(cut)[0]
+        dt = (xyz[tets[near]] - cracks.centre[k]) @ cracks.normal[k]
+        cut = (dt.max(axis=1) > 0.0) & (dt.min(axis=1) < 0.0) & (crack_of[near] < 0)
+        idx = near[cut]
+        if idx.size == 0:
+            continue
         rel = cen[idx] - cracks.centre[k]
         inplane = rel - np.outer(rel @ cracks.normal[k], cracks.normal[k])
         inside = np.einsum("ij,ij->i", inplane, inplane) < cracks.radius[k] ** 2
@@ -132,3 +146,24 @@ def cube_cracked(n: int = 96, n_cracks: int = 50, seed: int = 5, rmin: float = 0
     nodes = np.concatenate([lo, hi]).astype(np.int32)
     vals = np.concatenate([np.ones(lo.size), np.zeros(hi.size)])
     return mesh, cracks, nodes, vals
+
+
+def build_system(mesh, cracks: Cracks, sigma=1.0, enr: Enrichment | None = None):
+    """(fem.System of the enriched problem assembled on the GPU (msfem_xfem_system), Enrichment)."""
+    import ctypes as C
+
+    from . import fem
+    from ._lib import check, load
+    enr = enrich(mesh.xyz, mesh.tets, cracks) if enr is None else enr
+    xyz = np.ascontiguousarray(mesh.xyz, dtype=np.float64)
+    tets = np.ascontiguousarray(mesh.tets, dtype=np.int32)
+    sig = np.ascontiguousarray(np.broadcast_to(np.asarray(sigma, dtype=np.float64), (tets.shape[0],)))
+    cen = np.ascontiguousarray(cracks.centre, dtype=np.float64)
+    nor = np.ascontiguousarray(cracks.normal, dtype=np.float64)
+    cof = np.ascontiguousarray(enr.crack_of_tet, dtype=np.int32)
+    edf = np.ascontiguousarray(enr.enr_dof, dtype=np.int32)
+    P = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    h = C.c_void_p()
+    check(load().msfem_xfem_system(xyz.shape[0], P(xyz), tets.shape[0], P(tets), P(sig), cen.shape[0], P(cen), P(nor),
+                                   P(cof), P(edf), enr.n_dofs, C.byref(h)), "xfem_system")
+    return fem.System._from_handle(h), enr

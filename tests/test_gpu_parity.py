@@ -152,7 +152,7 @@ def reference_solution(port, A):
 
 @pytest.mark.parametrize("method,precision", [
     (fem.CG, fem.FP64), (fem.PCG_JACOBI, fem.FP64), (fem.BICGSTAB, fem.FP64), (fem.GMRES, fem.FP64),
-    (fem.MINRES, fem.FP64), (fem.MINRES, fem.FP32_IR)])
+    (fem.GMRES, fem.FP32_IR), (fem.MINRES, fem.FP64), (fem.MINRES, fem.FP32_IR)])
 def test_elastic_solvers(cuda, port, method, precision):
     p = meshgen.cube_elastic(n=8, n_spheres=4, contrast=10.0, rmin=0.1, rmax=0.2)
     with elastic_system(p) as S:
@@ -169,7 +169,7 @@ def test_elastic_solvers(cuda, port, method, precision):
 
 @pytest.mark.parametrize("method,precision", [
     (fem.PCG_JACOBI, fem.FP64), (fem.CG, fem.FP64), (fem.PCG_JACOBI, fem.FP32_IR), (fem.GMRES, fem.FP64),
-    (fem.MINRES, fem.FP64), (fem.MINRES, fem.FP32_IR)])
+    (fem.GMRES, fem.FP32_IR), (fem.MINRES, fem.FP64), (fem.MINRES, fem.FP32_IR)])
 def test_scalar_solvers(cuda, port, method, precision):
     p = meshgen.cube_scalar(n=14, n_spheres=10, rmin=0.05, rmax=0.1, contrast=100.0)
     with scalar_system(p) as S:
