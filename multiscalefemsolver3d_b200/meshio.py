@@ -162,21 +162,25 @@ _TYPES = {2: 102, 3: 203, 4: 304}
 
 def write_salome_dat(path, xyz, elems, vertex_ids=None):
     """Vertices numbered vertex_ids (default 1..n) and elements of 2, 3 or 4 vertices given by
-    their 0-based position in xyz (written 1-based)."""
+    their 0-based position in xyz.  Element lines name their vertices by those vertex ids, as the
+    format does: the reader keeps them (minus one) and maps them back to positions through
+    vertex_map (SimpleGrid::TransferIdGlobalIntoSelf, Library/Math.h:983-991; the MsFEM grids
+    renumber their face meshes that way, MsFEM/MsFEM_Grid.h:1126-1135)."""
     xyz = np.asarray(xyz, dtype=np.float64)
     elems = np.asarray(elems, dtype=np.int64)
     ids = np.arange(1, xyz.shape[0] + 1) if vertex_ids is None else np.asarray(vertex_ids, dtype=np.int64)
     typ = _TYPES[elems.shape[1]]
     lines = [f"{xyz.shape[0]} {elems.shape[0]}\n"]
     lines += [f"{int(i)} {x:.17g} {y:.17g} {z:.17g}\n" for i, (x, y, z) in zip(ids, xyz)]
-    lines += [f"{e + 1} {typ} " + " ".join(str(int(v) + 1) for v in row) + "\n" for e, row in enumerate(elems)]
+    lines += [f"{e + 1} {typ} " + " ".join(str(int(ids[v])) for v in row) + "\n" for e, row in enumerate(elems)]
     with open(path, "w") as f:
         f.write("".join(lines))
 
 
 def read_salome_dat(path, dim, with_map=False):
-    """(xyz, elements [ne, dim + 1] 0-based, vertex_map or None) as ReadFromSalomeDat returns
-    them; element lines of another type than 102/203/304 are skipped."""
+    """(xyz, elements [ne, dim + 1], vertex_map or None) as ReadFromSalomeDat returns them: the
+    elements name vertex ids minus one (vertex_map values, not positions); element lines of
+    another type than 102/203/304 are skipped."""
     with open(path) as f:
         tok = f.read().split()
     nv, ne = int(tok[0]), int(tok[1])
@@ -226,12 +230,15 @@ def write_cell_dirs(root, cm: CellMeshes, one_based=True):
 def write_macro_nvtr(directory, vertex_xyz, cell_vertex, mat=None):
     """The macro mesh as NVTR polyhedra: per cell `8 v0..v7 6 (4 face cycle)x6` (faces x0, x1,
     y0, y1, z0, z1), the polyhedral format MsFEM/MsFEM_Main.cpp:187 reads (k = -1), 0-based (the
-    only form the reference reads correctly)."""
+    only form the reference reads correctly).  The face cycles hold the cell's LOCAL vertex
+    numbers 0..7: the grid takes them as indices into the cell's own vertex list
+    (geometry::Polyhedron::CreateSubMeshInSelf, Library/GeometryShape.h:2709-2733, and
+    GetGlobalIdFace, :2783-2789); global ids there read past the list."""
     recs = []
     for cv in np.asarray(cell_vertex, dtype=np.int64):
         r = [8] + list(cv) + [6]
         for cyc in FACE_CYCLES:
-            r += [4] + [int(cv[v]) for v in cyc]
+            r += [4] + list(cyc)
         recs.append(np.array(r, dtype=np.int64))
     write_nvtr(directory, vertex_xyz, recs, mat, one_based=False)
 

@@ -70,6 +70,8 @@ def test_macro_polyhedra_and_cell_directories(tmp_path, ref):
     xyz, recs, kat, rfz = meshio.read_nvtr(d, -1)
     assert rfz and len(recs) == cc.cells.n_cells       # polyhedra are written 0-based
     np.testing.assert_array_equal(recs[0][1:9], cc.cell_vertex[0])
+    # face cycles in the cell's local vertex numbers
+    np.testing.assert_array_equal(recs[0][10:].reshape(6, 5)[:, 1:], meshio.FACE_CYCLES)
     rx, rrecs, rkat, rrfz = ref.read_nvtr(d, -1, vxyz.shape[0], cc.cells.n_cells, 40 * cc.cells.n_cells)
     assert rrfz == rfz
     for a, b in zip(recs, rrecs):
@@ -90,6 +92,9 @@ def test_macro_polyhedra_and_cell_directories(tmp_path, ref):
             # the map takes the face's vertices to the cell's own nodes, all on face f
             axis, side = f // 2, f % 2
             np.testing.assert_allclose(cx[fmap, axis], cb[2 * axis + side], atol=1e-15)
+            # elements name the cell's own node ids, each a tet face on face f
+            assert set(np.unique(fe)) <= set(fmap)
+            np.testing.assert_allclose(cx[fe, axis], cb[2 * axis + side], atol=1e-15)
             assert fe.shape[0] == 2 * cc.cells.m[c] ** 2
 
 
