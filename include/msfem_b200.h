@@ -310,6 +310,28 @@ int msfem_cells_build_bases(msfem_cells_t c, int precision, double tol, int maxi
  * as Points, MsFEM_Grid.h:5510-5530, transposed to node-major). */
 int msfem_cells_get_bases(msfem_cells_t c, double* bases, int on_device);
 
+/* The MsFEM Order2 basis of every cell (Grid_forMech::CreateFunctionalSpaces,
+ * MsFEM/MsFEM_Grid.h:1001-3080): 27 per cell, in the reference's order (:3045-3054) -- the 8
+ * vertices, the 12 edges in ascending global edge id (the edge's (lower, higher) global vertex
+ * pair), the 6 faces x0 x1 y0 y1 z0 z1, the cell bubble.  cell_vertex: [n_cells][8] global
+ * macro vertex ids of each cell's corners (host or device).  The edge problems are exact (every
+ * edge segment is material 0 in the reference), the face problems (4 linear + 4 edge bubbles per
+ * face, material 0, no load as FEM_2D leaves them) and the 27 volume problems with their bubble
+ * loads run on the GPU; precision / tol / maxiter / threads as for msfem_batch_solve. */
+int msfem_cells_build_order2(msfem_cells_t c, const int32_t* cell_vertex, int precision, double tol, int maxiter,
+                             int threads);
+
+/* bases: [n_nodes][27][3] doubles, node-major (self_basis_functions[i][node] of
+ * MsFEM_Grid.h:2926-2937 transposed). */
+int msfem_cells_get_order2_bases(msfem_cells_t c, double* bases, int on_device);
+
+/* The Order2 macro element matrices (FiniteElement_forMech_Poly::SolveLocalMatrix,
+ * MsFEM/MsFEM_Grid.h:34-171) from the cells' Order2 bases, each basis taken as its z component in
+ * all three components as the reference's macro basis functions return it (:2978-2979, :3038-3040);
+ * quadrature, micro-element lookup and D as msfem_cells_macro_matrices.
+ * K: [n_cells][27][27][3][3] doubles. */
+int msfem_cells_order2_macro_matrices(msfem_cells_t c, double* K, int on_device);
+
 /* Per-cell report of the last build (host arrays of n_cells, any may be NULL):
  * inner iterations, outer refinement steps and final relative residual of the volume
  * problems, and the worst relative residual of the cell's face problems.

@@ -93,6 +93,26 @@ class Cells:
         check(load().msfem_cells_get_bases(self.h, _p(out), 0), "cells_get_bases")
         return out
 
+    def build_order2(self, cell_vertex, precision=FP32_IR, tol=1e-8, maxiter=5000, threads=0):
+        """The 27 Order2 bases of every cell; cell_vertex [n_cells, 8]: the global macro vertex ids
+        of each cell's corners (they fix the order of the edge bases)."""
+        cv = _c(cell_vertex, np.int32)
+        if cv.shape != (self.n_cells, 8):
+            raise ValueError("cell_vertex must be [n_cells, 8]")
+        return check(load().msfem_cells_build_order2(self.h, _p(cv), precision, tol, maxiter, threads),
+                     "cells_build_order2")
+
+    def order2_bases(self):
+        out = np.empty((self.n_nodes, 27, 3))
+        check(load().msfem_cells_get_order2_bases(self.h, _p(out), 0), "cells_get_order2_bases")
+        return out
+
+    def order2_macro_matrices(self):
+        """[n_cells, 27, 27, 3, 3] Order2 macro element matrices of the current Order2 bases."""
+        K = np.empty((self.n_cells, 27, 27, 3, 3))
+        check(load().msfem_cells_order2_macro_matrices(self.h, _p(K), 0), "cells_order2_macro_matrices")
+        return K
+
     def set_bases(self, bases):
         """Replaces every cell's bases ([n_nodes, 8, 3])."""
         b = _c(bases, np.float64)

@@ -27,6 +27,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <utility>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -437,14 +438,17 @@ __device__ __forceinline__ void strain_column(const double* G, int a, double b[6
     }
 }
 
+// NB bases per cell ([node][NB][3]); ZREP: every component of basis I is its z component (the
+// Order2 macro bases, MsFEM_Grid.h:2978-2979)
+template <int NB, bool ZREP>
 __global__ void __launch_bounds__(256) k_macro_cells(const int64_t* __restrict__ tet_off, const int32_t* __restrict__ tets,
                                                      const double* __restrict__ xyz, const double* __restrict__ box,
                                                      const double* __restrict__ bases, const double* __restrict__ lame,
                                                      double* __restrict__ K, int* bad)
 {
     extern __shared__ double sm[];
-    double* sG = sm;                                 // [96][8][9]
-    double* sP = sG + kMacroQ * 72;                  // [96][3]
+    double* sG = sm;                                 // [96][NB][9]
+    double* sP = sG + kMacroQ * NB * 9;              // [96][3]
     double* sW = sP + kMacroQ * 3;                   // [96]
     int* sT = reinterpret_cast<int*>(sW + kMacroQ);  // [96]
     const int c = blockIdx.x, tid = threadIdx.x;
@@ -497,9 +501,9 @@ __global__ void __launch_bounds__(256) k_macro_cells(const int64_t* __restrict__
         }
     }
     __syncthreads();
-    for (int t = tid; t < kMacroQ * 8; t += blockDim.x) {
-        const int q = t / 8, I = t % 8;
-        double* out = sG + 72 * q + 9 * I;
+    for (int t = tid; t < kMacroQ * NB; t += blockDim.x) {
+        const int q = t / NB, I = t % NB;
+        double* out = sG + 9 * NB * q + 9 * I;
         if (sT[q] == 0x7fffffff) {
             atomicExch(bad, 1);
             for (int k = 0; k < 9; k++) out[k] = 0.0;
@@ -513,27 +517,27 @@ __global__ void __launch_bounds__(256) k_macro_cells(const int64_t* __restrict__
         for (int cc = 0; cc < 3; cc++)
             for (int d = 0; d < 3; d++) {
                 double g = 0.0;
-                for (int k = 0; k < 4; k++) g += bases[24 * (int64_t)v[k] + 3 * I + cc] * G.g[k][d];
+                for (int k = 0; k < 4; k++) g += bases[3 * NB * (int64_t)v[k] + 3 * I + (ZREP ? 2 : cc)] * G.g[k][d];
                 out[3 * cc + d] = g;
             }
     }
     __syncthreads();
     // D: lambda on the trace plus 2 mu on the normal strains, mu on the engineering shears
     const double lam = lame[0], mu = lame[1];
-    for (int t = tid; t < 576; t += blockDim.x) {
-        const int I = t / 72, J = (t / 9) % 8, r = (t / 3) % 3, cs = t % 3;
+    for (int t = tid; t < NB * NB * 9; t += blockDim.x) {
+        const int I = t / (9 * NB), J = (t / 9) % NB, r = (t / 3) % 3, cs = t % 3;
         double acc = 0.0;
         for (int q = 0; q < kMacroQ; q++) {
             double bi[6], bj[6];
-            strain_column(sG + 72 * q + 9 * I, cs, bi);
-            strain_column(sG + 72 * q + 9 * J, r, bj);
+            strain_column(sG + 9 * NB * q + 9 * I, cs, bi);
+            strain_column(sG + 9 * NB * q + 9 * J, r, bj);
             const double tr = bi[0] + bi[1] + bi[2];
             double v = 0.0;
             for (int k = 0; k < 3; k++) v += bj[k] * (lam * tr + 2.0 * mu * bi[k]);
             for (int k = 3; k < 6; k++) v += bj[k] * mu * bi[k];
             acc += sW[q] * v;
         }
-        K[576 * (int64_t)c + t] = acc;
+        K[NB * NB * 9 * (int64_t)c + t] = acc;
     }
 }
 
@@ -984,6 +988,406 @@ int cells_build(CellsHandle& h, int precision, double tol, int maxiter, int thre
     return 0;
 }
 
+// ---- MsFEM Order2 bases (Grid_forMech::CreateFunctionalSpaces, MsFEM_Grid.h:1001-3080): 27 per
+// cell, ordered vertex (8, the cell's vertex order) -> edge (12, ascending global edge id) ->
+// face (6, x0 x1 y0 y1 z0 z1) -> cell (1), :3045-3054.
+//   edges: every edge segment is material 0 (the reference reads the edge meshes out of its
+//     Salome face files, whose ReadFromSalomeDat leaves every material id 0, Library/Math.h:91-147),
+//     so the two linear edge problems are linear in arc length and the bubble problem (source of
+//     phi = 4 xi (1 - xi) (1,1,1), :1378-1400) is phi (1,1,1) at the nodes: P1 is nodally exact
+//     for a constant coefficient and load in 1-D;
+//   faces: 4 linear + 4 edge-bubble problems per face on material 0, no load (FEM_2D adds element
+//     loads only when it logs, FEM/FEM.h:4479-4490), one batch with R = 8; the face bubble is 0;
+//   volume: 8 linear problems without load and 19 bubble problems whose loads are the integrals
+//     of f . phi_I with the tetrahedron's 4-point rule (FEM/FEM_Grid.h:2521-2566), f the
+//     operator -[(lambda + mu) H (1,1,1) + mu tr(H) (1,1,1)] of the bubble's Hessian H
+//     (:2371-2480 edges, :2598-2700 faces, :2770-2830 cell) with the tetrahedron's own material,
+//     solved as 4 passes of 8 right-hand sides on the cell matrices.
+// For a box cell the reference's frames are the global axes up to sign, and every one of these
+// sources is unchanged by those signs, so the bubbles are written in global coordinates.
+
+// edge values at the interior edge nodes: eprof[node][0] = 1 - s (1 at the low end),
+// [1] = s (1 at the high end), [2] = 4 s (1 - s), s = arc length from the low end / edge length
+__global__ void k_o2_edges(int n_edges, int cap, const int32_t* __restrict__ edge_nodes,
+                           const int32_t* __restrict__ edge_len, const double* __restrict__ xyz,
+                           double* __restrict__ eprof)
+{
+    for (int eid = blockIdx.x * blockDim.x + threadIdx.x; eid < n_edges; eid += gridDim.x * blockDim.x) {
+        const int n = edge_len[eid];
+        if (n < 3) continue;
+        const int32_t* nodes = edge_nodes + (int64_t)eid * cap;
+        double total = 0.0;
+        for (int k = 0; k + 1 < n; k++) {
+            double L = 0.0;
+            for (int q = 0; q < 3; q++) {
+                const double u = xyz[3 * (int64_t)nodes[k + 1] + q] - xyz[3 * (int64_t)nodes[k] + q];
+                L += u * u;
+            }
+            total += sqrt(L);
+        }
+        double acc = 0.0;
+        for (int k = 1; k + 1 < n; k++) {
+            double L = 0.0;
+            for (int q = 0; q < 3; q++) {
+                const double u = xyz[3 * (int64_t)nodes[k] + q] - xyz[3 * (int64_t)nodes[k - 1] + q];
+                L += u * u;
+            }
+            acc += sqrt(L);
+            const double s = acc / total;
+            double* o = eprof + 3 * (int64_t)nodes[k];
+            o[0] = 1.0 - s;
+            o[1] = s;
+            o[2] = 4.0 * s * (1.0 - s);
+        }
+    }
+}
+
+// index of edge e among the 4 edges of face f (ascending e), or -1
+__host__ __device__ __forceinline__ int face_edge_index(int f, int e)
+{
+    int k = 0;
+    for (int q = 0; q < 12; q++) {
+        int axis, fa, fb, vl, vh;
+        edge_info(q, axis, fa, fb, vl, vh);
+        if (fa != f && fb != f) continue;
+        if (q == e) return k;
+        k++;
+    }
+    return -1;
+}
+
+// the edge of a non-corner boundary node that lies on face f (its other face g), or -1
+__device__ __forceinline__ int node_edge(int m, int f)
+{
+    const int rest = m & ~(1 << f);
+    if (__popc(m) != 2 || !rest) return -1;
+    const int g = __ffs(rest) - 1;
+    for (int e = 0; e < 12; e++) {
+        int axis, fa, fb, vl, vh;
+        edge_info(e, axis, fa, fb, vl, vh);
+        if ((fa == f && fb == g) || (fa == g && fb == f)) return e;
+    }
+    return -1;
+}
+
+// Dirichlet data of the Order2 face problems: fx[face node][8][3]; slots 0-3 the linear problems
+// of the face's vertices (increasing b), slots 4-7 the bubble problems of its edges (ascending e)
+__global__ void k_o2_face_dirichlet(int64_t n_fnodes, const int32_t* __restrict__ fcell_node,
+                                    const uint8_t* __restrict__ ffixed, const int64_t* __restrict__ fsys_node_off,
+                                    int n_fsys, const int32_t* __restrict__ mask, const int32_t* __restrict__ vert,
+                                    const double* __restrict__ eprof, double* __restrict__ fx)
+{
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n_fnodes; k += (int64_t)gridDim.x * blockDim.x) {
+        double* o = fx + 24 * k;
+        for (int q = 0; q < 24; q++) o[q] = 0.0;
+        if (!ffixed[k]) continue;
+        int lo = 0, hi = n_fsys - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (fsys_node_off[mid] <= k) lo = mid;
+            else hi = mid - 1;
+        }
+        const int c = lo / 6, f = lo % 6;
+        const int64_t i = fcell_node[k];
+        const int m = mask[i];
+        const bool corner = __popc(m) == 3;
+        const int e = corner ? -1 : node_edge(m, f);
+        for (int j = 0; j < 4; j++) {
+            const int v = face_vertex(f, j);
+            double val = 0.0;
+            if (corner) {
+                val = (i == vert[8 * c + v]) ? 1.0 : 0.0;
+            } else if (e >= 0) {
+                int axis, fa, fb, vl, vh;
+                edge_info(e, axis, fa, fb, vl, vh);
+                if (v == vl) val = eprof[3 * i];
+                else if (v == vh) val = eprof[3 * i + 1];
+            }
+            for (int q = 0; q < 3; q++) o[3 * j + q] = val;
+        }
+        if (e >= 0) {
+            const int j = 4 + face_edge_index(f, e);
+            for (int q = 0; q < 3; q++) o[3 * j + q] = eprof[3 * i + 2];
+        }
+    }
+}
+
+__device__ __forceinline__ int cell_of_node(const int64_t* __restrict__ node_off, int n_cells, int64_t i)
+{
+    int lo = 0, hi = n_cells - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (node_off[mid] <= i) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+struct O2Slots {
+    int dof[8];  // the basis each right-hand side of a volume pass solves for
+};
+
+// Dirichlet data of an Order2 volume pass: x[node][8][3] (boundary nodes; the rest 0)
+__global__ void k_o2_volume_dirichlet(int64_t n_nodes, const int64_t* __restrict__ node_off, int n_cells,
+                                     const int32_t* __restrict__ mask, const int32_t* __restrict__ fidx_all,
+                                     const int32_t* __restrict__ perm, const double* __restrict__ fx, O2Slots sl,
+                                     double* __restrict__ x)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_nodes; i += (int64_t)gridDim.x * blockDim.x) {
+        const int m = mask[i];
+        double* o = x + 24 * i;
+        for (int q = 0; q < 24; q++) o[q] = 0.0;
+        if (!m) continue;
+        const int c = cell_of_node(node_off, n_cells, i);
+        for (int s = 0; s < 8; s++) {
+            const int d = sl.dof[s];
+            int common = 0, j = -1;
+            if (d < 8) {
+                common = m & vertex_face_mask(d);
+            } else if (d < 20) {
+                int axis, fa, fb, vl, vh;
+                edge_info(perm[12 * c + d - 8], axis, fa, fb, vl, vh);
+                common = m & ((1 << fa) | (1 << fb));
+            }
+            if (!common) continue;
+            const int f = __ffs(common) - 1;  // the lowest face through both
+            j = d < 8 ? face_vertex_index(f, d) : 4 + face_edge_index(f, perm[12 * c + d - 8]);
+            const int64_t k = fidx_all[(int64_t)f * n_nodes + i];
+            for (int q = 0; q < 3; q++) o[3 * s + q] = fx[24 * k + 3 * j + q];
+        }
+    }
+}
+
+// (phi, phi', phi'') of one axis factor at xi: the bubble 4 xi (1 - xi), or the linear function
+// that is 1 on side `side` (0: xi = 0) and 0 on the other
+__device__ __forceinline__ void o2_factor(bool bubble, int side, double xi, double h, double out[3])
+{
+    if (bubble) {
+        out[0] = -4.0 * xi * xi + 4.0 * xi;
+        out[1] = -8.0 / h * xi + 4.0 / h;
+        out[2] = -8.0 / (h * h);
+    } else if (side == 0) {
+        out[0] = 1.0 - xi;
+        out[1] = -1.0 / h;
+        out[2] = 0.0;
+    } else {
+        out[0] = xi;
+        out[1] = 1.0 / h;
+        out[2] = 0.0;
+    }
+}
+
+// the source of bubble d (8..26) at x: -[(lambda + mu) H (1,1,1) + mu tr(H) (1,1,1)]
+__device__ void o2_source(int d, int e, const double* bx, const double x[3], double lam, double mu, double f[3])
+{
+    bool bub[3] = {true, true, true};
+    int side[3] = {0, 0, 0};
+    if (d < 20) {
+        int axis, fa, fb, vl, vh;
+        edge_info(e, axis, fa, fb, vl, vh);
+        bub[fa >> 1] = false;
+        side[fa >> 1] = fa & 1;
+        bub[fb >> 1] = false;
+        side[fb >> 1] = fb & 1;
+    } else if (d < 26) {
+        const int face = d - 20;
+        bub[face >> 1] = false;
+        side[face >> 1] = face & 1;
+    }
+    double F[3][3];
+    for (int a = 0; a < 3; a++) {
+        const double h = bx[2 * a + 1] - bx[2 * a];
+        o2_factor(bub[a], side[a], (x[a] - bx[2 * a]) / h, h, F[a]);
+    }
+    double H[3][3];
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) {
+            double v = 1.0;
+            for (int k = 0; k < 3; k++) v *= (a == b) ? (k == a ? F[k][2] : F[k][0]) : (k == a || k == b ? F[k][1] : F[k][0]);
+            H[a][b] = v;
+        }
+    const double tr = H[0][0] + H[1][1] + H[2][2];
+    for (int a = 0; a < 3; a++) f[a] = -((lam + mu) * (H[a][0] + H[a][1] + H[a][2]) + mu * tr);
+}
+
+// loads of an Order2 volume pass at every node, gathered over the node's tetrahedra in element
+// order (the contributions of its diagonal block): rhs[node][8][3]
+__global__ void k_o2_loads(int64_t n_nodes, const int64_t* __restrict__ node_off, int n_cells,
+                           const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
+                           const int64_t* __restrict__ cstart, const uint32_t* __restrict__ contrib,
+                           const int32_t* __restrict__ elems, const int32_t* __restrict__ emat,
+                           const double* __restrict__ lame, int n_mat, const double* __restrict__ xyz,
+                           const double* __restrict__ box, const int32_t* __restrict__ perm, O2Slots sl,
+                           double* __restrict__ rhs)
+{
+    const double u = (5.0 - sqrt(5.0)) / 20.0, vv = 1.0 - 3.0 * u;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_nodes; i += (int64_t)gridDim.x * blockDim.x) {
+        double acc[8][3];
+        for (int s = 0; s < 8; s++)
+            for (int q = 0; q < 3; q++) acc[s][q] = 0.0;
+        const int c = cell_of_node(node_off, n_cells, i);
+        const double* bx = box + 6 * c;
+        int64_t kd = -1;
+        for (int64_t k = row_ptr[i]; k < row_ptr[i + 1]; k++)
+            if (col[k] == i) kd = k;
+        if (kd >= 0)
+            for (int64_t t = cstart[kd]; t < cstart[kd + 1]; t++) {
+                const uint32_t tag = contrib[t];
+                const int64_t e = tag >> 4;
+                const int a = (tag >> 2) & 3;
+                int v[4];
+                for (int k = 0; k < 4; k++) v[k] = elems[4 * e + k];
+                TetGeom G;
+                tet_geometry(xyz, v, G);
+                const int mt = emat[e];
+                if (mt < 0 || mt >= n_mat) continue;  // rejected when the cell matrices were assembled
+                const double lam = lame[2 * mt], mu = lame[2 * mt + 1];
+                for (int q = 0; q < 4; q++) {
+                    double bar[4];
+                    for (int k = 0; k < 4; k++) bar[k] = (k == q) ? vv : u;
+                    double x[3] = {0, 0, 0};
+                    for (int k = 0; k < 4; k++)
+                        for (int r = 0; r < 3; r++) x[r] += bar[k] * xyz[3 * (int64_t)v[k] + r];
+                    const double w = 0.25 * G.vol * bar[a];
+                    for (int s = 0; s < 8; s++) {
+                        const int d = sl.dof[s];
+                        if (d < 8) continue;
+                        double f[3];
+                        o2_source(d, d < 20 ? perm[12 * c + d - 8] : -1, bx, x, lam, mu, f);
+                        for (int r = 0; r < 3; r++) acc[s][r] += w * f[r];
+                    }
+                }
+            }
+        double* o = rhs + 24 * i;
+        for (int s = 0; s < 8; s++)
+            for (int r = 0; r < 3; r++) o[3 * s + r] = acc[s][r];
+    }
+}
+
+__global__ void k_o2_scatter(int64_t n_nodes, const double* __restrict__ x, O2Slots sl, int n_real,
+                             double* __restrict__ bases)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_nodes; i += (int64_t)gridDim.x * blockDim.x)
+        for (int s = 0; s < n_real; s++)
+            for (int q = 0; q < 3; q++) bases[81 * i + 3 * sl.dof[s] + q] = x[24 * i + 3 * s + q];
+}
+
+int cells_build_order2(CellsHandle& h, const int32_t* cell_vertex, int precision, double tol, int maxiter, int threads)
+{
+    cudaStream_t st = h.stream;
+    BatchSys& F = h.faces;
+    BatchSys& F2 = h.faces2;
+    BatchSys& V = h.vols;
+    // DOF slot k of the edge bubbles -> local edge: ascending (lower, higher) global vertex pair
+    {
+        std::vector<int32_t> gv(8 * (size_t)h.n_cells), perm(12 * (size_t)h.n_cells);
+        MSFEM_CK(cudaMemcpyAsync(gv.data(), cell_vertex, sizeof(int32_t) * gv.size(), cudaMemcpyDefault, st));
+        MSFEM_CK(cudaStreamSynchronize(st));
+        for (int c = 0; c < h.n_cells; c++) {
+            const int32_t* g = gv.data() + 8 * c;
+            for (int a = 0; a < 8; a++)
+                for (int b = a + 1; b < 8; b++)
+                    if (g[a] == g[b]) {
+                        set_error("msfem_cells_build_order2: cell %d repeats the global vertex %d", c, g[a]);
+                        return MSFEM_ERR_ARGUMENT;
+                    }
+            int idx[12];
+            for (int e = 0; e < 12; e++) idx[e] = e;
+            auto key = [&](int e) {
+                int axis, fa, fb, vl, vh;
+                edge_info(e, axis, fa, fb, vl, vh);
+                return std::make_pair(std::min(g[vl], g[vh]), std::max(g[vl], g[vh]));
+            };
+            std::sort(idx, idx + 12, [&](int p, int q) { return key(p) < key(q); });
+            for (int k = 0; k < 12; k++) perm[12 * (size_t)c + k] = idx[k];
+        }
+        MSFEM_TRY(copy_in(st, h.edge_perm, perm.data(), perm.size()));
+    }
+    if (!h.faces2_ready) {
+        F2.dim = 2;
+        F2.k1 = 3;
+        F2.R = 8;
+        F2.n_sys = F.n_sys;
+        F2.stream = st;
+        F2.h_node_off = F.h_node_off;
+        F2.h_elem_off = F.h_elem_off;
+        F2.n_nodes = F.n_nodes;
+        F2.n_elems = F.n_elems;
+        MSFEM_TRY(copy_in(st, F2.node_off, F.h_node_off.data(), F.n_sys + 1));
+        MSFEM_TRY(copy_in(st, F2.elem_off, F.h_elem_off.data(), F.n_sys + 1));
+        MSFEM_TRY(F2.elems.alloc(3 * F.n_elems));
+        MSFEM_CK(cudaMemcpyAsync(F2.elems.p, F.elems.p, sizeof(int32_t) * 3 * F.n_elems, cudaMemcpyDeviceToDevice, st));
+        MSFEM_TRY(F2.fixed.alloc(F.n_nodes));
+        MSFEM_CK(cudaMemcpyAsync(F2.fixed.p, F.fixed.p, F.n_nodes, cudaMemcpyDeviceToDevice, st));
+        MSFEM_TRY(F2.emat.alloc(F.n_elems));
+        MSFEM_CK(cudaMemsetAsync(F2.emat.p, 0, sizeof(int32_t) * F.n_elems, st));
+        MSFEM_TRY(batch_build_pattern(F2, h.fxyz.p));
+        h.faces2_ready = true;
+    }
+    MSFEM_CK(cudaEventRecord(h.ev[0], st));
+    MSFEM_TRY(batch_assemble(F2, h.fxyz.p, h.lame.p, h.n_mat));
+    if (!h.vols_assembled) {
+        MSFEM_TRY(batch_assemble(V, h.xyz.p, h.lame.p, h.n_mat));
+        h.vols_assembled = true;
+    }
+    MSFEM_CK(cudaEventRecord(h.ev[1], st));
+    MSFEM_TRY(h.eprof2.alloc(3 * (size_t)h.n_nodes));
+    MSFEM_CK(cudaMemsetAsync(h.eprof2.p, 0, sizeof(double) * 3 * h.n_nodes, st));
+    const int n_edges = 12 * h.n_cells;
+    k_o2_edges<<<blocks_for(n_edges, 128), 128, 0, st>>>(n_edges, h.cap, h.edge_nodes.p, h.edge_len.p, h.xyz.p,
+                                                         h.eprof2.p);
+    MSFEM_TRY(h.fx2.alloc(24 * (size_t)F2.n_nodes));
+    k_o2_face_dirichlet<<<blocks_for(F2.n_nodes), 256, 0, st>>>(F2.n_nodes, h.fcell_node.p, F2.fixed.p, F2.node_off.p,
+                                                                F2.n_sys, h.mask.p, h.vert.p, h.eprof2.p, h.fx2.p);
+    MSFEM_CK(cudaGetLastError());
+    MSFEM_CK(cudaEventRecord(h.ev[2], st));
+    MSFEM_TRY(batch_solve(F2, h.fx2.p, precision, tol, maxiter, threads));
+    int nf = 0;
+    MSFEM_TRY(batch_finish(F2, &nf, tol, nullptr));
+    MSFEM_CK(cudaEventRecord(h.ev[3], st));
+    MSFEM_TRY(h.x2.alloc(24 * (size_t)h.n_nodes));
+    MSFEM_TRY(h.rhs2.alloc(24 * (size_t)h.n_nodes));
+    MSFEM_TRY(h.bases2.alloc(81 * (size_t)h.n_nodes));
+    // four passes of 8 right-hand sides: vertices; edges 0-7; edges 8-11 + faces 0-3; faces 4-5 +
+    // the cell bubble (repeated to fill the pass)
+    const O2Slots pass[4] = {{{0, 1, 2, 3, 4, 5, 6, 7}},
+                             {{8, 9, 10, 11, 12, 13, 14, 15}},
+                             {{16, 17, 18, 19, 20, 21, 22, 23}},
+                             {{24, 25, 26, 26, 26, 26, 26, 26}}};
+    const int n_real[4] = {8, 8, 8, 3};
+    int nv = 0;
+    for (int p = 0; p < 4; p++) {
+        k_o2_volume_dirichlet<<<blocks_for(h.n_nodes), 256, 0, st>>>(h.n_nodes, h.node_off.p, h.n_cells, h.mask.p,
+                                                                     h.fidx.p, h.edge_perm.p, h.fx2.p, pass[p], h.x2.p);
+        MSFEM_CK(cudaGetLastError());
+        if (p > 0) {
+            k_o2_loads<<<blocks_for(h.n_nodes, 128), 128, 0, st>>>(h.n_nodes, h.node_off.p, h.n_cells, V.row_ptr.p,
+                                                                  V.col.p, V.cstart.p, V.contrib.p, V.elems.p, V.emat.p,
+                                                                  h.lame.p, h.n_mat, h.xyz.p, h.box.p, h.edge_perm.p, pass[p],
+                                                                  h.rhs2.p);
+            MSFEM_CK(cudaGetLastError());
+            V.rhs = h.rhs2.p;
+        }
+        const int rc = batch_solve(V, h.x2.p, precision, tol, maxiter, threads);
+        V.rhs = nullptr;
+        MSFEM_TRY(rc);
+        int bad = 0;
+        MSFEM_TRY(batch_finish(V, &bad, tol, nullptr));
+        nv += bad;
+        k_o2_scatter<<<blocks_for(h.n_nodes), 256, 0, st>>>(h.n_nodes, h.x2.p, pass[p], n_real[p], h.bases2.p);
+        MSFEM_CK(cudaGetLastError());
+    }
+    MSFEM_CK(cudaEventRecord(h.ev[4], st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    for (int k = 0; k < 4; k++) MSFEM_CK(cudaEventElapsedTime(&h.ms2[k], h.ev[k], h.ev[k + 1]));
+    h.order2_built = true;
+    if (nf || nv) {
+        set_error("msfem_cells_build_order2: %d face and %d volume problems missed the tolerance", nf, nv);
+        return MSFEM_NOT_CONVERGED;
+    }
+    return 0;
+}
+
 }  // namespace
 }  // namespace msfem
 
@@ -1163,6 +1567,33 @@ int msfem_cells_get_bases(msfem_cells_t h, double* bases, int on_device)
     return MSFEM_OK;
 }
 
+int msfem_cells_build_order2(msfem_cells_t h, const int32_t* cell_vertex, int precision, double tol, int maxiter,
+                             int threads)
+{
+    using namespace msfem;
+    if (!h || !cell_vertex || maxiter <= 0 || !(tol > 0.0) ||
+        (precision != MSFEM_FP64 && precision != MSFEM_FP32_IR)) {
+        set_error("msfem_cells_build_order2: bad arguments");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    MSFEM_CK(cudaSetDevice(h->device));
+    return cells_build_order2(*h, cell_vertex, precision, tol, maxiter, threads);
+}
+
+int msfem_cells_get_order2_bases(msfem_cells_t h, double* bases, int on_device)
+{
+    using namespace msfem;
+    if (!h || !bases || !h->order2_built) {
+        set_error("msfem_cells_get_order2_bases: bad arguments or no Order2 bases built");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    MSFEM_CK(cudaSetDevice(h->device));
+    MSFEM_CK(cudaMemcpyAsync(bases, h->bases2.p, sizeof(double) * 81 * h->n_nodes,
+                             on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, h->stream));
+    MSFEM_CK(cudaStreamSynchronize(h->stream));
+    return MSFEM_OK;
+}
+
 int msfem_cells_set_bases(msfem_cells_t h, const double* bases, int on_device)
 {
     using namespace msfem;
@@ -1273,10 +1704,10 @@ int msfem_cells_macro_matrices(msfem_cells_t h, double* K, int on_device)
         out = dK.p;
     }
     const size_t smem = sizeof(double) * (96 * 72 + 96 * 3 + 96) + sizeof(int) * 96;
-    MSFEM_CK(cudaFuncSetAttribute(k_macro_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    MSFEM_CK(cudaFuncSetAttribute(k_macro_cells<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     MSFEM_CK(cudaMemsetAsync(h->flag.p, 0, sizeof(int), st));
-    k_macro_cells<<<h->n_cells, 256, smem, st>>>(h->tet_off.p, h->vols.elems.p, h->xyz.p, h->box.p, h->bx.p, h->lame.p,
-                                                 out, h->flag.p);
+    k_macro_cells<8, false><<<h->n_cells, 256, smem, st>>>(h->tet_off.p, h->vols.elems.p, h->xyz.p, h->box.p, h->bx.p,
+                                                           h->lame.p, out, h->flag.p);
     MSFEM_CK(cudaGetLastError());
     if (!on_device)
         MSFEM_CK(cudaMemcpyAsync(K, dK.p, sizeof(double) * 576 * h->n_cells, cudaMemcpyDeviceToHost, st));
@@ -1285,6 +1716,40 @@ int msfem_cells_macro_matrices(msfem_cells_t h, double* K, int on_device)
     MSFEM_CK(cudaStreamSynchronize(st));
     if (bad) {
         set_error("msfem_cells_macro_matrices: a quadrature point lies in no tetrahedron of its cell");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    return MSFEM_OK;
+}
+
+int msfem_cells_order2_macro_matrices(msfem_cells_t h, double* K, int on_device)
+{
+    using namespace msfem;
+    if (!h || !K || !h->order2_built) {
+        set_error("msfem_cells_order2_macro_matrices: bad arguments or no Order2 bases built");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    MSFEM_CK(cudaSetDevice(h->device));
+    cudaStream_t st = h->stream;
+    constexpr size_t per = 27 * 27 * 9;
+    DBuf<double> dK;
+    double* out = K;
+    if (!on_device) {
+        MSFEM_TRY(dK.alloc(per * (size_t)h->n_cells));
+        out = dK.p;
+    }
+    const size_t smem = sizeof(double) * (96 * 27 * 9 + 96 * 3 + 96) + sizeof(int) * 96;
+    MSFEM_CK(cudaFuncSetAttribute(k_macro_cells<27, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    MSFEM_CK(cudaMemsetAsync(h->flag.p, 0, sizeof(int), st));
+    k_macro_cells<27, true><<<h->n_cells, 256, smem, st>>>(h->tet_off.p, h->vols.elems.p, h->xyz.p, h->box.p,
+                                                           h->bases2.p, h->lame.p, out, h->flag.p);
+    MSFEM_CK(cudaGetLastError());
+    if (!on_device)
+        MSFEM_CK(cudaMemcpyAsync(K, dK.p, sizeof(double) * per * h->n_cells, cudaMemcpyDeviceToHost, st));
+    int bad = 0;
+    MSFEM_CK(cudaMemcpyAsync(&bad, h->flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    if (bad) {
+        set_error("msfem_cells_order2_macro_matrices: a quadrature point lies in no tetrahedron of its cell");
         return MSFEM_ERR_ARGUMENT;
     }
     return MSFEM_OK;

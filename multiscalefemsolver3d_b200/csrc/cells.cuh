@@ -39,6 +39,14 @@ struct CellsHandle {
     bool vols_assembled = false;  // volume problem matrices hold the current materials
     DBuf<int32_t> edge_nodes, edge_len, seg_tri;
     DBuf<int> flag;
+    // Order2 (27 bases per cell): face problems on material 0 with 8 right-hand sides, the edge
+    // values, the per-cell edge order (DOF slot -> local edge) and the bases [node][27][3]
+    BatchSys faces2;
+    bool faces2_ready = false;
+    DBuf<double> eprof2, fx2, x2, rhs2, bases2;
+    DBuf<int32_t> edge_perm;
+    bool order2_built = false;
+    float ms2[4] = {0, 0, 0, 0};
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     float ms[4] = {0, 0, 0, 0};
     ~CellsHandle()

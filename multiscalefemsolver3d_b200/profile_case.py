@@ -19,6 +19,11 @@ the multiplicative cycle and FP64 MINRES to 1e-8.
 runs the batched Order1 cell bases of n^3 macro cells of the 16^3-cell workload's kind (per-cell
 resolution from {8, 12, 16, 20}, ellipsoidal inclusions E 1:50): edges, faces, volumes.
 
+    python -m multiscalefemsolver3d_b200.profile_case --order2 8
+
+runs the batched Order2 cell bases (27 per cell) of the same n^3 cells, after their Order1 bases
+for comparison: face problems (R = 8), then the four volume passes (R = 8 each).
+
     python -m multiscalefemsolver3d_b200.profile_case --net 512
 
 runs the learned coarse space's forward pass over 512 sphere cells twice: layers 1-3 on the
@@ -39,8 +44,11 @@ def main():
     ap.add_argument("--twolevel", action="store_true", help="two-level elasticity solve at n^3")
     ap.add_argument("--cells", type=int, default=0, help="batched cell bases of cells^3 macro cells")
     ap.add_argument("--net", type=int, default=0, help="network forward passes over this many cells")
+    ap.add_argument("--order2", type=int, default=0, help="batched Order2 bases of order2^3 macro cells")
     a = ap.parse_args()
     from . import fem, meshgen
+    if a.order2:
+        return order2_case(a.order2)
     if a.net:
         return net_case(a.net)
     if a.cells:
@@ -79,6 +87,29 @@ def cells_case(nc):
     rc = C.build_bases(FP32_IR, 1e-8)
     r = C.report()
     print(json.dumps({"cells": cm.n_cells, "nodes": C.n_nodes, "rc": rc, "ms": r["ms"]}, default=str))
+    C.close()
+
+
+def order2_case(nc):
+    import time
+
+    import numpy as np
+
+    from . import meshgen
+    from .cells import FP32_IR, Cells
+    cm = meshgen.msfem_cells(n_coarse=nc, m_choices=(8, 12, 16, 20), seed=3, max_inclusions=3, contrast=50.0)
+    cv = np.array([[(c % nc + (b & 1)) + (nc + 1) * ((c // nc % nc + (b >> 1 & 1)) + (nc + 1) * (c // nc ** 2 + (b >> 2 & 1)))
+                    for b in range(8)] for c in range(nc ** 3)], dtype=np.int32)
+    C = Cells(cm)
+    t0 = time.perf_counter()
+    rc1 = C.build_bases(FP32_IR, 1e-8)
+    t1 = time.perf_counter()
+    rc2 = C.build_order2(cv, FP32_IR, 1e-8)
+    t2 = time.perf_counter()
+    C.build_order2(cv, FP32_IR, 1e-8)
+    t3 = time.perf_counter()
+    print(json.dumps({"cells": cm.n_cells, "nodes": C.n_nodes, "rc_order1": rc1, "rc_order2": rc2,
+                      "s_order1_first": t1 - t0, "s_order2_first": t2 - t1, "s_order2_again": t3 - t2}))
     C.close()
 
 

@@ -432,3 +432,27 @@ def run_reference(workdir, vertex_xyz, cell_vertex, cells, matrices=True, timeou
         res["bases"].append(np.stack([np.loadtxt(os.path.join(sub, f"BasisFunction_{b}.txt")).reshape(-1, 3)
                                       for b in range(27)], axis=1))
     return res
+
+
+def graded_cells(nc, m, grade, seed=1, contrast=10.0):
+    """(macro vertex xyz, cell_vertex [nc^3, 8], CellMeshes): nc^3 box cells of the unit cube
+    (meshgen.msfem_cells, ellipsoid inclusions), each cell's fine nodes moved along every axis by
+    u -> u + grade (1 + 0.3 axis) sin(2 pi u) / (2 pi) in cell units (graded, non-uniform
+    segments; the cell's faces and edges stay in place).  Graded edges keep the reference's edge
+    solves from meeting MIN_RESIDUAL on their first pass."""
+    from multiscalefemsolver3d_b200 import meshgen
+    cm = meshgen.msfem_cells(n_coarse=nc, m_choices=(m,), seed=seed, contrast=contrast)
+    for c in range(cm.n_cells):
+        a, b = cm.node_off[c], cm.node_off[c + 1]
+        for ax in range(3):
+            lo, hi = cm.box[c][2 * ax], cm.box[c][2 * ax + 1]
+            u = (cm.xyz[a:b, ax] - lo) / (hi - lo)
+            g = u + grade * (1 + 0.3 * ax) * np.sin(2 * np.pi * u) / (2 * np.pi)
+            g = np.where(np.abs(u) < 1e-14, 0.0, np.where(np.abs(u - 1) < 1e-14, 1.0, g))
+            cm.xyz[a:b, ax] = lo + (hi - lo) * g
+    s = np.arange(nc + 1) / nc
+    kk, jj, ii = np.meshgrid(s, s, s, indexing="ij")
+    vxyz = np.stack([ii.ravel(), jj.ravel(), kk.ravel()], axis=1)
+    cv = np.array([[(c % nc + (b & 1)) + (nc + 1) * ((c // nc % nc + (b >> 1 & 1)) + (nc + 1) * (c // nc ** 2 + (b >> 2 & 1)))
+                    for b in range(8)] for c in range(nc ** 3)])
+    return vxyz, cv, cm

@@ -7,38 +7,16 @@ import os
 import numpy as np
 import pytest
 
-from multiscalefemsolver3d_b200 import meshgen
 from oracle import order2 as o2
 
 pytestmark = pytest.mark.skipif(not os.path.exists(o2.ORDER2_REF),
                                 reason="oracle/_ref/order2_ref not built (make -C oracle ref)")
 
 
-def grid_cells(nc, m, grade, seed=1, contrast=10.0):
-    """nc^3 box cells of the unit cube (meshgen.msfem_cells, ellipsoid inclusions), each cell's
-    fine nodes moved along every axis by u -> u + grade (1 + 0.3 axis) sin(2 pi u) / (2 pi) in
-    cell units (graded, non-uniform segments; the cell's faces and edges stay in place)."""
-    cm = meshgen.msfem_cells(n_coarse=nc, m_choices=(m,), seed=seed, contrast=contrast)
-    for c in range(cm.n_cells):
-        a, b = cm.node_off[c], cm.node_off[c + 1]
-        for ax in range(3):
-            lo, hi = cm.box[c][2 * ax], cm.box[c][2 * ax + 1]
-            u = (cm.xyz[a:b, ax] - lo) / (hi - lo)
-            g = u + grade * (1 + 0.3 * ax) * np.sin(2 * np.pi * u) / (2 * np.pi)
-            g = np.where(np.abs(u) < 1e-14, 0.0, np.where(np.abs(u - 1) < 1e-14, 1.0, g))
-            cm.xyz[a:b, ax] = lo + (hi - lo) * g
-    s = np.arange(nc + 1) / nc
-    kk, jj, ii = np.meshgrid(s, s, s, indexing="ij")
-    vxyz = np.stack([ii.ravel(), jj.ravel(), kk.ravel()], axis=1)
-    cv = np.array([[(c % nc + (b & 1)) + (nc + 1) * ((c // nc % nc + (b >> 1 & 1)) + (nc + 1) * (c // nc ** 2 + (b >> 2 & 1)))
-                    for b in range(8)] for c in range(nc ** 3)])
-    return vxyz, cv, cm
-
-
 def test_order2_bases_and_macro_matrix_match_reference(tmp_path):
     """A graded 8^3 cell with inclusions (E 1:10): the 27 bases within 1e-11 of the reference's
     BasisFunction files, the 81 x 81 macro element matrix within 1e-11 of its SolveLocalMatrix."""
-    vxyz, cv, cm = grid_cells(1, 8, 0.5)
+    vxyz, cv, cm = o2.graded_cells(1, 8, 0.5)
     R = o2.run_reference(str(tmp_path), vxyz, cv, cm)
     xyz, tets, mat, box = cm.cell(0)
     assert 0 < mat.sum() < mat.size
@@ -62,7 +40,7 @@ def test_order2_bases_and_macro_matrix_match_reference(tmp_path):
 def test_order2_topology_and_dof_numbering(tmp_path):
     """2 x 2 x 2 cells: edges, faces, each face's edges and each cell's 27 DOF ids as the
     reference's CreateTopology and CreateFunctionalSpaces number them."""
-    vxyz, cv, cm = grid_cells(2, 1, 0.0)
+    vxyz, cv, cm = o2.graded_cells(2, 1, 0.0)
     R = o2.run_reference(str(tmp_path), vxyz, cv, cm, matrices=False)
     edges, faces, cell_faces, dofs = o2.macro_topology(cv)
     assert list(R["n"]) == [8, 27, len(edges), len(faces), 27 + len(edges) + len(faces) + 8]
@@ -84,7 +62,7 @@ def test_reference_loses_uniform_edge_solutions(tmp_path):
     pass and the restart loop returns the initial guess (FEM/FEM.h:3704-3771): its vertex bases
     are 0 inside the cell edges, where the converged edge solution is linear.  The restatement
     keeps the converged solution."""
-    vxyz, cv, cm = grid_cells(1, 3, 0.0)
+    vxyz, cv, cm = o2.graded_cells(1, 3, 0.0)
     R = o2.run_reference(str(tmp_path), vxyz, cv, cm, matrices=False)
     xyz, tets, mat, box = cm.cell(0)
     ours = o2.order2_bases(xyz, tets, mat, box, cm.E, cm.nu, cv[0])
