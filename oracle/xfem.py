@@ -70,3 +70,29 @@ def solve_dirichlet(A, nodes, values):
     rhs = -A[free][:, fixed] @ x[fixed]
     x[free] = spl.spsolve(A[free][:, free].tocsc(), rhs)
     return x
+
+
+def solve_dirichlet_gmres(A, nodes, values, tol=1e-8, restart=50, maxiter=200000):
+    """The same eliminated system solved by restarted GMRES(restart) with Jacobi preconditioning
+    (scipy), to ||r|| <= tol ||b|| of the eliminated system; returns (x, iterations)."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spl
+    n = A.shape[0]
+    x = np.zeros(n)
+    fixed = np.zeros(n, bool)
+    for v, val in zip(nodes, values):
+        x[v] = val
+        fixed[v] = True
+    free = ~fixed
+    A = A.tocsr()
+    Aff = A[free][:, free].tocsr()
+    rhs = -A[free][:, fixed] @ x[fixed]
+    M = sp.diags(1.0 / Aff.diagonal())
+    count = [0]
+
+    def cb(_):
+        count[0] += 1
+    y, info = spl.gmres(Aff, rhs, M=M, rtol=tol, atol=0.0, restart=restart, maxiter=maxiter,
+                        callback=cb, callback_type="pr_norm")
+    x[free] = y
+    return x, count[0]
