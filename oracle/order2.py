@@ -393,11 +393,13 @@ def macro_topology(cell_vertex):
 ORDER2_REF = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_ref", "order2_ref")
 
 
-def run_reference(workdir, vertex_xyz, cell_vertex, cells, matrices=True, timeout=1200):
+def run_reference(workdir, vertex_xyz, cell_vertex, cells, matrices=True, timeout=1200, groups=None,
+                  min_residual=1e-13):
     """Writes the macro mesh and cell directories under workdir (meshio writers), runs the
     reference's Order2 construction there and returns {"n": [ne, nv, n_edges, n_faces, n_dofs],
     "edges", "faces" (first-reached (id, n, edge ids...) records), "cell_dofs" [nc, 27],
-    "cell_faces" [nc, 6], "bases" [per cell: (n_nodes, 27, 3)], "K" [per cell: (81, 81)]}."""
+    "cell_faces" [nc, 6], "bases" [per cell: (n_nodes, 27, 3)], "K" [per cell: (81, 81)],
+    "solution" [n_dofs, 3] (groups given: the whole Order2 driver with those Dirichlet groups)}."""
     import subprocess
 
     from multiscalefemsolver3d_b200 import meshio
@@ -409,6 +411,14 @@ def run_reference(workdir, vertex_xyz, cell_vertex, cells, matrices=True, timeou
         args += [repr(float(e)), repr(float(n_))]
     if matrices:
         args.append("--matrices")
+    if groups is not None:
+        bc = os.path.join(workdir, "dirichlet.txt")
+        with open(bc, "w") as fb:
+            fb.write(f"{len(groups)}\n")
+            for verts, value, take in groups:
+                fb.write(" ".join(str(int(t)) for t in take) + " " + " ".join(repr(float(v)) for v in value) +
+                         f" {len(verts)} " + " ".join(str(int(v)) for v in verts) + "\n")
+        args += ["--driver", bc, repr(float(min_residual))]
     r = subprocess.run(args, stdin=subprocess.DEVNULL, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE,
                        timeout=timeout)
     if r.returncode != 0:
@@ -418,7 +428,7 @@ def run_reference(workdir, vertex_xyz, cell_vertex, cells, matrices=True, timeou
     while i < len(raw):
         tag, cnt = (int(t) for t in np.frombuffer(raw, np.int32, 2, i))
         i += 8
-        dt = np.float64 if tag == 5 else np.int32
+        dt = np.float64 if tag in (5, 6) else np.int32
         a = np.frombuffer(raw, dt, cnt, i)
         i += cnt * np.dtype(dt).itemsize
         recs.setdefault(tag, []).append(a)
@@ -426,7 +436,8 @@ def run_reference(workdir, vertex_xyz, cell_vertex, cells, matrices=True, timeou
     nc = int(head[0])
     el = recs[4][0].reshape(nc, 1 + 27 + 6)
     res = {"n": head, "edges": recs[2][0].reshape(-1, 2), "faces": recs[3][0], "cell_dofs": el[:, 1:28],
-           "cell_faces": el[:, 28:], "K": [k.reshape(81, 81) for k in recs.get(5, [])], "bases": []}
+           "cell_faces": el[:, 28:], "K": [k.reshape(81, 81) for k in recs.get(5, [])], "bases": [],
+           "solution": recs[6][0].reshape(-1, 3) if 6 in recs else None}
     for c in range(nc):
         sub = os.path.join(fine, f"Elem_{c}", "SubElem_0")
         res["bases"].append(np.stack([np.loadtxt(os.path.join(sub, f"BasisFunction_{b}.txt")).reshape(-1, 3)
@@ -456,3 +467,122 @@ def graded_cells(nc, m, grade, seed=1, contrast=10.0):
     cv = np.array([[(c % nc + (b & 1)) + (nc + 1) * ((c // nc % nc + (b >> 1 & 1)) + (nc + 1) * (c // nc ** 2 + (b >> 2 & 1)))
                     for b in range(8)] for c in range(nc ** 3)])
     return vxyz, cv, cm
+
+
+# --------------------------------------------------------------------------------------------
+# The Order2 macro driver (MsFEM/MsFEM.h:14-569)
+# --------------------------------------------------------------------------------------------
+
+def polygon_rule3(V):
+    """geometry::Polygon::SetIntegrationLaw(3) (Library/GeometryShape.h:2625-2640): the fan of
+    triangles (centroid, V_i, V_i+1), each with Triangle::SetIntegrationLaw(3) (:1482-1540) as
+    written there: weights 1/6 |e1 x e2| at (1/6, 1/6), (2/3, 1/6) and again (2/3, 1/6) -- its third
+    point repeats the second where the symmetric rule has (1/6, 2/3)."""
+    V = np.asarray(V, dtype=np.float64)
+    C = V.mean(axis=0)
+    pts, w = [], []
+    for i in range(V.shape[0]):
+        e1, e2 = V[i] - C, V[(i + 1) % V.shape[0]] - C
+        det = np.linalg.norm(np.cross(e1, e2))
+        for a, b in ((1 / 6, 1 / 6), (2 / 3, 1 / 6), (2 / 3, 1 / 6)):
+            pts.append(C + a * e1 + b * e2)
+            w.append(det / 6.0)
+    return np.array(pts), np.array(w)
+
+
+def _basis_at(xyz, tets, bases, I, x):
+    """z component of basis I at x, from the micro tetrahedron holding x (the nearest-element
+    lookup and P1 interpolation of the reference's macro basis functions, :2942-2950)."""
+    e = oc.locate(xyz, tets, x)
+    P = xyz[tets[e]]
+    lam = np.linalg.solve((P[1:] - P[0]).T, x - P[0])
+    bary = np.concatenate([[1 - lam.sum()], lam])
+    return float(bary @ bases[tets[e], I, 2])
+
+
+def order2_driver(vertex_xyz, cell_vertex, cells, groups, bases=None):
+    """The Order2 macro solution [n_dofs, 3] (MsFEM_forElasticDeformation_OrderBF2_forPoly):
+    groups = [(vertex ids, value (3,), take (3 bools))], the Dirichlet groups.  Steps:
+      * bases and macro element matrices of every cell (order2_bases, macro_element_matrix), D of
+        domain 0, summed into the 3x3-block system by the cells' DOF lists (macro_topology);
+      * per group (Grid_forMech::CreateBoundaryConditions, MsFEM_Grid.h:3303-3470): its DOFs (the
+        vertices, the edges with both ends in it, the faces with all vertices in it, ascending),
+        the L2 projection of its value onto them over its faces -- the mass matrix and load of the
+        faces' 9 DOFs (4 vertices, 4 edges, the face) with the polygon rule 3, the bases' z
+        components evaluated in the face's first element -- solved per component (the face
+        bubbles vanish on their faces: their values are 0);
+      * the scalar copy of the system (DOF 3 d + c), and for every group DOF in order, every taken
+        component: X = F = value, the row set to the identity and the column moved to F
+        (MsFEM.h:300-365);
+      * no Neumann data: the Order2 grid builds no boundary faces, so the loop at MsFEM.h:54-59 adds
+        nothing;
+      * the solve (here exact; the reference runs plain CG restarts, MsFEM.h:445-478).
+    bases: optional precomputed [per cell (n_nodes, 27, 3)]."""
+    edges, faces, cell_faces, dofs = macro_topology(cell_vertex)
+    vertex_xyz = np.asarray(vertex_xyz, dtype=np.float64)
+    nv, ne, nf = vertex_xyz.shape[0], len(edges), len(faces)
+    nd = nv + ne + nf + len(cell_vertex)
+    if bases is None:
+        bases = []
+        for c in range(cells.n_cells):
+            xyz, tets, mat, box = cells.cell(c)
+            bases.append(order2_bases(xyz, tets, mat, box, cells.E, cells.nu, cell_vertex[c]))
+    A = np.zeros((3 * nd, 3 * nd))
+    for c in range(cells.n_cells):
+        xyz, tets, mat, box = cells.cell(c)
+        K = macro_element_matrix(xyz, tets, bases[c], box, cells.E[0], cells.nu[0])
+        idx = (3 * dofs[c][:, None] + np.arange(3)).ravel()
+        A[np.ix_(idx, idx)] += K.transpose(0, 2, 1, 3).reshape(81, 81)
+    # the first element of each face (faces shared by two cells are interior, never Dirichlet)
+    face_cell = {}
+    for c in range(len(cell_vertex)):
+        for f in cell_faces[c]:
+            face_cell.setdefault(int(f), c)
+    eid = {tuple(p): i for i, p in enumerate(edges)}
+    fixed = []                                       # (scalar DOF, value) in the reference's order
+    for verts, value, take in groups:
+        vs = [int(v) for v in verts]
+        sv = set(vs)
+        gd = list(vs)
+        gd += [nv + i for i, (a, b) in enumerate(edges) if a in sv and b in sv]
+        tf = [i for i in range(nf) if set(int(v) for v in faces[i]) <= sv]
+        gd += [nv + ne + i for i in tf]
+        gd = sorted(gd)
+        pos = {d: k for k, d in enumerate(gd)}
+        M = np.zeros((len(gd), len(gd)))
+        Fg = np.zeros((len(gd), 3))
+        for f in tf:
+            cyc = [int(v) for v in faces[f]]
+            fd = cyc + [nv + eid[(min(cyc[k], cyc[(k + 1) % 4]), max(cyc[k], cyc[(k + 1) % 4]))] for k in range(4)]
+            fd += [nv + ne + f]
+            c = face_cell[f]
+            xyz, tets, mat, box = cells.cell(c)
+            loc = {int(d): k for k, d in enumerate(dofs[c])}
+            pts, w = polygon_rule3(vertex_xyz[cyc])
+            psi = np.array([[_basis_at(xyz, tets, bases[c], loc[d], x) for d in fd] for x in pts])   # [q, 9]
+            Ml = np.einsum("q,qi,qj->ij", w, psi, psi)
+            Fl = np.einsum("q,qi->i", w, psi)[:, None] * np.asarray(value, dtype=np.float64)[None, :]
+            for I, di in enumerate(fd):
+                if di not in pos:
+                    continue
+                for J, dj in enumerate(fd):
+                    if dj in pos:
+                        M[pos[di], pos[dj]] += Ml[I, J]
+                Fg[pos[di]] += Fl[I]
+        # the face bubble vanishes on its own face (its face problem has no load), so its row and
+        # column of M are zero; the reference's Gauss leaves 0 there, as the least-squares solve does
+        vals = np.linalg.lstsq(M, Fg, rcond=None)[0]
+        for k, d in enumerate(gd):
+            for comp in range(3):
+                if take[comp]:
+                    fixed.append((3 * d + comp, vals[k, comp]))
+    F = np.zeros(3 * nd)
+    for i, val in fixed:
+        col = A[:, i].copy()
+        col[i] = 0.0
+        F -= col * val
+        A[:, i] = 0.0
+        A[i, :] = 0.0
+        A[i, i] = 1.0
+        F[i] = val
+    return np.linalg.solve(A, F).reshape(nd, 3)

@@ -12,6 +12,13 @@
  * writing its output.
  *
  *   order2_ref <macro_dir> <fine_dir> <out_file> <n_mat> E0 nu0 [E1 nu1 ...] [--matrices]
+ *              [--driver <bc_file> <min_residual>]
+ *
+ * --driver runs the whole Order2 driver instead (MsFEM::MsFEM_forElasticDeformation_OrderBF2_forPoly,
+ * MsFEM/MsFEM.h:14-569) with the Dirichlet groups of bc_file (text: n_groups, then per group
+ * `take_x take_y take_z  vx vy vz  n  v_0 .. v_{n-1}`, the vertex lists and masked constant
+ * values MsFEM/MsFEM_Main.cpp:187-300 reads from its kraev1 file) and no Neumann data, and adds
+ *   tag 6: the solution, 3 doubles per macro DOF.
  *
  * The bases themselves are the reference's BasisFunction_<i>.txt files in each
  * Elem_<c>/SubElem_0 directory (written by CreateFunctionalSpaces, :2926-2937).
@@ -23,7 +30,7 @@
  *   tag 5: (--matrices) per element: the (3 n_dofs)^2 doubles of its local matrix,
  *          row 3I+i, column 3J+j = A[I][J].val[i][j]
  */
-#include "MsFEM/MsFEM_Grid.h"
+#include "MsFEM/MsFEM.h"
 
 #include <cstdio>
 #include <cstring>
@@ -65,7 +72,17 @@ int main(int argc, char** argv)
     }
     const int n_mat = atoi(argv[4]);
     if (argc < 5 + 2 * n_mat) return 2;
-    const bool matrices = argc > 5 + 2 * n_mat && strcmp(argv[5 + 2 * n_mat], "--matrices") == 0;
+    bool matrices = false;
+    const char* bc_file = nullptr;
+    double min_residual = 1e-12;
+    for (int a = 5 + 2 * n_mat; a < argc; a++) {
+        if (strcmp(argv[a], "--matrices") == 0) matrices = true;
+        if (strcmp(argv[a], "--driver") == 0 && a + 2 < argc) {
+            bc_file = argv[a + 1];
+            min_residual = atof(argv[a + 2]);
+            a += 2;
+        }
+    }
 
     math::SimpleGrid geo;
     geo.ReadFromNVTR(argv[1], -1);
@@ -78,7 +95,36 @@ int main(int argc, char** argv)
     }
     std::vector<Dirichlet> first;
     std::vector<Neumann> second;
-    grid->Initialization(geo, first, second, argv[2]);
+    std::vector<Point<double>> solution;
+    if (bc_file) {
+        FILE* fb = fopen(bc_file, "r");
+        if (!fb) return 4;
+        int ng = 0;
+        if (fscanf(fb, "%d", &ng) != 1) return 4;
+        first.resize(ng);
+        for (int g = 0; g < ng; g++) {
+            int tx, ty, tz, n;
+            double vx, vy, vz;
+            if (fscanf(fb, "%d %d %d %lf %lf %lf %d", &tx, &ty, &tz, &vx, &vy, &vz, &n) != 7) return 4;
+            for (int k = 0; k < n; k++) {
+                int v;
+                if (fscanf(fb, "%d", &v) != 1) return 4;
+                first[g].id_vertexes.push_back(v);
+            }
+            const Point<bool> take(tx != 0, ty != 0, tz != 0);
+            const Point<double> val(vx, vy, vz);
+            first[g].value = [take, val](Point<bool>& is_take) {
+                is_take = take;
+                return val;
+            };
+        }
+        fclose(fb);
+        CSSD_Matrix<Tensor2Rank3D, Point<double>> slae;
+        MsFEM::MsFEM_forElasticDeformation_OrderBF2_forPoly(false, min_residual, argv[2], geo, first, second, argv[2],
+                                                           *grid, solution, slae);
+    } else {
+        grid->Initialization(geo, first, second, argv[2]);
+    }
 
     FILE* f = fopen(argv[3], "wb");
     if (!f) return 3;
@@ -134,6 +180,17 @@ int main(int argc, char** argv)
             fwrite(h, sizeof(int), 2, f);
             fwrite(M.data(), sizeof(double), M.size(), f);
         }
+    }
+    if (bc_file) {
+        std::vector<double> sol;
+        for (auto& p : solution) {
+            sol.push_back(p.x);
+            sol.push_back(p.y);
+            sol.push_back(p.z);
+        }
+        int h[2] = {6, (int)sol.size()};
+        fwrite(h, sizeof(int), 2, f);
+        fwrite(sol.data(), sizeof(double), sol.size(), f);
     }
     fclose(f);
     fflush(stdout);
