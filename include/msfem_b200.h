@@ -321,6 +321,13 @@ int msfem_cells_get_bases(msfem_cells_t c, double* bases, int on_device);
 int msfem_cells_build_order2(msfem_cells_t c, const int32_t* cell_vertex, int precision, double tol, int maxiter,
                              int threads);
 
+/* Host only (no device work): the Order2 edge-bubble order of every cell -- order[c][k] = the
+ * cell-local edge (0..11: edge e runs along axis e / 4, at side (e >> 1) & 1 of the lower other
+ * axis and e & 1 of the higher one) of edge basis k, i.e. the cell's edges sorted by their
+ * (lower, higher) global vertex pair as the reference numbers its macro edges
+ * (MsFEM_Grid.h:597-760). */
+int msfem_order2_edge_order(int n_cells, const int32_t* cell_vertex, int32_t* order);
+
 /* bases: [n_nodes][27][3] doubles, node-major (self_basis_functions[i][node] of
  * MsFEM_Grid.h:2926-2937 transposed). */
 int msfem_cells_get_order2_bases(msfem_cells_t c, double* bases, int on_device);

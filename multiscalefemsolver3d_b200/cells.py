@@ -69,6 +69,15 @@ class BatchSystems:
             pass
 
 
+def order2_edge_order(cell_vertex):
+    """[n_cells, 12]: the cell-local edge of each Order2 edge basis (host computation in the
+    library; msfem_order2_edge_order)."""
+    cv = _c(cell_vertex, np.int32)
+    out = np.empty((cv.shape[0], 12), np.int32)
+    check(load().msfem_order2_edge_order(cv.shape[0], _p(cv), _p(out)), "order2_edge_order")
+    return out
+
+
 class Cells:
     def __init__(self, cm):
         """cm: meshgen.CellMeshes (or any object with the same fields)."""

@@ -1272,6 +1272,34 @@ __global__ void k_o2_scatter(int64_t n_nodes, const double* __restrict__ x, O2Sl
             for (int q = 0; q < 3; q++) bases[81 * i + 3 * sl.dof[s] + q] = x[24 * i + 3 * s + q];
 }
 
+}  // namespace
+
+// host: the local edge (edge_info numbering) of each Order2 edge-bubble slot, per cell
+int order2_edge_order(int n_cells, const int32_t* cell_vertex, int32_t* perm)
+{
+    for (int c = 0; c < n_cells; c++) {
+        const int32_t* g = cell_vertex + 8 * (size_t)c;
+        for (int a = 0; a < 8; a++)
+            for (int b = a + 1; b < 8; b++)
+                if (g[a] == g[b]) {
+                    set_error("Order2 cells: cell %d repeats the global vertex %d", c, g[a]);
+                    return MSFEM_ERR_ARGUMENT;
+                }
+        int idx[12];
+        for (int e = 0; e < 12; e++) idx[e] = e;
+        auto key = [&](int e) {
+            int axis, fa, fb, vl, vh;
+            edge_info(e, axis, fa, fb, vl, vh);
+            return std::make_pair(std::min(g[vl], g[vh]), std::max(g[vl], g[vh]));
+        };
+        std::sort(idx, idx + 12, [&](int p, int q) { return key(p) < key(q); });
+        for (int k = 0; k < 12; k++) perm[12 * (size_t)c + k] = idx[k];
+    }
+    return MSFEM_OK;
+}
+
+namespace {
+
 int cells_build_order2(CellsHandle& h, const int32_t* cell_vertex, int precision, double tol, int maxiter, int threads)
 {
     cudaStream_t st = h.stream;
@@ -1283,24 +1311,7 @@ int cells_build_order2(CellsHandle& h, const int32_t* cell_vertex, int precision
         std::vector<int32_t> gv(8 * (size_t)h.n_cells), perm(12 * (size_t)h.n_cells);
         MSFEM_CK(cudaMemcpyAsync(gv.data(), cell_vertex, sizeof(int32_t) * gv.size(), cudaMemcpyDefault, st));
         MSFEM_CK(cudaStreamSynchronize(st));
-        for (int c = 0; c < h.n_cells; c++) {
-            const int32_t* g = gv.data() + 8 * c;
-            for (int a = 0; a < 8; a++)
-                for (int b = a + 1; b < 8; b++)
-                    if (g[a] == g[b]) {
-                        set_error("msfem_cells_build_order2: cell %d repeats the global vertex %d", c, g[a]);
-                        return MSFEM_ERR_ARGUMENT;
-                    }
-            int idx[12];
-            for (int e = 0; e < 12; e++) idx[e] = e;
-            auto key = [&](int e) {
-                int axis, fa, fb, vl, vh;
-                edge_info(e, axis, fa, fb, vl, vh);
-                return std::make_pair(std::min(g[vl], g[vh]), std::max(g[vl], g[vh]));
-            };
-            std::sort(idx, idx + 12, [&](int p, int q) { return key(p) < key(q); });
-            for (int k = 0; k < 12; k++) perm[12 * (size_t)c + k] = idx[k];
-        }
+        MSFEM_TRY(order2_edge_order(h.n_cells, gv.data(), perm.data()));
         MSFEM_TRY(copy_in(st, h.edge_perm, perm.data(), perm.size()));
     }
     if (!h.faces2_ready) {
@@ -1565,6 +1576,15 @@ int msfem_cells_get_bases(msfem_cells_t h, double* bases, int on_device)
                              on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, h->stream));
     MSFEM_CK(cudaStreamSynchronize(h->stream));
     return MSFEM_OK;
+}
+
+int msfem_order2_edge_order(int n_cells, const int32_t* cell_vertex, int32_t* order)
+{
+    if (n_cells < 0 || (n_cells > 0 && (!cell_vertex || !order))) {
+        msfem::set_error("msfem_order2_edge_order: bad arguments");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    return msfem::order2_edge_order(n_cells, cell_vertex, order);
 }
 
 int msfem_cells_build_order2(msfem_cells_t h, const int32_t* cell_vertex, int precision, double tol, int maxiter,
