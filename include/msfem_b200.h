@@ -328,6 +328,15 @@ int msfem_cells_build_order2(msfem_cells_t c, const int32_t* cell_vertex, int pr
  * (MsFEM_Grid.h:597-760). */
 int msfem_order2_edge_order(int n_cells, const int32_t* cell_vertex, int32_t* order);
 
+/* Host only: the Order2 macro system as the scalar CSR of MakeCopyMatrix_A_into_B (DOF 3 d + c,
+ * whole 3x3 blocks of the DOF portrait, diagonal in place; Grid_forMech::CreationPortrait and
+ * SummPartOfMatrix, MsFEM/MsFEM.h:48-131) from the cells' DOF lists cell_dofs [n_cells][27] (the
+ * reference's numbering: vertices, NV + edge, NV + NE + face, NV + NE + NF + cell) and element
+ * matrices K [n_cells][27][27][3][3] (msfem_cells_order2_macro_matrices).  Call with row_ptr,
+ * col or val NULL to get *nnz; then row_ptr [3 n_dofs + 1], col / val [nnz]. */
+int msfem_order2_macro_csr(int n_cells, int n_dofs, const int32_t* cell_dofs, const double* K, int64_t* row_ptr,
+                           int32_t* col, double* val, int64_t* nnz);
+
 /* bases: [n_nodes][27][3] doubles, node-major (self_basis_functions[i][node] of
  * MsFEM_Grid.h:2926-2937 transposed). */
 int msfem_cells_get_order2_bases(msfem_cells_t c, double* bases, int on_device);

@@ -533,6 +533,25 @@ def order2_driver(vertex_xyz, cell_vertex, cells, groups, bases=None):
         K = macro_element_matrix(xyz, tets, bases[c], box, cells.E[0], cells.nu[0])
         idx = (3 * dofs[c][:, None] + np.arange(3)).ravel()
         A[np.ix_(idx, idx)] += K.transpose(0, 2, 1, 3).reshape(81, 81)
+    fixed = dirichlet_fixed(vertex_xyz, cell_vertex, cells, groups, bases)
+    F = np.zeros(3 * nd)
+    for i, val in fixed:
+        col = A[:, i].copy()
+        col[i] = 0.0
+        F -= col * val
+        A[:, i] = 0.0
+        A[i, :] = 0.0
+        A[i, i] = 1.0
+        F[i] = val
+    return np.linalg.solve(A, F).reshape(nd, 3)
+
+
+def dirichlet_fixed(vertex_xyz, cell_vertex, cells, groups, bases):
+    """[(scalar DOF, value)] of the Order2 Dirichlet groups in the reference's order (the
+    projection step of order2_driver)."""
+    edges, faces, cell_faces, dofs = macro_topology(cell_vertex)
+    vertex_xyz = np.asarray(vertex_xyz, dtype=np.float64)
+    nv, ne, nf = vertex_xyz.shape[0], len(edges), len(faces)
     # the first element of each face (faces shared by two cells are interior, never Dirichlet)
     face_cell = {}
     for c in range(len(cell_vertex)):
@@ -576,13 +595,4 @@ def order2_driver(vertex_xyz, cell_vertex, cells, groups, bases=None):
             for comp in range(3):
                 if take[comp]:
                     fixed.append((3 * d + comp, vals[k, comp]))
-    F = np.zeros(3 * nd)
-    for i, val in fixed:
-        col = A[:, i].copy()
-        col[i] = 0.0
-        F -= col * val
-        A[:, i] = 0.0
-        A[i, :] = 0.0
-        A[i, i] = 1.0
-        F[i] = val
-    return np.linalg.solve(A, F).reshape(nd, 3)
+    return fixed

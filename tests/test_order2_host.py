@@ -31,3 +31,58 @@ def test_order2_edge_order_matches_restatement(lib):
 def test_order2_edge_order_rejects_repeated_vertices(lib):
     with pytest.raises(Exception):
         gcells.order2_edge_order(np.array([[0, 1, 2, 3, 4, 5, 6, 6]], np.int32))
+
+
+def _case():
+    vxyz, cv, cm = o2.graded_cells(2, 3, 0.4)
+    bases = []
+    for c in range(cm.n_cells):
+        xyz, tets, mat, box = cm.cell(c)
+        bases.append(o2.order2_bases(xyz, tets, mat, box, cm.E, cm.nu, cv[c]))
+    bot = np.nonzero(np.abs(vxyz[:, 2]) < 1e-12)[0]
+    top = np.nonzero(np.abs(vxyz[:, 2] - 1) < 1e-12)[0]
+    side = np.nonzero(np.abs(vxyz[:, 0] - 1) < 1e-12)[0]
+    groups = [(bot, (0.0, 0.0, 0.0), (1, 1, 1)), (top, (0.01, -0.02, 0.05), (1, 1, 1)),
+              (side, (0.03, 0.0, 0.0), (1, 0, 0))]
+    return vxyz, cv, cm, bases, groups
+
+
+def test_order2_topology_macro_system_and_dirichlet_values_match_restatement(lib):
+    """The product's host side of the Order2 driver (macro topology, the macro CSR summed by the
+    library, the projected Dirichlet values) on the restatement's bases: the same topology, the
+    same system as the restatement's dense assembly, the same fixed values, and with them the same
+    macro solution.  (The GPU builds of the bases and element matrices, the Dirichlet rows and the
+    solve are covered by their own GPU tests.)"""
+    from multiscalefemsolver3d_b200 import order2 as p2
+    vxyz, cv, cm, bases, groups = _case()
+    topo = p2.macro_topology(cv, n_vertices=vxyz.shape[0])
+    edges, faces, cell_faces, dofs = o2.macro_topology(cv)
+    np.testing.assert_array_equal(topo.edges, edges)
+    np.testing.assert_array_equal(topo.faces, faces)
+    np.testing.assert_array_equal(topo.cell_faces, cell_faces)
+    np.testing.assert_array_equal(topo.cell_dofs, dofs)
+    K = np.stack([o2.macro_element_matrix(*cm.cell(c)[:2], bases[c], cm.cell(c)[3], cm.E[0], cm.nu[0])
+                  for c in range(cm.n_cells)])
+    A = p2.macro_csr(topo, K)
+    dense = np.zeros((3 * topo.n_dofs,) * 2)
+    for c in range(cm.n_cells):
+        idx = (3 * dofs[c][:, None] + np.arange(3)).ravel()
+        dense[np.ix_(idx, idx)] += K[c].transpose(0, 2, 1, 3).reshape(81, 81)
+    np.testing.assert_allclose(A.to_scipy().toarray(), dense, rtol=0, atol=1e-14 * np.abs(dense).max())
+    assert np.all(np.diff(A.row_ptr) % 3 == 0)            # whole 3x3 blocks per row
+    got = p2.dirichlet_values(vxyz, cm, topo, bases, groups)
+    want = o2.dirichlet_fixed(vxyz, cv, cm, groups, bases)
+    assert [i for i, _ in got] == [i for i, _ in want]
+    np.testing.assert_allclose([v for _, v in got], [v for _, v in want], rtol=0, atol=1e-13)
+    # the composition: eliminate and solve the product's system, compare with the restated driver
+    M = A.to_scipy().toarray()
+    F = np.zeros(M.shape[0])
+    for i, v in got:
+        F -= M[:, i] * v
+        M[:, i] = 0.0
+        M[i, :] = 0.0
+        M[i, i] = 1.0
+        F[i] = v
+    x = np.linalg.solve(M, F).reshape(-1, 3)
+    xo = o2.order2_driver(vxyz, cv, cm, groups, bases=bases)
+    assert np.linalg.norm(x - xo) <= 1e-11 * np.linalg.norm(xo)
