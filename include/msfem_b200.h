@@ -306,6 +306,13 @@ int msfem_cells_create(int n_cells, const int64_t* node_off, const double* xyz, 
  * precision / tol / maxiter / threads as for msfem_batch_solve. */
 int msfem_cells_build_bases(msfem_cells_t c, int precision, double tol, int maxiter, int threads);
 
+/* Materials of the Order1 face and edge problems: mode 0 (default) -- each face triangle and edge
+ * segment takes the material of the tetrahedra it bounds; mode 1 -- material 0 everywhere, which
+ * is what the reference computes: its face meshes come from Salome files whose ReadFromSalomeDat
+ * leaves every material id 0 (Library/Math.h:91-147; MsFEM_Grid.h:4848, the edge segments copy the
+ * face ids, :4905).  Takes effect at the next msfem_cells_build_bases. */
+int msfem_cells_set_face_material(msfem_cells_t c, int mode);
+
 /* bases: [n_nodes][8][3] doubles, node-major (the reference's self_basis_functions[v][node]
  * as Points, MsFEM_Grid.h:5510-5530, transposed to node-major). */
 int msfem_cells_get_bases(msfem_cells_t c, double* bases, int on_device);

@@ -88,6 +88,7 @@ _SIGS = [
                                      C.POINTER(C.c_void_p)]),
     ("msfem_cells_build_bases", C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int]),
     ("msfem_cells_get_bases", C.c_int, [C.c_void_p, _P, C.c_int]),
+    ("msfem_cells_set_face_material", C.c_int, [C.c_void_p, C.c_int]),
     ("msfem_cells_build_order2", C.c_int, [C.c_void_p, _P, C.c_int, C.c_double, C.c_int, C.c_int]),
     ("msfem_order2_edge_order", C.c_int, [C.c_int, _P, _P]),
     ("msfem_order2_macro_csr", C.c_int, [C.c_int, C.c_int, _P, _P, _P, _P, _P, C.POINTER(C.c_int64)]),

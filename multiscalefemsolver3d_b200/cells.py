@@ -97,6 +97,11 @@ class Cells:
         """threads = CTA size of the persistent solves; 0 autotunes it on the first build."""
         return check(load().msfem_cells_build_bases(self.h, precision, tol, maxiter, threads), "cells_build_bases")
 
+    def set_face_material(self, mode: str):
+        """"cells" (default): face triangles and edge segments take their tetrahedra's material;
+        "zero": material 0 everywhere, as the reference's construction computes."""
+        check(load().msfem_cells_set_face_material(self.h, {"cells": 0, "zero": 1}[mode]), "cells_set_face_material")
+
     def bases(self):
         out = np.empty((self.n_nodes, 8, 3))
         check(load().msfem_cells_get_bases(self.h, _p(out), 0), "cells_get_bases")

@@ -945,6 +945,24 @@ int cells_create(int n_cells, const int64_t* node_off, const double* xyz, const 
     return 0;
 }
 
+// the face batch's materials for the current face_material mode
+int set_face_materials(CellsHandle& h, int mode)
+{
+    cudaStream_t st = h.stream;
+    BatchSys& F = h.faces;
+    if (mode == h.face_material) return MSFEM_OK;
+    if (mode == 1) {
+        MSFEM_TRY(h.face_emat_cells.alloc(F.n_elems));
+        MSFEM_CK(cudaMemcpyAsync(h.face_emat_cells.p, F.emat.p, sizeof(int32_t) * F.n_elems, cudaMemcpyDeviceToDevice, st));
+        MSFEM_CK(cudaMemsetAsync(F.emat.p, 0, sizeof(int32_t) * F.n_elems, st));
+    } else {
+        MSFEM_CK(cudaMemcpyAsync(F.emat.p, h.face_emat_cells.p, sizeof(int32_t) * F.n_elems, cudaMemcpyDeviceToDevice, st));
+    }
+    MSFEM_CK(cudaStreamSynchronize(st));
+    h.face_material = mode;
+    return MSFEM_OK;
+}
+
 int cells_build(CellsHandle& h, int precision, double tol, int maxiter, int threads)
 {
     cudaStream_t st = h.stream;
@@ -1551,6 +1569,17 @@ int msfem_cells_create(int n_cells, const int64_t* node_off, const double* xyz, 
     MSFEM_TRY(cells_create(n_cells, node_off, xyz, tet_off, tets, material, box, n_materials, E, nu, *h));
     *out = h.release();
     return MSFEM_OK;
+}
+
+int msfem_cells_set_face_material(msfem_cells_t h, int mode)
+{
+    using namespace msfem;
+    if (!h || (mode != 0 && mode != 1)) {
+        set_error("msfem_cells_set_face_material: bad arguments");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    MSFEM_CK(cudaSetDevice(h->device));
+    return set_face_materials(*h, mode);
 }
 
 int msfem_cells_build_bases(msfem_cells_t h, int precision, double tol, int maxiter, int threads)

@@ -37,6 +37,10 @@ struct CellsHandle {
     DBuf<double> fxyz, prof, fx, bx;
     int cap = 0;
     bool vols_assembled = false;  // volume problem matrices hold the current materials
+    // materials of the face triangles and edge segments: 0 = those of the tetrahedra they bound,
+    // 1 = material 0 everywhere (the reference's Salome face meshes carry no materials)
+    int face_material = 0;
+    DBuf<int32_t> face_emat_cells;  // the cells' face-triangle materials, kept while mode 1 is on
     DBuf<int32_t> edge_nodes, edge_len, seg_tri;
     DBuf<int> flag;
     // Order2 (27 bases per cell): face problems on material 0 with 8 right-hand sides, the edge

@@ -181,9 +181,13 @@ def face_triangles(tets, mat, mask):
     return out
 
 
-def order1_bases(xyz, tets, mat, box, E, nu, solver=None):
+def order1_bases(xyz, tets, mat, box, E, nu, solver=None, face_material="cells"):
     """Bases [n_nodes, 8, 3] of one Order1 cell.  solver(dim, xyz, elems, mat, E, nu, bc_nodes, bc_values)
-    solves one sub-problem (default: the exact restatement `cell_problem`)."""
+    solves one sub-problem (default: the exact restatement `cell_problem`).  face_material:
+    "cells" -- the face triangles and edge segments take the material of the tetrahedra they
+    bound; "zero" -- material 0 everywhere, as the reference's construction has it (its face
+    meshes come from Salome files, whose ReadFromSalomeDat leaves every material id 0,
+    Library/Math.h:91-147, MsFEM_Grid.h:4848, and the edge segments copy the face ids, :4905)."""
     solve = solver or cell_problem
     xyz = np.asarray(xyz, dtype=np.float64)
     tets = np.asarray(tets, dtype=np.int64)
@@ -196,7 +200,9 @@ def order1_bases(xyz, tets, mat, box, E, nu, solver=None):
         hit = np.nonzero((mask & want) == want)[0]
         assert hit.size == 1, f"vertex {v}: {hit.size} nodes"
         vert[v] = hit[0]
-    tris = face_triangles(tets, mat, mask)
+    if face_material not in ("cells", "zero"):
+        raise ValueError("face_material must be 'cells' or 'zero'")
+    tris = face_triangles(tets, mat if face_material == "cells" else np.zeros_like(mat), mask)
 
     # edges: sorted nodes along the edge, segment materials, the two end profiles
     edge_sol = {}   # (edge id) -> (nodes [k], sol_low [k,3], sol_high [k,3])

@@ -28,6 +28,7 @@
 #include <random>
 #include <string>
 #include <vector>
+#include <sys/stat.h>
 #include <unistd.h>
 
 using std::abs;
@@ -47,7 +48,21 @@ static inline int fopen_s(FILE** f, const char* name, const char* mode)
     return *f ? 0 : 1;
 }
 
-static inline int CreateDirectory(LPCTSTR, void*) { return 0; }
+/* The reference's headers pass a wide string cast to LPCTSTR (MsFEM/MsFEM.h:600-601,
+ * MsFEM/MsFEM_Grid.h:4810-4811) and write into the directory right after: create it. */
+static inline int CreateDirectory(LPCTSTR p, void*)
+{
+    if (!p) return 0;
+    char buf[4096];
+    if (p[0] != 0 && p[1] == 0) {
+        const size_t k = std::wcstombs(buf, reinterpret_cast<const wchar_t*>(p), sizeof(buf) - 1);
+        if (k == (size_t)-1) return 0;
+        buf[k] = 0;
+    } else {
+        std::snprintf(buf, sizeof(buf), "%s", p);
+    }
+    return ::mkdir(buf, 0755) == 0;
+}
 
 static inline int mbstowcs_s(size_t* out_len, wchar_t* dst, size_t dst_len, const char* src, size_t)
 {

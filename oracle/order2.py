@@ -394,12 +394,15 @@ ORDER2_REF = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_ref", "o
 
 
 def run_reference(workdir, vertex_xyz, cell_vertex, cells, matrices=True, timeout=1200, groups=None,
-                  min_residual=1e-13):
+                  min_residual=1e-13, order1=False):
     """Writes the macro mesh and cell directories under workdir (meshio writers), runs the
     reference's Order2 construction there and returns {"n": [ne, nv, n_edges, n_faces, n_dofs],
     "edges", "faces" (first-reached (id, n, edge ids...) records), "cell_dofs" [nc, 27],
     "cell_faces" [nc, 6], "bases" [per cell: (n_nodes, 27, 3)], "K" [per cell: (81, 81)],
-    "solution" [n_dofs, 3] (groups given: the whole Order2 driver with those Dirichlet groups)}."""
+    "solution" [n_dofs, 3] (groups given: the whole Order2 driver with those Dirichlet groups)}.
+    order1=True (with groups): the Order1 driver instead (Grid_forMech_Poly_Order1,
+    MsFEM_forElasticDeformation_OrderBF1_forPoly): "solution" [n_vertices, 3] and "bases" [per cell:
+    (n_nodes, 8, 3)]."""
     import subprocess
 
     from multiscalefemsolver3d_b200 import meshio
@@ -419,6 +422,8 @@ def run_reference(workdir, vertex_xyz, cell_vertex, cells, matrices=True, timeou
                 fb.write(" ".join(str(int(t)) for t in take) + " " + " ".join(repr(float(v)) for v in value) +
                          f" {len(verts)} " + " ".join(str(int(v)) for v in verts) + "\n")
         args += ["--driver", bc, repr(float(min_residual))]
+        if order1:
+            args.append("--order1")
     r = subprocess.run(args, stdin=subprocess.DEVNULL, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE,
                        timeout=timeout)
     if r.returncode != 0:
@@ -432,6 +437,12 @@ def run_reference(workdir, vertex_xyz, cell_vertex, cells, matrices=True, timeou
         a = np.frombuffer(raw, dt, cnt, i)
         i += cnt * np.dtype(dt).itemsize
         recs.setdefault(tag, []).append(a)
+    if order1:
+        # the Order1 construction writes its bases under <result dir>/tmp/Elem_<c> (MsFEM.h:597-605,
+        # MsFEM_Grid.h:4808, :5556-5566)
+        return {"solution": recs[6][0].reshape(-1, 3),
+                "bases": [np.stack([np.loadtxt(os.path.join(fine, "tmp", f"Elem_{c}", f"BasisFunction_{b}.txt")).reshape(-1, 3)
+                                    for b in range(8)], axis=1) for c in range(cells.n_cells)]}
     head = recs[1][0]
     nc = int(head[0])
     el = recs[4][0].reshape(nc, 1 + 27 + 6)

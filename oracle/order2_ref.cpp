@@ -19,6 +19,9 @@
  * `take_x take_y take_z  vx vy vz  n  v_0 .. v_{n-1}`, the vertex lists and masked constant
  * values MsFEM/MsFEM_Main.cpp:187-300 reads from its kraev1 file) and no Neumann data, and adds
  *   tag 6: the solution, 3 doubles per macro DOF.
+ * --order1 (with --driver) runs the Order1 driver instead (MsFEM_forElasticDeformation_OrderBF1_forPoly,
+ * MsFEM/MsFEM.h:571-1062, on Grid_forMech_Poly_Order1): tag 6 holds 3 doubles per macro vertex,
+ * and only tag 6 is written.
  *
  * The bases themselves are the reference's BasisFunction_<i>.txt files in each
  * Elem_<c>/SubElem_0 directory (written by CreateFunctionalSpaces, :2926-2937).
@@ -34,8 +37,51 @@
 
 #include <cstdio>
 #include <cstring>
+#include <dlfcn.h>
+#include <mutex>
 #include <new>
+#include <set>
 #include <unistd.h>
+
+// The Order1 construction closes each TecPlot stream twice (printTecPlot3D_DiffDomains closes it,
+// then MsFEM_Grid.h:5607 again): streams closed once here ignore a second close until fopen hands
+// their address out again.
+namespace {
+struct ClosedStreams {
+    std::mutex mu;
+    std::set<FILE*> closed;
+};
+ClosedStreams& closed_streams()
+{
+    static ClosedStreams* c = new ClosedStreams();
+    return *c;
+}
+}  // namespace
+
+extern "C" int fclose(FILE* f)
+{
+    static int (*real_close)(FILE*) = reinterpret_cast<int (*)(FILE*)>(dlsym(RTLD_NEXT, "fclose"));
+    if (!f) return EOF;
+    ClosedStreams& c = closed_streams();
+    {
+        std::lock_guard<std::mutex> lock(c.mu);
+        if (!c.closed.insert(f).second) return 0;
+    }
+    return real_close(f);
+}
+
+extern "C" FILE* fopen(const char* path, const char* mode)
+{
+    static FILE* (*real_open)(const char*, const char*) =
+        reinterpret_cast<FILE* (*)(const char*, const char*)>(dlsym(RTLD_NEXT, "fopen"));
+    FILE* f = real_open(path, mode);
+    if (f) {
+        ClosedStreams& c = closed_streams();
+        std::lock_guard<std::mutex> lock(c.mu);
+        c.closed.erase(f);
+    }
+    return f;
+}
 
 void operator delete(void*) noexcept {}
 void operator delete(void*, std::size_t) noexcept {}
@@ -72,11 +118,12 @@ int main(int argc, char** argv)
     }
     const int n_mat = atoi(argv[4]);
     if (argc < 5 + 2 * n_mat) return 2;
-    bool matrices = false;
+    bool matrices = false, order1 = false;
     const char* bc_file = nullptr;
     double min_residual = 1e-12;
     for (int a = 5 + 2 * n_mat; a < argc; a++) {
         if (strcmp(argv[a], "--matrices") == 0) matrices = true;
+        if (strcmp(argv[a], "--order1") == 0) order1 = true;
         if (strcmp(argv[a], "--driver") == 0 && a + 2 < argc) {
             bc_file = argv[a + 1];
             min_residual = atof(argv[a + 2]);
@@ -120,6 +167,31 @@ int main(int argc, char** argv)
         }
         fclose(fb);
         CSSD_Matrix<Tensor2Rank3D, Point<double>> slae;
+        if (order1) {
+            auto* g1 = new MsFEM::Grid_forMech_Poly_Order1();
+            g1->is_print_logFile = false;
+            for (int m = 0; m < n_mat; m++) {
+                g1->AddDomain();
+                g1->GetDomain(m)->forMech.SetE(atof(argv[5 + 2 * m]));
+                g1->GetDomain(m)->forMech.SetV(atof(argv[6 + 2 * m]));
+            }
+            MsFEM::MsFEM_forElasticDeformation_OrderBF1_forPoly(false, min_residual, argv[2], geo, first, second,
+                                                               argv[2], *g1, solution, slae);
+            FILE* f1 = fopen(argv[3], "wb");
+            if (!f1) return 3;
+            std::vector<double> sol;
+            for (auto& p : solution) {
+                sol.push_back(p.x);
+                sol.push_back(p.y);
+                sol.push_back(p.z);
+            }
+            int h[2] = {6, (int)sol.size()};
+            fwrite(h, sizeof(int), 2, f1);
+            fwrite(sol.data(), sizeof(double), sol.size(), f1);
+            fclose(f1);
+            fflush(stdout);
+            _exit(0);
+        }
         MsFEM::MsFEM_forElasticDeformation_OrderBF2_forPoly(false, min_residual, argv[2], geo, first, second, argv[2],
                                                            *grid, solution, slae);
     } else {
