@@ -492,6 +492,8 @@ def cells_config(cm, extra=None):
          "tol": TOL, "solver": "one persistent launch per problem kind: MINRES on the Jacobi-scaled free block, "
                                "FP32 inner solves with FP64 residual refinement (FP64 fallback per cell)",
          "l2": "flushed between steps (256 MiB write); the per-cell vectors and matrices exceed L2",
+         "face_material": "face and edge problems on the materials of the tetrahedra they bound (the reference's "
+                          "own construction puts material 0 there; same cost)",
          "parallelism": "replicas"}
     if extra:
         c.update(extra)
