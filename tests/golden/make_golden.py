@@ -13,6 +13,13 @@ multiscalefemsolver3d_b200.meshgen; a coordinate checksum guards against drift):
                    with 3 spheres, the reference CG solution and the driver's own output
   c1_elastic.npz   the 20^3 elasticity workload (27,783 DOF): matrix checksums, the reference CG
                    solution to 1e-12 on the reference-assembled system, and the driver's output
+  msfem_order1.npz the reference's whole MsFEM Order1 run (oracle/_ref/order2_ref --order1) on
+                   oracle.order2.graded_cells(2, 4, 0.5): the bases of cells 0 and 7 and the
+                   driver's macro solution for u = 0 on z = 0, u = (0.01, -0.02, 0.05) on z = 1
+  msfem_order2.npz the reference's Order2 construction on graded_cells(1, 4, 0.5): the 27 bases
+                   and the macro element matrix; and its whole Order2 driver on graded_cells(2, 4,
+                   0.5) with the same Dirichlet groups: the macro solution
+Only the MsFEM fixtures:  python tests/golden/make_golden.py --msfem
 """
 import os
 import sys
@@ -67,5 +74,32 @@ def main():
     print(f"c1: cg residual {res:.2e} ({wall:.1f} s), driver {wd:.1f} s, total {time.time() - t0:.1f} s")
 
 
+def msfem():
+    import tempfile
+
+    from oracle import order2 as o2
+
+    def groups_of(vxyz):
+        bot = np.nonzero(np.abs(vxyz[:, 2]) < 1e-12)[0]
+        top = np.nonzero(np.abs(vxyz[:, 2] - 1) < 1e-12)[0]
+        return [(bot, (0.0, 0.0, 0.0), (1, 1, 1)), (top, (0.01, -0.02, 0.05), (1, 1, 1))]
+
+    vxyz, cv, cm = o2.graded_cells(2, 4, 0.5)
+    R1 = o2.run_reference(tempfile.mkdtemp(), vxyz, cv, cm, matrices=False, groups=groups_of(vxyz),
+                          min_residual=1e-13, order1=True)
+    np.savez_compressed(os.path.join(HERE, "msfem_order1.npz"), xyz_sum=cm.xyz.sum(), bases_0=R1["bases"][0],
+                        bases_7=R1["bases"][7], solution=R1["solution"])
+    vxyz1, cv1, cm1 = o2.graded_cells(1, 4, 0.5)
+    R2 = o2.run_reference(tempfile.mkdtemp(), vxyz1, cv1, cm1, matrices=True)
+    R3 = o2.run_reference(tempfile.mkdtemp(), vxyz, cv, cm, matrices=False, groups=groups_of(vxyz),
+                          min_residual=1e-13)
+    np.savez_compressed(os.path.join(HERE, "msfem_order2.npz"), xyz_sum_1=cm1.xyz.sum(), bases=R2["bases"][0],
+                        K=R2["K"][0], cell_dofs=R3["cell_dofs"], xyz_sum_2=cm.xyz.sum(), solution=R3["solution"])
+
+
 if __name__ == "__main__":
-    main()
+    if "--msfem" in sys.argv:
+        msfem()
+    else:
+        main()
+        msfem()
