@@ -139,6 +139,13 @@ int msfem_clear(msfem_system_t h);
  * FEM_Grid.h:103-152 with the 1-point rule, CSSD_Matrix.h:307-363).
  * sigma[material] is the element coefficient. */
 int msfem_assemble_scalar(msfem_system_t h, const double* sigma, int n_materials);
+/* The three-coefficient scalar element (FiniteElement_forScal::SolveLocalMatrix with stiffness,
+ * mass and source coefficients, FEM/FEM_Grid.h:25-102, as FEM_forBaseEliptic at FEM/FEM.h:206-397
+ * calls it): per tetrahedron e, with the one-point rule, A += V (S[e] grad(phi_I).grad(phi_J) +
+ * M[e] / 16) and F += V f[e] / 4; S, M, f: the coefficients at each element's centroid, n_tets
+ * each (host or device).  The driver then sets Dirichlet rows only (MSFEM_ROW_ONLY) and runs
+ * BiCG_Stab. */
+int msfem_assemble_scalar3(msfem_system_t h, const double* S, const double* M, const double* f, int on_device);
 
 /* Linear elasticity assembly (FEM/FEM.h:1349-1384, FEM_Grid.h:2125-2192): block
  * A[I][J] = V * B_J^T D(E, nu) B_I for J >= I and A[J][I] = A[I][J]^T (the

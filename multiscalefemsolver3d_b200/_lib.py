@@ -58,6 +58,7 @@ _SIGS = [
     ("msfem_get_stream", C.c_void_p, [C.c_void_p]),
     ("msfem_clear", C.c_int, [C.c_void_p]),
     ("msfem_assemble_scalar", C.c_int, [C.c_void_p, _P, C.c_int]),
+    ("msfem_assemble_scalar3", C.c_int, [C.c_void_p, _P, _P, _P, C.c_int]),
     ("msfem_assemble_elastic", C.c_int, [C.c_void_p, _P, _P, C.c_int]),
     ("msfem_assemble_elastic_textbook", C.c_int, [C.c_void_p, _P, _P, C.c_int]),
     ("msfem_add_traction", C.c_int, [C.c_void_p, C.c_int, _P, _P, C.c_int]),

@@ -68,6 +68,36 @@ __global__ void k_assemble_scalar(int count, const int32_t* __restrict__ elems, 
         }
 }
 
+// FEM_Grid.h:25-102, the three-coefficient element with the one-point rule (centroid, weight V):
+// A_IJ = V (S g_I.g_J + M / 16), F_I += V f / 4, with the element's coefficients S, M, f (the
+// reference's koef(elem, X) at the centroid).  Elements of one colour share no node, so the F
+// updates do not race.
+__global__ void k_assemble_scalar3(int count, const int32_t* __restrict__ elems, const int32_t* __restrict__ tets,
+                                   const double* __restrict__ xyz, const double* __restrict__ S,
+                                   const double* __restrict__ M, const double* __restrict__ f,
+                                   const int32_t* __restrict__ eslot, double* __restrict__ val, double* __restrict__ F)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const int e = elems[t];
+    int v[4], sl[16];
+    load_tet(tets, e, v);
+    load_slots(eslot, e, sl);
+    TetGeom G;
+    tet_geometry(xyz, v, G);
+    const double se = S[e], m16 = M[e] / 16.0;
+#pragma unroll
+    for (int I = 0; I < 4; I++)
+#pragma unroll
+        for (int J = 0; J < 4; J++) {
+            const double k = se * (G.g[I][0] * G.g[J][0] + G.g[I][1] * G.g[J][1] + G.g[I][2] * G.g[J][2]) + m16;
+            val[sl[4 * I + J]] += k * G.vol;
+        }
+    const double fe = f[e] * G.vol / 4.0;
+#pragma unroll
+    for (int I = 0; I < 4; I++) F[v[I]] += fe;
+}
+
 // FEM_Grid.h:2125-2192.  The reference forms B_J^T D B_I (3x6 * 6x6 * 6x3) at
 // each of the 4 quadrature points; for the isotropic D of Domain.h:53-78 with
 // lambda = k*a and mu = k*b that product is, entry by entry,
@@ -213,6 +243,39 @@ int assemble_scalar(System& s, const double* sigma, int n_mat)
         k_assemble_scalar<<<grid_for(cnt, 128), 128, 0, s.stream>>>(cnt, s.color_elems.p + s.color_off[c], s.tets.p,
                                                                     s.xyz.p, s.mat.p, d_sig.p, n_mat, s.eslot.p,
                                                                     s.val.p, bad.p);
+    }
+    MSFEM_CK(cudaGetLastError());
+    s.total_launches += nc;
+    return finish_assembly(s, bad);
+}
+
+int assemble_scalar3(System& s, const double* S, const double* M, const double* f, bool on_device)
+{
+    if (s.kind != MSFEM_SCALAR) {
+        set_error("assemble_scalar3 on an elasticity system");
+        return MSFEM_ERR_STATE;
+    }
+    if (!S || !M || !f) {
+        set_error("assemble_scalar3: coefficient arrays missing");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    const size_t ne = (size_t)s.n_tets;
+    DBuf<double> coef;
+    DBuf<int>& bad = s.flag;
+    MSFEM_TRY(coef.alloc(3 * ne));
+    MSFEM_TRY(bad.alloc(8));
+    MSFEM_CK(cudaEventRecord(s.ev0, s.stream));
+    const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    MSFEM_CK(cudaMemcpyAsync(coef.p, S, sizeof(double) * ne, kind, s.stream));
+    MSFEM_CK(cudaMemcpyAsync(coef.p + ne, M, sizeof(double) * ne, kind, s.stream));
+    MSFEM_CK(cudaMemcpyAsync(coef.p + 2 * ne, f, sizeof(double) * ne, kind, s.stream));
+    MSFEM_CK(cudaMemsetAsync(bad.p, 0, sizeof(int), s.stream));
+    const int nc = (int)s.color_off.size() - 1;
+    for (int c = 0; c < nc; c++) {
+        int cnt = s.color_off[c + 1] - s.color_off[c];
+        k_assemble_scalar3<<<grid_for(cnt, 128), 128, 0, s.stream>>>(cnt, s.color_elems.p + s.color_off[c], s.tets.p,
+                                                                     s.xyz.p, coef.p, coef.p + ne, coef.p + 2 * ne,
+                                                                     s.eslot.p, s.val.p, s.F.p);
     }
     MSFEM_CK(cudaGetLastError());
     s.total_launches += nc;

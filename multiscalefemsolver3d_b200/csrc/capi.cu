@@ -322,6 +322,14 @@ int msfem_assemble_scalar(msfem_system_t h, const double* sigma, int n_materials
     return assemble_scalar(*as_sys(h), sigma, n_materials);
 }
 
+int msfem_assemble_scalar3(msfem_system_t h, const double* S, const double* M, const double* f, int on_device)
+{
+    MSFEM_TRY(check_handle(h));
+    MSFEM_TRY(need_mesh(*as_sys(h), "msfem_assemble_scalar3"));
+    MSFEM_TRY(use_device(*as_sys(h)));
+    return assemble_scalar3(*as_sys(h), S, M, f, on_device != 0);
+}
+
 int msfem_assemble_elastic(msfem_system_t h, const double* E, const double* nu, int n_materials)
 {
     MSFEM_TRY(check_handle(h));

@@ -166,6 +166,7 @@ struct System {
 int build_topology(System& s);
 // ---- assembly (assemble.cu)
 int assemble_scalar(System& s, const double* sigma, int n_mat);
+int assemble_scalar3(System& s, const double* S, const double* M, const double* f, bool on_device);
 int assemble_elastic(System& s, const double* E, const double* nu, int n_mat, bool textbook = false);
 // lambda, mu per material from E, nu (host): lame[2m], lame[2m+1]
 void lame_params(const double* E, const double* nu, int n_mat, double* lame);

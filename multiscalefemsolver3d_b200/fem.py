@@ -159,6 +159,12 @@ class System:
         s = np.ascontiguousarray(sigma, dtype=np.float64)
         check(load().msfem_assemble_scalar(self.h, s.ctypes.data_as(C.c_void_p), s.size), "assemble_scalar")
 
+    def assemble_scalar3(self, S, M, f):
+        """The three-coefficient element (stiffness S, mass M, source f per tetrahedron, at its
+        centroid): A += V (S grad.grad + M / 16), F += V f / 4 (msfem_assemble_scalar3)."""
+        a = [np.ascontiguousarray(np.broadcast_to(np.asarray(x, dtype=np.float64), (self.n_tets,))) for x in (S, M, f)]
+        check(load().msfem_assemble_scalar3(self.h, *[x.ctypes.data_as(C.c_void_p) for x in a], 0), "assemble_scalar3")
+
     def assemble_elastic(self, E, nu):
         e = np.ascontiguousarray(E, dtype=np.float64)
         n = np.ascontiguousarray(nu, dtype=np.float64)

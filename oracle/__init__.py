@@ -87,9 +87,13 @@ class RefLib:
         L.ref_read_nvtr.argtypes = [C.c_char_p, _i, _i, _i, _i, _ip, _ip, _ip, _f64p, _i32p, _i32p, _i32p, _ip]
         L.ref_read_salome.argtypes = [C.c_char_p, _i, _i, _i, _i, _ip, _ip, _f64p, _i32p, _i32p]
         L.ref_postprocess.argtypes = [_i, _f64p, _i, _i32p, _i32p, _i, _f64p, _f64p, _f64p, _f64p]
+        L.ref_scalar3_local.argtypes = [_f64p, C.c_double, C.c_double, C.c_double, _f64p, _f64p]
+        L.ref_scalar3_driver.argtypes = [_i, _f64p, _i, _i32p, _f64p, _f64p, _f64p, _i, _i32p, _f64p, C.c_double,
+                                         _f64p]
         for f in ("ref_elastic_local", "ref_scalar_local", "ref_elastic_system", "ref_elastic_driver",
                   "ref_scalar_system", "ref_scalar_driver", "ref_cssd_solve", "ref_ssor_apply", "ref_cell_problem",
-                  "ref_poly_quadrature", "ref_mech_D", "ref_polygon_quadrature", "ref_read_nvtr", "ref_read_salome", "ref_postprocess"):
+                  "ref_poly_quadrature", "ref_mech_D", "ref_polygon_quadrature", "ref_read_nvtr", "ref_read_salome", "ref_postprocess",
+                  "ref_scalar3_local", "ref_scalar3_driver"):
             getattr(L, f).restype = C.c_int
         L.ref_set_quiet(1)
 
@@ -116,6 +120,24 @@ class RefLib:
         rc = self.L.ref_scalar_local(_c(xyz4, np.float64).ravel(), sigma, K)
         assert rc == 0
         return K.reshape(4, 4)
+
+    def scalar3_local(self, xyz4, S, M, f):
+        """(K + M [4, 4], F [4]) of FiniteElement_forScal::SolveLocalMatrix (FEM_Grid.h:25-102)."""
+        K, F = np.zeros(16), np.zeros(4)
+        rc = self.L.ref_scalar3_local(_c(xyz4, np.float64).ravel(), S, M, f, K, F)
+        assert rc == 0
+        return K.reshape(4, 4), F
+
+    def scalar3_driver(self, xyz, tets, S, M, f, bc_nodes, bc_values, min_residual=1e-12):
+        """The three-coefficient FEM_forBaseEliptic (FEM.h:206-397) with per-element coefficients."""
+        xyz = _c(xyz, np.float64)
+        tets = _c(tets, np.int32)
+        sol = np.zeros(xyz.shape[0])
+        rc = self.L.ref_scalar3_driver(xyz.shape[0], xyz.ravel(), tets.shape[0], tets.ravel(), _c(S, np.float64),
+                                       _c(M, np.float64), _c(f, np.float64), len(bc_nodes), _c(bc_nodes, np.int32),
+                                       _c(bc_values, np.float64), min_residual, sol)
+        assert rc == 0, rc
+        return sol
 
     def elastic_system(self, p, stage: int = 1, nthreads: int = 1):
         m = p.mesh

@@ -296,6 +296,64 @@ int ref_scalar_local(const double* xyz4, double sigma, double* K)
     return 0;
 }
 
+/* FiniteElement_forScal::SolveLocalMatrix with stiffness, mass and source coefficients
+ * (FEM/FEM_Grid.h:25-102, the one-point rule): K[16] = K + M of the element, F[4] its load, for the
+ * constant coefficients S, Mc, f. */
+int ref_scalar3_local(const double* xyz4, double S, double Mc, double f, double* K, double* F)
+{
+    StdoutSilencer s;
+    math::SimpleGrid g;
+    int tet[4] = {0, 1, 2, 3};
+    make_simple_grid(g, 4, xyz4, 1, tet, nullptr);
+    std::vector<DirichletScal> d;
+    std::vector<NeumannScal> nb;
+    auto* grid = new FEM::Grid_forScal();
+    grid->Initialization(g, d, nb);
+    DenseMatrix<double, double> local;
+    std::function<double(int, Point<double>)> ks = [S](int, Point<double>) { return S; };
+    std::function<double(int, Point<double>)> km = [Mc](int, Point<double>) { return Mc; };
+    std::function<double(int, Point<double>)> kf = [f](int, Point<double>) { return f; };
+    grid->GetElement(0)->SolveLocalMatrix(local, ks, km, kf);
+    for (int I = 0; I < 4; I++) {
+        F[I] = local.F[I];
+        for (int J = 0; J < 4; J++) K[I * 4 + J] = local.A[I][J];
+    }
+    return 0;
+}
+
+/* The three-coefficient scalar driver FEM_forBaseEliptic (FEM/FEM.h:206-397): K + M + F per element
+ * with per-element coefficients S[e], Mc[e], f[e], Dirichlet rows only, BiCG_Stab restarts to
+ * min_residual; solution: n_nodes doubles. */
+int ref_scalar3_driver(int n_nodes, const double* xyz, int n_tets, const int* tets, const double* S,
+                       const double* Mc, const double* f, int n_bc, const int* bc_node, const double* bc_val,
+                       double min_residual, double* solution)
+{
+    StdoutSilencer s;
+    math::NUM_THREADS = 1;
+    auto* g = new math::SimpleGrid();
+    make_simple_grid(*g, n_nodes, xyz, n_tets, tets, nullptr);
+    auto* dir = new std::vector<DirichletScal>();
+    auto* neu = new std::vector<NeumannScal>();
+    make_scal_boundaries(n_bc, bc_node, bc_val, *dir);
+    auto* vs = new std::vector<double>(S, S + n_tets);
+    auto* vm = new std::vector<double>(Mc, Mc + n_tets);
+    auto* vf = new std::vector<double>(f, f + n_tets);
+    auto* ks = new std::function<double(int, Point<double>)>([vs](int e, Point<double>) { return (*vs)[e]; });
+    auto* km = new std::function<double(int, Point<double>)>([vm](int e, Point<double>) { return (*vm)[e]; });
+    auto* kf = new std::function<double(int, Point<double>)>([vf](int e, Point<double>) { return (*vf)[e]; });
+    auto* grid = new FEM::Grid_forScal();
+    auto* sol = new std::vector<double>();
+    char* dirname = make_tmpdir();
+    if (!dirname) return -1;
+    FEM::FEM_forBaseEliptic(false, min_residual, *g, *dir, *neu, *ks, *km, *kf, dirname, *grid, *sol);
+    if ((int)sol->size() != n_nodes) return -3;
+    for (int i = 0; i < n_nodes; i++) solution[i] = (*sol)[i];
+    std::string cmd = std::string("rm -rf ") + dirname;
+    if (system(cmd.c_str()) != 0) { }
+    free(dirname);
+    return 0;
+}
+
 /* FEM_forElasticDeformation (FEM/FEM.h:1286-1813) up to the solve.
  * stage 0: the expanded scalar matrix before any boundary condition (FEM.h:1673-1674);
  * stage 1: after the Dirichlet rows and the column sweep (FEM.h:1676-1813).
