@@ -86,3 +86,74 @@ def test_order2_topology_macro_system_and_dirichlet_values_match_restatement(lib
     x = np.linalg.solve(M, F).reshape(-1, 3)
     xo = o2.order2_driver(vxyz, cv, cm, groups, bases=bases)
     assert np.linalg.norm(x - xo) <= 1e-11 * np.linalg.norm(xo)
+
+
+def test_order2_driver_orchestration_with_stand_ins(monkeypatch, lib):
+    """order2.order2_elastic_driver end to end with its two GPU objects replaced by stand-ins that
+    return the restatement's bases and element matrices and solve the eliminated system exactly:
+    the glue (DOF lists, the CSR from the library, the projected values, their elimination order,
+    the reshape) reproduces the restated driver."""
+    from multiscalefemsolver3d_b200 import cells as gcells
+    from multiscalefemsolver3d_b200 import fem
+    from multiscalefemsolver3d_b200 import order2 as p2
+    vxyz, cv, cm, bases, groups = _case()
+    K = np.stack([o2.macro_element_matrix(*cm.cell(c)[:2], bases[c], cm.cell(c)[3], cm.E[0], cm.nu[0])
+                  for c in range(cm.n_cells)])
+
+    class FakeCells:
+        def __init__(self, meshes):
+            assert meshes is cm
+
+        def build_order2(self, cell_vertex, precision, tol):
+            np.testing.assert_array_equal(cell_vertex, cv)
+            return 0
+
+        def order2_macro_matrices(self):
+            return K
+
+        def order2_bases(self):
+            return np.concatenate(bases)
+
+        def close(self):
+            pass
+
+    class FakeSystem:
+        @classmethod
+        def from_csr(cls, A, F=None, X=None):
+            self = cls()
+            self.A = A.to_scipy().toarray()
+            self.F = np.zeros(A.n)
+            return self
+
+        def apply_dirichlet(self, dofs, vals, mode):
+            assert mode == fem.ROW_AND_COLUMN
+            for i, v in zip(dofs, vals):
+                col = self.A[:, i].copy()
+                col[i] = 0.0
+                self.F -= col * v
+                self.A[:, i] = 0.0
+                self.A[i, :] = 0.0
+                self.A[i, i] = 1.0
+                self.F[i] = v
+
+        def copy_f_to_x(self):
+            pass
+
+        def solve(self, method, precision, tol, maxiter):
+            self.x = np.linalg.solve(self.A, self.F)
+            return 0.0, 1, 0
+
+        def get_x(self):
+            return self.x
+
+        def close(self):
+            pass
+
+    monkeypatch.setattr(gcells, "Cells", FakeCells)
+    monkeypatch.setattr(fem.System, "from_csr", FakeSystem.from_csr)
+    # groups without shared DOFs: the product eliminates each DOF once with its last value
+    g2 = groups[:2]
+    x, info = p2.order2_elastic_driver(cm, vxyz, cv, g2)
+    xo = o2.order2_driver(vxyz, cv, cm, g2, bases=bases)
+    assert info["n_dofs"] == xo.shape[0]
+    assert np.linalg.norm(x - xo) <= 1e-11 * np.linalg.norm(xo)
