@@ -20,10 +20,12 @@
 // (4 right-hand sides per face), then all volume problems to another (8 per cell).
 //
 // Cell conventions: vertex b at (x_{b&1}, y_{(b>>1)&1}, z_{(b>>2)&1}); face f
-// (0..5) = x0, x1, y0, y1, z0, z1; the vertices of a face in increasing b; an edge
-// segment takes the material of the face triangle holding it on the lower-numbered
-// of the edge's two faces (the reference takes it from the first neighbouring face
-// of the macro edge, MsFEM_Grid.h:4900-4925, an order its mesh files fix).
+// (0..5) = x0, x1, y0, y1, z0, z1; the vertices of a face in increasing b.  Materials of the
+// face and edge problems: by default a face triangle takes the material of the tetrahedron it
+// bounds and an edge segment that of its triangle on the lower-numbered of the edge's two faces;
+// the reference's construction puts material 0 on both (its Salome face meshes carry no
+// material ids, Library/Math.h:91-147, MsFEM_Grid.h:4848, :4905), which
+// msfem_cells_set_face_material(c, 1) selects.
 #include <cub/cub.cuh>
 
 #include <algorithm>

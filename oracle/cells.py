@@ -6,8 +6,9 @@ The reference builds 8 vector basis functions per cell, one per macro vertex v:
   edges  (MsFEM_Grid.h:5061-5200): on each of the 12 cell edges a 1-D elasticity
          problem (FEM::FEM_1D_forElasticDeformation, FEM/FEM.h:3796) with the
          Point (1,1,1) at one end and 0 at the other, over the fine segments on
-         the edge; each segment takes the material of the first face triangle
-         that holds it (:4900-4925);
+         the edge; each segment takes the material id of the first face triangle
+         that holds it (:4900-4925), which is 0: the face triangles come from the
+         cell's Salome face files, read without material ids;
   faces  (:5205-5340): on each of the 6 faces a 2-D elasticity problem
          (FEM_2D_forElasticDeformation, FEM/FEM.h:4367) over the fine triangles on
          the face, Dirichlet data on the face border from the two edge solutions
@@ -28,8 +29,12 @@ MsFEM_Grid.h does.
 
 Cell conventions shared with the GPU path: vertex b of the box
 [x0,x1]x[y0,y1]x[z0,z1] sits at (x_{b&1}, y_{(b>>1)&1}, z_{(b>>2)&1}); face f
-(0..5) is x=x0, x=x1, y=y0, y=y1, z=z0, z=z1; an edge segment takes its material
-from the triangle on the lower-numbered of the edge's two faces.
+(0..5) is x=x0, x=x1, y=y0, y=y1, z=z0, z=z1.  Face and edge materials: order1_bases'
+face_material="cells" (the GPU default) gives a face triangle its tetrahedron's material and an
+edge segment that of its triangle on the lower-numbered of the edge's two faces;
+face_material="zero" is the reference's construction (material 0 on both; its face meshes come
+from Salome files without material ids) and equals the reference's own bases
+(tests/test_msfem_reference.py).
 """
 from __future__ import annotations
 
