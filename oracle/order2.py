@@ -448,7 +448,8 @@ def run_reference(workdir, vertex_xyz, cell_vertex, cells, matrices=True, timeou
     el = recs[4][0].reshape(nc, 1 + 27 + 6)
     res = {"n": head, "edges": recs[2][0].reshape(-1, 2), "faces": recs[3][0], "cell_dofs": el[:, 1:28],
            "cell_faces": el[:, 28:], "K": [k.reshape(81, 81) for k in recs.get(5, [])], "bases": [],
-           "solution": recs[6][0].reshape(-1, 3) if 6 in recs else None}
+           "solution": recs[6][0].reshape(-1, 3) if 6 in recs else None,
+           "portrait": recs[7][0] if 7 in recs else None}
     for c in range(nc):
         sub = os.path.join(fine, f"Elem_{c}", "SubElem_0")
         res["bases"].append(np.stack([np.loadtxt(os.path.join(sub, f"BasisFunction_{b}.txt")).reshape(-1, 3)

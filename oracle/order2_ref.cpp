@@ -18,7 +18,8 @@
  * MsFEM/MsFEM.h:14-569) with the Dirichlet groups of bc_file (text: n_groups, then per group
  * `take_x take_y take_z  vx vy vz  n  v_0 .. v_{n-1}`, the vertex lists and masked constant
  * values MsFEM/MsFEM_Main.cpp:187-300 reads from its kraev1 file) and no Neumann data, and adds
- *   tag 6: the solution, 3 doubles per macro DOF.
+ *   tag 6: the solution, 3 doubles per macro DOF;
+ *   tag 7: the driver system's block portrait (per DOF row: n_down, its columns, n_up, its columns).
  * --order1 (with --driver) runs the Order1 driver instead (MsFEM_forElasticDeformation_OrderBF1_forPoly,
  * MsFEM/MsFEM.h:571-1062, on Grid_forMech_Poly_Order1): tag 6 holds 3 doubles per macro vertex,
  * and only tag 6 is written.
@@ -143,6 +144,7 @@ int main(int argc, char** argv)
     std::vector<Dirichlet> first;
     std::vector<Neumann> second;
     std::vector<Point<double>> solution;
+    CSSD_Matrix<Tensor2Rank3D, Point<double>> order2_slae;
     if (bc_file) {
         FILE* fb = fopen(bc_file, "r");
         if (!fb) return 4;
@@ -166,7 +168,7 @@ int main(int argc, char** argv)
             };
         }
         fclose(fb);
-        CSSD_Matrix<Tensor2Rank3D, Point<double>> slae;
+        CSSD_Matrix<Tensor2Rank3D, Point<double>>& slae = order2_slae;
         if (order1) {
             auto* g1 = new MsFEM::Grid_forMech_Poly_Order1();
             g1->is_print_logFile = false;
@@ -254,6 +256,16 @@ int main(int argc, char** argv)
         }
     }
     if (bc_file) {
+        // tag 7: the block portrait of the driver's system, per DOF row: n_down, its columns, n_up,
+        // its columns (CSSD_Matrix id_column_for_A_down / id_column_for_A_up)
+        std::vector<int> port;
+        for (int i = 0; i < (int)order2_slae.id_column_for_A_down.size(); i++) {
+            port.push_back((int)order2_slae.id_column_for_A_down[i].size());
+            for (int c : order2_slae.id_column_for_A_down[i]) port.push_back(c);
+            port.push_back((int)order2_slae.id_column_for_A_up[i].size());
+            for (int c : order2_slae.id_column_for_A_up[i]) port.push_back(c);
+        }
+        put(f, 7, port);
         std::vector<double> sol;
         for (auto& p : solution) {
             sol.push_back(p.x);
