@@ -18,7 +18,7 @@ from . import _lib
 from ._lib import (BICGSTAB, CG, ELASTIC, FP32_IR, FP64, GMRES, MINRES, PCG_JACOBI, ROW_AND_COLUMN, ROW_ONLY, SCALAR,
                    Stats, check, load)
 
-__all__ = ["System", "Csr", "fem_scalar_driver", "fem_elastic_driver", "CG", "PCG_JACOBI", "BICGSTAB", "GMRES", "MINRES",
+__all__ = ["System", "Csr", "fem_scalar_driver", "fem_scalar3_driver", "fem_elastic_driver", "CG", "PCG_JACOBI", "BICGSTAB", "GMRES", "MINRES",
            "FP64", "FP32_IR", "ROW_ONLY", "ROW_AND_COLUMN", "SCALAR", "ELASTIC"]
 
 
@@ -308,3 +308,18 @@ def fem_elastic_driver(p, method=PCG_JACOBI, precision=FP64, min_residual=1e-10,
                                                 precision, min_residual, maxiter, P(sol), C.byref(st)),
                "fem_elastic_driver")
     return sol, st.as_dict(), rc
+
+
+def fem_scalar3_driver(xyz, tets, S, M, f, bc_nodes, bc_values, min_residual=1e-10, maxiter=200000):
+    """The three-coefficient FEM::FEM_forBaseEliptic (FEM/FEM.h:206-397) on the GPU: the element loop
+    with stiffness, mass and source coefficients per tetrahedron (msfem_assemble_scalar3), Dirichlet
+    rows only (X = F = value, the columns left, FEM.h:291-310; later duplicates win), BiCGStab in
+    FP64 to ||F - A x|| <= min_residual ||F||.  Returns (solution, rel_residual, iterations, rc)."""
+    S_ = System(SCALAR, np.asarray(xyz, dtype=np.float64), np.asarray(tets, dtype=np.int32))
+    try:
+        S_.assemble_scalar3(S, M, f)
+        S_.apply_dirichlet(np.asarray(bc_nodes, dtype=np.int32), np.asarray(bc_values, dtype=np.float64), ROW_ONLY)
+        rel, it, rc = S_.solve(BICGSTAB, FP64, tol=min_residual, maxiter=maxiter)
+        return S_.get_x(), rel, it, rc
+    finally:
+        S_.close()

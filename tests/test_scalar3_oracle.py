@@ -8,9 +8,13 @@ import oracle
 from multiscalefemsolver3d_b200 import meshgen
 from oracle import scalar3
 
-pytestmark = pytest.mark.skipif(not oracle.ref_available(), reason="oracle/_ref not built")
 
 
+
+needs_ref = pytest.mark.skipif(not oracle.ref_available(), reason="oracle/_ref not built")
+
+
+@needs_ref
 def test_element_matches_reference():
     R = oracle.ref()
     rng = np.random.default_rng(3)
@@ -23,6 +27,7 @@ def test_element_matches_reference():
         np.testing.assert_allclose(F, Fr, rtol=0, atol=1e-12 * np.abs(Fr).max())
 
 
+@needs_ref
 def test_driver_matches_reference():
     """6^3 jittered cube, per-element coefficients, u = 1 on x = 0 and 0 on x = 1 (rows only)."""
     R = oracle.ref()
@@ -38,3 +43,50 @@ def test_driver_matches_reference():
     x = scalar3.driver(m.xyz, m.tets, S, M, f, nodes, vals)
     xr = R.scalar3_driver(m.xyz, m.tets, S, M, f, nodes, vals, min_residual=1e-13)
     assert np.linalg.norm(x - xr) <= 1e-9 * np.linalg.norm(xr)
+
+
+def test_driver_orchestration_with_stand_in(monkeypatch, lib):
+    """fem.fem_scalar3_driver end to end with its GPU system replaced by a stand-in that assembles
+    with the restated element, applies rows-only Dirichlet data and solves exactly: the glue hands
+    the coefficients, rows and solve through as the reference driver does."""
+    from multiscalefemsolver3d_b200 import fem
+
+    class FakeSystem:
+        def __init__(self, kind, xyz, tets, material=None):
+            assert kind == fem.SCALAR
+            self.xyz, self.tets = np.asarray(xyz), np.asarray(tets)
+            n = self.xyz.shape[0]
+            self.A, self.F = np.zeros((n, n)), np.zeros(n)
+
+        def assemble_scalar3(self, S, M, f):
+            for e, t in enumerate(self.tets):
+                A, Fe = scalar3.local(self.xyz[t], S[e], M[e], f[e])
+                self.A[np.ix_(t, t)] += A
+                self.F[t] += Fe
+
+        def apply_dirichlet(self, dofs, values, mode):
+            assert mode == fem.ROW_ONLY
+            for i, v in zip(dofs, values):
+                self.A[i, :] = 0.0
+                self.A[i, i] = 1.0
+                self.F[i] = v
+
+        def solve(self, method, precision, tol, maxiter):
+            assert method == fem.BICGSTAB and precision == fem.FP64
+            self.x = np.linalg.solve(self.A, self.F)
+            return 0.0, 1, 0
+
+        def get_x(self):
+            return self.x
+
+        def close(self):
+            pass
+
+    monkeypatch.setattr(fem, "System", FakeSystem)
+    m = meshgen.kuhn_cube(4, jitter=0.1, seed=6)
+    rng = np.random.default_rng(8)
+    S, M, f = rng.uniform(0.5, 3.0, m.n_tets), rng.uniform(0.0, 1.0, m.n_tets), rng.uniform(-1, 1, m.n_tets)
+    lo = np.nonzero(m.xyz[:, 2] < 1e-12)[0].astype(np.int32)
+    x, rel, it, rc = fem.fem_scalar3_driver(m.xyz, m.tets, S, M, f, lo, np.full(lo.size, 0.5))
+    xo = scalar3.driver(m.xyz, m.tets, S, M, f, lo, np.full(lo.size, 0.5))
+    assert rc == 0 and np.linalg.norm(x - xo) <= 1e-12 * np.linalg.norm(xo)
