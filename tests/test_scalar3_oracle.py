@@ -8,9 +8,6 @@ import oracle
 from multiscalefemsolver3d_b200 import meshgen
 from oracle import scalar3
 
-
-
-
 needs_ref = pytest.mark.skipif(not oracle.ref_available(), reason="oracle/_ref not built")
 
 
