@@ -217,7 +217,10 @@ int msfem_bench_spmv(msfem_system_t h, int precision, int reps, double* ms_per_p
  * n_rows to 4,194,304 (larger sizes return MSFEM_ERR_LIMIT).  All calls share that
  * array: calls whose kernels overlap on one GPU race and must be serialised.  The
  * first call on each device looks the array's address up (cudaGetSymbolAddress) with
- * that device current; make it before any stream capture on the calling thread. */
+ * that device current; make it before any stream capture on the calling thread.  Later
+ * calls check the kept address (cudaPointerGetAttributes) and look it up again when it no
+ * longer names device memory of the current device -- after cudaDeviceReset, or with a
+ * different context current -- so such a call is a first call too. */
 int msfem_residual_noalloc(int n_rows, const int32_t* row_ptr, const int32_t* col, const double* val,
                            const double* x, const double* f, double* r, double* rr, void* stream);
 
@@ -313,11 +316,11 @@ int msfem_cells_create(int n_cells, const int64_t* node_off, const double* xyz, 
  * precision / tol / maxiter / threads as for msfem_batch_solve. */
 int msfem_cells_build_bases(msfem_cells_t c, int precision, double tol, int maxiter, int threads);
 
-/* Materials of the Order1 face and edge problems: mode 0 (default) -- each face triangle and edge
- * segment takes the material of the tetrahedra it bounds; mode 1 -- material 0 everywhere, which
- * is what the reference computes: its face meshes come from Salome files whose ReadFromSalomeDat
- * leaves every material id 0 (Library/Math.h:91-147; MsFEM_Grid.h:4848, the edge segments copy the
- * face ids, :4905).  Takes effect at the next msfem_cells_build_bases. */
+/* Materials of the Order1 face and edge problems: mode 1 (the default) -- material 0 everywhere,
+ * which is what the reference computes: its face meshes come from Salome files whose
+ * ReadFromSalomeDat leaves every material id 0 (Library/Math.h:91-147; MsFEM_Grid.h:4848, the edge
+ * segments copy the face ids, :4905); mode 0 -- each face triangle and edge segment takes the
+ * material of the tetrahedra it bounds.  Takes effect at the next msfem_cells_build_bases. */
 int msfem_cells_set_face_material(msfem_cells_t c, int mode);
 
 /* bases: [n_nodes][8][3] doubles, node-major (the reference's self_basis_functions[v][node]

@@ -98,8 +98,9 @@ class Cells:
         return check(load().msfem_cells_build_bases(self.h, precision, tol, maxiter, threads), "cells_build_bases")
 
     def set_face_material(self, mode: str):
-        """"cells" (default): face triangles and edge segments take their tetrahedra's material;
-        "zero": material 0 everywhere, as the reference's construction computes."""
+        """"zero" (default): material 0 on the face and edge problems, as the reference's
+        construction computes; "cells": face triangles and edge segments take their tetrahedra's
+        material."""
         check(load().msfem_cells_set_face_material(self.h, {"cells": 0, "zero": 1}[mode]), "cells_set_face_material")
 
     def bases(self):

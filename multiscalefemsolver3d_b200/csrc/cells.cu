@@ -21,11 +21,11 @@
 //
 // Cell conventions: vertex b at (x_{b&1}, y_{(b>>1)&1}, z_{(b>>2)&1}); face f
 // (0..5) = x0, x1, y0, y1, z0, z1; the vertices of a face in increasing b.  Materials of the
-// face and edge problems: by default a face triangle takes the material of the tetrahedron it
-// bounds and an edge segment that of its triangle on the lower-numbered of the edge's two faces;
-// the reference's construction puts material 0 on both (its Salome face meshes carry no
-// material ids, Library/Math.h:91-147, MsFEM_Grid.h:4848, :4905), which
-// msfem_cells_set_face_material(c, 1) selects.
+// face and edge problems: by default material 0 on both, as the reference's construction computes
+// (its Salome face meshes carry no material ids, Library/Math.h:91-147, MsFEM_Grid.h:4848, and the
+// edge segments copy the face ids, :4905); msfem_cells_set_face_material(c, 0) instead gives a
+// face triangle the material of the tetrahedron it bounds and an edge segment that of its triangle
+// on the lower-numbered of the edge's two faces.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -1569,6 +1569,8 @@ int msfem_cells_create(int n_cells, const int64_t* node_off, const double* xyz, 
     MSFEM_CK(cudaGetDevice(&h->device));
     MSFEM_CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     MSFEM_TRY(cells_create(n_cells, node_off, xyz, tet_off, tets, material, box, n_materials, E, nu, *h));
+    // the reference's convention: material 0 on the face and edge problems
+    MSFEM_TRY(set_face_materials(*h, 1));
     *out = h.release();
     return MSFEM_OK;
 }

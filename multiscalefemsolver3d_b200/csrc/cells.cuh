@@ -38,7 +38,8 @@ struct CellsHandle {
     int cap = 0;
     bool vols_assembled = false;  // volume problem matrices hold the current materials
     // materials of the face triangles and edge segments: 0 = those of the tetrahedra they bound,
-    // 1 = material 0 everywhere (the reference's Salome face meshes carry no materials)
+    // 1 = material 0 everywhere (the reference's Salome face meshes carry no materials).  The
+    // face batch is built in mode 0; msfem_cells_create then switches to mode 1, the default.
     int face_material = 0;
     DBuf<int32_t> face_emat_cells;  // the cells' face-triangle materials, kept while mode 1 is on
     DBuf<int32_t> edge_nodes, edge_len, seg_tri;

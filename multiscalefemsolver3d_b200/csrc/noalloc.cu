@@ -21,6 +21,10 @@
 //  * the first call on a device (with that device current) looks up the
 //    array's device address with cudaGetSymbolAddress; make that first call
 //    before any stream capture is in progress on the calling thread.
+//  * the address is kept per device ordinal and checked on every call with
+//    cudaPointerGetAttributes; when it no longer names device memory of the
+//    current device (after cudaDeviceReset, or under another context) it is
+//    looked up again, so that call is a set-up call too.
 #include <mutex>
 
 #include "devutil.cuh"
@@ -76,6 +80,16 @@ int scratch_address(double** out)
         return MSFEM_ERR_LIMIT;
     }
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (g_scratch_addr[dev]) {
+        // the cached address belongs to the context that was current at look-up; after a device
+        // reset or under a different context it may name nothing, or other memory
+        cudaPointerAttributes a{};
+        const cudaError_t e = cudaPointerGetAttributes(&a, g_scratch_addr[dev]);
+        if (e != cudaSuccess || a.type != cudaMemoryTypeDevice || a.device != dev) {
+            (void)cudaGetLastError();  // a failed query must not surface as the launch's error
+            g_scratch_addr[dev] = nullptr;
+        }
+    }
     if (!g_scratch_addr[dev]) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);

@@ -30,11 +30,11 @@ MsFEM_Grid.h does.
 Cell conventions shared with the GPU path: vertex b of the box
 [x0,x1]x[y0,y1]x[z0,z1] sits at (x_{b&1}, y_{(b>>1)&1}, z_{(b>>2)&1}); face f
 (0..5) is x=x0, x=x1, y=y0, y=y1, z=z0, z=z1.  Face and edge materials: order1_bases'
-face_material="cells" (the GPU default) gives a face triangle its tetrahedron's material and an
-edge segment that of its triangle on the lower-numbered of the edge's two faces;
-face_material="zero" is the reference's construction (material 0 on both; its face meshes come
-from Salome files without material ids) and equals the reference's own bases
-(tests/test_msfem_reference.py).
+face_material="zero" (the default, as on the GPU) is the reference's construction (material 0 on
+both; its face meshes come from Salome files without material ids) and equals the reference's own
+bases (tests/test_msfem_reference.py); face_material="cells" gives a face triangle its
+tetrahedron's material and an edge segment that of its triangle on the lower-numbered of the
+edge's two faces.
 """
 from __future__ import annotations
 
@@ -186,13 +186,14 @@ def face_triangles(tets, mat, mask):
     return out
 
 
-def order1_bases(xyz, tets, mat, box, E, nu, solver=None, face_material="cells"):
+def order1_bases(xyz, tets, mat, box, E, nu, solver=None, face_material="zero"):
     """Bases [n_nodes, 8, 3] of one Order1 cell.  solver(dim, xyz, elems, mat, E, nu, bc_nodes, bc_values)
     solves one sub-problem (default: the exact restatement `cell_problem`).  face_material:
-    "cells" -- the face triangles and edge segments take the material of the tetrahedra they
-    bound; "zero" -- material 0 everywhere, as the reference's construction has it (its face
+    "zero" (default) -- material 0 everywhere, as the reference's construction has it (its face
     meshes come from Salome files, whose ReadFromSalomeDat leaves every material id 0,
-    Library/Math.h:91-147, MsFEM_Grid.h:4848, and the edge segments copy the face ids, :4905)."""
+    Library/Math.h:91-147, MsFEM_Grid.h:4848, and the edge segments copy the face ids, :4905);
+    "cells" -- the face triangles and edge segments take the material of the tetrahedra they
+    bound."""
     solve = solver or cell_problem
     xyz = np.asarray(xyz, dtype=np.float64)
     tets = np.asarray(tets, dtype=np.int64)

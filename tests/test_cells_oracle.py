@@ -173,10 +173,10 @@ def test_macro_face_quadrature_matches_reference(ref):
 @pytest.mark.parametrize("spheres", [0, 3])
 def test_msfem_driver_restatement_properties(spheres):
     """The restated macro driver on 8 cells of a cube: the loads add up to traction x area (the
-    bases are a partition of unity) and the Dirichlet vertices keep their values.  On the
-    homogeneous cube the fine solutions of neighbouring cells agree on their shared nodes; with
-    inclusions they need not, since each cell solves its own face problems with the material of its
-    own tetrahedra next to the face (cells.face_triangles), as the reference's cells do."""
+    bases are a partition of unity) and the Dirichlet vertices keep their values.  The fine solutions
+    of neighbouring cells agree on their shared nodes, inclusions or not: with the reference's
+    material 0 on the face and edge problems (face_material="zero"), two cells sharing a face solve
+    the same face problems.  With each cell's own materials on its faces ("cells") they need not."""
     from multiscalefemsolver3d_b200.msfem import cube_macro_boundary
     from oracle import msfem
     p = meshgen.cube_elastic(n=4, jitter=0.0, n_spheres=spheres, contrast=20.0, rmin=0.15, rmax=0.25, sphere_seed=2)
@@ -189,10 +189,10 @@ def test_msfem_driver_restatement_properties(spheres):
     assert np.all(U[fv] == 0)
     if spheres == 0:
         assert np.all(U[:, 2].reshape(3, 9)[1:] < 0)
-        g = cc.cell_node_global
-        ref_u = np.zeros((p.mesh.n_nodes, 3))
-        ref_u[g] = u
-        assert np.abs(ref_u[g] - u).max() <= 1e-9 * np.abs(u).max()
+    g = cc.cell_node_global
+    ref_u = np.zeros((p.mesh.n_nodes, 3))
+    ref_u[g] = u
+    assert np.abs(ref_u[g] - u).max() <= 1e-9 * np.abs(u).max()
 
 
 def test_postprocessing_restatement_matches_reference(ref):

@@ -99,14 +99,21 @@ def test_batched_face_problems_match_oracle(lib, cuda):
     assert np.abs(x - ref).max() <= SOL_TOL * np.abs(ref).max()
 
 
-def test_cell_bases_match_oracle_chain(lib, cuda):
+@pytest.mark.parametrize("face_material", ["zero", "cells", "default"])
+def test_cell_bases_match_oracle_chain(lib, cuda, face_material):
+    """Both face-material conventions against the oracle chain: "zero" (material 0 on the face and
+    edge problems, the reference's construction and the default) and "cells" (their tetrahedra's
+    materials); "default" sets nothing and must give the reference's convention."""
     cm = meshgen.msfem_cells(n_coarse=2, m_choices=(3, 4, 5), seed=11)
     C = Cells(cm)
+    if face_material != "default":
+        C.set_face_material(face_material)
     assert C.build_bases(precision=FP32_IR, tol=1e-10) == 0
     B = C.bases()
+    mode = "zero" if face_material == "default" else face_material
     for c in range(cm.n_cells):
         xyz, tets, mat, box = cm.cell(c)
-        want = ocells.order1_bases(xyz, tets, mat, box, cm.E, cm.nu)
+        want = ocells.order1_bases(xyz, tets, mat, box, cm.E, cm.nu, face_material=mode)
         got = B[cm.node_off[c]:cm.node_off[c + 1]]
         assert np.abs(got - want).max() <= SOL_TOL, (c, np.abs(got - want).max())
     rep = C.report()
@@ -165,8 +172,53 @@ def test_full_size_cell_matches_oracle(lib, cuda, full_cells):
     C = Cells(one)
     assert C.build_bases(precision=FP32_IR, tol=1e-12) == 0
     xyz, tets, mat, box = one.cell(0)
-    want = ocells.order1_bases(xyz, tets, mat, box, one.E, one.nu)
+    want = ocells.order1_bases(xyz, tets, mat, box, one.E, one.nu, face_material="zero")
     assert np.abs(C.bases() - want).max() <= SOL_TOL
+
+
+def test_face_material_switch_round_trip(lib, cuda):
+    """Switching to "cells" and back to "zero" gives the default's bases bit for bit: the switch
+    restores the face batch's materials exactly."""
+    cm = meshgen.msfem_cells(n_coarse=2, m_choices=(3, 4), seed=5)
+    C = Cells(cm)
+    assert C.build_bases(precision=FP64, tol=1e-11) == 0
+    B0 = C.bases()
+    C.set_face_material("cells")
+    assert C.build_bases(precision=FP64, tol=1e-11) == 0
+    B1 = C.bases()
+    C.set_face_material("zero")
+    assert C.build_bases(precision=FP64, tol=1e-11) == 0
+    np.testing.assert_array_equal(C.bases(), B0)
+    assert np.abs(B1 - B0).max() > 1e-6      # the inclusions make the conventions differ
+
+
+def test_order1_bases_and_driver_match_reference_run(lib, cuda):
+    """The reference's own whole Order1 run (tests/golden/msfem_order1.npz, made by oracle/_ref's
+    order2_ref --order1 from MsFEM::MsFEM_forElasticDeformation_OrderBF1_forPoly, MsFEM/MsFEM.h:
+    572-1010, on graded cells with inclusions): the GPU bases of cells 0 and 7 within 1e-8 of the
+    reference's, and the GPU Order1 driver's macro solution within 1e-8 relative L2 of its."""
+    import os
+    import types
+
+    from multiscalefemsolver3d_b200.msfem import msfem_elastic_driver
+    from oracle import order2 as o2
+    d = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "msfem_order1.npz"))
+    vxyz, cv, cm = o2.graded_cells(2, 4, 0.5)
+    assert abs(cm.xyz.sum() - float(d["xyz_sum"])) < 1e-9
+    C = Cells(cm)
+    assert C.build_bases(precision=FP64, tol=1e-12) == 0
+    B = C.bases()
+    for c in (0, 7):
+        got = B[cm.node_off[c]:cm.node_off[c + 1]]
+        assert np.abs(got - d[f"bases_{c}"]).max() <= SOL_TOL, (c, np.abs(got - d[f"bases_{c}"]).max())
+    bot = np.nonzero(np.abs(vxyz[:, 2]) < 1e-12)[0]
+    top = np.nonzero(np.abs(vxyz[:, 2] - 1) < 1e-12)[0]
+    fv = np.concatenate([bot, top]).astype(np.int32)
+    vals = np.concatenate([np.zeros((bot.size, 3)), np.tile([0.01, -0.02, 0.05], (top.size, 1))])
+    cc = types.SimpleNamespace(cells=cm, cell_vertex=cv, n_coarse_vertices=vxyz.shape[0])
+    res = msfem_elastic_driver(cc, fv, vals, np.zeros((0, 2), np.int32), np.zeros((0, 3)), precision=FP64,
+                               tol=1e-13, cell_tol=1e-12, cells=C)
+    assert np.linalg.norm(res.U - d["solution"]) <= 1e-8 * np.linalg.norm(d["solution"])
 
 
 def test_cells_reject_bad_meshes(lib, cuda):

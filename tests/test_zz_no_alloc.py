@@ -63,3 +63,52 @@ def test_noalloc_rejects_sizes_beyond_its_scratch(cuda):
     rc = L.msfem_residual_noalloc(4_194_305, P(i), P(i), P(d), P(d), P(d), P(d), P(d), None)
     assert rc == _lib.MSFEM_ERR_LIMIT
     assert b"4194304" in L.msfem_last_error()
+
+
+def _tridiagonal(n, seed):
+    """CSR of a diagonally dominant tridiagonal matrix with n rows (row i: i-1, i, i+1)."""
+    rng = np.random.default_rng(seed)
+    counts = np.full(n, 3, np.int64)
+    counts[0] = counts[-1] = 2
+    rp = np.zeros(n + 1, np.int64)
+    np.cumsum(counts, out=rp[1:])
+    rows = np.repeat(np.arange(n), counts)
+    k = np.arange(rp[-1]) - rp[rows]
+    col = (rows + k - (rows > 0)).astype(np.int32)
+    val = np.where(col == rows, 4.0, -1.0) + rng.uniform(-0.1, 0.1, col.size)
+    return rp.astype(np.int32), col, val
+
+
+@pytest.mark.parametrize("sizes", [(600_000, 4_194_304, 1_000)])
+def test_noalloc_large_grids_and_the_exact_limit(cuda, sizes):
+    """A call of 600,000 rows (2,344 blocks: the 8-way unrolled partial sum), one of exactly
+    4,194,304 rows (every slot of the fixed scratch), then a small call after the larger ones: r
+    against the residual computed in numpy, ||r||^2 against its exactly rounded sum (math.fsum).
+    The small call must not read partial sums the larger ones left in the shared array."""
+    import math
+
+    import torch
+    L = _lib.load()
+    dev = torch.device("cuda:0")
+    P = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    stream = torch.cuda.current_stream(dev)
+    for k, n in enumerate(sizes):
+        rp, col, val = _tridiagonal(n, seed=k)
+        rng = np.random.default_rng(100 + k)
+        xh = rng.normal(size=n)
+        fh = rng.normal(size=n)
+        t = [torch.from_numpy(a).to(dev) for a in (rp, col, val, xh, fh)]
+        r = torch.empty(n, dtype=torch.float64, device=dev)
+        rr = torch.full((1,), -1.0, dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
+        rc = L.msfem_residual_noalloc(n, *[P(a) for a in t], P(r), P(rr), C.c_void_p(stream.cuda_stream))
+        assert rc == 0, L.msfem_last_error()
+        torch.cuda.synchronize()
+        rows = np.repeat(np.arange(n), np.diff(rp))
+        ax = np.bincount(rows, weights=val * xh[col], minlength=n)
+        r_ref = fh - ax
+        scale = np.abs(val).max() * np.abs(xh).max() * 3 + np.abs(fh).max()
+        np.testing.assert_allclose(r.cpu().numpy(), r_ref, rtol=0, atol=TOL * scale)
+        rr_ref = math.fsum((r_ref * r_ref).tolist())
+        assert abs(rr.item() - rr_ref) <= TOL * rr_ref, (n, rr.item(), rr_ref)
+        del t, r, rr
