@@ -50,13 +50,30 @@ enum msfem_method {
     MSFEM_PCG_JACOBI = 1,  /* the PCG loop of MSG_PreconditioningSSOR (:1302-1398), M = diag(A)    */
     MSFEM_BICGSTAB = 2,    /* Jacobi-preconditioned BiCGStab (the role of BiCG_Stab/BCG_Stab2)      */
     MSFEM_GMRES = 3,       /* restarted GMRES(m), Jacobi-preconditioned (CSSD_Matrix::GMRES role)  */
-    MSFEM_MINRES = 4       /* MINRES on the Jacobi-scaled matrix: for symmetric indefinite systems,
+    MSFEM_MINRES = 4,      /* MINRES on the Jacobi-scaled matrix: for symmetric indefinite systems,
                               which the reference's elasticity assembly produces (its transposed
                               element blocks leave the global matrix symmetric but indefinite) */
+    MSFEM_PCG_SSOR = 5     /* MSG_PreconditioningSSOR (:1302-1398) with the reference's own SSOR
+                              (PrecondorSSOR + SolvePrecondorSSOR_SLAE, :458-547): the off-diagonal
+                              signs flipped, M = (D - wL) D^-1 (D - wU) / (w (2 - w)), w from
+                              msfem_set_ssor_omega (0.75, as both FEM drivers use).  The sweeps are
+                              level scheduled, one launch per level, and give the reference's bits
+                              for each application.  FP64 only.                                   */
 };
 
 enum msfem_precision {
     MSFEM_FP64 = 0,    /* everything in FP64                                                        */
+    MSFEM_FP64_REFERENCE = 2,  /* MSFEM_PCG_SSOR only: FP64 in the reference's operation order -- A x
+                          summed per row as MultiplicationMatrixVector does (CSSD_Matrix.h:395-423:
+                          the upper entries in ascending column order, then the lower ones, then
+                          the diagonal), inner products summed serially in index order
+                          (math::MakeInnerProduct, Library/Math.h:1633-1654), the updates of
+                          MSG_PreconditioningSSOR unfused, its loop test sqrt((r,r)/(F,F)) > E as
+                          written, the returned residual summed as it sums it (:1384-1397) -- so
+                          the iterates, iteration counts and residuals are the reference's bits
+                          (for CSSD lists in ascending column order, as CreationPortrait builds
+                          them).  The serial sums make it a parity mode: about 0.1 ms per inner
+                          product of 30,000 entries.                                             */
     MSFEM_FP32_IR = 1  /* FP32 matrix + FP32 Krylov inner solves inside FP64 iterative refinement:
                           r = F - A x and x accumulate in FP64.  The inner solver is CG on the
                           Jacobi-scaled matrix for MSFEM_PCG_JACOBI, MINRES on it for
@@ -187,6 +204,26 @@ int msfem_copy_f_to_x(msfem_system_t h);
 int msfem_solve(msfem_system_t h, int method, int precision, int restart_m, int maxiter, double tol,
                 double* rel_residual, int* iterations);
 
+/* The SSOR relaxation factor w of MSFEM_PCG_SSOR (PrecondorSSOR(w, ...), CSSD_Matrix.h:458);
+ * 0 < w < 2, default 0.75. */
+int msfem_set_ssor_omega(msfem_system_t h, double omega);
+/* z = M^-1 r with the reference's SSOR (SolvePrecondorSSOR_SLAE, CSSD_Matrix.h:514-547) on the
+ * current matrix: the same bits as the reference's sweeps.  r, z: n_rows doubles. */
+int msfem_ssor_apply(msfem_system_t h, const double* r, double* z, int on_device);
+
+/* The FEM drivers' solve as the reference runs it: a restart loop around `method` with the needed
+ * residual tightened tenfold after each success, a best-solution copy, and X rolled back to the
+ * best solution at the end (loop 0: FEM_forBaseEliptic, FEM/FEM.h:627-695 -- X = F first, targets
+ * 1e-1, 1e-2, ..., up to 6 tries per target, stop when a success does not improve on the best by
+ * 1e-10; loop 1: FEM_forElasticDeformation, FEM/FEM.h:1853-1939 -- targets 1e-2, 1e-3, ..., up to
+ * 5 tries per target).  Each solve runs from the current X with at most n_rows - 1 iterations, as
+ * MSG_PreconditioningSSOR(GetMatrixSize(), ...) does.  The loop ends at min_residual; as in the
+ * reference, a solve that reaches it is not copied into the best solution, so X is the best
+ * solution of the earlier solves.  best_residual: the loop's best true relative residual;
+ * n_solves / iterations: solves run and their iterations in total (any may be NULL). */
+int msfem_solve_driver_loop(msfem_system_t h, int loop, int method, int precision, double min_residual,
+                            double* best_residual, int* n_solves, int* iterations);
+
 /* y = A x in FP64 (CSSD_Matrix::MultiplicationMatrixVector, :395-423) */
 int msfem_spmv(msfem_system_t h, const double* x, double* y, int on_device);
 
@@ -225,6 +262,9 @@ int msfem_residual_noalloc(int n_rows, const int32_t* row_ptr, const int32_t* co
                            const double* x, const double* f, double* r, double* rr, void* stream);
 
 /* One-call drivers: the reference driver sequence on the GPU, host buffers in and out.
+ * With method MSFEM_PCG_SSOR the solve is the reference's own: its SSOR(0.75)-PCG inside its restart
+ * loop (msfem_solve_driver_loop; maxiter is then unused); any other method runs one solve to
+ * min_residual.
  *
  * FEM::FEM_forBaseEliptic, stiffness-only overload (FEM/FEM.h:398-717):
  * create -> assemble (sigma per material) -> Dirichlet rows + column sweep ->
@@ -477,6 +517,13 @@ int msfem_coarse_set_smoother(msfem_coarse_t c, msfem_system_t textbook, int deg
  * msfem_solve_twolevel widened it (x1.5, after a refinement step that raised the residual or
  * broke down; the step is undone and repeated).  Any argument may be NULL. */
 int msfem_coarse_stats(msfem_coarse_t c, int* trilinear_cells, double* lambda_max, int* widened);
+/* Measurement helper (no counterpart in the reference): times `reps` back-to-back launches of one
+ * Chebyshev smoothing step of the multiplicative cycle (the smoother's SpMV with its vector update,
+ * the dominant kernel of msfem_solve_twolevel) with CUDA events on the solve stream after 3 warm-up
+ * launches; reports the mean device time per step and its algorithmic bytes (matrix values in the
+ * stored width and block columns as stored, slice pointers, and 24 bytes of vector traffic per
+ * row), each counted once.  msfem_coarse_set_smoother must have been called. */
+int msfem_coarse_bench_smoother(msfem_coarse_t c, int reps, double* ms_per_step, int64_t* bytes_per_step);
 void msfem_coarse_destroy(msfem_coarse_t c);
 
 /* ---------------------------------------------------------------------------------------

@@ -18,8 +18,9 @@ MSFEM_ERR_ARGUMENT = -1
 MSFEM_ERR_LIMIT = -4
 
 SCALAR, ELASTIC = 0, 1
-CG, PCG_JACOBI, BICGSTAB, GMRES, MINRES = 0, 1, 2, 3, 4
-FP64, FP32_IR = 0, 1
+CG, PCG_JACOBI, BICGSTAB, GMRES, MINRES, PCG_SSOR = 0, 1, 2, 3, 4, 5
+LOOP_SCALAR, LOOP_ELASTIC = 0, 1
+FP64, FP32_IR, FP64_REFERENCE = 0, 1, 2
 ROW_ONLY, ROW_AND_COLUMN = 0, 1
 
 
@@ -70,6 +71,10 @@ _SIGS = [
     ("msfem_copy_f_to_x", C.c_int, [C.c_void_p]),
     ("msfem_solve", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                               C.POINTER(C.c_double), C.POINTER(C.c_int)]),
+    ("msfem_set_ssor_omega", C.c_int, [C.c_void_p, C.c_double]),
+    ("msfem_ssor_apply", C.c_int, [C.c_void_p, _P, _P, C.c_int]),
+    ("msfem_solve_driver_loop", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double,
+                                          C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("msfem_spmv", C.c_int, [C.c_void_p, _P, _P, C.c_int]),
     ("msfem_spmv_scaled32", C.c_int, [C.c_void_p, _P, _P, C.c_int]),
     ("msfem_export_csr", C.c_int, [C.c_void_p, _P, _P, _P, C.c_int]),
@@ -113,6 +118,7 @@ _SIGS = [
     ("msfem_coarse_apply", C.c_int, [C.c_void_p, _P, _P]),
     ("msfem_solve_twolevel", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double, C.POINTER(C.c_double),
                                        C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ("msfem_coarse_bench_smoother", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     ("msfem_coarse_set_smoother", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_int]),
     ("msfem_coarse_stats", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int)]),
     ("msfem_coarse_destroy", None, [C.c_void_p]),

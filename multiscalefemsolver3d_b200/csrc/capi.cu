@@ -453,6 +453,44 @@ int msfem_solve(msfem_system_t h, int method, int precision, int restart_m, int 
     return solve(*as_sys(h), method, precision, restart_m, maxiter, tol, rel_residual, iterations);
 }
 
+int msfem_set_ssor_omega(msfem_system_t h, double omega)
+{
+    MSFEM_TRY(check_handle(h));
+    if (!(omega > 0.0 && omega < 2.0)) {
+        set_error("msfem_set_ssor_omega: omega must lie in (0, 2), got %g", omega);
+        return MSFEM_ERR_ARGUMENT;
+    }
+    as_sys(h)->ssor_omega = omega;
+    return MSFEM_OK;
+}
+
+int msfem_ssor_apply(msfem_system_t h, const double* r, double* z, int on_device)
+{
+    (void)on_device;
+    MSFEM_TRY(check_handle(h));
+    System& s = *as_sys(h);
+    MSFEM_TRY(use_device(s));
+    if (!r || !z) {
+        set_error("msfem_ssor_apply: null vector");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    DBuf<double> buf;
+    MSFEM_TRY(buf.alloc(3 * (size_t)s.n_rows));
+    MSFEM_CK(cudaMemcpyAsync(buf.p, r, sizeof(double) * s.n_rows, cudaMemcpyDefault, s.stream));
+    MSFEM_TRY(ssor_apply(s, buf.p, buf.p + s.n_rows, buf.p + 2 * (size_t)s.n_rows, nullptr));
+    MSFEM_CK(cudaMemcpyAsync(z, buf.p + s.n_rows, sizeof(double) * s.n_rows, cudaMemcpyDefault, s.stream));
+    MSFEM_CK(cudaStreamSynchronize(s.stream));
+    return MSFEM_OK;
+}
+
+int msfem_solve_driver_loop(msfem_system_t h, int loop, int method, int precision, double min_residual,
+                            double* best_residual, int* n_solves, int* iterations)
+{
+    MSFEM_TRY(check_handle(h));
+    MSFEM_TRY(use_device(*as_sys(h)));
+    return driver_loop(*as_sys(h), loop, method, precision, min_residual, best_residual, n_solves, iterations);
+}
+
 int msfem_spmv(msfem_system_t h, const double* x, double* y, int on_device)
 {
     (void)on_device;

@@ -36,9 +36,15 @@ int msfem_fem_scalar_driver(int n_nodes, const double* xyz, int n_tets, const in
     if ((rc = msfem_assemble_scalar(H.h, sigma, n_materials)) < 0) return rc;
     // first boundary condition: rows, then the column sweep (FEM.h:506-619)
     if ((rc = msfem_apply_dirichlet(H.h, n_bc, bc_nodes, bc_values, MSFEM_ROW_AND_COLUMN, 0)) < 0) return rc;
-    // X = F (FEM.h:635), then the solve to MIN_RESIDUAL (FEM.h:641-681)
-    if ((rc = msfem_copy_f_to_x(H.h)) < 0) return rc;
-    int solve_rc = msfem_solve(H.h, method, precision, 30, maxiter, min_residual, nullptr, nullptr);
+    int solve_rc;
+    if (method == MSFEM_PCG_SSOR) {
+        // the reference's own solve: X = F, then SSOR(0.75)-PCG in its restart loop (FEM.h:627-695)
+        solve_rc = msfem_solve_driver_loop(H.h, 0, method, precision, min_residual, nullptr, nullptr, nullptr);
+    } else {
+        // X = F (FEM.h:635), then one solve to MIN_RESIDUAL
+        if ((rc = msfem_copy_f_to_x(H.h)) < 0) return rc;
+        solve_rc = msfem_solve(H.h, method, precision, 30, maxiter, min_residual, nullptr, nullptr);
+    }
     if (solve_rc < 0) return solve_rc;
     if ((rc = msfem_get_x(H.h, solution, 0)) < 0) return rc;
     fill_stats(H.h, stats);
@@ -74,8 +80,11 @@ int msfem_fem_elastic_driver(int n_nodes, const double* xyz, int n_tets, const i
             }
     if ((rc = msfem_apply_dirichlet(H.h, (int)dofs.size(), dofs.data(), vals.data(), MSFEM_ROW_AND_COLUMN, 0)) < 0)
         return rc;
-    // X holds the Dirichlet values and 0 elsewhere, as the reference's newSLAE.X
-    int solve_rc = msfem_solve(H.h, method, precision, 30, maxiter, min_residual, nullptr, nullptr);
+    // X holds the Dirichlet values and 0 elsewhere, as the reference's newSLAE.X; MSFEM_PCG_SSOR runs
+    // the reference's own solve, SSOR(0.75)-PCG in its restart loop (FEM.h:1853-1939)
+    const int solve_rc = method == MSFEM_PCG_SSOR
+                             ? msfem_solve_driver_loop(H.h, 1, method, precision, min_residual, nullptr, nullptr, nullptr)
+                             : msfem_solve(H.h, method, precision, 30, maxiter, min_residual, nullptr, nullptr);
     if (solve_rc < 0) return solve_rc;
     if ((rc = msfem_get_x(H.h, solution, 0)) < 0) return rc;
     fill_stats(H.h, stats);

@@ -152,6 +152,15 @@ struct System {
     // index = log2(chunk / 4)
     std::map<std::string, std::array<cudaGraphExec_t, 8>> graphs;
 
+    // the reference's SSOR (ssor.cu): node rows grouped by the level of the backward (upper) and
+    // forward (lower) triangular sweeps -- rows of one level depend only on earlier levels
+    double ssor_omega = 0.75;        // PrecondorSSOR(0.75, ...) in both FEM drivers
+    DBuf<int32_t> ssor_rows;         // [backward levels | forward levels], node ids
+    std::vector<int> ssor_off_b, ssor_off_f;  // host level offsets into ssor_rows
+    int64_t ssor_nnzb = -1;          // portrait the levels were built for
+    DBuf<double> loop_best;          // the drivers' restart loop: best solution so far
+    bool reference_order = false;    // MSFEM_PCG_SSOR in the reference's operation order (ssor.cu)
+
     bool zero_diag = false;
     bool force_col32 = false;  // keep 32-bit SELL columns even when 16-bit deltas fit
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -180,6 +189,15 @@ int spmv32(System& s, const float* x, float* y);
 int residual64(System& s, const double* x, const double* f, double* r, double* rr_out);
 // ---- Krylov (krylov.cu)
 int solve(System& s, int method, int precision, int restart_m, int maxiter, double tol, double* relres, int* iters);
+int ensure_state(System& s);
+int read_state(System& s);
+// ---- the reference's SSOR preconditioner and its PCG (ssor.cu)
+int ssor_apply(System& s, const double* r, double* z, double* zb, const KState* S);
+int solve_pcg_ssor(System& s, int maxiter, double tol, int* iters);
+int driver_loop(System& s, int loop, int method, int precision, double min_residual, double* best_residual,
+                int* n_solves, int* iterations);
+// ||F - A X|| / ||F|| summed serially in index order, with A X in the reference's row order
+int true_residual_reference(System& s, double* relres);
 // ---- MINRES (minres.cu): on S A S from x = 0 with right-hand side S r (FP64: x += S y) or r (FP32)
 template <class VT, bool SCALE>
 int minres_run(System& s, VT* x, const VT* r, int maxiter, double tol, int stall_unused, int* iters);

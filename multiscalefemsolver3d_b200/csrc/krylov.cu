@@ -449,6 +449,8 @@ struct Timer {
     }
 };
 
+}  // namespace
+
 int ensure_state(System& s)
 {
     if (!s.kstate.p) {
@@ -467,6 +469,8 @@ int read_state(System& s)
     MSFEM_CK(cudaStreamSynchronize(s.stream));
     return MSFEM_OK;
 }
+
+namespace {
 
 // sets S->ff, S->tol2 (= tol^2 * ff), S->maxiter and the stagnation window on the device
 __global__ void k_set_limits(KState* S, double tol, int maxiter, int use_rr_as_ff, int stall_limit)
@@ -764,6 +768,12 @@ int solve(System& s, int method, int precision, int restart_m, int maxiter, doub
         set_error("solve: maxiter must be > 0 and tol >= 0");
         return MSFEM_ERR_ARGUMENT;
     }
+    if (precision != MSFEM_FP64 && precision != MSFEM_FP32_IR &&
+        !(precision == MSFEM_FP64_REFERENCE && method == MSFEM_PCG_SSOR)) {
+        set_error("solve: precision %d is not available for method %d (MSFEM_FP64_REFERENCE is for MSFEM_PCG_SSOR)",
+                  precision, method);
+        return MSFEM_ERR_ARGUMENT;
+    }
     MSFEM_TRY(prepare_sell(s));
     MSFEM_TRY(ensure_state(s));
     s.launches = 0;
@@ -798,6 +808,14 @@ int solve(System& s, int method, int precision, int restart_m, int maxiter, doub
     case MSFEM_BICGSTAB:
         rc = solve_bicgstab64(s, maxiter, tol, &it);
         break;
+    case MSFEM_PCG_SSOR:
+        if (precision != MSFEM_FP64 && precision != MSFEM_FP64_REFERENCE) {
+            set_error("solve: the reference's SSOR-PCG runs in FP64 (precision %d)", precision);
+            return MSFEM_ERR_ARGUMENT;
+        }
+        s.reference_order = precision == MSFEM_FP64_REFERENCE;
+        rc = solve_pcg_ssor(s, maxiter, tol, &it);
+        break;
     case MSFEM_GMRES:
         if (precision == MSFEM_FP32_IR)
             rc = solve_refined(s, INNER_GMRES32, maxiter, tol, &it, &outer, restart_m > 0 ? restart_m : 30);
@@ -810,7 +828,8 @@ int solve(System& s, int method, int precision, int restart_m, int maxiter, doub
     if (rc == MSFEM_ERR_ARGUMENT) set_error("solve: unknown method %d / precision %d", method, precision);
     if (rc < 0) return rc;
     double rel = 0;
-    MSFEM_TRY(true_residual(s, &rel));
+    if (method == MSFEM_PCG_SSOR && precision == MSFEM_FP64_REFERENCE) MSFEM_TRY(true_residual_reference(s, &rel));
+    else MSFEM_TRY(true_residual(s, &rel));
     s.launches += 1;
     s.stats.ms_solve = timer.stop();
     s.stats.iterations = it;

@@ -15,11 +15,12 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _lib
-from ._lib import (BICGSTAB, CG, ELASTIC, FP32_IR, FP64, GMRES, MINRES, PCG_JACOBI, ROW_AND_COLUMN, ROW_ONLY, SCALAR,
-                   Stats, check, load)
+from ._lib import (BICGSTAB, CG, ELASTIC, FP32_IR, FP64, FP64_REFERENCE, GMRES, LOOP_ELASTIC, LOOP_SCALAR, MINRES, PCG_JACOBI, PCG_SSOR,
+                   ROW_AND_COLUMN, ROW_ONLY, SCALAR, Stats, check, load)
 
-__all__ = ["System", "Csr", "fem_scalar_driver", "fem_scalar3_driver", "fem_elastic_driver", "CG", "PCG_JACOBI", "BICGSTAB", "GMRES", "MINRES",
-           "FP64", "FP32_IR", "ROW_ONLY", "ROW_AND_COLUMN", "SCALAR", "ELASTIC"]
+__all__ = ["System", "Csr", "fem_scalar_driver", "fem_scalar3_driver", "fem_elastic_driver", "CG", "PCG_JACOBI",
+           "BICGSTAB", "GMRES", "MINRES", "PCG_SSOR", "LOOP_SCALAR", "LOOP_ELASTIC", "FP64", "FP32_IR", "FP64_REFERENCE", "ROW_ONLY",
+           "ROW_AND_COLUMN", "SCALAR", "ELASTIC"]
 
 
 def _ptr(a, dtype):
@@ -235,6 +236,28 @@ class System:
         rc = check(load().msfem_solve(self.h, method, precision, restart, maxiter, tol, C.byref(rel), C.byref(it)),
                    "solve")
         return rel.value, it.value, rc
+
+    def set_ssor_omega(self, omega: float):
+        """The relaxation factor of PCG_SSOR (PrecondorSSOR(omega, ...); default 0.75)."""
+        check(load().msfem_set_ssor_omega(self.h, float(omega)), "set_ssor_omega")
+
+    def ssor_apply(self, r):
+        """z = M^-1 r with the reference's SSOR (SolvePrecondorSSOR_SLAE) on the current matrix."""
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        z = np.empty(self.n_rows)
+        check(load().msfem_ssor_apply(self.h, r.ctypes.data_as(C.c_void_p), z.ctypes.data_as(C.c_void_p), 0),
+              "ssor_apply")
+        return z
+
+    def solve_driver_loop(self, loop: int, method: int = PCG_SSOR, precision: int = FP64,
+                          min_residual: float = 1e-10):
+        """The reference driver's restart loop around `method` (LOOP_SCALAR: FEM_forBaseEliptic, which
+        sets X = F first; LOOP_ELASTIC: FEM_forElasticDeformation); X ends as the loop's best
+        solution.  Returns (best_residual, n_solves, total_iterations)."""
+        best, ns, it = C.c_double(), C.c_int(), C.c_int()
+        check(load().msfem_solve_driver_loop(self.h, loop, method, precision, min_residual, C.byref(best),
+                                             C.byref(ns), C.byref(it)), "solve_driver_loop")
+        return best.value, ns.value, it.value
 
     def spmv(self, x):
         x = np.ascontiguousarray(x, dtype=np.float64)

@@ -377,3 +377,20 @@ def cube_cells(mesh: Mesh, E, nu, H: int) -> CubeCells:
     return CubeCells(cells=cm, cell_node_global=np.concatenate(cng).astype(np.int32),
                      cell_vertex=np.array(cvert, dtype=np.int32), cell_color=np.array(color, dtype=np.int32),
                      n_coarse_vertices=(nc + 1) ** 3)
+
+
+# ------------------------------------------------------------------ the benchmark workloads
+
+def heterogeneous_elasticity(n: int = 128):
+    """The 128^3 heterogeneous elasticity workload (and its smaller sizes): n^3 hexahedra of six Kuhn
+    tetrahedra on the unit cube, 2000 seeded non-overlapping spheres (radii U(0.015, 0.035),
+    sphere seed 4096) with E contrast 1:100, nu 0.3, u = 0 on z = 0, traction (0, 0, -1) on z = 1.
+    The spheres do not depend on n."""
+    return cube_elastic(n=n, jitter=0.0, n_spheres=2000, contrast=100.0, rmin=0.015, rmax=0.035, sphere_seed=4096)
+
+
+def electrostatics(n: int = 100):
+    """The 100^3 electrostatics workload (and its smaller sizes): permittivity 1, and 100 inside 200
+    seeded non-overlapping spheres (radii U(0.02, 0.06), sphere seed 2024); potential 1 on x = 0 and
+    0 on x = 1."""
+    return cube_scalar(n=n, n_spheres=200, contrast=100.0, rmin=0.02, rmax=0.06, sphere_seed=2024)

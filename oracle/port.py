@@ -131,6 +131,46 @@ class PortLib:
                                   C.byref(it))
         return X, res, it.value
 
+    def driver_loop(self, A, loop, min_residual=1e-10, w=0.75, solver=None):
+        """The FEM drivers' restart loop around SSOR(w)-PCG (loop 0: FEM_forBaseEliptic,
+        FEM/FEM.h:627-695, which sets X = F first; loop 1: FEM_forElasticDeformation,
+        FEM/FEM.h:1853-1939), from X = A.X.  Each solve gets maxiter = n (at most n - 1 iterations) and
+        the needed residual 10^-(ii+1); a solve that reaches min_residual is not copied into the best
+        solution (the reference breaks before the copy), and X ends as the best solution.  Returns
+        (X, best_residual, [(needed, residual, iterations) per solve]).  solver(A, X, maxiter, tol)
+        -> (X, residual, iterations) replaces the solve (default: this restatement's SSOR-PCG)."""
+        solve = solver or (lambda B, X, maxiter, tol: self.pcg_ssor(B, X0=X, maxiter=maxiter, tol=tol, w=w))
+        X = _c(A.X, np.float64).copy()
+        best = X.copy()
+        if loop == 0:
+            X = _c(A.F, np.float64).copy()
+        current, best_res = 1.0, 1e25
+        max_steps, ii = (5, 0) if loop == 0 else (4, 1)
+        log = []
+        i = 0
+        while i <= max_steps:
+            needed = 10.0 ** (-1 * (ii + 1))
+            if loop == 1 or current > needed:
+                X, res, it = solve(A, X, A.n, needed)
+                current = abs(res)
+                log.append((needed, current, it))
+            stop = False
+            if current < needed:
+                i = 0
+                ii += 1
+                if loop == 0 and current > best_res + 1e-10:
+                    stop = True
+            if not stop and current <= min_residual:
+                best_res = current
+                stop = True
+            if stop:
+                break
+            if current < best_res:
+                best_res = current
+                best = X.copy()
+            i += 1
+        return best, best_res, log
+
     def ssor_apply(self, A, r, w=0.75):
         z = np.zeros(A.n)
         self.L.fo_ssor_apply(A.n, _c(A.row_ptr, np.int32), _c(A.col, np.int32), _c(A.val, np.float64), w,

@@ -38,3 +38,27 @@ def test_c1_assembled_system_checksums(cuda):
     assert np.abs(A.val).sum() == pytest.approx(float(d["val_abs_sum"]), rel=1e-12)
     assert np.linalg.norm(A.val) == pytest.approx(float(d["val_fro"]), rel=1e-12)
     np.testing.assert_allclose(A.F, d["F"], rtol=0, atol=1e-10 * np.abs(d["F"]).max())  # see test_golden.py
+
+
+def test_c2_60_against_the_reference_driver_output(cuda, port):
+    """The electrostatics workload at 60^3 (226,981 DOF, 200 spheres eps 1:100) against the
+    reference's own FEM_forBaseEliptic output (tests/golden/scalar_c2_n60.npz, made by
+    tests/golden/make_workload_solutions.py).  That output is the reference's restart loop's best
+    solution, whose last solve (the one reaching 1e-10) is dropped, so it is 2.7e-7 from the
+    converged solution (measured against the C restatement's Jacobi-PCG to 1e-13).  Checked: the
+    GPU's tight solve within 1e-8 of the restatement's tight solve, and both the GPU's tight solve
+    and the GPU running the reference's own solve (SSOR-PCG restart loop in the reference's operation
+    order) within 1e-6 of the reference's output."""
+    d = np.load(os.path.join(G, "scalar_c2_n60.npz"))
+    p = meshgen.electrostatics(int(d["n"]))
+    assert abs(p.mesh.xyz.sum() - float(d["xyz_sum"])) < 1e-9
+    xr = d["x"]
+    x, stats, rc = fem.fem_scalar_driver(p, method=fem.PCG_JACOBI, precision=fem.FP64, min_residual=1e-12)
+    assert rc == 0
+    A = port.scalar_system(p, stage=1)
+    xo, res_o, _ = port.pcg_jacobi(A, X0=A.F.copy(), maxiter=100000, tol=1e-13)
+    assert np.linalg.norm(x - xo) <= 1e-8 * np.linalg.norm(xo)
+    assert np.linalg.norm(x - xr) <= 1e-6 * np.linalg.norm(xr)
+    x2, stats2, rc2 = fem.fem_scalar_driver(p, method=fem.PCG_SSOR, precision=fem.FP64_REFERENCE, min_residual=1e-10)
+    assert rc2 == 0
+    assert np.linalg.norm(x2 - xr) <= 1e-6 * np.linalg.norm(xr)
