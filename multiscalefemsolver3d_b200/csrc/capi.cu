@@ -588,7 +588,7 @@ int msfem_bench_spmv(msfem_system_t h, int precision, int reps, double* ms_per_p
     // stores: 2 bytes for 16-bit column deltas, else 4), row structure once, x and y once
     if (bytes_per_product) {
         const int64_t nnz_alg = s.nnzb * s.bs * s.bs;
-        const int64_t cw = (s.sell.col16.p && !fp32) ? 2 : 4;
+        const int64_t cw = (s.sell.col16.p && (!fp32 || s.sell.fp32_col16 == 1)) ? 2 : 4;
         if (s.bs == 1)
             *bytes_per_product = nnz_alg * (int64_t)(w + cw) + (int64_t)(n + 1) * 4 + 2 * (int64_t)n * w;
         else

@@ -83,6 +83,10 @@ struct Sell {
     DBuf<float> val32;  // Jacobi-scaled copy, D^-1/2 A D^-1/2, for the FP32 inner solves
     bool pattern_ok = false;
     bool values_ok = false;
+    // FP32 product on the 16-bit column deltas: -1 not yet tuned, 0 no, 1 yes (timed once per
+    // portrait: the FP32 product is gather-latency bound, so fewer bytes need not be faster)
+    int fp32_col16 = -1;
+    float tune_ms[2] = {0.f, 0.f};  // FP32 product time with 32-bit columns / 16-bit deltas
 };
 
 // Device-resident scalars of a Krylov solve.  Written by the last block of the

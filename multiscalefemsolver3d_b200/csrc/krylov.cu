@@ -198,6 +198,123 @@ __global__ void __launch_bounds__(kVecThreads) k_pcg_p(int n, const VT* z, VT* _
         p[i] = z[i] + beta * p[i];
 }
 
+// ------------------------------------------------------------------ FP32 CG in two kernels
+// The FP32 inner solve of the refinement runs CG in the Chronopoulos-Gear arrangement, which needs
+// one reduction phase per iteration instead of two:
+//   w = A r,  gamma = (r, r),  delta = (w, r)                      (k_cg2_spmv)
+//   beta = gamma / gamma_old,  alpha = gamma / (delta - beta gamma / alpha_old)
+//   p = r + beta p,  s = w + beta s,  x += alpha p,  r -= alpha s   (k_cg2_update)
+// k_cg2_spmv only writes per-block partial sums; every block of k_cg2_update adds the partials in
+// the same fixed order (so all blocks hold the same scalars, bit for bit) and block 0 records the
+// state.  The scalars of the previous iteration live in one of two slots (parity passed by the
+// host), so no block reads a value that block 0 overwrites in the same launch.
+// Slot layout in KState::mr: [5 * slot + 0] gamma, +1 alpha, +2 iterations, +3 lowest (r, r),
+// +4 iterations since (r, r) last set a 2 % low.
+
+__global__ void __launch_bounds__(256) k_cg2_spmv(SellView<float> A, const float* __restrict__ r,
+                                                  float* __restrict__ w, const KState* S,
+                                                  double* __restrict__ partial)
+{
+    if (S->done) return;
+    __shared__ double sh[64];
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    double acc[2] = {0.0, 0.0};
+    for (int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; warp < A.n_slices; warp += nw) {
+        if (A.bs == 1) {
+            const float v = sell_row_scalar<float>(A, warp, lane, r);
+            const int row = warp * kSlice + lane;
+            if (row < A.n_rows) {
+                w[row] = v;
+                const double rv = (double)r[row];
+                acc[0] += rv * rv;
+                acc[1] += (double)v * rv;
+            }
+        } else {
+            float v[3];
+            sell_row_block<float>(A, warp, lane, r, v);
+            const int brow = warp * kSlice + lane;
+            if (brow < A.n_brows)
+                for (int c = 0; c < 3; c++) {
+                    const int64_t i = 3 * (int64_t)brow + c;
+                    w[i] = v[c];
+                    const double rv = (double)r[i];
+                    acc[0] += rv * rv;
+                    acc[1] += (double)v[c] * rv;
+                }
+        }
+    }
+    block_sum<2>(acc, sh);
+    if (threadIdx.x == 0) {
+        partial[blockIdx.x] = acc[0];
+        partial[gridDim.x + blockIdx.x] = acc[1];
+    }
+}
+
+// first = 1: the start (beta = 0, p = r, s = w); slot: the parity of the previous scalars
+__global__ void __launch_bounds__(kVecThreads) k_cg2_update(int n, float* __restrict__ x, float* __restrict__ r,
+                                                            const float* __restrict__ w, float* __restrict__ p,
+                                                            float* __restrict__ s, KState* S,
+                                                            const double* __restrict__ partial, int g_spmv, int slot,
+                                                            int first)
+{
+    if (S->done) return;
+    __shared__ double sh[64];
+    __shared__ double sc[4];  // alpha, beta, done
+    double t[2];
+    reduce_partials<2>(partial, g_spmv, g_spmv, t, sh);
+    if (threadIdx.x == 0) {
+        const double gamma = t[0], delta = t[1];
+        const double* old = S->mr + 5 * slot;
+        const int iter = first ? 0 : (int)old[2];
+        double rr_min = first ? gamma : old[3];
+        int stall = first ? 0 : (int)old[4];
+        if (!first) {
+            if (gamma < 0.98 * rr_min) {
+                rr_min = gamma;
+                stall = 0;
+            } else {
+                stall += 1;
+            }
+        }
+        double beta = first ? 0.0 : gamma / old[0];
+        const double den = first ? delta : delta - beta * gamma / old[1];
+        const double alpha = gamma / den;
+        int done = 0;
+        if (gamma <= S->tol2) done = 1;
+        else if (iter >= S->maxiter) done = 2;
+        else if (!(den != 0.0) || den != den || gamma != gamma) done = 3;  // breakdown
+        else if (stall >= S->stall_limit) done = 4;  // FP32 attainable accuracy reached
+        sc[0] = alpha;
+        sc[1] = beta;
+        sc[2] = done;
+        if (blockIdx.x == 0) {
+            double* nw = S->mr + 5 * (1 - slot);
+            nw[0] = gamma;
+            nw[1] = alpha;
+            nw[2] = done ? iter : iter + 1;
+            nw[3] = rr_min;
+            nw[4] = stall;
+            S->rr = gamma;
+            S->iter = done ? iter : iter + 1;
+            if (done == 3) S->breakdown = 1;
+            if (done) S->done = done;
+        }
+    }
+    __syncthreads();
+    if (sc[2] != 0.0) return;
+    const float alpha = (float)sc[0], beta = (float)sc[1];
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float ri = r[i], wi = w[i];
+        const float pi = first ? ri : ri + beta * p[i];
+        const float si = first ? wi : wi + beta * s[i];
+        p[i] = pi;
+        s[i] = si;
+        x[i] += alpha * pi;
+        r[i] = ri - alpha * si;
+    }
+}
+
 // generic residual in VT: r = b - A x  (used by the FP32 inner solve with x = 0 -> r = b)
 template <class VT>
 __global__ void __launch_bounds__(kVecThreads) k_copy(int n, const VT* __restrict__ a, VT* __restrict__ b)
@@ -579,6 +696,32 @@ int pcg_run(System& s, PcgVectors<VT> v, int maxiter)
     return run_chunks(s, key, iteration, 3, maxiter);
 }
 
+// FP32 CG (Chronopoulos-Gear, two kernels per iteration) on the Jacobi-scaled FP32 matrix from
+// x = 0: r holds the right-hand side on entry; S->tol2 / maxiter / stall_limit set by the caller.
+// Vectors: x, r, w, p, s (n floats each).
+int cg2_run(System& s, float* x, float* r, float* w, float* p, float* sv, int maxiter)
+{
+    const int n = s.n_rows;
+    KState* S = s.kstate.p;
+    double* part = s.partial.p;
+    const SellView<float> A = sell_view<float>(s);
+    const unsigned g = spmv_grid_of((const void*)k_cg2_spmv, s);
+    MSFEM_CK(cudaMemsetAsync(x, 0, sizeof(float) * n, s.stream));
+    k_cg2_spmv<<<g, 256, 0, s.stream>>>(A, r, w, S, part);
+    k_cg2_update<<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, x, r, w, p, sv, S, part, (int)g, 1, 1);
+    MSFEM_CK(cudaGetLastError());
+    s.launches += 2;
+    int parity = 0;  // slot of the scalars the next update reads: the first update wrote slot 0
+    auto iteration = [&]() {
+        k_cg2_spmv<<<g, 256, 0, s.stream>>>(A, r, w, S, part);
+        k_cg2_update<<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, x, r, w, p, sv, S, part, (int)g, parity, 0);
+        parity ^= 1;
+    };
+    // every captured chunk holds an even number of iterations, so each replay starts on slot 0
+    const std::string key = graph_key("cg2_32", {x, r, w, p, sv, A.val, A.col, (const void*)S, part}, n);
+    return run_chunks(s, key, iteration, 2, maxiter);
+}
+
 int true_residual(System& s, double* relres)
 {
     double* r = s.work64.p;
@@ -633,7 +776,7 @@ int solve_refined(System& s, Inner inner, int maxiter, double tol, int* iters, i
     }
     if (inner != INNER_MINRES64) {
         // GMRES: d, r, then the (m+1) basis vectors and w
-        MSFEM_TRY(s.work32.alloc((inner == INNER_GMRES32 ? (size_t)restart_m + 4 : 4) * (size_t)n));
+        MSFEM_TRY(s.work32.alloc((inner == INNER_GMRES32 ? (size_t)restart_m + 4 : 5) * (size_t)n));
         d32 = s.work32.p;
         r32 = d32 + n;
         p32 = r32 + n;
@@ -682,8 +825,8 @@ int solve_refined(System& s, Inner inner, int maxiter, double tol, int* iters, i
                 k_dot_self<float><<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, r32, s.partial.p, &S->ticket[1], &S->rr);
                 k_set_limits<<<1, 32, 0, s.stream>>>(S, tau, maxiter - total_inner, 1, kInnerStall);
                 s.launches += 2;
-                PcgVectors<float> v{d32, r32, r32, p32, q32, nullptr};  // unit diagonal: z = r
-                MSFEM_TRY((pcg_run<float, false>(s, v, maxiter - total_inner)));
+                // d = x (from 0), r32 = the scaled right-hand side, then w, p, s
+                MSFEM_TRY(cg2_run(s, d32, r32, p32, q32, q32 + n, maxiter - total_inner));
                 MSFEM_TRY(read_state(s));
                 it = s.h_kstate->iter;
                 if (s.h_kstate->breakdown) rc = MSFEM_ERR_NUMERIC;

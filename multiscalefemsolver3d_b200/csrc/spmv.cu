@@ -222,6 +222,38 @@ __global__ void __launch_bounds__(256) k_residual(SellView<double> A, const doub
 
 }  // namespace
 
+// Times the FP32 product with the 32-bit columns and with the 16-bit deltas (3 warm-up and 20
+// timed launches each, on the system's stream) and keeps the faster for every later FP32 product.
+static int tune_fp32_columns(System& s)
+{
+    Sell& S = s.sell;
+    cudaStream_t st = s.stream;
+    DBuf<float> xy;
+    MSFEM_TRY(xy.alloc(2 * (size_t)s.n_rows));
+    MSFEM_CK(cudaMemsetAsync(xy.p, 0, sizeof(float) * 2 * (size_t)s.n_rows, st));
+    cudaEvent_t e[2];
+    MSFEM_CK(cudaEventCreate(&e[0]));
+    MSFEM_CK(cudaEventCreate(&e[1]));
+    const unsigned g = spmv_grid_of((const void*)k_spmv<float>, s);
+    for (int variant = 0; variant < 2; variant++) {
+        S.fp32_col16 = variant;
+        const SellView<float> v = sell_view<float>(s);
+        for (int i = 0; i < 3; i++) k_spmv<float><<<g, 256, 0, st>>>(v, xy.p, xy.p + s.n_rows);
+        MSFEM_CK(cudaEventRecord(e[0], st));
+        for (int i = 0; i < 20; i++) k_spmv<float><<<g, 256, 0, st>>>(v, xy.p, xy.p + s.n_rows);
+        MSFEM_CK(cudaEventRecord(e[1], st));
+        MSFEM_CK(cudaEventSynchronize(e[1]));
+        MSFEM_CK(cudaEventElapsedTime(&S.tune_ms[variant], e[0], e[1]));
+        S.tune_ms[variant] /= 20.f;
+    }
+    cudaEventDestroy(e[0]);
+    cudaEventDestroy(e[1]);
+    MSFEM_CK(cudaGetLastError());
+    S.fp32_col16 = S.tune_ms[1] < S.tune_ms[0] ? 1 : 0;
+    s.total_launches += 46;
+    return MSFEM_OK;
+}
+
 int prepare_sell(System& s)
 {
     Sell& S = s.sell;
@@ -275,6 +307,7 @@ int prepare_sell(System& s)
         }
         S.pattern_ok = true;
         S.values_ok = false;
+        S.fp32_col16 = S.col16.p ? -1 : 0;
         s.total_launches += 2;
     }
     if (!S.values_ok) {
@@ -302,6 +335,7 @@ int prepare_sell(System& s)
         s.zero_diag = h_bad != 0;  // only the Jacobi-preconditioned methods care; they check it
         s.total_launches += 2;
     }
+    if (S.fp32_col16 < 0) MSFEM_TRY(tune_fp32_columns(s));
     return MSFEM_OK;
 }
 
@@ -316,8 +350,8 @@ SellView<VT> sell_view(System& s)
     v.sp = s.sell.slice_ptr.p;
     v.col = s.sell.col.p;
     // 16-bit deltas pay off where the product is bandwidth-bound (FP64); the FP32 product is
-    // bound by gather latency and runs faster on the plain 32-bit columns
-    v.col16 = sizeof(VT) == 8 ? s.sell.col16.p : nullptr;
+    // bound by gather latency, so it uses them only where the timing at set-up says they are faster
+    v.col16 = (sizeof(VT) == 8 || s.sell.fp32_col16 == 1) ? s.sell.col16.p : nullptr;
     if constexpr (sizeof(VT) == 8) v.val = reinterpret_cast<const VT*>(s.sell.val64.p);
     else v.val = reinterpret_cast<const VT*>(s.sell.val32.p);
     return v;

@@ -694,8 +694,11 @@ __global__ void __launch_bounds__(kVecThreads) k_tl_correct(int n, double* __res
 // FP16 values of block column k of a slice sit as 5 half2 words per lane, word p at
 // 5 * blk + 32 p + lane (blk = the slice's first block of the column; word 4 = (v8, 0)): each of
 // the 5 loads is one 128-byte line per warp.
-__device__ __forceinline__ void sell_row_block_mixed(const SellView<float>& A, const __half2* __restrict__ v16, int warp,
-                                                     int lane, const float* __restrict__ x, float (&acc)[3])
+// c16, when set, holds each stored block's column as a 16-bit delta from its block row (the last
+// row for the padding lanes past the end), 2 instead of 4 bytes per block.
+__device__ __forceinline__ void sell_row_block_mixed(const SellView<float>& A, const __half2* __restrict__ v16,
+                                                     const int16_t* __restrict__ c16, int warp, int lane,
+                                                     const float* __restrict__ x, float (&acc)[3])
 {
     if (!v16) {
         sell_row_block<float>(A, warp, lane, x, acc);
@@ -703,11 +706,12 @@ __device__ __forceinline__ void sell_row_block_mixed(const SellView<float>& A, c
     }
     const int64_t base = A.sp[warp];
     const int w = (int)((A.sp[warp + 1] - base) >> 5);
+    const int row0 = min(warp * kSlice + lane, A.n_brows - 1);
     acc[0] = acc[1] = acc[2] = 0.0f;
 #pragma unroll 2
     for (int k = 0; k < w; k++) {
         const int64_t blk = base + (int64_t)k * kSlice;
-        const int c = __ldcs(A.col + blk + lane);
+        const int c = c16 ? row0 + (int)__ldcs(c16 + blk + lane) : __ldcs(A.col + blk + lane);
         const unsigned int* vb = reinterpret_cast<const unsigned int*>(v16) + 5 * blk + lane;
         const float x0 = __ldg(x + 3 * (int64_t)c), x1 = __ldg(x + 3 * (int64_t)c + 1), x2 = __ldg(x + 3 * (int64_t)c + 2);
         float v[10];
@@ -734,6 +738,25 @@ __global__ void k_to_half(int64_t stored, const float* __restrict__ a, __half2* 
         for (int e = 0; e < 9; e++) v[e] = a[9 * blk + 32 * e + l];
         v[9] = 0.0f;
         for (int p = 0; p < 5; p++) h[5 * blk + 32 * p + l] = __floats2half2_rn(v[2 * p], v[2 * p + 1]);
+    }
+}
+
+// block columns of the SELL copy as 16-bit deltas from the block row (overflow -> flag)
+__global__ void k_block_delta16(int n_brows, int n_slices, const int64_t* __restrict__ sp,
+                                const int32_t* __restrict__ col, int16_t* __restrict__ c16, int* overflow)
+{
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    const int slice = row / kSlice, lane = row % kSlice;
+    if (slice >= n_slices) return;
+    const int64_t base = sp[slice];
+    const int w = (int)((sp[slice + 1] - base) / kSlice);
+    const int row0 = min(row, n_brows - 1);
+    for (int k = 0; k < w; k++) {
+        const int64_t pos = base + (int64_t)k * kSlice + lane;
+        // lanes past the last row hold zero blocks: any valid column will do, so point them at row0
+        const int d = (row < n_brows ? col[pos] : row0) - row0;
+        if (d < -32768 || d > 32767) atomicExch(overflow, 1);
+        c16[pos] = (int16_t)d;
     }
 }
 
@@ -769,7 +792,7 @@ __global__ void __launch_bounds__(kVecThreads) k_mg_in(int n, const double* __re
 
 // one Chebyshev step: res -= K^ d_prev; d = a d_prev + b res; x += d
 __global__ void __launch_bounds__(256) k_mg_cheb(SellView<float> A, const __half2* __restrict__ v16,
-                                                 const float* __restrict__ dprev,
+                                                 const int16_t* __restrict__ c16, const float* __restrict__ dprev,
                                                  float* __restrict__ d, float* __restrict__ res, float* __restrict__ x,
                                                  float a, float b, const TlState* S)
 {
@@ -778,7 +801,7 @@ __global__ void __launch_bounds__(256) k_mg_cheb(SellView<float> A, const __half
     const int nw = (gridDim.x * blockDim.x) >> 5;
     for (int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; warp < A.n_slices; warp += nw) {
         float kd[3];
-        sell_row_block_mixed(A, v16, warp, lane, dprev, kd);
+        sell_row_block_mixed(A, v16, c16, warp, lane, dprev, kd);
         const int brow = warp * kSlice + lane;
         if (brow < A.n_brows)
             for (int c = 0; c < 3; c++) {
@@ -795,7 +818,7 @@ __global__ void __launch_bounds__(256) k_mg_cheb(SellView<float> A, const __half
 // res = rhat - K^ x; with `start`: also the first post-smoothing step d = res / theta,
 // x2 = x + d (into a second buffer: x is being gathered)
 __global__ void __launch_bounds__(256) k_mg_resid(SellView<float> A, const __half2* __restrict__ v16,
-                                                  const float* __restrict__ rhat,
+                                                  const int16_t* __restrict__ c16, const float* __restrict__ rhat,
                                                   const float* __restrict__ x, float* __restrict__ res,
                                                   float* __restrict__ d, float* __restrict__ x2, float inv_theta,
                                                   const TlState* S, int start)
@@ -805,7 +828,7 @@ __global__ void __launch_bounds__(256) k_mg_resid(SellView<float> A, const __hal
     const int nw = (gridDim.x * blockDim.x) >> 5;
     for (int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; warp < A.n_slices; warp += nw) {
         float kx[3];
-        sell_row_block_mixed(A, v16, warp, lane, x, kx);
+        sell_row_block_mixed(A, v16, c16, warp, lane, x, kx);
         const int brow = warp * kSlice + lane;
         if (brow < A.n_brows)
             for (int c = 0; c < 3; c++) {
@@ -944,6 +967,7 @@ struct CoarseHandle {
     DBuf<double> xkeep;         // X before the current refinement step (restored when the step fails)
     DBuf<float> psi_t, mgv;
     DBuf<__half2> val16;  // FP16 copy of the textbook system's scaled SELL values, paired (when requested)
+    DBuf<int16_t> col16;  // its block columns as 16-bit deltas (empty when some delta does not fit)
     bool half_matrix = false;
     ~CoarseHandle()
     {
@@ -1303,19 +1327,20 @@ void mg_cycle(CoarseHandle& C, const double* z, const double* r2, double* r_out,
     const unsigned gvec = kReduceBlocks;
     const double* s_t = T.dscale.p;
     const __half2* v16 = C.half_matrix ? C.val16.p : nullptr;
+    const int16_t* c16 = C.half_matrix ? C.col16.p : nullptr;
     k_mg_in<<<gvec, kVecThreads, 0, st>>>(n, z, r2, r_out, s_t, rhat, res, dA, x, C.cc, S, lanczos);
     float* d[2] = {dA, dB};
     for (int i = 1; i < C.cheb_deg; i++)
-        k_mg_cheb<<<gsp, 256, 0, st>>>(At, v16, d[(i - 1) & 1], d[i & 1], res, x, C.cc.a[i], C.cc.b[i], S);
-    k_mg_resid<<<gsp, 256, 0, st>>>(At, v16, rhat, x, res, nullptr, nullptr, 0.0f, S, 0);
+        k_mg_cheb<<<gsp, 256, 0, st>>>(At, v16, c16, d[(i - 1) & 1], d[i & 1], res, x, C.cc.a[i], C.cc.b[i], S);
+    k_mg_resid<<<gsp, 256, 0, st>>>(At, v16, c16, rhat, x, res, nullptr, nullptr, 0.0f, S, 0);
     k_tl_restrict<float><<<C.n_cells, 128, 0, st>>>(C.own_ptr.p, C.own.p, C.psi_t.p, res, nullptr, nullptr, C.cpart.p,
                                                     nullptr, S, 0);
     k_tl_gather<<<gridn(C.n_cf), 256, 0, st>>>(C.n_cf, C.dptr.p, C.dent.p, C.cpart.p, C.rc.p, S);
     k_tl_gemv<<<gridn((int64_t)C.n_cf * 32), 256, 0, st>>>(C.n_cf, C.n_pad, C.Cinv.p, C.rc.p, C.ec.p, S);
     k_mg_prolong<<<gvec, kVecThreads, 0, st>>>(C.n_fine, C.owner.p, C.cdof.p, C.psi_t.p, C.ec.p, x, S);
-    k_mg_resid<<<gsp, 256, 0, st>>>(At, v16, rhat, x, res, dA, x2, C.cc.inv_theta, S, 1);
+    k_mg_resid<<<gsp, 256, 0, st>>>(At, v16, c16, rhat, x, res, dA, x2, C.cc.inv_theta, S, 1);
     for (int i = 1; i < C.cheb_deg; i++)
-        k_mg_cheb<<<gsp, 256, 0, st>>>(At, v16, d[(i - 1) & 1], d[i & 1], res, x2, C.cc.a[i], C.cc.b[i], S);
+        k_mg_cheb<<<gsp, 256, 0, st>>>(At, v16, c16, d[(i - 1) & 1], d[i & 1], res, x2, C.cc.a[i], C.cc.b[i], S);
     k_mg_out<<<gvec, kVecThreads, 0, st>>>(n, x2, s_t, lanczos ? r_out : z, y, S, C.partial.p, init);
 }
 
@@ -1469,9 +1494,21 @@ int set_smoother(CoarseHandle& C, System& T, int degree, double ratio, int half_
     C.widened = 0;
     C.text = &T;
     C.half_matrix = half_matrix != 0;
+    C.col16.release();
     if (C.half_matrix) {
         MSFEM_TRY(C.val16.alloc(5 * (size_t)T.sell.stored));
         k_to_half<<<gridn(T.sell.stored), 256, 0, st>>>(T.sell.stored, T.sell.val32.p, C.val16.p);
+        DBuf<int> ovf;
+        MSFEM_TRY(ovf.alloc(1));
+        MSFEM_TRY(C.col16.alloc((size_t)T.sell.stored));
+        MSFEM_CK(cudaMemsetAsync(ovf.p, 0, sizeof(int), st));
+        k_block_delta16<<<gridn((int64_t)T.sell.n_slices * kSlice), 256, 0, st>>>(T.n_nodes, T.sell.n_slices,
+                                                                                  T.sell.slice_ptr.p, T.sell.col.p,
+                                                                                  C.col16.p, ovf.p);
+        int h_ovf = 0;
+        MSFEM_CK(cudaMemcpyAsync(&h_ovf, ovf.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        MSFEM_CK(cudaStreamSynchronize(st));
+        if (h_ovf) C.col16.release();
     }
     MSFEM_CK(cudaGetLastError());
     return MSFEM_OK;
@@ -1700,6 +1737,58 @@ int msfem_coarse_set_smoother(msfem_coarse_t c, msfem_system_t textbook, int deg
     }
     MSFEM_CK(cudaSetDevice(c->fine->device));
     return set_smoother(*c, *reinterpret_cast<System*>(textbook), degree, ratio, half_matrix);
+}
+
+int msfem_coarse_bench_smoother(msfem_coarse_t c, int reps, double* ms_per_step, int64_t* bytes_per_step)
+{
+    using namespace msfem;
+    if (!c || !c->text || reps <= 0 || !ms_per_step || !bytes_per_step) {
+        set_error("msfem_coarse_bench_smoother: bad arguments (set the smoother first)");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    CoarseHandle& C = *c;
+    System& T = *C.text;
+    MSFEM_CK(cudaSetDevice(C.fine->device));
+    cudaStream_t st = C.fine->stream;
+    const int n = T.n_rows;
+    float* res = C.mgv.p + n;
+    float* dA = res + n;
+    float* dB = dA + n;
+    float* x = dB + n;
+    MSFEM_CK(cudaMemsetAsync(C.mgv.p, 0, sizeof(float) * 6 * (size_t)n, st));
+    DBuf<TlState> run;  // a state that is not done, so the kernel does its work
+    MSFEM_TRY(run.alloc(1));
+    MSFEM_CK(cudaMemsetAsync(run.p, 0, sizeof(TlState), st));
+    const SellView<float> At = sell_view<float>(T);
+    const unsigned gsp = spmv_grid_of((const void*)k_mg_cheb, T);
+    const __half2* v16 = C.half_matrix ? C.val16.p : nullptr;
+    const int16_t* c16 = C.half_matrix ? C.col16.p : nullptr;
+    auto step = [&](int i) {
+        k_mg_cheb<<<gsp, 256, 0, st>>>(At, v16, c16, (i & 1) ? dB : dA, (i & 1) ? dA : dB, res, x, C.cc.a[1],
+                                       C.cc.b[1], run.p);
+    };
+    for (int i = 0; i < 3; i++) step(i);
+    cudaEvent_t e0, e1;
+    MSFEM_CK(cudaEventCreate(&e0));
+    MSFEM_CK(cudaEventCreate(&e1));
+    MSFEM_CK(cudaEventRecord(e0, st));
+    for (int i = 0; i < reps; i++) step(i);
+    MSFEM_CK(cudaEventRecord(e1, st));
+    MSFEM_CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    MSFEM_CK(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    MSFEM_CK(cudaGetLastError());
+    *ms_per_step = ms / reps;
+    // matrix values (FP16 pairs: 5 x 4 B per block, FP32: 36 B) and block columns, each once;
+    // slice pointers; per DOF the previous direction (4 B), res read and written (8 B), the new
+    // direction (4 B), x read and written (8 B)
+    const int64_t vb = C.half_matrix ? 20 : 36;
+    const int64_t cb = c16 ? 2 : 4;
+    *bytes_per_step = T.sell.stored * (vb + cb) + (int64_t)(T.sell.n_slices + 1) * 8 + (int64_t)n * 24;
+    T.total_launches += 3 + reps;
+    return MSFEM_OK;
 }
 
 void msfem_coarse_destroy(msfem_coarse_t c)

@@ -117,15 +117,17 @@ class CoarseNet:
 
 
 def train_on_cells(net: CoarseNet, n_cells: int, seed: int = 0, chunk: int = 4096, epochs: int = 20, batch: int = 128,
-                   lr: float = 2e-3, **cell_kw) -> dict:
+                   lr: float = 2e-3, face_material: str = "zero", **cell_kw) -> dict:
     """Generates n_cells training cells (meshgen.sphere_cells), solves their exact bases with the
-    batched cell solver, adds them to the training set and trains `epochs` passes with a cosine
-    learning-rate decay.  Returns timings and the loss curve."""
+    batched cell solver (face and edge problems on `face_material`, Cells.set_face_material), adds
+    them to the training set and trains `epochs` passes with a cosine learning-rate decay.  Returns
+    timings and the loss curve."""
     t0 = time.perf_counter()
     ms_solve = 0.0
     for k, c0 in enumerate(range(0, n_cells, chunk)):
         cm = meshgen.sphere_cells(min(chunk, n_cells - c0), seed=seed * 1000 + k, **cell_kw)
         cells = Cells(cm)
+        cells.set_face_material(face_material)
         rc = cells.build_bases(FP32_IR, 1e-8)
         if rc != 0:
             raise RuntimeError(f"training cells: bases rc={rc}")
@@ -149,14 +151,15 @@ def train_on_cells(net: CoarseNet, n_cells: int, seed: int = 0, chunk: int = 409
 
 
 def learned_bases(net: CoarseNet, cells: Cells, cell_meshes, threshold: float = 1.0, precision=FP32_IR,
-                  tol: float = 1e-8) -> dict:
+                  tol: float = 1e-8, face_material: str = "zero") -> dict:
     """Predicted bases for every cell of `cells`; each cell whose predicted bases leave a volume
     residual above `threshold` (Cells.basis_residual) is re-solved exactly (the batched cell
     solver on those cells only) and its exact bases replace the prediction.  The default 1.0 is
     the residual of the trivial interior extension (psi_I = 0): only predictions worse than that
     fall back.  A lower threshold is not better by itself -- on the sphere workloads the exact
     MsFEM bases make a weaker coarse space for the textbook-operator cycle than the predicted
-    ones, so replacing moderately wrong predictions raised the iteration count."""
+    ones, so replacing moderately wrong predictions raised the iteration count.  face_material: the
+    convention of the exact fallback solves (as the network's training targets were made)."""
     t0 = time.perf_counter()
     ms_pred = net.predict(cells)
     rel = cells.basis_residual()
@@ -164,6 +167,7 @@ def learned_bases(net: CoarseNet, cells: Cells, cell_meshes, threshold: float = 
     ms_fallback = 0.0
     if bad.size:
         sub = Cells(meshgen.subset_cells(cell_meshes, bad))
+        sub.set_face_material(face_material)
         rc = sub.build_bases(precision, tol)
         if rc != 0:
             raise RuntimeError(f"fallback cells: bases rc={rc}")

@@ -55,6 +55,12 @@ class TwoLevel:
         check(load().msfem_coarse_set_smoother(self.h, textbook_system.h, degree, ratio, int(half_matrix)),
               "coarse_set_smoother")
 
+    def bench_smoother(self, reps=100):
+        """(ms per Chebyshev step, algorithmic bytes per step) of the cycle's smoothing kernel."""
+        ms, nb = C.c_double(), C.c_int64()
+        check(load().msfem_coarse_bench_smoother(self.h, reps, C.byref(ms), C.byref(nb)), "coarse_bench_smoother")
+        return ms.value, nb.value
+
     def stats(self):
         """{'trilinear_cells', 'lambda_max', 'widened'}: see msfem_coarse_stats."""
         t, w = C.c_int(), C.c_int()

@@ -692,3 +692,121 @@ double fo_gmres_ref(int n, const int* rp, const int* ci, double* v, double* F, d
     free(V); free(W); free(r); free(Help);
     return sqrt(temp) / Norma_F;
 }
+
+/* ---------------------------------------------------------------------------------------------
+ * MINRES on S A S (S = |diag A|^-1/2) inside FP64 iterative refinement -- not a reference
+ * routine: the CPU counterpart of the GPU's Jacobi MINRES, for matrices that are symmetric but
+ * indefinite (the reference's elasticity assembly), where CG need not converge.  Recurrences as in
+ * Elman, Silvester and Wathen, "Finite Elements and Fast Iterative Solvers", Algorithm 2.4.
+ * ------------------------------------------------------------------------------------------- */
+static double pdot(int n, const double* a, const double* b)
+{
+    double r = 0.0;
+#pragma omp parallel for reduction(+ : r) schedule(static)
+    for (int i = 0; i < n; i++) r += a[i] * b[i];
+    return r;
+}
+
+/* y = S A S x */
+static void scaled_spmv(int n, const int* rp, const int* ci, const double* v, const double* s, const double* x,
+                        double* t, double* y)
+{
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; i++) t[i] = s[i] * x[i];
+    fo_spmv(n, rp, ci, v, t, y);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; i++) y[i] *= s[i];
+}
+
+/* y += solution of (S A S) y = b to ||b - S A S y|| <= tau ||b||, from y = 0; returns iterations */
+static int minres_scaled(int n, const int* rp, const int* ci, const double* v, const double* s, const double* b,
+                         double* y, int maxiter, double tau)
+{
+    double* vp = (double*)calloc((size_t)n, sizeof(double));
+    double* vc = (double*)malloc(sizeof(double) * (size_t)n);
+    double* vn = (double*)malloc(sizeof(double) * (size_t)n);
+    double* wp = (double*)calloc((size_t)n, sizeof(double));
+    double* wc = (double*)calloc((size_t)n, sizeof(double));
+    double* t = (double*)malloc(sizeof(double) * (size_t)n);
+    double g1 = sqrt(pdot(n, b, b));
+    int it = 0;
+    if (g1 == 0.0) goto done;
+    for (int i = 0; i < n; i++) vc[i] = b[i] / g1;
+    double gam = g1, eta = g1, c0 = 1.0, c1 = 1.0, s0 = 0.0, s1 = 0.0;
+    for (it = 0; it < maxiter && fabs(eta) > tau * g1; it++) {
+        scaled_spmv(n, rp, ci, v, s, vc, t, vn);
+        const double del = pdot(n, vn, vc);
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < n; i++) vn[i] -= del * vc[i] + gam * vp[i];
+        const double gn = sqrt(pdot(n, vn, vn));
+        const double a0 = c1 * del - c0 * s1 * gam;
+        const double a1 = sqrt(a0 * a0 + gn * gn);
+        const double a2 = s1 * del + c0 * c1 * gam;
+        const double a3 = s0 * gam;
+        const double cn = a0 / a1, sn = gn / a1;
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < n; i++) {
+            const double wn = (vc[i] - a3 * wp[i] - a2 * wc[i]) / a1;
+            wp[i] = wc[i];
+            wc[i] = wn;
+            y[i] += cn * eta * wn;
+            vp[i] = vc[i];
+            vc[i] = gn > 0.0 ? vn[i] / gn : 0.0;
+        }
+        eta = -sn * eta;
+        gam = gn;
+        c0 = c1;
+        c1 = cn;
+        s0 = s1;
+        s1 = sn;
+        if (gn == 0.0) {
+            it++;
+            break;
+        }
+    }
+done:
+    free(vp); free(vc); free(vn); free(wp); free(wc); free(t);
+    return it;
+}
+
+double fo_minres(int n, const int* rp, const int* ci, const double* v, const double* F, double* X,
+                 int maxiter, double tol, int* iters)
+{
+    double* s = (double*)malloc(sizeof(double) * (size_t)n);
+    double* r = (double*)malloc(sizeof(double) * (size_t)n);
+    double* b = (double*)malloc(sizeof(double) * (size_t)n);
+    double* y = (double*)malloc(sizeof(double) * (size_t)n);
+    for (int i = 0; i < n; i++) {
+        double d = 0.0;
+        for (int p = rp[i]; p < rp[i + 1]; p++)
+            if (ci[p] == i) d = v[p];
+        s[i] = d != 0.0 ? 1.0 / sqrt(fabs(d)) : 1.0;
+    }
+    const double ff = pdot(n, F, F);
+    int total = 0;
+    double rel = 1.0;
+    for (int outer = 0; outer < 30; outer++) {
+        fo_spmv(n, rp, ci, v, X, r);
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < n; i++) r[i] = F[i] - r[i];
+        const double rr = pdot(n, r, r);
+        rel = ff > 0.0 ? sqrt(rr / ff) : sqrt(rr);
+        if (rel <= tol || total >= maxiter) break;
+        /* the reduction still missing, with some margin; at least 1e-14 */
+        double tau = 0.5 * tol / rel;
+        if (tau < 1e-14) tau = 1e-14;
+        if (tau > 0.5) tau = 0.5;
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < n; i++) {
+            b[i] = s[i] * r[i];
+            y[i] = 0.0;
+        }
+        total += minres_scaled(n, rp, ci, v, s, b, y, maxiter - total, tau);
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < n; i++) X[i] += s[i] * y[i];
+    }
+    if (iters) *iters = total;
+    free(s); free(r); free(b); free(y);
+    return rel;
+}
+

@@ -64,6 +64,11 @@ double fo_gmres(int n, const int* rp, const int* ci, const double* v, const doub
 double fo_gmres_ref(int n, const int* rp, const int* ci, double* v, double* F, double* X,
                     int maxiter, double tol, int* iters);                            /* CSSD_Matrix.h:1774-1989, quirks included */
 void fo_ssor_apply(int n, const int* rp, const int* ci, const double* v, double w, const double* r, double* z);
+/* Not in the reference (test infrastructure and the CPU baseline of the elasticity benchmark):
+ * MINRES (Paige-Saunders) on the Jacobi-scaled matrix inside FP64 iterative refinement, OpenMP
+ * products; stops when ||F - A X|| <= tol ||F||.  Returns that relative residual. */
+double fo_minres(int n, const int* rp, const int* ci, const double* v, const double* F, double* X,
+                 int maxiter, double tol, int* iters);
 
 #ifdef __cplusplus
 }

@@ -45,7 +45,8 @@ class PortLib:
         L.fo_gmres.argtypes = sol + [C.c_int, C.c_int, C.c_double, C.POINTER(C.c_int)]
         L.fo_gmres_ref.argtypes = sol + [C.c_int, C.c_double, C.POINTER(C.c_int)]
         L.fo_ssor_apply.argtypes = [C.c_int, _i32p, _i32p, _f64p, C.c_double, _f64p, _f64p]
-        for f in ("fo_cg", "fo_pcg_ssor", "fo_pcg_jacobi", "fo_bicgstab", "fo_gmres", "fo_gmres_ref"):
+        L.fo_minres.argtypes = sol + [C.c_int, C.c_double, C.POINTER(C.c_int)]
+        for f in ("fo_cg", "fo_pcg_ssor", "fo_pcg_jacobi", "fo_bicgstab", "fo_gmres", "fo_gmres_ref", "fo_minres"):
             getattr(L, f).restype = C.c_double
 
     @staticmethod
@@ -114,6 +115,10 @@ class PortLib:
 
     def pcg_jacobi(self, A, X0=None, maxiter=100000, tol=1e-10):
         return self._solve(self.L.fo_pcg_jacobi, A, X0, maxiter, tol)
+
+    def minres(self, A, X0=None, maxiter=1000000, tol=1e-8):
+        """Jacobi-scaled MINRES in FP64 refinement to ||F - AX|| <= tol ||F|| (not a reference routine)."""
+        return self._solve(self.L.fo_minres, A, X0, maxiter, tol)
 
     def bicgstab(self, A, X0=None, maxiter=100000, tol=1e-10):
         return self._solve(self.L.fo_bicgstab, A, X0, maxiter, tol)

@@ -20,9 +20,11 @@ def pytest_configure(config):
 
 
 def _ensure_oracle():
+    """Builds the oracle libraries when missing; oracle/Makefile builds the reference harness too
+    when it finds the reference's sources (MSFEM_REFERENCE_DIR or its default)."""
     port = os.path.join(ROOT, "oracle", "_build", "libfemoracle.so")
     ref = os.path.join(ROOT, "oracle", "_ref", "libfemref.so")
-    if not os.path.exists(port) or (not os.path.exists(ref) and os.path.isdir("/root/reference")):
+    if not os.path.exists(port) or not os.path.exists(ref):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
 
 
