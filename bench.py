@@ -548,12 +548,33 @@ def cells_config(cm, extra=None):
          "tol": TOL, "solver": "one persistent launch per problem kind: MINRES on the Jacobi-scaled free block, "
                                "FP32 inner solves with FP64 residual refinement (FP64 fallback per cell)",
          "l2": "flushed between steps (256 MiB write); the per-cell vectors and matrices exceed L2",
-         "face_material": "face and edge problems on the materials of the tetrahedra they bound (the reference's "
-                          "own construction puts material 0 there; --face-material zero; same cost)",
+         "face_material": "material 0 on the face and edge problems, as the reference's own construction",
          "parallelism": "replicas"}
     if extra:
         c.update(extra)
     return c
+
+
+def cells_oracle_error(cm, B, face_material):
+    """The GPU bases of the first cell of resolution 8 and of 12 against the restated Order1 chain
+    (oracle/cells.py: every sub-problem solved exactly by sparse LU; pinned to the reference's own
+    construction): the largest absolute difference (the bases are O(1)), and the oracle's own
+    relative residual of the GPU bases in the cell's volume problems."""
+    from oracle import cells as ocells
+    out = {"oracle": "oracle/cells.py order1_bases (sparse LU per sub-problem)", "cells": []}
+    for m in (8, 12):
+        idx = np.nonzero(cm.m == m)[0]
+        if idx.size == 0:
+            continue
+        c = int(idx[0])
+        xyz, tets, mat, box = cm.cell(c)
+        want = ocells.order1_bases(xyz, tets, mat, box, cm.E, cm.nu, face_material=face_material)
+        got = B[cm.node_off[c]:cm.node_off[c + 1]]
+        K = ocells.assemble(xyz, tets, mat, cm.E, cm.nu)
+        bnd = np.nonzero(ocells.face_masks(xyz, box))[0]
+        out["cells"].append({"cell": c, "m": m, "max_abs_err": float(np.abs(got - want).max()),
+                             "oracle_rel_residual_max": float(ocells.residual(K, got, bnd).max())})
+    return out
 
 
 def kuhn_blocks(m):
@@ -571,8 +592,7 @@ def run_cells(args, D):
     dev = torch.device("cuda", D.local)
     cm = cells_workload()
     C = Cells(cm)
-    if args.face_material != "cells":
-        C.set_face_material(args.face_material)
+    C.set_face_material(args.face_material)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     for _ in range(args.warmup):
         C.build_bases(FP32_IR, TOL)
@@ -604,6 +624,9 @@ def run_cells(args, D):
     ach = algo / (vol_ms * 1e-3) / 1e9
     peak, peak_kind = peaks()
     tuned = int(rep["threads"]["volumes"])  # the e2e calls reuse the CTA size tuned above
+    check = None
+    if D.rank == 0 and not args.no_oracle_check:
+        check = cells_oracle_error(cm, C.bases(), args.face_material)
     C.close()
 
     # e2e: create (topology + portraits) + build + bases copied back, host (pinned) buffers
@@ -620,6 +643,8 @@ def run_cells(args, D):
         _lib.check(L.msfem_cells_create(cm.n_cells, P(h[0]), P(h[1]), P(h[2]), P(h[3]), P(h[4]), P(h[5]),
                                         h[6].numel(), P(h[6]), P(h[7]), 0, C_.byref(hh)), "cells_create")
         try:
+            _lib.check(L.msfem_cells_set_face_material(hh, {"cells": 0, "zero": 1}[args.face_material]),
+                       "cells_set_face_material")
             rc = L.msfem_cells_build_bases(hh, FP32_IR, TOL, 5000, tuned)
             if rc != 0:
                 raise RuntimeError(f"cells build rc={rc}")
@@ -645,8 +670,11 @@ def run_cells(args, D):
                  "refinement_steps_mean": float(rep["outer"].mean()), "rel_residual_max": float(rep["rel"].max()),
                  "face_rel_residual_max": float(rep["face_rel"].max()), "step_ms_all": ts,
                  "autotuned_cta_threads": rep["threads"]}
-        if args.face_material != "cells":
-            extra["face_material"] = "material 0 on the face and edge problems, as the reference's own construction"
+        extra["face_material"] = ("material 0 on the face and edge problems, as the reference's own construction"
+                                  if args.face_material == "zero" else
+                                  "face and edge problems on the materials of the tetrahedra they bound")
+        if check:
+            extra["err_vs_oracle"] = check
         line = {"metric": METRIC, "value": ms, "unit": UNIT, "n_gpus": D.world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
                 "vs_baseline": None, "dtype": "fp32-in-f64-ir", "data": "synthetic",
@@ -1089,7 +1117,10 @@ def run_xfem(args, D):
     S.close()
     cpu = None
     if D.rank == 0 and not args.no_cpu_baseline:
-        cpu = xfem_cpu_baseline(args.n, 40)
+        cpu = xfem_cpu_baseline(args.n)
+    check = None
+    if D.rank == 0 and not args.no_oracle_check:
+        check = xfem_oracle_error()
     peak, peak_kind = peaks()
     ach = b32 / (spmv32_ms * 1e-3) / 1e9
     if D.rank == 0:
@@ -1104,6 +1135,8 @@ def run_xfem(args, D):
              "plain_fp64_gmres_iterations": it64, "plain_fp64_gmres_rel_residual": rel64,
              "plain_fp64_gmres_reached_tol": bool(rc64 == 0), "spmv_fp32_ms": spmv32_ms, "spmv_fp32_gbs": ach,
              "step_ms_all": ts}
+        if check:
+            c["err_vs_oracle"] = check
         c.update(info)
         line = {"metric": METRIC, "value": ms, "unit": UNIT, "n_gpus": D.world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
@@ -1116,6 +1149,28 @@ def run_xfem(args, D):
                 "note": "step timed on the host clock around synchronised GPU work (several streams); the step "
                         "already copies the mesh and crack data from host arrays, e2e adds the solution's read-back"}
         print(json.dumps(line))
+
+
+def xfem_oracle_error(n=32):
+    """Relative L2 errors of the GPU's enriched system solves (GMRES(50), FP32 Krylov in FP64
+    refinement, to 1e-8 and to 1e-11) against the restatement's exact sparse-LU solution of the
+    same workload at n^3 (oracle/xfem.py: its own side volumes, cut detection and assembly)."""
+    import oracle.xfem as ox
+    from multiscalefemsolver3d_b200 import fem, xfem
+    mesh, cr, nodes, vals = xfem.cube_cracked(n=n, n_cracks=50, seed=5)
+    enr_o = ox.enrich(mesh.xyz, mesh.tets, cr)
+    A = ox.assemble(mesh.xyz, mesh.tets, np.ones(mesh.n_tets), cr, enr_o)
+    xo = ox.solve_dirichlet(A, nodes, vals)
+    out = {"oracle": "oracle/xfem.py assembly + sparse LU (FP64)", "n": n, "n_dofs": int(xo.size)}
+    for tol, key in ((TOL, "rel_l2_tol_1e-8"), (1e-11, "rel_l2_tol_1e-11")):
+        S, _ = xfem.build_system(mesh, cr)
+        S.apply_dirichlet(nodes, vals, fem.ROW_AND_COLUMN)
+        S.copy_f_to_x()
+        rel, it, rc = S.solve(fem.GMRES, fem.FP32_IR, tol=tol, maxiter=200000, restart=50)
+        x = S.get_x()
+        S.close()
+        out[key] = float(np.linalg.norm(x - xo) / np.linalg.norm(xo))
+    return out
 
 
 def xfem_cpu_baseline(n_full, ladder=(24, 32, 40)):

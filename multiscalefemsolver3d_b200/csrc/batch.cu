@@ -784,13 +784,13 @@ int batch_build_pattern(BatchSys& b, const double* d_xyz)
     return 0;
 }
 
-int batch_assemble(BatchSys& b, const double* d_xyz, const double* d_lame, int n_mat)
+int batch_assemble_enqueue(BatchSys& b, const double* d_xyz, const double* d_lame, int n_mat)
 {
     cudaStream_t st = b.stream;
     MSFEM_TRY(b.val64.alloc(std::max<int64_t>(1, 9 * b.nnzb)));
     MSFEM_TRY(b.val32.alloc(std::max<int64_t>(1, 9 * b.nnzb)));
     MSFEM_TRY(b.dscale.alloc(std::max<int64_t>(1, 3 * b.n_nodes)));
-    DBuf<int> flag;
+    DBuf<int>& flag = b.aflag;
     MSFEM_TRY(flag.alloc(1));
     MSFEM_CK(cudaMemsetAsync(flag.p, 0, sizeof(int), st));
     const int blocks = (int)std::min<int64_t>((b.nnzb + 255) / 256, 148 * 16);
@@ -808,8 +808,15 @@ int batch_assemble(BatchSys& b, const double* d_xyz, const double* d_lame, int n
         k_batch_val32<<<nblk, 256, 0, st>>>(b.n_nodes, b.row_ptr.p, b.col.p, b.val64.p, b.dscale.p, b.val32.p);
     }
     MSFEM_CK(cudaGetLastError());
+    return 0;
+}
+
+int batch_assemble(BatchSys& b, const double* d_xyz, const double* d_lame, int n_mat)
+{
+    MSFEM_TRY(batch_assemble_enqueue(b, d_xyz, d_lame, n_mat));
+    cudaStream_t st = b.stream;
     int bad = 0;
-    MSFEM_CK(cudaMemcpyAsync(&bad, flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MSFEM_CK(cudaMemcpyAsync(&bad, b.aflag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     MSFEM_CK(cudaStreamSynchronize(st));
     if (bad) {
         set_error("batched systems: material id out of range");
@@ -900,6 +907,13 @@ int autotune(BatchSys& b, double* d_x, int start64, double tol, int maxiter)
 }
 
 }  // namespace
+
+int batch_threads(const BatchSys& b, int precision, int threads)
+{
+    if (b.n_sys == 0) return 256;
+    if (threads > 0) return threads;
+    return (b.tuned_threads != 0 && b.tuned_precision == precision) ? b.tuned_threads : 0;
+}
 
 int batch_solve(BatchSys& b, double* d_x, int precision, double tol, int maxiter, int threads)
 {

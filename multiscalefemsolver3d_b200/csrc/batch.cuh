@@ -48,17 +48,23 @@ struct BatchSys {
     std::vector<float> tune_ms;                   // trial times of the candidates 128/256/384/512
     int64_t work_stride = 0;
     float last_ms = 0.f;
+    DBuf<int> aflag;  // set by the assembly when an element's material id is out of range
 };
 
 // pattern: elems/emat/node_off/elem_off/fixed filled; builds row_ptr, col, cstart, contrib
 int batch_build_pattern(BatchSys& b, const double* d_xyz);
 // values from the current materials (lame: [n_mat][2] lambda, mu on the device)
 int batch_assemble(BatchSys& b, const double* d_xyz, const double* d_lame, int n_mat);
+// the same launches without waiting for them (no host synchronisation, no allocation once the
+// buffers exist): capturable into a CUDA graph; a bad material id is left in b.aflag
+int batch_assemble_enqueue(BatchSys& b, const double* d_xyz, const double* d_lame, int n_mat);
 // values from caller-given element blocks [n_elems][k1][k1][9] (device)
 int batch_assemble_given(BatchSys& b, const double* d_eblocks);
 // solves every system; x: [n_nodes][R][3] FP64, fixed entries hold the Dirichlet data on
 // entry, free entries are overwritten.  precision: MSFEM_FP64 or MSFEM_FP32_IR.  threads <= 0:
 // the CTA size is autotuned on the first call (cached per batch and precision).
 int batch_solve(BatchSys& b, double* d_x, int precision, double tol, int maxiter, int threads);
+// the CTA size batch_solve would use with `threads` (0 when the autotuner has not run yet)
+int batch_threads(const BatchSys& b, int precision, int threads);
 
 }  // namespace msfem

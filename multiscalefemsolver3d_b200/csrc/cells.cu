@@ -965,15 +965,17 @@ int set_face_materials(CellsHandle& h, int mode)
     return MSFEM_OK;
 }
 
-int cells_build(CellsHandle& h, int precision, double tol, int maxiter, int threads)
+// The launches of one Order1 build, in order: both assemblies, the closed-form edges, the face
+// problems' Dirichlet data, the face batch, the volume problems' Dirichlet data, the volume batch.
+// `tf` / `tv`: the face / volume CTA sizes (0: batch_solve autotunes, which synchronises).
+int cells_enqueue(CellsHandle& h, int precision, double tol, int maxiter, int tf, int tv)
 {
     cudaStream_t st = h.stream;
     BatchSys& F = h.faces;
     BatchSys& V = h.vols;
     MSFEM_CK(cudaEventRecord(h.ev[0], st));
-    MSFEM_TRY(batch_assemble(F, h.fxyz.p, h.lame.p, h.n_mat));
-    MSFEM_TRY(batch_assemble(V, h.xyz.p, h.lame.p, h.n_mat));
-    h.vols_assembled = true;
+    MSFEM_TRY(batch_assemble_enqueue(F, h.fxyz.p, h.lame.p, h.n_mat));
+    MSFEM_TRY(batch_assemble_enqueue(V, h.xyz.p, h.lame.p, h.n_mat));
     MSFEM_CK(cudaEventRecord(h.ev[1], st));
     MSFEM_CK(cudaMemsetAsync(h.flag.p, 0, sizeof(int), st));
     MSFEM_CK(cudaMemsetAsync(h.prof.p, 0, sizeof(double) * 6 * h.n_nodes, st));
@@ -984,16 +986,71 @@ int cells_build(CellsHandle& h, int precision, double tol, int maxiter, int thre
                                                             h.mask.p, h.vert.p, h.node_off.p, h.n_cells, h.prof.p, h.fx.p);
     MSFEM_CK(cudaGetLastError());
     MSFEM_CK(cudaEventRecord(h.ev[2], st));
-    MSFEM_TRY(batch_solve(F, h.fx.p, precision, tol, maxiter, threads));
+    MSFEM_TRY(batch_solve(F, h.fx.p, precision, tol, maxiter, tf));
     MSFEM_CK(cudaEventRecord(h.ev[3], st));
     k_volume_dirichlet<<<blocks_for(h.n_nodes), 256, 0, st>>>(h.n_nodes, h.mask.p, h.fidx.p, h.fx.p, h.bx.p);
     MSFEM_CK(cudaGetLastError());
-    MSFEM_TRY(batch_solve(V, h.bx.p, precision, tol, maxiter, threads));
+    MSFEM_TRY(batch_solve(V, h.bx.p, precision, tol, maxiter, tv));
     MSFEM_CK(cudaEventRecord(h.ev[4], st));
+    return 0;
+}
+
+int cells_build(CellsHandle& h, int precision, double tol, int maxiter, int threads)
+{
+    cudaStream_t st = h.stream;
+    BatchSys& F = h.faces;
+    BatchSys& V = h.vols;
+    h.vols_assembled = true;
+    const int tf = batch_threads(F, precision, threads), tv = batch_threads(V, precision, threads);
+    const double key[5] = {(double)precision, tol, (double)maxiter, (double)tf, (double)tv};
+    const bool have_graph = h.build_graph && std::memcmp(key, h.build_key, sizeof(key)) == 0;
+    // capture only a build whose launches have run once with this key: every buffer is then
+    // allocated and the CTA sizes tuned, so the capture holds launches and copies only
+    const bool can_capture = tf > 0 && tv > 0 && std::memcmp(key, h.eager_key, sizeof(key)) == 0;
+    if (have_graph || can_capture) {
+        if (!have_graph) {
+            if (h.build_graph) {
+                cudaGraphExecDestroy(h.build_graph);
+                h.build_graph = nullptr;
+            }
+            cudaGraph_t g;
+            MSFEM_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            const int rc = cells_enqueue(h, precision, tol, maxiter, tf, tv);
+            const cudaError_t e = cudaStreamEndCapture(st, &g);
+            if (rc < 0) return rc;
+            if (e != cudaSuccess) {
+                set_error("msfem_cells_build_bases: graph capture failed: %s", cudaGetErrorString(e));
+                return MSFEM_ERR_CUDA;
+            }
+            const cudaError_t ei = cudaGraphInstantiate(&h.build_graph, g, 0);
+            cudaGraphDestroy(g);
+            if (ei != cudaSuccess) {
+                h.build_graph = nullptr;
+                set_error("msfem_cells_build_bases: graph instantiate failed: %s", cudaGetErrorString(ei));
+                return MSFEM_ERR_CUDA;
+            }
+            std::memcpy(h.build_key, key, sizeof(key));
+        }
+        MSFEM_CK(cudaGraphLaunch(h.build_graph, st));
+        h.graph_builds++;
+    } else {
+        // launch by launch (the first build tunes the persistent launches' CTA sizes, which
+        // synchronises); the next build with the same key is captured
+        MSFEM_TRY(cells_enqueue(h, precision, tol, maxiter, tf, tv));
+        const double k2[5] = {(double)precision, tol, (double)maxiter, (double)batch_threads(F, precision, threads),
+                              (double)batch_threads(V, precision, threads)};
+        std::memcpy(h.eager_key, k2, sizeof(k2));
+    }
     MSFEM_CK(cudaStreamSynchronize(st));
     for (int k = 0; k < 4; k++) MSFEM_CK(cudaEventElapsedTime(&h.ms[k], h.ev[k], h.ev[k + 1]));
-    int bad = 0;
+    int bad = 0, bad_f = 0, bad_v = 0;
     MSFEM_TRY(read_flag(st, h.flag, &bad));
+    MSFEM_TRY(read_flag(st, F.aflag, &bad_f));
+    MSFEM_TRY(read_flag(st, V.aflag, &bad_v));
+    if (bad_f || bad_v) {
+        set_error("msfem_cells_build_bases: a material id is out of range");
+        return MSFEM_ERR_ARGUMENT;
+    }
     if (bad) {
         set_error("msfem_cells_build_bases: an edge segment has a material with zero shear modulus");
         return MSFEM_ERR_ARGUMENT;

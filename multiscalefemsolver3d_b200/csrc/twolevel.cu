@@ -742,21 +742,24 @@ __global__ void k_to_half(int64_t stored, const float* __restrict__ a, __half2* 
 }
 
 // block columns of the SELL copy as 16-bit deltas from the block row (overflow -> flag)
+// (grid-stride over the rows: the launch helper caps the grid)
 __global__ void k_block_delta16(int n_brows, int n_slices, const int64_t* __restrict__ sp,
                                 const int32_t* __restrict__ col, int16_t* __restrict__ c16, int* overflow)
 {
-    const int row = blockIdx.x * blockDim.x + threadIdx.x;
-    const int slice = row / kSlice, lane = row % kSlice;
-    if (slice >= n_slices) return;
-    const int64_t base = sp[slice];
-    const int w = (int)((sp[slice + 1] - base) / kSlice);
-    const int row0 = min(row, n_brows - 1);
-    for (int k = 0; k < w; k++) {
-        const int64_t pos = base + (int64_t)k * kSlice + lane;
-        // lanes past the last row hold zero blocks: any valid column will do, so point them at row0
-        const int d = (row < n_brows ? col[pos] : row0) - row0;
-        if (d < -32768 || d > 32767) atomicExch(overflow, 1);
-        c16[pos] = (int16_t)d;
+    const int64_t n_lanes = (int64_t)n_slices * kSlice;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n_lanes; t += (int64_t)gridDim.x * blockDim.x) {
+        const int row = (int)t;
+        const int slice = row / kSlice, lane = row % kSlice;
+        const int64_t base = sp[slice];
+        const int w = (int)((sp[slice + 1] - base) / kSlice);
+        const int row0 = min(row, n_brows - 1);
+        for (int k = 0; k < w; k++) {
+            const int64_t pos = base + (int64_t)k * kSlice + lane;
+            // lanes past the last row hold zero blocks: any valid column will do, so point them at row0
+            const int d = (row < n_brows ? col[pos] : row0) - row0;
+            if (d < -32768 || d > 32767) atomicExch(overflow, 1);
+            c16[pos] = (int16_t)d;
+        }
     }
 }
 

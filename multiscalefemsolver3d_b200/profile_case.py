@@ -8,11 +8,12 @@ Kernel launch order (for ncu -k/-s/-c): portrait and assembly kernels, the
 Dirichlet kernels, the solve (if --solve), then k_spmv<float> x5, then
 k_spmv<double> x5.
 
-    python -m multiscalefemsolver3d_b200.profile_case --twolevel --n 64
+    python -m multiscalefemsolver3d_b200.profile_case --twolevel --n 64 [--maxiter K]
 
-runs the two-level elasticity solve of the 128^3 workload's kind at n^3 (n/8 macro cells per
-axis, spheres scaled with the volume): both assemblies, Dirichlet, the cell bases, coarse setup,
-the multiplicative cycle and FP64 MINRES to 1e-8.
+runs the two-level elasticity solve of the 128^3 workload (meshgen.heterogeneous_elasticity) at
+n^3 (n/8 macro cells per axis): both assemblies, Dirichlet, the exact cell bases, coarse setup,
+the multiplicative cycle and FP64 MINRES to 1e-8 (or K iterations: every iteration launches the
+same kernels, so a launch list of a few hundred iterations shows the solve's mix).
 
     python -m multiscalefemsolver3d_b200.profile_case --cells 8
 
@@ -45,6 +46,7 @@ def main():
     ap.add_argument("--cells", type=int, default=0, help="batched cell bases of cells^3 macro cells")
     ap.add_argument("--net", type=int, default=0, help="network forward passes over this many cells")
     ap.add_argument("--order2", type=int, default=0, help="batched Order2 bases of order2^3 macro cells")
+    ap.add_argument("--maxiter", type=int, default=400000, help="two-level: MINRES iteration limit")
     a = ap.parse_args()
     from . import fem, meshgen
     if a.order2:
@@ -54,7 +56,7 @@ def main():
     if a.cells:
         return cells_case(a.cells)
     if a.twolevel:
-        return twolevel_case(a.n)
+        return twolevel_case(a.n, a.maxiter)
     if a.elastic:
         p = meshgen.cube_elastic(n=a.n, n_spheres=200, contrast=100.0, rmin=0.02, rmax=0.06)
         S = fem.System(fem.ELASTIC, p.mesh.xyz, p.mesh.tets, p.mesh.mat)
@@ -113,15 +115,13 @@ def order2_case(nc):
     C.close()
 
 
-def twolevel_case(n):
+def twolevel_case(n, maxiter=400000):
     import numpy as np
 
     from . import fem, meshgen
     from .cells import FP32_IR, FP64, Cells
     from .twolevel import TwoLevel
-    spheres = max(1, round(2000 * (n / 128.0) ** 3))
-    p = meshgen.cube_elastic(n=n, jitter=0.0, n_spheres=spheres, contrast=100.0, rmin=0.015, rmax=0.035,
-                             sphere_seed=11)
+    p = meshgen.heterogeneous_elasticity(n)
     m = p.mesh
     dofs = (3 * p.bc_nodes[:, None] + np.arange(3)).ravel().astype(np.int32)
     zval = np.zeros(dofs.size)
@@ -134,10 +134,11 @@ def twolevel_case(n):
     K.apply_dirichlet(dofs, zval, fem.ROW_AND_COLUMN)
     cc = meshgen.cube_cells(m, p.E, p.nu, 8)
     C = Cells(cc.cells)
+    C.set_face_material("cells")
     rcb = C.build_bases(FP32_IR, 1e-8)
     T = TwoLevel(S, C, cc, dofs)
     T.set_smoother(K, degree=3, half_matrix=True)
-    rel, it, out, rc = T.solve(tol=1e-8, maxiter=400000, precision=FP64)
+    rel, it, out, rc = T.solve(tol=1e-8, maxiter=maxiter, precision=FP64)
     print(json.dumps({"n": n, "dofs": S.n_rows, "rc_bases": rcb, "rc": rc, "rel": rel, "iterations": it,
                       "ms_solve": S.stats()["ms_solve"]}))
     T.close()

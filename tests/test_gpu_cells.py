@@ -256,3 +256,25 @@ def test_full_size_macro_matrices_translation_free(lib, cuda, full_cells):
     f = np.einsum("cijrs,s->cir", K, np.array([1.0, 1.0, 1.0]))
     # the bases add up to (1,1,1) to the solve's accuracy (ill-conditioned cells: ~1e-4 here)
     assert np.abs(f).max() <= 1e-3 * np.abs(K).max()
+
+
+def test_build_graph_replay_is_bit_identical(lib, cuda):
+    """The first build runs launch by launch (and tunes the persistent launches' CTA sizes), the
+    second is captured into a CUDA graph, the third replays it: the same bases, bit for bit, and
+    the oracle chain's within 1e-8; changing the face materials between replays changes values in
+    place, which the replayed graph picks up."""
+    cm = meshgen.msfem_cells(n_coarse=2, m_choices=(3, 4, 5), seed=11)
+    C = Cells(cm)
+    out = []
+    for _ in range(3):
+        assert C.build_bases(precision=FP32_IR, tol=1e-10) == 0
+        out.append(C.bases())
+    np.testing.assert_array_equal(out[0], out[1])
+    np.testing.assert_array_equal(out[0], out[2])
+    C.set_face_material("cells")
+    assert C.build_bases(precision=FP32_IR, tol=1e-10) == 0
+    B = C.bases()
+    for c in range(cm.n_cells):
+        xyz, tets, mat, box = cm.cell(c)
+        want = ocells.order1_bases(xyz, tets, mat, box, cm.E, cm.nu, face_material="cells")
+        assert np.abs(B[cm.node_off[c]:cm.node_off[c + 1]] - want).max() <= SOL_TOL
