@@ -564,8 +564,10 @@ int msfem_net_forward(msfem_net_t n, int cells, const float* vox, float* out);
 int msfem_net_predict(msfem_net_t n, msfem_cells_t c, float* ms);
 /* Tensor-core path of layers 1-3 (forward and data gradient): 0 = warp-level mma.sync, 1 =
  * tcgen05 with TMEM accumulators and M = 64 voxel tiles (N = 32 channels), 2 = tcgen05 on the
- * transposed product (M = 64 channel rows, N = 256 voxels of a plane).  All compute the same
- * function (FP32 accumulation order may differ). */
+ * transposed product (M = 64 channel rows, N = 256 voxels of a plane), 3 = the M = 64 tcgen05
+ * tiles in a persistent warp-specialised kernel (a producer warp fills a ring of plane slots, one
+ * thread issues the MMAs into two TMEM accumulators, four epilogue warps drain them).  All compute
+ * the same function (FP32 accumulation order may differ). */
 int msfem_net_set_tensor_path(msfem_net_t n, int tcgen05);
 int msfem_net_destroy(msfem_net_t n);
 

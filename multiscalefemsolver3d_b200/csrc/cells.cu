@@ -965,33 +965,41 @@ int set_face_materials(CellsHandle& h, int mode)
     return MSFEM_OK;
 }
 
-// The launches of one Order1 build, in order: both assemblies, the closed-form edges, the face
-// problems' Dirichlet data, the face batch, the volume problems' Dirichlet data, the volume batch.
-// `tf` / `tv`: the face / volume CTA sizes (0: batch_solve autotunes, which synchronises).
-int cells_enqueue(CellsHandle& h, int precision, double tol, int maxiter, int tf, int tv)
+// The launches of one stage of the Order1 build: 0 both assemblies, 1 the closed-form edges and
+// the face problems' Dirichlet data, 2 the face batch, 3 the volume problems' Dirichlet data and
+// the volume batch.  `tf` / `tv`: the face / volume CTA sizes (0: batch_solve autotunes, which
+// synchronises).
+int cells_stage(CellsHandle& h, int stage, int precision, double tol, int maxiter, int tf, int tv)
 {
     cudaStream_t st = h.stream;
     BatchSys& F = h.faces;
     BatchSys& V = h.vols;
-    MSFEM_CK(cudaEventRecord(h.ev[0], st));
-    MSFEM_TRY(batch_assemble_enqueue(F, h.fxyz.p, h.lame.p, h.n_mat));
-    MSFEM_TRY(batch_assemble_enqueue(V, h.xyz.p, h.lame.p, h.n_mat));
-    MSFEM_CK(cudaEventRecord(h.ev[1], st));
-    MSFEM_CK(cudaMemsetAsync(h.flag.p, 0, sizeof(int), st));
-    MSFEM_CK(cudaMemsetAsync(h.prof.p, 0, sizeof(double) * 6 * h.n_nodes, st));
-    const int n_edges = 12 * h.n_cells;
-    k_edge_profiles<<<blocks_for(n_edges, 128), 128, 0, st>>>(n_edges, h.cap, h.edge_nodes.p, h.edge_len.p, h.seg_tri.p,
-                                                              F.emat.p, h.lame.p, h.n_mat, h.xyz.p, h.prof.p, h.flag.p);
-    k_face_dirichlet<<<blocks_for(F.n_nodes), 256, 0, st>>>(F.n_nodes, h.fcell_node.p, F.fixed.p, F.node_off.p, F.n_sys,
-                                                            h.mask.p, h.vert.p, h.node_off.p, h.n_cells, h.prof.p, h.fx.p);
-    MSFEM_CK(cudaGetLastError());
-    MSFEM_CK(cudaEventRecord(h.ev[2], st));
-    MSFEM_TRY(batch_solve(F, h.fx.p, precision, tol, maxiter, tf));
-    MSFEM_CK(cudaEventRecord(h.ev[3], st));
-    k_volume_dirichlet<<<blocks_for(h.n_nodes), 256, 0, st>>>(h.n_nodes, h.mask.p, h.fidx.p, h.fx.p, h.bx.p);
-    MSFEM_CK(cudaGetLastError());
-    MSFEM_TRY(batch_solve(V, h.bx.p, precision, tol, maxiter, tv));
-    MSFEM_CK(cudaEventRecord(h.ev[4], st));
+    switch (stage) {
+    case 0:
+        MSFEM_TRY(batch_assemble_enqueue(F, h.fxyz.p, h.lame.p, h.n_mat));
+        MSFEM_TRY(batch_assemble_enqueue(V, h.xyz.p, h.lame.p, h.n_mat));
+        break;
+    case 1: {
+        MSFEM_CK(cudaMemsetAsync(h.flag.p, 0, sizeof(int), st));
+        MSFEM_CK(cudaMemsetAsync(h.prof.p, 0, sizeof(double) * 6 * h.n_nodes, st));
+        const int n_edges = 12 * h.n_cells;
+        k_edge_profiles<<<blocks_for(n_edges, 128), 128, 0, st>>>(n_edges, h.cap, h.edge_nodes.p, h.edge_len.p,
+                                                                  h.seg_tri.p, F.emat.p, h.lame.p, h.n_mat, h.xyz.p,
+                                                                  h.prof.p, h.flag.p);
+        k_face_dirichlet<<<blocks_for(F.n_nodes), 256, 0, st>>>(F.n_nodes, h.fcell_node.p, F.fixed.p, F.node_off.p,
+                                                                F.n_sys, h.mask.p, h.vert.p, h.node_off.p, h.n_cells,
+                                                                h.prof.p, h.fx.p);
+        MSFEM_CK(cudaGetLastError());
+        break;
+    }
+    case 2:
+        MSFEM_TRY(batch_solve(F, h.fx.p, precision, tol, maxiter, tf));
+        break;
+    default:
+        k_volume_dirichlet<<<blocks_for(h.n_nodes), 256, 0, st>>>(h.n_nodes, h.mask.p, h.fidx.p, h.fx.p, h.bx.p);
+        MSFEM_CK(cudaGetLastError());
+        MSFEM_TRY(batch_solve(V, h.bx.p, precision, tol, maxiter, tv));
+    }
     return 0;
 }
 
@@ -1003,40 +1011,51 @@ int cells_build(CellsHandle& h, int precision, double tol, int maxiter, int thre
     h.vols_assembled = true;
     const int tf = batch_threads(F, precision, threads), tv = batch_threads(V, precision, threads);
     const double key[5] = {(double)precision, tol, (double)maxiter, (double)tf, (double)tv};
-    const bool have_graph = h.build_graph && std::memcmp(key, h.build_key, sizeof(key)) == 0;
+    const bool have_graph = h.build_graph[0] && std::memcmp(key, h.build_key, sizeof(key)) == 0;
     // capture only a build whose launches have run once with this key: every buffer is then
     // allocated and the CTA sizes tuned, so the capture holds launches and copies only
     const bool can_capture = tf > 0 && tv > 0 && std::memcmp(key, h.eager_key, sizeof(key)) == 0;
     if (have_graph || can_capture) {
         if (!have_graph) {
-            if (h.build_graph) {
-                cudaGraphExecDestroy(h.build_graph);
-                h.build_graph = nullptr;
-            }
-            cudaGraph_t g;
-            MSFEM_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-            const int rc = cells_enqueue(h, precision, tol, maxiter, tf, tv);
-            const cudaError_t e = cudaStreamEndCapture(st, &g);
-            if (rc < 0) return rc;
-            if (e != cudaSuccess) {
-                set_error("msfem_cells_build_bases: graph capture failed: %s", cudaGetErrorString(e));
-                return MSFEM_ERR_CUDA;
-            }
-            const cudaError_t ei = cudaGraphInstantiate(&h.build_graph, g, 0);
-            cudaGraphDestroy(g);
-            if (ei != cudaSuccess) {
-                h.build_graph = nullptr;
-                set_error("msfem_cells_build_bases: graph instantiate failed: %s", cudaGetErrorString(ei));
-                return MSFEM_ERR_CUDA;
+            for (auto& g : h.build_graph)
+                if (g) {
+                    cudaGraphExecDestroy(g);
+                    g = nullptr;
+                }
+            for (int k = 0; k < 4; k++) {
+                cudaGraph_t g;
+                MSFEM_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                const int rc = cells_stage(h, k, precision, tol, maxiter, tf, tv);
+                const cudaError_t e = cudaStreamEndCapture(st, &g);
+                if (rc < 0) return rc;
+                if (e != cudaSuccess) {
+                    set_error("msfem_cells_build_bases: graph capture failed: %s", cudaGetErrorString(e));
+                    return MSFEM_ERR_CUDA;
+                }
+                const cudaError_t ei = cudaGraphInstantiate(&h.build_graph[k], g, 0);
+                cudaGraphDestroy(g);
+                if (ei != cudaSuccess) {
+                    h.build_graph[k] = nullptr;
+                    set_error("msfem_cells_build_bases: graph instantiate failed: %s", cudaGetErrorString(ei));
+                    return MSFEM_ERR_CUDA;
+                }
             }
             std::memcpy(h.build_key, key, sizeof(key));
         }
-        MSFEM_CK(cudaGraphLaunch(h.build_graph, st));
+        for (int k = 0; k < 4; k++) {
+            MSFEM_CK(cudaEventRecord(h.ev[k], st));
+            MSFEM_CK(cudaGraphLaunch(h.build_graph[k], st));
+        }
+        MSFEM_CK(cudaEventRecord(h.ev[4], st));
         h.graph_builds++;
     } else {
         // launch by launch (the first build tunes the persistent launches' CTA sizes, which
         // synchronises); the next build with the same key is captured
-        MSFEM_TRY(cells_enqueue(h, precision, tol, maxiter, tf, tv));
+        for (int k = 0; k < 4; k++) {
+            MSFEM_CK(cudaEventRecord(h.ev[k], st));
+            MSFEM_TRY(cells_stage(h, k, precision, tol, maxiter, tf, tv));
+        }
+        MSFEM_CK(cudaEventRecord(h.ev[4], st));
         const double k2[5] = {(double)precision, tol, (double)maxiter, (double)batch_threads(F, precision, threads),
                               (double)batch_threads(V, precision, threads)};
         std::memcpy(h.eager_key, k2, sizeof(k2));

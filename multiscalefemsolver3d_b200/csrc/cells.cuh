@@ -54,16 +54,18 @@ struct CellsHandle {
     float ms2[4] = {0, 0, 0, 0};
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     float ms[4] = {0, 0, 0, 0};
-    // the whole Order1 build (assemblies, edges, face batch, volume batch) captured into a CUDA
-    // graph once the persistent launches' CTA sizes are tuned; replayed by later builds with the
-    // same key (precision, tolerance, iteration limit, CTA sizes)
-    cudaGraphExec_t build_graph = nullptr;
+    // the Order1 build's four stages (assemblies, edges, face batch, volume batch) captured into
+    // CUDA graphs once the persistent launches' CTA sizes are tuned; replayed by later builds with
+    // the same key (precision, tolerance, iteration limit, CTA sizes), with the timing events
+    // recorded between the graphs
+    cudaGraphExec_t build_graph[4] = {nullptr, nullptr, nullptr, nullptr};  // one per stage
     double build_key[5] = {0, 0, 0, 0, 0};
     double eager_key[5] = {-1, 0, 0, 0, 0};  // key of the last build run launch by launch
     int graph_builds = 0;  // builds run by replaying the graph
     ~CellsHandle()
     {
-        if (build_graph) cudaGraphExecDestroy(build_graph);
+        for (auto g : build_graph)
+            if (g) cudaGraphExecDestroy(g);
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         if (stream) cudaStreamDestroy(stream);

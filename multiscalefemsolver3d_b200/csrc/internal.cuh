@@ -191,6 +191,8 @@ int prepare_sell(System& s);
 int spmv64(System& s, const double* x, double* y);
 int spmv32(System& s, const float* x, float* y);
 int residual64(System& s, const double* x, const double* f, double* r, double* rr_out);
+// allocates the solver state (KState) zeroed on first use
+int ensure_kstate(System& s);
 // ---- Krylov (krylov.cu)
 int solve(System& s, int method, int precision, int restart_m, int maxiter, double tol, double* relres, int* iters);
 int ensure_state(System& s);

@@ -570,10 +570,7 @@ struct Timer {
 
 int ensure_state(System& s)
 {
-    if (!s.kstate.p) {
-        MSFEM_TRY(s.kstate.alloc(1));
-        MSFEM_CK(cudaMemsetAsync(s.kstate.p, 0, sizeof(KState), s.stream));
-    }
+    MSFEM_TRY(ensure_kstate(s));
     if (!s.h_kstate) MSFEM_CK(cudaMallocHost(&s.h_kstate, sizeof(KState)));
     const unsigned g = spmv_grid(s);
     MSFEM_TRY(s.partial.alloc(std::max<size_t>(3 * (size_t)g, 3 * (size_t)kReduceBlocks) + 64));

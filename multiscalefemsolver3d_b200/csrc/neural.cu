@@ -662,6 +662,270 @@ __global__ void __launch_bounds__(128, 1) k_conv32_tt(const __nv_bfloat16* __res
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;\n" ::"r"(tbase));
 }
 
+// ---- the M = 64 tcgen05 convolution, warp-specialised and persistent.
+// Operands and tiles as k_conv32_tc (planes stored once as [chunk][18 y][18 x] records, weights
+// [chunk][tap][co], per plane 4 M = 64 tiles x 27 taps x 2 k16 steps into TMEM), but the three
+// stages run in different warps and overlap:
+//   warp 4       producer: copies planes -1 .. 16 of each cell into a ring of kWsSlots plane
+//                slots (cp.async; zeros outside the cell), then arrives on the slot's `full`
+//                barrier; it reuses a slot only after the MMAs that read it have completed
+//                (`empty`, signalled by tcgen05.commit);
+//   warp 5       one thread issues the plane's 216 tcgen05.mma into one of two TMEM accumulator
+//                buffers (64 columns each), commits them to `accf[b]` and releases the plane slot
+//                no later MMA reads;
+//   warps 0-3    epilogue: each reads its quadrant of TMEM lanes (tcgen05.ld), hands the buffer
+//                back (`acce[b]`), adds the bias / applies ReLU or the mask and stores the voxels.
+// So the loads of the next planes and the epilogue of plane z overlap the MMAs of plane z + 1.
+// One CTA per SM walks cells blockIdx.x, + gridDim.x, ... with the weights loaded once.  Every
+// wait is bounded: a timeout sets *err, raises a shared abort flag that every role polls, and
+// the CTA still waits (bounded) for its issued MMAs before it frees TMEM.
+constexpr int kWsSlots = 6;
+constexpr int kWsA = kWsSlots * kTcSlot;                   // 124,416 B
+constexpr int kWsBar = kWsA + kTcB;                         // barriers after ring and weights
+constexpr int kWsNBar = 2 * kWsSlots + 2 + 2 + 1;           // full, empty, accf, acce, fin
+constexpr int kWsSmem = kWsBar + 8 * kWsNBar + 16;
+constexpr int kWsThreads = 192;
+constexpr int kWsTmemCols = 128;
+
+__device__ __forceinline__ void mb_init(uint32_t bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count));
+}
+
+__device__ __forceinline__ void mb_arrive(uint32_t bar)
+{
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}\n" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar) : "memory");
+}
+
+// bounded wait on phase `parity` of `bar`; gives up early when another role raised *abort
+__device__ __forceinline__ bool ws_wait(uint32_t bar, uint32_t parity, volatile int* abort)
+{
+    for (int i = 0; i < (1 << 22); i++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if ((i & 255) == 255 && *abort) return false;
+    }
+    *abort = 1;
+    return false;
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(kWsThreads, 1) k_conv32_ws(int n_cells, const __nv_bfloat16* __restrict__ in,
+                                                             const __nv_bfloat16* __restrict__ w,
+                                                             const float* __restrict__ bias,
+                                                             const __nv_bfloat16* __restrict__ mask,
+                                                             __nv_bfloat16* __restrict__ out, float* __restrict__ outf,
+                                                             int* err)
+{
+    extern __shared__ __align__(128) unsigned char sm[];
+    unsigned char* A = sm;
+    unsigned char* B = sm + kWsA;
+    const uint32_t bar0 = smem_u32(sm + kWsBar);
+    auto full = [&](int s) { return bar0 + 8u * s; };
+    auto empty = [&](int s) { return bar0 + 8u * (kWsSlots + s); };
+    auto accf = [&](int b) { return bar0 + 8u * (2 * kWsSlots + b); };
+    auto acce = [&](int b) { return bar0 + 8u * (2 * kWsSlots + 2 + b); };
+    const uint32_t fin = bar0 + 8u * (2 * kWsSlots + 4);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kWsBar + 8 * kWsNBar);
+    volatile int* abort = reinterpret_cast<volatile int*>(sm + kWsBar + 8 * kWsNBar + 4);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        for (int s = 0; s < kWsSlots; s++) {
+            mb_init(full(s), 32);
+            mb_init(empty(s), 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            mb_init(accf(b), 1);
+            mb_init(acce(b), 128);
+        }
+        mb_init(fin, 1);
+        *abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tslot)),
+                     "r"(kWsTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    // weights [chunk][tap][co] x 16 B from w[tap][co][ci], once for all the CTA's cells
+    for (int q = tid; q < kTaps * kCh * 4; q += blockDim.x) {
+        const int row = q >> 2, c = q & 3;
+        cp_async16(smem_u32(B) + (c * kTaps * kCh + row) * 16, w + (size_t)row * kCh + c * 8);
+    }
+    cp_async_wait_all();
+    asm volatile("fence.proxy.async.shared::cta;\n" ::);
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    const uint32_t tbase = *tslot;
+    const int my_cells = blockIdx.x < n_cells ? (n_cells - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+
+    if (warp == 4) {
+        // ---- producer: planes -1 .. 16 of each cell, plane g of the CTA in slot g % kWsSlots
+        for (int k = 0; k < my_cells && !*abort; k++) {
+            const __nv_bfloat16* inc = in + (size_t)(blockIdx.x + (size_t)k * gridDim.x) * kVox * kCh;
+            for (int p = -1; p <= kV; p++) {
+                const int g = 18 * k + p + 1, s = g % kWsSlots, use = g / kWsSlots;
+                if (use > 0 && !ws_wait(empty(s), (use - 1) & 1, abort)) break;
+                for (int q = lane; q < 4 * 18 * 18; q += 32) {
+                    const int c = q / 324, hy = (q / 18) % 18, hx = q % 18;
+                    const int gy = hy - 1, gx = hx - 1;
+                    const uint32_t off = s * kTcSlot + c * kTcChunk + (hy * 18 + hx) * 16;
+                    if (p >= 0 && p < kV && gy >= 0 && gy < kV && gx >= 0 && gx < kV)
+                        cp_async16(smem_u32(A) + off, inc + ((size_t)((p * kV + gy) * kV + gx) * kCh + c * 8));
+                    else
+                        *reinterpret_cast<uint4*>(A + off) = make_uint4(0, 0, 0, 0);
+                }
+                cp_async_wait_all();
+                asm volatile("fence.proxy.async.shared::cta;\n" ::);
+                mb_arrive(full(s));
+            }
+        }
+    } else if (warp == 5) {
+        // ---- MMA issuer
+        if (lane == 0) {
+            const uint32_t a0 = smem_u32(A), b0 = smem_u32(B);
+            int issued = 0;
+            for (int k = 0; k < my_cells && !*abort; k++) {
+                bool ok = true;
+                for (int z = 0; z < kV && ok; z++) {
+                    // planes z - 1, z, z + 1 of the cell: g = 18 k + z .. 18 k + z + 2
+                    for (int g = 18 * k + (z == 0 ? 0 : z + 2); g <= 18 * k + z + 2 && ok; g++)
+                        ok = ws_wait(full(g % kWsSlots), (g / kWsSlots) & 1, abort);
+                    const int t = 16 * k + z, b = t & 1, use = t >> 1;
+                    if (ok && use > 0) ok = ws_wait(acce(b), (use - 1) & 1, abort);
+                    if (!ok) break;
+                    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+                    const uint32_t dcol = tbase + 64u * b;
+                    for (int yb = 0; yb < 2; yb++)
+                        for (int hh = 0; hh < 2; hh++)
+                            for (int tap = 0; tap < kTaps; tap++) {
+                                const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
+                                const int slot = (18 * k + z + dz) % kWsSlots;
+                                for (int kc = 0; kc < 2; kc++) {
+                                    const uint32_t aoff =
+                                        slot * kTcSlot + 2 * kc * kTcChunk + ((8 * yb + dy) * 18 + 8 * hh + dx) * 16;
+                                    const uint32_t boff = (2 * kc * kTaps + tap) * kCh * 16;
+                                    tc_mma(dcol + ((uint32_t)(16 * hh) << 16) + 32 * yb,
+                                           tc_desc(a0 + aoff, kTcChunk, kTcRow), tc_desc(b0 + boff, kTaps * kCh * 16, 128),
+                                           (tap | kc) != 0);
+                                }
+                            }
+                    issued = 1;
+                    tc_commit(accf(b));
+                    // plane z - 1 is read by no later MMA; after the last plane, neither are z, z + 1
+                    tc_commit(empty((18 * k + z) % kWsSlots));
+                    if (z == kV - 1) {
+                        tc_commit(empty((18 * k + z + 1) % kWsSlots));
+                        tc_commit(empty((18 * k + z + 2) % kWsSlots));
+                    }
+                }
+            }
+            // every issued MMA has completed before the CTA frees TMEM
+            if (issued) {
+                tc_commit(fin);
+                if (!ws_wait(fin, 0, abort)) {
+                    // the bounded wait gave up: wait once more without the abort shortcut
+                    for (int i = 0; i < (1 << 22); i++) {
+                        uint32_t done;
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+                            "selp.b32 %0, 1, 0, p;\n\t}\n"
+                            : "=r"(done)
+                            : "r"(fin)
+                            : "memory");
+                        if (done) break;
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---- epilogue: warp q reads TMEM lanes 32 q .. 32 q + 31 (tile rows m = 16 q + lane % 16
+        // of x-half lane / 16), both y blocks of one plane per accumulator buffer
+        const int h = lane >> 4, m = 16 * warp + (lane & 15);
+        for (int k = 0; k < my_cells && !*abort; k++) {
+            const int cell = blockIdx.x + k * gridDim.x;
+            for (int z = 0; z < kV; z++) {
+                const int t = 16 * k + z, b = t & 1;
+                if (!ws_wait(accf(b), (t >> 1) & 1, abort)) break;
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+                uint32_t v[2][32];
+#pragma unroll
+                for (int yb = 0; yb < 2; yb++)
+                    asm volatile(
+                        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+                        "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+                        : "=r"(v[yb][0]), "=r"(v[yb][1]), "=r"(v[yb][2]), "=r"(v[yb][3]), "=r"(v[yb][4]), "=r"(v[yb][5]),
+                          "=r"(v[yb][6]), "=r"(v[yb][7]), "=r"(v[yb][8]), "=r"(v[yb][9]), "=r"(v[yb][10]), "=r"(v[yb][11]),
+                          "=r"(v[yb][12]), "=r"(v[yb][13]), "=r"(v[yb][14]), "=r"(v[yb][15]), "=r"(v[yb][16]),
+                          "=r"(v[yb][17]), "=r"(v[yb][18]), "=r"(v[yb][19]), "=r"(v[yb][20]), "=r"(v[yb][21]),
+                          "=r"(v[yb][22]), "=r"(v[yb][23]), "=r"(v[yb][24]), "=r"(v[yb][25]), "=r"(v[yb][26]),
+                          "=r"(v[yb][27]), "=r"(v[yb][28]), "=r"(v[yb][29]), "=r"(v[yb][30]), "=r"(v[yb][31])
+                        : "r"(tbase + ((uint32_t)(32 * warp) << 16) + 64u * b + 32 * yb));
+                asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+                asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+                mb_arrive(acce(b));  // the buffer is free for the MMAs of plane z + 2
+#pragma unroll
+                for (int yb = 0; yb < 2; yb++) {
+                    const int y = 8 * yb + (m >> 3), xv = 8 * h + (m & 7);
+                    const size_t vox = (size_t)cell * kVox + (z * kV + y) * kV + xv;
+                    if (EPI == kEpiF32) {
+                        float4* o = reinterpret_cast<float4*>(outf + vox * kCh);
+#pragma unroll
+                        for (int q = 0; q < 8; q++)
+                            o[q] = make_float4(__uint_as_float(v[yb][4 * q]) + bias[4 * q],
+                                               __uint_as_float(v[yb][4 * q + 1]) + bias[4 * q + 1],
+                                               __uint_as_float(v[yb][4 * q + 2]) + bias[4 * q + 2],
+                                               __uint_as_float(v[yb][4 * q + 3]) + bias[4 * q + 3]);
+                    } else {
+                        __nv_bfloat162 hv[16];
+                        if (EPI == kEpiRelu) {
+#pragma unroll
+                            for (int q = 0; q < 16; q++)
+                                hv[q] = __floats2bfloat162_rn(fmaxf(__uint_as_float(v[yb][2 * q]) + bias[2 * q], 0.f),
+                                                              fmaxf(__uint_as_float(v[yb][2 * q + 1]) + bias[2 * q + 1], 0.f));
+                        } else {
+                            uint4 mm[4];
+                            const uint4* mp = reinterpret_cast<const uint4*>(mask + vox * kCh);
+#pragma unroll
+                            for (int q = 0; q < 4; q++) mm[q] = mp[q];
+                            const __nv_bfloat162* m2 = reinterpret_cast<const __nv_bfloat162*>(mm);
+#pragma unroll
+                            for (int q = 0; q < 16; q++)
+                                hv[q] = __floats2bfloat162_rn(
+                                    __bfloat162float(m2[q].x) > 0.f ? __uint_as_float(v[yb][2 * q]) : 0.f,
+                                    __bfloat162float(m2[q].y) > 0.f ? __uint_as_float(v[yb][2 * q + 1]) : 0.f);
+                        }
+                        uint4* o = reinterpret_cast<uint4*>(out + vox * kCh);
+                        const uint4* hs = reinterpret_cast<const uint4*>(hv);
+#pragma unroll
+                        for (int q = 0; q < 4; q++) o[q] = hs[q];
+                    }
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    if (*abort && tid == 0) atomicExch(err, 1);
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tbase), "r"(kWsTmemCols));
+}
+
 // dW[tap][co][ci] = sum_v dZ[v][co] A[v + tap][ci] and db[co] = sum_v dZ[v][co] over the cells of
 // this CTA (one fixed-order partial per CTA).  M = co (two m16 tiles, A operand = dZ^T through
 // ldmatrix.trans), N = ci (four n8 tiles, B operand = shifted activations through ldmatrix.trans),
@@ -1009,7 +1273,9 @@ struct NetHandle {
     DBuf<int32_t> idx;
     DBuf<int> flag;
     DBuf<int> err;       // set by a tcgen05 kernel whose completion wait timed out
-    int tcgen05 = 0;     // layers 1-3: 0 mma.sync (k_conv32), 1 tcgen05 M=64 tiles (k_conv32_tc), 2 tcgen05 transposed (k_conv32_tt)
+    int tcgen05 = 0;     // layers 1-3: 0 mma.sync (k_conv32), 1 tcgen05 M=64 tiles (k_conv32_tc), 2 tcgen05 transposed
+                         // (k_conv32_tt), 3 tcgen05 M=64 tiles warp-specialised and persistent (k_conv32_ws)
+    int sms = 148;       // multiprocessors of the device (the persistent kernel's grid)
     ~NetHandle()
     {
         if (stream) cudaStreamDestroy(stream);
@@ -1052,6 +1318,9 @@ int conv_attrs()
     MSFEM_CK(cudaFuncSetAttribute(k_conv32_tt<kEpiRelu>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTtSmem));
     MSFEM_CK(cudaFuncSetAttribute(k_conv32_tt<kEpiF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTtSmem));
     MSFEM_CK(cudaFuncSetAttribute(k_conv32_tt<kEpiMask>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTtSmem));
+    MSFEM_CK(cudaFuncSetAttribute(k_conv32_ws<kEpiRelu>, cudaFuncAttributeMaxDynamicSharedMemorySize, kWsSmem));
+    MSFEM_CK(cudaFuncSetAttribute(k_conv32_ws<kEpiF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, kWsSmem));
+    MSFEM_CK(cudaFuncSetAttribute(k_conv32_ws<kEpiMask>, cudaFuncAttributeMaxDynamicSharedMemorySize, kWsSmem));
     done = true;
     return 0;
 }
@@ -1061,7 +1330,9 @@ template <int EPI>
 void conv(NetHandle& N, int n, const __nv_bfloat16* in, const __nv_bfloat16* w, const float* bias, const __nv_bfloat16* mask,
           __nv_bfloat16* out, float* outf)
 {
-    if (N.tcgen05 == 2)
+    if (N.tcgen05 == 3)
+        k_conv32_ws<EPI><<<std::min(n, N.sms), kWsThreads, kWsSmem, N.stream>>>(n, in, w, bias, mask, out, outf, N.err.p);
+    else if (N.tcgen05 == 2)
         k_conv32_tt<EPI><<<n, 128, kTtSmem, N.stream>>>(in, w, bias, mask, out, outf, N.err.p);
     else if (N.tcgen05 == 1)
         k_conv32_tc<EPI><<<n, 128, kTcSmem, N.stream>>>(in, w, bias, mask, out, outf, N.err.p);
@@ -1219,6 +1490,7 @@ int msfem_net_create(uint64_t seed, double E_ref, double in_scale, msfem_net_t* 
         return MSFEM_ERR_ARGUMENT;
     }
     MSFEM_CK(cudaGetDevice(&h->device));
+    MSFEM_CK(cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device));
     MSFEM_CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     h->E_ref = E_ref;
     h->in_scale = in_scale;
@@ -1467,7 +1739,7 @@ int msfem_net_predict(msfem_net_t h, msfem_cells_t cells, float* ms)
 int msfem_net_set_tensor_path(msfem_net_t h, int tcgen05)
 {
     using namespace msfem;
-    if (!h || tcgen05 < 0 || tcgen05 > 2) {
+    if (!h || tcgen05 < 0 || tcgen05 > 3) {
         set_error("msfem_net_set_tensor_path: bad arguments");
         return MSFEM_ERR_ARGUMENT;
     }

@@ -394,12 +394,24 @@ int spmv32(System& s, const float* x, float* y)
 }
 
 // r = f - A x (FP64); *rr_out (device pointer) = (r, r)
+// The solver state, zeroed when it is first allocated: its arrival tickets must start at 0 (the
+// last block of a two-stage reduction is the one that sees count - 1), and fresh device memory
+// need not be zero.
+int ensure_kstate(System& s)
+{
+    if (!s.kstate.p) {
+        MSFEM_TRY(s.kstate.alloc(1));
+        MSFEM_CK(cudaMemsetAsync(s.kstate.p, 0, sizeof(KState), s.stream));
+    }
+    return MSFEM_OK;
+}
+
 int residual64(System& s, const double* x, const double* f, double* r, double* rr_out)
 {
     MSFEM_TRY(prepare_sell(s));
     const unsigned g = spmv_grid_of((const void*)k_residual, s);
     MSFEM_TRY(s.partial.alloc(std::max<size_t>(3 * (size_t)spmv_grid(s), 3 * (size_t)kReduceBlocks) + 64));
-    MSFEM_TRY(s.kstate.alloc(1));
+    MSFEM_TRY(ensure_kstate(s));
     k_residual<<<g, 256, 0, s.stream>>>(sell_view<double>(s), x, f, r, s.partial.p, &s.kstate.p->ticket[3], rr_out);
     MSFEM_CK(cudaGetLastError());
     return MSFEM_OK;

@@ -1522,7 +1522,7 @@ int solve_twolevel(CoarseHandle& C, int precision, int maxiter, double tol, doub
     System& F = *C.fine;
     cudaStream_t st = F.stream;
     MSFEM_TRY(prepare_sell(F));
-    MSFEM_TRY(F.kstate.alloc(1));
+    MSFEM_TRY(ensure_kstate(F));
     const int n = F.n_rows;
     const bool f32 = precision == MSFEM_FP32_IR;
     DBuf<double>& rr = F.sc_f64[1];

@@ -52,7 +52,8 @@ class CoarseNet:
 
     def set_tensor_path(self, path: int):
         """Layers 1-3: 0 = warp-level mma.sync, 1 = tcgen05 with M = 64 voxel tiles, 2 = tcgen05
-        transposed product (N = 256 voxels per instruction)."""
+        transposed product (N = 256 voxels per instruction), 3 = tcgen05 with M = 64 voxel tiles,
+        warp-specialised (load / MMA / epilogue warps) and persistent over cells."""
         check(load().msfem_net_set_tensor_path(self.h, int(path)), "net_set_tensor_path")
 
     def params(self) -> np.ndarray:

@@ -27,9 +27,9 @@ for comparison: face problems (R = 8), then the four volume passes (R = 8 each).
 
     python -m multiscalefemsolver3d_b200.profile_case --net 512
 
-runs the learned coarse space's forward pass over 512 sphere cells twice: layers 1-3 on the
-mma.sync kernels (k_conv32<0>, k_conv32<0>, k_conv32<1>), then on tcgen05 (k_conv32_tc, same
-order).
+predicts the bases of 512 sphere cells with the learned coarse space on each tensor-core path of
+layers 1-3 in turn (0: mma.sync k_conv32, 1: k_conv32_tc, 2: k_conv32_tt, 3: k_conv32_ws), five
+predictions per path, and prints the device time of each path.
 """
 from __future__ import annotations
 
@@ -148,8 +148,9 @@ def twolevel_case(n, maxiter=400000):
 
 
 def net_case(n):
-    import time
-
+    """The learned coarse space's prediction of n sphere cells (voxelisation, the 4 layers, the
+    basis write) on each tensor-core path of layers 1-3, in path order 0 (mma.sync), 1, 2, 3
+    (tcgen05): 2 warm-up predictions and 3 timed ones each (device ms from msfem_net_predict)."""
     import numpy as np
 
     from . import meshgen
@@ -157,13 +158,13 @@ def net_case(n):
     from .learned import CoarseNet
     net = CoarseNet(seed=0)
     C = Cells(meshgen.sphere_cells(n, seed=3))
-    vox = net.voxelise(C)
     out = {"cells": n}
-    for tc in (False, True):
-        net.set_tensor_path(tc)
-        t = time.perf_counter()
-        o = net.forward(vox)
-        out["tcgen05" if tc else "mma_sync"] = {"s_wall": time.perf_counter() - t, "checksum": float(np.abs(o).sum())}
+    for path in (0, 1, 2, 3):
+        net.set_tensor_path(path)
+        for _ in range(2):
+            net.predict(C)
+        ms = [net.predict(C) for _ in range(3)]
+        out[f"path{path}"] = {"ms_predict_min": min(ms), "checksum": float(np.abs(C.bases()).sum())}
     print(json.dumps(out))
     net.close()
     C.close()

@@ -154,9 +154,9 @@ def test_rejects_cells_that_are_not_kuhn_cubes_of_8(lib, cuda):
 
 
 def test_tcgen05_path_matches_mma_sync(lib, cuda):
-    """Layers 1-3 on tcgen05 (TMEM accumulators, shared-memory descriptors; voxel-tile and
-    transposed forms) compute the same function as the warp-level mma.sync kernels: forward
-    outputs, loss and every gradient (measured: bit-identical)."""
+    """Layers 1-3 on tcgen05 (TMEM accumulators, shared-memory descriptors; voxel-tile, transposed
+    and warp-specialised persistent forms) compute the same function as the warp-level mma.sync
+    kernels: forward outputs, loss and every gradient."""
     p = on.init_params(5)
     net = CoarseNet()
     net.set_params(p)
@@ -166,7 +166,7 @@ def test_tcgen05_path_matches_mma_sync(lib, cuda):
     o_ref = net.forward(vox)
     l_ref, g_ref = net.loss_grad(vox, tgt)
     ref = on.forward(p, vox)
-    for path in (1, 2):
+    for path in (1, 2, 3):
         net.set_tensor_path(path)
         o_tc = net.forward(vox)
         l_tc, g_tc = net.loss_grad(vox, tgt)
@@ -175,3 +175,20 @@ def test_tcgen05_path_matches_mma_sync(lib, cuda):
         assert np.linalg.norm(g_tc - g_ref) <= 1e-4 * np.linalg.norm(g_ref), path
         for k in range(3):
             assert np.linalg.norm(o_tc[k] - ref[k][1]) <= 5e-3 * np.linalg.norm(ref[k][1])
+
+
+def test_persistent_tcgen05_path_over_many_cells(lib, cuda):
+    """The warp-specialised tcgen05 kernel walks several cells per CTA (a ring of plane slots and
+    two TMEM accumulators carried across cells): 400 cells (more than one per SM) give the
+    mma.sync path's forward output."""
+    net = CoarseNet()
+    net.set_params(on.init_params(7))
+    vox = np.random.default_rng(3).normal(0.0, 1.0, (400, 4096)).astype(np.float32)
+    net.set_tensor_path(0)
+    o_ref = net.forward(vox)
+    net.set_tensor_path(3)
+    o_ws = net.forward(vox)
+    assert np.linalg.norm(o_ws - o_ref) <= 1e-5 * np.linalg.norm(o_ref)
+    for k in (0, 147, 148, 399):
+        assert np.linalg.norm(o_ws[k] - o_ref[k]) <= 1e-5 * np.linalg.norm(o_ref[k]), k
+
