@@ -70,6 +70,9 @@ def parse():
     ap.add_argument("--coarse", default="learned", choices=["learned", "exact"],
                     help="elastic: coarse-space bases predicted by the trained network (with the exact cell solve "
                          "as per-cell fallback) or solved exactly for every cell")
+    ap.add_argument("--operator", default="matrix-free", choices=["matrix-free", "assembled"],
+                    help="elastic: the cycle's smoother and MINRES's products matrix-free on the Kuhn grid, or "
+                         "from the assembled SELL matrices (FP16 smoother values)")
     ap.add_argument("--coarse-face-material", default="cells", choices=["cells", "zero"],
                     help="elastic: the face-problem materials of the coarse space's cell bases (and of the "
                          "network's training targets): cells (default) -- each face on the materials of the "
@@ -859,6 +862,18 @@ def run_twolevel(args, D):
     stream = torch.cuda.ExternalStream(S.stream, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     DEG, HALF = 3, True
+    MF = args.operator == "matrix-free"
+    if MF:  # the mesh's structure, checked once like the portraits
+        S.set_kuhn_grid(args.n)
+        K.set_kuhn_grid(args.n)
+
+    def smoother(T_, K_):
+        if MF:
+            T_.set_smoother(K_, degree=DEG, matrix_free=True)
+            T_.set_matrix_free(True)
+        else:
+            T_.set_smoother(K_, degree=DEG, half_matrix=HALF)
+
     learned = args.coarse == "learned"
     net, train_info = None, {}
     if learned:
@@ -895,7 +910,7 @@ def run_twolevel(args, D):
         K.apply_dirichlet(dofs, zval, fem.ROW_AND_COLUMN)
         binfo = coarse_bases(C, cc.cells)
         T = TwoLevel(S, C, cc, dofs_np)
-        T.set_smoother(K, degree=DEG, half_matrix=HALF)
+        smoother(T, K)
         S.set_x(xzero)
         rel, it, out, rc = T.solve(tol=TOL, maxiter=400000, precision=FP64)
         info = {"rel_residual": rel, "iterations": it, "refinement_steps": out, "coarse_dofs": T.n_coarse_dofs,
@@ -935,7 +950,7 @@ def run_twolevel(args, D):
         rcb = C.build_bases(FP32_IR, TOL)
         ms_b = sum(C.report()["ms"].values())
         T = TwoLevel(S, C, cc, dofs_np)
-        T.set_smoother(K, degree=DEG, half_matrix=HALF)
+        smoother(T, K)
         S.set_x(xzero)
         rel, it, out, rc = T.solve(tol=TOL, maxiter=400000, precision=FP64)
         comp.update({"exact_bases_ms_bases": ms_b, "exact_bases_iterations": it, "exact_bases_rel_residual": rel,
@@ -948,7 +963,7 @@ def run_twolevel(args, D):
         C.build_bases(FP32_IR, TOL)
         ms_b = sum(C.report()["ms"].values())
         T = TwoLevel(S, C, cc, dofs_np)
-        T.set_smoother(K, degree=DEG, half_matrix=HALF)
+        smoother(T, K)
         S.set_x(xzero)
         rel, it, out, rc = T.solve(tol=TOL, maxiter=400000, precision=FP64)
         comp.update({f"exact_bases_face_{other}_iterations": it,
@@ -957,7 +972,7 @@ def run_twolevel(args, D):
         C.set_face_material(args.coarse_face_material)
     # the dominant kernel of the solve: one Chebyshev step of the smoother (FP16 SpMV + update)
     T = TwoLevel(S, C, cc, dofs_np)
-    T.set_smoother(K, degree=DEG, half_matrix=HALF)
+    smoother(T, K)
     cheb_ms, cheb_bytes = T.bench_smoother(reps=200)
     T.close()
     if not args.no_compare:
@@ -999,7 +1014,10 @@ def run_twolevel(args, D):
         K2.apply_dirichlet(dofs_p, np.zeros(dofs_p.size), fem.ROW_AND_COLUMN)
         coarse_bases(C2, ccp.cells)
         T2 = TwoLevel(S2, C2, ccp, dofs_p)
-        T2.set_smoother(K2, degree=DEG, half_matrix=HALF)
+        if MF:
+            S2.set_kuhn_grid(mm.n)
+            K2.set_kuhn_grid(mm.n)
+        smoother(T2, K2)
         S2.set_x(np.zeros(3 * mm.n_nodes))
         rel, it, out, rc = T2.solve(tol=tol, maxiter=400000, precision=FP64)
         sol = S2.get_x()
@@ -1031,8 +1049,12 @@ def run_twolevel(args, D):
         extra.update(spmv_c2)
         extra["coarse_face_material"] = args.coarse_face_material
         extra.update({"speedup_vs_jacobi_fp64_minres": (comp["jacobi_fp64_minres_ms"] / ms) if comp else None,
-                      "smoother": f"Chebyshev degree {DEG} on the textbook operator, matrix values in "
-                                  f"{'FP16' if HALF else 'FP32'}, FP32 arithmetic; coarse: 8^3-hexahedron MsFEM cells, "
+                      "operator": args.operator,
+                      "smoother": f"Chebyshev degree {DEG} on the textbook operator, "
+                                  + ("formed matrix-free on the Kuhn grid from per-tetrahedron materials (MINRES's "
+                                     "FP64 products too)" if MF else
+                                     f"matrix values in {'FP16' if HALF else 'FP32'}")
+                                  + ", FP32 arithmetic; coarse: 8^3-hexahedron MsFEM cells, "
                                   + ("bases predicted by the learned operator (4 conv layers, 32 channels, BF16 "
                                      "tensor cores), exact cell solve as fallback" if learned else "exact bases"),
                       "spmv_fp32_ms": spmv32_ms, "spmv_fp32_gbs": ach, "spmv_fp64_ms": spmv64_ms,
@@ -1049,9 +1071,11 @@ def run_twolevel(args, D):
                 "e2e": {"value": e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
                 "gpu_launches": int(launches),
                 "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                             "traffic": read_traffic("cheb_smoother_elastic_128.md"),
-                             "kernel": "k_mg_cheb (Chebyshev step of the smoother: FP16 3x3-block SELL SpMV of the "
-                                       "textbook operator + vector update)",
+                             "traffic": read_traffic("kuhn_cheb_elastic_128.md" if MF else "cheb_smoother_elastic_128.md"),
+                             "kernel": ("k_kuhn<EpiCheb> (Chebyshev step of the smoother: matrix-free textbook "
+                                        "operator on the Kuhn grid + vector update)" if MF else
+                                        "k_mg_cheb (Chebyshev step of the smoother: FP16 3x3-block SELL SpMV of the "
+                                        "textbook operator + vector update)"),
                              "ms_per_launch": cheb_ms, "bytes_per_launch": cheb_bytes,
                              "peak_source": f"{peak_kind} hbm_gbs"},
                 "cpu_baseline": base,

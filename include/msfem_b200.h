@@ -231,6 +231,19 @@ int msfem_spmv(msfem_system_t h, const double* x, double* y, int on_device);
  * inner solves of MSFEM_FP32_IR apply (no counterpart in the reference; exposed so that the
  * FP32 path can be checked on its own).  x, y: n_rows floats. */
 int msfem_spmv_scaled32(msfem_system_t h, const float* x, float* y, int on_device);
+/* Structured Kuhn grid (no reference counterpart; the mesh of the reference's generated cubes):
+ * checks on the device that the system's mesh is nx x ny x nz hexahedra, each cut into the six
+ * Kuhn tetrahedra of its 0-7 diagonal -- tetrahedra 6c .. 6c+5 of hexahedron c = i + nx (j + ny k)
+ * with corners {0,1,3,7} {0,1,5,7} {0,2,3,7} {0,2,6,7} {0,4,5,7} {0,4,6,7} in that vertex order,
+ * corner b at node (i + (b&1)) + (nx+1) ((j + (b>>1&1)) + (ny+1) (k + (b>>2&1))), nodes on a
+ * regular grid -- with material ids in [0, 64).  MSFEM_ERR_ARGUMENT (first offending tetrahedron or
+ * node in the message) otherwise.  Elasticity systems only. */
+int msfem_set_kuhn_grid(msfem_system_t h, int nx, int ny, int nz);
+/* y = A x formed matrix-free on the Kuhn grid (FP64): A is the system's values -- one
+ * msfem_assemble_elastic or msfem_assemble_elastic_textbook since the last msfem_clear, plus its
+ * Dirichlet rows -- applied from the tetrahedra's materials; checked against the assembled product
+ * on a probe vector first (MSFEM_ERR_STATE if the relative distance exceeds 1e-12). */
+int msfem_kuhn_spmv(msfem_system_t h, const double* x, double* y, int on_device);
 
 /* CSR export of the assembled matrix (sizes from msfem_system_info), host or device buffers. */
 int msfem_export_csr(msfem_system_t h, int32_t* row_ptr, int32_t* col, double* val, int on_device);
@@ -505,11 +518,20 @@ int msfem_solve_twolevel(msfem_system_t fine, msfem_coarse_t c, int precision, i
  * `degree` Chebyshev steps on its Jacobi-scaled FP32 matrix (spectrum bound [lmax/ratio, lmax],
  * lmax from 50 power steps x 1.1, widened by the solve if a step fails), the coarse correction,
  * the same Chebyshev steps again; SPD, so
- * MINRES on the reference's matrix keeps its guarantees.  half_matrix = 1 stores the smoother's
- * matrix values in FP16 (arithmetic stays FP32; rounding each entry keeps the matrix symmetric, so
- * the cycle stays SPD; it halves the bytes of the 2*degree SpMVs per cycle).  The textbook system
- * must outlive c. */
-int msfem_coarse_set_smoother(msfem_coarse_t c, msfem_system_t textbook, int degree, double ratio, int half_matrix);
+ * MINRES on the reference's matrix keeps its guarantees.  storage: 0 the FP32 SELL matrix; 1 its
+ * values in FP16 (arithmetic stays FP32; rounding each entry keeps the matrix symmetric, so the
+ * cycle stays SPD; it halves the bytes of the 2*degree SpMVs per cycle); 2 matrix-free on the
+ * structured Kuhn grid (msfem_set_kuhn_grid on `textbook`, whose values must be one textbook
+ * assembly plus Dirichlet rows since the last msfem_clear): the product is formed from each
+ * tetrahedron's material code, FP32, and is checked here against the assembled matrix on a probe
+ * vector (relative 1e-5); MSFEM_ERR_STATE if it differs.  The textbook system must outlive c. */
+int msfem_coarse_set_smoother(msfem_coarse_t c, msfem_system_t textbook, int degree, double ratio, int storage);
+/* on = 1: msfem_solve_twolevel's FP64 MINRES products with the fine (reference) matrix are formed
+ * matrix-free on its Kuhn grid (msfem_set_kuhn_grid on the fine system, whose values must be one
+ * msfem_assemble_elastic plus Dirichlet rows since the last msfem_clear), checked here against the
+ * assembled matrix on a probe vector (relative 1e-12; MSFEM_ERR_STATE if it differs).  The
+ * solve's true residuals stay on the assembled matrix.  on = 0: the assembled SELL product. */
+int msfem_coarse_set_matrix_free(msfem_coarse_t c, int on);
 /* Robustness record of the two-level preconditioner: cells whose bases left [-3, 3] and were
  * replaced by the trilinear functions of their box in the prolongation (the reference's cell
  * operator is indefinite; a nearly singular cell problem returns bases in the thousands, which

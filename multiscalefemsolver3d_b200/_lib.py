@@ -77,6 +77,8 @@ _SIGS = [
                                           C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("msfem_spmv", C.c_int, [C.c_void_p, _P, _P, C.c_int]),
     ("msfem_spmv_scaled32", C.c_int, [C.c_void_p, _P, _P, C.c_int]),
+    ("msfem_set_kuhn_grid", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
+    ("msfem_kuhn_spmv", C.c_int, [C.c_void_p, _P, _P, C.c_int]),
     ("msfem_export_csr", C.c_int, [C.c_void_p, _P, _P, _P, C.c_int]),
     ("msfem_bench_spmv", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     ("msfem_residual_noalloc", C.c_int, [C.c_int, _P, _P, _P, _P, _P, _P, _P, C.c_void_p]),
@@ -120,6 +122,7 @@ _SIGS = [
                                        C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("msfem_coarse_bench_smoother", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     ("msfem_coarse_set_smoother", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_int]),
+    ("msfem_coarse_set_matrix_free", C.c_int, [C.c_void_p, C.c_int]),
     ("msfem_coarse_stats", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int)]),
     ("msfem_coarse_destroy", None, [C.c_void_p]),
     ("msfem_net_param_count", C.c_int, []),

@@ -330,6 +330,13 @@ int assemble_elastic(System& s, const double* E, const double* nu, int n_mat, bo
     }
     MSFEM_CK(cudaGetLastError());
     s.total_launches += nc;
+    // a matrix-free operator (kuhn.cu) can stand for the values only while they hold one assembly
+    if (s.elastic_form == 0) {
+        s.elastic_form = textbook ? 2 : 1;
+        s.lame_host = lame;
+    } else {
+        s.elastic_form = -1;
+    }
     return finish_assembly(s, bad);
 }
 

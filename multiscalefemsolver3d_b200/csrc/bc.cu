@@ -65,6 +65,17 @@ __global__ void k_dirichlet_rows(int L, const int32_t* __restrict__ sdof, const 
     }
 }
 
+// per node Dirichlet bits for the matrix-free operators (kuhn.cu): bit a row, bit 3+a column
+__global__ void k_dirichlet_mask(int L, const int32_t* __restrict__ dofs, int bs, int columns, uint32_t* __restrict__ mask,
+                                 const int* bad)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= L || *bad) return;
+    const int d = dofs[i];
+    const int node = d / bs, a = d - bs * node;
+    atomicOr(mask + node, (1u << a) | (columns ? (1u << (3 + a)) : 0u));
+}
+
 __global__ void k_sparse_level(int L, int half, const int32_t* __restrict__ prev, int32_t* __restrict__ cur)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -181,8 +192,14 @@ int apply_dirichlet(System& s, int L, const int32_t* d_dofs, const double* d_val
     MSFEM_CK(cub::DeviceRadixSort::SortPairs(s.sc_tmp.p, tmp_bytes, d_dofs, sdof.p, pos.p, spos.p, L, 0, 32, st));
     k_dirichlet_rows<<<grid_for(L, 128), 128, 0, st>>>(L, sdof.p, spos.p, d_values, s.bs, s.nrp.p, s.ncol.p, s.val.p,
                                                        s.F.p, s.X.p, bad.p);
+    if (!s.dmask.p) {
+        MSFEM_TRY(s.dmask.alloc((size_t)s.n_nodes));
+        MSFEM_CK(cudaMemsetAsync(s.dmask.p, 0, sizeof(uint32_t) * s.n_nodes, st));
+    }
+    k_dirichlet_mask<<<grid_for(L, 256), 256, 0, st>>>(L, d_dofs, s.bs, mode == MSFEM_ROW_AND_COLUMN, s.dmask.p,
+                                                       bad.p);
     MSFEM_CK(cudaGetLastError());
-    s.total_launches += 3;  // check, iota, rows (the radix sort's own kernels are not counted)
+    s.total_launches += 4;  // check, iota, rows, mask (the radix sort's own kernels are not counted)
     if (mode == MSFEM_ROW_AND_COLUMN) {
         MSFEM_CK(cudaMemcpyAsync(table.p, d_dofs, sizeof(int32_t) * L, cudaMemcpyDeviceToDevice, st));
         for (int t = 1; t <= T; t++)

@@ -9,6 +9,7 @@
 
 #include "devutil.cuh"
 #include "internal.cuh"
+#include "kuhn_op.cuh"
 #include "spmv.cuh"
 
 namespace msfem {
@@ -309,7 +310,10 @@ int msfem_clear(msfem_system_t h)
     MSFEM_CK(cudaMemsetAsync(s.val.p, 0, sizeof(double) * s.val.n, s.stream));
     MSFEM_CK(cudaMemsetAsync(s.F.p, 0, sizeof(double) * s.F.n, s.stream));
     MSFEM_CK(cudaMemsetAsync(s.X.p, 0, sizeof(double) * s.X.n, s.stream));
+    if (s.dmask.p) MSFEM_CK(cudaMemsetAsync(s.dmask.p, 0, sizeof(uint32_t) * s.dmask.n, s.stream));
     MSFEM_CK(cudaStreamSynchronize(s.stream));
+    s.elastic_form = 0;
+    s.lame_host.clear();
     s.invalidate_values();
     return MSFEM_OK;
 }
@@ -519,6 +523,36 @@ int msfem_spmv_scaled32(msfem_system_t h, const float* x, float* y, int on_devic
     MSFEM_TRY(spmv32(s, dx.p, dy.p));
     MSFEM_CK(cudaMemcpyAsync(y, dy.p, sizeof(float) * s.n_rows, cudaMemcpyDefault, s.stream));
     MSFEM_CK(cudaStreamSynchronize(s.stream));
+    return MSFEM_OK;
+}
+
+int msfem_set_kuhn_grid(msfem_system_t h, int nx, int ny, int nz)
+{
+    MSFEM_TRY(check_handle(h));
+    System& s = *as_sys(h);
+    MSFEM_TRY(use_device(s));
+    return kuhn_set_grid(s, nx, ny, nz);
+}
+
+int msfem_kuhn_spmv(msfem_system_t h, const double* x, double* y, int on_device)
+{
+    (void)on_device;
+    MSFEM_TRY(check_handle(h));
+    System& s = *as_sys(h);
+    MSFEM_TRY(use_device(s));
+    if (!x || !y) {
+        set_error("msfem_kuhn_spmv: null vector");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    KuhnOperator op;
+    MSFEM_TRY(kuhn_operator_build(s, s.elastic_form, true, false, op));
+    DBuf<double> dx, dy;
+    MSFEM_TRY(to_device(s, dx, x, (size_t)s.n_rows));
+    MSFEM_TRY(dy.alloc((size_t)s.n_rows));
+    MSFEM_TRY(kuhn_spmv64(op, dx.p, dy.p, s.stream));
+    MSFEM_CK(cudaMemcpyAsync(y, dy.p, sizeof(double) * s.n_rows, cudaMemcpyDefault, s.stream));
+    MSFEM_CK(cudaStreamSynchronize(s.stream));
+    s.total_launches += 1;
     return MSFEM_OK;
 }
 

@@ -165,6 +165,20 @@ struct System {
     DBuf<double> loop_best;          // the drivers' restart loop: best solution so far
     bool reference_order = false;    // MSFEM_PCG_SSOR in the reference's operation order (ssor.cu)
 
+    // structured Kuhn grid (kuhn.cu): hexahedra per axis and spacing, set by msfem_set_kuhn_grid
+    // once the mesh is checked to be that grid; material code per tetrahedron
+    int kuhn_n[3] = {0, 0, 0};
+    double kuhn_h[3] = {0.0, 0.0, 0.0};
+    DBuf<uint8_t> kuhn_mat;
+    // what the values hold since the last clear: 0 nothing, 1 the reference's elasticity assembly,
+    // 2 the textbook orientation, -1 anything else (two assemblies, imported values); the lambda,
+    // mu table of that assembly; per node the Dirichlet bits (bit a: row 3n+a is a Dirichlet row,
+    // bit 3+a: its column was eliminated)
+    int elastic_form = 0;
+    std::vector<double> lame_host;
+    DBuf<uint32_t> dmask;
+    uint64_t values_version = 0;  // bumped whenever the values change
+
     bool zero_diag = false;
     bool force_col32 = false;  // keep 32-bit SELL columns even when 16-bit deltas fit
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -172,7 +186,11 @@ struct System {
     int launches = 0;          // kernels of the current solve
     int64_t total_launches = 0;  // kernels of this library launched on the handle
 
-    void invalidate_values() { sell.values_ok = false; }
+    void invalidate_values()
+    {
+        sell.values_ok = false;
+        values_version++;
+    }
 };
 
 // ---- mesh / portrait (portrait.cu)

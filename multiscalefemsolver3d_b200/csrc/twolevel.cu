@@ -44,6 +44,7 @@
 #include "devutil.cuh"
 #include "element.cuh"
 #include "internal.cuh"
+#include "kuhn_op.cuh"
 #include "spmv.cuh"
 
 namespace msfem {
@@ -847,6 +848,105 @@ __global__ void __launch_bounds__(256) k_mg_resid(SellView<float> A, const __hal
     }
 }
 
+// The same two smoothing kernels and the MINRES product on a Kuhn grid, matrix-free (kuhn.cuh):
+// epilogues of the brick kernel, applied to each owned node's product y.
+// one Chebyshev step (k_mg_cheb): res -= K^ dprev; d = a dprev + b res; x += d
+struct EpiCheb {
+    const float* __restrict__ dprev;
+    float* __restrict__ d;
+    float* __restrict__ res;
+    float* __restrict__ x;
+    float a, b;
+    const TlState* S;
+    __device__ __forceinline__ bool skip() const { return S->done; }
+    __device__ __forceinline__ void operator()(int64_t g, const float* y)
+    {
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const int64_t i = 3 * g + c;
+            const float ri = res[i] - y[c];
+            res[i] = ri;
+            const float di = a * dprev[i] + b * ri;
+            d[i] = di;
+            x[i] += di;
+        }
+    }
+    __device__ __forceinline__ void finish() {}
+};
+
+// res = rhat - K^ x; with `start` also d = res / theta, x2 = x + d (k_mg_resid)
+struct EpiResid {
+    const float* __restrict__ rhat;
+    const float* __restrict__ xin;
+    float* __restrict__ res;
+    float* __restrict__ d;
+    float* __restrict__ x2;
+    float inv_theta;
+    const TlState* S;
+    int start;
+    __device__ __forceinline__ bool skip() const { return S->done; }
+    __device__ __forceinline__ void operator()(int64_t g, const float* y)
+    {
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const int64_t i = 3 * g + c;
+            const float ri = rhat[i] - y[c];
+            res[i] = ri;
+            if (start) {
+                const float di = ri * inv_theta;
+                d[i] = di;
+                x2[i] = xin[i] + di;
+            }
+        }
+    }
+    __device__ __forceinline__ void finish() {}
+};
+
+// v = y / beta; z = A y / beta - (beta / oldb) r1; alfa = (v, z) (k_tl_spmv<double>)
+struct EpiMinres {
+    const double* __restrict__ y;
+    double* __restrict__ v;
+    double* __restrict__ z;
+    const double* __restrict__ r1;
+    TlState* S;
+    double* __restrict__ partial;
+    double acc;
+    __device__ __forceinline__ bool skip() const { return S->done; }
+    __device__ __forceinline__ void operator()(int64_t g, const double* ay)
+    {
+        const double inv = 1.0 / S->beta;
+        const double coef = S->iter > 0 ? S->beta / S->oldb : 0.0;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const int64_t i = 3 * g + c;
+            const double vi = y[i] * inv;
+            const double zi = ay[c] * inv - coef * r1[i];
+            v[i] = vi;
+            z[i] = zi;
+            acc += vi * zi;
+        }
+    }
+    __device__ __forceinline__ void finish()
+    {
+        __shared__ double sh[32];
+        double t[1] = {acc};
+        block_sum<1>(t, sh);
+        if (threadIdx.x == 0) partial[blockIdx.x] = t[0];
+        if (arrive_last(&S->ticket[1])) {
+            double r[1];
+            reduce_partials<1>(partial, gridDim.x, 0, r, sh);
+            if (threadIdx.x == 0) {
+                S->alfa = r[0];
+                S->ticket[1] = 0;
+            }
+        }
+    }
+};
+
+using KCheb = KuhnKernel<2, KuhnCfg32, float, EpiCheb>;
+using KResid = KuhnKernel<2, KuhnCfg32, float, EpiResid>;
+using KMinres = KuhnKernel<1, KuhnCfg64, double, EpiMinres>;
+
 // x += P^_t ec
 __global__ void __launch_bounds__(kVecThreads) k_mg_prolong(int n_fine, const int32_t* __restrict__ owner,
                                                            const int32_t* __restrict__ cdof,
@@ -972,6 +1072,11 @@ struct CoarseHandle {
     DBuf<__half2> val16;  // FP16 copy of the textbook system's scaled SELL values, paired (when requested)
     DBuf<int16_t> col16;  // its block columns as 16-bit deltas (empty when some delta does not fit)
     bool half_matrix = false;
+    // the smoother's operator: 0 FP32 SELL, 1 FP16 SELL (half_matrix), 2 matrix-free on the Kuhn grid
+    int storage = 0;
+    KuhnOperator kt;      // matrix-free textbook operator (storage 2)
+    KuhnOperator ka;      // matrix-free reference operator for MINRES's products (msfem_coarse_set_matrix_free)
+    bool mf_fine = false;
     ~CoarseHandle()
     {
         for (auto g : graph)
@@ -1331,19 +1436,32 @@ void mg_cycle(CoarseHandle& C, const double* z, const double* r2, double* r_out,
     const double* s_t = T.dscale.p;
     const __half2* v16 = C.half_matrix ? C.val16.p : nullptr;
     const int16_t* c16 = C.half_matrix ? C.col16.p : nullptr;
+    const bool mf = C.storage == 2;
+    const KuhnView<float>& Kv = C.kt.v32;
+    const int sms = C.kt.sms;
+    auto cheb = [&](float* dprev, float* dnew, float* xx, int i) {
+        if (mf)
+            KCheb::launch(Kv, dprev, EpiCheb{dprev, dnew, res, xx, C.cc.a[i], C.cc.b[i], S}, sms, st);
+        else
+            k_mg_cheb<<<gsp, 256, 0, st>>>(At, v16, c16, dprev, dnew, res, xx, C.cc.a[i], C.cc.b[i], S);
+    };
+    auto resid = [&](float* d0, float* x2, float inv_theta, int start) {
+        if (mf)
+            KResid::launch(Kv, x, EpiResid{rhat, x, res, d0, x2, inv_theta, S, start}, sms, st);
+        else
+            k_mg_resid<<<gsp, 256, 0, st>>>(At, v16, c16, rhat, x, res, d0, x2, inv_theta, S, start);
+    };
     k_mg_in<<<gvec, kVecThreads, 0, st>>>(n, z, r2, r_out, s_t, rhat, res, dA, x, C.cc, S, lanczos);
     float* d[2] = {dA, dB};
-    for (int i = 1; i < C.cheb_deg; i++)
-        k_mg_cheb<<<gsp, 256, 0, st>>>(At, v16, c16, d[(i - 1) & 1], d[i & 1], res, x, C.cc.a[i], C.cc.b[i], S);
-    k_mg_resid<<<gsp, 256, 0, st>>>(At, v16, c16, rhat, x, res, nullptr, nullptr, 0.0f, S, 0);
+    for (int i = 1; i < C.cheb_deg; i++) cheb(d[(i - 1) & 1], d[i & 1], x, i);
+    resid(nullptr, nullptr, 0.0f, 0);
     k_tl_restrict<float><<<C.n_cells, 128, 0, st>>>(C.own_ptr.p, C.own.p, C.psi_t.p, res, nullptr, nullptr, C.cpart.p,
                                                     nullptr, S, 0);
     k_tl_gather<<<gridn(C.n_cf), 256, 0, st>>>(C.n_cf, C.dptr.p, C.dent.p, C.cpart.p, C.rc.p, S);
     k_tl_gemv<<<gridn((int64_t)C.n_cf * 32), 256, 0, st>>>(C.n_cf, C.n_pad, C.Cinv.p, C.rc.p, C.ec.p, S);
     k_mg_prolong<<<gvec, kVecThreads, 0, st>>>(C.n_fine, C.owner.p, C.cdof.p, C.psi_t.p, C.ec.p, x, S);
-    k_mg_resid<<<gsp, 256, 0, st>>>(At, v16, c16, rhat, x, res, dA, x2, C.cc.inv_theta, S, 1);
-    for (int i = 1; i < C.cheb_deg; i++)
-        k_mg_cheb<<<gsp, 256, 0, st>>>(At, v16, c16, d[(i - 1) & 1], d[i & 1], res, x2, C.cc.a[i], C.cc.b[i], S);
+    resid(dA, x2, C.cc.inv_theta, 1);
+    for (int i = 1; i < C.cheb_deg; i++) cheb(d[(i - 1) & 1], d[i & 1], x2, i);
     k_mg_out<<<gvec, kVecThreads, 0, st>>>(n, x2, s_t, lanczos ? r_out : z, y, S, C.partial.p, init);
 }
 
@@ -1382,7 +1500,10 @@ int inner_solve_mg(CoarseHandle& C, int maxiter, double tau, int* iters)
             double* r2 = R[1 - p];
             double* w1 = Wb[p];
             double* w2 = Wb[1 - p];
-            k_tl_spmv<double><<<gsp, 256, 0, st>>>(A, Y, V, Z, r1, S, C.partial.p + 2048);
+            if (C.mf_fine)
+                KMinres::launch(C.ka.v64, Y, EpiMinres{Y, V, Z, r1, S, C.partial.p + 2048, 0.0}, C.ka.sms, st);
+            else
+                k_tl_spmv<double><<<gsp, 256, 0, st>>>(A, Y, V, Z, r1, S, C.partial.p + 2048);
             mg_cycle(C, Z, r2, r1, Y, 1, 0, st);  // r2_new over r1's buffer, then y = M^-1 r2_new
             k_tl_update<double><<<gvec, kVecThreads, 0, st>>>(n, V, w1, w2, X, S);
             k_tl_applied<<<1, 1, 0, st>>>(S);
@@ -1446,11 +1567,15 @@ void cheb_coefs(CoarseHandle& C, double lmax, double ratio, int degree)
 // 50 power steps (times 1.1), lambda_min = lambda_max / ratio.  The smoother -- and with it the
 // symmetric cycle -- is SPD only while lambda_max really bounds the spectrum; the power estimate
 // approaches it from below, so solve_twolevel widens the bound if a step ever raises the residual.
-int set_smoother(CoarseHandle& C, System& T, int degree, double ratio, int half_matrix)
+int set_smoother(CoarseHandle& C, System& T, int degree, double ratio, int storage)
 {
     System& F = *C.fine;
     if (T.kind != MSFEM_ELASTIC || T.n_rows != F.n_rows || T.device != F.device) {
         set_error("msfem_coarse_set_smoother: the textbook system must be an elasticity system on the fine mesh");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    if (storage < 0 || storage > 2) {
+        set_error("msfem_coarse_set_smoother: storage must be 0 (FP32), 1 (FP16) or 2 (matrix-free)");
         return MSFEM_ERR_ARGUMENT;
     }
     if (degree < 1 || degree > 8 || !(ratio > 1.0)) {
@@ -1496,8 +1621,17 @@ int set_smoother(CoarseHandle& C, System& T, int degree, double ratio, int half_
     cheb_coefs(C, 1.1 * lam, ratio, degree);
     C.widened = 0;
     C.text = &T;
-    C.half_matrix = half_matrix != 0;
+    C.storage = storage;
+    C.half_matrix = storage == 1;
     C.col16.release();
+    C.val16.release();
+    if (storage == 2) {
+        C.text = nullptr;  // usable only once the matrix-free operator passed its check
+        MSFEM_TRY(kuhn_operator_build(T, 2, false, true, C.kt));
+        MSFEM_CK(KCheb::prepare());
+        MSFEM_CK(KResid::prepare());
+        C.text = &T;
+    }
     if (C.half_matrix) {
         MSFEM_TRY(C.val16.alloc(5 * (size_t)T.sell.stored));
         k_to_half<<<gridn(T.sell.stored), 256, 0, st>>>(T.sell.stored, T.sell.val32.p, C.val16.p);
@@ -1544,6 +1678,8 @@ int solve_twolevel(CoarseHandle& C, int precision, int maxiter, double tol, doub
     int total = 0, k = 0, rc = MSFEM_OK;
     double r2 = 0.0, prev = -1.0;
     const bool mg = C.text && !f32;
+    if (mg && C.storage == 2) MSFEM_TRY(kuhn_operator_current(C.kt));
+    if (mg && C.mf_fine) MSFEM_TRY(kuhn_operator_current(C.ka));
     if (mg) MSFEM_TRY(C.xkeep.alloc(n));
     for (k = 0; k < 40; k++) {
         MSFEM_TRY(residual64(F, F.X.p, F.F.p, C.r64.p, rr.p));
@@ -1731,7 +1867,7 @@ int msfem_solve_twolevel(msfem_system_t fine, msfem_coarse_t c, int precision, i
     return rc;
 }
 
-int msfem_coarse_set_smoother(msfem_coarse_t c, msfem_system_t textbook, int degree, double ratio, int half_matrix)
+int msfem_coarse_set_smoother(msfem_coarse_t c, msfem_system_t textbook, int degree, double ratio, int storage)
 {
     using namespace msfem;
     if (!c || !textbook) {
@@ -1739,7 +1875,28 @@ int msfem_coarse_set_smoother(msfem_coarse_t c, msfem_system_t textbook, int deg
         return MSFEM_ERR_ARGUMENT;
     }
     MSFEM_CK(cudaSetDevice(c->fine->device));
-    return set_smoother(*c, *reinterpret_cast<System*>(textbook), degree, ratio, half_matrix);
+    return set_smoother(*c, *reinterpret_cast<System*>(textbook), degree, ratio, storage);
+}
+
+int msfem_coarse_set_matrix_free(msfem_coarse_t c, int on)
+{
+    using namespace msfem;
+    if (!c) {
+        set_error("msfem_coarse_set_matrix_free: bad arguments");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    CoarseHandle& C = *c;
+    MSFEM_CK(cudaSetDevice(C.fine->device));
+    C.mf_fine = false;
+    if (C.graph[2]) {
+        cudaGraphExecDestroy(C.graph[2]);
+        C.graph[2] = nullptr;
+    }
+    if (!on) return MSFEM_OK;
+    MSFEM_TRY(kuhn_operator_build(*C.fine, 1, true, false, C.ka));
+    MSFEM_CK(KMinres::prepare());
+    C.mf_fine = true;
+    return MSFEM_OK;
 }
 
 int msfem_coarse_bench_smoother(msfem_coarse_t c, int reps, double* ms_per_step, int64_t* bytes_per_step)
@@ -1766,9 +1923,15 @@ int msfem_coarse_bench_smoother(msfem_coarse_t c, int reps, double* ms_per_step,
     const unsigned gsp = spmv_grid_of((const void*)k_mg_cheb, T);
     const __half2* v16 = C.half_matrix ? C.val16.p : nullptr;
     const int16_t* c16 = C.half_matrix ? C.col16.p : nullptr;
+    const bool mf = C.storage == 2;
+    if (mf) MSFEM_TRY(kuhn_operator_current(C.kt));
     auto step = [&](int i) {
-        k_mg_cheb<<<gsp, 256, 0, st>>>(At, v16, c16, (i & 1) ? dB : dA, (i & 1) ? dA : dB, res, x, C.cc.a[1],
-                                       C.cc.b[1], run.p);
+        float* dp = (i & 1) ? dB : dA;
+        float* dn = (i & 1) ? dA : dB;
+        if (mf)
+            KCheb::launch(C.kt.v32, dp, EpiCheb{dp, dn, res, x, C.cc.a[1], C.cc.b[1], run.p}, C.kt.sms, st);
+        else
+            k_mg_cheb<<<gsp, 256, 0, st>>>(At, v16, c16, dp, dn, res, x, C.cc.a[1], C.cc.b[1], run.p);
     };
     for (int i = 0; i < 3; i++) step(i);
     cudaEvent_t e0, e1;
@@ -1786,10 +1949,15 @@ int msfem_coarse_bench_smoother(msfem_coarse_t c, int reps, double* ms_per_step,
     *ms_per_step = ms / reps;
     // matrix values (FP16 pairs: 5 x 4 B per block, FP32: 36 B) and block columns, each once;
     // slice pointers; per DOF the previous direction (4 B), res read and written (8 B), the new
-    // direction (4 B), x read and written (8 B)
-    const int64_t vb = C.half_matrix ? 20 : 36;
-    const int64_t cb = c16 ? 2 : 4;
-    *bytes_per_step = T.sell.stored * (vb + cb) + (int64_t)(T.sell.n_slices + 1) * 8 + (int64_t)n * 24;
+    // direction (4 B), x read and written (8 B).  Matrix-free: per DOF the Jacobi scale (4 B)
+    // instead of the matrix, per node its Dirichlet bits (4 B), per tetrahedron its material (1 B)
+    if (mf) {
+        *bytes_per_step = (int64_t)n * (24 + 4) + (int64_t)T.n_nodes * 4 + (int64_t)T.n_tets;
+    } else {
+        const int64_t vb = C.half_matrix ? 20 : 36;
+        const int64_t cb = c16 ? 2 : 4;
+        *bytes_per_step = T.sell.stored * (vb + cb) + (int64_t)(T.sell.n_slices + 1) * 8 + (int64_t)n * 24;
+    }
     T.total_launches += 3 + reps;
     return MSFEM_OK;
 }

@@ -273,6 +273,21 @@ class System:
               "spmv_scaled32")
         return y
 
+    def set_kuhn_grid(self, nx, ny=None, nz=None):
+        """Declares the mesh a structured Kuhn grid of nx x ny x nz hexahedra (the layout of
+        meshgen.kuhn_cube); checked on the device, MsfemError if the mesh is not that grid."""
+        ny = nx if ny is None else ny
+        nz = nx if nz is None else nz
+        check(load().msfem_set_kuhn_grid(self.h, int(nx), int(ny), int(nz)), "set_kuhn_grid")
+
+    def kuhn_spmv(self, x):
+        """y = A x formed matrix-free on the Kuhn grid from the tetrahedra's materials (FP64)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty(self.n_rows)
+        check(load().msfem_kuhn_spmv(self.h, x.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p), 0),
+              "kuhn_spmv")
+        return y
+
     def export_csr(self) -> Csr:
         rp = np.empty(self.n_rows + 1, dtype=np.int32)
         col = np.empty(self.nnz, dtype=np.int32)

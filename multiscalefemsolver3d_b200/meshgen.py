@@ -156,6 +156,21 @@ class ElasticProblem:
     traction: np.ndarray      # [f, 3]
 
 
+def kuhn_box(nx: int, ny: int, nz: int, size=(1.0, 1.0, 1.0), origin=(0.0, 0.0, 0.0)) -> Mesh:
+    """nx x ny x nz hexahedra on a box, six Kuhn tets each, in kuhn_cube's layout (node id
+    i + (nx+1) (j + (ny+1) k), hexahedron i + nx (j + ny k))."""
+    hx, hy, hz = size[0] / nx, size[1] / ny, size[2] / nz
+    k, j, i = np.meshgrid(np.arange(nz + 1.0), np.arange(ny + 1.0), np.arange(nx + 1.0), indexing="ij")
+    xyz = np.stack([i.ravel() * hx + origin[0], j.ravel() * hy + origin[1], k.ravel() * hz + origin[2]], axis=1)
+    ck, cj, ci = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    ci, cj, ck = ci.ravel(), cj.ravel(), ck.ravel()
+    corners = np.stack([(ci + (b & 1)) + (nx + 1) * ((cj + ((b >> 1) & 1)) + (ny + 1) * (ck + ((b >> 2) & 1)))
+                        for b in range(8)], axis=1)
+    tets = corners[:, KUHN_TETS].reshape(-1, 4).astype(np.int32)
+    return Mesh(xyz=xyz, tets=tets, mat=np.zeros(tets.shape[0], dtype=np.int32), n=nx,
+                meta={"box": (nx, ny, nz), "size": tuple(size)})
+
+
 @dataclass
 class ScalarProblem:
     mesh: Mesh

@@ -47,6 +47,8 @@ def main():
     ap.add_argument("--net", type=int, default=0, help="network forward passes over this many cells")
     ap.add_argument("--order2", type=int, default=0, help="batched Order2 bases of order2^3 macro cells")
     ap.add_argument("--maxiter", type=int, default=400000, help="two-level: MINRES iteration limit")
+    ap.add_argument("--matrix-free", action="store_true", help="two-level: matrix-free operators on the Kuhn grid")
+    ap.add_argument("--smoother-reps", type=int, default=0, help="two-level: time this many smoothing steps first")
     a = ap.parse_args()
     from . import fem, meshgen
     if a.order2:
@@ -56,7 +58,7 @@ def main():
     if a.cells:
         return cells_case(a.cells)
     if a.twolevel:
-        return twolevel_case(a.n, a.maxiter)
+        return twolevel_case(a.n, a.maxiter, a.matrix_free, a.smoother_reps)
     if a.elastic:
         p = meshgen.cube_elastic(n=a.n, n_spheres=200, contrast=100.0, rmin=0.02, rmax=0.06)
         S = fem.System(fem.ELASTIC, p.mesh.xyz, p.mesh.tets, p.mesh.mat)
@@ -115,7 +117,7 @@ def order2_case(nc):
     C.close()
 
 
-def twolevel_case(n, maxiter=400000):
+def twolevel_case(n, maxiter=400000, matrix_free=False, smoother_reps=0):
     import numpy as np
 
     from . import fem, meshgen
@@ -137,10 +139,20 @@ def twolevel_case(n, maxiter=400000):
     C.set_face_material("cells")
     rcb = C.build_bases(FP32_IR, 1e-8)
     T = TwoLevel(S, C, cc, dofs)
-    T.set_smoother(K, degree=3, half_matrix=True)
+    if matrix_free:
+        S.set_kuhn_grid(n)
+        K.set_kuhn_grid(n)
+        T.set_smoother(K, degree=3, matrix_free=True)
+        T.set_matrix_free(True)
+    else:
+        T.set_smoother(K, degree=3, half_matrix=True)
+    out_info = {}
+    if smoother_reps:
+        ms, nb = T.bench_smoother(reps=smoother_reps)
+        out_info = {"smoother_ms": ms, "smoother_bytes": nb, "smoother_gbs": nb / (ms * 1e-3) / 1e9}
     rel, it, out, rc = T.solve(tol=1e-8, maxiter=maxiter, precision=FP64)
-    print(json.dumps({"n": n, "dofs": S.n_rows, "rc_bases": rcb, "rc": rc, "rel": rel, "iterations": it,
-                      "ms_solve": S.stats()["ms_solve"]}))
+    print(json.dumps({"n": n, "dofs": S.n_rows, "matrix_free": matrix_free, "rc_bases": rcb, "rc": rc, "rel": rel,
+                      "iterations": it, "ms_solve": S.stats()["ms_solve"], **out_info}))
     T.close()
     C.close()
     K.close()

@@ -47,13 +47,19 @@ class TwoLevel:
                                                C.byref(it), C.byref(out)), "solve_twolevel")
         return rel.value, it.value, out.value, rc
 
-    def set_smoother(self, textbook_system, degree=3, ratio=30.0, half_matrix=False):
+    def set_smoother(self, textbook_system, degree=3, ratio=30.0, half_matrix=False, matrix_free=False):
         """Multiplicative cycle with Chebyshev smoothing on the textbook-orientation system
         (fem.System assembled with assemble_elastic_textbook, same Dirichlet rows); half_matrix
-        stores the smoother's matrix values in FP16."""
+        stores the smoother's matrix values in FP16; matrix_free applies the operator from the
+        tetrahedra's materials on the system's Kuhn grid (System.set_kuhn_grid)."""
         self._text = textbook_system
-        check(load().msfem_coarse_set_smoother(self.h, textbook_system.h, degree, ratio, int(half_matrix)),
+        storage = 2 if matrix_free else (1 if half_matrix else 0)
+        check(load().msfem_coarse_set_smoother(self.h, textbook_system.h, degree, ratio, storage),
               "coarse_set_smoother")
+
+    def set_matrix_free(self, on=True):
+        """MINRES's FP64 products with the fine matrix formed matrix-free on its Kuhn grid."""
+        check(load().msfem_coarse_set_matrix_free(self.h, int(bool(on))), "coarse_set_matrix_free")
 
     def bench_smoother(self, reps=100):
         """(ms per Chebyshev step, algorithmic bytes per step) of the cycle's smoothing kernel."""

@@ -111,21 +111,28 @@ def test_textbook_assembly_is_the_blockwise_transpose(case):
     del perm
 
 
-@pytest.fixture(scope="module", params=[False, True], ids=["fp32-smoother", "fp16-smoother"])
+@pytest.fixture(scope="module", params=[0, 1, 2], ids=["fp32-smoother", "fp16-smoother", "matrix-free"])
 def mg_case(lib, cuda, request):
     p, S, cc, cells, dofs = _setup()
     K = fem.System(fem.ELASTIC, p.mesh.xyz, p.mesh.tets, p.mesh.mat)
     K.assemble_elastic_textbook(p.E, p.nu)
     K.apply_dirichlet(dofs, np.zeros(dofs.size), fem.ROW_AND_COLUMN)
     T = TwoLevel(S, cells, cc, dofs)
-    T.set_smoother(K, degree=3, ratio=30.0, half_matrix=request.param)
+    if request.param == 2:
+        S.set_kuhn_grid(p.mesh.n)
+        K.set_kuhn_grid(p.mesh.n)
+        T.set_smoother(K, degree=3, ratio=30.0, matrix_free=True)
+        T.set_matrix_free(True)
+    else:
+        T.set_smoother(K, degree=3, ratio=30.0, half_matrix=request.param == 1)
     return p, S, K, T, dofs
 
 
 def test_multiplicative_cycle_solve(mg_case):
     """MINRES (FP64) on the reference's indefinite matrix with the multiplicative two-level cycle on
-    the textbook operator (smoother matrix in FP32 or FP16): the exact solution to 1e-8, in fewer
-    iterations than Jacobi MINRES."""
+    the textbook operator (smoother matrix in FP32, FP16, or formed matrix-free on the Kuhn grid
+    together with MINRES's own products): the exact solution to 1e-8, in fewer iterations than
+    Jacobi MINRES."""
     p, S, K, T, dofs = mg_case
     A = S.export_csr()
     x_exact = spl.spsolve(A.to_scipy().tocsc(), A.F)
