@@ -193,8 +193,8 @@ int apply_dirichlet(System& s, int L, const int32_t* d_dofs, const double* d_val
     k_dirichlet_rows<<<grid_for(L, 128), 128, 0, st>>>(L, sdof.p, spos.p, d_values, s.bs, s.nrp.p, s.ncol.p, s.val.p,
                                                        s.F.p, s.X.p, bad.p);
     if (!s.dmask.p) {
-        MSFEM_TRY(s.dmask.alloc((size_t)s.n_nodes));
-        MSFEM_CK(cudaMemsetAsync(s.dmask.p, 0, sizeof(uint32_t) * s.n_nodes, st));
+        MSFEM_TRY(s.dmask.alloc((size_t)s.n_nodes + 4));  // 4 words of slack: staging copies
+        MSFEM_CK(cudaMemsetAsync(s.dmask.p, 0, sizeof(uint32_t) * s.dmask.n, st));
     }
     k_dirichlet_mask<<<grid_for(L, 256), 256, 0, st>>>(L, d_dofs, s.bs, mode == MSFEM_ROW_AND_COLUMN, s.dmask.p,
                                                        bad.p);

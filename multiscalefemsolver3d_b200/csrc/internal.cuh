@@ -166,7 +166,8 @@ struct System {
     bool reference_order = false;    // MSFEM_PCG_SSOR in the reference's operation order (ssor.cu)
 
     // structured Kuhn grid (kuhn.cu): hexahedra per axis and spacing, set by msfem_set_kuhn_grid
-    // once the mesh is checked to be that grid; material code per tetrahedron
+    // once the mesh is checked to be that grid; per hexahedron the material codes of its six
+    // tetrahedra in bytes 0..5 of 8
     int kuhn_n[3] = {0, 0, 0};
     double kuhn_h[3] = {0.0, 0.0, 0.0};
     DBuf<uint8_t> kuhn_mat;

@@ -36,7 +36,8 @@ __global__ void k_kuhn_check_tets(int nx, int ny, int nz, const int32_t* __restr
         }
         const int m = mat ? mat[e] : 0;
         if (m < 0 || m >= kKuhnMaxMat) ok = false;
-        code[e] = (uint8_t)(m < 0 ? 0 : (m > 255 ? 255 : m));
+        code[8 * c + t] = (uint8_t)(m < 0 || m >= kKuhnMaxMat ? 0 : m);
+        if (t == 5) code[8 * c + 6] = code[8 * c + 7] = 0;
         if (!ok) atomicMin(bad, (int)(e < INT32_MAX ? e : INT32_MAX - 1));
     }
 }
@@ -155,7 +156,8 @@ int kuhn_set_grid(System& s, int nx, int ny, int nz)
     MSFEM_TRY(bad.alloc(2));
     const int big[2] = {INT32_MAX, INT32_MAX};
     MSFEM_CK(cudaMemcpyAsync(bad.p, big, sizeof(big), cudaMemcpyHostToDevice, st));
-    MSFEM_TRY(s.kuhn_mat.alloc((size_t)s.n_tets));
+    // 8 bytes per hexahedron (six codes + padding), and two hexahedra of slack for the staging copies
+    MSFEM_TRY(s.kuhn_mat.alloc(8 * (size_t)(s.n_tets / 6 + 2)));
     const unsigned g = std::min<unsigned>(grid_for(s.n_tets, 256), 148 * 16);
     k_kuhn_check_tets<<<g, 256, 0, st>>>(nx, ny, nz, s.tets.p, s.mat.p, s.kuhn_mat.p, bad.p);
     const double tol = 1e-9 * std::max(hx, std::max(hy, hz));
@@ -199,9 +201,17 @@ static void fill_view(const System& s, KuhnView<T>& v, int bx, int by, int bz)
         v.ih[a] = (T)(1.0 / s.kuhn_h[a]);
         v.vh[a] = (T)(V / s.kuhn_h[a]);
     }
-    v.mat = s.kuhn_mat.p;
+    v.mat = reinterpret_cast<const uint2*>(s.kuhn_mat.p);
     v.fix = s.dmask.p;
     v.n_mat = (int)(s.lame_host.size() / 2);
+    v.iso = 0;
+}
+
+// hx = hy = hz to 1e-12: the z-marching kernel folds V / h^2 into the material table
+static bool kuhn_isotropic(const System& s)
+{
+    const double h = s.kuhn_h[0];
+    return std::fabs(s.kuhn_h[1] - h) <= 1e-12 * h && std::fabs(s.kuhn_h[2] - h) <= 1e-12 * h;
 }
 
 int kuhn_operator_build(System& s, int form, bool fp64, bool scaled, KuhnOperator& op)
@@ -222,8 +232,8 @@ int kuhn_operator_build(System& s, int form, bool fp64, bool scaled, KuhnOperato
         return MSFEM_ERR_LIMIT;
     }
     if (!s.dmask.p) {  // no Dirichlet rows yet: an all-zero mask
-        MSFEM_TRY(s.dmask.alloc((size_t)s.n_nodes));
-        MSFEM_CK(cudaMemsetAsync(s.dmask.p, 0, sizeof(uint32_t) * s.n_nodes, s.stream));
+        MSFEM_TRY(s.dmask.alloc((size_t)s.n_nodes + 4));  // 4 words of slack: staging copies
+        MSFEM_CK(cudaMemsetAsync(s.dmask.p, 0, sizeof(uint32_t) * s.dmask.n, s.stream));
     }
     MSFEM_TRY(prepare_sell(s));  // the assembled product the check compares with, and the Jacobi scale
     cudaStream_t st = s.stream;
@@ -231,6 +241,8 @@ int kuhn_operator_build(System& s, int form, bool fp64, bool scaled, KuhnOperato
     op.form = form;
     op.fp64 = fp64;
     op.scaled = scaled;
+    MSFEM_TRY(op.err.alloc(1));
+    MSFEM_CK(cudaMemsetAsync(op.err.p, 0, sizeof(int), st));
     int dev = 0, sms = 0;
     MSFEM_CK(cudaGetDevice(&dev));
     MSFEM_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -246,17 +258,20 @@ int kuhn_operator_build(System& s, int form, bool fp64, bool scaled, KuhnOperato
         op.v64.scale = nullptr;
         op.v64.lame = op.lame64.p;
     } else {
+        const bool iso = kuhn_isotropic(s);
+        const double fold = iso ? s.kuhn_h[0] * s.kuhn_h[1] * s.kuhn_h[2] / 6.0 / (s.kuhn_h[0] * s.kuhn_h[0]) : 1.0;
         std::vector<float> l32(2 * (size_t)n_mat);
-        for (int i = 0; i < 2 * n_mat; i++) l32[i] = (float)s.lame_host[i];
+        for (int i = 0; i < 2 * n_mat; i++) l32[i] = (float)(s.lame_host[i] * fold);
         MSFEM_TRY(op.lame32.alloc(2 * (size_t)n_mat));
         MSFEM_CK(cudaMemcpyAsync(op.lame32.p, l32.data(), sizeof(float) * 2 * n_mat, cudaMemcpyHostToDevice, st));
         if (scaled) {
-            MSFEM_TRY(op.scale32.alloc((size_t)n));
+            MSFEM_TRY(op.scale32.alloc((size_t)n + 16));  // 16 elements of slack for the staging copies
             k_to_t<float><<<grid_for(n, 256), 256, 0, st>>>(n, s.dscale.p, op.scale32.p);
         }
         fill_view(s, op.v32, KuhnCfg32::BX, KuhnCfg32::BY, KuhnCfg32::BZ);
         op.v32.scale = scaled ? op.scale32.p : nullptr;
         op.v32.lame = op.lame32.p;
+        op.v32.iso = iso ? 1 : 0;
     }
     // the check: one probe vector through both products
     double rl2 = 0.0, rmax = 0.0;
@@ -276,7 +291,7 @@ int kuhn_operator_build(System& s, int form, bool fp64, bool scaled, KuhnOperato
         }
     } else {
         DBuf<float> x, y1, y2;
-        MSFEM_TRY(x.alloc(n));
+        MSFEM_TRY(x.alloc(n + 16));
         MSFEM_TRY(y1.alloc(n));
         MSFEM_TRY(y2.alloc(n));
         k_kuhn_probe<float><<<148 * 4, 256, 0, st>>>(n, x.p);
@@ -287,6 +302,7 @@ int kuhn_operator_build(System& s, int form, bool fp64, bool scaled, KuhnOperato
             set_error("matrix-free operator: the FP32 operator is the Jacobi-scaled one");
             return MSFEM_ERR_ARGUMENT;
         }
+        MSFEM_TRY(kuhn_check_err(op, st));
         MSFEM_TRY(compare<float>(st, n, y1.p, y2.p, &rl2, &rmax));
         if (!(rl2 <= 1e-5 && rmax <= 1e-4)) {
             set_error("matrix-free operator: its product differs from the assembled matrix's (relative %.3g in l2, "
@@ -342,12 +358,27 @@ int kuhn_spmv64(KuhnOperator& op, const double* x, double* y, cudaStream_t st)
 
 int kuhn_spmv32(KuhnOperator& op, const float* x, float* y, cudaStream_t st)
 {
-    EpiStore<float> e{y};
-    const int nb = op.v32.nbx * op.v32.nby * op.v32.nbz;
-    cudaError_t err = op.form == 2 ? kuhn_launch<2, KuhnCfg32>(op.v32, x, e, nb, op.sms, st)
-                                   : kuhn_launch<1, KuhnCfg32>(op.v32, x, e, nb, op.sms, st);
+    EpiStoreZ<float> e{y};
+    cudaError_t err = op.form == 2
+                          ? KzKernel<2, float, kKzTX, kKzTY, kKzMinB, EpiStoreZ<float>>::launch(op.v32, x, e, op.sms,
+                                                                                                 op.err.p, st)
+                          : KzKernel<1, float, kKzTX, kKzTY, kKzMinB, EpiStoreZ<float>>::launch(op.v32, x, e, op.sms,
+                                                                                                 op.err.p, st);
     if (err != cudaSuccess) {
         set_error("matrix-free FP32 product: %s", cudaGetErrorString(err));
+        return MSFEM_ERR_CUDA;
+    }
+    return MSFEM_OK;
+}
+
+int kuhn_check_err(KuhnOperator& op, cudaStream_t st)
+{
+    int h = 0;
+    MSFEM_CK(cudaMemcpyAsync(&h, op.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    if (h) {
+        MSFEM_CK(cudaMemsetAsync(op.err.p, 0, sizeof(int), st));
+        set_error("matrix-free product: a staging wait expired (bulk copies did not complete)");
         return MSFEM_ERR_CUDA;
     }
     return MSFEM_OK;

@@ -33,11 +33,12 @@ struct KuhnView {
     int nbx, nby, nbz;                  // bricks per axis
     T ih[3];                            // 1 / h per axis
     T vh[3];                            // V / h per axis (V = hx hy hz / 6)
-    const uint8_t* __restrict__ mat;    // material code per tetrahedron
+    const uint2* __restrict__ mat;      // per hexahedron the material codes of its six tetrahedra (bytes 0..5)
     const uint32_t* __restrict__ fix;   // per node: bit a = row 3n+a is a Dirichlet row; bit 3+a = column eliminated
     const T* __restrict__ scale;        // per DOF Jacobi scale of the operator S K S (nullptr: K itself)
-    const T* __restrict__ lame;         // [n_mat][2] lambda, mu
+    const T* __restrict__ lame;         // [n_mat][2] lambda, mu (iso: lambda V/h^2, mu V/h^2)
     int n_mat;
+    int iso;                            // hx = hy = hz and the table folded (kuhn_tet_iso)
 };
 
 // the forces of one tetrahedron {0, P, Q, 7} with corner path axes (A, B, C) on its corners
@@ -75,6 +76,47 @@ __device__ __forceinline__ void kuhn_tet(const T* u0, const T* up, const T* uq, 
     }
 }
 
+// The same forces on an isotropic grid (hx = hy = hz = h) with the material table holding
+// lambda V / h^2 and mu V / h^2: the gradient columns are the raw corner differences and the
+// column scaling is folded into the table (18 multiplies fewer); the textbook stress is formed
+// once per symmetric pair.
+template <int FORM, int A, int B, int C, class T>
+__device__ __forceinline__ void kuhn_tet_iso(const T* u0, const T* up, const T* uq, const T* u7, T lam, T mu, T* f0,
+                                             T* fp, T* fq, T* f7)
+{
+    T col[3][3];  // col[s][r] = h du_r / dx_s
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        col[A][r] = up[r] - u0[r];
+        col[B][r] = uq[r] - up[r];
+        col[C][r] = u7[r] - uq[r];
+    }
+    const T tr = col[0][0] + col[1][1] + col[2][2];
+    T sg[3][3];  // sg[s][r] = sigma[r][s], scaled
+    if (FORM == 2) {
+        const T lt = lam * tr, m2 = mu + mu;
+#pragma unroll
+        for (int r = 0; r < 3; r++) sg[r][r] = m2 * col[r][r] + lt;
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int s = r + 1; s < 3; s++) sg[s][r] = sg[r][s] = mu * (col[s][r] + col[r][s]);
+    } else {
+        const T mt = mu * tr;
+#pragma unroll
+        for (int s = 0; s < 3; s++)
+#pragma unroll
+            for (int r = 0; r < 3; r++) sg[s][r] = mu * col[s][r] + lam * col[r][s] + (r == s ? mt : T(0));
+    }
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        f0[r] -= sg[A][r];
+        fp[r] += sg[A][r] - sg[B][r];
+        fq[r] += sg[B][r] - sg[C][r];
+        f7[r] += sg[C][r];
+    }
+}
+
 // shared memory of one brick: staged input (3 components x halo nodes) + corner sums (24 x hexahedra)
 template <class T, int BX, int BY, int BZ>
 struct KuhnBrick {
@@ -96,33 +138,63 @@ __device__ __forceinline__ void kuhn_brick(const KuhnView<T>& K, const T* __rest
     const int bz = brick / (K.nbx * K.nby);
     const int i0 = bx * BX, j0 = by * BY, k0 = bz * BZ;
     const int nnx = K.nx + 1, nny = K.ny + 1, nnz = K.nz + 1;
-    // phase 0: staged u = s x on nodes i0-1 .. i0+BX (zero outside the grid and on eliminated columns)
-    for (int e = threadIdx.x; e < 3 * L::NH; e += THREADS) {
+    // phase 0: staged u = s x on nodes i0-1 .. i0+BX (zero outside the grid and on eliminated
+    // columns).  Every load of the phase is independent and issued before any is used (addresses
+    // clamped into the arrays, results selected afterwards), and the material codes of this
+    // thread's phase-1 hexahedra are fetched with them: one memory round trip per brick.
+    constexpr int kE0 = 3 * L::NH, kPer0 = (kE0 + THREADS - 1) / THREADS;
+    constexpr int kPer1 = (L::NC + THREADS - 1) / THREADS;
+    T xv[kPer0], sv[kPer0];
+    uint32_t fx[kPer0];
+    bool in0[kPer0];
+#pragma unroll
+    for (int r = 0; r < kPer0; r++) {
+        const int e = threadIdx.x + r * THREADS;
         const int row = e / (3 * L::HX);
         const int w = e - row * (3 * L::HX);
         const int hi = w / 3, a = w - 3 * hi;
         const int hj = row % L::HY, hk = row / L::HY;
         const int gi = i0 - 1 + hi, gj = j0 - 1 + hj, gk = k0 - 1 + hk;
-        T v = T(0);
-        if (gi >= 0 && gi < nnx && gj >= 0 && gj < nny && gk >= 0 && gk < nnz) {
-            const int64_t g = gi + (int64_t)nnx * (gj + (int64_t)nny * gk);
-            if (!((__ldg(K.fix + g) >> (3 + a)) & 1u)) {
-                v = __ldg(x + 3 * g + a);
-                if (K.scale) v *= __ldg(K.scale + 3 * g + a);
-            }
+        in0[r] = e < kE0 && gi >= 0 && gi < nnx && gj >= 0 && gj < nny && gk >= 0 && gk < nnz;
+        const int64_t g = in0[r] ? gi + (int64_t)nnx * (gj + (int64_t)nny * gk) : 0;
+        fx[r] = __ldg(K.fix + g);
+        xv[r] = __ldg(x + 3 * g + (in0[r] ? a : 0));
+        sv[r] = K.scale ? __ldg(K.scale + 3 * g + (in0[r] ? a : 0)) : T(1);
+    }
+    uint2 mc[kPer1];
+    bool in1[kPer1];
+#pragma unroll
+    for (int r = 0; r < kPer1; r++) {
+        const int c = threadIdx.x + r * THREADS;
+        const int ci = c % L::CX, cj = (c / L::CX) % L::CY, ck = c / (L::CX * L::CY);
+        const int gi = i0 - 1 + ci, gj = j0 - 1 + cj, gk = k0 - 1 + ck;
+        in1[r] = c < L::NC && gi >= 0 && gi < K.nx && gj >= 0 && gj < K.ny && gk >= 0 && gk < K.nz;
+        const int64_t cube = in1[r] ? gi + (int64_t)K.nx * (gj + (int64_t)K.ny * gk) : 0;
+        mc[r] = __ldg(K.mat + cube);
+    }
+#pragma unroll
+    for (int r = 0; r < kPer0; r++) {
+        const int e = threadIdx.x + r * THREADS;
+        if (e < kE0) {
+            const int row = e / (3 * L::HX);
+            const int w = e - row * (3 * L::HX);
+            const int hi = w / 3, a = w - 3 * hi;
+            const int hj = row % L::HY, hk = row / L::HY;
+            const bool keep = in0[r] && !((fx[r] >> (3 + a)) & 1u);
+            su[a * L::NH + hi + L::HX * (hj + L::HY * hk)] = keep ? xv[r] * sv[r] : T(0);
         }
-        su[a * L::NH + hi + L::HX * (hj + L::HY * hk)] = v;
     }
     __syncthreads();
     // phase 1: per hexahedron, the corner sums of its six tetrahedra
-    for (int c = threadIdx.x; c < L::NC; c += THREADS) {
+#pragma unroll
+    for (int r = 0; r < kPer1; r++) {
+        const int c = threadIdx.x + r * THREADS;
+        if (c >= L::NC) break;
         const int ci = c % L::CX, cj = (c / L::CX) % L::CY, ck = c / (L::CX * L::CY);
-        const int gi = i0 - 1 + ci, gj = j0 - 1 + cj, gk = k0 - 1 + ck;
         T f[8][3];
 #pragma unroll
         for (int b = 0; b < 8; b++) f[b][0] = f[b][1] = f[b][2] = T(0);
-        if (gi >= 0 && gi < K.nx && gj >= 0 && gj < K.ny && gk >= 0 && gk < K.nz) {
-            const int64_t cube = gi + (int64_t)K.nx * (gj + (int64_t)K.ny * gk);
+        if (in1[r]) {
             T u[8][3];
 #pragma unroll
             for (int b = 0; b < 8; b++) {
@@ -133,7 +205,7 @@ __device__ __forceinline__ void kuhn_brick(const KuhnView<T>& K, const T* __rest
             T lam[6], mu[6];
 #pragma unroll
             for (int t = 0; t < 6; t++) {
-                const int m = __ldg(K.mat + 6 * cube + t);
+                const int m = ((t < 4 ? mc[r].x >> (8 * t) : mc[r].y >> (8 * (t - 4)))) & 0xff;
                 lam[t] = slame[2 * m];
                 mu[t] = slame[2 * m + 1];
             }

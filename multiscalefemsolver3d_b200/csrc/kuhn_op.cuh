@@ -6,22 +6,23 @@
 
 #include "internal.cuh"
 #include "kuhn.cuh"
+#include "kuhn25.cuh"
 
 namespace msfem {
 
 // brick shapes: FP32 8 x 8 x 8 nodes (82 KB of shared memory, two CTAs per SM), FP64 8 x 8 x 4
 // (93 KB, two CTAs per SM)
 struct KuhnCfg32 {
-    static constexpr int BX = 8, BY = 8, BZ = 8, THREADS = 256;
+    static constexpr int BX = 8, BY = 8, BZ = 8, THREADS = 256, MINB = 2;
 };
 struct KuhnCfg64 {
-    static constexpr int BX = 8, BY = 8, BZ = 4, THREADS = 256;
+    static constexpr int BX = 8, BY = 8, BZ = 4, THREADS = 256, MINB = 2;
 };
 
 // persistent: CTA b takes bricks b, b + grid, ... (a fixed assignment, so block partial sums are
 // reproducible); the epilogue functor sees every owned node once and finishes the block
-template <int FORM, int BX, int BY, int BZ, int THREADS, class T, class Epi>
-__global__ void __launch_bounds__(THREADS) k_kuhn(KuhnView<T> K, const T* __restrict__ x, Epi epi)
+template <int FORM, int BX, int BY, int BZ, int THREADS, int MINB, class T, class Epi>
+__global__ void __launch_bounds__(THREADS, MINB) k_kuhn(KuhnView<T> K, const T* __restrict__ x, Epi epi)
 {
     if (epi.skip()) return;
     using L = KuhnBrick<T, BX, BY, BZ>;
@@ -39,7 +40,7 @@ __global__ void __launch_bounds__(THREADS) k_kuhn(KuhnView<T> K, const T* __rest
 template <int FORM, class Cfg, class T, class Epi>
 struct KuhnKernel {
     using L = KuhnBrick<T, Cfg::BX, Cfg::BY, Cfg::BZ>;
-    static constexpr auto kernel = k_kuhn<FORM, Cfg::BX, Cfg::BY, Cfg::BZ, Cfg::THREADS, T, Epi>;
+    static constexpr auto kernel = k_kuhn<FORM, Cfg::BX, Cfg::BY, Cfg::BZ, Cfg::THREADS, Cfg::MINB, T, Epi>;
     inline static int blocks_per_sm = 0;
     inline static uint64_t prepared = 0;  // devices (bit = ordinal) where the attribute is set
     // shared-memory opt-in and occupancy, per device; call outside stream capture before the
@@ -71,6 +72,75 @@ struct KuhnKernel {
     }
 };
 
+// the z-marching kernel (kuhn25.cuh): TX x TY hexahedron columns per CTA
+template <int FORM, class T, int TX, int TY, int MINB, class Epi>
+struct KzKernel {
+    using L = KzLayout<T, TX, TY, Epi::NE>;
+    static constexpr auto kernel_iso = k_kuhn_z<FORM, true, T, TX, TY, MINB, Epi>;
+    static constexpr auto kernel_aniso = k_kuhn_z<FORM, false, T, TX, TY, MINB, Epi>;
+    inline static int blocks_per_sm = 0;
+    inline static uint64_t prepared = 0;
+    static cudaError_t prepare()
+    {
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        const uint64_t bit = 1ull << (dev & 63);
+        if (prepared & bit) return cudaSuccess;
+        e = cudaFuncSetAttribute(kernel_iso, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::smem);
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(kernel_aniso, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::smem);
+        if (e != cudaSuccess) return e;
+        int nb = 0, nb2 = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel_iso, L::THREADS, L::smem);
+        if (e != cudaSuccess) return e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb2, kernel_aniso, L::THREADS, L::smem);
+        if (e != cudaSuccess) return e;
+        blocks_per_sm = std::max(std::min(nb, nb2), 1);
+        prepared |= bit;
+        return cudaSuccess;
+    }
+    // The bulk copies need 16-byte-aligned sources (and read up to 12 bytes past a vector's last
+    // element, so every staged vector carries 16 bytes of slack): refused here, never launched.
+    static bool aligned(const void* p) { return ((uintptr_t)p & 15) == 0; }
+    static cudaError_t launch(const KuhnView<T>& K, const T* x, const Epi& epi, int sms, int* err, cudaStream_t st)
+    {
+        cudaError_t e = prepare();
+        if (e != cudaSuccess) return e;
+        const T* ev[Epi::NE > 0 ? Epi::NE : 1] = {};
+        epi.sources(ev);
+        bool ok = aligned(x) && aligned(K.fix) && aligned(K.mat) && (!K.scale || aligned(K.scale));
+        for (int q = 0; q < Epi::NE; q++) ok = ok && aligned(ev[q]);
+        if (!ok) return cudaErrorMisalignedAddress;
+        KzArgs<T> A;
+        A.K = K;
+        A.x = x;
+        A.err = err;
+        A.tiles_x = (K.nx + 1 + L::OX - 1) / L::OX;
+        A.tiles_y = (K.ny + 1 + L::OY - 1) / L::OY;
+        const int nnz = K.nz + 1, tiles = A.tiles_x * A.tiles_y;
+        // z segments: the count that minimises waves x steps per CTA (a segment of s layers takes
+        // s + 1 steps; the CTAs run in ceil(tiles * segments / resident CTAs) waves)
+        const int64_t slots = (int64_t)blocks_per_sm * sms;
+        int64_t best = -1;
+        for (int n_seg = 1; n_seg <= nnz; n_seg++) {
+            const int len = (nnz + n_seg - 1) / n_seg;
+            const int segs = (nnz + len - 1) / len;
+            const int64_t cost = ((int64_t)tiles * segs + slots - 1) / slots * (len + 1);
+            if (best < 0 || cost < best) {
+                best = cost;
+                A.seg_len = len;
+                A.n_seg = segs;
+            }
+        }
+        if (K.iso)
+            kernel_iso<<<tiles * A.n_seg, L::THREADS, L::smem, st>>>(A, epi);
+        else
+            kernel_aniso<<<tiles * A.n_seg, L::THREADS, L::smem, st>>>(A, epi);
+        return cudaGetLastError();
+    }
+};
+
 template <int FORM, class Cfg, class T, class Epi>
 inline cudaError_t kuhn_launch(const KuhnView<T>& K, const T* x, const Epi& epi, int /*n_bricks*/, int sms,
                                cudaStream_t st)
@@ -87,6 +157,7 @@ struct KuhnOperator {
     bool scaled = false;
     int sms = 0;
     double check_l2 = 0.0, check_max = 0.0;  // relative distance to the assembled product at set-up
+    DBuf<int> err;       // raised by a z-marching launch whose staging wait expired
     DBuf<double> lame64;
     DBuf<float> lame32, scale32;
     KuhnView<double> v64{};
@@ -98,5 +169,27 @@ int kuhn_operator_build(System& s, int form, bool fp64, bool scaled, KuhnOperato
 int kuhn_operator_current(const KuhnOperator& op);
 int kuhn_spmv64(KuhnOperator& op, const double* x, double* y, cudaStream_t st);
 int kuhn_spmv32(KuhnOperator& op, const float* x, float* y, cudaStream_t st);
+// MSFEM_ERR_CUDA (and the flag cleared) if a z-marching launch on op raised its staging error
+int kuhn_check_err(KuhnOperator& op, cudaStream_t st);
+
+// y = op x (FP32) through the z-marching kernel
+template <class T>
+struct EpiStoreZ {
+    static constexpr int NE = 0;
+    T* y;
+    __device__ __forceinline__ bool skip() const { return false; }
+    __host__ __device__ __forceinline__ void sources(const T** ev) const { (void)ev; }
+    __device__ __forceinline__ void operator()(int64_t g, const T* v, const T* xin, const T (*e)[3])
+    {
+        (void)xin;
+        (void)e;
+        y[3 * g] = v[0];
+        y[3 * g + 1] = v[1];
+        y[3 * g + 2] = v[2];
+    }
+    __device__ __forceinline__ void finish() {}
+};
+// the z-marching FP32 configuration: 16 x 16 hexahedron columns (15 x 15 owned nodes), two CTAs per SM
+constexpr int kKzTX = 16, kKzTY = 16, kKzMinB = 2;
 
 }  // namespace msfem

@@ -848,60 +848,8 @@ __global__ void __launch_bounds__(256) k_mg_resid(SellView<float> A, const __hal
     }
 }
 
-// The same two smoothing kernels and the MINRES product on a Kuhn grid, matrix-free (kuhn.cuh):
-// epilogues of the brick kernel, applied to each owned node's product y.
-// one Chebyshev step (k_mg_cheb): res -= K^ dprev; d = a dprev + b res; x += d
-struct EpiCheb {
-    const float* __restrict__ dprev;
-    float* __restrict__ d;
-    float* __restrict__ res;
-    float* __restrict__ x;
-    float a, b;
-    const TlState* S;
-    __device__ __forceinline__ bool skip() const { return S->done; }
-    __device__ __forceinline__ void operator()(int64_t g, const float* y)
-    {
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-            const int64_t i = 3 * g + c;
-            const float ri = res[i] - y[c];
-            res[i] = ri;
-            const float di = a * dprev[i] + b * ri;
-            d[i] = di;
-            x[i] += di;
-        }
-    }
-    __device__ __forceinline__ void finish() {}
-};
-
-// res = rhat - K^ x; with `start` also d = res / theta, x2 = x + d (k_mg_resid)
-struct EpiResid {
-    const float* __restrict__ rhat;
-    const float* __restrict__ xin;
-    float* __restrict__ res;
-    float* __restrict__ d;
-    float* __restrict__ x2;
-    float inv_theta;
-    const TlState* S;
-    int start;
-    __device__ __forceinline__ bool skip() const { return S->done; }
-    __device__ __forceinline__ void operator()(int64_t g, const float* y)
-    {
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-            const int64_t i = 3 * g + c;
-            const float ri = rhat[i] - y[c];
-            res[i] = ri;
-            if (start) {
-                const float di = ri * inv_theta;
-                d[i] = di;
-                x2[i] = xin[i] + di;
-            }
-        }
-    }
-    __device__ __forceinline__ void finish() {}
-};
-
+// The MINRES product on a Kuhn grid, matrix-free (kuhn.cuh): the brick kernel's epilogue, applied
+// to each owned node's product.
 // v = y / beta; z = A y / beta - (beta / oldb) r1; alfa = (v, z) (k_tl_spmv<double>)
 struct EpiMinres {
     const double* __restrict__ y;
@@ -943,8 +891,66 @@ struct EpiMinres {
     }
 };
 
-using KCheb = KuhnKernel<2, KuhnCfg32, float, EpiCheb>;
-using KResid = KuhnKernel<2, KuhnCfg32, float, EpiResid>;
+// the smoothing kernels' epilogues on the z-marching kernel (kuhn25.cuh), whose per-node inputs
+// arrive staged: xin = the product's input at the node, e[q] = the staged vectors of sources()
+struct EpiChebZ {
+    static constexpr int NE = 2;  // res, x
+    float* __restrict__ d;
+    float* __restrict__ res;
+    float* __restrict__ x;
+    float a, b;
+    const TlState* S;
+    __device__ __forceinline__ bool skip() const { return S->done; }
+    __host__ __device__ __forceinline__ void sources(const float** ev) const
+    {
+        ev[0] = res;
+        ev[1] = x;
+    }
+    __device__ __forceinline__ void operator()(int64_t g, const float* y, const float* dprev, const float (*e)[3])
+    {
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const int64_t i = 3 * g + c;
+            const float ri = e[0][c] - y[c];
+            res[i] = ri;
+            const float di = a * dprev[c] + b * ri;
+            d[i] = di;
+            x[i] = e[1][c] + di;
+        }
+    }
+    __device__ __forceinline__ void finish() {}
+};
+
+struct EpiResidZ {
+    static constexpr int NE = 1;  // rhat
+    const float* __restrict__ rhat;
+    float* __restrict__ res;
+    float* __restrict__ d;
+    float* __restrict__ x2;
+    float inv_theta;
+    const TlState* S;
+    int start;
+    __device__ __forceinline__ bool skip() const { return S->done; }
+    __host__ __device__ __forceinline__ void sources(const float** ev) const { ev[0] = rhat; }
+    __device__ __forceinline__ void operator()(int64_t g, const float* y, const float* xin, const float (*e)[3])
+    {
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const int64_t i = 3 * g + c;
+            const float ri = e[0][c] - y[c];
+            res[i] = ri;
+            if (start) {
+                const float di = ri * inv_theta;
+                d[i] = di;
+                x2[i] = xin[c] + di;
+            }
+        }
+    }
+    __device__ __forceinline__ void finish() {}
+};
+
+using KCheb = KzKernel<2, float, kKzTX, kKzTY, kKzMinB, EpiChebZ>;
+using KResid = KzKernel<2, float, kKzTX, kKzTY, kKzMinB, EpiResidZ>;
 using KMinres = KuhnKernel<1, KuhnCfg64, double, EpiMinres>;
 
 // x += P^_t ec
@@ -1069,6 +1075,7 @@ struct CoarseHandle {
     ChebCoef cc{};
     DBuf<double> xkeep;         // X before the current refinement step (restored when the step fails)
     DBuf<float> psi_t, mgv;
+    int64_t ldv = 0;            // stride of the cycle's six FP32 vectors in mgv (16-byte aligned, with slack)
     DBuf<__half2> val16;  // FP16 copy of the textbook system's scaled SELL values, paired (when requested)
     DBuf<int16_t> col16;  // its block columns as 16-bit deltas (empty when some delta does not fit)
     bool half_matrix = false;
@@ -1423,12 +1430,13 @@ void mg_cycle(CoarseHandle& C, const double* z, const double* r2, double* r_out,
 {
     System& T = *C.text;
     const int n = T.n_rows;
+    const int64_t ld = C.ldv;
     float* rhat = C.mgv.p;
-    float* res = rhat + n;
-    float* dA = res + n;
-    float* dB = dA + n;
-    float* x = dB + n;
-    float* x2 = x + n;
+    float* res = rhat + ld;
+    float* dA = res + ld;
+    float* dB = dA + ld;
+    float* x = dB + ld;
+    float* x2 = x + ld;
     TlState* S = C.st.p;
     const SellView<float> At = sell_view<float>(T);
     const unsigned gsp = spmv_grid_of((const void*)k_mg_cheb, T);
@@ -1439,15 +1447,16 @@ void mg_cycle(CoarseHandle& C, const double* z, const double* r2, double* r_out,
     const bool mf = C.storage == 2;
     const KuhnView<float>& Kv = C.kt.v32;
     const int sms = C.kt.sms;
+    int* kerr = C.kt.err.p;
     auto cheb = [&](float* dprev, float* dnew, float* xx, int i) {
         if (mf)
-            KCheb::launch(Kv, dprev, EpiCheb{dprev, dnew, res, xx, C.cc.a[i], C.cc.b[i], S}, sms, st);
+            KCheb::launch(Kv, dprev, EpiChebZ{dnew, res, xx, C.cc.a[i], C.cc.b[i], S}, sms, kerr, st);
         else
             k_mg_cheb<<<gsp, 256, 0, st>>>(At, v16, c16, dprev, dnew, res, xx, C.cc.a[i], C.cc.b[i], S);
     };
     auto resid = [&](float* d0, float* x2, float inv_theta, int start) {
         if (mf)
-            KResid::launch(Kv, x, EpiResid{rhat, x, res, d0, x2, inv_theta, S, start}, sms, st);
+            KResid::launch(Kv, x, EpiResidZ{rhat, res, d0, x2, inv_theta, S, start}, sms, kerr, st);
         else
             k_mg_resid<<<gsp, 256, 0, st>>>(At, v16, c16, rhat, x, res, d0, x2, inv_theta, S, start);
     };
@@ -1588,12 +1597,13 @@ int set_smoother(CoarseHandle& C, System& T, int degree, double ratio, int stora
     const int n = T.n_rows;
     MSFEM_TRY(C.psi_t.alloc(24 * (size_t)C.n_fine));
     k_mg_psi<<<gridn(24 * (int64_t)C.n_fine), 256, 0, st>>>(C.n_fine, C.psi_hat.p, F.dscale.p, T.dscale.p, C.psi_t.p);
-    MSFEM_TRY(C.mgv.alloc(6 * (size_t)n));
+    C.ldv = (n + 16 + 63) / 64 * 64;  // 16-byte aligned sub-vectors with 16 elements of slack
+    MSFEM_TRY(C.mgv.alloc(6 * (size_t)C.ldv));
     // power iteration from a fixed pseudo-random start
     std::vector<float> h0(n);
     for (int i = 0; i < n; i++) h0[i] = (float)((hash32((unsigned)i) & 0xffff) / 65536.0 - 0.5);
     float* v = C.mgv.p;
-    float* w = v + n;
+    float* w = v + C.ldv;
     MSFEM_CK(cudaMemcpyAsync(v, h0.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st));
     DBuf<double> nb;
     MSFEM_TRY(nb.alloc(2));
@@ -1741,6 +1751,7 @@ int solve_twolevel(CoarseHandle& C, int precision, int maxiter, double tol, doub
     F.stats.rel_residual = *rel;
     *iters = total;
     *outer = k;
+    if (mg && C.storage == 2) MSFEM_TRY(kuhn_check_err(C.kt, st));
     if (rc == MSFEM_ERR_NUMERIC) {
         set_error("two-level solve: the inner MINRES broke down");
         return MSFEM_ERR_NUMERIC;
@@ -1911,11 +1922,12 @@ int msfem_coarse_bench_smoother(msfem_coarse_t c, int reps, double* ms_per_step,
     MSFEM_CK(cudaSetDevice(C.fine->device));
     cudaStream_t st = C.fine->stream;
     const int n = T.n_rows;
-    float* res = C.mgv.p + n;
-    float* dA = res + n;
-    float* dB = dA + n;
-    float* x = dB + n;
-    MSFEM_CK(cudaMemsetAsync(C.mgv.p, 0, sizeof(float) * 6 * (size_t)n, st));
+    const int64_t ld = C.ldv;
+    float* res = C.mgv.p + ld;
+    float* dA = res + ld;
+    float* dB = dA + ld;
+    float* x = dB + ld;
+    MSFEM_CK(cudaMemsetAsync(C.mgv.p, 0, sizeof(float) * 6 * (size_t)ld, st));
     DBuf<TlState> run;  // a state that is not done, so the kernel does its work
     MSFEM_TRY(run.alloc(1));
     MSFEM_CK(cudaMemsetAsync(run.p, 0, sizeof(TlState), st));
@@ -1929,7 +1941,7 @@ int msfem_coarse_bench_smoother(msfem_coarse_t c, int reps, double* ms_per_step,
         float* dp = (i & 1) ? dB : dA;
         float* dn = (i & 1) ? dA : dB;
         if (mf)
-            KCheb::launch(C.kt.v32, dp, EpiCheb{dp, dn, res, x, C.cc.a[1], C.cc.b[1], run.p}, C.kt.sms, st);
+            KCheb::launch(C.kt.v32, dp, EpiChebZ{dn, res, x, C.cc.a[1], C.cc.b[1], run.p}, C.kt.sms, C.kt.err.p, st);
         else
             k_mg_cheb<<<gsp, 256, 0, st>>>(At, v16, c16, dp, dn, res, x, C.cc.a[1], C.cc.b[1], run.p);
     };
@@ -1959,6 +1971,7 @@ int msfem_coarse_bench_smoother(msfem_coarse_t c, int reps, double* ms_per_step,
         *bytes_per_step = T.sell.stored * (vb + cb) + (int64_t)(T.sell.n_slices + 1) * 8 + (int64_t)n * 24;
     }
     T.total_launches += 3 + reps;
+    if (mf) MSFEM_TRY(kuhn_check_err(C.kt, st));
     return MSFEM_OK;
 }
 
