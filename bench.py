@@ -861,7 +861,8 @@ def run_twolevel(args, D):
     C = Cells(cc.cells)
     stream = torch.cuda.ExternalStream(S.stream, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    DEG, HALF = 3, True
+    # degree and spectrum ratio of the Chebyshev smoother: profiles/smoother_sweep_elastic_128.md
+    DEG, RATIO, HALF = 5, 100.0, True
     MF = args.operator == "matrix-free"
     if MF:  # the mesh's structure, checked once like the portraits
         S.set_kuhn_grid(args.n)
@@ -869,10 +870,10 @@ def run_twolevel(args, D):
 
     def smoother(T_, K_):
         if MF:
-            T_.set_smoother(K_, degree=DEG, matrix_free=True)
+            T_.set_smoother(K_, degree=DEG, ratio=RATIO, matrix_free=True)
             T_.set_matrix_free(True)
         else:
-            T_.set_smoother(K_, degree=DEG, half_matrix=HALF)
+            T_.set_smoother(K_, degree=DEG, ratio=RATIO, half_matrix=HALF)
 
     learned = args.coarse == "learned"
     net, train_info = None, {}

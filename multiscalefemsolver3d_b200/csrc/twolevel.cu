@@ -384,13 +384,88 @@ __global__ void __launch_bounds__(256) k_sweep_update(double* __restrict__ A, in
         for (int w = 0; w < 4; w++) A[(i0 + tr + 16 * u) * ld + j0 + tc + 16 * w] -= acc[u][w];
 }
 
-// C = -A (the swept matrix) in FP32, rows of length ld with zero columns past n
-__global__ void k_neg_to32(const double* __restrict__ A, int64_t ld, int n, float* __restrict__ C)
+// The coarse inverse is symmetric: only its upper 64 x 64 blocks (I <= J) are stored, packed row by
+// row of blocks, each block row-major, FP32 (half the bytes of the dense matrix).  ec = Cinv rc is
+// one CTA per stored block -- the block times rc_J gives block row I's share, its transpose times
+// rc_I (I < J) block row J's share -- into a partial per (block row, block column), then a fixed-
+// order sum over the block columns.
+constexpr int kSymB = 64;
+
+// pack -A (the swept matrix, FP64, leading dimension ld) into the upper blocks; zero past n
+__global__ void k_pack_sym(const double* __restrict__ A, int64_t ld, int n, const int2* __restrict__ blocks,
+                           int n_blocks, float* __restrict__ P)
 {
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < (int64_t)n * ld; t += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = t / ld, j = t % ld;
-        C[t] = j < n ? (float)(-A[i * ld + j]) : 0.0f;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < (int64_t)n_blocks * kSymB * kSymB;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = t / (kSymB * kSymB);
+        const int e = (int)(t - b * kSymB * kSymB), r = e / kSymB, c = e % kSymB;
+        const int i = blocks[b].x * kSymB + r, j = blocks[b].y * kSymB + c;
+        P[t] = (i < n && j < n) ? (float)(-A[(int64_t)i * ld + j]) : 0.0f;
     }
+}
+
+// per stored block (I, J): part[I][J] = C_IJ x_J and, for I < J, part[J][I] = C_IJ^T x_I.  Thread t
+// owns row t/4, columns 16 (t%4) .. +15; rows reduce over the 4 lanes of a row, columns over the
+// warp's 8 rows (shuffles), then over the 8 warps in shared memory, in fixed orders.
+__global__ void __launch_bounds__(256) k_tl_symv(int nb, const int2* __restrict__ blocks, const float* __restrict__ P,
+                                                 const float* __restrict__ x, float* __restrict__ part,
+                                                 const TlState* S)
+{
+    if (S->done) return;
+    __shared__ float colp[8][kSymB];
+    const int b = blockIdx.x;
+    const int I = blocks[b].x, J = blocks[b].y;
+    const int t = threadIdx.x, r = t >> 2, q = t & 3, lane = t & 31, warp = t >> 5;
+    const float* blk = P + (int64_t)b * kSymB * kSymB + r * kSymB + 16 * q;
+    const float* xj = x + J * kSymB + 16 * q;
+    const float xi = x[I * kSymB + r];
+    float rowsum = 0.0f, cs[16];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const float4 a = __ldcs(reinterpret_cast<const float4*>(blk) + k);
+        const float4 v = __ldg(reinterpret_cast<const float4*>(xj) + k);
+        rowsum += a.x * v.x + a.y * v.y + a.z * v.z + a.w * v.w;
+        cs[4 * k] = a.x * xi;
+        cs[4 * k + 1] = a.y * xi;
+        cs[4 * k + 2] = a.z * xi;
+        cs[4 * k + 3] = a.w * xi;
+    }
+    rowsum += __shfl_xor_sync(0xffffffffu, rowsum, 1);
+    rowsum += __shfl_xor_sync(0xffffffffu, rowsum, 2);
+    if (q == 0) part[((int64_t)I * nb + J) * kSymB + r] = rowsum;
+    if (I == J) return;  // uniform across the CTA
+#pragma unroll
+    for (int c = 0; c < 16; c++) {
+        float v = cs[c];
+        v += __shfl_xor_sync(0xffffffffu, v, 4);
+        v += __shfl_xor_sync(0xffffffffu, v, 8);
+        v += __shfl_xor_sync(0xffffffffu, v, 16);
+        cs[c] = v;
+    }
+    if (lane < 4)
+#pragma unroll
+        for (int c = 0; c < 16; c++) colp[warp][16 * lane + c] = cs[c];
+    __syncthreads();
+    if (t < kSymB) {
+        float v = 0.0f;
+#pragma unroll
+        for (int w = 0; w < 8; w++) v += colp[w][t];
+        part[((int64_t)J * nb + I) * kSymB + t] = v;
+    }
+}
+
+// y[i] = sum over block columns K of part[i / 64][K][i % 64], K ascending
+__global__ void k_tl_symv_sum(int n_pad, int nb, const float* __restrict__ part, float* __restrict__ y,
+                              const TlState* S)
+{
+    if (S->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_pad) return;
+    const int I = i / kSymB, r = i % kSymB;
+    const float* p = part + (int64_t)I * nb * kSymB + r;
+    float v = 0.0f;
+    for (int K = 0; K < nb; K++) v += p[(int64_t)K * kSymB];
+    y[i] = v;
 }
 
 // ---- preconditioner application kernels (FP32)
@@ -465,26 +540,6 @@ __global__ void k_tl_gather(int n_cf, const int32_t* __restrict__ dptr, const in
     }
 }
 
-// ec = Cinv rc, one warp per row; rows of length ld (a multiple of 64, zero padded, so every
-// float4 load is 16-byte aligned), x zero beyond n
-__global__ void __launch_bounds__(256) k_tl_gemv(int n, int ld, const float* __restrict__ C, const float* __restrict__ x,
-                                                 float* __restrict__ y, const TlState* S)
-{
-    if (S->done) return;
-    const int lane = threadIdx.x & 31;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += nw) {
-        const float* c = C + (int64_t)row * ld;
-        float s = 0.0f;
-        for (int k = lane * 4; k < ld; k += 128) {
-            const float4 a = __ldcs(reinterpret_cast<const float4*>(c + k));
-            const float4 b = __ldg(reinterpret_cast<const float4*>(x + k));
-            s += a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w;
-        }
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-        if (lane == 0) y[row] = s;
-    }
-}
 
 // bb = (r, M^-1 r) of the new Lanczos vector: beta' = sqrt(bb) and the MINRES Givens step;
 // init: the first application (beta1).  One thread.
@@ -685,6 +740,32 @@ __global__ void __launch_bounds__(kVecThreads) k_tl_correct(int n, double* __res
     const double sc = sqrt(S->bb);
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         X[i] += sc * (s ? s[i] : 1.0) * (double)x[i];
+}
+
+// the outer system's true residual after the inner correction so far: ||r - sqrt(bb) A x||^2 (the
+// inner MINRES solves for r / ||r||, r = the refinement step's residual) into *out
+__global__ void __launch_bounds__(kVecThreads) k_tl_true_norm(int n, const double* __restrict__ r,
+                                                             const double* __restrict__ ax, const TlState* S,
+                                                             double* __restrict__ partial, unsigned int* ticket,
+                                                             double* out)
+{
+    __shared__ double sh[32];
+    const double sc = sqrt(S->bb);
+    double acc[1] = {0.0};
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double d = r[i] - sc * ax[i];
+        acc[0] += d * d;
+    }
+    block_sum<1>(acc, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = acc[0];
+    if (arrive_last(ticket)) {
+        double t[1];
+        reduce_partials<1>(partial, gridDim.x, 0, t, sh);
+        if (threadIdx.x == 0) {
+            *out = t[0];
+            *ticket = 0;
+        }
+    }
 }
 
 // ---- symmetric multiplicative two-level cycle on the textbook operator (FP32, its
@@ -1056,7 +1137,10 @@ struct CoarseHandle {
     DBuf<int32_t> own_ptr, own;      // owned fine nodes per cell
     DBuf<float> psi_hat;             // [n_fine][24]
     DBuf<int32_t> dptr, dent;        // coarse DOF -> cell partial entries
-    DBuf<float> Cinv;                // [n_cf][n_cf]
+    DBuf<float> Csym;                // upper 64 x 64 blocks of the FP32 coarse inverse, packed
+    DBuf<int2> sym_blocks;           // (block row, block column) of each stored block
+    DBuf<float> sym_part;            // [nb][nb][64] partial products
+    int sym_nb = 0, sym_n = 0;
     DBuf<double> Ac;                 // dense coarse matrix (kept for inspection), n_cf x n_cf
     DBuf<float> cpart, rc, ec;
     DBuf<double> vec;                // 8 fine vectors (FP64 room; the FP32 solve uses the front half)
@@ -1074,6 +1158,8 @@ struct CoarseHandle {
     int n_trilinear = 0;        // cells whose wild bases were replaced by trilinear functions
     ChebCoef cc{};
     DBuf<double> xkeep;         // X before the current refinement step (restored when the step fails)
+    DBuf<double> rtmp, rr_true;  // the inner solve's true-residual check: A x, ||r - A x||^2
+    DBuf<unsigned int> tk;       // its reduction ticket
     DBuf<float> psi_t, mgv;
     int64_t ldv = 0;            // stride of the cycle's six FP32 vectors in mgv (16-byte aligned, with slack)
     DBuf<__half2> val16;  // FP16 copy of the textbook system's scaled SELL values, paired (when requested)
@@ -1299,8 +1385,22 @@ int coarse_build(CoarseHandle& C, System& F, CellsHandle& Ce, const int32_t* h_c
         set_error("msfem_coarse_create: the coarse matrix is not positive definite");
         return MSFEM_ERR_NUMERIC;
     }
-    MSFEM_TRY(C.Cinv.alloc((size_t)C.n_cf * ld));
-    k_neg_to32<<<gridn((int64_t)C.n_cf * ld), 256, 0, st>>>(W.p, ld, C.n_cf, C.Cinv.p);
+    {
+        const int nb = (int)(ld / kSymB);
+        std::vector<int2> hb;
+        hb.reserve((size_t)nb * (nb + 1) / 2);
+        for (int I = 0; I < nb; I++)
+            for (int J = I; J < nb; J++) hb.push_back(make_int2(I, J));
+        C.sym_nb = nb;
+        C.sym_n = (int)hb.size();
+        MSFEM_TRY(C.sym_blocks.alloc(hb.size()));
+        MSFEM_CK(cudaMemcpyAsync(C.sym_blocks.p, hb.data(), sizeof(int2) * hb.size(), cudaMemcpyHostToDevice, st));
+        MSFEM_TRY(C.Csym.alloc(hb.size() * kSymB * kSymB));
+        MSFEM_TRY(C.sym_part.alloc((size_t)nb * nb * kSymB));
+        k_pack_sym<<<gridn((int64_t)C.sym_n * kSymB * kSymB), 256, 0, st>>>(W.p, ld, C.n_cf, C.sym_blocks.p, C.sym_n,
+                                                                               C.Csym.p);
+        MSFEM_CK(cudaStreamSynchronize(st));  // the host block list is released here
+    }
     // solver storage
     const int n = F.n_rows;
     MSFEM_TRY(C.cpart.alloc(24 * (size_t)C.n_cells));
@@ -1321,6 +1421,13 @@ int coarse_build(CoarseHandle& C, System& F, CellsHandle& Ce, const int32_t* h_c
     return MSFEM_OK;
 }
 
+// ec = Cinv rc (symmetric packed blocks)
+void coarse_solve(CoarseHandle& C, const TlState* S, cudaStream_t st)
+{
+    k_tl_symv<<<C.sym_n, 256, 0, st>>>(C.sym_nb, C.sym_blocks.p, C.Csym.p, C.rc.p, C.sym_part.p, S);
+    k_tl_symv_sum<<<(C.n_pad + 255) / 256, 256, 0, st>>>(C.n_pad, C.sym_nb, C.sym_part.p, C.ec.p, S);
+}
+
 // y = M^-1 r into y (FP32: scaled system; FP64: original unknowns with s = D^-1/2);
 // init: also sets beta1 etc.
 template <class VT>
@@ -1329,7 +1436,7 @@ void precondition(CoarseHandle& C, const VT* r, VT* y, int init, cudaStream_t st
     k_tl_restrict<VT><<<C.n_cells, 128, 0, st>>>(C.own_ptr.p, C.own.p, C.psi_hat.p, r, nullptr, nullptr, C.cpart.p, s,
                                                  C.st.p, 0);
     k_tl_gather<<<gridn(C.n_cf), 256, 0, st>>>(C.n_cf, C.dptr.p, C.dent.p, C.cpart.p, C.rc.p, C.st.p);
-    k_tl_gemv<<<gridn((int64_t)C.n_cf * 32), 256, 0, st>>>(C.n_cf, C.n_pad, C.Cinv.p, C.rc.p, C.ec.p, C.st.p);
+    coarse_solve(C, C.st.p, st);
     k_tl_prolong<VT><<<gprol, kVecThreads, 0, st>>>(C.n_fine, C.owner.p, C.cdof.p, C.psi_hat.p, C.ec.p, r, y, s, C.st.p,
                                                     C.partial.p, init);
 }
@@ -1386,7 +1493,7 @@ int inner_solve(CoarseHandle& C, int maxiter, double tau, int* iters)
             // r2_new = z - (alfa/beta) r2 over r1's buffer, and its restriction partials
             k_tl_restrict<VT><<<C.n_cells, 128, 0, st>>>(C.own_ptr.p, C.own.p, C.psi_hat.p, Z, r2, r1, C.cpart.p, s, S, 1);
             k_tl_gather<<<gridn(C.n_cf), 256, 0, st>>>(C.n_cf, C.dptr.p, C.dent.p, C.cpart.p, C.rc.p, S);
-            k_tl_gemv<<<gridn((int64_t)C.n_cf * 32), 256, 0, st>>>(C.n_cf, C.n_pad, C.Cinv.p, C.rc.p, C.ec.p, S);
+            coarse_solve(C, S, st);
             k_tl_prolong<VT><<<gprol, kVecThreads, 0, st>>>(C.n_fine, C.owner.p, C.cdof.p, C.psi_hat.p, C.ec.p, r1, Y, s,
                                                             S, C.partial.p, 0);
             k_tl_update<VT><<<gvec, kVecThreads, 0, st>>>(n, V, w1, w2, X, S);
@@ -1467,7 +1574,7 @@ void mg_cycle(CoarseHandle& C, const double* z, const double* r2, double* r_out,
     k_tl_restrict<float><<<C.n_cells, 128, 0, st>>>(C.own_ptr.p, C.own.p, C.psi_t.p, res, nullptr, nullptr, C.cpart.p,
                                                     nullptr, S, 0);
     k_tl_gather<<<gridn(C.n_cf), 256, 0, st>>>(C.n_cf, C.dptr.p, C.dent.p, C.cpart.p, C.rc.p, S);
-    k_tl_gemv<<<gridn((int64_t)C.n_cf * 32), 256, 0, st>>>(C.n_cf, C.n_pad, C.Cinv.p, C.rc.p, C.ec.p, S);
+    coarse_solve(C, S, st);
     k_mg_prolong<<<gvec, kVecThreads, 0, st>>>(C.n_fine, C.owner.p, C.cdof.p, C.psi_t.p, C.ec.p, x, S);
     resid(dA, x2, C.cc.inv_theta, 1);
     for (int i = 1; i < C.cheb_deg; i++) cheb(d[(i - 1) & 1], d[i & 1], x2, i);
@@ -1475,7 +1582,10 @@ void mg_cycle(CoarseHandle& C, const double* z, const double* r2, double* r_out,
 }
 
 // FP64 MINRES on the original matrix with the multiplicative cycle as preconditioner
-int inner_solve_mg(CoarseHandle& C, int maxiter, double tau, int* iters)
+// stop2 > 0: also stop once the outer system's true residual, checked every 64 iterations (one
+// FP64 product), has fallen to stop2 (squared 2-norm) -- the preconditioned residual MINRES
+// tracks is in the cycle's norm, whose distance to the 2-norm depends on the smoother
+int inner_solve_mg(CoarseHandle& C, int maxiter, double tau, double stop2, int* iters)
 {
     System& F = *C.fine;
     cudaStream_t st = F.stream;
@@ -1535,11 +1645,37 @@ int inner_solve_mg(CoarseHandle& C, int maxiter, double tau, int* iters)
             return MSFEM_ERR_CUDA;
         }
     }
+    if (stop2 > 0.0) {
+        MSFEM_TRY(C.rtmp.alloc(n));
+        if (!C.tk.p) {
+            MSFEM_TRY(C.tk.alloc(1));
+            MSFEM_CK(cudaMemsetAsync(C.tk.p, 0, sizeof(unsigned int), st));
+        }
+        MSFEM_TRY(C.rr_true.alloc(1));
+    }
     int rounds = 0;
     for (;;) {
         MSFEM_TRY(read_st(C, st));
         if (C.h_st->done) break;
         if (16 * rounds > maxiter + 32) break;
+        if (stop2 > 0.0 && rounds > 0) {
+            if (C.mf_fine)
+                MSFEM_TRY(kuhn_spmv64(C.ka, X, C.rtmp.p, st));
+            else
+                MSFEM_TRY(spmv64(F, X, C.rtmp.p));
+            k_tl_true_norm<<<gvec, kVecThreads, 0, st>>>(n, C.r64.p, C.rtmp.p, S, C.partial.p + 1024, C.tk.p,
+                                                         C.rr_true.p);
+            double r2 = 0.0;
+            MSFEM_CK(cudaMemcpyAsync(&r2, C.rr_true.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+            MSFEM_CK(cudaStreamSynchronize(st));
+            F.total_launches += 2;
+            if (r2 <= stop2) {  // converged for the outer system: stop the inner solve here
+                C.h_st->done = 1;
+                MSFEM_CK(cudaMemcpyAsync(&S->done, &C.h_st->done, sizeof(int), cudaMemcpyHostToDevice, st));
+                MSFEM_CK(cudaStreamSynchronize(st));
+                break;
+            }
+        }
         for (int k = 0; k < 4; k++) MSFEM_CK(cudaGraphLaunch(graph, st));
         rounds += 4;
         F.total_launches += 4 * 16 * (11 + 2 * (C.cheb_deg - 1));
@@ -1723,7 +1859,7 @@ int solve_twolevel(CoarseHandle& C, int precision, int maxiter, double tol, doub
         const double tau = f32 ? std::max(1e-5, std::min(0.5, 0.3 * need))
                                : std::max(1e-14, (C.text ? 0.02 : 0.1) * need);
         int it = 0;
-        if (mg) rc = inner_solve_mg(C, maxiter - total, tau, &it);
+        if (mg) rc = inner_solve_mg(C, maxiter - total, tau, 0.81 * tol * tol * ff, &it);
         else rc = f32 ? inner_solve<float>(C, maxiter - total, tau, &it) : inner_solve<double>(C, maxiter - total, tau, &it);
         total += it;
         if (std::getenv("MSFEM_TRACE"))

@@ -49,6 +49,10 @@ def main():
     ap.add_argument("--maxiter", type=int, default=400000, help="two-level: MINRES iteration limit")
     ap.add_argument("--matrix-free", action="store_true", help="two-level: matrix-free operators on the Kuhn grid")
     ap.add_argument("--smoother-reps", type=int, default=0, help="two-level: time this many smoothing steps first")
+    ap.add_argument("--sweep-smoother", action="store_true",
+                    help="two-level at n^3: every Chebyshev degree of --degrees x ratio of --ratios")
+    ap.add_argument("--degrees", default="2,3,4,5")
+    ap.add_argument("--ratios", default="10,30,100")
     a = ap.parse_args()
     from . import fem, meshgen
     if a.order2:
@@ -59,6 +63,9 @@ def main():
         return cells_case(a.cells)
     if a.twolevel:
         return twolevel_case(a.n, a.maxiter, a.matrix_free, a.smoother_reps)
+    if a.sweep_smoother:
+        return smoother_sweep(a.n, [int(v) for v in a.degrees.split(",")], [float(v) for v in a.ratios.split(",")],
+                              a.maxiter)
     if a.elastic:
         p = meshgen.cube_elastic(n=a.n, n_spheres=200, contrast=100.0, rmin=0.02, rmax=0.06)
         S = fem.System(fem.ELASTIC, p.mesh.xyz, p.mesh.tets, p.mesh.mat)
@@ -117,6 +124,49 @@ def order2_case(nc):
     C.close()
 
 
+def smoother_sweep(n, degrees, ratios, maxiter=400000):
+    """The two-level solve of the heterogeneous elasticity case at n^3 (exact MsFEM bases, the
+    cells' own face materials, matrix-free operators) for every Chebyshev degree x spectrum ratio:
+    one JSON line each with iterations, solve time and ms per iteration."""
+    import numpy as np
+
+    from . import fem, meshgen
+    from .cells import FP32_IR, FP64, Cells
+    from .twolevel import TwoLevel
+    p = meshgen.heterogeneous_elasticity(n)
+    m = p.mesh
+    dofs = (3 * p.bc_nodes[:, None] + np.arange(3)).ravel().astype(np.int32)
+    zval = np.zeros(dofs.size)
+    S = fem.System(fem.ELASTIC, m.xyz, m.tets, m.mat)
+    S.add_traction(p.faces, p.traction)
+    S.assemble_elastic(p.E, p.nu)
+    S.apply_dirichlet(dofs, zval, fem.ROW_AND_COLUMN)
+    K = fem.System(fem.ELASTIC, m.xyz, m.tets, m.mat)
+    K.assemble_elastic_textbook(p.E, p.nu)
+    K.apply_dirichlet(dofs, zval, fem.ROW_AND_COLUMN)
+    S.set_kuhn_grid(n)
+    K.set_kuhn_grid(n)
+    cc = meshgen.cube_cells(m, p.E, p.nu, 8)
+    C = Cells(cc.cells)
+    C.set_face_material("cells")
+    C.build_bases(FP32_IR, 1e-8)
+    for deg in degrees:
+        for ratio in ratios:
+            T = TwoLevel(S, C, cc, dofs)
+            T.set_smoother(K, degree=deg, ratio=ratio, matrix_free=True)
+            T.set_matrix_free(True)
+            S.set_x(np.zeros(S.n_rows))
+            rel, it, out, rc = T.solve(tol=1e-8, maxiter=maxiter, precision=FP64)
+            ms = S.stats()["ms_solve"]
+            print(json.dumps({"n": n, "degree": deg, "ratio": ratio, "rc": rc, "rel": rel, "iterations": it,
+                              "ms_solve": ms, "ms_per_iteration": ms / max(1, it),
+                              "widened": T.stats()["widened"]}), flush=True)
+            T.close()
+    C.close()
+    K.close()
+    S.close()
+
+
 def twolevel_case(n, maxiter=400000, matrix_free=False, smoother_reps=0):
     import numpy as np
 
@@ -142,10 +192,10 @@ def twolevel_case(n, maxiter=400000, matrix_free=False, smoother_reps=0):
     if matrix_free:
         S.set_kuhn_grid(n)
         K.set_kuhn_grid(n)
-        T.set_smoother(K, degree=3, matrix_free=True)
+        T.set_smoother(K, matrix_free=True)
         T.set_matrix_free(True)
     else:
-        T.set_smoother(K, degree=3, half_matrix=True)
+        T.set_smoother(K, half_matrix=True)
     out_info = {}
     if smoother_reps:
         ms, nb = T.bench_smoother(reps=smoother_reps)

@@ -100,7 +100,7 @@ def _elastic_case(n=32):
 
 def _iterations(S, K, cc, dofs, C):
     T = TwoLevel(S, C, cc, dofs)
-    T.set_smoother(K, degree=3, half_matrix=True)
+    T.set_smoother(K, degree=3, ratio=30.0, half_matrix=True)
     S.set_x(np.zeros(S.n_rows))
     rel, it, _, rc = T.solve(tol=1e-8, maxiter=100000, precision=FP64)
     T.close()

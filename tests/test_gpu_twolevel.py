@@ -174,7 +174,7 @@ def test_wild_cell_bases_do_not_break_the_cycle(lib, cuda):
     A, _ = T.coarse_matrix()
     w = np.linalg.eigvalsh(A)
     assert w[0] > 0 and w[-1] / w[0] < 1e6
-    T.set_smoother(K, degree=3, half_matrix=True)
+    T.set_smoother(K, degree=3, ratio=30.0, half_matrix=True)
     S.set_x(np.zeros(S.n_rows))
     rel, it, _, rc = T.solve(tol=1e-8, maxiter=100000, precision=FP64)
     assert rc == 0 and rel <= 1e-8
