@@ -547,7 +547,8 @@ int msfem_kuhn_spmv(msfem_system_t h, const double* x, double* y, int on_device)
     KuhnOperator op;
     MSFEM_TRY(kuhn_operator_build(s, s.elastic_form, true, false, op));
     DBuf<double> dx, dy;
-    MSFEM_TRY(to_device(s, dx, x, (size_t)s.n_rows));
+    MSFEM_TRY(dx.alloc((size_t)s.n_rows + 16));  // slack for the staging copies
+    MSFEM_CK(cudaMemcpyAsync(dx.p, x, sizeof(double) * s.n_rows, cudaMemcpyDefault, s.stream));
     MSFEM_TRY(dy.alloc((size_t)s.n_rows));
     MSFEM_TRY(kuhn_spmv64(op, dx.p, dy.p, s.stream));
     MSFEM_CK(cudaMemcpyAsync(y, dy.p, sizeof(double) * s.n_rows, cudaMemcpyDefault, s.stream));

@@ -188,14 +188,11 @@ int kuhn_set_grid(System& s, int nx, int ny, int nz)
 }
 
 template <class T>
-static void fill_view(const System& s, KuhnView<T>& v, int bx, int by, int bz)
+static void fill_view(const System& s, KuhnView<T>& v)
 {
     v.nx = s.kuhn_n[0];
     v.ny = s.kuhn_n[1];
     v.nz = s.kuhn_n[2];
-    v.nbx = (v.nx + 1 + bx - 1) / bx;
-    v.nby = (v.ny + 1 + by - 1) / by;
-    v.nbz = (v.nz + 1 + bz - 1) / bz;
     const double V = s.kuhn_h[0] * s.kuhn_h[1] * s.kuhn_h[2] / 6.0;
     for (int a = 0; a < 3; a++) {
         v.ih[a] = (T)(1.0 / s.kuhn_h[a]);
@@ -252,11 +249,17 @@ int kuhn_operator_build(System& s, int form, bool fp64, bool scaled, KuhnOperato
             set_error("matrix-free operator: the FP64 operator is unscaled");
             return MSFEM_ERR_ARGUMENT;
         }
+        const bool iso = kuhn_isotropic(s);
+        const double fold = iso ? s.kuhn_h[0] * s.kuhn_h[1] * s.kuhn_h[2] / 6.0 / (s.kuhn_h[0] * s.kuhn_h[0]) : 1.0;
+        std::vector<double> l64(2 * (size_t)n_mat);
+        for (int i = 0; i < 2 * n_mat; i++) l64[i] = s.lame_host[i] * fold;
         MSFEM_TRY(op.lame64.alloc(2 * (size_t)n_mat));
-        MSFEM_CK(cudaMemcpyAsync(op.lame64.p, s.lame_host.data(), sizeof(double) * 2 * n_mat, cudaMemcpyHostToDevice, st));
-        fill_view(s, op.v64, KuhnCfg64::BX, KuhnCfg64::BY, KuhnCfg64::BZ);
+        MSFEM_CK(cudaMemcpyAsync(op.lame64.p, l64.data(), sizeof(double) * 2 * n_mat, cudaMemcpyHostToDevice, st));
+        MSFEM_CK(cudaStreamSynchronize(st));  // l64 is released here
+        fill_view(s, op.v64);
         op.v64.scale = nullptr;
         op.v64.lame = op.lame64.p;
+        op.v64.iso = iso ? 1 : 0;
     } else {
         const bool iso = kuhn_isotropic(s);
         const double fold = iso ? s.kuhn_h[0] * s.kuhn_h[1] * s.kuhn_h[2] / 6.0 / (s.kuhn_h[0] * s.kuhn_h[0]) : 1.0;
@@ -264,11 +267,12 @@ int kuhn_operator_build(System& s, int form, bool fp64, bool scaled, KuhnOperato
         for (int i = 0; i < 2 * n_mat; i++) l32[i] = (float)(s.lame_host[i] * fold);
         MSFEM_TRY(op.lame32.alloc(2 * (size_t)n_mat));
         MSFEM_CK(cudaMemcpyAsync(op.lame32.p, l32.data(), sizeof(float) * 2 * n_mat, cudaMemcpyHostToDevice, st));
+        MSFEM_CK(cudaStreamSynchronize(st));  // l32 is released here
         if (scaled) {
             MSFEM_TRY(op.scale32.alloc((size_t)n + 16));  // 16 elements of slack for the staging copies
             k_to_t<float><<<grid_for(n, 256), 256, 0, st>>>(n, s.dscale.p, op.scale32.p);
         }
-        fill_view(s, op.v32, KuhnCfg32::BX, KuhnCfg32::BY, KuhnCfg32::BZ);
+        fill_view(s, op.v32);
         op.v32.scale = scaled ? op.scale32.p : nullptr;
         op.v32.lame = op.lame32.p;
         op.v32.iso = iso ? 1 : 0;
@@ -277,12 +281,13 @@ int kuhn_operator_build(System& s, int form, bool fp64, bool scaled, KuhnOperato
     double rl2 = 0.0, rmax = 0.0;
     if (fp64) {
         DBuf<double> x, y1, y2;
-        MSFEM_TRY(x.alloc(n));
+        MSFEM_TRY(x.alloc(n + 16));
         MSFEM_TRY(y1.alloc(n));
         MSFEM_TRY(y2.alloc(n));
         k_kuhn_probe<double><<<148 * 4, 256, 0, st>>>(n, x.p);
         MSFEM_TRY(kuhn_spmv64(op, x.p, y1.p, st));
         MSFEM_TRY(spmv64(s, x.p, y2.p));
+        MSFEM_TRY(kuhn_check_err(op, st));
         MSFEM_TRY(compare<double>(st, n, y1.p, y2.p, &rl2, &rmax));
         if (!(rl2 <= 1e-12 && rmax <= 1e-11)) {
             set_error("matrix-free operator: its product differs from the assembled matrix's (relative %.3g in l2, "
@@ -328,27 +333,14 @@ int kuhn_operator_current(const KuhnOperator& op)
     return MSFEM_OK;
 }
 
-namespace {
-template <class T>
-struct EpiStore {
-    T* y;
-    __device__ __forceinline__ bool skip() const { return false; }
-    __device__ __forceinline__ void operator()(int64_t g, const T* v)
-    {
-        y[3 * g] = v[0];
-        y[3 * g + 1] = v[1];
-        y[3 * g + 2] = v[2];
-    }
-    __device__ __forceinline__ void finish() {}
-};
-}  // namespace
-
 int kuhn_spmv64(KuhnOperator& op, const double* x, double* y, cudaStream_t st)
 {
-    EpiStore<double> e{y};
-    const int nb = op.v64.nbx * op.v64.nby * op.v64.nbz;
-    cudaError_t err = op.form == 2 ? kuhn_launch<2, KuhnCfg64>(op.v64, x, e, nb, op.sms, st)
-                                   : kuhn_launch<1, KuhnCfg64>(op.v64, x, e, nb, op.sms, st);
+    EpiStoreZ<double> e{y};
+    cudaError_t err = op.form == 2
+                          ? KzKernel<2, false, double, kKzTX, kKzTY, kKzMinB64, EpiStoreZ<double>>::launch(
+                                op.v64, x, e, op.sms, op.err.p, st)
+                          : KzKernel<1, false, double, kKzTX, kKzTY, kKzMinB64, EpiStoreZ<double>>::launch(
+                                op.v64, x, e, op.sms, op.err.p, st);
     if (err != cudaSuccess) {
         set_error("matrix-free FP64 product: %s", cudaGetErrorString(err));
         return MSFEM_ERR_CUDA;
@@ -360,10 +352,10 @@ int kuhn_spmv32(KuhnOperator& op, const float* x, float* y, cudaStream_t st)
 {
     EpiStoreZ<float> e{y};
     cudaError_t err = op.form == 2
-                          ? KzKernel<2, float, kKzTX, kKzTY, kKzMinB, EpiStoreZ<float>>::launch(op.v32, x, e, op.sms,
-                                                                                                 op.err.p, st)
-                          : KzKernel<1, float, kKzTX, kKzTY, kKzMinB, EpiStoreZ<float>>::launch(op.v32, x, e, op.sms,
-                                                                                                 op.err.p, st);
+                          ? KzKernel<2, true, float, kKzTX, kKzTY, kKzMinB, EpiStoreZ<float>>::launch(
+                                op.v32, x, e, op.sms, op.err.p, st)
+                          : KzKernel<1, true, float, kKzTX, kKzTY, kKzMinB, EpiStoreZ<float>>::launch(
+                                op.v32, x, e, op.sms, op.err.p, st);
     if (err != cudaSuccess) {
         set_error("matrix-free FP32 product: %s", cudaGetErrorString(err));
         return MSFEM_ERR_CUDA;

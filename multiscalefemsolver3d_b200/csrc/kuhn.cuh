@@ -13,12 +13,7 @@
 // -- the two block formulas of k_assemble_elastic, summed over the element's columns -- so the
 // product of the assembled matrix with a vector needs only a material code per tetrahedron: about
 // 100 bytes per node (vectors included) instead of ~430 bytes of FP16 blocks or ~1.2 KB of FP64.
-//
-// One CTA owns a brick of BX x BY x BZ nodes.  Phase 0 stages the input on the brick's nodes and a
-// one-node halo in shared memory (scaled by the Jacobi scale, zero on eliminated Dirichlet
-// columns); phase 1 has one thread per hexahedron touching the brick add its six tetrahedra's
-// forces into its eight corner sums (fixed order); phase 2 gives each owned node the sum of the
-// eight hexahedra around it, corner 0 .. 7 in order.  No atomics: the product is deterministic.
+// The kernel that applies it is the z-marching one of kuhn25.cuh.
 #pragma once
 
 #include <cstdint>
@@ -30,7 +25,6 @@ constexpr int kKuhnMaxMat = 64;  // materials in the table a launch stages in sh
 template <class T>
 struct KuhnView {
     int nx, ny, nz;                     // hexahedra per axis
-    int nbx, nby, nbz;                  // bricks per axis
     T ih[3];                            // 1 / h per axis
     T vh[3];                            // V / h per axis (V = hx hy hz / 6)
     const uint2* __restrict__ mat;      // per hexahedron the material codes of its six tetrahedra (bytes 0..5)
@@ -114,138 +108,6 @@ __device__ __forceinline__ void kuhn_tet_iso(const T* u0, const T* up, const T* 
         fp[r] += sg[A][r] - sg[B][r];
         fq[r] += sg[B][r] - sg[C][r];
         f7[r] += sg[C][r];
-    }
-}
-
-// shared memory of one brick: staged input (3 components x halo nodes) + corner sums (24 x hexahedra)
-template <class T, int BX, int BY, int BZ>
-struct KuhnBrick {
-    static constexpr int HX = BX + 2, HY = BY + 2, HZ = BZ + 2;  // staged nodes
-    static constexpr int CX = BX + 1, CY = BY + 1, CZ = BZ + 1;  // hexahedra touching the brick
-    static constexpr int NH = HX * HY * HZ;
-    static constexpr int NC = CX * CY * CZ;
-    static constexpr size_t smem = sizeof(T) * (3 * (size_t)NH + 24 * (size_t)NC + 2 * kKuhnMaxMat);
-};
-
-// y = (S K S) x on brick `brick` (rows of Dirichlet DOFs: y = x); epi(node, y[3]) per owned node
-template <int FORM, int BX, int BY, int BZ, int THREADS, class T, class Epi>
-__device__ __forceinline__ void kuhn_brick(const KuhnView<T>& K, const T* __restrict__ x, int brick, T* su, T* sc,
-                                           const T* slame, Epi& epi)
-{
-    using L = KuhnBrick<T, BX, BY, BZ>;
-    const int bx = brick % K.nbx;
-    const int by = (brick / K.nbx) % K.nby;
-    const int bz = brick / (K.nbx * K.nby);
-    const int i0 = bx * BX, j0 = by * BY, k0 = bz * BZ;
-    const int nnx = K.nx + 1, nny = K.ny + 1, nnz = K.nz + 1;
-    // phase 0: staged u = s x on nodes i0-1 .. i0+BX (zero outside the grid and on eliminated
-    // columns).  Every load of the phase is independent and issued before any is used (addresses
-    // clamped into the arrays, results selected afterwards), and the material codes of this
-    // thread's phase-1 hexahedra are fetched with them: one memory round trip per brick.
-    constexpr int kE0 = 3 * L::NH, kPer0 = (kE0 + THREADS - 1) / THREADS;
-    constexpr int kPer1 = (L::NC + THREADS - 1) / THREADS;
-    T xv[kPer0], sv[kPer0];
-    uint32_t fx[kPer0];
-    bool in0[kPer0];
-#pragma unroll
-    for (int r = 0; r < kPer0; r++) {
-        const int e = threadIdx.x + r * THREADS;
-        const int row = e / (3 * L::HX);
-        const int w = e - row * (3 * L::HX);
-        const int hi = w / 3, a = w - 3 * hi;
-        const int hj = row % L::HY, hk = row / L::HY;
-        const int gi = i0 - 1 + hi, gj = j0 - 1 + hj, gk = k0 - 1 + hk;
-        in0[r] = e < kE0 && gi >= 0 && gi < nnx && gj >= 0 && gj < nny && gk >= 0 && gk < nnz;
-        const int64_t g = in0[r] ? gi + (int64_t)nnx * (gj + (int64_t)nny * gk) : 0;
-        fx[r] = __ldg(K.fix + g);
-        xv[r] = __ldg(x + 3 * g + (in0[r] ? a : 0));
-        sv[r] = K.scale ? __ldg(K.scale + 3 * g + (in0[r] ? a : 0)) : T(1);
-    }
-    uint2 mc[kPer1];
-    bool in1[kPer1];
-#pragma unroll
-    for (int r = 0; r < kPer1; r++) {
-        const int c = threadIdx.x + r * THREADS;
-        const int ci = c % L::CX, cj = (c / L::CX) % L::CY, ck = c / (L::CX * L::CY);
-        const int gi = i0 - 1 + ci, gj = j0 - 1 + cj, gk = k0 - 1 + ck;
-        in1[r] = c < L::NC && gi >= 0 && gi < K.nx && gj >= 0 && gj < K.ny && gk >= 0 && gk < K.nz;
-        const int64_t cube = in1[r] ? gi + (int64_t)K.nx * (gj + (int64_t)K.ny * gk) : 0;
-        mc[r] = __ldg(K.mat + cube);
-    }
-#pragma unroll
-    for (int r = 0; r < kPer0; r++) {
-        const int e = threadIdx.x + r * THREADS;
-        if (e < kE0) {
-            const int row = e / (3 * L::HX);
-            const int w = e - row * (3 * L::HX);
-            const int hi = w / 3, a = w - 3 * hi;
-            const int hj = row % L::HY, hk = row / L::HY;
-            const bool keep = in0[r] && !((fx[r] >> (3 + a)) & 1u);
-            su[a * L::NH + hi + L::HX * (hj + L::HY * hk)] = keep ? xv[r] * sv[r] : T(0);
-        }
-    }
-    __syncthreads();
-    // phase 1: per hexahedron, the corner sums of its six tetrahedra
-#pragma unroll
-    for (int r = 0; r < kPer1; r++) {
-        const int c = threadIdx.x + r * THREADS;
-        if (c >= L::NC) break;
-        const int ci = c % L::CX, cj = (c / L::CX) % L::CY, ck = c / (L::CX * L::CY);
-        T f[8][3];
-#pragma unroll
-        for (int b = 0; b < 8; b++) f[b][0] = f[b][1] = f[b][2] = T(0);
-        if (in1[r]) {
-            T u[8][3];
-#pragma unroll
-            for (int b = 0; b < 8; b++) {
-                const int h = (ci + (b & 1)) + L::HX * ((cj + ((b >> 1) & 1)) + L::HY * (ck + ((b >> 2) & 1)));
-#pragma unroll
-                for (int a = 0; a < 3; a++) u[b][a] = su[a * L::NH + h];
-            }
-            T lam[6], mu[6];
-#pragma unroll
-            for (int t = 0; t < 6; t++) {
-                const int m = ((t < 4 ? mc[r].x >> (8 * t) : mc[r].y >> (8 * (t - 4)))) & 0xff;
-                lam[t] = slame[2 * m];
-                mu[t] = slame[2 * m + 1];
-            }
-            // {0,1,3,7}: x y z   {0,1,5,7}: x z y   {0,2,3,7}: y x z
-            // {0,2,6,7}: y z x   {0,4,5,7}: z x y   {0,4,6,7}: z y x
-            kuhn_tet<FORM, 0, 1, 2>(u[0], u[1], u[3], u[7], lam[0], mu[0], K.ih, K.vh, f[0], f[1], f[3], f[7]);
-            kuhn_tet<FORM, 0, 2, 1>(u[0], u[1], u[5], u[7], lam[1], mu[1], K.ih, K.vh, f[0], f[1], f[5], f[7]);
-            kuhn_tet<FORM, 1, 0, 2>(u[0], u[2], u[3], u[7], lam[2], mu[2], K.ih, K.vh, f[0], f[2], f[3], f[7]);
-            kuhn_tet<FORM, 1, 2, 0>(u[0], u[2], u[6], u[7], lam[3], mu[3], K.ih, K.vh, f[0], f[2], f[6], f[7]);
-            kuhn_tet<FORM, 2, 0, 1>(u[0], u[4], u[5], u[7], lam[4], mu[4], K.ih, K.vh, f[0], f[4], f[5], f[7]);
-            kuhn_tet<FORM, 2, 1, 0>(u[0], u[4], u[6], u[7], lam[5], mu[5], K.ih, K.vh, f[0], f[4], f[6], f[7]);
-        }
-#pragma unroll
-        for (int b = 0; b < 8; b++)
-#pragma unroll
-            for (int a = 0; a < 3; a++) sc[(3 * b + a) * L::NC + c] = f[b][a];
-    }
-    __syncthreads();
-    // phase 2: each owned node sums its eight hexahedra (corner b of hexahedron node - offset(b))
-    for (int q = threadIdx.x; q < BX * BY * BZ; q += THREADS) {
-        const int ni = q % BX, nj = (q / BX) % BY, nk = q / (BX * BY);
-        const int gi = i0 + ni, gj = j0 + nj, gk = k0 + nk;
-        if (gi >= nnx || gj >= nny || gk >= nnz) continue;
-        const int64_t g = gi + (int64_t)nnx * (gj + (int64_t)nny * gk);
-        T y[3] = {T(0), T(0), T(0)};
-#pragma unroll
-        for (int b = 0; b < 8; b++) {
-            const int c = (ni + 1 - (b & 1)) + L::CX * ((nj + 1 - ((b >> 1) & 1)) + L::CY * (nk + 1 - ((b >> 2) & 1)));
-#pragma unroll
-            for (int a = 0; a < 3; a++) y[a] += sc[(3 * b + a) * L::NC + c];
-        }
-        const uint32_t fx = __ldg(K.fix + g);
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-            if ((fx >> a) & 1u)
-                y[a] = __ldg(x + 3 * g + a);
-            else if (K.scale)
-                y[a] *= __ldg(K.scale + 3 * g + a);
-        }
-        epi(g, y);
     }
 }
 

@@ -29,9 +29,10 @@ namespace msfem {
 
 __host__ __device__ constexpr int kz_round_up(int v, int m) { return (v + m - 1) / m * m; }
 
-template <class T, int TX_, int TY_, int NE_>
+template <class T, int TX_, int TY_, int NE_, bool SC_>
 struct KzLayout {
     static constexpr int TX = TX_, TY = TY_, NE = NE_;
+    static constexpr bool SC = SC_;                 // a Jacobi scale is staged (S K S)
     static constexpr int THREADS = TX * TY;        // one thread per hexahedron column
     static constexpr int WX = TX + 1, WY = TY + 1;  // staged node window per layer
     static constexpr int OX = TX - 1, OY = TY - 1;  // owned nodes per layer
@@ -43,7 +44,7 @@ struct KzLayout {
     // one stage, bytes (every part a multiple of 16)
     static constexpr int X_OFF = 0;
     static constexpr int S_OFF = X_OFF + WY * XP * (int)sizeof(T);
-    static constexpr int F_OFF = S_OFF + WY * XP * (int)sizeof(T);
+    static constexpr int F_OFF = S_OFF + (SC ? WY * XP * (int)sizeof(T) : 0);
     static constexpr int M_OFF = F_OFF + WY * FP * 4;
     static constexpr int STAGE = M_OFF + TY * MP * 8;
     // after the ring: two converted layers, bottom corner sums, two sets of top corner sums, barriers.
@@ -133,7 +134,7 @@ __device__ __forceinline__ KzCopy kz_copy_of(const KuhnView<T>& K, int i0, int j
     if (q < 3 * L::WY) {
         const int part = q / L::WY, wj = q - part * L::WY;
         const int gj = j0 - 1 + wj;
-        if (gj >= 0 && gj < nny && (part != 1 || K.scale)) {
+        if (gj >= 0 && gj < nny && (part != 1 || L::SC)) {
             c.kind = part;
             c.lo0 = gi_lo + (int64_t)nnx * gj;
             c.cnt = gi_hi - gi_lo + 1;
@@ -189,10 +190,10 @@ __device__ __forceinline__ void kz_issue(const KzArgs<T>& A, const KzCopy& c, in
 
 // the z-marching product; Epi: NE per-node input vectors (sources(ev)), skip(), finish(),
 // operator()(node, y[3], input x[3], e[NE][3] = those vectors at the node)
-template <int FORM, bool ISO, class T, int TX, int TY, int MINB, class Epi>
+template <int FORM, bool ISO, bool SC, class T, int TX, int TY, int MINB, class Epi>
 __global__ void __launch_bounds__(TX* TY, MINB) k_kuhn_z(KzArgs<T> A, Epi epi)
 {
-    using L = KzLayout<T, TX, TY, Epi::NE>;
+    using L = KzLayout<T, TX, TY, Epi::NE, SC>;
     if (epi.skip()) return;
     extern __shared__ __align__(128) unsigned char kz_smem[];
     const KuhnView<T>& K = A.K;
@@ -250,7 +251,7 @@ __global__ void __launch_bounds__(TX* TY, MINB) k_kuhn_z(KzArgs<T> A, Epi epi)
 #pragma unroll
                 for (int a = 0; a < 3; a++) {
                     T t = xr[xo + a];
-                    if (K.scale) t *= sr[xo + a];
+                    if (SC) t *= sr[xo + a];
                     v[a] = ((fx >> (3 + a)) & 1u) ? T(0) : t;
                 }
             }
@@ -377,7 +378,7 @@ __global__ void __launch_bounds__(TX* TY, MINB) k_kuhn_z(KzArgs<T> A, Epi epi)
                 xin[a] = xr[wj * L::XP + xo + a];
                 if ((fx >> a) & 1u)
                     y[a] = xin[a];
-                else if (K.scale)
+                else if (SC)
                     y[a] *= sr[wj * L::XP + xo + a];
             }
             epi(gk, y, xin, e);

@@ -1,5 +1,5 @@
-// Host side of the matrix-free Kuhn-grid operators (kuhn.cuh): the persistent kernel over bricks,
-// its launch configuration, and the operator state a solver keeps.
+// Host side of the matrix-free Kuhn-grid operators (kuhn.cuh, kuhn25.cuh): the z-marching kernel's
+// launch configuration and the operator state a solver keeps.
 #pragma once
 
 #include <algorithm>
@@ -10,74 +10,12 @@
 
 namespace msfem {
 
-// brick shapes: FP32 8 x 8 x 8 nodes (82 KB of shared memory, two CTAs per SM), FP64 8 x 8 x 4
-// (93 KB, two CTAs per SM)
-struct KuhnCfg32 {
-    static constexpr int BX = 8, BY = 8, BZ = 8, THREADS = 256, MINB = 2;
-};
-struct KuhnCfg64 {
-    static constexpr int BX = 8, BY = 8, BZ = 4, THREADS = 256, MINB = 2;
-};
-
-// persistent: CTA b takes bricks b, b + grid, ... (a fixed assignment, so block partial sums are
-// reproducible); the epilogue functor sees every owned node once and finishes the block
-template <int FORM, int BX, int BY, int BZ, int THREADS, int MINB, class T, class Epi>
-__global__ void __launch_bounds__(THREADS, MINB) k_kuhn(KuhnView<T> K, const T* __restrict__ x, Epi epi)
-{
-    if (epi.skip()) return;
-    using L = KuhnBrick<T, BX, BY, BZ>;
-    extern __shared__ __align__(16) unsigned char kuhn_smem[];
-    T* su = reinterpret_cast<T*>(kuhn_smem);
-    T* sc = su + 3 * L::NH;
-    T* sl = sc + 24 * L::NC;
-    kuhn_stage_lame(K, sl);
-    __syncthreads();
-    const int nb = K.nbx * K.nby * K.nbz;
-    for (int b = blockIdx.x; b < nb; b += gridDim.x) kuhn_brick<FORM, BX, BY, BZ, THREADS>(K, x, b, su, sc, sl, epi);
-    epi.finish();
-}
-
-template <int FORM, class Cfg, class T, class Epi>
-struct KuhnKernel {
-    using L = KuhnBrick<T, Cfg::BX, Cfg::BY, Cfg::BZ>;
-    static constexpr auto kernel = k_kuhn<FORM, Cfg::BX, Cfg::BY, Cfg::BZ, Cfg::THREADS, Cfg::MINB, T, Epi>;
-    inline static int blocks_per_sm = 0;
-    inline static uint64_t prepared = 0;  // devices (bit = ordinal) where the attribute is set
-    // shared-memory opt-in and occupancy, per device; call outside stream capture before the
-    // first launch on a device
-    static cudaError_t prepare()
-    {
-        int dev = 0;
-        cudaError_t e = cudaGetDevice(&dev);
-        if (e != cudaSuccess) return e;
-        const uint64_t bit = 1ull << (dev & 63);
-        if (prepared & bit) return cudaSuccess;
-        e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::smem);
-        if (e != cudaSuccess) return e;
-        int nb = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, Cfg::THREADS, L::smem);
-        if (e != cudaSuccess) return e;
-        blocks_per_sm = std::max(nb, 1);
-        prepared |= bit;
-        return cudaSuccess;
-    }
-    static int grid(int n_bricks, int sms) { return std::max(1, std::min(n_bricks, blocks_per_sm * sms)); }
-    static cudaError_t launch(const KuhnView<T>& K, const T* x, const Epi& epi, int sms, cudaStream_t st)
-    {
-        cudaError_t e = prepare();
-        if (e != cudaSuccess) return e;
-        const int nb = K.nbx * K.nby * K.nbz;
-        kernel<<<grid(nb, sms), Cfg::THREADS, L::smem, st>>>(K, x, epi);
-        return cudaGetLastError();
-    }
-};
-
 // the z-marching kernel (kuhn25.cuh): TX x TY hexahedron columns per CTA
-template <int FORM, class T, int TX, int TY, int MINB, class Epi>
+template <int FORM, bool SC, class T, int TX, int TY, int MINB, class Epi>
 struct KzKernel {
-    using L = KzLayout<T, TX, TY, Epi::NE>;
-    static constexpr auto kernel_iso = k_kuhn_z<FORM, true, T, TX, TY, MINB, Epi>;
-    static constexpr auto kernel_aniso = k_kuhn_z<FORM, false, T, TX, TY, MINB, Epi>;
+    using L = KzLayout<T, TX, TY, Epi::NE, SC>;
+    static constexpr auto kernel_iso = k_kuhn_z<FORM, true, SC, T, TX, TY, MINB, Epi>;
+    static constexpr auto kernel_aniso = k_kuhn_z<FORM, false, SC, T, TX, TY, MINB, Epi>;
     inline static int blocks_per_sm = 0;
     inline static uint64_t prepared = 0;
     static cudaError_t prepare()
@@ -109,8 +47,8 @@ struct KzKernel {
         if (e != cudaSuccess) return e;
         const T* ev[Epi::NE > 0 ? Epi::NE : 1] = {};
         epi.sources(ev);
-        bool ok = aligned(x) && aligned(K.fix) && aligned(K.mat) && (!K.scale || aligned(K.scale));
-        for (int q = 0; q < Epi::NE; q++) ok = ok && aligned(ev[q]);
+        bool ok = aligned(x) && aligned(K.fix) && aligned(K.mat) && (SC ? (K.scale && aligned(K.scale)) : !K.scale);
+        for (int q = 0; q < Epi::NE; q++) ok = ok && ev[q];
         if (!ok) return cudaErrorMisalignedAddress;
         KzArgs<T> A;
         A.K = K;
@@ -141,13 +79,6 @@ struct KzKernel {
     }
 };
 
-template <int FORM, class Cfg, class T, class Epi>
-inline cudaError_t kuhn_launch(const KuhnView<T>& K, const T* x, const Epi& epi, int /*n_bricks*/, int sms,
-                               cudaStream_t st)
-{
-    return KuhnKernel<FORM, Cfg, T, Epi>::launch(K, x, epi, sms, st);
-}
-
 // one matrix-free operator, checked against the assembled matrix of `sys` at values_version
 struct KuhnOperator {
     System* sys = nullptr;
@@ -172,7 +103,7 @@ int kuhn_spmv32(KuhnOperator& op, const float* x, float* y, cudaStream_t st);
 // MSFEM_ERR_CUDA (and the flag cleared) if a z-marching launch on op raised its staging error
 int kuhn_check_err(KuhnOperator& op, cudaStream_t st);
 
-// y = op x (FP32) through the z-marching kernel
+// y = op x through the z-marching kernel
 template <class T>
 struct EpiStoreZ {
     static constexpr int NE = 0;
@@ -189,7 +120,8 @@ struct EpiStoreZ {
     }
     __device__ __forceinline__ void finish() {}
 };
-// the z-marching FP32 configuration: 16 x 16 hexahedron columns (15 x 15 owned nodes), two CTAs per SM
-constexpr int kKzTX = 16, kKzTY = 16, kKzMinB = 2;
+// the z-marching configurations: 16 x 16 hexahedron columns (15 x 15 owned nodes); FP32 two CTAs
+// per SM, FP64 one
+constexpr int kKzTX = 16, kKzTY = 16, kKzMinB = 2, kKzMinB64 = 1;
 
 }  // namespace msfem

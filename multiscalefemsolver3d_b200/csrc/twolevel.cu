@@ -406,51 +406,58 @@ __global__ void k_pack_sym(const double* __restrict__ A, int64_t ld, int n, cons
 
 // per stored block (I, J): part[I][J] = C_IJ x_J and, for I < J, part[J][I] = C_IJ^T x_I.  Thread t
 // owns row t/4, columns 16 (t%4) .. +15; rows reduce over the 4 lanes of a row, columns over the
-// warp's 8 rows (shuffles), then over the 8 warps in shared memory, in fixed orders.
-__global__ void __launch_bounds__(256) k_tl_symv(int nb, const int2* __restrict__ blocks, const float* __restrict__ P,
-                                                 const float* __restrict__ x, float* __restrict__ part,
-                                                 const TlState* S)
+// warp's 8 rows (shuffles), then over the 8 warps in shared memory, in fixed orders.  Persistent:
+// CTA c takes blocks c, c + grid, ...
+__global__ void __launch_bounds__(256) k_tl_symv(int nb, int n_blocks, const int2* __restrict__ blocks,
+                                                 const float* __restrict__ P, const float* __restrict__ x,
+                                                 float* __restrict__ part, const TlState* S)
 {
     if (S->done) return;
     __shared__ float colp[8][kSymB];
-    const int b = blockIdx.x;
-    const int I = blocks[b].x, J = blocks[b].y;
     const int t = threadIdx.x, r = t >> 2, q = t & 3, lane = t & 31, warp = t >> 5;
-    const float* blk = P + (int64_t)b * kSymB * kSymB + r * kSymB + 16 * q;
-    const float* xj = x + J * kSymB + 16 * q;
-    const float xi = x[I * kSymB + r];
-    float rowsum = 0.0f, cs[16];
+    for (int b = blockIdx.x; b < n_blocks; b += gridDim.x) {
+        const int I = blocks[b].x, J = blocks[b].y;
+        const float4* blk = reinterpret_cast<const float4*>(P + (int64_t)b * kSymB * kSymB + r * kSymB + 16 * q);
+        const float4* xj = reinterpret_cast<const float4*>(x + J * kSymB + 16 * q);
+        float4 a[4], v[4];
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-        const float4 a = __ldcs(reinterpret_cast<const float4*>(blk) + k);
-        const float4 v = __ldg(reinterpret_cast<const float4*>(xj) + k);
-        rowsum += a.x * v.x + a.y * v.y + a.z * v.z + a.w * v.w;
-        cs[4 * k] = a.x * xi;
-        cs[4 * k + 1] = a.y * xi;
-        cs[4 * k + 2] = a.z * xi;
-        cs[4 * k + 3] = a.w * xi;
-    }
-    rowsum += __shfl_xor_sync(0xffffffffu, rowsum, 1);
-    rowsum += __shfl_xor_sync(0xffffffffu, rowsum, 2);
-    if (q == 0) part[((int64_t)I * nb + J) * kSymB + r] = rowsum;
-    if (I == J) return;  // uniform across the CTA
+        for (int k = 0; k < 4; k++) {
+            a[k] = __ldcs(blk + k);
+            v[k] = __ldg(xj + k);
+        }
+        const float xi = x[I * kSymB + r];
+        float rowsum = 0.0f, cs[16];
 #pragma unroll
-    for (int c = 0; c < 16; c++) {
-        float v = cs[c];
-        v += __shfl_xor_sync(0xffffffffu, v, 4);
-        v += __shfl_xor_sync(0xffffffffu, v, 8);
-        v += __shfl_xor_sync(0xffffffffu, v, 16);
-        cs[c] = v;
-    }
-    if (lane < 4)
+        for (int k = 0; k < 4; k++) {
+            rowsum += a[k].x * v[k].x + a[k].y * v[k].y + a[k].z * v[k].z + a[k].w * v[k].w;
+            cs[4 * k] = a[k].x * xi;
+            cs[4 * k + 1] = a[k].y * xi;
+            cs[4 * k + 2] = a[k].z * xi;
+            cs[4 * k + 3] = a[k].w * xi;
+        }
+        rowsum += __shfl_xor_sync(0xffffffffu, rowsum, 1);
+        rowsum += __shfl_xor_sync(0xffffffffu, rowsum, 2);
+        if (q == 0) part[((int64_t)I * nb + J) * kSymB + r] = rowsum;
+        if (I == J) continue;  // uniform across the CTA
 #pragma unroll
-        for (int c = 0; c < 16; c++) colp[warp][16 * lane + c] = cs[c];
-    __syncthreads();
-    if (t < kSymB) {
-        float v = 0.0f;
+        for (int c = 0; c < 16; c++) {
+            float w = cs[c];
+            w += __shfl_xor_sync(0xffffffffu, w, 4);
+            w += __shfl_xor_sync(0xffffffffu, w, 8);
+            w += __shfl_xor_sync(0xffffffffu, w, 16);
+            cs[c] = w;
+        }
+        if (lane < 4)
 #pragma unroll
-        for (int w = 0; w < 8; w++) v += colp[w][t];
-        part[((int64_t)J * nb + I) * kSymB + t] = v;
+            for (int c = 0; c < 16; c++) colp[warp][16 * lane + c] = cs[c];
+        __syncthreads();
+        if (t < kSymB) {
+            float w = 0.0f;
+#pragma unroll
+            for (int k = 0; k < 8; k++) w += colp[k][t];
+            part[((int64_t)J * nb + I) * kSymB + t] = w;
+        }
+        __syncthreads();
     }
 }
 
@@ -929,11 +936,10 @@ __global__ void __launch_bounds__(256) k_mg_resid(SellView<float> A, const __hal
     }
 }
 
-// The MINRES product on a Kuhn grid, matrix-free (kuhn.cuh): the brick kernel's epilogue, applied
-// to each owned node's product.
-// v = y / beta; z = A y / beta - (beta / oldb) r1; alfa = (v, z) (k_tl_spmv<double>)
-struct EpiMinres {
-    const double* __restrict__ y;
+// v = y / beta; z = A y / beta - (beta / oldb) r1; alfa = (v, z) (k_tl_spmv<double>) as the epilogue
+// of the z-marching matrix-free product (kuhn25.cuh): y = the product's input at the node
+struct EpiMinresZ {
+    static constexpr int NE = 1;  // r1
     double* __restrict__ v;
     double* __restrict__ z;
     const double* __restrict__ r1;
@@ -941,15 +947,16 @@ struct EpiMinres {
     double* __restrict__ partial;
     double acc;
     __device__ __forceinline__ bool skip() const { return S->done; }
-    __device__ __forceinline__ void operator()(int64_t g, const double* ay)
+    __host__ __device__ __forceinline__ void sources(const double** ev) const { ev[0] = r1; }
+    __device__ __forceinline__ void operator()(int64_t g, const double* ay, const double* y, const double (*e)[3])
     {
         const double inv = 1.0 / S->beta;
         const double coef = S->iter > 0 ? S->beta / S->oldb : 0.0;
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             const int64_t i = 3 * g + c;
-            const double vi = y[i] * inv;
-            const double zi = ay[c] * inv - coef * r1[i];
+            const double vi = y[c] * inv;
+            const double zi = ay[c] * inv - coef * e[0][c];
             v[i] = vi;
             z[i] = zi;
             acc += vi * zi;
@@ -1030,9 +1037,9 @@ struct EpiResidZ {
     __device__ __forceinline__ void finish() {}
 };
 
-using KCheb = KzKernel<2, float, kKzTX, kKzTY, kKzMinB, EpiChebZ>;
-using KResid = KzKernel<2, float, kKzTX, kKzTY, kKzMinB, EpiResidZ>;
-using KMinres = KuhnKernel<1, KuhnCfg64, double, EpiMinres>;
+using KCheb = KzKernel<2, true, float, kKzTX, kKzTY, kKzMinB, EpiChebZ>;
+using KResid = KzKernel<2, true, float, kKzTX, kKzTY, kKzMinB, EpiResidZ>;
+using KMinres = KzKernel<1, false, double, kKzTX, kKzTY, kKzMinB64, EpiMinresZ>;
 
 // x += P^_t ec
 __global__ void __launch_bounds__(kVecThreads) k_mg_prolong(int n_fine, const int32_t* __restrict__ owner,
@@ -1144,6 +1151,7 @@ struct CoarseHandle {
     DBuf<double> Ac;                 // dense coarse matrix (kept for inspection), n_cf x n_cf
     DBuf<float> cpart, rc, ec;
     DBuf<double> vec;                // 8 fine vectors (FP64 room; the FP32 solve uses the front half)
+    int64_t ldv64 = 0;               // their stride
     DBuf<double> r64, partial;
     DBuf<TlState> st;
     TlState* h_st = nullptr;
@@ -1407,7 +1415,10 @@ int coarse_build(CoarseHandle& C, System& F, CellsHandle& Ce, const int32_t* h_c
     MSFEM_TRY(C.rc.alloc(C.n_pad));
     MSFEM_TRY(C.ec.alloc(C.n_pad));
     MSFEM_CK(cudaMemsetAsync(C.rc.p, 0, sizeof(float) * C.n_pad, st));  // the GEMV reads the zero tail
-    MSFEM_TRY(C.vec.alloc(8 * (size_t)n));  // doubles: room for the FP64 solve
+    // eight vectors of doubles (room for the FP64 solve) at a 16-byte-aligned stride with slack,
+    // as the z-marching kernel's staging copies need
+    C.ldv64 = (n + 16 + 7) / 8 * 8;
+    MSFEM_TRY(C.vec.alloc(8 * (size_t)C.ldv64));
     MSFEM_TRY(C.r64.alloc(n));
     MSFEM_TRY(C.partial.alloc(4096));
     MSFEM_TRY(C.st.alloc(1));
@@ -1424,7 +1435,8 @@ int coarse_build(CoarseHandle& C, System& F, CellsHandle& Ce, const int32_t* h_c
 // ec = Cinv rc (symmetric packed blocks)
 void coarse_solve(CoarseHandle& C, const TlState* S, cudaStream_t st)
 {
-    k_tl_symv<<<C.sym_n, 256, 0, st>>>(C.sym_nb, C.sym_blocks.p, C.Csym.p, C.rc.p, C.sym_part.p, S);
+    k_tl_symv<<<std::min(C.sym_n, 148 * 8), 256, 0, st>>>(C.sym_nb, C.sym_n, C.sym_blocks.p, C.Csym.p, C.rc.p,
+                                                          C.sym_part.p, S);
     k_tl_symv_sum<<<(C.n_pad + 255) / 256, 256, 0, st>>>(C.n_pad, C.sym_nb, C.sym_part.p, C.ec.p, S);
 }
 
@@ -1458,12 +1470,13 @@ int inner_solve(CoarseHandle& C, int maxiter, double tau, int* iters)
     const int n = F.n_rows;
     constexpr bool f32 = sizeof(VT) == 4;
     const double* s = f32 ? nullptr : F.dscale.p;  // FP64 works in the original unknowns
+    const int64_t ld = C.ldv64;
     VT* X = reinterpret_cast<VT*>(C.vec.p);
-    VT* V = X + n;
-    VT* Z = V + n;
-    VT* Y = Z + n;
-    VT* R[2] = {Y + n, Y + 2 * (size_t)n};
-    VT* Wb[2] = {Y + 3 * (size_t)n, Y + 4 * (size_t)n};
+    VT* V = X + ld;
+    VT* Z = V + ld;
+    VT* Y = Z + ld;
+    VT* R[2] = {Y + ld, Y + 2 * ld};
+    VT* Wb[2] = {Y + 3 * ld, Y + 4 * ld};
     TlState* S = C.st.p;
     const unsigned gvec = kReduceBlocks;
     k_tl_norm<<<gvec, kVecThreads, 0, st>>>(n, C.r64.p, f32 ? F.dscale.p : nullptr, S, C.partial.p);
@@ -1590,12 +1603,13 @@ int inner_solve_mg(CoarseHandle& C, int maxiter, double tau, double stop2, int* 
     System& F = *C.fine;
     cudaStream_t st = F.stream;
     const int n = F.n_rows;
+    const int64_t ld = C.ldv64;
     double* X = C.vec.p;
-    double* V = X + n;
-    double* Z = V + n;
-    double* Y = Z + n;
-    double* R[2] = {Y + n, Y + 2 * (size_t)n};
-    double* Wb[2] = {Y + 3 * (size_t)n, Y + 4 * (size_t)n};
+    double* V = X + ld;
+    double* Z = V + ld;
+    double* Y = Z + ld;
+    double* R[2] = {Y + ld, Y + 2 * ld};
+    double* Wb[2] = {Y + 3 * ld, Y + 4 * ld};
     TlState* S = C.st.p;
     const unsigned gvec = kReduceBlocks;
     k_tl_norm<<<gvec, kVecThreads, 0, st>>>(n, C.r64.p, nullptr, S, C.partial.p);
@@ -1620,7 +1634,8 @@ int inner_solve_mg(CoarseHandle& C, int maxiter, double tau, double stop2, int* 
             double* w1 = Wb[p];
             double* w2 = Wb[1 - p];
             if (C.mf_fine)
-                KMinres::launch(C.ka.v64, Y, EpiMinres{Y, V, Z, r1, S, C.partial.p + 2048, 0.0}, C.ka.sms, st);
+                KMinres::launch(C.ka.v64, Y, EpiMinresZ{V, Z, r1, S, C.partial.p + 2048, 0.0}, C.ka.sms, C.ka.err.p,
+                                st);
             else
                 k_tl_spmv<double><<<gsp, 256, 0, st>>>(A, Y, V, Z, r1, S, C.partial.p + 2048);
             mg_cycle(C, Z, r2, r1, Y, 1, 0, st);  // r2_new over r1's buffer, then y = M^-1 r2_new
@@ -1866,6 +1881,7 @@ int solve_twolevel(CoarseHandle& C, int precision, int maxiter, double tol, doub
             std::fprintf(stderr, "[msfem] two-level refine %d (%s): rel %.3e tau %.1e inner %d\n", k, f32 ? "fp32" : "fp64",
                          std::sqrt(r2 / ff), tau, it);
         if (rc == MSFEM_ERR_NUMERIC && !mg) break;
+        if (mg && C.mf_fine) MSFEM_TRY(kuhn_check_err(C.ka, st));
         if (rc != MSFEM_ERR_NUMERIC) {
             if (f32)
                 k_tl_correct<float><<<kReduceBlocks, kVecThreads, 0, st>>>(n, F.X.p, reinterpret_cast<float*>(C.vec.p),
