@@ -314,36 +314,38 @@ __global__ void __launch_bounds__(256) k_sweep_pivot(const double* __restrict__ 
     }
 }
 
-// Bp = A[:, K] (old panel), Cp = Bp * Pinv
+// Bp = A[:, K] (old panel), Cp = Bp * Pinv.  Only the upper block triangle of A is kept up to date
+// (the swept matrix stays symmetric): rows below the pivot block read the panel from its mirror,
+// A[i][K] = A[K][i].
 __global__ void __launch_bounds__(256) k_sweep_panel(const double* __restrict__ A, int64_t ld, int n, int k0,
                                                      const double* __restrict__ Pinv, double* __restrict__ Bp,
                                                      double* __restrict__ Cp)
 {
     __shared__ double P[kSB][kSB];
+    __shared__ double a[4][kSB];
     for (int t = threadIdx.x; t < kSB * kSB; t += blockDim.x) P[t / kSB][t % kSB] = Pinv[t];
+    const int r = threadIdx.x / 64, j = threadIdx.x % 64;
+    const int row = blockIdx.x * 4 + r;  // 4 rows per CTA, 64 threads per row
+    if (row < n) a[r][j] = row < k0 + kSB ? A[(int64_t)row * ld + k0 + j] : A[(int64_t)(k0 + j) * ld + row];
     __syncthreads();
-    const int row = blockIdx.x * 4 + threadIdx.x / 64;  // 4 rows per CTA, 64 threads per row
-    const int j = threadIdx.x % 64;
     if (row >= n) return;
-    const double* a = A + (int64_t)row * ld + k0;
-    const double bj = a[j];
-    Bp[(int64_t)row * kSB + j] = bj;
-    __syncwarp();
+    Bp[(int64_t)row * kSB + j] = a[r][j];
     double s = 0.0;
-    for (int k = 0; k < kSB; k++) s += a[k] * P[k][j];
+    for (int k = 0; k < kSB; k++) s += a[r][k] * P[k][j];
     Cp[(int64_t)row * kSB + j] = s;
 }
 
-// tile (I, J) of 64 x 64: A_IJ -= C_I B_J^T off the pivot block row/column; the pivot
-// row/column take C, the pivot block -Pinv
+// upper tile (I, J), I <= J, of 64 x 64 (one CTA per entry of `tiles`): A_IJ -= C_I B_J^T off the
+// pivot block row/column; the pivot row/column take C, the pivot block -Pinv
 __global__ void __launch_bounds__(256) k_sweep_update(double* __restrict__ A, int64_t ld, int kb,
+                                                      const int2* __restrict__ tiles,
                                                       const double* __restrict__ Pinv, const double* __restrict__ Bp,
                                                       const double* __restrict__ Cp)
 {
     extern __shared__ double sm[];
     double* Cs = sm;                 // [64][65]
     double* Bs = sm + kSB * (kSB + 1);  // [64][65]
-    const int I = blockIdx.y, J = blockIdx.x;
+    const int I = tiles[blockIdx.x].x, J = tiles[blockIdx.x].y;
     const int tid = threadIdx.x;
     const int64_t i0 = (int64_t)I * kSB, j0 = (int64_t)J * kSB;
     if (I == kb && J == kb) {
@@ -1381,10 +1383,18 @@ int coarse_build(CoarseHandle& C, System& F, CellsHandle& Ce, const int32_t* h_c
     MSFEM_CK(cudaFuncSetAttribute(k_sweep_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     MSFEM_CK(cudaFuncSetAttribute(k_sweep_pivot, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     MSFEM_CK(cudaMemsetAsync(flag.p, 0, sizeof(int), st));
+    // the swept matrix stays symmetric: only its upper block triangle is updated
+    std::vector<int2> up;
+    up.reserve((size_t)nblk * (nblk + 1) / 2);
+    for (int I = 0; I < nblk; I++)
+        for (int J = I; J < nblk; J++) up.push_back(make_int2(I, J));
+    DBuf<int2> d_up;
+    MSFEM_TRY(d_up.alloc(up.size()));
+    MSFEM_CK(cudaMemcpyAsync(d_up.p, up.data(), sizeof(int2) * up.size(), cudaMemcpyHostToDevice, st));
     for (int kb = 0; kb < nblk; kb++) {
         k_sweep_pivot<<<1, 256, smem, st>>>(W.p, ld, kb * kSB, Pinv.p, flag.p);
         k_sweep_panel<<<(C.n_pad + 3) / 4, 256, 0, st>>>(W.p, ld, C.n_pad, kb * kSB, Pinv.p, Bp.p, Cp.p);
-        k_sweep_update<<<dim3(nblk, nblk), 256, smem, st>>>(W.p, ld, kb, Pinv.p, Bp.p, Cp.p);
+        k_sweep_update<<<(unsigned)up.size(), 256, smem, st>>>(W.p, ld, kb, d_up.p, Pinv.p, Bp.p, Cp.p);
     }
     MSFEM_CK(cudaGetLastError());
     MSFEM_CK(cudaMemcpyAsync(&bad, flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));

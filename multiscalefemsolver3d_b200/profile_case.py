@@ -202,7 +202,8 @@ def twolevel_case(n, maxiter=400000, matrix_free=False, smoother_reps=0):
         out_info = {"smoother_ms": ms, "smoother_bytes": nb, "smoother_gbs": nb / (ms * 1e-3) / 1e9}
     rel, it, out, rc = T.solve(tol=1e-8, maxiter=maxiter, precision=FP64)
     print(json.dumps({"n": n, "dofs": S.n_rows, "matrix_free": matrix_free, "rc_bases": rcb, "rc": rc, "rel": rel,
-                      "iterations": it, "ms_solve": S.stats()["ms_solve"], **out_info}))
+                      "iterations": it, "ms_solve": S.stats()["ms_solve"], "coarse_setup_ms": T.ms_setup,
+                      **out_info}))
     T.close()
     C.close()
     K.close()
