@@ -406,52 +406,62 @@ __global__ void k_pack_sym(const double* __restrict__ A, int64_t ld, int n, cons
     }
 }
 
-// per stored block (I, J): part[I][J] = C_IJ x_J and, for I < J, part[J][I] = C_IJ^T x_I.  Thread t
-// owns row t/4, columns 16 (t%4) .. +15; rows reduce over the 4 lanes of a row, columns over the
-// warp's 8 rows (shuffles), then over the 8 warps in shared memory, in fixed orders.  Persistent:
-// CTA c takes blocks c, c + grid, ...
+// per stored block (I, J): part[I][J] = C_IJ x_J and, for I < J, part[J][I] = C_IJ^T x_I.  The
+// block's 1024 float4 chunks are read by consecutive threads (warp loads of 512 contiguous bytes):
+// thread t holds rows t/16 + 16k (k = 0..3), columns 4 (t%16) .. +3.  Row sums reduce over the 16
+// lanes of a row, column sums over the lane pair (l, l+16) and then the 8 warps in shared memory,
+// in fixed orders.  Persistent: CTA c takes blocks c, c + grid, ...
 __global__ void __launch_bounds__(256) k_tl_symv(int nb, int n_blocks, const int2* __restrict__ blocks,
                                                  const float* __restrict__ P, const float* __restrict__ x,
                                                  float* __restrict__ part, const TlState* S)
 {
     if (S->done) return;
     __shared__ float colp[8][kSymB];
-    const int t = threadIdx.x, r = t >> 2, q = t & 3, lane = t & 31, warp = t >> 5;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int cq = t & 15, r0 = t >> 4;
+    // the next block's chunks are loaded while this one is reduced: two blocks in flight per thread
+    float4 a[4], an[4];
+    if (blockIdx.x < n_blocks) {
+        const float4* blk = reinterpret_cast<const float4*>(P + (int64_t)blockIdx.x * kSymB * kSymB);
+#pragma unroll
+        for (int k = 0; k < 4; k++) an[k] = __ldcs(blk + t + 256 * k);
+    }
     for (int b = blockIdx.x; b < n_blocks; b += gridDim.x) {
         const int I = blocks[b].x, J = blocks[b].y;
-        const float4* blk = reinterpret_cast<const float4*>(P + (int64_t)b * kSymB * kSymB + r * kSymB + 16 * q);
-        const float4* xj = reinterpret_cast<const float4*>(x + J * kSymB + 16 * q);
-        float4 a[4], v[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) a[k] = an[k];
+        if (b + (int)gridDim.x < n_blocks) {
+            const float4* nxt = reinterpret_cast<const float4*>(P + (int64_t)(b + gridDim.x) * kSymB * kSymB);
+#pragma unroll
+            for (int k = 0; k < 4; k++) an[k] = __ldcs(nxt + t + 256 * k);
+        }
+        const float4 xq = __ldg(reinterpret_cast<const float4*>(x + J * kSymB) + cq);
+        float xi[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) xi[k] = x[I * kSymB + r0 + 16 * k];
+        float rs[4], cs[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-            a[k] = __ldcs(blk + k);
-            v[k] = __ldg(xj + k);
+            rs[k] = a[k].x * xq.x + a[k].y * xq.y + a[k].z * xq.z + a[k].w * xq.w;
+            cs[0] += a[k].x * xi[k];
+            cs[1] += a[k].y * xi[k];
+            cs[2] += a[k].z * xi[k];
+            cs[3] += a[k].w * xi[k];
         }
-        const float xi = x[I * kSymB + r];
-        float rowsum = 0.0f, cs[16];
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-            rowsum += a[k].x * v[k].x + a[k].y * v[k].y + a[k].z * v[k].z + a[k].w * v[k].w;
-            cs[4 * k] = a[k].x * xi;
-            cs[4 * k + 1] = a[k].y * xi;
-            cs[4 * k + 2] = a[k].z * xi;
-            cs[4 * k + 3] = a[k].w * xi;
+#pragma unroll
+            for (int o = 1; o < 16; o <<= 1) rs[k] += __shfl_xor_sync(0xffffffffu, rs[k], o);
         }
-        rowsum += __shfl_xor_sync(0xffffffffu, rowsum, 1);
-        rowsum += __shfl_xor_sync(0xffffffffu, rowsum, 2);
-        if (q == 0) part[((int64_t)I * nb + J) * kSymB + r] = rowsum;
+        if (cq == 0)
+#pragma unroll
+            for (int k = 0; k < 4; k++) part[((int64_t)I * nb + J) * kSymB + r0 + 16 * k] = rs[k];
         if (I == J) continue;  // uniform across the CTA
 #pragma unroll
-        for (int c = 0; c < 16; c++) {
-            float w = cs[c];
-            w += __shfl_xor_sync(0xffffffffu, w, 4);
-            w += __shfl_xor_sync(0xffffffffu, w, 8);
-            w += __shfl_xor_sync(0xffffffffu, w, 16);
-            cs[c] = w;
-        }
-        if (lane < 4)
+        for (int c = 0; c < 4; c++) cs[c] += __shfl_xor_sync(0xffffffffu, cs[c], 16);
+        if (lane < 16)
 #pragma unroll
-            for (int c = 0; c < 16; c++) colp[warp][16 * lane + c] = cs[c];
+            for (int c = 0; c < 4; c++) colp[warp][4 * cq + c] = cs[c];
         __syncthreads();
         if (t < kSymB) {
             float w = 0.0f;
@@ -1445,7 +1455,7 @@ int coarse_build(CoarseHandle& C, System& F, CellsHandle& Ce, const int32_t* h_c
 // ec = Cinv rc (symmetric packed blocks)
 void coarse_solve(CoarseHandle& C, const TlState* S, cudaStream_t st)
 {
-    k_tl_symv<<<std::min(C.sym_n, 148 * 8), 256, 0, st>>>(C.sym_nb, C.sym_n, C.sym_blocks.p, C.Csym.p, C.rc.p,
+    k_tl_symv<<<std::min(C.sym_n, 148 * 4), 256, 0, st>>>(C.sym_nb, C.sym_n, C.sym_blocks.p, C.Csym.p, C.rc.p,
                                                           C.sym_part.p, S);
     k_tl_symv_sum<<<(C.n_pad + 255) / 256, 256, 0, st>>>(C.n_pad, C.sym_nb, C.sym_part.p, C.ec.p, S);
 }
@@ -1774,7 +1784,7 @@ int set_smoother(CoarseHandle& C, System& T, int degree, double ratio, int stora
     k_mg_norm2<<<kReduceBlocks, kVecThreads, 0, st>>>(n, v, C.partial.p, tk.p, nb.p);
     k_mg_scale<<<kReduceBlocks, kVecThreads, 0, st>>>(n, v, nb.p);
     MSFEM_CK(cudaStreamSynchronize(st));
-    double lam = 0.0;
+    // the 50 steps run back to back on the device (the norm stays there); the host reads the last
     for (int it = 0; it < 50; it++) {
         cudaStream_t ts = T.stream;
         T.stream = st;  // run the textbook system's SpMV on the solve stream
@@ -1783,12 +1793,12 @@ int set_smoother(CoarseHandle& C, System& T, int degree, double ratio, int stora
         MSFEM_TRY(rc);
         k_mg_norm2<<<kReduceBlocks, kVecThreads, 0, st>>>(n, w, C.partial.p, tk.p, nb.p);
         k_mg_scale<<<kReduceBlocks, kVecThreads, 0, st>>>(n, w, nb.p);
-        double nrm2 = 0.0;
-        MSFEM_CK(cudaMemcpyAsync(&nrm2, nb.p, sizeof(double), cudaMemcpyDeviceToHost, st));
-        MSFEM_CK(cudaStreamSynchronize(st));
-        lam = std::sqrt(nrm2);
         std::swap(v, w);
     }
+    double nrm2 = 0.0;
+    MSFEM_CK(cudaMemcpyAsync(&nrm2, nb.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    const double lam = std::sqrt(nrm2);
     cheb_coefs(C, 1.1 * lam, ratio, degree);
     C.widened = 0;
     C.text = &T;
