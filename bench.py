@@ -1073,7 +1073,7 @@ def run_twolevel(args, D):
                 "gpu_launches": int(launches),
                 "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                              "traffic": read_traffic("kuhn_cheb_elastic_128.md" if MF else "cheb_smoother_elastic_128.md"),
-                             "kernel": ("k_kuhn<EpiCheb> (Chebyshev step of the smoother: matrix-free textbook "
+                             "kernel": ("k_kuhn_z<EpiChebZ> (Chebyshev step of the smoother: matrix-free textbook "
                                         "operator on the Kuhn grid + vector update)" if MF else
                                         "k_mg_cheb (Chebyshev step of the smoother: FP16 3x3-block SELL SpMV of the "
                                         "textbook operator + vector update)"),

@@ -239,6 +239,12 @@ int msfem_spmv_scaled32(msfem_system_t h, const float* x, float* y, int on_devic
  * regular grid -- with material ids in [0, 64).  MSFEM_ERR_ARGUMENT (first offending tetrahedron or
  * node in the message) otherwise.  Elasticity systems only. */
 int msfem_set_kuhn_grid(msfem_system_t h, int nx, int ny, int nz);
+/* The library's device buffers come from a caching allocator: a released buffer's memory stays
+ * with the library (per device, by size class, at most 48 GiB) for the next buffer of that class,
+ * so handles built and destroyed step after step do not pay cudaMalloc / cudaFree each time; a
+ * release synchronises the device first, as cudaFree does.  This returns every cached block to the
+ * driver (no reference counterpart). */
+void msfem_release_cached_memory(void);
 /* y = A x formed matrix-free on the Kuhn grid (FP64): A is the system's values -- one
  * msfem_assemble_elastic or msfem_assemble_elastic_textbook since the last msfem_clear, plus its
  * Dirichlet rows -- applied from the tetrahedra's materials; checked against the assembled product

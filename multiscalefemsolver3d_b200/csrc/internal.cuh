@@ -17,6 +17,10 @@ namespace msfem {
 
 void set_error(const char* fmt, ...);
 
+// device memory through the library's caching allocator (devpool.cu)
+void* dev_alloc(size_t bytes, cudaError_t* err);
+void dev_free(void* p, size_t bytes);
+
 #define MSFEM_CK(call)                                                                                   \
     do {                                                                                                 \
         cudaError_t e_ = (call);                                                                         \
@@ -49,11 +53,10 @@ struct DBuf {
     ~DBuf() { release(); }
     int alloc(size_t count) {
         if (count <= n && p) return 0;
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
+        release();
         if (count == 0) return 0;
-        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        cudaError_t e = cudaSuccess;
+        p = static_cast<T*>(dev_alloc(count * sizeof(T), &e));
         if (e != cudaSuccess) {
             set_error("cudaMalloc(%zu bytes): %s", count * sizeof(T), cudaGetErrorString(e));
             p = nullptr;
@@ -63,7 +66,7 @@ struct DBuf {
         return 0;
     }
     void release() {
-        if (p) cudaFree(p);
+        if (p) dev_free(p, n * sizeof(T));
         p = nullptr;
         n = 0;
     }
