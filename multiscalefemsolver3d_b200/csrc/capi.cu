@@ -270,6 +270,9 @@ int msfem_system_destroy(msfem_system_t h)
     cudaSetDevice(s->device);
     cudaStreamSynchronize(s->stream);
     if (s->h_kstate) cudaFreeHost(s->h_kstate);
+    if (s->h_ahead) cudaFreeHost(s->h_ahead);
+    for (auto& e : s->ev_chunk)
+        if (e) cudaEventDestroy(e);
     cudaStream_t st = s->stream;
     cudaEvent_t e0 = s->ev0, e1 = s->ev1;
     for (auto& kv : s->graphs)

@@ -101,6 +101,7 @@ struct KState {
     double tol2_rel;            // MINRES: tol^2, scaled by the initial residual norm on the device
     int mr_applied;             // MINRES: iteration whose solution update has been applied after stopping
     double rr_min;              // smallest (r, r) seen in this solve
+    double cg2_gd[2];           // Chronopoulos-Gear CG: (r, r) and (A r, r) of the last product
     int stall, stall_limit;     // iterations since rr_min last fell by 2 %; stop when it reaches stall_limit
     int iter, maxiter, done, breakdown, primed;
     unsigned int ticket[4];
@@ -143,6 +144,8 @@ struct System {
     DBuf<double> partial; // reduction partials
     DBuf<KState> kstate;
     KState* h_kstate = nullptr;  // pinned mirror for polling
+    KState* h_ahead = nullptr;   // two pinned snapshots taken after queued iteration chunks
+    cudaEvent_t ev_chunk[2] = {nullptr, nullptr};
     DBuf<double> gm;      // GMRES: Hessenberg / rotations / y on the device
     DBuf<double> mr64;    // MINRES vectors (FP64)
     DBuf<float> mr32;     // MINRES vectors (FP32)

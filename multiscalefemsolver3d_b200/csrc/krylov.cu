@@ -204,9 +204,9 @@ __global__ void __launch_bounds__(kVecThreads) k_pcg_p(int n, const VT* z, VT* _
 //   w = A r,  gamma = (r, r),  delta = (w, r)                      (k_cg2_spmv)
 //   beta = gamma / gamma_old,  alpha = gamma / (delta - beta gamma / alpha_old)
 //   p = r + beta p,  s = w + beta s,  x += alpha p,  r -= alpha s   (k_cg2_update)
-// k_cg2_spmv only writes per-block partial sums; every block of k_cg2_update adds the partials in
-// the same fixed order (so all blocks hold the same scalars, bit for bit) and block 0 records the
-// state.  The scalars of the previous iteration live in one of two slots (parity passed by the
+// k_cg2_spmv writes per-block partial sums and its last block adds them in a fixed order into
+// S->cg2_gd; every block of k_cg2_update forms the step's scalars from those two numbers (so all
+// blocks hold the same scalars, bit for bit) and block 0 records the state.  The scalars of the previous iteration live in one of two slots (parity passed by the
 // host), so no block reads a value that block 0 overwrites in the same launch.
 // Slot layout in KState::mr: [5 * slot + 0] gamma, +1 alpha, +2 iterations, +3 lowest (r, r),
 // +4 iterations since (r, r) last set a 2 % low.
@@ -249,6 +249,16 @@ __global__ void __launch_bounds__(256) k_cg2_spmv(SellView<float> A, const float
         partial[blockIdx.x] = acc[0];
         partial[gridDim.x + blockIdx.x] = acc[1];
     }
+    KState* Sw = const_cast<KState*>(S);
+    if (arrive_last(&Sw->ticket[2])) {
+        double t[2];
+        reduce_partials<2>(partial, gridDim.x, gridDim.x, t, sh);
+        if (threadIdx.x == 0) {
+            Sw->cg2_gd[0] = t[0];
+            Sw->cg2_gd[1] = t[1];
+            Sw->ticket[2] = 0;
+        }
+    }
 }
 
 // first = 1: the start (beta = 0, p = r, s = w); slot: the parity of the previous scalars
@@ -259,12 +269,11 @@ __global__ void __launch_bounds__(kVecThreads) k_cg2_update(int n, float* __rest
                                                             int first)
 {
     if (S->done) return;
-    __shared__ double sh[64];
     __shared__ double sc[4];  // alpha, beta, done
-    double t[2];
-    reduce_partials<2>(partial, g_spmv, g_spmv, t, sh);
+    (void)partial;
+    (void)g_spmv;
     if (threadIdx.x == 0) {
-        const double gamma = t[0], delta = t[1];
+        const double gamma = S->cg2_gd[0], delta = S->cg2_gd[1];
         const double* old = S->mr + 5 * slot;
         const int iter = first ? 0 : (int)old[2];
         double rr_min = first ? gamma : old[3];
@@ -614,11 +623,15 @@ int run_chunks(System& s, const std::string& key, F&& enqueue_iteration, int per
         it = s.graphs.emplace(key, empty).first;
     }
     cudaGraphExec_t* exec = it->second.data();
+    MSFEM_TRY(read_state(s));
+    if (s.h_kstate->done) return MSFEM_OK;
+    if (!s.h_ahead) {
+        MSFEM_CK(cudaMallocHost(&s.h_ahead, 2 * sizeof(KState)));
+        for (auto& e : s.ev_chunk) MSFEM_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
     int k = 0;
-    int rc = MSFEM_OK;
-    while (true) {
-        MSFEM_TRY(read_state(s));
-        if (s.h_kstate->done) break;
+    // one chunk of iterations (4, 8, 16, then 32), then a snapshot of the state behind it
+    auto launch = [&](int slot) -> int {
         int ci = 0;
         while ((4 << ci) < chunk) ci++;
         if (!exec[ci]) {
@@ -628,29 +641,36 @@ int run_chunks(System& s, const std::string& key, F&& enqueue_iteration, int per
             cudaError_t e = cudaStreamEndCapture(s.stream, &g);
             if (e != cudaSuccess) {
                 set_error("graph capture failed: %s", cudaGetErrorString(e));
-                rc = MSFEM_ERR_CUDA;
-                break;
+                return MSFEM_ERR_CUDA;
             }
             e = cudaGraphInstantiate(&exec[ci], g, 0);
             cudaGraphDestroy(g);
             if (e != cudaSuccess) {
                 set_error("graph instantiate failed: %s", cudaGetErrorString(e));
-                rc = MSFEM_ERR_CUDA;
-                break;
+                return MSFEM_ERR_CUDA;
             }
         }
-        cudaError_t e = cudaGraphLaunch(exec[ci], s.stream);
-        if (e != cudaSuccess) {
-            set_error("graph launch failed: %s", cudaGetErrorString(e));
-            rc = MSFEM_ERR_CUDA;
-            break;
-        }
+        MSFEM_CK(cudaGraphLaunch(exec[ci], s.stream));
+        MSFEM_CK(cudaMemcpyAsync(s.h_ahead + slot, s.kstate.p, sizeof(KState), cudaMemcpyDeviceToHost, s.stream));
+        MSFEM_CK(cudaEventRecord(s.ev_chunk[slot], s.stream));
         s.launches += chunk * per_iter;
         k += chunk;
-        if (k > maxiter + 64) break;  // the device state also stops at maxiter; this is a host-side bound
         if (chunk < 32) chunk *= 2;
+        return MSFEM_OK;
+    };
+    // the next chunk is always queued before the host waits for the previous one's snapshot, so
+    // the GPU does not idle while the host polls; iterations queued past the stop exit at once (every
+    // iteration kernel checks the device flag), exactly as the rest of the stopping chunk does
+    MSFEM_TRY(launch(0));
+    int cur = 0;
+    for (;;) {
+        const bool more = k <= maxiter + 64;  // the device state also stops at maxiter; a host-side bound
+        if (more) MSFEM_TRY(launch(cur ^ 1));
+        MSFEM_CK(cudaEventSynchronize(s.ev_chunk[cur]));
+        if (s.h_ahead[cur].done || !more) break;
+        cur ^= 1;
     }
-    return rc;
+    return read_state(s);
 }
 
 std::string graph_key(const char* tag, std::initializer_list<const void*> ptrs, int n)
@@ -814,8 +834,10 @@ int solve_refined(System& s, Inner inner, int maxiter, double tol, int* iters, i
             rc = minres_run<double, true>(s, s.X.p, r64, maxiter - total_inner, tau, 0, &it);
             s.launches += 0;
         } else {
-            // inner tolerance: 1e-4 (what FP32 reaches comfortably), or just what is still missing
-            tau = std::max(1e-4, std::min(0.5, 0.3 * need));
+            // inner tolerance: what FP32 reaches comfortably (CG, whose stall test stops it at FP32's
+            // attainable accuracy: 1e-5, a deeper first pass saving a restart of the Krylov space;
+            // GMRES 1e-4), or just what is still missing
+            tau = std::max(inner == INNER_CG32 ? 1e-5 : 1e-4, std::min(0.5, 0.3 * need));
             k_scale_to32<<<kReduceBlocks, kVecThreads, 0, s.stream>>>(n, r64, rr_dev.p, s.dscale.p, r32, d32);
             s.launches += 1;
             if (inner == INNER_CG32) {
