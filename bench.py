@@ -80,6 +80,9 @@ def parse():
                          "MsFEM construction (the library default)")
     ap.add_argument("--train-cells", type=int, default=20480, help="elastic, learned: training cells")
     ap.add_argument("--train-epochs", type=int, default=24, help="elastic, learned: training epochs")
+    ap.add_argument("--cell-precision", default="fp64", choices=["fp64", "fp32ir"],
+                    help="cells: inner solves of the timed steps in FP64, or FP32 inside FP64 refinement (the other "
+                         "is timed once as a comparator)")
     ap.add_argument("--face-material", default="zero", choices=["zero", "cells"],
                     help="cells: zero (default) -- material 0 on the face and edge problems, as the reference's "
                          "construction; cells -- the materials of the tetrahedra they bound")
@@ -589,16 +592,19 @@ def kuhn_blocks(m):
 def run_cells(args, D):
     import torch
     from multiscalefemsolver3d_b200 import _lib
-    from multiscalefemsolver3d_b200.cells import FP32_IR, Cells
+    from multiscalefemsolver3d_b200.cells import FP32_IR, FP64, Cells
 
     torch.cuda.set_device(D.local)
     dev = torch.device("cuda", D.local)
     cm = cells_workload()
     C = Cells(cm)
     C.set_face_material(args.face_material)
+    # FP64 inner solves are the faster choice on this workload: FP32 inner steps need ~2 restarts
+    # of the Krylov space and the ill-conditioned cells fall back to FP64 anyway
+    PREC, OTHER = (FP64, FP32_IR) if args.cell_precision == "fp64" else (FP32_IR, FP64)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     for _ in range(args.warmup):
-        C.build_bases(FP32_IR, TOL)
+        C.build_bases(PREC, TOL)
     D.barrier()
     torch.cuda.synchronize()
     ts, reps = [], []
@@ -606,7 +612,7 @@ def run_cells(args, D):
         for _ in range(args.steps):
             flush.fill_(1.0)
             torch.cuda.synchronize()
-            rc = C.build_bases(FP32_IR, TOL)
+            rc = C.build_bases(PREC, TOL)
             if rc != 0:
                 raise RuntimeError(f"cells build rc={rc}")
             rep = C.report()
@@ -630,6 +636,16 @@ def run_cells(args, D):
     check = None
     if D.rank == 0 and not args.no_oracle_check:
         check = cells_oracle_error(cm, C.bases(), args.face_material)
+    # the other inner precision, once (after a warm-up build of its own)
+    C.build_bases(OTHER, TOL)
+    flush.fill_(1.0)
+    torch.cuda.synchronize()
+    rc_other = C.build_bases(OTHER, TOL)
+    rep_other = C.report()
+    other = {"inner_precision": "FP32 in FP64 refinement" if OTHER == FP32_IR else "FP64", "rc": int(rc_other),
+             "ms": float(sum(rep_other["ms"].values())), "ms_volumes": float(rep_other["ms"]["volumes"]),
+             "inner_iterations_mean": float(rep_other["inner"].mean()),
+             "refinement_steps_mean": float(rep_other["outer"].mean())}
     C.close()
 
     # e2e: create (topology + portraits) + build + bases copied back, host (pinned) buffers
@@ -648,7 +664,7 @@ def run_cells(args, D):
         try:
             _lib.check(L.msfem_cells_set_face_material(hh, {"cells": 0, "zero": 1}[args.face_material]),
                        "cells_set_face_material")
-            rc = L.msfem_cells_build_bases(hh, FP32_IR, TOL, 5000, tuned)
+            rc = L.msfem_cells_build_bases(hh, PREC, TOL, 5000, tuned)
             if rc != 0:
                 raise RuntimeError(f"cells build rc={rc}")
             _lib.check(L.msfem_cells_get_bases(hh, P(out), 0), "cells_get_bases")
@@ -672,7 +688,9 @@ def run_cells(args, D):
                  "inner_iterations_mean": float(rep["inner"].mean()), "inner_iterations_max": int(rep["inner"].max()),
                  "refinement_steps_mean": float(rep["outer"].mean()), "rel_residual_max": float(rep["rel"].max()),
                  "face_rel_residual_max": float(rep["face_rel"].max()), "step_ms_all": ts,
-                 "autotuned_cta_threads": rep["threads"]}
+                 "autotuned_cta_threads": rep["threads"],
+                 "inner_precision": "FP64" if PREC == FP64 else "FP32 in FP64 refinement",
+                 "comparator_other_precision": other}
         extra["face_material"] = ("material 0 on the face and edge problems, as the reference's own construction"
                                   if args.face_material == "zero" else
                                   "face and edge problems on the materials of the tetrahedra they bound")
@@ -680,7 +698,7 @@ def run_cells(args, D):
             extra["err_vs_oracle"] = check
         line = {"metric": METRIC, "value": ms, "unit": UNIT, "n_gpus": D.world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
-                "vs_baseline": None, "dtype": "fp32-in-f64-ir", "data": "synthetic",
+                "vs_baseline": None, "dtype": "f64" if PREC == FP64 else "fp32-in-f64-ir", "data": "synthetic",
                 "config": cells_config(cm, extra),
                 "e2e": {"value": e2e_ms, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "gpu_launches": 11,
