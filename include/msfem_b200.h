@@ -453,6 +453,19 @@ int msfem_cells_face_loads(msfem_cells_t c, int n_items, const int32_t* items, c
  * u[b] = sum_v U[cell_vertex[8c+v]] (.) psi_v(b), component by component.  U: [n_vertices][3],
  * u: [cell nodes][3] (concatenated cell numbering), host arrays. */
 int msfem_cells_reconstruct(msfem_cells_t c, int n_vertices, const int32_t* cell_vertex, const double* U, double* u);
+/* The whole Order1 macro phase of MsFEM::MsFEM_forElasticDeformation_OrderBF1_forPoly (MsFEM/
+ * MsFEM.h:572-1010) on the device after the bases are built: the macro element matrices
+ * (msfem_cells_macro_matrices), the boundary loads of the items (msfem_cells_face_loads) summed
+ * over the macro vertices item by item (SummPartOfVector, the reference's order), the Dirichlet
+ * vertices and the macro solve (msfem_macro_solve), and the fine reconstruction
+ * (msfem_cells_reconstruct), without the matrices or loads leaving the GPU.  Host arrays: items
+ * [n_items][2], traction [n_items][3], U [n_vertices][3] out; u [cell nodes][3], K_out
+ * [n_cells][8][8][3][3] and F_out [n_vertices][3] are optional outputs (NULL: not copied). */
+int msfem_cells_order1_macro_solve(msfem_cells_t c, int n_vertices, const int32_t* cell_vertex, int n_items,
+                                   const int32_t* items, const double* traction, int n_fixed,
+                                   const int32_t* fixed_vertices, const double* fixed_values, int precision, double tol,
+                                   int maxiter, double* U, double* u, double* K_out, double* F_out, int32_t* iterations,
+                                   double* rel_residual);
 /* Replace the bases of every cell ([n_nodes][8][3] doubles, as msfem_cells_get_bases returns
  * them), e.g. with predicted ones.  No reference counterpart. */
 int msfem_cells_set_bases(msfem_cells_t c, const double* bases, int on_device);

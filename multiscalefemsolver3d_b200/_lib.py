@@ -107,6 +107,9 @@ _SIGS = [
     ("msfem_cells_macro_matrices", C.c_int, [C.c_void_p, _P, C.c_int]),
     ("msfem_cells_face_loads", C.c_int, [C.c_void_p, C.c_int, _P, _P, _P]),
     ("msfem_cells_reconstruct", C.c_int, [C.c_void_p, C.c_int, _P, _P, _P]),
+    ("msfem_cells_order1_macro_solve", C.c_int, [C.c_void_p, C.c_int, _P, C.c_int, _P, _P, C.c_int, _P, _P, C.c_int,
+                                                  C.c_double, C.c_int, _P, _P, _P, _P, C.POINTER(C.c_int32),
+                                                  C.POINTER(C.c_double)]),
     ("msfem_postprocess_elastic", C.c_int, [C.c_void_p, C.c_int, _P, _P, _P, C.c_int]),
     ("msfem_cells_set_bases", C.c_int, [C.c_void_p, _P, C.c_int]),
     ("msfem_cells_basis_residual", C.c_int, [C.c_void_p, _P]),

@@ -670,6 +670,19 @@ __global__ void __launch_bounds__(256) k_basis_residual(const int64_t* __restric
 }
 
 // fine solution of every cell from the macro one: u[b] = sum_v U[V(c, v)] (.) psi_v(b)
+// F[cell_vertex[8 c_i + v]] += loads[i][v] over the items in order (SummPartOfVector item by item,
+// the reference's order): one thread per component walks the items, so each vertex sums in order
+__global__ void k_macro_load_sum(int n_items, const int32_t* __restrict__ items, const int32_t* __restrict__ cell_vertex,
+                                 const double* __restrict__ loads, double* __restrict__ F)
+{
+    const int a = threadIdx.x;
+    if (a >= 3) return;
+    for (int i = 0; i < n_items; i++) {
+        const int c = items[2 * i];
+        for (int v = 0; v < 8; v++) F[3 * (int64_t)cell_vertex[8 * c + v] + a] += loads[24 * (int64_t)i + 3 * v + a];
+    }
+}
+
 __global__ void k_reconstruct(int n_cells, const int64_t* __restrict__ node_off, const int32_t* __restrict__ cell_vertex,
                               const double* __restrict__ U, const double* __restrict__ bases, double* __restrict__ u)
 {
@@ -1947,6 +1960,80 @@ int msfem_cells_reconstruct(msfem_cells_t h, int n_vertices, const int32_t* cell
     MSFEM_CK(cudaMemcpyAsync(u, du.p, sizeof(double) * 3 * h->n_nodes, cudaMemcpyDeviceToHost, st));
     MSFEM_CK(cudaStreamSynchronize(st));
     return MSFEM_OK;
+}
+
+int msfem_cells_order1_macro_solve(msfem_cells_t h, int n_vertices, const int32_t* cell_vertex, int n_items,
+                                   const int32_t* items, const double* traction, int n_fixed,
+                                   const int32_t* fixed_vertices, const double* fixed_values, int precision, double tol,
+                                   int maxiter, double* U, double* u, double* K_out, double* F_out, int32_t* iterations,
+                                   double* rel_residual)
+{
+    using namespace msfem;
+    if (!h || n_vertices <= 0 || !cell_vertex || n_items < 0 || (n_items > 0 && (!items || !traction)) || !U) {
+        set_error("msfem_cells_order1_macro_solve: bad arguments");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    for (int k = 0; k < 8 * h->n_cells; k++)
+        if (cell_vertex[k] < 0 || cell_vertex[k] >= n_vertices) {
+            set_error("msfem_cells_order1_macro_solve: coarse vertex id %d out of range", cell_vertex[k]);
+            return MSFEM_ERR_ARGUMENT;
+        }
+    for (int i = 0; i < n_items; i++)
+        if (items[2 * i] < 0 || items[2 * i] >= h->n_cells || items[2 * i + 1] < 0 || items[2 * i + 1] > 5) {
+            set_error("msfem_cells_order1_macro_solve: item %d names cell %d face %d", i, items[2 * i], items[2 * i + 1]);
+            return MSFEM_ERR_ARGUMENT;
+        }
+    MSFEM_CK(cudaSetDevice(h->device));
+    cudaStream_t st = h->stream;
+    const int nc = h->n_cells;
+    DBuf<int32_t> dv, di;
+    DBuf<double> dK, dt, dl, dF, dU, du;
+    MSFEM_TRY(dv.alloc(8 * (size_t)nc));
+    MSFEM_TRY(dK.alloc(576 * (size_t)nc));
+    MSFEM_TRY(dF.alloc(3 * (size_t)n_vertices));
+    MSFEM_TRY(dU.alloc(3 * (size_t)n_vertices));
+    MSFEM_CK(cudaMemcpyAsync(dv.p, cell_vertex, sizeof(int32_t) * 8 * nc, cudaMemcpyHostToDevice, st));
+    MSFEM_CK(cudaMemsetAsync(dF.p, 0, sizeof(double) * 3 * n_vertices, st));
+    MSFEM_CK(cudaMemsetAsync(h->flag.p, 0, sizeof(int), st));
+    // macro element matrices (SolveLocalMatrix), on the device
+    const size_t smem = sizeof(double) * (96 * 72 + 96 * 3 + 96) + sizeof(int) * 96;
+    MSFEM_CK(cudaFuncSetAttribute(k_macro_cells<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_macro_cells<8, false><<<nc, 256, smem, st>>>(h->tet_off.p, h->vols.elems.p, h->xyz.p, h->box.p, h->bx.p,
+                                                   h->lame.p, dK.p, h->flag.p);
+    // boundary loads and their sum over the macro vertices, item by item (SummPartOfVector)
+    if (n_items > 0) {
+        MSFEM_TRY(di.alloc(2 * (size_t)n_items));
+        MSFEM_TRY(dt.alloc(3 * (size_t)n_items));
+        MSFEM_TRY(dl.alloc(24 * (size_t)n_items));
+        MSFEM_CK(cudaMemcpyAsync(di.p, items, sizeof(int32_t) * 2 * n_items, cudaMemcpyHostToDevice, st));
+        MSFEM_CK(cudaMemcpyAsync(dt.p, traction, sizeof(double) * 3 * n_items, cudaMemcpyHostToDevice, st));
+        k_face_loads<<<n_items, 128, 0, st>>>(n_items, di.p, dt.p, h->tet_off.p, h->vols.elems.p, h->xyz.p, h->box.p,
+                                              h->bx.p, dl.p, h->flag.p);
+        k_macro_load_sum<<<1, 32, 0, st>>>(n_items, di.p, dv.p, dl.p, dF.p);
+    }
+    MSFEM_CK(cudaGetLastError());
+    int bad = 0;
+    MSFEM_CK(cudaMemcpyAsync(&bad, h->flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    if (bad) {
+        set_error("msfem_cells_order1_macro_solve: a quadrature point lies in no tetrahedron of its cell");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    // the macro solve on those device arrays, then the fine reconstruction
+    const int rc = macro_solve_device(n_vertices, nc, cell_vertex, dK.p, dF.p, n_fixed, fixed_vertices, fixed_values,
+                                      precision, tol, maxiter, dU.p, iterations, rel_residual, st);
+    if (rc < 0) return rc;
+    MSFEM_CK(cudaMemcpyAsync(U, dU.p, sizeof(double) * 3 * n_vertices, cudaMemcpyDeviceToHost, st));
+    if (u) {
+        MSFEM_TRY(du.alloc(3 * (size_t)h->n_nodes));
+        k_reconstruct<<<nc, 256, 0, st>>>(nc, h->node_off.p, dv.p, dU.p, h->bx.p, du.p);
+        MSFEM_CK(cudaGetLastError());
+        MSFEM_CK(cudaMemcpyAsync(u, du.p, sizeof(double) * 3 * h->n_nodes, cudaMemcpyDeviceToHost, st));
+    }
+    if (K_out) MSFEM_CK(cudaMemcpyAsync(K_out, dK.p, sizeof(double) * 576 * nc, cudaMemcpyDeviceToHost, st));
+    if (F_out) MSFEM_CK(cudaMemcpyAsync(F_out, dF.p, sizeof(double) * 3 * n_vertices, cudaMemcpyDeviceToHost, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    return rc;
 }
 
 void msfem_cells_destroy(msfem_cells_t h)

@@ -222,6 +222,10 @@ int ensure_kstate(System& s);
 int solve(System& s, int method, int precision, int restart_m, int maxiter, double tol, double* relres, int* iters);
 int ensure_state(System& s);
 int read_state(System& s);
+// ---- the MsFEM macro solve on device data (macro.cu)
+int macro_solve_device(int n_vertices, int n_cells, const int32_t* cell_vertex, const double* dK, const double* dF,
+                       int n_fixed, const int32_t* fixed_vertices, const double* fixed_values, int precision, double tol,
+                       int maxiter, double* dU, int32_t* iterations, double* rel_residual, cudaStream_t st);
 // ---- the reference's SSOR preconditioner and its PCG (ssor.cu)
 int ssor_apply(System& s, const double* r, double* z, double* zb, const KState* S);
 int solve_pcg_ssor(System& s, int maxiter, double tol, int* iters);

@@ -12,13 +12,15 @@
 #include "batch.cuh"
 #include "internal.cuh"
 
-extern "C" int msfem_macro_solve(int n_vertices, int n_cells, const int32_t* cell_vertex, const double* K,
-                                 const double* F, int n_fixed, const int32_t* fixed_vertices,
-                                 const double* fixed_values, int precision, double tol, int maxiter, double* U,
-                                 int32_t* iterations, double* rel_residual)
+namespace msfem {
+
+// The macro solve on device data: K [n_cells][8][8][3][3] and F [n_vertices][3] (or null) on the
+// device, cell_vertex and the Dirichlet list on the host (checked here); U [n_vertices][3] device out.
+int macro_solve_device(int n_vertices, int n_cells, const int32_t* cell_vertex, const double* dK, const double* dF,
+                       int n_fixed, const int32_t* fixed_vertices, const double* fixed_values, int precision, double tol,
+                       int maxiter, double* dU, int32_t* iterations, double* rel_residual, cudaStream_t st)
 {
-    using namespace msfem;
-    if (n_vertices <= 0 || n_cells <= 0 || !cell_vertex || !K || !U || n_fixed < 0 ||
+    if (n_vertices <= 0 || n_cells <= 0 || !cell_vertex || !dK || !dU || n_fixed < 0 ||
         (n_fixed > 0 && (!fixed_vertices || !fixed_values)) || !(tol > 0.0) || maxiter <= 0 ||
         (precision != MSFEM_FP64 && precision != MSFEM_FP32_IR)) {
         set_error("msfem_macro_solve: bad arguments");
@@ -40,12 +42,6 @@ extern "C" int msfem_macro_solve(int n_vertices, int n_cells, const int32_t* cel
         fixed[v] = 1;  // a later duplicate overwrites the value, as in the reference
         for (int a = 0; a < 3; a++) x0[3 * (size_t)v + a] = fixed_values[3 * i + a];
     }
-    cudaStream_t st = nullptr;
-    MSFEM_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    struct StreamGuard {
-        cudaStream_t s;
-        ~StreamGuard() { cudaStreamSynchronize(s), cudaStreamDestroy(s); }
-    } guard{st};
     BatchSys b;
     b.dim = 3;
     b.k1 = 8;
@@ -65,22 +61,16 @@ extern "C" int msfem_macro_solve(int n_vertices, int n_cells, const int32_t* cel
     MSFEM_TRY(up(b.elem_off, b.h_elem_off.data(), 2));
     MSFEM_TRY(up(b.elems, cell_vertex, 8 * (size_t)n_cells));
     MSFEM_TRY(up(b.fixed, fixed.data(), (size_t)n_vertices));
-    DBuf<double> dK, dF, dx;
-    MSFEM_TRY(up(dK, K, 576 * (size_t)n_cells));
-    MSFEM_TRY(up(dx, x0.data(), x0.size()));
-    if (F) {
-        MSFEM_TRY(up(dF, F, 3 * (size_t)n_vertices));
-        b.rhs = dF.p;
-    }
+    MSFEM_CK(cudaMemcpyAsync(dU, x0.data(), sizeof(double) * x0.size(), cudaMemcpyHostToDevice, st));
+    b.rhs = const_cast<double*>(dF);
     MSFEM_TRY(batch_build_pattern(b, nullptr));
-    MSFEM_TRY(batch_assemble_given(b, dK.p));
-    MSFEM_TRY(batch_solve(b, dx.p, precision, tol, maxiter, 0));
-    MSFEM_CK(cudaMemcpyAsync(U, dx.p, sizeof(double) * 3 * n_vertices, cudaMemcpyDeviceToHost, st));
+    MSFEM_TRY(batch_assemble_given(b, dK));
+    MSFEM_TRY(batch_solve(b, dU, precision, tol, maxiter, 0));
     int32_t it = 0;
     double rel = 0.0;
     MSFEM_CK(cudaMemcpyAsync(&it, b.iters.p, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     MSFEM_CK(cudaMemcpyAsync(&rel, b.rel.p, sizeof(double), cudaMemcpyDeviceToHost, st));
-    MSFEM_CK(cudaStreamSynchronize(st));
+    MSFEM_CK(cudaStreamSynchronize(st));  // the host vectors above are released here
     if (iterations) *iterations = it;
     if (rel_residual) *rel_residual = rel;
     if (!(rel <= tol)) {
@@ -88,4 +78,39 @@ extern "C" int msfem_macro_solve(int n_vertices, int n_cells, const int32_t* cel
         return MSFEM_NOT_CONVERGED;
     }
     return MSFEM_OK;
+}
+
+}  // namespace msfem
+
+extern "C" int msfem_macro_solve(int n_vertices, int n_cells, const int32_t* cell_vertex, const double* K,
+                                 const double* F, int n_fixed, const int32_t* fixed_vertices,
+                                 const double* fixed_values, int precision, double tol, int maxiter, double* U,
+                                 int32_t* iterations, double* rel_residual)
+{
+    using namespace msfem;
+    if (n_vertices <= 0 || n_cells <= 0 || !cell_vertex || !K || !U) {
+        set_error("msfem_macro_solve: bad arguments");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    cudaStream_t st = nullptr;
+    MSFEM_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    struct StreamGuard {
+        cudaStream_t s;
+        ~StreamGuard() { cudaStreamSynchronize(s), cudaStreamDestroy(s); }
+    } guard{st};
+    DBuf<double> dK, dF, dU;
+    MSFEM_TRY(dK.alloc(576 * (size_t)n_cells));
+    MSFEM_CK(cudaMemcpyAsync(dK.p, K, sizeof(double) * 576 * n_cells, cudaMemcpyHostToDevice, st));
+    if (F) {
+        MSFEM_TRY(dF.alloc(3 * (size_t)n_vertices));
+        MSFEM_CK(cudaMemcpyAsync(dF.p, F, sizeof(double) * 3 * n_vertices, cudaMemcpyHostToDevice, st));
+    }
+    MSFEM_TRY(dU.alloc(3 * (size_t)n_vertices));
+    const int rc = macro_solve_device(n_vertices, n_cells, cell_vertex, dK.p, F ? dF.p : nullptr, n_fixed,
+                                      fixed_vertices, fixed_values, precision, tol, maxiter, dU.p, iterations,
+                                      rel_residual, st);
+    if (rc < 0) return rc;
+    MSFEM_CK(cudaMemcpyAsync(U, dU.p, sizeof(double) * 3 * n_vertices, cudaMemcpyDeviceToHost, st));
+    MSFEM_CK(cudaStreamSynchronize(st));
+    return rc;
 }

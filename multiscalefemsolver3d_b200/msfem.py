@@ -58,28 +58,24 @@ def msfem_elastic_driver(cc, fixed_vertices, fixed_values, load_items, tractions
         rc = C_.build_bases(precision=precision, tol=cell_tol)
         if rc != 0:
             raise RuntimeError(f"cell bases rc={rc}")
-        K = C_.macro_matrices()
+        # the macro phase in one device-side call: element matrices, boundary loads summed item by
+        # item (SummPartOfVector), Dirichlet vertices, the macro solve and the fine reconstruction
         items = _c(load_items, np.int32).reshape(-1, 2)
         tr = _c(tractions, np.float64).reshape(-1, 3)
-        loads = np.zeros((items.shape[0], 8, 3))
-        if items.shape[0]:
-            check(L.msfem_cells_face_loads(C_.h, items.shape[0], _p(items), _p(tr), _p(loads)), "cells_face_loads")
         cv = _c(cc.cell_vertex, np.int32)
         nv = int(cc.n_coarse_vertices)
-        F = np.zeros((nv, 3))
-        for i in range(items.shape[0]):          # SummPartOfVector, item by item
-            F[cv[items[i, 0]]] += loads[i]
         fv = _c(fixed_vertices, np.int32)
         fval = _c(fixed_values, np.float64).reshape(-1, 3)
         U = np.zeros((nv, 3))
+        u = np.zeros((C_.n_nodes, 3))
+        K = np.zeros((cv.shape[0], 8, 8, 3, 3))
+        F = np.zeros((nv, 3))
         it, rel = C.c_int32(), C.c_double()
-        Kc = _c(K, np.float64)
-        rc = check(L.msfem_macro_solve(nv, cv.shape[0], _p(cv), _p(Kc), _p(F), fv.size, _p(fv), _p(fval), 0, tol,
-                                       maxiter, _p(U), C.byref(it), C.byref(rel)), "macro_solve")
+        rc = check(L.msfem_cells_order1_macro_solve(C_.h, nv, _p(cv), items.shape[0], _p(items), _p(tr), fv.size,
+                                                    _p(fv), _p(fval), 0, tol, maxiter, _p(U), _p(u), _p(K), _p(F),
+                                                    C.byref(it), C.byref(rel)), "cells_order1_macro_solve")
         if rc != 0:
             raise RuntimeError(f"macro solve stopped at {rel.value:.3e}")
-        u = np.zeros((C_.n_nodes, 3))
-        check(L.msfem_cells_reconstruct(C_.h, nv, _p(cv), _p(U), _p(u)), "cells_reconstruct")
         return MsfemResult(U=U, u_cells=u, K=K, F=F, iterations=it.value, rel_residual=rel.value)
     finally:
         if own:
