@@ -404,14 +404,6 @@ int msfem_cells_build_order2(msfem_cells_t c, const int32_t* cell_vertex, int pr
  * (MsFEM_Grid.h:597-760). */
 int msfem_order2_edge_order(int n_cells, const int32_t* cell_vertex, int32_t* order);
 
-/* Host only: the Order2 macro system as the scalar CSR of MakeCopyMatrix_A_into_B (DOF 3 d + c,
- * whole 3x3 blocks of the DOF portrait, diagonal in place; Grid_forMech::CreationPortrait and
- * SummPartOfMatrix, MsFEM/MsFEM.h:48-131) from the cells' DOF lists cell_dofs [n_cells][27] (the
- * reference's numbering: vertices, NV + edge, NV + NE + face, NV + NE + NF + cell) and element
- * matrices K [n_cells][27][27][3][3] (msfem_cells_order2_macro_matrices).  Call with row_ptr,
- * col or val NULL to get *nnz; then row_ptr [3 n_dofs + 1], col / val [nnz]. */
-int msfem_order2_macro_csr(int n_cells, int n_dofs, const int32_t* cell_dofs, const double* K, int64_t* row_ptr,
-                           int32_t* col, double* val, int64_t* nnz);
 
 /* bases: [n_nodes][27][3] doubles, node-major (self_basis_functions[i][node] of
  * MsFEM_Grid.h:2926-2937 transposed). */
@@ -423,6 +415,52 @@ int msfem_cells_get_order2_bases(msfem_cells_t c, double* bases, int on_device);
  * quadrature, micro-element lookup and D as msfem_cells_macro_matrices.
  * K: [n_cells][27][27][3][3] doubles. */
 int msfem_cells_order2_macro_matrices(msfem_cells_t c, double* K, int on_device);
+
+/* The MsFEM Order2 macro system on the device (MsFEM::MsFEM_forElasticDeformation_OrderBF2_forPoly,
+ * MsFEM/MsFEM.h:53-131: Grid_forMech::CreationPortrait + CSSD_Matrix::SummPartOfMatrix, then
+ * math::MakeCopyMatrix_A_into_B): the cells' element matrices (msfem_cells_order2_macro_matrices)
+ * summed by the cells' DOF lists cell_dofs [n_cells][27] (host; the reference's numbering:
+ * vertices, NV + edge, NV + NE + face, NV + NE + NF + cell; every DOF in some cell) into the
+ * scalar system of DOF 3 d + c, whole 3x3 blocks of the DOF portrait, diagonal in place, each
+ * block summed in (cell, I, J) order.  *out: a new scalar system (no mesh) with F = X = 0; the
+ * caller destroys it.  Replaces the host assembly loop of MsFEM.h:61-131. */
+int msfem_cells_order2_macro_system(msfem_cells_t c, int n_dofs, const int32_t* cell_dofs, msfem_system_t* out);
+
+/* The Order2 Dirichlet values on the device (Grid_forMech::CreateBoundaryConditions,
+ * MsFEM/MsFEM_Grid.h:3303-3470): per group, the L2 projection of its constant value over its faces
+ * onto its DOFs.  Host arrays:
+ *   vertex_xyz [n_vertices][3]: the macro vertices;
+ *   faces [n_faces][10]: per group face (grouped by group, in the group's face order): its cell
+ *     and its 9 DOF ids -- its 4 cycle vertices (a vertex's DOF id is its vertex id; the
+ *     quadrature runs over this cycle), the edges between cycle nodes k and k+1, the face;
+ *   group_dof_off [n_groups + 1], group_dofs: each group's DOF list, ascending;
+ *   group_face_off [n_groups + 1]: each group's faces in `faces`;
+ *   group_values [n_groups][3]: each group's value.
+ * Per face: the mass matrix and load of its 9 DOFs with the polygon rule 3 (GeometryShape.h:
+ * 2625-2640 with the triangle rule of :1482-1540 as written there), the bases' z components from
+ * the lowest-numbered micro tetrahedron holding each point; summed per group in face order and
+ * solved by Cholesky on the rows that carry mass (rows whose diagonal is at most n eps times the
+ * largest diagonal -- the face bubbles, DOFs on no group face -- hold 0).  At most 16384 DOFs
+ * per group.  values: host [group_dof_off[n_groups]][3] out, the projected value of each group
+ * DOF. */
+int msfem_cells_order2_dirichlet(msfem_cells_t c, int n_dofs, const int32_t* cell_dofs, int n_vertices,
+                                 const double* vertex_xyz, int n_faces, const int32_t* faces, int n_groups,
+                                 const int32_t* group_dof_off, const int32_t* group_dofs, const int32_t* group_face_off,
+                                 const double* group_values, double* values);
+
+/* The Order2 macro phase in one call, on the device: msfem_cells_order2_macro_system, the
+ * projected values of msfem_cells_order2_dirichlet, the elimination of the rows fixed_dofs
+ * [n_fixed] (scalar rows 3 d + c, in elimination order) with values projected[fixed_src[i]]
+ * (index 3 k + c into the projection's [group DOF k][c] output) by rows and columns
+ * (MsFEM/MsFEM.h:300-365; MSFEM_ROW_AND_COLUMN of msfem_apply_dirichlet), X = F, and MINRES
+ * (precision MSFEM_FP64 or MSFEM_FP32_IR) to ||F - A X|| <= tol ||F||.  The reference runs plain
+ * CG restarts on the same system (MsFEM.h:445-478).  U: host [n_dofs][3] out. */
+int msfem_cells_order2_macro_solve(msfem_cells_t c, int n_dofs, const int32_t* cell_dofs, int n_vertices,
+                                   const double* vertex_xyz, int n_faces, const int32_t* faces, int n_groups,
+                                   const int32_t* group_dof_off, const int32_t* group_dofs,
+                                   const int32_t* group_face_off, const double* group_values, int n_fixed,
+                                   const int32_t* fixed_dofs, const int32_t* fixed_src, int precision, double tol,
+                                   int maxiter, double* U, int32_t* iterations, double* rel_residual);
 
 /* Per-cell report of the last build (host arrays of n_cells, any may be NULL):
  * inner iterations, outer refinement steps and final relative residual of the volume

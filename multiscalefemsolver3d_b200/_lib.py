@@ -100,9 +100,14 @@ _SIGS = [
     ("msfem_cells_set_face_material", C.c_int, [C.c_void_p, C.c_int]),
     ("msfem_cells_build_order2", C.c_int, [C.c_void_p, _P, C.c_int, C.c_double, C.c_int, C.c_int]),
     ("msfem_order2_edge_order", C.c_int, [C.c_int, _P, _P]),
-    ("msfem_order2_macro_csr", C.c_int, [C.c_int, C.c_int, _P, _P, _P, _P, _P, C.POINTER(C.c_int64)]),
     ("msfem_cells_get_order2_bases", C.c_int, [C.c_void_p, _P, C.c_int]),
     ("msfem_cells_order2_macro_matrices", C.c_int, [C.c_void_p, _P, C.c_int]),
+    ("msfem_cells_order2_macro_system", C.c_int, [C.c_void_p, C.c_int, _P, C.POINTER(C.c_void_p)]),
+    ("msfem_cells_order2_dirichlet", C.c_int, [C.c_void_p, C.c_int, _P, C.c_int, _P, C.c_int, _P, C.c_int, _P, _P, _P,
+                                               _P, _P]),
+    ("msfem_cells_order2_macro_solve", C.c_int, [C.c_void_p, C.c_int, _P, C.c_int, _P, C.c_int, _P, C.c_int, _P, _P,
+                                                 _P, _P, C.c_int, _P, _P, C.c_int, C.c_double, C.c_int, _P,
+                                                 C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
     ("msfem_cells_report", C.c_int, [C.c_void_p, _P, _P, _P, _P, _P, _P]),
     ("msfem_cells_macro_matrices", C.c_int, [C.c_void_p, _P, C.c_int]),
     ("msfem_cells_face_loads", C.c_int, [C.c_void_p, C.c_int, _P, _P, _P]),

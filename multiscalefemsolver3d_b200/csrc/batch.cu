@@ -58,7 +58,8 @@ __global__ void k_check_elements(int n_sys, const int64_t* __restrict__ node_off
         }
 }
 
-__host__ __device__ __forceinline__ int tag_bits(int k1) { return k1 > 4 ? 3 : 2; }
+// bits of each element-local index in a contribution tag (element << 2 tb | I << tb | J)
+__host__ __device__ __forceinline__ int tag_bits(int k1) { return k1 > 8 ? 5 : (k1 > 4 ? 3 : 2); }
 
 __global__ void k_emit_pairs(int64_t e0, int64_t e1, int64_t n0, int nb, const int32_t* __restrict__ elems, int k1,
                              uint64_t* __restrict__ key, uint32_t* __restrict__ tag)
@@ -639,7 +640,7 @@ int batch_build_pattern(BatchSys& b, const double* d_xyz)
 {
     (void)d_xyz;
     cudaStream_t st = b.stream;
-    if (b.k1 > 8 || b.n_elems >= ((int64_t)1 << (32 - 2 * tag_bits(b.k1)))) {
+    if (b.k1 > 32 || b.n_elems >= ((int64_t)1 << (32 - 2 * tag_bits(b.k1)))) {
         set_error("batched systems: %lld elements of %d nodes exceed the contribution tags", (long long)b.n_elems, b.k1);
         return MSFEM_ERR_LIMIT;
     }
@@ -825,17 +826,19 @@ int batch_assemble(BatchSys& b, const double* d_xyz, const double* d_lame, int n
     return 0;
 }
 
-int batch_assemble_given(BatchSys& b, const double* d_eblocks)
+int batch_assemble_given(BatchSys& b, const double* d_eblocks, bool scaled)
 {
     cudaStream_t st = b.stream;
     MSFEM_TRY(b.val64.alloc(std::max<int64_t>(1, 9 * b.nnzb)));
-    MSFEM_TRY(b.val32.alloc(std::max<int64_t>(1, 9 * b.nnzb)));
-    MSFEM_TRY(b.dscale.alloc(std::max<int64_t>(1, 3 * b.n_nodes)));
+    if (scaled) {
+        MSFEM_TRY(b.val32.alloc(std::max<int64_t>(1, 9 * b.nnzb)));
+        MSFEM_TRY(b.dscale.alloc(std::max<int64_t>(1, 3 * b.n_nodes)));
+    }
     const int blocks = (int)std::min<int64_t>((b.nnzb + 255) / 256, 148 * 16);
     if (b.nnzb)
         k_assemble_given<<<blocks, 256, 0, st>>>(b.nnzb, b.cstart.p, b.contrib.p, b.k1, d_eblocks, b.val64.p);
     const int nblk = (int)std::min<int64_t>((b.n_nodes + 255) / 256, 148 * 16);
-    if (b.n_nodes) {
+    if (scaled && b.n_nodes) {
         k_batch_scale<<<nblk, 256, 0, st>>>(b.n_nodes, b.row_ptr.p, b.col.p, b.val64.p, b.dscale.p);
         k_batch_val32<<<nblk, 256, 0, st>>>(b.n_nodes, b.row_ptr.p, b.col.p, b.val64.p, b.dscale.p, b.val32.p);
     }

@@ -16,7 +16,7 @@ namespace msfem {
 // the sum of its element contributions in element order.
 struct BatchSys {
     int dim = 3;  // 2: triangles, 3: tetrahedra
-    int k1 = 4;   // nodes per element
+    int k1 = 4;   // nodes per element (at most 32)
     int n_sys = 0;
     int R = 1;    // right-hand sides per system
     int64_t n_nodes = 0, n_elems = 0, nnzb = 0, n_pairs = 0;
@@ -58,8 +58,10 @@ int batch_assemble(BatchSys& b, const double* d_xyz, const double* d_lame, int n
 // the same launches without waiting for them (no host synchronisation, no allocation once the
 // buffers exist): capturable into a CUDA graph; a bad material id is left in b.aflag
 int batch_assemble_enqueue(BatchSys& b, const double* d_xyz, const double* d_lame, int n_mat);
-// values from caller-given element blocks [n_elems][k1][k1][9] (device)
-int batch_assemble_given(BatchSys& b, const double* d_eblocks);
+// values from caller-given element blocks [n_elems][k1][k1][9] (device), each block the sum of
+// its element contributions in element order; scaled: also the Jacobi scale and the FP32 copy
+// the batched solver reads
+int batch_assemble_given(BatchSys& b, const double* d_eblocks, bool scaled = true);
 // solves every system; x: [n_nodes][R][3] FP64, fixed entries hold the Dirichlet data on
 // entry, free entries are overwritten.  precision: MSFEM_FP64 or MSFEM_FP32_IR.  threads <= 0:
 // the CTA size is autotuned on the first call (cached per batch and precision).

@@ -104,6 +104,49 @@ int need_mesh(System& s, const char* who)
 }
 
 }  // namespace
+
+template <class T>
+static void take_buffer(DBuf<T>& dst, DBuf<T>& src)
+{
+    dst.release();
+    dst.p = src.p;
+    dst.n = src.n;
+    src.p = nullptr;
+    src.n = 0;
+}
+
+int system_adopt_csr(int n, DBuf<int32_t>& row_ptr, DBuf<int32_t>& col, DBuf<double>& val, int64_t nnz,
+                     msfem_system_t* out)
+{
+    *out = nullptr;
+    std::unique_ptr<System> s(new (std::nothrow) System());
+    if (!s) {
+        set_error("out of host memory");
+        return MSFEM_ERR_LIMIT;
+    }
+    s->kind = MSFEM_SCALAR;
+    s->bs = 1;
+    s->n_nodes = n;
+    s->n_tets = 0;
+    s->n_rows = n;
+    s->nnzb = nnz;
+    s->color_off = {0};
+    MSFEM_CK(cudaGetDevice(&s->device));
+    MSFEM_CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    MSFEM_CK(cudaEventCreate(&s->ev0));
+    MSFEM_CK(cudaEventCreate(&s->ev1));
+    take_buffer(s->nrp, row_ptr);
+    take_buffer(s->ncol, col);
+    take_buffer(s->val, val);
+    MSFEM_TRY(s->F.alloc((size_t)n));
+    MSFEM_TRY(s->X.alloc((size_t)n));
+    MSFEM_CK(cudaMemsetAsync(s->F.p, 0, sizeof(double) * n, s->stream));
+    MSFEM_CK(cudaMemsetAsync(s->X.p, 0, sizeof(double) * n, s->stream));
+    MSFEM_CK(cudaStreamSynchronize(s->stream));
+    *out = reinterpret_cast<msfem_system_t>(s.release());
+    return MSFEM_OK;
+}
+
 }  // namespace msfem
 
 using namespace msfem;

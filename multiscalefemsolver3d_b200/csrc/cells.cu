@@ -1515,7 +1515,6 @@ using msfem::BatchHandle;
 using msfem::CellsHandle;
 
 struct msfem_batch : BatchHandle {};
-struct msfem_cells : CellsHandle {};
 
 extern "C" {
 

@@ -74,3 +74,6 @@ struct CellsHandle {
 
 
 }  // namespace msfem
+
+// the C ABI's opaque cells handle (msfem_cells_t)
+struct msfem_cells : msfem::CellsHandle {};

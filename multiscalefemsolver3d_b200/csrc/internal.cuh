@@ -202,6 +202,10 @@ struct System {
 
 // ---- mesh / portrait (portrait.cu)
 int build_topology(System& s);
+// a scalar system (no mesh) owning a device CSR with the diagonal in every row, F = X = 0; the
+// buffers are moved into it (capi.cu)
+int system_adopt_csr(int n, DBuf<int32_t>& row_ptr, DBuf<int32_t>& col, DBuf<double>& val, int64_t nnz,
+                     msfem_system_t* out);
 // ---- assembly (assemble.cu)
 int assemble_scalar(System& s, const double* sigma, int n_mat);
 int assemble_scalar3(System& s, const double* S, const double* M, const double* f, bool on_device);

@@ -1,9 +1,8 @@
 """MsFEM Order2 (MsFEM/MsFEM.h:14-569, MsFEM_Grid.h:1001-3470) on the GPU: the macro topology and
-DOF numbering of a box macro mesh, the cells' 27 bases and macro element matrices
-(libmsfem_b200: msfem_cells_build_order2, msfem_cells_order2_macro_matrices), the macro system
-(msfem_order2_macro_csr), the Dirichlet values (the L2 projection Grid_forMech::
-CreateBoundaryConditions makes, :3303-3470) and the solve (msfem_system_from_cssd, Dirichlet rows
-and columns, a Krylov solve on the GPU).
+DOF numbering of a box macro mesh and the Dirichlet groups' DOF and face lists on the host; the
+cells' 27 bases (msfem_cells_build_order2) and the macro phase (msfem_cells_order2_macro_solve:
+element matrices, the macro system, the Dirichlet values as the L2 projection Grid_forMech::
+CreateBoundaryConditions makes, :3303-3470, their elimination and the solve) on the device.
 
 Macro mesh conventions: cell c's corners cell_vertex[c][b] sit at the box vertex b
 (x_{b&1}, y_{(b>>1)&1}, z_{(b>>2)&1}); its faces are the cycles FACE_CYCLES (x0, x1, y0, y1,
@@ -16,9 +15,10 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._lib import FP32_IR, MINRES, check, load
+from ._lib import FP32_IR, check, load
 
-__all__ = ["FACE_CYCLES", "MacroTopology", "macro_topology", "macro_csr", "dirichlet_values", "order2_elastic_driver"]
+__all__ = ["FACE_CYCLES", "MacroTopology", "macro_topology", "DirichletLayout", "dirichlet_layout", "macro_system",
+           "dirichlet_projection", "order2_elastic_driver"]
 
 FACE_CYCLES = np.array([[0, 2, 6, 4], [1, 3, 7, 5], [0, 1, 5, 4], [2, 3, 7, 6], [0, 1, 3, 2], [4, 5, 7, 6]])
 
@@ -61,152 +61,124 @@ def macro_topology(cell_vertex, n_vertices=None) -> MacroTopology:
     return MacroTopology(edges, faces, face_edges, cell_faces, dofs.astype(np.int64), nv)
 
 
-def macro_csr(topo: MacroTopology, K):
-    """The Order2 macro system (fem.Csr, DOF 3 d + c) from element matrices K [nc, 27, 27, 3, 3]."""
-    from .fem import Csr
-    L = load()
-    d = np.ascontiguousarray(topo.cell_dofs, dtype=np.int32)
-    K = np.ascontiguousarray(K, dtype=np.float64)
-    nd = topo.n_dofs
-    nnz = C.c_int64()
-    P = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
-    check(L.msfem_order2_macro_csr(d.shape[0], nd, P(d), P(K), None, None, None, C.byref(nnz)), "order2_macro_csr")
-    row_ptr = np.empty(3 * nd + 1, np.int64)
-    col = np.empty(nnz.value, np.int32)
-    val = np.empty(nnz.value, np.float64)
-    check(L.msfem_order2_macro_csr(d.shape[0], nd, P(d), P(K), P(row_ptr), P(col), P(val), C.byref(nnz)),
-          "order2_macro_csr")
-    return Csr(row_ptr, col, val, np.zeros(3 * nd), np.zeros(3 * nd))
+@dataclass
+class DirichletLayout:
+    """The integer bookkeeping of the Order2 Dirichlet groups, as msfem_cells_order2_dirichlet and
+    msfem_cells_order2_macro_solve take it."""
+    faces: np.ndarray           # int32 [n_faces, 10]: cell, 9 DOF ids (4 cycle vertices, 4 edges, face)
+    group_dof_off: np.ndarray   # int32 [n_groups + 1]
+    group_dofs: np.ndarray      # int32: each group's DOFs, ascending
+    group_face_off: np.ndarray  # int32 [n_groups + 1]
+    group_values: np.ndarray    # float64 [n_groups, 3]
+    fixed_dofs: np.ndarray      # int32: scalar rows 3 d + c in elimination order
+    fixed_src: np.ndarray       # int32: 3 k + c into the projected values [group DOF k][c]
 
 
-def _rule3(V):
-    """Polygon::SetIntegrationLaw(3) (Library/GeometryShape.h:2625-2640) over the cycle V: the fan
-    (centroid, V_i, V_i+1) with the triangle rule of :1495-1499 as the reference has it --
-    weights |e1 x e2| / 6 at (1/6, 1/6), (2/3, 1/6), (2/3, 1/6)."""
-    Cn = V.mean(axis=0)
-    ab = np.array([[1 / 6, 1 / 6], [2 / 3, 1 / 6], [2 / 3, 1 / 6]])
-    pts, w = [], []
-    for i in range(len(V)):
-        e1, e2 = V[i] - Cn, V[(i + 1) % len(V)] - Cn
-        area2 = np.linalg.norm(np.cross(e1, e2))
-        pts.append(Cn + ab[:, :1] * e1 + ab[:, 1:] * e2)
-        w.append(np.full(3, area2 / 6.0))
-    return np.concatenate(pts), np.concatenate(w)
-
-
-def _face_values(xyz, tets, bases_z, box, f_local, pts):
-    """bases_z [n_nodes, 27] at the points on local face f_local of the cell, interpolated in the
-    lowest-numbered tetrahedron whose face on that plane holds the point (the P1 value there)."""
-    axis, side = f_local // 2, f_local % 2
-    plane = box[2 * axis + side]
-    size = max(box[1] - box[0], box[3] - box[2], box[5] - box[4])
-    on = np.abs(xyz[:, axis] - plane) <= 1e-9 * size
-    hit = on[tets]
-    rows = np.nonzero(hit.sum(axis=1) == 3)[0]
-    tri = np.array([tets[e][hit[e]] for e in rows], dtype=np.int64).reshape(-1, 3)
-    other = [a for a in range(3) if a != axis]
-    P = xyz[tri][:, :, other]                                           # [t, 3, 2]
-    out = np.empty((len(pts), bases_z.shape[1]))
-    for q, x in enumerate(pts):
-        y = x[other]
-        T = np.stack([P[:, 1] - P[:, 0], P[:, 2] - P[:, 0]], axis=2)      # [t, 2, 2]
-        lam = np.linalg.solve(T, (y - P[:, 0])[:, :, None])[:, :, 0]
-        l0 = 1 - lam.sum(axis=1)
-        ok = np.nonzero((lam.min(axis=1) >= -1e-12) & (l0 >= -1e-12))[0]
-        if ok.size == 0:
-            raise ValueError("a boundary quadrature point lies on no face triangle of its cell")
-        t = ok[0]
-        bary = np.array([l0[t], lam[t, 0], lam[t, 1]])
-        out[q] = bary @ bases_z[tri[t]]
-    return out
-
-
-def dirichlet_values(vertex_xyz, cells, topo: MacroTopology, bases, groups):
-    """[(scalar DOF 3 d + c, value)] in the reference's order: per Dirichlet group (vertex ids,
-    value (3,), take (3 bools)) its DOFs (the vertices, the edges with both ends in it, the faces
-    with all four in it, ascending) with the L2 projection of its value over its faces (the faces'
-    9 DOFs, the bases' z components, polygon rule 3), each taken component of each DOF in turn.
-    bases: [per cell (n_nodes, 27, 3)] (Cells.order2_bases split by cell).  A group's faces must lie
-    on the boundary (one cell each)."""
-    vertex_xyz = np.asarray(vertex_xyz, dtype=np.float64)
-    nv, ne = topo.n_vertices, len(topo.edges)
-    face_cell = {}
-    for c in range(len(topo.cell_faces)):
-        for fl, f in enumerate(topo.cell_faces[c]):
-            face_cell.setdefault(int(f), []).append((c, fl))
-    out = []
+def dirichlet_layout(topo: MacroTopology, groups) -> DirichletLayout:
+    """Per Dirichlet group (vertex ids, value (3,), take (3 bools)) -- Grid_forMech::
+    CreateBoundaryConditions, MsFEM_Grid.h:3303-3470 -- its DOFs (the vertices, the edges with both
+    ends in it, the faces with all four vertices in it, ascending), its faces (ascending face id,
+    each on one cell only) with their 9 DOFs (the cycle vertices, the edges between cycle nodes k
+    and k + 1, the face), and the rows to eliminate: each group DOF in order, each taken component
+    (scalar row 3 d + c).  A row named twice is eliminated once, at its first place, with the
+    later group's value (the reference would already have moved the earlier value into the other
+    rows by then, MsFEM.h:300-365; that inconsistency is not copied)."""
+    nv, ne, nf = topo.n_vertices, len(topo.edges), len(topo.faces)
+    nc = topo.cell_faces.shape[0]
+    count = np.bincount(topo.cell_faces.ravel(), minlength=nf)
+    face_cell = np.full(nf, -1, np.int64)
+    face_cell[topo.cell_faces.ravel()] = np.repeat(np.arange(nc), 6)
+    faces, dof_off, dofs, face_off, values = [], [0], [], [0], []
+    rows, src = [], []
     for verts, value, take in groups:
-        sv = set(int(v) for v in verts)
-        value = np.asarray(value, dtype=np.float64)
-        on_e = [nv + i for i, (a, b) in enumerate(topo.edges) if a in sv and b in sv]
-        tf = [i for i in range(len(topo.faces)) if set(int(v) for v in topo.faces[i]) <= sv]
-        gd = sorted([int(v) for v in verts] + on_e + [nv + ne + i for i in tf])
-        pos = {d: k for k, d in enumerate(gd)}
-        M = np.zeros((len(gd), len(gd)))
-        Fg = np.zeros((len(gd), 3))
+        verts = np.unique(np.asarray(verts, dtype=np.int64))
+        inside = np.zeros(nv, bool)
+        inside[verts] = True
+        on_e = np.nonzero(inside[topo.edges[:, 0]] & inside[topo.edges[:, 1]])[0]
+        tf = np.nonzero(inside[topo.faces].all(axis=1))[0]
+        gd = np.sort(np.concatenate([verts, nv + on_e, nv + ne + tf]))
         for f in tf:
-            if len(face_cell[f]) != 1:
+            if count[f] != 1:
                 raise ValueError(f"Dirichlet face {f} is shared by two cells")
-            c, fl = face_cell[f][0]
-            cyc = [int(v) for v in topo.faces[f]]
-            fd = cyc + [nv + int(e) for e in topo.face_edges[f]] + [nv + ne + f]
-            xyz, tets, mat, box = cells.cell(c)
-            loc = {int(d): k for k, d in enumerate(topo.cell_dofs[c])}
-            pts, w = _rule3(vertex_xyz[cyc])
-            psi = _face_values(xyz, np.asarray(tets, np.int64), bases[c][:, :, 2], box, fl, pts)[:, [loc[d] for d in fd]]
-            Ml = (psi * w[:, None]).T @ psi
-            Fl = (psi * w[:, None]).sum(axis=0)[:, None] * value[None, :]
-            idx = [pos.get(d, -1) for d in fd]
-            for I, gi in enumerate(idx):
-                if gi < 0:
-                    continue
-                for J, gj in enumerate(idx):
-                    if gj >= 0:
-                        M[gi, gj] += Ml[I, J]
-                Fg[gi] += Fl[I]
-        # the face bubbles vanish on their own faces: empty rows, value 0 (least squares)
-        vals = np.linalg.lstsq(M, Fg, rcond=None)[0]
+            faces.append(np.concatenate([[face_cell[f]], topo.faces[f], nv + topo.face_edges[f], [nv + ne + f]]))
+        base = dof_off[-1]
         for k, d in enumerate(gd):
             for comp in range(3):
                 if take[comp]:
-                    out.append((3 * d + comp, float(vals[k, comp])))
-    return out
+                    rows.append(3 * int(d) + comp)
+                    src.append(3 * (base + k) + comp)
+        dofs.append(gd)
+        dof_off.append(base + len(gd))
+        face_off.append(face_off[-1] + len(tf))
+        values.append(np.asarray(value, dtype=np.float64).reshape(3))
+    last = {}
+    for r, i in zip(rows, src):
+        last[r] = i
+    return DirichletLayout(
+        faces=np.asarray(faces, np.int32).reshape(-1, 10),
+        group_dof_off=np.asarray(dof_off, np.int32),
+        group_dofs=(np.concatenate(dofs) if dofs else np.zeros(0)).astype(np.int32),
+        group_face_off=np.asarray(face_off, np.int32),
+        group_values=np.asarray(values, np.float64).reshape(-1, 3),
+        fixed_dofs=np.asarray(list(last.keys()), np.int32),
+        fixed_src=np.asarray(list(last.values()), np.int32))
+
+
+def _args(topo: MacroTopology, vertex_xyz, lay: DirichletLayout):
+    P = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    keep = [np.ascontiguousarray(topo.cell_dofs, dtype=np.int32), np.ascontiguousarray(vertex_xyz, dtype=np.float64)]
+    keep += [np.ascontiguousarray(a) for a in (lay.faces, lay.group_dof_off, lay.group_dofs, lay.group_face_off,
+                                               lay.group_values)]
+    cd, vx, fa, do, gd, fo, gv = keep
+    args = [topo.n_dofs, P(cd), vx.shape[0], P(vx), fa.shape[0], P(fa), gv.shape[0], P(do), P(gd), P(fo), P(gv)]
+    return args, keep
+
+
+def macro_system(cells_gpu, topo: MacroTopology):
+    """The Order2 macro system on the device (msfem_cells_order2_macro_system): a matrix-only
+    fem.System, scalar rows 3 d + c, from the built Order2 bases of `cells_gpu` (cells.Cells)."""
+    from .fem import System
+    cd = np.ascontiguousarray(topo.cell_dofs, dtype=np.int32)
+    h = C.c_void_p()
+    check(load().msfem_cells_order2_macro_system(cells_gpu.h, topo.n_dofs, cd.ctypes.data_as(C.c_void_p),
+                                                 C.byref(h)), "cells_order2_macro_system")
+    return System._from_handle(h)
+
+
+def dirichlet_projection(cells_gpu, topo: MacroTopology, vertex_xyz, lay: DirichletLayout):
+    """The projected Dirichlet values [len(lay.group_dofs), 3] on the device
+    (msfem_cells_order2_dirichlet)."""
+    args, keep = _args(topo, vertex_xyz, lay)
+    out = np.empty((max(1, lay.group_dofs.size), 3))
+    check(load().msfem_cells_order2_dirichlet(cells_gpu.h, *args, out.ctypes.data_as(C.c_void_p)),
+          "cells_order2_dirichlet")
+    return out[:lay.group_dofs.size]
 
 
 def order2_elastic_driver(cells, vertex_xyz, cell_vertex, groups, precision=FP32_IR, tol=1e-8, cell_tol=1e-8,
                           maxiter=200000):
     """MsFEM_forElasticDeformation_OrderBF2_forPoly on the GPU: returns (macro solution [n_dofs, 3],
-    info).  The cell bases and element matrices are built on the GPU, the macro system is summed on
-    the host and solved on the GPU with its Dirichlet rows and columns (MINRES, FP32 inner solves
-    in FP64 refinement by default) to ||F - A x|| <= tol ||F||; the reference runs plain CG restarts
-    on the same system (MsFEM.h:445-478)."""
-    from . import fem
+    info).  The cell bases (msfem_cells_build_order2) and the whole macro phase
+    (msfem_cells_order2_macro_solve: element matrices, the macro system, the projected Dirichlet
+    values, their elimination by rows and columns, MINRES with FP32 inner solves in FP64
+    refinement by default, to ||F - A x|| <= tol ||F||) run on the device; the host computes the
+    macro topology and the groups' DOF and face lists.  The reference runs plain CG restarts on
+    the same system (MsFEM.h:445-478)."""
     from .cells import Cells
-    topo = macro_topology(cell_vertex, n_vertices=np.asarray(vertex_xyz).shape[0])
+    vertex_xyz = np.asarray(vertex_xyz, dtype=np.float64)
+    topo = macro_topology(cell_vertex, n_vertices=vertex_xyz.shape[0])
+    lay = dirichlet_layout(topo, groups)
+    args, keep = _args(topo, vertex_xyz, lay)
+    fd = np.ascontiguousarray(lay.fixed_dofs, dtype=np.int32)
+    fs = np.ascontiguousarray(lay.fixed_src, dtype=np.int32)
+    U = np.empty((topo.n_dofs, 3))
+    it, rel = C.c_int32(), C.c_double()
+    P = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
     cg = Cells(cells)
     try:
         cg.build_order2(np.asarray(cell_vertex, np.int32), precision, cell_tol)
-        K = cg.order2_macro_matrices()
-        allb = cg.order2_bases()
+        rc = check(load().msfem_cells_order2_macro_solve(cg.h, *args, fd.size, P(fd), P(fs), precision, tol, maxiter,
+                                                         P(U), C.byref(it), C.byref(rel)), "cells_order2_macro_solve")
     finally:
         cg.close()
-    bases = [allb[cells.node_off[c]:cells.node_off[c + 1]] for c in range(cells.n_cells)]
-    fixed = dirichlet_values(vertex_xyz, cells, topo, bases, groups)
-    A = macro_csr(topo, K)
-    S = fem.System.from_csr(A, F=np.zeros(A.n), X=np.zeros(A.n))
-    try:
-        # a DOF in two groups keeps the later group's value; the reference then has moved the earlier
-        # value into the other rows already (its column sweep runs per group), an inconsistency
-        # this elimination does not copy
-        last = {}
-        for i, v in fixed:
-            last[i] = v
-        dofs = np.array(list(last.keys()), np.int32)
-        vals = np.array(list(last.values()))
-        S.apply_dirichlet(dofs, vals, fem.ROW_AND_COLUMN)
-        S.copy_f_to_x()
-        rel, it, rc = S.solve(MINRES, precision, tol=tol, maxiter=maxiter)
-        x = S.get_x()
-    finally:
-        S.close()
-    return x.reshape(-1, 3), {"rel_residual": rel, "iterations": it, "rc": rc, "n_dofs": topo.n_dofs}
+    return U, {"rel_residual": rel.value, "iterations": it.value, "rc": rc, "n_dofs": topo.n_dofs}

@@ -393,6 +393,16 @@ def macro_topology(cell_vertex):
 ORDER2_REF = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_ref", "order2_ref")
 
 
+def macro_portrait(cell_dofs, n_dofs):
+    """The Order2 macro portrait (Grid_forMech::CreationPortrait, MsFEM/MsFEM.h:53-55): DOF row d
+    holds the DOFs sharing a cell with d, the diagonal included, ascending."""
+    rows = [set() for _ in range(n_dofs)]
+    for dl in np.asarray(cell_dofs):
+        for d in dl:
+            rows[int(d)].update(int(e) for e in dl)
+    return [np.array(sorted(r), dtype=np.int64) for r in rows]
+
+
 def run_reference(workdir, vertex_xyz, cell_vertex, cells, matrices=True, timeout=1200, groups=None,
                   min_residual=1e-13, order1=False):
     """Writes the macro mesh and cell directories under workdir (meshio writers), runs the

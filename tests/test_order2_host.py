@@ -47,12 +47,30 @@ def _case():
     return vxyz, cv, cm, bases, groups
 
 
-def test_order2_topology_macro_system_and_dirichlet_values_match_restatement(lib):
-    """The product's host side of the Order2 driver (macro topology, the macro CSR summed by the
-    library, the projected Dirichlet values) on the restatement's bases: the same topology, the
-    same system as the restatement's dense assembly, the same fixed values, and with them the same
-    macro solution.  (The GPU builds of the bases and element matrices, the Dirichlet rows and the
-    solve are covered by their own GPU tests.)"""
+def _expected_projection(lay, groups, want):
+    """The restatement's fixed list [(scalar DOF, value)] read back into the layout's [group DOF
+    k][c] slots: entry j of the list is the j-th (group, k, taken c) in the layout's order, so its
+    DOF must be 3 gd[k] + c."""
+    P = np.full(3 * lay.group_dofs.size, np.nan)
+    j = 0
+    for g, (_, _, take) in enumerate(groups):
+        for k in range(lay.group_dof_off[g], lay.group_dof_off[g + 1]):
+            for comp in range(3):
+                if take[comp]:
+                    assert want[j][0] == 3 * int(lay.group_dofs[k]) + comp
+                    P[3 * k + comp] = want[j][1]
+                    j += 1
+    assert j == len(want)
+    return P
+
+
+def test_order2_topology_and_dirichlet_layout_match_restatement(lib):
+    """The product's host side of the Order2 driver (macro topology, the groups' DOF and face
+    lists, the elimination order) against the restatement (oracle/order2.py, pinned against the
+    reference's topology and whole driver): the same topology; per group the restatement's DOFs in
+    its order, its faces with their 9 DOFs; and the rows eliminated, with the restatement's
+    projected values gathered through the layout, give the restated driver's solution.  (The
+    projection itself, the macro system and the solve run on the GPU: tests/test_gpu_order2.py.)"""
     from multiscalefemsolver3d_b200 import order2 as p2
     vxyz, cv, cm, bases, groups = _case()
     topo = p2.macro_topology(cv, n_vertices=vxyz.shape[0])
@@ -61,24 +79,43 @@ def test_order2_topology_macro_system_and_dirichlet_values_match_restatement(lib
     np.testing.assert_array_equal(topo.faces, faces)
     np.testing.assert_array_equal(topo.cell_faces, cell_faces)
     np.testing.assert_array_equal(topo.cell_dofs, dofs)
-    K = np.stack([o2.macro_element_matrix(*cm.cell(c)[:2], bases[c], cm.cell(c)[3], cm.E[0], cm.nu[0])
-                  for c in range(cm.n_cells)])
-    A = p2.macro_csr(topo, K)
-    dense = np.zeros((3 * topo.n_dofs,) * 2)
-    for c in range(cm.n_cells):
-        idx = (3 * dofs[c][:, None] + np.arange(3)).ravel()
-        dense[np.ix_(idx, idx)] += K[c].transpose(0, 2, 1, 3).reshape(81, 81)
-    np.testing.assert_allclose(A.to_scipy().toarray(), dense, rtol=0, atol=1e-14 * np.abs(dense).max())
-    assert np.all(np.diff(A.row_ptr) % 3 == 0)            # whole 3x3 blocks per row
-    got = p2.dirichlet_values(vxyz, cm, topo, bases, groups)
+    lay = p2.dirichlet_layout(topo, groups)
+    nv, ne = vxyz.shape[0], len(edges)
+    eid = {tuple(e): i for i, e in enumerate(edges)}
+    for g, (verts, _, _) in enumerate(groups):
+        sv = set(int(v) for v in verts)
+        tf = [i for i in range(len(faces)) if set(int(v) for v in faces[i]) <= sv]
+        rows = lay.faces[lay.group_face_off[g]:lay.group_face_off[g + 1]]
+        assert len(rows) == len(tf)
+        for r, f in zip(rows, tf):
+            cyc = [int(v) for v in faces[f]]
+            fd = cyc + [nv + eid[(min(cyc[k], cyc[(k + 1) % 4]), max(cyc[k], cyc[(k + 1) % 4]))] for k in range(4)]
+            assert list(r[1:]) == fd + [nv + ne + f]
+            assert f in cell_faces[r[0]]
     want = o2.dirichlet_fixed(vxyz, cv, cm, groups, bases)
-    assert [i for i, _ in got] == [i for i, _ in want]
-    np.testing.assert_allclose([v for _, v in got], [v for _, v in want], rtol=0, atol=1e-13)
-    # the composition: eliminate and solve the product's system, compare with the restated driver
-    M = A.to_scipy().toarray()
-    F = np.zeros(M.shape[0])
-    for i, v in got:
-        F -= M[:, i] * v
+    P = _expected_projection(lay, groups, want)
+    last = {}
+    for i, v in want:
+        last[i] = v
+    np.testing.assert_array_equal(lay.fixed_dofs, list(last.keys()))
+    np.testing.assert_array_equal(P[lay.fixed_src], list(last.values()))
+    # the composition: the dense macro system, the layout's eliminations, the restated driver, on
+    # groups without shared DOFs (the product eliminates a shared row once, with its last value)
+    groups = groups[:2]
+    lay = p2.dirichlet_layout(topo, groups)
+    P = _expected_projection(lay, groups, o2.dirichlet_fixed(vxyz, cv, cm, groups, bases))
+    n = 3 * topo.n_dofs
+    M = np.zeros((n, n))
+    for c in range(cm.n_cells):
+        K = o2.macro_element_matrix(*cm.cell(c)[:2], bases[c], cm.cell(c)[3], cm.E[0], cm.nu[0])
+        idx = (3 * dofs[c][:, None] + np.arange(3)).ravel()
+        M[np.ix_(idx, idx)] += K.transpose(0, 2, 1, 3).reshape(81, 81)
+    F = np.zeros(n)
+    for i, s in zip(lay.fixed_dofs, lay.fixed_src):
+        v = P[s]
+        col = M[:, i].copy()
+        col[i] = 0.0
+        F -= col * v
         M[:, i] = 0.0
         M[i, :] = 0.0
         M[i, i] = 1.0
@@ -88,72 +125,12 @@ def test_order2_topology_macro_system_and_dirichlet_values_match_restatement(lib
     assert np.linalg.norm(x - xo) <= 1e-11 * np.linalg.norm(xo)
 
 
-def test_order2_driver_orchestration_with_stand_ins(monkeypatch, lib):
-    """order2.order2_elastic_driver end to end with its two GPU objects replaced by stand-ins that
-    return the restatement's bases and element matrices and solve the eliminated system exactly:
-    the glue (DOF lists, the CSR from the library, the projected values, their elimination order,
-    the reshape) reproduces the restated driver."""
-    from multiscalefemsolver3d_b200 import cells as gcells
-    from multiscalefemsolver3d_b200 import fem
+def test_order2_layout_rejects_shared_faces(lib):
+    """A group holding an interior face (shared by two cells) is refused, as the restatement
+    assumes every Dirichlet face lies on the boundary."""
     from multiscalefemsolver3d_b200 import order2 as p2
-    vxyz, cv, cm, bases, groups = _case()
-    K = np.stack([o2.macro_element_matrix(*cm.cell(c)[:2], bases[c], cm.cell(c)[3], cm.E[0], cm.nu[0])
-                  for c in range(cm.n_cells)])
-
-    class FakeCells:
-        def __init__(self, meshes):
-            assert meshes is cm
-
-        def build_order2(self, cell_vertex, precision, tol):
-            np.testing.assert_array_equal(cell_vertex, cv)
-            return 0
-
-        def order2_macro_matrices(self):
-            return K
-
-        def order2_bases(self):
-            return np.concatenate(bases)
-
-        def close(self):
-            pass
-
-    class FakeSystem:
-        @classmethod
-        def from_csr(cls, A, F=None, X=None):
-            self = cls()
-            self.A = A.to_scipy().toarray()
-            self.F = np.zeros(A.n)
-            return self
-
-        def apply_dirichlet(self, dofs, vals, mode):
-            assert mode == fem.ROW_AND_COLUMN
-            for i, v in zip(dofs, vals):
-                col = self.A[:, i].copy()
-                col[i] = 0.0
-                self.F -= col * v
-                self.A[:, i] = 0.0
-                self.A[i, :] = 0.0
-                self.A[i, i] = 1.0
-                self.F[i] = v
-
-        def copy_f_to_x(self):
-            pass
-
-        def solve(self, method, precision, tol, maxiter):
-            self.x = np.linalg.solve(self.A, self.F)
-            return 0.0, 1, 0
-
-        def get_x(self):
-            return self.x
-
-        def close(self):
-            pass
-
-    monkeypatch.setattr(gcells, "Cells", FakeCells)
-    monkeypatch.setattr(fem.System, "from_csr", FakeSystem.from_csr)
-    # groups without shared DOFs: the product eliminates each DOF once with its last value
-    g2 = groups[:2]
-    x, info = p2.order2_elastic_driver(cm, vxyz, cv, g2)
-    xo = o2.order2_driver(vxyz, cv, cm, g2, bases=bases)
-    assert info["n_dofs"] == xo.shape[0]
-    assert np.linalg.norm(x - xo) <= 1e-11 * np.linalg.norm(xo)
+    vxyz, cv, cm = o2.graded_cells(2, 1, 0.0)
+    topo = p2.macro_topology(cv, n_vertices=vxyz.shape[0])
+    mid = np.nonzero(np.abs(vxyz[:, 2] - 0.5) < 1e-12)[0]
+    with pytest.raises(ValueError):
+        p2.dirichlet_layout(topo, [(mid, (0.0, 0.0, 0.0), (1, 1, 1))])

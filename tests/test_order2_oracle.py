@@ -94,23 +94,23 @@ def test_order2_driver_matches_reference(tmp_path):
 
 
 def test_order2_macro_portrait_matches_reference(tmp_path, lib):
-    """The library's Order2 macro CSR (msfem_order2_macro_csr) has the reference driver's block
+    """The restatement's portrait rule (o2.macro_portrait: the DOFs sharing a cell; the GPU macro
+    system is checked against it in tests/test_gpu_order2.py) is the reference driver's block
     portrait: per DOF row, the columns below and above the diagonal (CreationPortrait)."""
-    from multiscalefemsolver3d_b200 import order2 as p2
     vxyz, cv, cm = o2.graded_cells(2, 1, 0.0)
     top = np.nonzero(np.abs(vxyz[:, 2] - 1) < 1e-12)[0]
     R = o2.run_reference(str(tmp_path), vxyz, cv, cm, matrices=False,
                          groups=[(top, (0.0, 0.0, 0.01), (1, 1, 1))], min_residual=1e-12)
-    topo = p2.macro_topology(cv, n_vertices=vxyz.shape[0])
-    A = p2.macro_csr(topo, np.zeros((cm.n_cells, 27, 27, 3, 3)))
+    edges, faces, _, dofs = o2.macro_topology(cv)
+    n_dofs = vxyz.shape[0] + len(edges) + len(faces) + len(cv)
+    rule = o2.macro_portrait(dofs, n_dofs)
     rec, i = R["portrait"], 0
-    for d in range(topo.n_dofs):
+    for d in range(n_dofs):
         nd = rec[i]
         down = rec[i + 1:i + 1 + nd]
         i += 1 + nd
         nu = rec[i]
         up = rec[i + 1:i + 1 + nu]
         i += 1 + nu
-        cols = A.col[A.row_ptr[3 * d]:A.row_ptr[3 * d + 1]][::3] // 3      # the block columns of DOF row d
-        np.testing.assert_array_equal(cols, np.concatenate([np.sort(down), [d], np.sort(up)]))
+        np.testing.assert_array_equal(rule[d], np.concatenate([np.sort(down), [d], np.sort(up)]))
     assert i == rec.size
