@@ -572,8 +572,10 @@ int msfem_solve_twolevel(msfem_system_t fine, msfem_coarse_t c, int precision, i
 /* Switches msfem_solve_twolevel (precision MSFEM_FP64) to the symmetric multiplicative cycle
  * on the textbook operator: `textbook` is a second system on the same mesh assembled with
  * msfem_assemble_elastic_textbook and given the same Dirichlet rows.  One application of M^-1:
- * `degree` Chebyshev steps on its Jacobi-scaled FP32 matrix (spectrum bound [lmax/ratio, lmax],
- * lmax from 50 power steps x 1.1, widened by the solve if a step fails), the coarse correction,
+ * `degree` Chebyshev steps on its Jacobi-scaled FP32 matrix (ratio > 1: the first-kind polynomial
+ * for the spectrum bound [lmax/ratio, lmax]; ratio 0: the fourth-kind polynomial on [0, lmax],
+ * which needs no lower bound; lmax from 50 power steps x 1.1, widened by the solve if a step
+ * fails), the coarse correction,
  * the same Chebyshev steps again; SPD, so
  * MINRES on the reference's matrix keeps its guarantees.  storage: 0 the FP32 SELL matrix; 1 its
  * values in FP16 (arithmetic stays FP32; rounding each entry keeps the matrix symmetric, so the

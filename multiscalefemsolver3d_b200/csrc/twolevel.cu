@@ -1719,22 +1719,34 @@ int inner_solve_mg(CoarseHandle& C, int maxiter, double tau, double stop2, int* 
     return C.h_st->done == 3 ? MSFEM_ERR_NUMERIC : MSFEM_OK;
 }
 
-// Chebyshev step coefficients for the spectrum bound [lmax / ratio, lmax] of the Jacobi-scaled
-// textbook operator; drops the captured cycle (it holds the old coefficients)
+// Chebyshev step coefficients of the Jacobi-scaled textbook operator; drops the captured cycle (it
+// holds the old coefficients).  ratio > 1: the first-kind polynomial for the spectrum bound
+// [lmax / ratio, lmax]; ratio 0: the fourth-kind polynomial on [0, lmax] (J. Lottes, "Optimal
+// polynomial smoothers for multigrid V-cycles", 2023: d_0 = 4 / (3 lmax) r_0,
+// d_k = (2k - 1) / (2k + 3) d_k-1 + (8k + 4) / ((2k + 3) lmax) r_k), which needs no lower bound
 void cheb_coefs(CoarseHandle& C, double lmax, double ratio, int degree)
 {
     C.lmax = lmax;
     C.ratio = ratio;
-    C.lmin = C.lmax / ratio;
-    const double theta = 0.5 * (C.lmax + C.lmin), delta = 0.5 * (C.lmax - C.lmin), sigma = theta / delta;
-    double rho = 1.0 / sigma;
     C.cc = ChebCoef{};
-    C.cc.inv_theta = (float)(1.0 / theta);
-    for (int i = 1; i < degree; i++) {
-        const double rn = 1.0 / (2.0 * sigma - rho);
-        C.cc.a[i] = (float)(rn * rho);
-        C.cc.b[i] = (float)(2.0 * rn / delta);
-        rho = rn;
+    if (ratio == 0.0) {
+        C.lmin = 0.0;
+        C.cc.inv_theta = (float)(4.0 / (3.0 * lmax));
+        for (int k = 1; k < degree; k++) {
+            C.cc.a[k] = (float)((2.0 * k - 1.0) / (2.0 * k + 3.0));
+            C.cc.b[k] = (float)((8.0 * k + 4.0) / ((2.0 * k + 3.0) * lmax));
+        }
+    } else {
+        C.lmin = C.lmax / ratio;
+        const double theta = 0.5 * (C.lmax + C.lmin), delta = 0.5 * (C.lmax - C.lmin), sigma = theta / delta;
+        double rho = 1.0 / sigma;
+        C.cc.inv_theta = (float)(1.0 / theta);
+        for (int i = 1; i < degree; i++) {
+            const double rn = 1.0 / (2.0 * sigma - rho);
+            C.cc.a[i] = (float)(rn * rho);
+            C.cc.b[i] = (float)(2.0 * rn / delta);
+            rho = rn;
+        }
     }
     C.cheb_deg = degree;
     if (C.graph[2]) {
@@ -1758,8 +1770,8 @@ int set_smoother(CoarseHandle& C, System& T, int degree, double ratio, int stora
         set_error("msfem_coarse_set_smoother: storage must be 0 (FP32), 1 (FP16) or 2 (matrix-free)");
         return MSFEM_ERR_ARGUMENT;
     }
-    if (degree < 1 || degree > 8 || !(ratio > 1.0)) {
-        set_error("msfem_coarse_set_smoother: degree must be 1..8 and ratio > 1");
+    if (degree < 1 || degree > 8 || !(ratio > 1.0 || ratio == 0.0)) {
+        set_error("msfem_coarse_set_smoother: degree must be 1..8 and ratio > 1 (or 0: fourth kind)");
         return MSFEM_ERR_ARGUMENT;
     }
     MSFEM_TRY(prepare_sell(T));

@@ -51,8 +51,10 @@ class TwoLevel:
         """Multiplicative cycle with Chebyshev smoothing on the textbook-orientation system
         (fem.System assembled with assemble_elastic_textbook, same Dirichlet rows); half_matrix
         stores the smoother's matrix values in FP16; matrix_free applies the operator from the
-        tetrahedra's materials on the system's Kuhn grid (System.set_kuhn_grid).  The default
-        degree and spectrum ratio were the fastest of a sweep on the 128^3 elasticity case."""
+        tetrahedra's materials on the system's Kuhn grid (System.set_kuhn_grid).  ratio > 1: the
+        first-kind Chebyshev polynomial for [lambda_max / ratio, lambda_max]; ratio 0: the
+        fourth-kind polynomial on [0, lambda_max].  The default degree and spectrum ratio were the
+        fastest of a sweep on the 128^3 elasticity case."""
         self._text = textbook_system
         storage = 2 if matrix_free else (1 if half_matrix else 0)
         check(load().msfem_coarse_set_smoother(self.h, textbook_system.h, degree, ratio, storage),

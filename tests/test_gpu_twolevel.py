@@ -111,17 +111,19 @@ def test_textbook_assembly_is_the_blockwise_transpose(case):
     del perm
 
 
-@pytest.fixture(scope="module", params=[0, 1, 2], ids=["fp32-smoother", "fp16-smoother", "matrix-free"])
+@pytest.fixture(scope="module", params=[0, 1, 2, 3],
+                ids=["fp32-smoother", "fp16-smoother", "matrix-free", "matrix-free-fourth-kind"])
 def mg_case(lib, cuda, request):
     p, S, cc, cells, dofs = _setup()
     K = fem.System(fem.ELASTIC, p.mesh.xyz, p.mesh.tets, p.mesh.mat)
     K.assemble_elastic_textbook(p.E, p.nu)
     K.apply_dirichlet(dofs, np.zeros(dofs.size), fem.ROW_AND_COLUMN)
     T = TwoLevel(S, cells, cc, dofs)
-    if request.param == 2:
+    if request.param >= 2:
         S.set_kuhn_grid(p.mesh.n)
         K.set_kuhn_grid(p.mesh.n)
-        T.set_smoother(K, degree=3, ratio=30.0, matrix_free=True)
+        # param 3: the fourth-kind polynomial (ratio 0, no lower spectrum bound)
+        T.set_smoother(K, degree=3, ratio=30.0 if request.param == 2 else 0.0, matrix_free=True)
         T.set_matrix_free(True)
     else:
         T.set_smoother(K, degree=3, ratio=30.0, half_matrix=request.param == 1)
