@@ -211,6 +211,38 @@ static bool kuhn_isotropic(const System& s)
     return std::fabs(s.kuhn_h[1] - h) <= 1e-12 * h && std::fabs(s.kuhn_h[2] - h) <= 1e-12 * h;
 }
 
+namespace {
+
+// xh = s x with the eliminated columns zero: the input of the pre-scaled kernel (k_kuhn_zp)
+__global__ void k_kuhn_prescale(int64_t n, const float* __restrict__ x, const float* __restrict__ scale,
+                                const uint32_t* __restrict__ fix, float* __restrict__ xh)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        xh[i] = ((fix[i / 3] >> (3 + i % 3)) & 1u) ? 0.0f : scale[i] * x[i];
+}
+
+// y = S K S x through the pre-scaled kernel: y = x on the Dirichlet rows, s (K xh) elsewhere
+struct EpiStoreP {
+    static constexpr int NE = 2;  // x, the Jacobi scale
+    float* y;
+    const float* x;
+    const float* scale;
+    __device__ __forceinline__ bool skip() const { return false; }
+    __host__ __device__ __forceinline__ void sources(const float** ev) const
+    {
+        ev[0] = x;
+        ev[1] = scale;
+    }
+    __device__ __forceinline__ void operator()(int64_t g, const float* v, uint32_t fx, const float (*e)[3])
+    {
+#pragma unroll
+        for (int c = 0; c < 3; c++) y[3 * g + c] = ((fx >> c) & 1u) ? e[0][c] : v[c] * e[1][c];
+    }
+    __device__ __forceinline__ void finish() {}
+};
+
+}  // namespace
+
 int kuhn_operator_build(System& s, int form, bool fp64, bool scaled, KuhnOperator& op)
 {
     op.sys = nullptr;
@@ -313,6 +345,27 @@ int kuhn_operator_build(System& s, int form, bool fp64, bool scaled, KuhnOperato
             set_error("matrix-free operator: its product differs from the assembled matrix's (relative %.3g in l2, "
                       "%.3g in max); the values are not the Kuhn grid's elasticity operator", rl2, rmax);
             return MSFEM_ERR_STATE;
+        }
+        if (form == 2) {
+            // the pre-scaled kernel the smoother steps run: the same product, bit for bit
+            DBuf<float> xh;
+            MSFEM_TRY(xh.alloc(n + 16));
+            k_kuhn_prescale<<<148 * 4, 256, 0, st>>>(n, x.p, op.scale32.p, op.v32.fix, xh.p);
+            const cudaError_t e = KzpKernel<2, float, kKzTX, kKzTY, kKzMinB, EpiStoreP>::launch(
+                op.v32, xh.p, EpiStoreP{y2.p, x.p, op.scale32.p}, op.sms, op.err.p, st);
+            if (e != cudaSuccess) {
+                set_error("matrix-free FP32 product (pre-scaled input): %s", cudaGetErrorString(e));
+                return MSFEM_ERR_CUDA;
+            }
+            MSFEM_TRY(kuhn_check_err(op, st));
+            double pl2 = 0.0, pmax = 0.0;
+            MSFEM_TRY(compare<float>(st, n, y2.p, y1.p, &pl2, &pmax));
+            if (pmax != 0.0) {
+                set_error("matrix-free operator: the pre-scaled kernel's product differs from the staged-scale "
+                          "kernel's (relative %.3g in max)", pmax);
+                return MSFEM_ERR_STATE;
+            }
+            s.total_launches += 2;
         }
     }
     op.check_l2 = rl2;

@@ -22,6 +22,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 
 #include "kuhn.cuh"
 
@@ -187,6 +188,13 @@ __device__ __forceinline__ void kz_issue(const KzArgs<T>& A, const KzCopy& c, in
     __syncwarp();
     if (bytes) kz_bulk(kz_smem_addr(stage + c.dst), src, bytes, bar);
 }
+
+// an epilogue with `static constexpr bool WANTS_SV = true` also gets the node's Jacobi scale (1
+// without one) and its Dirichlet word: operator()(node, y, xin, e, s[3], fix)
+template <class E, class = void>
+struct kz_wants_sv : std::false_type {};
+template <class E>
+struct kz_wants_sv<E, std::void_t<decltype(E::WANTS_SV)>> : std::bool_constant<E::WANTS_SV> {};
 
 // the z-marching product; Epi: NE per-node input vectors (sources(ev)), skip(), finish(),
 // operator()(node, y[3], input x[3], e[NE][3] = those vectors at the node)
@@ -372,16 +380,204 @@ __global__ void __launch_bounds__(TX* TY, MINB) k_kuhn_z(KzArgs<T> A, Epi epi)
             const int wj = cj + 1;
             const int xo = ((3 * wrow + P3m * kz) & (L::EL - 1)) + 3 * (gi - gi_lo);
             const uint32_t fx = fr[wj * L::FP + ((wrow + Pm4 * kz) & 3) + (gi - gi_lo)];
-            T xin[3];
+            T xin[3], sv[3];
 #pragma unroll
             for (int a = 0; a < 3; a++) {
                 xin[a] = xr[wj * L::XP + xo + a];
+                sv[a] = SC ? sr[wj * L::XP + xo + a] : T(1);
                 if ((fx >> a) & 1u)
                     y[a] = xin[a];
                 else if (SC)
-                    y[a] *= sr[wj * L::XP + xo + a];
+                    y[a] *= sv[a];
             }
-            epi(gk, y, xin, e);
+            if constexpr (kz_wants_sv<Epi>::value)
+                epi(gk, y, xin, e, sv, fx);
+            else
+                epi(gk, y, xin, e);
+        }
+    }
+    if (!ok) {
+        if (tid == 0) atomicExch(A.err, 1);
+        // the copies this CTA issued must land before it leaves: bounded waits on the stages issued
+        // and not yet seen complete
+        for (int layer = landed + 1; layer <= issued; layer++) kz_wait(bar0 + 8 * slot(layer), parity(layer));
+        return;
+    }
+    epi.finish();
+}
+
+// ---- the pre-scaled variant: the input arrives as s x with the eliminated columns already zero
+// (its producer writes that copy next to x), so a stage holds the input rows, the Dirichlet bits
+// and the material codes only; the corners are read straight from the staged rows (each row at
+// its own 16-byte misalignment) and no layer is converted.  With the conversion gone a step needs
+// one barrier: the bottom corner sums are double- and the top ones triple-buffered, so a step's
+// sums never overwrite those a slower thread still gathers, and a five-slot ring keeps four
+// stages in flight.  The epilogue gets the raw sums y = K (s x) at its node and the node's
+// Dirichlet word, and applies the scale and the Dirichlet rows itself: operator()(node, y, fix, e).
+template <class T, int TX, int TY, int NE>
+struct KzpLayout : KzLayout<T, TX, TY, NE, false> {
+    using B = KzLayout<T, TX, TY, NE, false>;
+    static constexpr int RING = 5;
+    static constexpr int B_OFF = RING * B::STAGE;
+    static constexpr int T_OFF = B_OFF + 2 * 12 * B::THREADS * (int)sizeof(T);
+    static constexpr int L_OFF = T_OFF + 3 * 12 * B::THREADS * (int)sizeof(T);
+    static constexpr int BAR_OFF = kz_round_up(L_OFF + 2 * kKuhnMaxMat * (int)sizeof(T), 16);
+    static constexpr size_t smem = BAR_OFF + 8 * RING;
+};
+
+template <int FORM, bool ISO, class T, int TX, int TY, int MINB, class Epi>
+__global__ void __launch_bounds__(TX* TY, MINB) k_kuhn_zp(KzArgs<T> A, Epi epi)
+{
+    using L = KzpLayout<T, TX, TY, Epi::NE>;
+    if (epi.skip()) return;
+    extern __shared__ __align__(128) unsigned char kz_smem[];
+    const KuhnView<T>& K = A.K;
+    T* Bc = reinterpret_cast<T*>(kz_smem + L::B_OFF);
+    T* Tc = reinterpret_cast<T*>(kz_smem + L::T_OFF);
+    T* slame = reinterpret_cast<T*>(kz_smem + L::L_OFF);
+    const uint32_t bar0 = kz_smem_addr(kz_smem + L::BAR_OFF);
+    const int tid = threadIdx.x;
+    kuhn_stage_lame(K, slame);
+    if (tid == 0) {
+        for (int s = 0; s < L::RING; s++)  // one arrival per warp and stage
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar0 + 8 * s), "r"(L::THREADS / 32));
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
+        asm volatile("fence.proxy.async.shared::cta;\n" ::);
+    }
+    __syncthreads();
+    const int nnx = K.nx + 1, nny = K.ny + 1, nnz = K.nz + 1;
+    const int tile = blockIdx.x % (A.tiles_x * A.tiles_y);
+    const int seg = blockIdx.x / (A.tiles_x * A.tiles_y);
+    const int i0 = (tile % A.tiles_x) * L::OX, j0 = (tile / A.tiles_x) * L::OY;
+    const int k0 = seg * A.seg_len;
+    const int k1 = (k0 + A.seg_len) < nnz ? (k0 + A.seg_len) : nnz;
+    if (k0 >= k1) return;  // whole-CTA exit before any copy
+    const T* ev[Epi::NE > 0 ? Epi::NE : 1] = {};
+    epi.sources(ev);
+    const int first = k0 - 1;  // the first stage (and slab) of the march
+    auto slot = [&](int layer) { return (layer - first) % L::RING; };
+    auto parity = [&](int layer) { return (uint32_t)(((layer - first) / L::RING) & 1); };
+    auto stage_of = [&](int layer) { return kz_smem + slot(layer) * L::STAGE; };
+    const int gi_lo = i0 - 1 < 0 ? 0 : i0 - 1;
+    const int64_t P = (int64_t)nnx * nny;
+    const int Pm4 = (int)(P & 3), P3m = (int)((3 * P) & (L::EL - 1));
+    const int Qm2 = (int)(((int64_t)K.nx * K.ny) & 1);
+    // prologue: stages first .. first+RING-2 in flight
+    const KzCopy cp = kz_copy_of<L>(K, i0, j0);
+    const int64_t Q = (int64_t)K.nx * K.ny;
+    int issued = first - 1;
+    for (int layer = first; layer <= first + L::RING - 2 && layer <= k1; layer++) {
+        kz_issue<L>(A, cp, P, Q, layer, stage_of(layer), bar0 + 8 * slot(layer));
+        issued = layer;
+    }
+    int landed = first - 1;
+    bool ok = kz_wait(bar0 + 8 * slot(first), parity(first));
+    const int ci = tid % TX, cj = tid / TX;
+    const int gci = i0 - 1 + ci, gcj = j0 - 1 + cj;
+    const bool col_ok = gci >= 0 && gci < K.nx && gcj >= 0 && gcj < K.ny;
+    const int mrow = gi_lo + K.nx * gcj;  // hexahedron row start at layer 0 (when col_ok)
+    // staged input rows cj, cj + 1 of this thread's hexahedron: row start at layer 0 and the
+    // element of its first corner column
+    const int r0b = gi_lo + nnx * gcj, r0t = r0b + nnx;
+    const int cx = 3 * (gci - gi_lo);
+    // the node this thread completes: (ni, nj) = (ci, cj) when both are below the owned extent
+    const int gi = i0 + ci, gj = j0 + cj;
+    const bool own = ci < L::OX && cj < L::OY && gi < nnx && gj < nny;
+    const int64_t g0 = gi + (int64_t)nnx * gj;
+    const int wrow = gi_lo + nnx * gj;
+    for (int kz = first; kz < k1; kz++) {
+        // stage kz+1 (the slab's top layer)
+        ok = kz_wait(bar0 + 8 * slot(kz + 1), parity(kz + 1)) && ok;
+        // the epilogue's per-node vectors, loaded now so the loads overlap the hexahedron
+        T e[Epi::NE > 0 ? Epi::NE : 1][3];
+        const int64_t gk = g0 + P * kz;
+        if (kz >= k0 && own) {
+#pragma unroll
+            for (int q = 0; q < Epi::NE; q++)
+#pragma unroll
+                for (int a = 0; a < 3; a++) e[q][a] = __ldg(ev[q] + 3 * gk + a);
+        }
+        // slab kz: this thread's hexahedron
+        {
+            T f[8][3];
+#pragma unroll
+            for (int b = 0; b < 8; b++) f[b][0] = f[b][1] = f[b][2] = T(0);
+            if (ok && col_ok && kz >= 0 && kz < K.nz) {
+                const unsigned char* stb = stage_of(kz);
+                const T* xb = reinterpret_cast<const T*>(stb + L::X_OFF);
+                const T* xt = reinterpret_cast<const T*>(stage_of(kz + 1) + L::X_OFF);
+                // corner b at row cj + ((b >> 1) & 1) of layer kz + (b >> 2)
+                const int o[4] = {cj * L::XP + ((3 * r0b + P3m * kz) & (L::EL - 1)) + cx,
+                                  (cj + 1) * L::XP + ((3 * r0t + P3m * kz) & (L::EL - 1)) + cx,
+                                  cj * L::XP + ((3 * r0b + P3m * (kz + 1)) & (L::EL - 1)) + cx,
+                                  (cj + 1) * L::XP + ((3 * r0t + P3m * (kz + 1)) & (L::EL - 1)) + cx};
+                T u[8][3];
+#pragma unroll
+                for (int b = 0; b < 8; b++) {
+                    const T* src = (b & 4) ? xt : xb;
+                    const int w = o[b >> 1] + 3 * (b & 1);
+#pragma unroll
+                    for (int a = 0; a < 3; a++) u[b][a] = src[w + a];
+                }
+                const uint2* mr = reinterpret_cast<const uint2*>(stb + L::M_OFF);
+                const uint2 mc = mr[cj * L::MP + ((mrow + Qm2 * kz) & 1) + (gci - gi_lo)];
+                T lam[6], mu[6];
+#pragma unroll
+                for (int t = 0; t < 6; t++) {
+                    const int m = ((t < 4 ? mc.x >> (8 * t) : mc.y >> (8 * (t - 4)))) & 0xff;
+                    lam[t] = slame[2 * m];
+                    mu[t] = slame[2 * m + 1];
+                }
+                if (ISO) {
+                    kuhn_tet_iso<FORM, 0, 1, 2>(u[0], u[1], u[3], u[7], lam[0], mu[0], f[0], f[1], f[3], f[7]);
+                    kuhn_tet_iso<FORM, 0, 2, 1>(u[0], u[1], u[5], u[7], lam[1], mu[1], f[0], f[1], f[5], f[7]);
+                    kuhn_tet_iso<FORM, 1, 0, 2>(u[0], u[2], u[3], u[7], lam[2], mu[2], f[0], f[2], f[3], f[7]);
+                    kuhn_tet_iso<FORM, 1, 2, 0>(u[0], u[2], u[6], u[7], lam[3], mu[3], f[0], f[2], f[6], f[7]);
+                    kuhn_tet_iso<FORM, 2, 0, 1>(u[0], u[4], u[5], u[7], lam[4], mu[4], f[0], f[4], f[5], f[7]);
+                    kuhn_tet_iso<FORM, 2, 1, 0>(u[0], u[4], u[6], u[7], lam[5], mu[5], f[0], f[4], f[6], f[7]);
+                } else {
+                    kuhn_tet<FORM, 0, 1, 2>(u[0], u[1], u[3], u[7], lam[0], mu[0], K.ih, K.vh, f[0], f[1], f[3], f[7]);
+                    kuhn_tet<FORM, 0, 2, 1>(u[0], u[1], u[5], u[7], lam[1], mu[1], K.ih, K.vh, f[0], f[1], f[5], f[7]);
+                    kuhn_tet<FORM, 1, 0, 2>(u[0], u[2], u[3], u[7], lam[2], mu[2], K.ih, K.vh, f[0], f[2], f[3], f[7]);
+                    kuhn_tet<FORM, 1, 2, 0>(u[0], u[2], u[6], u[7], lam[3], mu[3], K.ih, K.vh, f[0], f[2], f[6], f[7]);
+                    kuhn_tet<FORM, 2, 0, 1>(u[0], u[4], u[5], u[7], lam[4], mu[4], K.ih, K.vh, f[0], f[4], f[5], f[7]);
+                    kuhn_tet<FORM, 2, 1, 0>(u[0], u[4], u[6], u[7], lam[5], mu[5], K.ih, K.vh, f[0], f[4], f[6], f[7]);
+                }
+            }
+            T* bc = Bc + ((kz - first) & 1) * 12 * L::THREADS;
+            T* tc = Tc + ((kz - first) % 3) * 12 * L::THREADS;
+#pragma unroll
+            for (int b = 0; b < 4; b++)
+#pragma unroll
+                for (int a = 0; a < 3; a++) {
+                    bc[(3 * b + a) * L::THREADS + tid] = f[b][a];
+                    tc[(3 * b + a) * L::THREADS + tid] = f[b + 4][a];
+                }
+        }
+        // the sums are complete; every thread is past step kz-1, so stage kz-1's slot is free
+        ok = __syncthreads_and(ok);
+        if (!ok) break;
+        landed = kz + 1;
+        if (kz + L::RING - 1 <= k1) {
+            kz_issue<L>(A, cp, P, Q, kz + L::RING - 1, stage_of(kz + L::RING - 1), bar0 + 8 * slot(kz + L::RING - 1));
+            issued = kz + L::RING - 1;
+        }
+        // node layer kz: bottom corners of slab kz, then top corners of slab kz-1
+        if (kz >= k0 && own) {
+            const T* bp = Bc + ((kz - first) & 1) * 12 * L::THREADS;
+            const T* tp = Tc + ((kz - 1 - first) % 3) * 12 * L::THREADS;
+            T y[3] = {T(0), T(0), T(0)};
+#pragma unroll
+            for (int b = 0; b < 8; b++) {
+                const int c = tid + (1 - ((b >> 1) & 1)) * TX + 1 - (b & 1);
+                const T* src = (b & 4) ? tp : bp;
+                const int k = 3 * (b & 3);
+#pragma unroll
+                for (int a = 0; a < 3; a++) y[a] += src[(k + a) * L::THREADS + c];
+            }
+            const uint32_t* fr = reinterpret_cast<const uint32_t*>(stage_of(kz) + L::F_OFF);
+            const uint32_t fx = fr[(cj + 1) * L::FP + ((wrow + Pm4 * kz) & 3) + (gi - gi_lo)];
+            epi(gk, y, fx, e);
         }
     }
     if (!ok) {

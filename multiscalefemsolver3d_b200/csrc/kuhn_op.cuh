@@ -79,6 +79,73 @@ struct KzKernel {
     }
 };
 
+// the pre-scaled z-marching kernel (k_kuhn_zp): x = s u with the eliminated columns zero, staged as
+// it is; the grid and segment choice as KzKernel's
+template <int FORM, class T, int TX, int TY, int MINB, class Epi>
+struct KzpKernel {
+    using L = KzpLayout<T, TX, TY, Epi::NE>;
+    static constexpr auto kernel_iso = k_kuhn_zp<FORM, true, T, TX, TY, MINB, Epi>;
+    static constexpr auto kernel_aniso = k_kuhn_zp<FORM, false, T, TX, TY, MINB, Epi>;
+    inline static int blocks_per_sm = 0;
+    inline static uint64_t prepared = 0;
+    static cudaError_t prepare()
+    {
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        const uint64_t bit = 1ull << (dev & 63);
+        if (prepared & bit) return cudaSuccess;
+        e = cudaFuncSetAttribute(kernel_iso, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::smem);
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(kernel_aniso, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::smem);
+        if (e != cudaSuccess) return e;
+        int nb = 0, nb2 = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel_iso, L::THREADS, L::smem);
+        if (e != cudaSuccess) return e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb2, kernel_aniso, L::THREADS, L::smem);
+        if (e != cudaSuccess) return e;
+        blocks_per_sm = std::max(std::min(nb, nb2), 1);
+        prepared |= bit;
+        return cudaSuccess;
+    }
+    // 16-byte-aligned sources with 16 bytes of slack, as KzKernel
+    static bool aligned(const void* p) { return ((uintptr_t)p & 15) == 0; }
+    static cudaError_t launch(const KuhnView<T>& K, const T* x, const Epi& epi, int sms, int* err, cudaStream_t st)
+    {
+        cudaError_t e = prepare();
+        if (e != cudaSuccess) return e;
+        const T* ev[Epi::NE > 0 ? Epi::NE : 1] = {};
+        epi.sources(ev);
+        bool ok = aligned(x) && aligned(K.fix) && aligned(K.mat);
+        for (int q = 0; q < Epi::NE; q++) ok = ok && ev[q];
+        if (!ok) return cudaErrorMisalignedAddress;
+        KzArgs<T> A;
+        A.K = K;
+        A.x = x;
+        A.err = err;
+        A.tiles_x = (K.nx + 1 + L::OX - 1) / L::OX;
+        A.tiles_y = (K.ny + 1 + L::OY - 1) / L::OY;
+        const int nnz = K.nz + 1, tiles = A.tiles_x * A.tiles_y;
+        const int64_t slots = (int64_t)blocks_per_sm * sms;
+        int64_t best = -1;
+        for (int n_seg = 1; n_seg <= nnz; n_seg++) {
+            const int len = (nnz + n_seg - 1) / n_seg;
+            const int segs = (nnz + len - 1) / len;
+            const int64_t cost = ((int64_t)tiles * segs + slots - 1) / slots * (len + 1);
+            if (best < 0 || cost < best) {
+                best = cost;
+                A.seg_len = len;
+                A.n_seg = segs;
+            }
+        }
+        if (K.iso)
+            kernel_iso<<<tiles * A.n_seg, L::THREADS, L::smem, st>>>(A, epi);
+        else
+            kernel_aniso<<<tiles * A.n_seg, L::THREADS, L::smem, st>>>(A, epi);
+        return cudaGetLastError();
+    }
+};
+
 // one matrix-free operator, checked against the assembled matrix of `sys` at values_version
 struct KuhnOperator {
     System* sys = nullptr;

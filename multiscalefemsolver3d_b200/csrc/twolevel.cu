@@ -870,12 +870,15 @@ struct ChebCoef {
 };
 
 // entry of the cycle: r_new = z - (alfa / beta) r2 (lanczos; else r_new = z), written over `out`;
-// rhat = S_t r_new; res = rhat; d = rhat / theta; x = d
+// rhat = S_t r_new; res = rhat; d = rhat / theta; x = d; and, for the matrix-free smoother (dh
+// non-null), dh = s d with the eliminated columns zero (s32: the operator's FP32 Jacobi scale,
+// fixw: its Dirichlet words, bit 3 + c of node i / 3 for component c)
 __global__ void __launch_bounds__(kVecThreads) k_mg_in(int n, const double* __restrict__ z, const double* __restrict__ r2,
                                                       double* __restrict__ out, const double* __restrict__ st,
                                                       float* __restrict__ rhat, float* __restrict__ res,
                                                       float* __restrict__ d, float* __restrict__ x, ChebCoef cc,
-                                                      const TlState* S, int lanczos)
+                                                      const TlState* S, int lanczos, const float* __restrict__ s32,
+                                                      const uint32_t* __restrict__ fixw, float* __restrict__ dh)
 {
     if (S->done) return;
     const double coef = lanczos ? S->alfa / S->beta : 0.0;
@@ -891,6 +894,7 @@ __global__ void __launch_bounds__(kVecThreads) k_mg_in(int n, const double* __re
         const float di = rh * cc.inv_theta;
         d[i] = di;
         x[i] = di;
+        if (dh) dh[i] = ((fixw[i / 3] >> (3 + i % 3)) & 1u) ? 0.0f : s32[i] * di;
     }
 }
 
@@ -993,11 +997,17 @@ struct EpiMinresZ {
 
 // the smoothing kernels' epilogues on the z-marching kernel (kuhn25.cuh), whose per-node inputs
 // arrive staged: xin = the product's input at the node, e[q] = the staged vectors of sources()
-struct EpiChebZ {
-    static constexpr int NE = 2;  // res, x
+// one Chebyshev step on the pre-scaled z-marching kernel (k_kuhn_zp), whose input is dh = s d with
+// the eliminated columns zero: y = K dh at the node; the Dirichlet rows take d itself, the others
+// s y; then res -= y, d = a d + b res, x += d, and dh = s d (masked) for the next step
+struct EpiChebP {
+    static constexpr int NE = 4;  // res, x, the previous d, the Jacobi scale
     float* __restrict__ d;
+    float* __restrict__ dh;
     float* __restrict__ res;
     float* __restrict__ x;
+    const float* __restrict__ dprev;
+    const float* __restrict__ scale;
     float a, b;
     const TlState* S;
     __device__ __forceinline__ bool skip() const { return S->done; }
@@ -1005,17 +1015,22 @@ struct EpiChebZ {
     {
         ev[0] = res;
         ev[1] = x;
+        ev[2] = dprev;
+        ev[3] = scale;
     }
-    __device__ __forceinline__ void operator()(int64_t g, const float* y, const float* dprev, const float (*e)[3])
+    __device__ __forceinline__ void operator()(int64_t g, const float* y, uint32_t fx, const float (*e)[3])
     {
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             const int64_t i = 3 * g + c;
-            const float ri = e[0][c] - y[c];
+            const float dp = e[2][c], sc = e[3][c];
+            const float yc = ((fx >> c) & 1u) ? dp : y[c] * sc;
+            const float ri = e[0][c] - yc;
             res[i] = ri;
-            const float di = a * dprev[c] + b * ri;
+            const float di = a * dp + b * ri;
             d[i] = di;
             x[i] = e[1][c] + di;
+            dh[i] = ((fx >> (3 + c)) & 1u) ? 0.0f : sc * di;
         }
     }
     __device__ __forceinline__ void finish() {}
@@ -1023,16 +1038,19 @@ struct EpiChebZ {
 
 struct EpiResidZ {
     static constexpr int NE = 1;  // rhat
+    static constexpr bool WANTS_SV = true;
     const float* __restrict__ rhat;
     float* __restrict__ res;
     float* __restrict__ d;
+    float* __restrict__ dh;  // start: also s d with the eliminated columns zero (the next input)
     float* __restrict__ x2;
     float inv_theta;
     const TlState* S;
     int start;
     __device__ __forceinline__ bool skip() const { return S->done; }
     __host__ __device__ __forceinline__ void sources(const float** ev) const { ev[0] = rhat; }
-    __device__ __forceinline__ void operator()(int64_t g, const float* y, const float* xin, const float (*e)[3])
+    __device__ __forceinline__ void operator()(int64_t g, const float* y, const float* xin, const float (*e)[3],
+                                               const float* sv, uint32_t fx)
     {
 #pragma unroll
         for (int c = 0; c < 3; c++) {
@@ -1042,6 +1060,7 @@ struct EpiResidZ {
             if (start) {
                 const float di = ri * inv_theta;
                 d[i] = di;
+                dh[i] = ((fx >> (3 + c)) & 1u) ? 0.0f : sv[c] * di;
                 x2[i] = xin[c] + di;
             }
         }
@@ -1049,7 +1068,7 @@ struct EpiResidZ {
     __device__ __forceinline__ void finish() {}
 };
 
-using KCheb = KzKernel<2, true, float, kKzTX, kKzTY, kKzMinB, EpiChebZ>;
+using KChebP = KzpKernel<2, float, kKzTX, kKzTY, kKzMinB, EpiChebP>;
 using KResid = KzKernel<2, true, float, kKzTX, kKzTY, kKzMinB, EpiResidZ>;
 using KMinres = KzKernel<1, false, double, kKzTX, kKzTY, kKzMinB64, EpiMinresZ>;
 
@@ -1181,7 +1200,7 @@ struct CoarseHandle {
     DBuf<double> rtmp, rr_true;  // the inner solve's true-residual check: A x, ||r - A x||^2
     DBuf<unsigned int> tk;       // its reduction ticket
     DBuf<float> psi_t, mgv;
-    int64_t ldv = 0;            // stride of the cycle's six FP32 vectors in mgv (16-byte aligned, with slack)
+    int64_t ldv = 0;            // stride of the cycle's eight FP32 vectors in mgv (16-byte aligned, with slack)
     DBuf<__half2> val16;  // FP16 copy of the textbook system's scaled SELL values, paired (when requested)
     DBuf<int16_t> col16;  // its block columns as 16-bit deltas (empty when some delta does not fit)
     bool half_matrix = false;
@@ -1577,6 +1596,8 @@ void mg_cycle(CoarseHandle& C, const double* z, const double* r2, double* r_out,
     float* dB = dA + ld;
     float* x = dB + ld;
     float* x2 = x + ld;
+    float* dhA = x2 + ld;  // matrix-free: s d with the eliminated columns zero, the next step's input
+    float* dhB = dhA + ld;
     TlState* S = C.st.p;
     const SellView<float> At = sell_view<float>(T);
     const unsigned gsp = spmv_grid_of((const void*)k_mg_cheb, T);
@@ -1588,21 +1609,25 @@ void mg_cycle(CoarseHandle& C, const double* z, const double* r2, double* r_out,
     const KuhnView<float>& Kv = C.kt.v32;
     const int sms = C.kt.sms;
     int* kerr = C.kt.err.p;
-    auto cheb = [&](float* dprev, float* dnew, float* xx, int i) {
+    float* d[2] = {dA, dB};
+    float* dh[2] = {dhA, dhB};
+    auto cheb = [&](int i, float* xx) {
+        float *dprev = d[(i - 1) & 1], *dnew = d[i & 1];
         if (mf)
-            KCheb::launch(Kv, dprev, EpiChebZ{dnew, res, xx, C.cc.a[i], C.cc.b[i], S}, sms, kerr, st);
+            KChebP::launch(Kv, dh[(i - 1) & 1],
+                           EpiChebP{dnew, dh[i & 1], res, xx, dprev, Kv.scale, C.cc.a[i], C.cc.b[i], S}, sms, kerr, st);
         else
             k_mg_cheb<<<gsp, 256, 0, st>>>(At, v16, c16, dprev, dnew, res, xx, C.cc.a[i], C.cc.b[i], S);
     };
     auto resid = [&](float* d0, float* x2, float inv_theta, int start) {
         if (mf)
-            KResid::launch(Kv, x, EpiResidZ{rhat, res, d0, x2, inv_theta, S, start}, sms, kerr, st);
+            KResid::launch(Kv, x, EpiResidZ{rhat, res, d0, dhA, x2, inv_theta, S, start}, sms, kerr, st);
         else
             k_mg_resid<<<gsp, 256, 0, st>>>(At, v16, c16, rhat, x, res, d0, x2, inv_theta, S, start);
     };
-    k_mg_in<<<gvec, kVecThreads, 0, st>>>(n, z, r2, r_out, s_t, rhat, res, dA, x, C.cc, S, lanczos);
-    float* d[2] = {dA, dB};
-    for (int i = 1; i < C.cheb_deg; i++) cheb(d[(i - 1) & 1], d[i & 1], x, i);
+    k_mg_in<<<gvec, kVecThreads, 0, st>>>(n, z, r2, r_out, s_t, rhat, res, dA, x, C.cc, S, lanczos, Kv.scale, Kv.fix,
+                                          mf ? dhA : nullptr);
+    for (int i = 1; i < C.cheb_deg; i++) cheb(i, x);
     resid(nullptr, nullptr, 0.0f, 0);
     k_tl_restrict<float><<<C.n_cells, 128, 0, st>>>(C.own_ptr.p, C.own.p, C.psi_t.p, res, nullptr, nullptr, C.cpart.p,
                                                     nullptr, S, 0);
@@ -1610,7 +1635,7 @@ void mg_cycle(CoarseHandle& C, const double* z, const double* r2, double* r_out,
     coarse_solve(C, S, st);
     k_mg_prolong<<<gvec, kVecThreads, 0, st>>>(C.n_fine, C.owner.p, C.cdof.p, C.psi_t.p, C.ec.p, x, S);
     resid(dA, x2, C.cc.inv_theta, 1);
-    for (int i = 1; i < C.cheb_deg; i++) cheb(d[(i - 1) & 1], d[i & 1], x2, i);
+    for (int i = 1; i < C.cheb_deg; i++) cheb(i, x2);
     k_mg_out<<<gvec, kVecThreads, 0, st>>>(n, x2, s_t, lanczos ? r_out : z, y, S, C.partial.p, init);
 }
 
@@ -1781,7 +1806,7 @@ int set_smoother(CoarseHandle& C, System& T, int degree, double ratio, int stora
     MSFEM_TRY(C.psi_t.alloc(24 * (size_t)C.n_fine));
     k_mg_psi<<<gridn(24 * (int64_t)C.n_fine), 256, 0, st>>>(C.n_fine, C.psi_hat.p, F.dscale.p, T.dscale.p, C.psi_t.p);
     C.ldv = (n + 16 + 63) / 64 * 64;  // 16-byte aligned sub-vectors with 16 elements of slack
-    MSFEM_TRY(C.mgv.alloc(6 * (size_t)C.ldv));
+    MSFEM_TRY(C.mgv.alloc(8 * (size_t)C.ldv));
     // power iteration from a fixed pseudo-random start
     std::vector<float> h0(n);
     for (int i = 0; i < n; i++) h0[i] = (float)((hash32((unsigned)i) & 0xffff) / 65536.0 - 0.5);
@@ -1821,7 +1846,7 @@ int set_smoother(CoarseHandle& C, System& T, int degree, double ratio, int stora
     if (storage == 2) {
         C.text = nullptr;  // usable only once the matrix-free operator passed its check
         MSFEM_TRY(kuhn_operator_build(T, 2, false, true, C.kt));
-        MSFEM_CK(KCheb::prepare());
+        MSFEM_CK(KChebP::prepare());
         MSFEM_CK(KResid::prepare());
         C.text = &T;
     }
@@ -2111,7 +2136,9 @@ int msfem_coarse_bench_smoother(msfem_coarse_t c, int reps, double* ms_per_step,
     float* dA = res + ld;
     float* dB = dA + ld;
     float* x = dB + ld;
-    MSFEM_CK(cudaMemsetAsync(C.mgv.p, 0, sizeof(float) * 6 * (size_t)ld, st));
+    float* dhA = x + 2 * ld;
+    float* dhB = dhA + ld;
+    MSFEM_CK(cudaMemsetAsync(C.mgv.p, 0, sizeof(float) * 8 * (size_t)ld, st));
     DBuf<TlState> run;  // a state that is not done, so the kernel does its work
     MSFEM_TRY(run.alloc(1));
     MSFEM_CK(cudaMemsetAsync(run.p, 0, sizeof(TlState), st));
@@ -2125,7 +2152,9 @@ int msfem_coarse_bench_smoother(msfem_coarse_t c, int reps, double* ms_per_step,
         float* dp = (i & 1) ? dB : dA;
         float* dn = (i & 1) ? dA : dB;
         if (mf)
-            KCheb::launch(C.kt.v32, dp, EpiChebZ{dn, res, x, C.cc.a[1], C.cc.b[1], run.p}, C.kt.sms, C.kt.err.p, st);
+            KChebP::launch(C.kt.v32, (i & 1) ? dhB : dhA,
+                           EpiChebP{dn, (i & 1) ? dhA : dhB, res, x, dp, C.kt.v32.scale, C.cc.a[1], C.cc.b[1], run.p},
+                           C.kt.sms, C.kt.err.p, st);
         else
             k_mg_cheb<<<gsp, 256, 0, st>>>(At, v16, c16, dp, dn, res, x, C.cc.a[1], C.cc.b[1], run.p);
     };
@@ -2145,10 +2174,11 @@ int msfem_coarse_bench_smoother(msfem_coarse_t c, int reps, double* ms_per_step,
     *ms_per_step = ms / reps;
     // matrix values (FP16 pairs: 5 x 4 B per block, FP32: 36 B) and block columns, each once;
     // slice pointers; per DOF the previous direction (4 B), res read and written (8 B), the new
-    // direction (4 B), x read and written (8 B).  Matrix-free: per DOF the Jacobi scale (4 B)
-    // instead of the matrix, per node its Dirichlet bits (4 B), per tetrahedron its material (1 B)
+    // direction (4 B), x read and written (8 B).  Matrix-free: instead of the matrix, per DOF the
+    // Jacobi scale (4 B) and the scaled input read and the next one written (8 B), per node its
+    // Dirichlet bits (4 B), per tetrahedron its material (1 B)
     if (mf) {
-        *bytes_per_step = (int64_t)n * (24 + 4) + (int64_t)T.n_nodes * 4 + (int64_t)T.n_tets;
+        *bytes_per_step = (int64_t)n * (24 + 12) + (int64_t)T.n_nodes * 4 + (int64_t)T.n_tets;
     } else {
         const int64_t vb = C.half_matrix ? 20 : 36;
         const int64_t cb = c16 ? 2 : 4;
