@@ -1091,8 +1091,8 @@ def run_twolevel(args, D):
                 "gpu_launches": int(launches),
                 "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                              "traffic": read_traffic("kuhn_cheb_elastic_128.md" if MF else "cheb_smoother_elastic_128.md"),
-                             "kernel": ("k_kuhn_z<EpiChebZ> (Chebyshev step of the smoother: matrix-free textbook "
-                                        "operator on the Kuhn grid + vector update)" if MF else
+                             "kernel": ("k_kuhn_zp<EpiChebP> (Chebyshev step of the smoother: matrix-free textbook "
+                                        "operator on the Kuhn grid from the pre-scaled input + vector update)" if MF else
                                         "k_mg_cheb (Chebyshev step of the smoother: FP16 3x3-block SELL SpMV of the "
                                         "textbook operator + vector update)"),
                              "ms_per_launch": cheb_ms, "bytes_per_launch": cheb_bytes,

@@ -22,7 +22,6 @@
 #pragma once
 
 #include <cstdint>
-#include <type_traits>
 
 #include "kuhn.cuh"
 
@@ -188,13 +187,6 @@ __device__ __forceinline__ void kz_issue(const KzArgs<T>& A, const KzCopy& c, in
     __syncwarp();
     if (bytes) kz_bulk(kz_smem_addr(stage + c.dst), src, bytes, bar);
 }
-
-// an epilogue with `static constexpr bool WANTS_SV = true` also gets the node's Jacobi scale (1
-// without one) and its Dirichlet word: operator()(node, y, xin, e, s[3], fix)
-template <class E, class = void>
-struct kz_wants_sv : std::false_type {};
-template <class E>
-struct kz_wants_sv<E, std::void_t<decltype(E::WANTS_SV)>> : std::bool_constant<E::WANTS_SV> {};
 
 // the z-marching product; Epi: NE per-node input vectors (sources(ev)), skip(), finish(),
 // operator()(node, y[3], input x[3], e[NE][3] = those vectors at the node)
@@ -380,20 +372,16 @@ __global__ void __launch_bounds__(TX* TY, MINB) k_kuhn_z(KzArgs<T> A, Epi epi)
             const int wj = cj + 1;
             const int xo = ((3 * wrow + P3m * kz) & (L::EL - 1)) + 3 * (gi - gi_lo);
             const uint32_t fx = fr[wj * L::FP + ((wrow + Pm4 * kz) & 3) + (gi - gi_lo)];
-            T xin[3], sv[3];
+            T xin[3];
 #pragma unroll
             for (int a = 0; a < 3; a++) {
                 xin[a] = xr[wj * L::XP + xo + a];
-                sv[a] = SC ? sr[wj * L::XP + xo + a] : T(1);
                 if ((fx >> a) & 1u)
                     y[a] = xin[a];
                 else if (SC)
-                    y[a] *= sv[a];
+                    y[a] *= sr[wj * L::XP + xo + a];
             }
-            if constexpr (kz_wants_sv<Epi>::value)
-                epi(gk, y, xin, e, sv, fx);
-            else
-                epi(gk, y, xin, e);
+            epi(gk, y, xin, e);
         }
     }
     if (!ok) {

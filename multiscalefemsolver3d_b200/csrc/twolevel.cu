@@ -1010,6 +1010,7 @@ struct EpiChebP {
     const float* __restrict__ scale;
     float a, b;
     const TlState* S;
+    float* __restrict__ xh;  // non-null (the last step before a residual): also s x, masked
     __device__ __forceinline__ bool skip() const { return S->done; }
     __host__ __device__ __forceinline__ void sources(const float** ev) const
     {
@@ -1029,39 +1030,51 @@ struct EpiChebP {
             res[i] = ri;
             const float di = a * dp + b * ri;
             d[i] = di;
-            x[i] = e[1][c] + di;
-            dh[i] = ((fx >> (3 + c)) & 1u) ? 0.0f : sc * di;
+            const float xi = e[1][c] + di;
+            x[i] = xi;
+            const bool col = (fx >> (3 + c)) & 1u;
+            dh[i] = col ? 0.0f : sc * di;
+            if (xh) xh[i] = col ? 0.0f : sc * xi;
         }
     }
     __device__ __forceinline__ void finish() {}
 };
 
-struct EpiResidZ {
-    static constexpr int NE = 1;  // rhat
-    static constexpr bool WANTS_SV = true;
+// the cycle's residual on the pre-scaled kernel: y = K xh at the node with xh = s x (masked);
+// res = rhat - (x on the Dirichlet rows, s y elsewhere); start (after the coarse correction): also
+// d = res / theta, dh = s d (masked, the next step's input) and x2 = x + d
+struct EpiResidP {
+    static constexpr int NE = 3;  // rhat, x, the Jacobi scale
     const float* __restrict__ rhat;
     float* __restrict__ res;
     float* __restrict__ d;
-    float* __restrict__ dh;  // start: also s d with the eliminated columns zero (the next input)
+    float* __restrict__ dh;
     float* __restrict__ x2;
+    const float* __restrict__ x;
+    const float* __restrict__ scale;
     float inv_theta;
     const TlState* S;
     int start;
     __device__ __forceinline__ bool skip() const { return S->done; }
-    __host__ __device__ __forceinline__ void sources(const float** ev) const { ev[0] = rhat; }
-    __device__ __forceinline__ void operator()(int64_t g, const float* y, const float* xin, const float (*e)[3],
-                                               const float* sv, uint32_t fx)
+    __host__ __device__ __forceinline__ void sources(const float** ev) const
+    {
+        ev[0] = rhat;
+        ev[1] = x;
+        ev[2] = scale;
+    }
+    __device__ __forceinline__ void operator()(int64_t g, const float* y, uint32_t fx, const float (*e)[3])
     {
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             const int64_t i = 3 * g + c;
-            const float ri = e[0][c] - y[c];
+            const float xc = e[1][c], sc = e[2][c];
+            const float ri = e[0][c] - (((fx >> c) & 1u) ? xc : y[c] * sc);
             res[i] = ri;
             if (start) {
                 const float di = ri * inv_theta;
                 d[i] = di;
-                dh[i] = ((fx >> (3 + c)) & 1u) ? 0.0f : sv[c] * di;
-                x2[i] = xin[c] + di;
+                dh[i] = ((fx >> (3 + c)) & 1u) ? 0.0f : sc * di;
+                x2[i] = xc + di;
             }
         }
     }
@@ -1069,14 +1082,17 @@ struct EpiResidZ {
 };
 
 using KChebP = KzpKernel<2, float, kKzTX, kKzTY, kKzMinB, EpiChebP>;
-using KResid = KzKernel<2, true, float, kKzTX, kKzTY, kKzMinB, EpiResidZ>;
+using KResidP = KzpKernel<2, float, kKzTX, kKzTY, kKzMinB, EpiResidP>;
 using KMinres = KzKernel<1, false, double, kKzTX, kKzTY, kKzMinB64, EpiMinresZ>;
 
-// x += P^_t ec
+// x += P^_t ec; with xh non-null also xh = s x with the eliminated columns zero (the next product's
+// input: s32 the operator's FP32 Jacobi scale, fixw its Dirichlet words)
 __global__ void __launch_bounds__(kVecThreads) k_mg_prolong(int n_fine, const int32_t* __restrict__ owner,
                                                            const int32_t* __restrict__ cdof,
                                                            const float* __restrict__ psi, const float* __restrict__ ec,
-                                                           float* __restrict__ x, const TlState* S)
+                                                           float* __restrict__ x, const TlState* S,
+                                                           const float* __restrict__ s32,
+                                                           const uint32_t* __restrict__ fixw, float* __restrict__ xh)
 {
     if (S->done) return;
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n_fine; g += (int64_t)gridDim.x * blockDim.x) {
@@ -1094,8 +1110,13 @@ __global__ void __launch_bounds__(kVecThreads) k_mg_prolong(int n_fine, const in
             for (int t = 0; t < 4; t++)
                 if (dd[t] >= 0) z[(4 * q + t) % 3] += pp[t] * ec[dd[t]];
         }
+        const uint32_t fw = xh ? fixw[g] : 0u;
 #pragma unroll
-        for (int a = 0; a < 3; a++) x[3 * g + a] += z[a];
+        for (int a = 0; a < 3; a++) {
+            const float xa = x[3 * g + a] + z[a];
+            x[3 * g + a] = xa;
+            if (xh) xh[3 * g + a] = ((fw >> (3 + a)) & 1u) ? 0.0f : s32[3 * g + a] * xa;
+        }
     }
 }
 
@@ -1200,7 +1221,7 @@ struct CoarseHandle {
     DBuf<double> rtmp, rr_true;  // the inner solve's true-residual check: A x, ||r - A x||^2
     DBuf<unsigned int> tk;       // its reduction ticket
     DBuf<float> psi_t, mgv;
-    int64_t ldv = 0;            // stride of the cycle's eight FP32 vectors in mgv (16-byte aligned, with slack)
+    int64_t ldv = 0;            // stride of the cycle's nine FP32 vectors in mgv (16-byte aligned, with slack)
     DBuf<__half2> val16;  // FP16 copy of the textbook system's scaled SELL values, paired (when requested)
     DBuf<int16_t> col16;  // its block columns as 16-bit deltas (empty when some delta does not fit)
     bool half_matrix = false;
@@ -1598,6 +1619,7 @@ void mg_cycle(CoarseHandle& C, const double* z, const double* r2, double* r_out,
     float* x2 = x + ld;
     float* dhA = x2 + ld;  // matrix-free: s d with the eliminated columns zero, the next step's input
     float* dhB = dhA + ld;
+    float* xh = dhB + ld;  // matrix-free: s x (masked), the residual products' input
     TlState* S = C.st.p;
     const SellView<float> At = sell_view<float>(T);
     const unsigned gsp = spmv_grid_of((const void*)k_mg_cheb, T);
@@ -1611,31 +1633,35 @@ void mg_cycle(CoarseHandle& C, const double* z, const double* r2, double* r_out,
     int* kerr = C.kt.err.p;
     float* d[2] = {dA, dB};
     float* dh[2] = {dhA, dhB};
-    auto cheb = [&](int i, float* xx) {
+    // the pre-smoothing's last step also writes xh (with degree 1, xh is d_0's own scaled copy)
+    auto cheb = [&](int i, float* xx, float* xhout) {
         float *dprev = d[(i - 1) & 1], *dnew = d[i & 1];
         if (mf)
             KChebP::launch(Kv, dh[(i - 1) & 1],
-                           EpiChebP{dnew, dh[i & 1], res, xx, dprev, Kv.scale, C.cc.a[i], C.cc.b[i], S}, sms, kerr, st);
+                           EpiChebP{dnew, dh[i & 1], res, xx, dprev, Kv.scale, C.cc.a[i], C.cc.b[i], S, xhout}, sms,
+                           kerr, st);
         else
             k_mg_cheb<<<gsp, 256, 0, st>>>(At, v16, c16, dprev, dnew, res, xx, C.cc.a[i], C.cc.b[i], S);
     };
-    auto resid = [&](float* d0, float* x2, float inv_theta, int start) {
+    auto resid = [&](const float* xin_h, float* d0, float* x2, float inv_theta, int start) {
         if (mf)
-            KResid::launch(Kv, x, EpiResidZ{rhat, res, d0, dhA, x2, inv_theta, S, start}, sms, kerr, st);
+            KResidP::launch(Kv, xin_h, EpiResidP{rhat, res, d0, dhA, x2, x, Kv.scale, inv_theta, S, start}, sms, kerr,
+                            st);
         else
             k_mg_resid<<<gsp, 256, 0, st>>>(At, v16, c16, rhat, x, res, d0, x2, inv_theta, S, start);
     };
     k_mg_in<<<gvec, kVecThreads, 0, st>>>(n, z, r2, r_out, s_t, rhat, res, dA, x, C.cc, S, lanczos, Kv.scale, Kv.fix,
                                           mf ? dhA : nullptr);
-    for (int i = 1; i < C.cheb_deg; i++) cheb(i, x);
-    resid(nullptr, nullptr, 0.0f, 0);
+    for (int i = 1; i < C.cheb_deg; i++) cheb(i, x, i == C.cheb_deg - 1 ? xh : nullptr);
+    resid(C.cheb_deg > 1 ? xh : dhA, nullptr, nullptr, 0.0f, 0);
     k_tl_restrict<float><<<C.n_cells, 128, 0, st>>>(C.own_ptr.p, C.own.p, C.psi_t.p, res, nullptr, nullptr, C.cpart.p,
                                                     nullptr, S, 0);
     k_tl_gather<<<gridn(C.n_cf), 256, 0, st>>>(C.n_cf, C.dptr.p, C.dent.p, C.cpart.p, C.rc.p, S);
     coarse_solve(C, S, st);
-    k_mg_prolong<<<gvec, kVecThreads, 0, st>>>(C.n_fine, C.owner.p, C.cdof.p, C.psi_t.p, C.ec.p, x, S);
-    resid(dA, x2, C.cc.inv_theta, 1);
-    for (int i = 1; i < C.cheb_deg; i++) cheb(i, x2);
+    k_mg_prolong<<<gvec, kVecThreads, 0, st>>>(C.n_fine, C.owner.p, C.cdof.p, C.psi_t.p, C.ec.p, x, S, Kv.scale, Kv.fix,
+                                               mf ? xh : nullptr);
+    resid(xh, dA, x2, C.cc.inv_theta, 1);
+    for (int i = 1; i < C.cheb_deg; i++) cheb(i, x2, nullptr);
     k_mg_out<<<gvec, kVecThreads, 0, st>>>(n, x2, s_t, lanczos ? r_out : z, y, S, C.partial.p, init);
 }
 
@@ -1806,7 +1832,7 @@ int set_smoother(CoarseHandle& C, System& T, int degree, double ratio, int stora
     MSFEM_TRY(C.psi_t.alloc(24 * (size_t)C.n_fine));
     k_mg_psi<<<gridn(24 * (int64_t)C.n_fine), 256, 0, st>>>(C.n_fine, C.psi_hat.p, F.dscale.p, T.dscale.p, C.psi_t.p);
     C.ldv = (n + 16 + 63) / 64 * 64;  // 16-byte aligned sub-vectors with 16 elements of slack
-    MSFEM_TRY(C.mgv.alloc(8 * (size_t)C.ldv));
+    MSFEM_TRY(C.mgv.alloc(9 * (size_t)C.ldv));
     // power iteration from a fixed pseudo-random start
     std::vector<float> h0(n);
     for (int i = 0; i < n; i++) h0[i] = (float)((hash32((unsigned)i) & 0xffff) / 65536.0 - 0.5);
@@ -1847,7 +1873,7 @@ int set_smoother(CoarseHandle& C, System& T, int degree, double ratio, int stora
         C.text = nullptr;  // usable only once the matrix-free operator passed its check
         MSFEM_TRY(kuhn_operator_build(T, 2, false, true, C.kt));
         MSFEM_CK(KChebP::prepare());
-        MSFEM_CK(KResid::prepare());
+        MSFEM_CK(KResidP::prepare());
         C.text = &T;
     }
     if (C.half_matrix) {
@@ -2138,7 +2164,7 @@ int msfem_coarse_bench_smoother(msfem_coarse_t c, int reps, double* ms_per_step,
     float* x = dB + ld;
     float* dhA = x + 2 * ld;
     float* dhB = dhA + ld;
-    MSFEM_CK(cudaMemsetAsync(C.mgv.p, 0, sizeof(float) * 8 * (size_t)ld, st));
+    MSFEM_CK(cudaMemsetAsync(C.mgv.p, 0, sizeof(float) * 9 * (size_t)ld, st));
     DBuf<TlState> run;  // a state that is not done, so the kernel does its work
     MSFEM_TRY(run.alloc(1));
     MSFEM_CK(cudaMemsetAsync(run.p, 0, sizeof(TlState), st));
@@ -2153,7 +2179,8 @@ int msfem_coarse_bench_smoother(msfem_coarse_t c, int reps, double* ms_per_step,
         float* dn = (i & 1) ? dA : dB;
         if (mf)
             KChebP::launch(C.kt.v32, (i & 1) ? dhB : dhA,
-                           EpiChebP{dn, (i & 1) ? dhA : dhB, res, x, dp, C.kt.v32.scale, C.cc.a[1], C.cc.b[1], run.p},
+                           EpiChebP{dn, (i & 1) ? dhA : dhB, res, x, dp, C.kt.v32.scale, C.cc.a[1], C.cc.b[1], run.p,
+                                    nullptr},
                            C.kt.sms, C.kt.err.p, st);
         else
             k_mg_cheb<<<gsp, 256, 0, st>>>(At, v16, c16, dp, dn, res, x, C.cc.a[1], C.cc.b[1], run.p);
