@@ -250,6 +250,12 @@ void msfem_release_cached_memory(void);
  * Dirichlet rows -- applied from the tetrahedra's materials; checked against the assembled product
  * on a probe vector first (MSFEM_ERR_STATE if the relative distance exceeds 1e-12). */
 int msfem_kuhn_spmv(msfem_system_t h, const double* x, double* y, int on_device);
+/* y = S A S x in FP32 formed matrix-free on the Kuhn grid (S = diag(1/sqrt|A_ii|), the scaling of
+ * msfem_spmv_scaled32) by the kernel the two-level cycle's smoother runs: the input is first scaled
+ * to s x with the eliminated columns zero, then staged as it is.  At set-up the product is checked
+ * against the assembled FP32 product (relative 1e-5) and against the staged-scale matrix-free
+ * kernel bit for bit (MSFEM_ERR_STATE otherwise).  No reference counterpart. */
+int msfem_kuhn_spmv_scaled32(msfem_system_t h, const float* x, float* y, int on_device);
 
 /* CSR export of the assembled matrix (sizes from msfem_system_info), host or device buffers. */
 int msfem_export_csr(msfem_system_t h, int32_t* row_ptr, int32_t* col, double* val, int on_device);

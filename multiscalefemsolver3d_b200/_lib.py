@@ -80,6 +80,7 @@ _SIGS = [
     ("msfem_set_kuhn_grid", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
     ("msfem_release_cached_memory", None, []),
     ("msfem_kuhn_spmv", C.c_int, [C.c_void_p, _P, _P, C.c_int]),
+    ("msfem_kuhn_spmv_scaled32", C.c_int, [C.c_void_p, _P, _P, C.c_int]),
     ("msfem_export_csr", C.c_int, [C.c_void_p, _P, _P, _P, C.c_int]),
     ("msfem_bench_spmv", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     ("msfem_residual_noalloc", C.c_int, [C.c_int, _P, _P, _P, _P, _P, _P, _P, C.c_void_p]),

@@ -603,6 +603,30 @@ int msfem_kuhn_spmv(msfem_system_t h, const double* x, double* y, int on_device)
     return MSFEM_OK;
 }
 
+int msfem_kuhn_spmv_scaled32(msfem_system_t h, const float* x, float* y, int on_device)
+{
+    (void)on_device;
+    MSFEM_TRY(check_handle(h));
+    System& s = *as_sys(h);
+    MSFEM_TRY(use_device(s));
+    if (!x || !y) {
+        set_error("msfem_kuhn_spmv_scaled32: null vector");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    KuhnOperator op;
+    MSFEM_TRY(kuhn_operator_build(s, s.elastic_form, false, true, op));
+    DBuf<float> dx, dxh, dy;
+    MSFEM_TRY(dx.alloc((size_t)s.n_rows + 16));  // slack for the staging copies
+    MSFEM_TRY(dxh.alloc((size_t)s.n_rows + 16));
+    MSFEM_TRY(dy.alloc((size_t)s.n_rows));
+    MSFEM_CK(cudaMemcpyAsync(dx.p, x, sizeof(float) * s.n_rows, cudaMemcpyDefault, s.stream));
+    MSFEM_TRY(kuhn_spmv32_pre(op, dx.p, dxh.p, dy.p, s.stream));
+    MSFEM_TRY(kuhn_check_err(op, s.stream));
+    MSFEM_CK(cudaMemcpyAsync(y, dy.p, sizeof(float) * s.n_rows, cudaMemcpyDefault, s.stream));
+    MSFEM_CK(cudaStreamSynchronize(s.stream));
+    return MSFEM_OK;
+}
+
 int msfem_export_csr(msfem_system_t h, int32_t* row_ptr, int32_t* col, double* val, int on_device)
 {
     (void)on_device;

@@ -346,26 +346,20 @@ int kuhn_operator_build(System& s, int form, bool fp64, bool scaled, KuhnOperato
                       "%.3g in max); the values are not the Kuhn grid's elasticity operator", rl2, rmax);
             return MSFEM_ERR_STATE;
         }
-        if (form == 2) {
-            // the pre-scaled kernel the smoother steps run: the same product, bit for bit
-            DBuf<float> xh;
-            MSFEM_TRY(xh.alloc(n + 16));
-            k_kuhn_prescale<<<148 * 4, 256, 0, st>>>(n, x.p, op.scale32.p, op.v32.fix, xh.p);
-            const cudaError_t e = KzpKernel<2, float, kKzTX, kKzTY, kKzMinB, EpiStoreP>::launch(
-                op.v32, xh.p, EpiStoreP{y2.p, x.p, op.scale32.p}, op.sms, op.err.p, st);
-            if (e != cudaSuccess) {
-                set_error("matrix-free FP32 product (pre-scaled input): %s", cudaGetErrorString(e));
-                return MSFEM_ERR_CUDA;
-            }
-            MSFEM_TRY(kuhn_check_err(op, st));
-            double pl2 = 0.0, pmax = 0.0;
-            MSFEM_TRY(compare<float>(st, n, y2.p, y1.p, &pl2, &pmax));
-            if (pmax != 0.0) {
-                set_error("matrix-free operator: the pre-scaled kernel's product differs from the staged-scale "
-                          "kernel's (relative %.3g in max)", pmax);
-                return MSFEM_ERR_STATE;
-            }
-            s.total_launches += 2;
+        // the pre-scaled kernel the smoother steps run: the same product, bit for bit
+        DBuf<float> xh;
+        MSFEM_TRY(xh.alloc(n + 16));
+        op.sys = &s;  // for the pre-scaled product below; cleared again if the check fails
+        const int rc = kuhn_spmv32_pre(op, x.p, xh.p, y2.p, st);
+        op.sys = nullptr;
+        MSFEM_TRY(rc);
+        MSFEM_TRY(kuhn_check_err(op, st));
+        double pl2 = 0.0, pmax = 0.0;
+        MSFEM_TRY(compare<float>(st, n, y2.p, y1.p, &pl2, &pmax));
+        if (pmax != 0.0) {
+            set_error("matrix-free operator: the pre-scaled kernel's product differs from the staged-scale "
+                      "kernel's (relative %.3g in max)", pmax);
+            return MSFEM_ERR_STATE;
         }
     }
     op.check_l2 = rl2;
@@ -413,6 +407,28 @@ int kuhn_spmv32(KuhnOperator& op, const float* x, float* y, cudaStream_t st)
         set_error("matrix-free FP32 product: %s", cudaGetErrorString(err));
         return MSFEM_ERR_CUDA;
     }
+    return MSFEM_OK;
+}
+
+int kuhn_spmv32_pre(KuhnOperator& op, const float* x, float* xh, float* y, cudaStream_t st)
+{
+    if (!op.scaled || op.fp64) {
+        set_error("matrix-free FP32 product (pre-scaled input): the operator is not the Jacobi-scaled FP32 one");
+        return MSFEM_ERR_ARGUMENT;
+    }
+    const int64_t n = op.sys ? op.sys->n_rows : 0;
+    k_kuhn_prescale<<<148 * 4, 256, 0, st>>>(n, x, op.scale32.p, op.v32.fix, xh);
+    const EpiStoreP e{y, x, op.scale32.p};
+    cudaError_t err = op.form == 2
+                          ? KzpKernel<2, float, kKzTX, kKzTY, kKzMinB, EpiStoreP>::launch(op.v32, xh, e, op.sms,
+                                                                                           op.err.p, st)
+                          : KzpKernel<1, float, kKzTX, kKzTY, kKzMinB, EpiStoreP>::launch(op.v32, xh, e, op.sms,
+                                                                                           op.err.p, st);
+    if (err != cudaSuccess) {
+        set_error("matrix-free FP32 product (pre-scaled input): %s", cudaGetErrorString(err));
+        return MSFEM_ERR_CUDA;
+    }
+    if (op.sys) op.sys->total_launches += 2;
     return MSFEM_OK;
 }
 

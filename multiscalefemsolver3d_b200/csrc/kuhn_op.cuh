@@ -167,6 +167,9 @@ int kuhn_operator_build(System& s, int form, bool fp64, bool scaled, KuhnOperato
 int kuhn_operator_current(const KuhnOperator& op);
 int kuhn_spmv64(KuhnOperator& op, const double* x, double* y, cudaStream_t st);
 int kuhn_spmv32(KuhnOperator& op, const float* x, float* y, cudaStream_t st);
+// y = S K S x through the pre-scaled kernel (k_kuhn_zp): xh (n + 16 elements, scratch) receives
+// s x with the eliminated columns zero first; op.sys set
+int kuhn_spmv32_pre(KuhnOperator& op, const float* x, float* xh, float* y, cudaStream_t st);
 // MSFEM_ERR_CUDA (and the flag cleared) if a z-marching launch on op raised its staging error
 int kuhn_check_err(KuhnOperator& op, cudaStream_t st);
 

@@ -288,6 +288,15 @@ class System:
               "kuhn_spmv")
         return y
 
+    def kuhn_spmv_scaled32(self, x):
+        """y = S A S x in FP32 formed matrix-free on the Kuhn grid by the smoother's kernel (input
+        scaled and masked first); S as spmv_scaled32's."""
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.empty(self.n_rows, dtype=np.float32)
+        check(load().msfem_kuhn_spmv_scaled32(self.h, x.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p), 0),
+              "kuhn_spmv_scaled32")
+        return y
+
     def export_csr(self) -> Csr:
         rp = np.empty(self.n_rows + 1, dtype=np.int32)
         col = np.empty(self.nnz, dtype=np.int32)

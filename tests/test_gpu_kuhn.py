@@ -151,6 +151,24 @@ def test_values_must_be_one_assembly(cuda):
         np.testing.assert_array_equal(S.kuhn_spmv(x), y1)   # deterministic
 
 
+@pytest.mark.parametrize("case", list(CASES))
+@pytest.mark.parametrize("textbook", [False, True], ids=["reference", "textbook"])
+def test_scaled_fp32_product_on_pre_scaled_input(cuda, case, textbook):
+    """The smoother's kernel (input s x with the eliminated columns zero, staged as it is) on cubes
+    and anisotropic boxes, both orientations: S A S x equals the assembled FP32 product at the FP32
+    bar, and its set-up check compared it bit for bit with the staged-scale kernel (it would have
+    raised otherwise); repeated calls agree bit for bit."""
+    p = CASES[case]()
+    n = p.mesh.meta.get("box", (p.mesh.n,) * 3)
+    with _system(p, textbook=textbook) as S:
+        S.set_kuhn_grid(*n)
+        x = np.random.default_rng(3).standard_normal(S.n_rows).astype(np.float32)
+        y = S.kuhn_spmv_scaled32(x)
+        ya = S.spmv_scaled32(x)
+        assert np.linalg.norm(y - ya) <= 1e-5 * np.linalg.norm(ya)
+        np.testing.assert_array_equal(S.kuhn_spmv_scaled32(x), y)
+
+
 def test_two_level_refuses_a_changed_system(cuda):
     from multiscalefemsolver3d_b200.cells import FP64, Cells
     from multiscalefemsolver3d_b200.twolevel import TwoLevel
