@@ -446,8 +446,8 @@ int msfem_cells_order2_macro_system(msfem_cells_t c, int n_dofs, const int32_t* 
  * 2625-2640 with the triangle rule of :1482-1540 as written there), the bases' z components from
  * the lowest-numbered micro tetrahedron holding each point; summed per group in face order and
  * solved by Cholesky on the rows that carry mass (rows whose diagonal is at most n eps times the
- * largest diagonal -- the face bubbles, DOFs on no group face -- hold 0).  At most 16384 DOFs
- * per group.  values: host [group_dof_off[n_groups]][3] out, the projected value of each group
+ * largest diagonal -- the face bubbles, DOFs on no group face -- hold 0).  At most 4096 DOFs
+ * per group (one CTA's dense Cholesky).  values: host [group_dof_off[n_groups]][3] out, the projected value of each group
  * DOF. */
 int msfem_cells_order2_dirichlet(msfem_cells_t c, int n_dofs, const int32_t* cell_dofs, int n_vertices,
                                  const double* vertex_xyz, int n_faces, const int32_t* faces, int n_groups,

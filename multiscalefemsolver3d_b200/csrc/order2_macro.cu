@@ -33,7 +33,9 @@ namespace {
 // face table row: the cell, then the face's 9 DOF ids -- its 4 cycle vertices (a vertex's DOF id is
 // its vertex id), the edges between cycle nodes k and k + 1, the face
 constexpr int kFaceInts = 10;
-constexpr int kMaxGroupDofs = 16384;
+// a group's projection is one CTA's dense Cholesky (n^3 / 6 FMA): 4096 DOFs is a face of about
+// 32 x 32 macro cells and a few seconds
+constexpr int kMaxGroupDofs = 4096;
 
 // scalar CSR (row 3 d + a) from the block CSR of the DOF portrait: the blocks of DOF row d, each
 // as its three columns 3 e + b
@@ -226,10 +228,13 @@ __global__ void __launch_bounds__(256) k_o2_group_project(const int32_t* __restr
             if (act[i]) M[(int64_t)i * n + k] /= l;
         if (tid == 0) M[(int64_t)k * n + k] = l;
         __syncthreads();
-        const int m = n - k - 1;
-        for (int64_t t = tid; t < (int64_t)m * m; t += nt) {
-            const int i = k + 1 + (int)(t / m), j = k + 1 + (int)(t % m);
-            if (j <= i && act[i] && act[j]) M[(int64_t)i * n + j] -= M[(int64_t)i * n + k] * M[(int64_t)j * n + k];
+        // the lower trailing triangle: a warp per row, its lanes along the row
+        const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
+        for (int i = k + 1 + warp; i < n; i += nwarp) {
+            if (!act[i]) continue;
+            const double lik = M[(int64_t)i * n + k];
+            for (int j = k + 1 + lane; j <= i; j += 32)
+                if (act[j]) M[(int64_t)i * n + j] -= lik * M[(int64_t)j * n + k];
         }
         __syncthreads();
     }
