@@ -134,3 +134,25 @@ def test_order2_layout_rejects_shared_faces(lib):
     mid = np.nonzero(np.abs(vxyz[:, 2] - 0.5) < 1e-12)[0]
     with pytest.raises(ValueError):
         p2.dirichlet_layout(topo, [(mid, (0.0, 0.0, 0.0), (1, 1, 1))])
+
+
+def test_order2_layout_of_a_group_without_faces(lib):
+    """A Dirichlet group holding no whole face (one vertex; an edge's two vertices): its DOF list is
+    the vertices and edges it holds, it has no faces -- so its projection matrix is empty and the
+    projected values are 0, as the restatement's least-squares solve gives -- and its taken
+    components are still eliminated, in order."""
+    from multiscalefemsolver3d_b200 import order2 as p2
+    vxyz, cv, cm = o2.graded_cells(2, 1, 0.0)
+    topo = p2.macro_topology(cv, n_vertices=vxyz.shape[0])
+    a, b = (int(v) for v in topo.edges[0])
+    groups = [([a], (0.1, 0.2, 0.3), (1, 0, 1)), ([a, b], (0.0, 0.0, 0.0), (0, 1, 0))]
+    lay = p2.dirichlet_layout(topo, groups)
+    assert lay.faces.shape == (0, 10)
+    np.testing.assert_array_equal(lay.group_face_off, [0, 0, 0])
+    nv = topo.n_vertices
+    np.testing.assert_array_equal(lay.group_dofs, [a, min(a, b), max(a, b), nv + 0])
+    np.testing.assert_array_equal(lay.group_dof_off, [0, 1, 4])
+    # rows: group 0 takes x and z of a; group 1 takes y of a, b and the edge
+    want_rows = [3 * a, 3 * a + 2] + [3 * d + 1 for d in sorted([a, b])] + [3 * (nv + 0) + 1]
+    np.testing.assert_array_equal(lay.fixed_dofs, want_rows)
+    np.testing.assert_array_equal(lay.fixed_src, [0, 2] + [3 * k + 1 for k in (1, 2, 3)])
