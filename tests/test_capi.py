@@ -52,3 +52,20 @@ def test_null_handle_is_an_error_not_a_crash(lib):
     assert lib.msfem_system_destroy(None) == 0
     out = ctypes.c_void_p()
     assert lib.msfem_system_create(5, 10, None, 10, None, None, 0, ctypes.byref(out)) == -1
+
+
+def test_new_entry_points_refuse_null_handles(lib):
+    """The device-side Order2 macro calls and the scaled matrix-free product check their handles
+    before any CUDA call: a null handle is an argument error with a message, not a crash."""
+    out = ctypes.c_void_p()
+    assert lib.msfem_cells_order2_macro_system(None, 10, None, ctypes.byref(out)) == -1
+    assert b"msfem_cells_order2_macro_system" in lib.msfem_last_error()
+    assert lib.msfem_cells_order2_dirichlet(None, 10, None, 1, None, 0, None, 1, None, None, None, None,
+                                            None) == -1
+    assert b"msfem_cells_order2_dirichlet" in lib.msfem_last_error()
+    it, rel = ctypes.c_int32(), ctypes.c_double()
+    assert lib.msfem_cells_order2_macro_solve(None, 10, None, 1, None, 0, None, 0, None, None, None, None, 0,
+                                              None, None, 0, 1e-8, 10, None, ctypes.byref(it),
+                                              ctypes.byref(rel)) == -1
+    assert b"msfem_cells_order2_macro_solve" in lib.msfem_last_error()
+    assert lib.msfem_kuhn_spmv_scaled32(None, None, None, 0) == -1
